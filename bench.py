@@ -1,0 +1,378 @@
+"""Benchmark of the SimPL quadratic-solve hot path on B200.
+
+One step = one SimPL global iteration of the path on a 211k-cell synthetic
+netlist shaped like ISPD-2005 adaptec1 (211,000 movable cells, 221,000 nets,
+550 macros, 1,000 pads, 890 rows):
+  B2B assembly of the x and y systems (alpha 0.2, anchors given),
+  FP64 Jacobi-PCG of both systems from the warm start to rtol 1e-6,
+  HPWL of the solution, and its 512x512 density map + scaled overflow.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device time per step with inputs resident in HBM (CUDA events on
+the launching stream, L2 flushed between steps). `e2e` runs the same step
+through the C ABI in host-pointer mode from pinned host buffers, copies
+included. `--impl reference` times the reference's own CPU code (compiled
+from its sources into oracle/_ref) on the same workload with all host cores.
+With N > 1 (torchrun), every rank solves its own netlist (weak scaling, no
+data-path collective); timings are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GP CG solve ms/iter @210k cells: learned+FP32 PCG vs plain FP64 PCG, equal HPWL"
+UNIT = "ms/iter"
+ALPHA = 0.2
+TOL = 1e-6
+MAX_ITER = 100000
+GRID = 512
+WORKLOAD = ("simpl-global-iteration on synth211k (adaptec1-shaped): B2B build x+y (alpha 0.2), "
+            "FP64 Jacobi-PCG x+y warm-start to rtol 1e-6, HPWL, 512x512 density+overflow")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_workload(seed: int):
+    from ktplace_b200 import synth, netlist
+    raw = synth.generate(synth.spec_adaptec1_like(seed))
+    nl = netlist.flatten(raw)
+    x, y = synth.seed_positions(raw, nl.num_movable, 100 + seed)
+    ax, ay = synth.seed_positions(raw, nl.num_movable, 200 + seed)
+    return raw, nl, x, y, ax, ay
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---- CPU: the reference's own code --------------------------------------------
+
+def reference_steps(nl, x, y, ax, ay, steps: int, threads: int):
+    """Runs `steps` SimPL iterations of the path with the reference's code;
+    returns per-step seconds and the last step's results."""
+    import oracle
+    used = oracle.set_ref_threads(threads)
+    ref = oracle.RefDesign.from_netlist(nl)
+    ref.grid(GRID, 1.0)
+    out = []
+    res = None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref.build_b2b(x, y, ALPHA, ax, ay)
+        r = ref.solve(x, y, TOL, MAX_ITER)
+        h = ref.hpwl(r["x"], r["y"])
+        occ, ov = ref.occupancy_map(r["x"], r["y"], GRID * GRID)
+        out.append(time.perf_counter() - t0)
+        res = dict(iters=r["iters"], hpwl=h, overflow=ov)
+    return out, res, used
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libktref.so was not built"}))
+        return 0
+    raw, nl, x, y, ax, ay = make_workload(1)
+    threads = os.cpu_count() or 1
+    reference_steps(nl, x, y, ax, ay, max(1, min(args.warmup, 1)), threads)
+    times, res, used = reference_steps(nl, x, y, ax, ay, args.steps, threads)
+    ms = 1000.0 * statistics.mean(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, adaptec1 shape)",
+        "config": {"workload": WORKLOAD, "cells": nl.num_movable, "nets": nl.num_nets,
+                   "pins": nl.num_pins, "grid": GRID, "cg_iters": res["iters"]},
+        "cpu_baseline": {"value": ms, "unit": UNIT, "cores": used, "kind": "reference",
+                         "sample": f"{args.steps} full steps on {cpu_model()}"},
+        "e2e": {"value": ms, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "result": {"hpwl": res["hpwl"], "overflow": res["overflow"]},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---- GPU ------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def pcg_bytes(n: int, m: int, iters: int) -> float:
+    """Algorithmic bytes of one axis's PCG: start pass + iters iterations.
+    Iteration: val f64 + col i32 per entry, row_ptr, 14 n-vector passes (SpMV
+    reads diag and p and writes Ap; update reads x, p, r, Ap, diag and writes
+    x, r, z; direction reads z, p and writes p). Start: one SpMV on x plus
+    reading diag, x, rhs and writing r, z, p."""
+    it = 12.0 * m + 4.0 * (n + 1) + 8.0 * n * 14
+    start = 12.0 * m + 4.0 * (n + 1) + 8.0 * n * 6
+    return start + iters * it
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from ktplace_b200.gpu import Context
+    from ktplace_b200 import grid as kgrid
+    from ktplace_b200._lib import SolveInfo
+
+    raw, nl, x, y, ax, ay = make_workload(1 + rank)
+    fx, fy = nl.floors()
+    bg = kgrid.build_grid(nl, GRID, 1.0)
+    ctx = Context(local)
+    ctx.upload_netlist(nl)
+    ctx.set_grid(bg)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    n = nl.num_movable
+    with torch.cuda.stream(stream):
+        dx = torch.tensor(x, device=dev)
+        dy = torch.tensor(y, device=dev)
+        dax = torch.tensor(ax, device=dev)
+        day = torch.tensor(ay, device=dev)
+        wx = torch.empty_like(dx)
+        wy = torch.empty_like(dy)
+        info = torch.zeros(ctypes.sizeof(SolveInfo), dtype=torch.uint8, device=dev)
+        scal = torch.zeros(4, dtype=torch.float64, device=dev)
+        occ = torch.zeros(GRID * GRID, dtype=torch.float64, device=dev)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    ev_solve = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def step(timed_solve=None):
+        ctx.build_b2b_dev(dx, dy, ALPHA, dax, day, fx, fy)
+        wx.copy_(dx)
+        wy.copy_(dy)
+        if timed_solve is not None:
+            timed_solve[0].record(stream)
+        ctx.solve_dev(wx, wy, TOL, MAX_ITER, info)
+        if timed_solve is not None:
+            timed_solve[1].record(stream)
+        ctx.hpwl_dev(wx, wy, scal[0:1])
+        ctx.occupancy_dev(wx, wy, occ, scal[1:2])
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize(dev)
+
+    # ---- timed: device-resident inputs ------------------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    s_starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    s_ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = ctx.launches
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            step((s_starts[k], s_ends[k]))
+            ends[k].record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    launches = ctx.launches - launches0
+    clk = clocks.stop()
+    step_ms = [starts[k].elapsed_time(ends[k]) for k in range(args.steps)]
+    solve_ms = [s_starts[k].elapsed_time(s_ends[k]) for k in range(args.steps)]
+    total_ms = float(sum(step_ms))
+    inf = SolveInfo.from_buffer_copy(bytes(info.cpu().numpy()))
+    sx_n, sx_m = ctx.system_info(0)
+    _, sy_m = ctx.system_info(1)
+
+    # ---- e2e: host buffers through the C ABI, copies included --------------
+    pinned = [torch.tensor(a).pin_memory() for a in (x, y, ax, ay, x, y)]
+    hx, hy, hax, hay, px, py = (t.numpy() for t in pinned)
+    e2e_ms = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for k in range(max(1, args.steps // 2) + 1):
+        px[...] = hx  # fresh warm start for every step, outside the timed region
+        py[...] = hy
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        ctx.build_b2b(hx, hy, ALPHA, hax, hay, fx, fy)
+        ctx.solve(px, py, TOL, MAX_ITER, inplace=True)
+        ctx.hpwl(px, py)
+        ctx.occupancy(px, py, want_map=True)
+        e1.record(stream)
+        e1.synchronize()
+        if k > 0:
+            e2e_ms.append(e0.elapsed_time(e1))
+    h2d = 8 * n * (4 + 2 + 2 + 2)
+    d2h = 8 * n * 2 + 8 * GRID * GRID + 8 * 3 + ctypes.sizeof(SolveInfo)
+
+    # ---- max over ranks --------------------------------------------------------
+    vals = torch.tensor([total_ms, float(np.mean(e2e_ms)) * args.steps], dtype=torch.float64,
+                        device=dev)
+    if dist:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    total_max, e2e_total_max = float(vals[0]), float(vals[1])
+    value = total_max / (args.steps * world)
+    e2e_value = e2e_total_max / (args.steps * world)
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        solve_med = statistics.median(solve_ms)
+        byts = pcg_bytes(sx_n, sx_m, inf.iters_x) + pcg_bytes(sx_n, sy_m, inf.iters_y)
+        achieved = byts / (solve_med * 1e-3) / 1e9
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle
+            if oracle.ref_available():
+                threads = os.cpu_count() or 1
+                t, res, used = reference_steps(nl, x, y, ax, ay, args.cpu_sample_steps, threads)
+                cpu = {"value": 1000.0 * statistics.mean(t), "unit": UNIT, "cores": used,
+                       "kind": "reference",
+                       "sample": f"{args.cpu_sample_steps} full steps of the same workload "
+                                 f"(oracle/_ref, OpenMP on {cpu_model()})",
+                       "cg_iters": res["iters"]}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": value * world,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, adaptec1 shape; 256 MiB L2 flush between steps)",
+            "config": {"workload": WORKLOAD, "cells": n, "nets": nl.num_nets,
+                       "pins": nl.num_pins, "nnz_x": sx_m, "nnz_y": sy_m, "grid": GRID,
+                       "cg_iters": int(inf.iters), "l2": "flushed between steps",
+                       "parallelism": f"replicas x{world} (independent netlists)"},
+            "breakdown": {"solve_ms": solve_med, "solve_ms_per_cg_iter": solve_med / inf.iters,
+                          "other_ms": statistics.median(step_ms) - solve_med},
+            "roofline": {"kernel": "k_pcg (persistent cooperative PCG, x+y)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes": byts},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,202 @@
+/* ktplace_b200 — B200 (sm_100a) implementation of KTPlace's SimPL
+ * quadratic-solve hot path, exposed as a C ABI.
+ *
+ * The path has three parts, each replacing a reference function:
+ *   - B2B net-model assembly into CSR for x and y
+ *       LinearSystems::buildB2B   globalPlacer/simpl/simpl_lss.cc:11-114
+ *   - Jacobi-preconditioned CG on both systems
+ *       solveBothAxes             globalPlacer/simpl/simpl_lss.cc:203-290
+ *       (SparseSystem::multiply   globalPlacer/simpl/simpl_lss.h:49-57)
+ *   - HPWL and density-bin reductions
+ *       simplPlacer::Impl::getHpwl / getOccupancy / getOverflow
+ *                                 globalPlacer/simpl/simpl_placer.cc:256-297
+ *
+ * Conventions
+ *   - Every entry point returns KTG_OK (0) or a negative KTG_ERR_* code and
+ *     never throws; ktg_last_error() describes the last failure.
+ *   - One context owns one device, one CUDA stream and the device-resident
+ *     netlist and systems. A context is not thread-safe; use one per thread.
+ *   - Pointer mode (ktg_set_pointer_mode) decides how vector and scalar
+ *     arguments are read:
+ *       KTG_PTR_HOST   (default) host memory; the call copies in and out and
+ *                      returns after the results are in host memory.
+ *       KTG_PTR_DEVICE device memory of the context's device; the call only
+ *                      enqueues work on the context's stream (scalar outputs
+ *                      are written to device memory too).
+ *     Netlist, grid and system upload/download arguments are always host
+ *     memory.
+ *   - Indices are 0-based. Movable cell i is variable i; vertices include the
+ *     fixed cells. A netlist's pins must be deduplicated per cell and sorted
+ *     by cell id inside each net, as SimPL's collectNets does
+ *     (globalPlacer/simpl/simpl_dm.cc:49-63).
+ */
+#ifndef KTPLACE_B200_H
+#define KTPLACE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KTG_OK 0
+#define KTG_ERR_ARG (-1)      /* bad argument or size                       */
+#define KTG_ERR_CUDA (-2)     /* a CUDA runtime call failed                 */
+#define KTG_ERR_NOMEM (-3)    /* device or host allocation failed           */
+#define KTG_ERR_STATE (-4)    /* call out of order (e.g. no netlist yet)    */
+#define KTG_ERR_TIMEOUT (-5)  /* a bounded device wait gave up              */
+#define KTG_ERR_RANGE (-6)    /* a size exceeds the 32-bit index range      */
+
+#define KTG_PTR_HOST 0
+#define KTG_PTR_DEVICE 1
+
+#define KTG_AXIS_X 0
+#define KTG_AXIS_Y 1
+
+typedef struct ktg_ctx ktg_ctx;
+
+/* SimPL's flattened netlist (Netlist, globalPlacer/simpl/simpl_lss.h:27-36)
+ * as structure-of-arrays. All pointers are host memory. */
+typedef struct {
+    int64_t num_vertices;          /* V: movable + fixed                       */
+    int64_t num_movable;           /* n                                        */
+    int64_t num_nets;              /* N                                        */
+    const int32_t *mov_vertex;     /* [n]   vertex of variable i (movVertex)   */
+    const int32_t *var_of_vertex;  /* [V]   variable of vertex, -1 when fixed  */
+    const double *fixed_x;         /* [V]   vertex positions (fixedX)          */
+    const double *fixed_y;         /* [V]                                      */
+    const int64_t *net_start;      /* [N+1] pins of net k: [net_start[k], ..)  */
+    const int32_t *pin_cell;       /* [P]   vertex of each pin (NetPins.cells) */
+    const double *off_x;           /* [P]   lower-left-relative pin offsets    */
+    const double *off_y;           /* [P]                                      */
+    const double *net_weight;      /* [N]                                      */
+    const int64_t *pin_start;      /* [n+1] cell -> (net, pin) CSR (pinStart)  */
+    const int32_t *pin_net;        /* [Pm]  pinsOfCell[e].net                  */
+    const int32_t *pin_q;          /* [Pm]  pinsOfCell[e].pin                  */
+    const double *width;           /* [n]   movable cell widths (density)      */
+    const double *height;          /* [n]   movable cell heights               */
+} ktg_netlist_view;
+
+/* SimPL's bin grid (BinGrid, globalPlacer/simpl/simpl_grid.h:67-128). Bin
+ * (ix, iy) is element iy * nx + ix. Host memory. */
+typedef struct {
+    double origin_x;
+    double origin_y;
+    double dx;
+    double dy;
+    int64_t nx;
+    int64_t ny;
+    const double *avail;           /* [nx*ny] free row area per bin            */
+    double total_avail;
+    double density_limit;          /* g of getOverflow, clamped to [0.05, 1]   */
+} ktg_grid_view;
+
+/* Result of one ktg_solve: the last relative residual of each axis (the
+ * Residuals of solveBothAxes) and the number of lock-step iterations. */
+typedef struct {
+    double resid_x;
+    double resid_y;
+    int64_t iters;                 /* loop iterations, as the observer counts  */
+    int64_t iters_x;               /* steps taken by the x axis                */
+    int64_t iters_y;
+    int32_t status;                /* KTG_OK or KTG_ERR_TIMEOUT                */
+    int32_t live;                  /* bit 0 / bit 1: x / y still live at exit  */
+} ktg_solve_info;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Creates a context on CUDA device `device`. No reference counterpart: the
+ * reference owns its systems as members of simplPlacer::Impl
+ * (simpl_placer.cc:158-159). */
+int ktg_create(int device, ktg_ctx **out);
+void ktg_destroy(ktg_ctx *ctx);
+const char *ktg_last_error(const ktg_ctx *ctx);
+const char *ktg_version(void);
+
+/* Work is enqueued on `stream` (a cudaStream_t); NULL selects the context's
+ * own stream. */
+int ktg_set_stream(ktg_ctx *ctx, void *stream);
+int ktg_set_pointer_mode(ktg_ctx *ctx, int mode);
+
+/* ---- netlist ------------------------------------------------------------ */
+
+/* Uploads the netlist topology once per design; it stays device-resident.
+ * Replaces the per-call reads of Netlist in buildB2B and getHpwl
+ * (simpl_lss.cc:11-27, simpl_placer.cc:256-275). */
+int ktg_upload_netlist(ktg_ctx *ctx, const ktg_netlist_view *nl);
+
+/* ---- B2B assembly --------------------------------------------------------- */
+
+/* LinearSystems::buildB2B (simpl_lss.cc:11-114) for both axes. x, y, ax, ay
+ * hold the n movable positions and anchors; ax/ay may be NULL when
+ * alpha <= 0. floor_x/floor_y are the minimum edge lengths (LinearSystems::
+ * floorX/floorY). The systems stay on the device for ktg_solve. As a
+ * by-product the HPWL of (x, y) is computed (ktg_build_hpwl). */
+int ktg_build_b2b(ktg_ctx *ctx, const double *x, const double *y, double alpha,
+                  const double *ax, const double *ay, double floor_x, double floor_y);
+
+/* HPWL of the positions given to the last ktg_build_b2b, equal to
+ * simplPlacer::Impl::getHpwl on those positions (simpl_placer.cc:256-275).
+ * Pointer mode applies to `out`. */
+int ktg_build_hpwl(ktg_ctx *ctx, double *out);
+
+/* Size of the system of one axis: n rows and nnz stored off-diagonal entries
+ * (SparseSystem::size() and rowPtr.back(), simpl_lss.h:38-47). Host output;
+ * synchronises the stream. */
+int ktg_system_info(ktg_ctx *ctx, int axis, int64_t *n, int64_t *nnz);
+
+/* Copies one axis system to host memory in SparseSystem's layout
+ * (simpl_lss.h:38-43): row_ptr [n+1], col [nnz], val [nnz], diag [n],
+ * rhs [n]. Any pointer may be NULL to skip it. */
+int ktg_download_system(ktg_ctx *ctx, int axis, int64_t *row_ptr, int32_t *col, double *val,
+                        double *diag, double *rhs);
+
+/* Bound pins chosen for each net (the `extremes` of buildB2BAxis,
+ * simpl_lss.cc:32-45): lo[k], hi[k] are pin indices inside net k. Host. */
+int ktg_download_bound_pins(ktg_ctx *ctx, int axis, uint32_t *lo, uint32_t *hi);
+
+/* Installs a caller-built system for one axis (host memory), for solving
+ * systems assembled elsewhere (e.g. buildStar, simpl_lss.cc:116-201). */
+int ktg_upload_system(ktg_ctx *ctx, int axis, int64_t n, const int64_t *row_ptr,
+                      const int32_t *col, const double *val, const double *diag,
+                      const double *rhs);
+
+/* ---- PCG ------------------------------------------------------------------ */
+
+/* solveBothAxes (simpl_lss.cc:203-290) on the current systems: FP64
+ * Jacobi-PCG, x and y warm-started from and updated in place, stopping each
+ * axis when its recursive relative residual ||r||/||b|| <= tol or after
+ * max_iter steps, and deactivating an axis on non-positive p.Ap or r.z.
+ * hist_x/hist_y (may be NULL) receive the residuals after each loop
+ * iteration, as the IterateObserver sees them (capacity hist_cap).
+ * Pointer mode applies to x, y, info, hist_x, hist_y. */
+int ktg_solve(ktg_ctx *ctx, double *x, double *y, double tol, int64_t max_iter,
+              ktg_solve_info *info, double *hist_x, double *hist_y, int64_t hist_cap);
+
+/* ---- HPWL and density ---------------------------------------------------- */
+
+/* simplPlacer::Impl::getHpwl (simpl_placer.cc:256-275). */
+int ktg_hpwl(ktg_ctx *ctx, const double *x, const double *y, double *out);
+
+/* Installs the bin grid used by ktg_occupancy (host memory). */
+int ktg_set_grid(ktg_ctx *ctx, const ktg_grid_view *grid);
+
+/* Impl::getOccupancy then Impl::getOverflow (simpl_placer.cc:282-297):
+ * centre-binned movable area per bin (occ, [nx*ny], may be NULL) and the
+ * scaled overflow. Bin sums are accumulated in 64-bit fixed point, so the map
+ * is identical from run to run. */
+int ktg_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ,
+                  double *overflow);
+
+/* ---- introspection -------------------------------------------------------- */
+
+/* Number of kernels this context has launched since creation (all entry
+ * points). */
+int64_t ktg_launch_count(const ktg_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KTPLACE_B200_H */

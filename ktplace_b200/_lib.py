@@ -1,0 +1,104 @@
+"""ctypes binding of the C ABI in include/ktplace_b200.h.
+
+Loads ``_build/libktplace_b200.so`` (built in-tree by ``ktplace_b200.build``).
+There is no fallback: if the library is missing or cannot be loaded, every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libktplace_b200.so")
+
+KTG_OK = 0
+KTG_ERR_ARG = -1
+KTG_ERR_CUDA = -2
+KTG_ERR_NOMEM = -3
+KTG_ERR_STATE = -4
+KTG_ERR_TIMEOUT = -5
+KTG_ERR_RANGE = -6
+KTG_PTR_HOST = 0
+KTG_PTR_DEVICE = 1
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+class NetlistView(ctypes.Structure):
+    _fields_ = [("num_vertices", ctypes.c_int64), ("num_movable", ctypes.c_int64),
+                ("num_nets", ctypes.c_int64), ("mov_vertex", _i32p), ("var_of_vertex", _i32p),
+                ("fixed_x", _f64p), ("fixed_y", _f64p), ("net_start", _i64p),
+                ("pin_cell", _i32p), ("off_x", _f64p), ("off_y", _f64p),
+                ("net_weight", _f64p), ("pin_start", _i64p), ("pin_net", _i32p),
+                ("pin_q", _i32p), ("width", _f64p), ("height", _f64p)]
+
+
+class GridView(ctypes.Structure):
+    _fields_ = [("origin_x", ctypes.c_double), ("origin_y", ctypes.c_double),
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("nx", ctypes.c_int64),
+                ("ny", ctypes.c_int64), ("avail", _f64p), ("total_avail", ctypes.c_double),
+                ("density_limit", ctypes.c_double)]
+
+
+class SolveInfo(ctypes.Structure):
+    _fields_ = [("resid_x", ctypes.c_double), ("resid_y", ctypes.c_double),
+                ("iters", ctypes.c_int64), ("iters_x", ctypes.c_int64),
+                ("iters_y", ctypes.c_int64), ("status", ctypes.c_int32),
+                ("live", ctypes.c_int32)]
+
+
+# (name, restype, argtypes) of every entry point in include/ktplace_b200.h
+SIGNATURES = [
+    ("ktg_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ktg_destroy", None, [_vp]),
+    ("ktg_last_error", ctypes.c_char_p, [_vp]),
+    ("ktg_version", ctypes.c_char_p, []),
+    ("ktg_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("ktg_set_pointer_mode", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("ktg_upload_netlist", ctypes.c_int, [_vp, ctypes.POINTER(NetlistView)]),
+    ("ktg_build_b2b", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _vp, _vp, ctypes.c_double,
+                                     ctypes.c_double]),
+    ("ktg_build_hpwl", ctypes.c_int, [_vp, _vp]),
+    ("ktg_system_info", ctypes.c_int, [_vp, ctypes.c_int, _i64p, _i64p]),
+    ("ktg_download_system", ctypes.c_int, [_vp, ctypes.c_int, _i64p, _i32p, _f64p, _f64p,
+                                           _f64p]),
+    ("ktg_download_bound_pins", ctypes.c_int, [_vp, ctypes.c_int, _u32p, _u32p]),
+    ("ktg_upload_system", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64, _i64p, _i32p,
+                                         _f64p, _f64p, _f64p]),
+    ("ktg_solve", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int64, _vp, _vp, _vp,
+                                 ctypes.c_int64]),
+    ("ktg_hpwl", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("ktg_set_grid", ctypes.c_int, [_vp, ctypes.POINTER(GridView)]),
+    ("ktg_occupancy", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("ktg_launch_count", ctypes.c_int64, [_vp]),
+]
+
+_lib = None
+
+
+def load():
+    """Loads the CUDA library; raises if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"ktplace_b200 CUDA library not built: {LIB_PATH} is missing "
+                "(run `python -m ktplace_b200.build`)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class KtgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ktplace_b200 error {code}: {msg}")
+        self.code = code

@@ -1,0 +1,633 @@
+// C ABI of ktplace_b200: context management, netlist/grid upload, and the
+// entry points declared in include/ktplace_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ktg_context.h"
+#include "ktplace_b200.h"
+
+namespace ktg {
+
+int set_error(ktg_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_check(ktg_ctx *ctx, cudaError_t e, const char *what) {
+    return set_error(ctx, KTG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace ktg
+
+namespace {
+
+using ktg::set_error;
+
+template <typename T>
+int dev_alloc(ktg_ctx *c, T **p, int64_t count) {
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    if (count <= 0) count = 1;
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * count);
+    if (e != cudaSuccess) return ktg::cuda_check(c, e, "cudaMalloc");
+    return KTG_OK;
+}
+
+template <typename T>
+void dev_free(T *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+template <typename T>
+int upload(ktg_ctx *c, T *dst, const T *src, int64_t count) {
+    if (count <= 0) return KTG_OK;
+    KTG_CUDA(c, cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyHostToDevice, c->stream));
+    return KTG_OK;
+}
+
+int sync(ktg_ctx *c) {
+    KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KTG_OK;
+}
+
+// Reads the device status word; returns its KTG code (0 when fine).
+int device_status(ktg_ctx *c) {
+    KTG_CUDA(c, cudaMemcpyAsync(c->h_status, c->status, sizeof(int), cudaMemcpyDeviceToHost,
+                                c->stream));
+    KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return *c->h_status;
+}
+
+int set_device(ktg_ctx *c) {
+    KTG_CUDA(c, cudaSetDevice(c->device));
+    return KTG_OK;
+}
+
+void free_netlist(ktg_ctx *c) {
+    dev_free(c->var_of_vertex);
+    dev_free(c->fixed_x);
+    dev_free(c->fixed_y);
+    dev_free(c->net_start);
+    dev_free(c->pin_cell);
+    dev_free(c->pin_var);
+    dev_free(c->off_x);
+    dev_free(c->off_y);
+    dev_free(c->net_base);
+    dev_free(c->net_mov);
+    dev_free(c->pin_start);
+    dev_free(c->pin_ref);
+    dev_free(c->width);
+    dev_free(c->height);
+    dev_free(c->area);
+    dev_free(c->row_cnt);
+    dev_free(c->block_sum);
+    c->have_netlist = false;
+}
+
+void free_systems(ktg_ctx *c) {
+    for (auto &s : c->sys) {
+        dev_free(s.row_ptr);
+        dev_free(s.col);
+        dev_free(s.val);
+        dev_free(s.diag);
+        dev_free(s.rhs);
+        dev_free(s.lo);
+        dev_free(s.hi);
+        dev_free(s.r);
+        dev_free(s.z);
+        dev_free(s.p);
+        dev_free(s.ap);
+    }
+    dev_free(c->x);
+    dev_free(c->y);
+    dev_free(c->ax);
+    dev_free(c->ay);
+    c->sys_cap_n = 0;
+    c->sys_cap_nnz = 0;
+    c->stage_cap = 0;
+    c->have_system = false;
+    c->axis_valid[0] = c->axis_valid[1] = false;
+}
+
+// Makes room for systems of `rows` rows and `nnz` entries per axis and for
+// per-net bound pins of the current netlist.
+int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
+    int rc;
+    if (rows > c->sys_cap_n) {
+        for (auto &s : c->sys) {
+            if ((rc = dev_alloc(c, &s.row_ptr, rows + 1))) return rc;
+            if ((rc = dev_alloc(c, &s.diag, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.rhs, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.r, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.z, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.p, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.ap, rows))) return rc;
+        }
+        if ((rc = dev_alloc(c, &c->x, rows))) return rc;
+        if ((rc = dev_alloc(c, &c->y, rows))) return rc;
+        if ((rc = dev_alloc(c, &c->ax, rows))) return rc;
+        if ((rc = dev_alloc(c, &c->ay, rows))) return rc;
+        c->sys_cap_n = rows;
+        c->stage_cap = rows;
+    }
+    if (nnz > c->sys_cap_nnz) {
+        for (auto &s : c->sys) {
+            if ((rc = dev_alloc(c, &s.col, nnz))) return rc;
+            if ((rc = dev_alloc(c, &s.val, nnz))) return rc;
+        }
+        c->sys_cap_nnz = nnz;
+    }
+    return KTG_OK;
+}
+
+int reserve_partials(ktg_ctx *c, int64_t count) {
+    if (count > c->partials_cap) {
+        int rc = dev_alloc(c, &c->partials, count);
+        if (rc) return rc;
+        c->partials_cap = count;
+    }
+    return KTG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ktg_version(void) { return "ktplace_b200 0.1 (sm_100a)"; }
+
+int ktg_create(int device, ktg_ctx **out) {
+    if (out == nullptr) return KTG_ERR_ARG;
+    *out = nullptr;
+    ktg_ctx *c = new (std::nothrow) ktg_ctx();
+    if (c == nullptr) return KTG_ERR_NOMEM;
+    c->device = device;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device < 0 || device >= count) {
+        delete c;
+        return KTG_ERR_CUDA;
+    }
+    int rc = KTG_OK;
+    auto fail = [&](int code) {
+        ktg_destroy(c);
+        return code;
+    };
+    if ((rc = set_device(c))) return fail(rc);
+    if (cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return fail(KTG_ERR_CUDA);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (!coop) return fail(KTG_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(KTG_ERR_CUDA);
+    c->stream = c->own_stream;
+    if ((rc = dev_alloc(c, &c->counters, 8))) return fail(rc);
+    if ((rc = dev_alloc(c, &c->status, 1))) return fail(rc);
+    if ((rc = dev_alloc(c, &c->scalars, 8))) return fail(rc);
+    if ((rc = dev_alloc(c, &c->info_dev, 1))) return fail(rc);
+    if ((rc = dev_alloc(c, &c->nnz_dev, 2))) return fail(rc);
+    if ((rc = reserve_partials(c, 16384))) return fail(rc);
+    if (cudaMemset(c->counters, 0, 8 * sizeof(unsigned)) != cudaSuccess) return fail(KTG_ERR_CUDA);
+    if (cudaMemset(c->status, 0, sizeof(int)) != cudaSuccess) return fail(KTG_ERR_CUDA);
+    if (cudaMallocHost(&c->h_scalars, 8 * sizeof(double)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
+    if (cudaMallocHost(&c->h_info, sizeof(ktg_solve_info)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
+    if (cudaMallocHost(&c->h_nnz, 2 * sizeof(int64_t)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
+    if (cudaMallocHost(&c->h_status, sizeof(int)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
+    *out = c;
+    return KTG_OK;
+}
+
+void ktg_destroy(ktg_ctx *c) {
+    if (c == nullptr) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_netlist(c);
+    free_systems(c);
+    dev_free(c->partials);
+    dev_free(c->counters);
+    dev_free(c->status);
+    dev_free(c->scalars);
+    dev_free(c->info_dev);
+    dev_free(c->hist_dev);
+    dev_free(c->nnz_dev);
+    dev_free(c->avail);
+    dev_free(c->occ_fx);
+    dev_free(c->occ);
+    if (c->h_scalars) cudaFreeHost(c->h_scalars);
+    if (c->h_info) cudaFreeHost(c->h_info);
+    if (c->h_nnz) cudaFreeHost(c->h_nnz);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+const char *ktg_last_error(const ktg_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int ktg_set_stream(ktg_ctx *c, void *stream) {
+    if (!c) return KTG_ERR_ARG;
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    return KTG_OK;
+}
+
+int ktg_set_pointer_mode(ktg_ctx *c, int mode) {
+    if (!c || (mode != KTG_PTR_HOST && mode != KTG_PTR_DEVICE)) return KTG_ERR_ARG;
+    c->ptr_mode = mode;
+    return KTG_OK;
+}
+
+int64_t ktg_launch_count(const ktg_ctx *c) { return c ? c->launches : 0; }
+
+int ktg_upload_netlist(ktg_ctx *c, const ktg_netlist_view *nl) {
+    if (!c || !nl) return KTG_ERR_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int64_t V = nl->num_vertices, n = nl->num_movable, N = nl->num_nets;
+    if (V < 0 || n < 0 || N < 0 || n > V) return set_error(c, KTG_ERR_ARG, "negative sizes");
+    if ((V > 0 && (!nl->var_of_vertex || !nl->fixed_x || !nl->fixed_y)) ||
+        (n > 0 && (!nl->mov_vertex || !nl->pin_start || !nl->width || !nl->height)) ||
+        !nl->net_start || (N > 0 && !nl->net_weight))
+        return set_error(c, KTG_ERR_ARG, "missing netlist array");
+    const int64_t P = nl->net_start[N];
+    const int64_t Pm = n > 0 ? nl->pin_start[n] : 0;
+    if (P < 0 || Pm < 0 || Pm > P) return set_error(c, KTG_ERR_ARG, "bad pin counts");
+    if (P > 0 && (!nl->pin_cell || !nl->off_x || !nl->off_y))
+        return set_error(c, KTG_ERR_ARG, "missing pin arrays");
+    if (Pm > 0 && (!nl->pin_net || !nl->pin_q)) return set_error(c, KTG_ERR_ARG, "missing pin refs");
+    const int64_t lim = 0x7fffffffll;
+    if (V > lim || P > lim || N > lim || 2 * n > lim)
+        return set_error(c, KTG_ERR_RANGE, "netlist exceeds 32-bit indices");
+
+    // Validate indices on the host once, so no kernel can read out of bounds.
+    for (int64_t k = 0; k < N; ++k)
+        if (nl->net_start[k + 1] < nl->net_start[k])
+            return set_error(c, KTG_ERR_ARG, "net_start not monotone");
+    for (int64_t i = 0; i < n; ++i) {
+        if (nl->pin_start[i + 1] < nl->pin_start[i])
+            return set_error(c, KTG_ERR_ARG, "pin_start not monotone");
+        const int32_t v = nl->mov_vertex[i];
+        if (v < 0 || v >= V || nl->var_of_vertex[v] != i)
+            return set_error(c, KTG_ERR_ARG, "mov_vertex / var_of_vertex disagree");
+    }
+    std::vector<int32_t> pin_var(P), net_mov(N, 0);
+    std::vector<int32_t> net_start32(N + 1), pin_start32(n + 1);
+    std::vector<double> net_base(N);
+    std::vector<int2> pin_ref(Pm);
+    for (int64_t p = 0; p < P; ++p) {
+        const int32_t cell = nl->pin_cell[p];
+        if (cell < 0 || cell >= V) return set_error(c, KTG_ERR_ARG, "pin_cell out of range");
+        const int32_t var = nl->var_of_vertex[cell];
+        if (var >= n) return set_error(c, KTG_ERR_ARG, "var_of_vertex out of range");
+        pin_var[p] = var < 0 ? -1 : var;
+    }
+    int64_t cap = 0;
+    for (int64_t k = 0; k < N; ++k) {
+        net_start32[k] = static_cast<int32_t>(nl->net_start[k]);
+        const int64_t deg = nl->net_start[k + 1] - nl->net_start[k];
+        // simpl_lss.cc:68: base = weight / (cells.size() - 1), per net
+        net_base[k] = nl->net_weight[k] / static_cast<double>(static_cast<uint64_t>(deg - 1));
+        int32_t m = 0;
+        for (int64_t p = nl->net_start[k]; p < nl->net_start[k + 1]; ++p) m += pin_var[p] >= 0;
+        net_mov[k] = m;
+        // Bound rows (2) get m-1 movable ends, the others at most 2 each.
+        if (m > 0) cap += 4 * static_cast<int64_t>(m);
+    }
+    net_start32[N] = static_cast<int32_t>(P);
+    for (int64_t i = 0; i <= n; ++i) pin_start32[i] = static_cast<int32_t>(nl->pin_start[i]);
+    for (int64_t e = 0; e < Pm; ++e) {
+        const int32_t k = nl->pin_net[e], q = nl->pin_q[e];
+        if (k < 0 || k >= N || q < 0 || q >= nl->net_start[k + 1] - nl->net_start[k])
+            return set_error(c, KTG_ERR_ARG, "pin_ref out of range");
+        pin_ref[e] = make_int2(k, q);
+    }
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t e = nl->pin_start[i]; e < nl->pin_start[i + 1]; ++e) {
+            const int64_t p = nl->net_start[nl->pin_net[e]] + nl->pin_q[e];
+            if (pin_var[p] != i) return set_error(c, KTG_ERR_ARG, "pin_ref does not point to its cell");
+        }
+    if (cap > lim) return set_error(c, KTG_ERR_RANGE, "B2B systems exceed 32-bit indices");
+    std::vector<double> area(n);
+    double total_area = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        area[i] = nl->width[i] * nl->height[i];
+        total_area += std::fabs(area[i]);
+    }
+    // Fixed-point shift for the density map: total area * 2^s < 2^61.
+    int s = 60;
+    if (total_area > 0.0) s = std::min(60, 61 - static_cast<int>(std::ceil(std::log2(total_area + 1.0))));
+    s = std::max(s, 0);
+    c->fx_scale = std::ldexp(1.0, s);
+
+    KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_netlist(c);
+    free_systems(c);
+    c->V = V;
+    c->n = n;
+    c->N = N;
+    c->P = P;
+    c->Pm = Pm;
+    c->cap_nnz = std::max<int64_t>(cap, 1);
+    if ((rc = dev_alloc(c, &c->var_of_vertex, V))) return rc;
+    if ((rc = dev_alloc(c, &c->fixed_x, V))) return rc;
+    if ((rc = dev_alloc(c, &c->fixed_y, V))) return rc;
+    if ((rc = dev_alloc(c, &c->net_start, N + 1))) return rc;
+    if ((rc = dev_alloc(c, &c->pin_cell, P))) return rc;
+    if ((rc = dev_alloc(c, &c->pin_var, P))) return rc;
+    if ((rc = dev_alloc(c, &c->off_x, P))) return rc;
+    if ((rc = dev_alloc(c, &c->off_y, P))) return rc;
+    if ((rc = dev_alloc(c, &c->net_base, N))) return rc;
+    if ((rc = dev_alloc(c, &c->net_mov, N))) return rc;
+    if ((rc = dev_alloc(c, &c->pin_start, n + 1))) return rc;
+    if ((rc = dev_alloc(c, &c->pin_ref, Pm))) return rc;
+    if ((rc = dev_alloc(c, &c->width, n))) return rc;
+    if ((rc = dev_alloc(c, &c->height, n))) return rc;
+    if ((rc = dev_alloc(c, &c->area, n))) return rc;
+    const int64_t bpa = (n + 255) / 256;
+    if ((rc = dev_alloc(c, &c->row_cnt, 2 * n))) return rc;
+    if ((rc = dev_alloc(c, &c->block_sum, 2 * bpa))) return rc;
+    if ((rc = reserve_systems(c, n, c->cap_nnz))) return rc;
+    for (auto &s2 : c->sys) {
+        if ((rc = dev_alloc(c, &s2.lo, N))) return rc;
+        if ((rc = dev_alloc(c, &s2.hi, N))) return rc;
+    }
+    if ((rc = reserve_partials(c, (N + 255) / 256 + 64))) return rc;
+    if ((rc = upload(c, c->var_of_vertex, nl->var_of_vertex, V))) return rc;
+    if ((rc = upload(c, c->fixed_x, nl->fixed_x, V))) return rc;
+    if ((rc = upload(c, c->fixed_y, nl->fixed_y, V))) return rc;
+    if ((rc = upload(c, c->net_start, net_start32.data(), N + 1))) return rc;
+    if ((rc = upload(c, c->pin_cell, nl->pin_cell, P))) return rc;
+    if ((rc = upload(c, c->pin_var, pin_var.data(), P))) return rc;
+    if ((rc = upload(c, c->off_x, nl->off_x, P))) return rc;
+    if ((rc = upload(c, c->off_y, nl->off_y, P))) return rc;
+    if ((rc = upload(c, c->net_base, net_base.data(), N))) return rc;
+    if ((rc = upload(c, c->net_mov, net_mov.data(), N))) return rc;
+    if ((rc = upload(c, c->pin_start, pin_start32.data(), n + 1))) return rc;
+    if ((rc = upload(c, c->pin_ref, pin_ref.data(), Pm))) return rc;
+    if ((rc = upload(c, c->width, nl->width, n))) return rc;
+    if ((rc = upload(c, c->height, nl->height, n))) return rc;
+    if ((rc = upload(c, c->area, area.data(), n))) return rc;
+    if ((rc = sync(c))) return rc;
+    c->have_netlist = true;
+    c->have_system = false;
+    c->sys_n = n;
+    return KTG_OK;
+}
+
+int ktg_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha, const double *ax,
+                  const double *ay, double floor_x, double floor_y) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");
+    if (c->n > 0 && (!x || !y)) return set_error(c, KTG_ERR_ARG, "null positions");
+    if (alpha > 0.0 && c->n > 0 && (!ax || !ay)) return set_error(c, KTG_ERR_ARG, "null anchors");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = reserve_systems(c, c->n, c->cap_nnz))) return rc;
+    const double *dx = x, *dy = y, *dax = ax, *day = ay;
+    if (c->ptr_mode == KTG_PTR_HOST) {
+        if ((rc = upload(c, c->x, x, c->n))) return rc;
+        if ((rc = upload(c, c->y, y, c->n))) return rc;
+        dx = c->x;
+        dy = c->y;
+        if (alpha > 0.0) {
+            if ((rc = upload(c, c->ax, ax, c->n))) return rc;
+            if ((rc = upload(c, c->ay, ay, c->n))) return rc;
+            dax = c->ax;
+            day = c->ay;
+        }
+    }
+    if ((rc = ktg::launch_build_b2b(c, dx, dy, alpha, dax, day, floor_x, floor_y))) return rc;
+    c->sys_n = c->n;
+    c->have_system = true;
+    c->axis_valid[0] = c->axis_valid[1] = true;
+    if (c->ptr_mode == KTG_PTR_HOST) {
+        const int st = device_status(c);
+        if (st < 0) return st;
+        if (st != 0) return set_error(c, st, "B2B system exceeds its capacity");
+    }
+    return KTG_OK;
+}
+
+int ktg_build_hpwl(ktg_ctx *c, double *out) {
+    if (!c || !out) return KTG_ERR_ARG;
+    if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no B2B build yet");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (c->ptr_mode == KTG_PTR_DEVICE) {
+        KTG_CUDA(c, cudaMemcpyAsync(out, c->scalars + 0, sizeof(double), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+        return KTG_OK;
+    }
+    KTG_CUDA(c, cudaMemcpyAsync(c->h_scalars, c->scalars, sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    if ((rc = sync(c))) return rc;
+    *out = c->h_scalars[0];
+    return KTG_OK;
+}
+
+int ktg_system_info(ktg_ctx *c, int axis, int64_t *n, int64_t *nnz) {
+    if (!c || (axis != 0 && axis != 1)) return KTG_ERR_ARG;
+    if (!c->axis_valid[axis]) return set_error(c, KTG_ERR_STATE, "no system for this axis");
+    int rc = set_device(c);
+    if (rc) return rc;
+    int32_t m = 0;
+    KTG_CUDA(c, cudaMemcpyAsync(&m, c->sys[axis].row_ptr + c->sys_n, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    if (n) *n = c->sys_n;
+    if (nnz) *nnz = m;
+    return KTG_OK;
+}
+
+int ktg_download_system(ktg_ctx *c, int axis, int64_t *row_ptr, int32_t *col, double *val,
+                        double *diag, double *rhs) {
+    int64_t n = 0, m = 0;
+    int rc = ktg_system_info(c, axis, &n, &m);
+    if (rc) return rc;
+    const ktg::AxisSystem &s = c->sys[axis];
+    std::vector<int32_t> rp(n + 1);
+    KTG_CUDA(c, cudaMemcpy(rp.data(), s.row_ptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost));
+    if (row_ptr)
+        for (int64_t i = 0; i <= n; ++i) row_ptr[i] = rp[i];
+    if (col && m) KTG_CUDA(c, cudaMemcpy(col, s.col, sizeof(int32_t) * m, cudaMemcpyDeviceToHost));
+    if (val && m) KTG_CUDA(c, cudaMemcpy(val, s.val, sizeof(double) * m, cudaMemcpyDeviceToHost));
+    if (diag && n) KTG_CUDA(c, cudaMemcpy(diag, s.diag, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (rhs && n) KTG_CUDA(c, cudaMemcpy(rhs, s.rhs, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return KTG_OK;
+}
+
+int ktg_download_bound_pins(ktg_ctx *c, int axis, uint32_t *lo, uint32_t *hi) {
+    if (!c || (axis != 0 && axis != 1)) return KTG_ERR_ARG;
+    if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = sync(c))) return rc;
+    if (lo && c->N)
+        KTG_CUDA(c, cudaMemcpy(lo, c->sys[axis].lo, sizeof(uint32_t) * c->N, cudaMemcpyDeviceToHost));
+    if (hi && c->N)
+        KTG_CUDA(c, cudaMemcpy(hi, c->sys[axis].hi, sizeof(uint32_t) * c->N, cudaMemcpyDeviceToHost));
+    return KTG_OK;
+}
+
+int ktg_upload_system(ktg_ctx *c, int axis, int64_t n, const int64_t *row_ptr, const int32_t *col,
+                      const double *val, const double *diag, const double *rhs) {
+    if (!c || (axis != 0 && axis != 1) || n < 0 || !row_ptr) return KTG_ERR_ARG;
+    if (n > 0 && (!diag || !rhs)) return KTG_ERR_ARG;
+    const int64_t m = row_ptr[n];
+    if (m < 0 || m > 0x7fffffffll || n > 0x3fffffffll)
+        return set_error(c, KTG_ERR_RANGE, "system exceeds 32-bit indices");
+    if (m > 0 && (!col || !val)) return KTG_ERR_ARG;
+    std::vector<int32_t> rp(n + 1);
+    for (int64_t i = 0; i <= n; ++i) {
+        if (row_ptr[i] < 0 || (i > 0 && row_ptr[i] < row_ptr[i - 1]))
+            return set_error(c, KTG_ERR_ARG, "row_ptr not monotone");
+        rp[i] = static_cast<int32_t>(row_ptr[i]);
+    }
+    for (int64_t e = 0; e < m; ++e)
+        if (col[e] < 0 || col[e] >= n) return set_error(c, KTG_ERR_ARG, "col out of range");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = sync(c))) return rc;
+    if ((rc = reserve_systems(c, n, std::max<int64_t>(m, c->sys_cap_nnz)))) return rc;
+    ktg::AxisSystem &s = c->sys[axis];
+    if ((rc = upload(c, s.row_ptr, rp.data(), n + 1))) return rc;
+    if ((rc = upload(c, s.col, col, m))) return rc;
+    if ((rc = upload(c, s.val, val, m))) return rc;
+    if ((rc = upload(c, s.diag, diag, n))) return rc;
+    if ((rc = upload(c, s.rhs, rhs, n))) return rc;
+    if ((rc = sync(c))) return rc;
+    if (n != c->sys_n) c->axis_valid[1 - axis] = false;
+    c->axis_valid[axis] = true;
+    c->sys_n = n;
+    c->have_system = c->axis_valid[0] && c->axis_valid[1];
+    return KTG_OK;
+}
+
+int ktg_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter, ktg_solve_info *info,
+              double *hist_x, double *hist_y, int64_t hist_cap) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no system to solve");
+    if (c->sys_n > 0 && (!x || !y)) return set_error(c, KTG_ERR_ARG, "null positions");
+    if (max_iter < 0 || hist_cap < 0) return set_error(c, KTG_ERR_ARG, "negative count");
+    if (hist_cap > 0 && !hist_x && !hist_y) hist_cap = 0;
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int64_t n = c->sys_n;
+    if (c->ptr_mode == KTG_PTR_DEVICE) {
+        if ((rc = ktg::launch_solve(c, x, y, tol, max_iter, info ? info : c->info_dev, hist_x,
+                                    hist_y, hist_cap)))
+            return rc;
+        return KTG_OK;
+    }
+    if (hist_cap > c->hist_cap_dev) {
+        if ((rc = dev_alloc(c, &c->hist_dev, 2 * hist_cap))) return rc;
+        c->hist_cap_dev = hist_cap;
+    }
+    if ((rc = upload(c, c->x, x, n))) return rc;
+    if ((rc = upload(c, c->y, y, n))) return rc;
+    if ((rc = ktg::launch_solve(c, c->x, c->y, tol, max_iter, c->info_dev,
+                                hist_x ? c->hist_dev : nullptr,
+                                hist_y ? c->hist_dev + hist_cap : nullptr, hist_cap)))
+        return rc;
+    KTG_CUDA(c, cudaMemcpyAsync(x, c->x, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    KTG_CUDA(c, cudaMemcpyAsync(y, c->y, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    KTG_CUDA(c, cudaMemcpyAsync(c->h_info, c->info_dev, sizeof(ktg_solve_info),
+                                cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    const ktg_solve_info inf = *c->h_info;
+    if (info) *info = inf;
+    if (inf.status != KTG_OK) return set_error(c, inf.status, "PCG barrier wait timed out");
+    if (hist_cap > 0) {
+        const int64_t k = std::min<int64_t>(inf.iters, hist_cap);
+        if (hist_x && k)
+            KTG_CUDA(c, cudaMemcpy(hist_x, c->hist_dev, sizeof(double) * k, cudaMemcpyDeviceToHost));
+        if (hist_y && k)
+            KTG_CUDA(c, cudaMemcpy(hist_y, c->hist_dev + hist_cap, sizeof(double) * k,
+                                   cudaMemcpyDeviceToHost));
+    }
+    return KTG_OK;
+}
+
+int ktg_hpwl(ktg_ctx *c, const double *x, const double *y, double *out) {
+    if (!c || !out) return KTG_ERR_ARG;
+    if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");
+    if (c->n > 0 && (!x || !y)) return set_error(c, KTG_ERR_ARG, "null positions");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (c->ptr_mode == KTG_PTR_DEVICE) return ktg::launch_hpwl(c, x, y, out);
+    if ((rc = reserve_systems(c, c->n, 0))) return rc;
+    if ((rc = upload(c, c->x, x, c->n))) return rc;
+    if ((rc = upload(c, c->y, y, c->n))) return rc;
+    if ((rc = ktg::launch_hpwl(c, c->x, c->y, c->scalars + 1))) return rc;
+    KTG_CUDA(c, cudaMemcpyAsync(c->h_scalars + 1, c->scalars + 1, sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    *out = c->h_scalars[1];
+    return KTG_OK;
+}
+
+int ktg_set_grid(ktg_ctx *c, const ktg_grid_view *g) {
+    if (!c || !g) return KTG_ERR_ARG;
+    if (g->nx <= 0 || g->ny <= 0 || !g->avail || !(g->dx > 0.0) || !(g->dy > 0.0))
+        return set_error(c, KTG_ERR_ARG, "bad grid");
+    if (g->nx * g->ny > 0x7fffffffll || g->nx > 0x7fffffffll || g->ny > 0x7fffffffll)
+        return set_error(c, KTG_ERR_RANGE, "grid exceeds 32-bit indices");
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int64_t bins = g->nx * g->ny;
+    if ((rc = sync(c))) return rc;
+    if (bins > c->bins_cap) {
+        if ((rc = dev_alloc(c, &c->avail, bins))) return rc;
+        if ((rc = dev_alloc(c, &c->occ_fx, bins))) return rc;
+        if ((rc = dev_alloc(c, &c->occ, bins))) return rc;
+        c->bins_cap = bins;
+    }
+    if ((rc = reserve_partials(c, (bins + 255) / 256 + 64))) return rc;
+    KTG_CUDA(c, cudaMemsetAsync(c->occ_fx, 0, sizeof(unsigned long long) * bins, c->stream));
+    if ((rc = upload(c, c->avail, g->avail, bins))) return rc;
+    if ((rc = sync(c))) return rc;
+    c->nx = g->nx;
+    c->ny = g->ny;
+    c->origin_x = g->origin_x;
+    c->origin_y = g->origin_y;
+    c->dx = g->dx;
+    c->dy = g->dy;
+    c->total_avail = g->total_avail;
+    c->density_limit = std::clamp(g->density_limit, 0.05, 1.0);
+    c->have_grid = true;
+    return KTG_OK;
+}
+
+int ktg_occupancy(ktg_ctx *c, const double *x, const double *y, double *occ, double *overflow) {
+    if (!c || !overflow) return KTG_ERR_ARG;
+    if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");
+    if (!c->have_grid) return set_error(c, KTG_ERR_STATE, "no grid installed");
+    if (c->n > 0 && (!x || !y)) return set_error(c, KTG_ERR_ARG, "null positions");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (c->ptr_mode == KTG_PTR_DEVICE) return ktg::launch_occupancy(c, x, y, occ, overflow);
+    if ((rc = reserve_systems(c, c->n, 0))) return rc;
+    if ((rc = upload(c, c->x, x, c->n))) return rc;
+    if ((rc = upload(c, c->y, y, c->n))) return rc;
+    if ((rc = ktg::launch_occupancy(c, c->x, c->y, occ ? c->occ : nullptr, c->scalars + 2)))
+        return rc;
+    const int64_t bins = c->nx * c->ny;
+    if (occ)
+        KTG_CUDA(c, cudaMemcpyAsync(occ, c->occ, sizeof(double) * bins, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    KTG_CUDA(c, cudaMemcpyAsync(c->h_scalars + 2, c->scalars + 2, sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    *overflow = c->h_scalars[2];
+    return KTG_OK;
+}
+
+}  // extern "C"

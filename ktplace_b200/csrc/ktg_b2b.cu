@@ -1,0 +1,394 @@
+// B2B net-model assembly and HPWL (sm_100a).
+//
+// Replaces LinearSystems::buildB2B / buildB2BAxis (globalPlacer/simpl/
+// simpl_lss.cc:11-114) and simplPlacer::Impl::getHpwl (simpl_placer.cc:
+// 256-275). Four launches build both axes at once:
+//
+//   k_bound_pins  one thread per net: first-index argmin/argmax of the pin
+//                 coordinate for x and y (simpl_lss.cc:32-45) and, from the
+//                 same pass, the net's half perimeter (HPWL of the inputs).
+//   k_row_count   one thread per (axis, movable cell): number of movable
+//                 other ends of its B2B edges (simpl_lss.cc:75-83), plus a
+//                 per-block total.
+//   k_scan_blocks one block: exclusive scan of the block totals -> the first
+//                 CSR slot of every block and nnz per axis.
+//   k_fill        one thread per (axis, movable cell): block scan of the row
+//                 counts -> row_ptr, then the row's edges in the reference's
+//                 order (simpl_lss.cc:47-73, 89-113) so that diag and rhs are
+//                 summed exactly as the reference sums them.
+//
+// Bit-exactness: the library is compiled with -fmad=false (no FMA
+// contraction, like the reference's -ffp-contract=off) and CUDA's IEEE
+// double division, so every w, val, diag and rhs equals the reference's.
+#include "ktg_common.cuh"
+#include "ktg_context.h"
+
+namespace ktg {
+namespace {
+
+constexpr int kBuildThreads = 256;
+
+struct NetlistDev {
+    const int32_t *var_of_vertex;
+    const double *fixed_x;
+    const double *fixed_y;
+    const int32_t *net_start;
+    const int32_t *pin_cell;
+    const int32_t *pin_var;
+    const double *off_x;
+    const double *off_y;
+    const double *net_base;
+    const int32_t *net_mov;
+    const int32_t *pin_start;
+    const int2 *pin_ref;
+    int32_t n;
+    int32_t N;
+};
+
+NetlistDev view_of(const ktg_ctx *c) {
+    return NetlistDev{c->var_of_vertex, c->fixed_x, c->fixed_y, c->net_start, c->pin_cell,
+                      c->pin_var,       c->off_x,   c->off_y,   c->net_base,  c->net_mov,
+                      c->pin_start,     c->pin_ref, static_cast<int32_t>(c->n),
+                      static_cast<int32_t>(c->N)};
+}
+
+// Position of a pin's cell: movable cells read the variable vector, fixed
+// cells their fixed coordinate (simpl_lss.cc:14-19).
+__device__ __forceinline__ double cell_pos(const double *pos, const double *fixed, int32_t var,
+                                           int32_t cell) {
+    return var >= 0 ? pos[var] : fixed[cell];
+}
+
+// One thread per net. WithBounds: also choose the bound pins of both axes.
+template <bool WithBounds>
+__global__ void __launch_bounds__(kBuildThreads)
+    k_bound_pins(NetlistDev nl, const double *__restrict__ x, const double *__restrict__ y,
+                 uint32_t *__restrict__ lo_x, uint32_t *__restrict__ hi_x,
+                 uint32_t *__restrict__ lo_y, uint32_t *__restrict__ hi_y,
+                 double *__restrict__ partials, unsigned *__restrict__ ticket,
+                 double *__restrict__ hpwl_out) {
+    __shared__ double scratch[40];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double term = 0.0;
+    if (k < nl.N) {
+        const int32_t s = nl.net_start[k];
+        const int32_t deg = nl.net_start[k + 1] - s;
+        uint32_t lx = 0, hx = 0, ly = 0, hy = 0;
+        double vlx = 0.0, vhx = 0.0, vly = 0.0, vhy = 0.0;
+        // BBox::getEmpty then BBox::extend (geometry/kt_geometry.cc:70-75)
+        double bx0 = __longlong_as_double(0x7ff0000000000000ll);   // +inf
+        double by0 = bx0;
+        double bx1 = -bx0;
+        double by1 = -bx0;
+        for (int32_t q = 0; q < deg; ++q) {
+            const int32_t p = s + q;
+            const int32_t cell = nl.pin_cell[p];
+            const int32_t var = nl.pin_var[p];
+            const double px = cell_pos(x, nl.fixed_x, var, cell) + nl.off_x[p];
+            const double py = cell_pos(y, nl.fixed_y, var, cell) + nl.off_y[p];
+            if (WithBounds) {
+                if (q == 0) {
+                    vlx = vhx = px;
+                    vly = vhy = py;
+                } else {
+                    // lo = pinAt(q) < pinAt(lo) ? q : lo (simpl_lss.cc:41-42)
+                    if (px < vlx) { lx = q; vlx = px; }
+                    if (px > vhx) { hx = q; vhx = px; }
+                    if (py < vly) { ly = q; vly = py; }
+                    if (py > vhy) { hy = q; vhy = py; }
+                }
+            }
+            bx0 = ref_min(bx0, px);
+            by0 = ref_min(by0, py);
+            bx1 = ref_max(bx1, px);
+            by1 = ref_max(by1, py);
+        }
+        if (WithBounds) {
+            lo_x[k] = lx;
+            hi_x[k] = hx;
+            lo_y[k] = ly;
+            hi_y[k] = hy;
+        }
+        // getHalfPerimeter: 0 for an empty box; nets with < 2 pins add 0.
+        if (deg >= 2 && !(bx0 > bx1 || by0 > by1)) term = (bx1 - bx0) + (by1 - by0);
+    }
+    const double bs = block_sum(term, scratch);
+    if (threadIdx.x == 0) __stcg(partials + blockIdx.x, bs);
+    if (last_block_done(ticket)) {
+        const double total = sum_partials(partials, gridDim.x, scratch);
+        if (threadIdx.x == 0) *hpwl_out = total;
+    }
+}
+
+// Edges of movable cell i's row on one axis, in the reference's order.
+// Visit(cell_var, other_pos_of_cell, there, own_offset, w) for every edge.
+template <typename Visit>
+__device__ __forceinline__ void for_each_edge(const NetlistDev &nl, const double *pos,
+                                              const double *fixed, const double *off,
+                                              const uint32_t *lo, const uint32_t *hi,
+                                              double floor_len, int32_t i, Visit &&visit) {
+    const double own_pos = pos[i];
+    const int32_t e0 = nl.pin_start[i];
+    const int32_t e1 = nl.pin_start[i + 1];
+    for (int32_t e = e0; e < e1; ++e) {
+        const int2 ref = nl.pin_ref[e];
+        const int32_t k = ref.x;
+        const uint32_t q = static_cast<uint32_t>(ref.y);
+        const uint32_t l = lo[k];
+        const uint32_t h = hi[k];
+        if (l == h) continue;
+        const int32_t s = nl.net_start[k];
+        const double base = nl.net_base[k];
+        const double own = own_pos + off[s + q];
+        const double own_offset = own - own_pos;
+        auto edge = [&](uint32_t t) {
+            const int32_t p = s + static_cast<int32_t>(t);
+            const int32_t var = nl.pin_var[p];
+            const double cp = cell_pos(pos, fixed, var, nl.pin_cell[p]);
+            const double there = cp + off[p];
+            const double w = base / ref_max(fabs(own - there), floor_len);
+            visit(var, cp, there, own_offset, w);
+        };
+        if (q == l || q == h) {
+            const int32_t deg = nl.net_start[k + 1] - s;
+            for (int32_t t = 0; t < deg; ++t)
+                if (static_cast<uint32_t>(t) != q) edge(static_cast<uint32_t>(t));
+        } else {
+            edge(l);
+            edge(h);
+        }
+    }
+}
+
+struct AxisArgs {
+    const double *pos;
+    const double *fixed;
+    const double *off;
+    const uint32_t *lo;
+    const uint32_t *hi;
+    double floor_len;
+    const double *anchor;
+    int32_t *row_ptr;
+    int32_t *col;
+    double *val;
+    double *diag;
+    double *rhs;
+};
+
+// Count of movable other ends per row; per-block totals for the scan.
+__global__ void __launch_bounds__(kBuildThreads)
+    k_row_count(NetlistDev nl, AxisArgs ax, AxisArgs ay, int32_t blocks_per_axis,
+                int32_t *__restrict__ row_cnt, int64_t *__restrict__ block_sum_out) {
+    __shared__ int32_t warp_tot[kBuildThreads / kWarp];
+    const int axis = blockIdx.x >= blocks_per_axis ? 1 : 0;
+    const AxisArgs &a = axis ? ay : ax;
+    const int32_t i = (blockIdx.x - axis * blocks_per_axis) * blockDim.x + threadIdx.x;
+    int32_t cnt = 0;
+    if (i < nl.n) {
+        const int32_t e0 = nl.pin_start[i];
+        const int32_t e1 = nl.pin_start[i + 1];
+        for (int32_t e = e0; e < e1; ++e) {
+            const int2 ref = nl.pin_ref[e];
+            const int32_t k = ref.x;
+            const uint32_t q = static_cast<uint32_t>(ref.y);
+            const uint32_t l = a.lo[k];
+            const uint32_t h = a.hi[k];
+            if (l == h) continue;
+            if (q == l || q == h) {
+                cnt += nl.net_mov[k] - 1;  // every other movable pin of the net
+            } else {
+                const int32_t s = nl.net_start[k];
+                cnt += (nl.pin_var[s + l] >= 0 ? 1 : 0) + (nl.pin_var[s + h] >= 0 ? 1 : 0);
+            }
+        }
+        row_cnt[axis * nl.n + i] = cnt;
+    }
+    int32_t v = cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) warp_tot[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t t = 0;
+        for (int w = 0; w < kBuildThreads / kWarp; ++w) t += warp_tot[w];
+        block_sum_out[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the per-block totals of both axes (one block). Writes the
+// first slot of every block in place, nnz per axis, row_ptr[n] and flags a
+// capacity overflow.
+__global__ void __launch_bounds__(1024)
+    k_scan_blocks(int64_t *__restrict__ block_sum, int32_t blocks_per_axis, int32_t n,
+                  int64_t cap, int32_t *__restrict__ row_ptr_x, int32_t *__restrict__ row_ptr_y,
+                  int64_t *__restrict__ nnz_out, int *__restrict__ status) {
+    __shared__ int64_t warp_tot[32];
+    __shared__ int64_t carry;
+    for (int axis = 0; axis < 2; ++axis) {
+        int64_t *bs = block_sum + axis * blocks_per_axis;
+        const int per = (blocks_per_axis + blockDim.x - 1) / blockDim.x;
+        const int b0 = threadIdx.x * per;
+        const int b1 = min(b0 + per, blocks_per_axis);
+        int64_t local = 0;
+        for (int b = b0; b < b1; ++b) local += bs[b];
+        // block exclusive scan of `local`
+        int64_t incl = local;
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warp_tot[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            int64_t w = warp_tot[threadIdx.x];
+            int64_t wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (threadIdx.x >= o) wi += t;
+            }
+            warp_tot[threadIdx.x] = wi - w;  // exclusive warp offsets
+            if (threadIdx.x == 31) carry = wi;
+        }
+        __syncthreads();
+        int64_t run = warp_tot[threadIdx.x >> 5] + incl - local;
+        for (int b = b0; b < b1; ++b) {
+            const int64_t v = bs[b];
+            bs[b] = run;
+            run += v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int64_t total = carry;
+            nnz_out[axis] = total;
+            if (total > cap) {
+                atomicCAS(status, kStatusOk, kStatusCapacity);
+                (axis ? row_ptr_y : row_ptr_x)[n] = 0;
+            } else {
+                (axis ? row_ptr_y : row_ptr_x)[n] = static_cast<int32_t>(total);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Row pointers from a block scan of the counts, then the row's entries.
+__global__ void __launch_bounds__(kBuildThreads)
+    k_fill(NetlistDev nl, AxisArgs ax, AxisArgs ay, int32_t blocks_per_axis, double alpha,
+           const int32_t *__restrict__ row_cnt, const int64_t *__restrict__ block_first,
+           int64_t cap, const int *__restrict__ status) {
+    __shared__ int32_t warp_tot[kBuildThreads / kWarp];
+    const int axis = blockIdx.x >= blocks_per_axis ? 1 : 0;
+    const AxisArgs &a = axis ? ay : ax;
+    const int32_t i = (blockIdx.x - axis * blocks_per_axis) * blockDim.x + threadIdx.x;
+    const int32_t cnt = (i < nl.n) ? row_cnt[axis * nl.n + i] : 0;
+    // block exclusive scan of cnt
+    int32_t incl = cnt;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[threadIdx.x >> 5] = incl;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int32_t w = threadIdx.x < kBuildThreads / kWarp ? warp_tot[threadIdx.x] : 0;
+        int32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (threadIdx.x >= o) wi += t;
+        }
+        if (threadIdx.x < kBuildThreads / kWarp) warp_tot[threadIdx.x] = wi - w;
+    }
+    __syncthreads();
+    if (i >= nl.n) return;
+    if (*status != kStatusOk) return;  // capacity exceeded: leave the buffers alone
+    int64_t slot = block_first[blockIdx.x] + warp_tot[threadIdx.x >> 5] + (incl - cnt);
+    a.row_ptr[i] = static_cast<int32_t>(slot);
+    double dg = 0.0;
+    double rh = 0.0;
+    for_each_edge(nl, a.pos, a.fixed, a.off, a.lo, a.hi, a.floor_len, i,
+                  [&](int32_t var, double cp, double there, double own_offset, double w) {
+                      dg += w;
+                      if (var >= 0) {
+                          if (slot < cap) {
+                              a.col[slot] = var;
+                              a.val[slot] = -w;
+                          }
+                          ++slot;
+                          rh += w * ((there - cp) - own_offset);
+                      } else {
+                          rh += w * (there - own_offset);
+                      }
+                  });
+    if (alpha > 0.0) {
+        const double p = a.pos[i];
+        const double w = alpha / ref_max(fabs(p - a.anchor[i]), a.floor_len);
+        dg += w;
+        rh += w * a.anchor[i];
+    }
+    a.diag[i] = ref_max(dg, 1e-12);
+    a.rhs[i] = rh;
+}
+
+}  // namespace
+
+int launch_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha,
+                     const double *ax, const double *ay, double floor_x, double floor_y) {
+    const NetlistDev nl = view_of(c);
+    const int32_t n = static_cast<int32_t>(c->n);
+    const int net_blocks = static_cast<int>((c->N + kBuildThreads - 1) / kBuildThreads);
+    const int32_t bpa = static_cast<int32_t>((c->n + kBuildThreads - 1) / kBuildThreads);
+    KTG_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+    if (c->N > 0) {
+        k_bound_pins<true><<<net_blocks, kBuildThreads, 0, c->stream>>>(
+            nl, x, y, c->sys[0].lo, c->sys[0].hi, c->sys[1].lo, c->sys[1].hi, c->partials,
+            c->counters + 0, c->scalars + 0);
+        ++c->launches;
+    } else {
+        KTG_CUDA(c, cudaMemsetAsync(c->scalars + 0, 0, sizeof(double), c->stream));
+    }
+    AxisArgs a[2];
+    for (int axis = 0; axis < 2; ++axis) {
+        ktg::AxisSystem &s = c->sys[axis];
+        a[axis] = AxisArgs{axis ? y : x, axis ? c->fixed_y : c->fixed_x, axis ? c->off_y : c->off_x,
+                           s.lo, s.hi, axis ? floor_y : floor_x, axis ? ay : ax,
+                           s.row_ptr, s.col, s.val, s.diag, s.rhs};
+    }
+    if (n > 0) {
+        k_row_count<<<2 * bpa, kBuildThreads, 0, c->stream>>>(nl, a[0], a[1], bpa, c->row_cnt,
+                                                              c->block_sum);
+        k_scan_blocks<<<1, 1024, 0, c->stream>>>(c->block_sum, bpa, n, c->cap_nnz,
+                                                 c->sys[0].row_ptr, c->sys[1].row_ptr,
+                                                 c->nnz_dev, c->status);
+        k_fill<<<2 * bpa, kBuildThreads, 0, c->stream>>>(nl, a[0], a[1], bpa, alpha, c->row_cnt,
+                                                         c->block_sum, c->cap_nnz, c->status);
+        c->launches += 3;
+    } else {
+        KTG_CUDA(c, cudaMemsetAsync(c->sys[0].row_ptr, 0, sizeof(int32_t), c->stream));
+        KTG_CUDA(c, cudaMemsetAsync(c->sys[1].row_ptr, 0, sizeof(int32_t), c->stream));
+        KTG_CUDA(c, cudaMemsetAsync(c->nnz_dev, 0, 2 * sizeof(int64_t), c->stream));
+    }
+    KTG_CUDA(c, cudaGetLastError());
+    return KTG_OK;
+}
+
+int launch_hpwl(ktg_ctx *c, const double *x, const double *y, double *out_dev) {
+    if (c->N == 0) {
+        KTG_CUDA(c, cudaMemsetAsync(out_dev, 0, sizeof(double), c->stream));
+        return KTG_OK;
+    }
+    const NetlistDev nl = view_of(c);
+    const int net_blocks = static_cast<int>((c->N + kBuildThreads - 1) / kBuildThreads);
+    k_bound_pins<false><<<net_blocks, kBuildThreads, 0, c->stream>>>(
+        nl, x, y, nullptr, nullptr, nullptr, nullptr, c->partials, c->counters + 0, out_dev);
+    ++c->launches;
+    KTG_CUDA(c, cudaGetLastError());
+    return KTG_OK;
+}
+
+}  // namespace ktg

@@ -1,0 +1,122 @@
+// Host-side context of the ktplace_b200 C ABI.
+//
+// Device layout (all device-resident for the life of a netlist):
+//   netlist  : var_of_vertex[V] i32, fixed_x/y[V] f64,
+//              net_start[N+1] i32, pin_cell/pin_var[P] i32, off_x/off_y[P] f64,
+//              net_base[N] f64 (= weight / (degree - 1)), net_mov[N] i32,
+//              pin_start[n+1] i32, pin_ref[Pm] int2 (net, pin),
+//              width/height/area[n] f64
+//   systems  : per axis row_ptr[n+1] i32, col[cap] i32, val[cap] f64,
+//              diag[n], rhs[n] f64, bound pins lo/hi[N] u32
+//   PCG      : per axis r, z, p, ap [n] f64, positions x/y, anchors [n] f64
+//   density  : occ_fx[bins] i64 fixed point, avail[bins] f64
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "ktplace_b200.h"
+
+namespace ktg {
+
+struct AxisSystem {
+    int32_t *row_ptr = nullptr;  // [n+1]
+    int32_t *col = nullptr;      // [cap]
+    double *val = nullptr;       // [cap]
+    double *diag = nullptr;      // [n]
+    double *rhs = nullptr;       // [n]
+    uint32_t *lo = nullptr;      // [N]
+    uint32_t *hi = nullptr;      // [N]
+    double *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;  // [n]
+};
+
+}  // namespace ktg
+
+struct ktg_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int ptr_mode = KTG_PTR_HOST;
+    std::string err;
+    int64_t launches = 0;
+
+    // netlist sizes
+    bool have_netlist = false;
+    int64_t V = 0, n = 0, N = 0, P = 0, Pm = 0;
+    int64_t cap_nnz = 0;  // col/val capacity per axis (upper bound on nnz)
+    double fx_scale = 1.0;
+
+    // netlist arrays
+    int32_t *var_of_vertex = nullptr;
+    double *fixed_x = nullptr, *fixed_y = nullptr;
+    int32_t *net_start = nullptr, *pin_cell = nullptr, *pin_var = nullptr;
+    double *off_x = nullptr, *off_y = nullptr, *net_base = nullptr;
+    int32_t *net_mov = nullptr;
+    int32_t *pin_start = nullptr;
+    int2 *pin_ref = nullptr;
+    double *width = nullptr, *height = nullptr, *area = nullptr;
+
+    // systems
+    ktg::AxisSystem sys[2];
+    bool have_system = false;  // both axes valid with sys_n rows
+    bool axis_valid[2] = {false, false};
+    int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
+    int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
+    int64_t sys_cap_nnz = 0;  // allocated entries for col/val
+
+    // staging (host pointer mode) and scratch
+    double *x = nullptr, *y = nullptr, *ax = nullptr, *ay = nullptr;  // [max(n, sys_cap_n)]
+    int64_t stage_cap = 0;
+    int32_t *row_cnt = nullptr;      // [2n]
+    int64_t *block_sum = nullptr;    // [2 * blocks]
+    int64_t *nnz_dev = nullptr;      // [2]
+    double *partials = nullptr;      // reduction partials
+    int64_t partials_cap = 0;
+    unsigned *counters = nullptr;    // [8] last-block tickets, barrier count/gen
+    int *status = nullptr;           // [1]
+    double *scalars = nullptr;       // [8] hpwl of build, hpwl, overflow, ...
+    ktg_solve_info *info_dev = nullptr;
+    double *hist_dev = nullptr;      // [2 * hist_cap_dev]
+    int64_t hist_cap_dev = 0;
+
+    // host pinned mirrors for scalar results
+    double *h_scalars = nullptr;     // [8]
+    ktg_solve_info *h_info = nullptr;
+    int64_t *h_nnz = nullptr;        // [2]
+    int *h_status = nullptr;
+
+    // density grid
+    bool have_grid = false;
+    int64_t nx = 0, ny = 0;
+    double origin_x = 0, origin_y = 0, dx = 1, dy = 1, total_avail = 0, density_limit = 1;
+    double *avail = nullptr;         // [bins]
+    unsigned long long *occ_fx = nullptr;  // [bins] two's-complement fixed point
+    double *occ = nullptr;           // [bins] staging for host mode
+    int64_t bins_cap = 0;
+};
+
+namespace ktg {
+
+// Launchers (one per kernel family), implemented in the .cu files. They
+// enqueue on ctx->stream and return a KTG_* code.
+int launch_build_b2b(ktg_ctx *ctx, const double *x, const double *y, double alpha,
+                     const double *ax, const double *ay, double floor_x, double floor_y);
+int launch_hpwl(ktg_ctx *ctx, const double *x, const double *y, double *out_dev);
+int launch_solve(ktg_ctx *ctx, double *x, double *y, double tol, int64_t max_iter,
+                 ktg_solve_info *info_dev, double *hist_x, double *hist_y, int64_t hist_cap);
+int launch_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ_dev,
+                     double *overflow_dev);
+
+int set_error(ktg_ctx *ctx, int code, const std::string &msg);
+int cuda_check(ktg_ctx *ctx, cudaError_t e, const char *what);
+
+}  // namespace ktg
+
+#define KTG_CUDA(ctx, call)                                           \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return ktg::cuda_check((ctx), e_, #call); \
+    } while (0)

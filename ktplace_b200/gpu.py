@@ -1,0 +1,226 @@
+"""Python handle on one ktplace_b200 context (one device, one stream).
+
+Thin wrapper over the C ABI (include/ktplace_b200.h). Host-mode calls take
+numpy arrays; device-mode calls (``*_dev``) take torch CUDA tensors and only
+enqueue work on the context's stream.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import KtgError, NetlistView, GridView, SolveInfo
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _tptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+class Context:
+    """Owns a ``ktg_ctx``: the device-resident netlist, systems and grid."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self.lib.ktg_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise KtgError(rc, f"ktg_create(device={device}) failed")
+        self.h = h
+        self.device = device
+        self._mode = _lib.KTG_PTR_HOST
+        self._keep = None
+        self.nl = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ktg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- plumbing --------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != 0:
+            raise KtgError(rc, self.lib.ktg_last_error(self.h).decode())
+
+    def set_stream(self, stream_handle: int):
+        self._check(self.lib.ktg_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def _set_mode(self, mode: int):
+        if mode != self._mode:
+            self._check(self.lib.ktg_set_pointer_mode(self.h, mode))
+            self._mode = mode
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.ktg_launch_count(self.h))
+
+    # -- netlist -----------------------------------------------------------------
+    def upload_netlist(self, nl):
+        k = dict(
+            mov_vertex=_c(nl.mov_vertex, np.int32), var_of_vertex=_c(nl.var_of_vertex, np.int32),
+            fixed_x=_c(nl.fixed_x, np.float64), fixed_y=_c(nl.fixed_y, np.float64),
+            net_start=_c(nl.net_start, np.int64), pin_cell=_c(nl.pin_cell, np.int32),
+            off_x=_c(nl.off_x, np.float64), off_y=_c(nl.off_y, np.float64),
+            net_weight=_c(nl.net_weight, np.float64), pin_start=_c(nl.pin_start, np.int64),
+            pin_net=_c(nl.pin_net, np.int32), pin_q=_c(nl.pin_q, np.int32),
+            width=_c(nl.width, np.float64), height=_c(nl.height, np.float64))
+
+        def p(name, t):
+            return k[name].ctypes.data_as(ctypes.POINTER(t))
+        i32, i64, f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        v = NetlistView(nl.num_vertices, nl.num_movable, nl.num_nets, p("mov_vertex", i32),
+                        p("var_of_vertex", i32), p("fixed_x", f64), p("fixed_y", f64),
+                        p("net_start", i64), p("pin_cell", i32), p("off_x", f64),
+                        p("off_y", f64), p("net_weight", f64), p("pin_start", i64),
+                        p("pin_net", i32), p("pin_q", i32), p("width", f64), p("height", f64))
+        self._check(self.lib.ktg_upload_netlist(self.h, ctypes.byref(v)))
+        self.nl = nl
+
+    # -- B2B ---------------------------------------------------------------------
+    def build_b2b(self, x, y, alpha, ax=None, ay=None, floor_x=1.0, floor_y=1.0):
+        self._set_mode(_lib.KTG_PTR_HOST)
+        x, y = _c(x, np.float64), _c(y, np.float64)
+        ax = None if ax is None else _c(ax, np.float64)
+        ay = None if ay is None else _c(ay, np.float64)
+        self._check(self.lib.ktg_build_b2b(self.h, _ptr(x), _ptr(y), alpha, _ptr(ax), _ptr(ay),
+                                           floor_x, floor_y))
+
+    def build_b2b_dev(self, x, y, alpha, ax=None, ay=None, floor_x=1.0, floor_y=1.0):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_build_b2b(self.h, _tptr(x), _tptr(y), alpha, _tptr(ax),
+                                           _tptr(ay), floor_x, floor_y))
+
+    def build_hpwl(self) -> float:
+        self._set_mode(_lib.KTG_PTR_HOST)
+        out = ctypes.c_double()
+        self._check(self.lib.ktg_build_hpwl(self.h, ctypes.byref(out)))
+        return float(out.value)
+
+    def build_hpwl_dev(self, out):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_build_hpwl(self.h, _tptr(out)))
+
+    def system_info(self, axis: int):
+        n, m = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.ktg_system_info(self.h, axis, ctypes.byref(n), ctypes.byref(m)))
+        return int(n.value), int(m.value)
+
+    def system(self, axis: int) -> dict:
+        n, m = self.system_info(axis)
+        s = dict(row_ptr=np.zeros(n + 1, np.int64), col=np.zeros(max(m, 1), np.int32),
+                 val=np.zeros(max(m, 1)), diag=np.zeros(max(n, 1)), rhs=np.zeros(max(n, 1)))
+        P = ctypes.POINTER
+        self._check(self.lib.ktg_download_system(
+            self.h, axis, s["row_ptr"].ctypes.data_as(P(ctypes.c_int64)),
+            s["col"].ctypes.data_as(P(ctypes.c_int32)), s["val"].ctypes.data_as(P(ctypes.c_double)),
+            s["diag"].ctypes.data_as(P(ctypes.c_double)),
+            s["rhs"].ctypes.data_as(P(ctypes.c_double))))
+        s["col"], s["val"] = s["col"][:m], s["val"][:m]
+        s["diag"], s["rhs"] = s["diag"][:n], s["rhs"][:n]
+        return s
+
+    def bound_pins(self, axis: int):
+        N = self.nl.num_nets
+        lo = np.zeros(max(N, 1), np.uint32)
+        hi = np.zeros(max(N, 1), np.uint32)
+        P = ctypes.POINTER(ctypes.c_uint32)
+        self._check(self.lib.ktg_download_bound_pins(self.h, axis, lo.ctypes.data_as(P),
+                                                     hi.ctypes.data_as(P)))
+        return lo[:N], hi[:N]
+
+    def upload_system(self, axis: int, s: dict):
+        rp = _c(s["row_ptr"], np.int64)
+        col = _c(s["col"], np.int32)
+        val, diag, rhs = (_c(s[k], np.float64) for k in ("val", "diag", "rhs"))
+        P = ctypes.POINTER
+        self._check(self.lib.ktg_upload_system(
+            self.h, axis, diag.shape[0], rp.ctypes.data_as(P(ctypes.c_int64)),
+            col.ctypes.data_as(P(ctypes.c_int32)), val.ctypes.data_as(P(ctypes.c_double)),
+            diag.ctypes.data_as(P(ctypes.c_double)), rhs.ctypes.data_as(P(ctypes.c_double))))
+
+    # -- PCG ---------------------------------------------------------------------
+    def solve(self, x, y, tol: float, max_iter: int, hist_cap: int = 0,
+              inplace: bool = False) -> dict:
+        """Host-mode solve; returns new x, y, residuals and iteration counts.
+        With ``inplace`` the given float64 arrays are updated directly (e.g.
+        pinned buffers); otherwise copies are solved and returned."""
+        self._set_mode(_lib.KTG_PTR_HOST)
+        if inplace:
+            for a in (x, y):
+                if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError("inplace solve needs contiguous float64 arrays")
+        else:
+            x, y = _c(x, np.float64).copy(), _c(y, np.float64).copy()
+        info = SolveInfo()
+        hx = np.zeros(hist_cap) if hist_cap else None
+        hy = np.zeros(hist_cap) if hist_cap else None
+        self._check(self.lib.ktg_solve(self.h, _ptr(x), _ptr(y), tol, max_iter,
+                                       ctypes.byref(info), _ptr(hx), _ptr(hy), hist_cap))
+        k = int(info.iters)
+        return dict(x=x, y=y, resid=(info.resid_x, info.resid_y), iters=k,
+                    iters_x=int(info.iters_x), iters_y=int(info.iters_y), live=int(info.live),
+                    hist_x=None if hx is None else hx[:min(k, hist_cap)],
+                    hist_y=None if hy is None else hy[:min(k, hist_cap)])
+
+    def solve_dev(self, x, y, tol: float, max_iter: int, info=None, hist_x=None, hist_y=None,
+                  hist_cap: int = 0):
+        """Device-mode solve: x, y (and info: a uint8 tensor of
+        ctypes.sizeof(SolveInfo) bytes) are CUDA tensors updated in place."""
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_solve(self.h, _tptr(x), _tptr(y), tol, max_iter, _tptr(info),
+                                       _tptr(hist_x), _tptr(hist_y), hist_cap))
+
+    # -- HPWL / density ------------------------------------------------------------
+    def hpwl(self, x, y) -> float:
+        self._set_mode(_lib.KTG_PTR_HOST)
+        x, y = _c(x, np.float64), _c(y, np.float64)
+        out = ctypes.c_double()
+        self._check(self.lib.ktg_hpwl(self.h, _ptr(x), _ptr(y), ctypes.byref(out)))
+        return float(out.value)
+
+    def hpwl_dev(self, x, y, out):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_hpwl(self.h, _tptr(x), _tptr(y), _tptr(out)))
+
+    def set_grid(self, g):
+        self._grid_avail = _c(g.avail, np.float64)
+        v = GridView(g.origin_x, g.origin_y, g.dx, g.dy, g.nx, g.ny,
+                     self._grid_avail.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     g.total_avail, g.density_limit)
+        self._check(self.lib.ktg_set_grid(self.h, ctypes.byref(v)))
+        self.grid = g
+
+    def occupancy(self, x, y, want_map: bool = True):
+        self._set_mode(_lib.KTG_PTR_HOST)
+        x, y = _c(x, np.float64), _c(y, np.float64)
+        occ = np.zeros(self.grid.size) if want_map else None
+        ov = ctypes.c_double()
+        self._check(self.lib.ktg_occupancy(self.h, _ptr(x), _ptr(y), _ptr(occ), ctypes.byref(ov)))
+        return occ, float(ov.value)
+
+    def occupancy_dev(self, x, y, occ, overflow):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_occupancy(self.h, _tptr(x), _tptr(y), _tptr(occ),
+                                           _tptr(overflow)))

@@ -1,0 +1,139 @@
+"""The reference's SimPL solve interface, backed by the B200 path.
+
+Mirrors, name for name, the types and calls of globalPlacer/simpl/simpl_lss.h
+so code written against the reference reads the same:
+
+  SparseSystem         simpl_lss.h:38-58 (rowPtr/col/val/diag/rhs, multiply)
+  Residuals            simpl_lss.h:60-63
+  LinearSystems        simpl_lss.h:68-84 (buildB2B)
+  solveBothAxes        simpl_lss.h:86-88
+  getHpwl, getOccupancy, getOverflow
+                       simplPlacer::Impl, simpl_placer.cc:256-297
+
+All arithmetic runs in the CUDA library through the C ABI; nothing here
+computes a result on the CPU. A SparseSystem produced by buildB2B remembers
+the context whose device copy it mirrors, so solveBothAxes reuses that copy
+instead of uploading the CSR again (any other system is uploaded).
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Callable, Optional
+
+import numpy as np
+
+from .gpu import Context
+from .grid import BinGrid
+
+
+@dataclasses.dataclass
+class SparseSystem:
+    rowPtr: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(1, np.int64))
+    col: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
+    val: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+    diag: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+    rhs: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+    _ctx: Optional[Context] = dataclasses.field(default=None, repr=False)
+    _gen: int = dataclasses.field(default=-1, repr=False)
+    _axis: int = dataclasses.field(default=-1, repr=False)
+
+    def size(self) -> int:
+        return int(self.diag.shape[0])
+
+    def as_dict(self) -> dict:
+        return dict(row_ptr=self.rowPtr, col=self.col, val=self.val, diag=self.diag,
+                    rhs=self.rhs)
+
+
+@dataclasses.dataclass
+class Residuals:
+    x: float = 0.0
+    y: float = 0.0
+
+
+IterateObserver = Callable[[int, Residuals, bool], None]
+
+
+class LinearSystems:
+    """simpl_lss.h:68-84. ``context`` is the GPU context holding the netlist."""
+
+    def __init__(self, netlist, sysX: SparseSystem, sysY: SparseSystem, floorX: float,
+                 floorY: float, context: Context):
+        self.netlist = netlist
+        self.sysX = sysX
+        self.sysY = sysY
+        self.floorX = floorX
+        self.floorY = floorY
+        self.ctx = context
+        if context.nl is not netlist:
+            context.upload_netlist(netlist)
+
+    def buildB2B(self, x, y, alpha: float, anchorX, anchorY):
+        """LinearSystems::buildB2B (simpl_lss.cc:11-114)."""
+        ax = anchorX if alpha > 0.0 else None
+        ay = anchorY if alpha > 0.0 else None
+        self.ctx.build_b2b(x, y, alpha, ax, ay, self.floorX, self.floorY)
+        gen = getattr(self.ctx, "_gen", 0) + 1
+        self.ctx._gen = gen
+        for axis, s in enumerate((self.sysX, self.sysY)):
+            d = self.ctx.system(axis)
+            s.rowPtr, s.col, s.val, s.diag, s.rhs = (d["row_ptr"], d["col"], d["val"],
+                                                     d["diag"], d["rhs"])
+            s._ctx, s._gen, s._axis = self.ctx, gen, axis
+
+
+def _on_device(ctx: Context, s: SparseSystem, axis: int) -> bool:
+    return s._ctx is ctx and s._axis == axis and s._gen == getattr(ctx, "_gen", -2)
+
+
+def solveBothAxes(sysX: SparseSystem, x: np.ndarray, sysY: SparseSystem, y: np.ndarray,
+                  tolerance: float, maxIterations: int,
+                  observe: Optional[IterateObserver] = None,
+                  context: Optional[Context] = None) -> Residuals:
+    """solveBothAxes (simpl_lss.cc:203-290): x and y are updated in place.
+
+    The observer is called once per loop iteration with that iteration's
+    residuals, after the device solve returns (the residual history is
+    recorded on the device)."""
+    ctx = context or sysX._ctx or sysY._ctx
+    if ctx is None:
+        raise ValueError("solveBothAxes needs a Context (or systems built by one)")
+    if sysX.size() != sysY.size():
+        raise ValueError("x and y systems differ in size")
+    for axis, s in enumerate((sysX, sysY)):
+        if not _on_device(ctx, s, axis):
+            ctx.upload_system(axis, s.as_dict())
+    for axis, s in enumerate((sysX, sysY)):
+        s._ctx, s._axis = ctx, axis
+        s._gen = getattr(ctx, "_gen", 0)
+    cap = int(min(maxIterations, 1 << 20)) if observe else 0
+    r = ctx.solve(x, y, tolerance, maxIterations, hist_cap=cap)
+    x[...] = r["x"]
+    y[...] = r["y"]
+    if observe:
+        k = r["iters"]
+        for it in range(1, k + 1):
+            last = it == k and r["live"] == 0
+            observe(it, Residuals(float(r["hist_x"][it - 1]), float(r["hist_y"][it - 1])), last)
+    return Residuals(r["resid"][0], r["resid"][1])
+
+
+def getHpwl(context: Context, x, y) -> float:
+    """simplPlacer::Impl::getHpwl (simpl_placer.cc:256-275)."""
+    return context.hpwl(x, y)
+
+
+def getOccupancy(context: Context, grid: BinGrid, x, y) -> np.ndarray:
+    """simplPlacer::Impl::getOccupancy (simpl_placer.cc:282-289)."""
+    if getattr(context, "grid", None) is not grid:
+        context.set_grid(grid)
+    occ, _ = context.occupancy(x, y, want_map=True)
+    return occ
+
+
+def getOverflowOf(context: Context, grid: BinGrid, x, y) -> float:
+    """getOverflow(getOccupancy(x, y)) (simpl_placer.cc:291-297) in one pass."""
+    if getattr(context, "grid", None) is not grid:
+        context.set_grid(grid)
+    _, ov = context.occupancy(x, y, want_map=False)
+    return ov
