@@ -189,7 +189,13 @@ int ktg_set_grid(ktg_ctx *ctx, const ktg_grid_view *grid);
 int ktg_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ,
                   double *overflow);
 
-/* ---- introspection -------------------------------------------------------- */
+/* ---- tuning and introspection ------------------------------------------- */
+
+/* Sets a kernel-shape option of this context (no reference counterpart; the
+ * values are what the project autotuner chooses between):
+ *   "pcg_lanes"  1 or 4: threads per matrix row in the PCG SpMV (0 = default)
+ * Returns KTG_ERR_ARG for an unknown key or value. */
+int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
 
 /* Number of kernels this context has launched since creation (all entry
  * points). */

@@ -76,6 +76,7 @@ SIGNATURES = [
     ("ktg_set_grid", ctypes.c_int, [_vp, ctypes.POINTER(GridView)]),
     ("ktg_occupancy", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("ktg_launch_count", ctypes.c_int64, [_vp]),
+    ("ktg_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
 ]
 
 _lib = None

@@ -247,6 +247,18 @@ int ktg_set_pointer_mode(ktg_ctx *c, int mode) {
 
 int64_t ktg_launch_count(const ktg_ctx *c) { return c ? c->launches : 0; }
 
+int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
+    if (!c || !key) return KTG_ERR_ARG;
+    const std::string k(key);
+    if (k == "pcg_lanes") {
+        if (value != 0 && value != 1 && value != 4)
+            return set_error(c, KTG_ERR_ARG, "pcg_lanes must be 0, 1 or 4");
+        c->pcg_lanes = static_cast<int>(value);
+        return KTG_OK;
+    }
+    return set_error(c, KTG_ERR_ARG, "unknown option " + k);
+}
+
 int ktg_upload_netlist(ktg_ctx *c, const ktg_netlist_view *nl) {
     if (!c || !nl) return KTG_ERR_ARG;
     int rc = set_device(c);

@@ -42,6 +42,7 @@ struct ktg_ctx {
     int ptr_mode = KTG_PTR_HOST;
     std::string err;
     int64_t launches = 0;
+    int pcg_lanes = 0;  // 0: library default; 1 or 4 lanes per row in the PCG SpMV
 
     // netlist sizes
     bool have_netlist = false;

@@ -5,11 +5,17 @@
 // SparseSystem::multiply (simpl_lss.h:49-57). The whole solve -- warm start,
 // every iteration, the stopping test -- runs inside one kernel, so there is no
 // host round trip per iteration. Each block owns a contiguous slice of the
-// combined row space [x rows | y rows]; three grid barriers per iteration
-// separate
-//   A: Ap = A p (8 lanes per row, coalesced val/col loads) and p.Ap partials
+// combined row space [x rows | y rows] (one 1024-thread block per SM); three
+// grid barriers per iteration separate
+//   A: Ap = A p and p.Ap partials
 //   B: x += a p, r -= a Ap, z = r / diag, and r.r, r.z partials
 //   C: p = z + b p
+// When a block's rows fit, its slices of x, r, z, p, diag and Ap live in
+// shared memory for the whole solve, so phases B and C never leave the SM
+// and only p is published to global memory for the other blocks' gathers.
+// SpMV runs either one thread per row with four independent gathers in
+// flight (the row sum then adds terms in the reference's order) or four lanes
+// per row; the launcher picks by problem size.
 // Scalars (alpha, beta, residuals, live flags) are recomputed identically by
 // every block from the same partials in a fixed order, so all blocks take the
 // same branch and the result is identical from run to run.
@@ -28,8 +34,10 @@
 namespace ktg {
 namespace {
 
-constexpr int kPcgThreads = 512;
-constexpr int kLanesPerRow = 8;
+constexpr int kPcgThreads = 1024;
+// Shared-memory budget for the per-block vector slices (6 doubles per row).
+constexpr int kPcgSmemBytes = 216 * 1024;
+constexpr int kVecsPerRow = 6;
 
 struct PcgAxis {
     const int32_t *rp;
@@ -69,7 +77,6 @@ __device__ __forceinline__ double *slot_ptr(const PcgArgs &A, int slot, int axis
     return A.part + (static_cast<size_t>(slot) * 2 + axis) * gridDim.x;
 }
 
-// Block-sums `v` (per-thread) and stores the block partial of (slot, axis).
 template <int K>
 __device__ __forceinline__ void store_partials(const PcgArgs &A, double (&v)[K],
                                                const int (&slot)[K], const int (&axis)[K],
@@ -81,7 +88,6 @@ __device__ __forceinline__ void store_partials(const PcgArgs &A, double (&v)[K],
     }
 }
 
-// Sums the grid's partials of K (slot, axis) pairs in a fixed order.
 template <int K>
 __device__ __forceinline__ void reduce_partials(const PcgArgs &A, double (&out)[K],
                                                 const int (&slot)[K], const int (&axis)[K],
@@ -95,58 +101,153 @@ __device__ __forceinline__ void reduce_partials(const PcgArgs &A, double (&out)[
     block_sum_k<K>(out, scratch);
 }
 
-__global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
+// Off-diagonal part of row i of S times `in` (gathered from global memory,
+// L1 bypassed because other blocks rewrite it between phases), one thread:
+// terms are added in storage order, four gathers in flight.
+__device__ __forceinline__ double row_offdiag_seq(const PcgAxis &S, int32_t i, double sum,
+                                                  const double *in) {
+    int32_t e = __ldg(S.rp + i);
+    const int32_t e1 = __ldg(S.rp + i + 1);
+    for (; e + 4 <= e1; e += 4) {
+        const int32_t c0 = __ldg(S.col + e), c1 = __ldg(S.col + e + 1);
+        const int32_t c2 = __ldg(S.col + e + 2), c3 = __ldg(S.col + e + 3);
+        const double v0 = __ldg(S.val + e), v1 = __ldg(S.val + e + 1);
+        const double v2 = __ldg(S.val + e + 2), v3 = __ldg(S.val + e + 3);
+        const double g0 = __ldcg(in + c0), g1 = __ldcg(in + c1);
+        const double g2 = __ldcg(in + c2), g3 = __ldcg(in + c3);
+        sum += v0 * g0;
+        sum += v1 * g1;
+        sum += v2 * g2;
+        sum += v3 * g3;
+    }
+    for (; e < e1; ++e) sum += __ldg(S.val + e) * __ldcg(in + __ldg(S.col + e));
+    return sum;
+}
+
+// Same with four lanes per row; every lane of the warp must call it.
+__device__ __forceinline__ double row_offdiag_vec4(const PcgAxis &S, int32_t i, bool valid,
+                                                   const double *in) {
+    const int sub = threadIdx.x & 3;
+    double s = 0.0;
+    if (valid) {
+        int32_t e = __ldg(S.rp + i) + sub;
+        const int32_t e1 = __ldg(S.rp + i + 1);
+        for (; e + 4 < e1; e += 8) {
+            const int32_t c0 = __ldg(S.col + e), c1 = __ldg(S.col + e + 4);
+            const double v0 = __ldg(S.val + e), v1 = __ldg(S.val + e + 4);
+            const double g0 = __ldcg(in + c0), g1 = __ldcg(in + c1);
+            s += v0 * g0;
+            s += v1 * g1;
+        }
+        if (e < e1) s += __ldg(S.val + e) * __ldcg(in + __ldg(S.col + e));
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    return s;
+}
+
+template <bool Smem, int Lanes>
+__global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
+    extern __shared__ double dyn[];
     __shared__ double scratch[33 * 4];
     __shared__ PcgAxis sax[2];
     if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
-    __syncthreads();
     const uint64_t t_start = global_timer_ns();
     const uint64_t total_deadline = t_start + A.total_timeout_ns;
-    const int32_t n0 = sax[0].n;
     const int32_t r0 = blockIdx.x * A.rows_per_block;
     const int32_t r1 = min(r0 + A.rows_per_block, A.total_rows);
-    const int lane = threadIdx.x & 31;
-    const int sub = lane & (kLanesPerRow - 1);
-    const int warp = threadIdx.x >> 5;
-    const int nwarps = blockDim.x >> 5;
-    constexpr int kRowsPerWarp = kWarp / kLanesPerRow;
-
+    const int32_t R = max(r1 - r0, 0);
+    const int32_t cap = A.rows_per_block;
+    double *sx = dyn, *sr = dyn + cap, *sz = dyn + 2 * cap;
+    double *sp = dyn + 3 * cap, *sd = dyn + 4 * cap, *sap = dyn + 5 * cap;
+    __syncthreads();
+    const int32_t n0 = sax[0].n;
     auto deadline = [&]() {
         const uint64_t d = global_timer_ns() + A.barrier_timeout_ns;
         return d < total_deadline ? d : total_deadline;
+    };
+    // Row l of this block: axis and row index inside that axis.
+    auto locate = [&](int32_t l, int &axis, int32_t &i) {
+        const int32_t c = r0 + l;
+        axis = c >= n0 ? 1 : 0;
+        i = c - (axis ? n0 : 0);
+    };
+    // Vector accessors: shared-memory slice or global array.
+#define KTG_V(sm, field) (Smem ? sm[l] : sax[axis].field[i])
+
+    if (Smem) {
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            sx[l] = sax[axis].x[i];
+            sd[l] = __ldg(sax[axis].diag + i);
+        }
+        __syncthreads();
+    }
+
+    // SpMV over this block's rows: out[l] = diag * in_own + A_off in_global.
+    // `own` reads the row's own input element, `in` selects the gathered
+    // vector per axis.
+    auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
+        if (Lanes == 1) {
+            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(l, axis, i);
+                if (live && !live[axis]) continue;
+                const PcgAxis &S = sax[axis];
+                const double d = Smem ? sd[l] : __ldg(S.diag + i);
+                const double v = own(l, axis, i);
+                const double s = row_offdiag_seq(S, i, d * v, in_of(axis));
+                emit(l, axis, i, v, s);
+            }
+        } else {
+            const int32_t groups = blockDim.x / 4;
+            const int32_t g = threadIdx.x / 4;
+            for (int32_t base = 0; base < R; base += groups) {
+                const int32_t l = base + g;
+                int axis = 0;
+                int32_t i = 0;
+                bool valid = l < R;
+                if (valid) locate(l, axis, i);
+                if (valid && live && !live[axis]) valid = false;
+                const PcgAxis &S = sax[axis];
+                const double s = row_offdiag_vec4(S, i, valid, in_of(axis));
+                if (valid && (threadIdx.x & 3) == 0) {
+                    const double d = Smem ? sd[l] : __ldg(S.diag + i);
+                    const double v = own(l, axis, i);
+                    emit(l, axis, i, v, d * v + s);
+                }
+            }
+        }
     };
 
     // ---- start: Ap = A x, r = b - Ap, z = r / diag, p = z ------------------
     {
         double acc[6] = {0, 0, 0, 0, 0, 0};  // bb, rz, rr for x then y
-        for (int32_t base = r0 + warp * kRowsPerWarp; base < r1; base += nwarps * kRowsPerWarp) {
-            const int32_t c = base + (lane / kLanesPerRow);
-            const bool valid = c < r1;
-            const int axis = (valid && c >= n0) ? 1 : 0;
-            const PcgAxis &S = sax[axis];
-            const int32_t i = valid ? c - (axis ? n0 : 0) : 0;
-            double s = 0.0;
-            if (valid) {
-                const int32_t e1 = __ldg(S.rp + i + 1);
-                for (int32_t e = __ldg(S.rp + i) + sub; e < e1; e += kLanesPerRow)
-                    s += __ldg(S.val + e) * __ldcg(S.x + __ldg(S.col + e));
-            }
-            s += __shfl_xor_sync(0xffffffffu, s, 4);
-            s += __shfl_xor_sync(0xffffffffu, s, 2);
-            s += __shfl_xor_sync(0xffffffffu, s, 1);
-            if (valid && sub == 0) {
-                const double ap = S.diag[i] * S.x[i] + s;
-                const double b = S.rhs[i];
-                const double r = b - ap;
-                const double z = r / S.diag[i];
-                S.r[i] = r;
-                S.z[i] = z;
-                S.p[i] = z;
-                acc[axis * 3 + 0] += b * b;
-                acc[axis * 3 + 1] += r * z;
-                acc[axis * 3 + 2] += r * r;
-            }
-        }
+        spmv([&](int32_t l, int axis, int32_t i) { return KTG_V(sx, x); },
+             [&](int axis) -> const double * { return sax[axis].x; },
+             [&](int32_t l, int axis, int32_t i, double, double ap) {
+                 const PcgAxis &S = sax[axis];
+                 const double b = __ldg(S.rhs + i);
+                 const double r = b - ap;
+                 const double d = Smem ? sd[l] : __ldg(S.diag + i);
+                 const double z = r / d;
+                 if (Smem) {
+                     sr[l] = r;
+                     sz[l] = z;
+                     sp[l] = z;
+                 } else {
+                     S.r[i] = r;
+                     S.z[i] = z;
+                 }
+                 __stcg(S.p + i, z);
+                 acc[axis * 3 + 0] += b * b;
+                 acc[axis * 3 + 1] += r * z;
+                 acc[axis * 3 + 2] += r * r;
+             },
+             nullptr);
         double v0[3] = {acc[0], acc[1], acc[2]};
         double v1[3] = {acc[3], acc[4], acc[5]};
         const int sl[3] = {kBB, kRZ0, kRR0};
@@ -183,35 +284,23 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
 
     int64_t it = 0;
     for (;;) {
-        const bool live0 = active[0] && resid[0] > A.tol;
-        const bool live1 = active[1] && resid[1] > A.tol;
-        if (it >= A.max_iter || !(live0 || live1)) break;
-        const bool live[2] = {live0, live1};
+        bool live[2];
+        live[0] = active[0] && resid[0] > A.tol;
+        live[1] = active[1] && resid[1] > A.tol;
+        if (it >= A.max_iter || !(live[0] || live[1])) break;
 
         // ---- A: Ap = A p, p.Ap ------------------------------------------
         double pap_acc[2] = {0.0, 0.0};
-        for (int32_t base = r0 + warp * kRowsPerWarp; base < r1; base += nwarps * kRowsPerWarp) {
-            const int32_t c = base + (lane / kLanesPerRow);
-            const int axis = (c < r1 && c >= n0) ? 1 : 0;
-            const bool valid = c < r1 && live[axis];
-            const PcgAxis &S = sax[axis];
-            const int32_t i = c - (axis ? n0 : 0);
-            double s = 0.0;
-            if (valid) {
-                const int32_t e1 = __ldg(S.rp + i + 1);
-                for (int32_t e = __ldg(S.rp + i) + sub; e < e1; e += kLanesPerRow)
-                    s += __ldg(S.val + e) * __ldcg(S.p + __ldg(S.col + e));
-            }
-            s += __shfl_xor_sync(0xffffffffu, s, 4);
-            s += __shfl_xor_sync(0xffffffffu, s, 2);
-            s += __shfl_xor_sync(0xffffffffu, s, 1);
-            if (valid && sub == 0) {
-                const double pi = S.p[i];
-                const double ap = S.diag[i] * pi + s;
-                S.ap[i] = ap;
-                pap_acc[axis] += pi * ap;
-            }
-        }
+        spmv([&](int32_t l, int axis, int32_t i) { return Smem ? sp[l] : __ldcg(sax[axis].p + i); },
+             [&](int axis) -> const double * { return sax[axis].p; },
+             [&](int32_t l, int axis, int32_t i, double pi, double ap) {
+                 if (Smem)
+                     sap[l] = ap;
+                 else
+                     sax[axis].ap[i] = ap;
+                 pap_acc[axis] += pi * ap;
+             },
+             live);
         {
             const int sl[2] = {kPAP, kPAP};
             const int ax[2] = {0, 1};
@@ -235,18 +324,21 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
 
         // ---- B: x, r, z update, r.r and r.z ------------------------------
         double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rr x, rz x, rr y, rz y
-        for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
-            const int axis = c >= n0 ? 1 : 0;
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
             if (!ok[axis]) continue;
             const PcgAxis &S = sax[axis];
-            const int32_t i = c - (axis ? n0 : 0);
             const double a = alpha[axis];
-            const double pi = S.p[i];
-            S.x[i] += a * pi;
-            const double r = S.r[i] - a * S.ap[i];
-            const double z = r / S.diag[i];
-            S.r[i] = r;
-            S.z[i] = z;
+            const double pi = KTG_V(sp, p);
+            const double apv = KTG_V(sap, ap);
+            const double d = Smem ? sd[l] : __ldg(S.diag + i);
+            KTG_V(sx, x) += a * pi;
+            const double r = KTG_V(sr, r) - a * apv;
+            const double z = r / d;
+            KTG_V(sr, r) = r;
+            KTG_V(sz, z) = z;
             acc[axis * 2 + 0] += r * r;
             acc[axis * 2 + 1] += r * z;
         }
@@ -276,12 +368,14 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
         }
 
         // ---- C: p = z + beta p -------------------------------------------
-        for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
-            const int axis = c >= n0 ? 1 : 0;
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
             if (!ok2[axis]) continue;
-            const PcgAxis &S = sax[axis];
-            const int32_t i = c - (axis ? n0 : 0);
-            S.p[i] = S.z[i] + beta[axis] * S.p[i];
+            const double pn = KTG_V(sz, z) + beta[axis] * KTG_V(sp, p);
+            if (Smem) sp[l] = pn;
+            __stcg(sax[axis].p + i, pn);
         }
 #pragma unroll
         for (int a = 0; a < 2; ++a) {
@@ -297,7 +391,16 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
         ++it;
         if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
     }
+#undef KTG_V
 
+    if (Smem) {
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            sax[axis].x[i] = sx[l];
+        }
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ktg_solve_info inf;
         inf.resid_x = resid[0];
@@ -316,7 +419,22 @@ __global__ void k_solve_status(const int *status, ktg_solve_info *info) {
     if (*status != kStatusOk) info->status = *status;
 }
 
+using PcgKernel = void (*)(PcgArgs);
+
+struct Variant {
+    PcgKernel fn;
+    bool smem;
+    int lanes;
+};
+
+Variant pick_variant(bool smem, int lanes) {
+    if (smem) return lanes == 4 ? Variant{k_pcg<true, 4>, true, 4} : Variant{k_pcg<true, 1>, true, 1};
+    return lanes == 4 ? Variant{k_pcg<false, 4>, false, 4} : Variant{k_pcg<false, 1>, false, 1};
+}
+
 }  // namespace
+
+int pcg_lanes_default = 4;
 
 int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
                  ktg_solve_info *info_dev, double *hist_x, double *hist_y, int64_t hist_cap) {
@@ -328,17 +446,28 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
                           s.r, s.z, s.p, s.ap, static_cast<int32_t>(nsys)};
     }
     A.total_rows = static_cast<int32_t>(2 * nsys);
-    static int max_blocks_per_sm = -1;
-    if (max_blocks_per_sm < 0) {
-        KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks_per_sm, k_pcg,
-                                                                   kPcgThreads, 0));
-        if (max_blocks_per_sm < 1) return set_error(c, KTG_ERR_CUDA, "k_pcg cannot be resident");
-    }
-    const int64_t coresident = static_cast<int64_t>(max_blocks_per_sm) * c->num_sms;
+    // One 1024-thread block per SM; small systems use fewer blocks so each
+    // block still owns about a thousand rows.
     const int64_t want = (A.total_rows + 1023) / 1024;
-    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(coresident, want)));
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(c->num_sms, want)));
     A.rows_per_block = static_cast<int32_t>((A.total_rows + grid - 1) / grid);
     if (A.rows_per_block == 0) A.rows_per_block = 1;
+    const size_t smem = sizeof(double) * kVecsPerRow * static_cast<size_t>(A.rows_per_block);
+    const bool use_smem = smem <= static_cast<size_t>(kPcgSmemBytes);
+    const int lanes = c->pcg_lanes > 0 ? c->pcg_lanes : pcg_lanes_default;
+    const Variant v = pick_variant(use_smem, lanes);
+    const size_t dyn = use_smem ? smem : 0;
+    static bool attr_set[2][2] = {{false, false}, {false, false}};
+    bool &done = attr_set[use_smem][lanes == 4];
+    if (!done) {
+        KTG_CUDA(c, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kPcgSmemBytes));
+        done = true;
+    }
+    int per_sm = 0;
+    KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, kPcgThreads, dyn));
+    if (per_sm < 1 || grid > per_sm * c->num_sms)
+        return set_error(c, KTG_ERR_CUDA, "PCG blocks cannot all be resident");
     if (c->partials_cap < 12 * static_cast<int64_t>(grid))
         return set_error(c, KTG_ERR_STATE, "partials buffer too small");
     A.tol = tol;
@@ -357,8 +486,8 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     // A solve that gave up may have left the arrival counter part-way.
     KTG_CUDA(c, cudaMemsetAsync(c->counters + 2, 0, sizeof(unsigned), c->stream));
     void *args[] = {&A};
-    KTG_CUDA(c, cudaLaunchCooperativeKernel((void *)k_pcg, dim3(grid), dim3(kPcgThreads), args, 0,
-                                            c->stream));
+    KTG_CUDA(c, cudaLaunchCooperativeKernel((void *)v.fn, dim3(grid), dim3(kPcgThreads), args,
+                                            dyn, c->stream));
     k_solve_status<<<1, 1, 0, c->stream>>>(c->status, info_dev);
     c->launches += 2;
     KTG_CUDA(c, cudaGetLastError());

@@ -72,6 +72,9 @@ class Context:
             self._check(self.lib.ktg_set_pointer_mode(self.h, mode))
             self._mode = mode
 
+    def set_option(self, key: str, value: int):
+        self._check(self.lib.ktg_set_option(self.h, key.encode(), int(value)))
+
     @property
     def launches(self) -> int:
         return int(self.lib.ktg_launch_count(self.h))
