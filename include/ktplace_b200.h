@@ -201,6 +201,37 @@ int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
  * points). */
 int64_t ktg_launch_count(const ktg_ctx *ctx);
 
+/* ---- allocation-free HPWL ------------------------------------------------ */
+
+/* Largest net count ktg_hpwl_noalloc accepts. */
+#define KTG_NOALLOC_HPWL_MAX_NETS 4194304
+
+/* HPWL of the movable positions (x, y), like ktg_hpwl, for callers that may
+ * not allocate GPU memory: code running where cudaMalloc is forbidden or
+ * unsafe (inside a host callback, under a memory pool or allocator owned by
+ * another runtime, in a service with a fixed memory budget). It has no
+ * counterpart in the reference, which never allocates device memory at all.
+ *
+ * Nothing is allocated or freed, and no context is needed: every argument is
+ * a device pointer on the current device (netlist arrays as in
+ * ktg_netlist_view, with 32-bit net_start), `out` receives one double, and
+ * the work is enqueued on `stream` (a cudaStream_t, NULL = legacy default).
+ * The reduction's scratch (one partial per 256 nets plus a ticket, about
+ * 128 KiB) is a static device array that every GPU which loads this library
+ * holds until the process exits. Limits and caveats:
+ *   - num_nets above KTG_NOALLOC_HPWL_MAX_NETS returns KTG_ERR_RANGE;
+ *   - the first call with a given device current looks up that device's
+ *     scratch address (cudaGetSymbolAddress), so make that first call before
+ *     any stream capture begins;
+ *   - all calls share the one scratch array: calls that overlap on the GPU
+ *     (different streams, or host threads without ordering) race and give
+ *     wrong sums. Serialise them on one stream.
+ * Returns KTG_OK or a negative KTG_ERR_* code. */
+int ktg_hpwl_noalloc(const int32_t *net_start, const int32_t *pin_cell,
+                     const int32_t *var_of_vertex, const double *off_x, const double *off_y,
+                     const double *fixed_x, const double *fixed_y, const double *x,
+                     const double *y, int64_t num_nets, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

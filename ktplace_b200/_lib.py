@@ -77,6 +77,8 @@ SIGNATURES = [
     ("ktg_occupancy", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("ktg_launch_count", ctypes.c_int64, [_vp]),
     ("ktg_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
+    ("ktg_hpwl_noalloc", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                        ctypes.c_int64, _vp, _vp]),
 ]
 
 _lib = None
