@@ -1,0 +1,290 @@
+// Drop-in replacement for KTPlace's globalPlacer/simpl/simpl_lss.cc.
+//
+// Compiled against the reference's own header (globalPlacer/simpl/
+// simpl_lss.h), it defines the same three symbols the SimPL placer calls and
+// runs them on a B200 through the ktplace_b200 C ABI:
+//
+//   LinearSystems::buildB2B  (reference: simpl_lss.cc:11-114)  -> ktg_build_b2b
+//   LinearSystems::buildStar (reference: simpl_lss.cc:116-201) -> host assembly,
+//                            solved on the GPU like any other system
+//   solveBothAxes            (reference: simpl_lss.cc:203-290) -> ktg_solve
+//
+// Link this object instead of simpl_lss.o. One GPU
+// context per process (device $KTPLACE_B200_DEVICE, default 0) holds the
+// netlist, uploaded the first time a Netlist is seen and again whenever a
+// different one is. Errors from the GPU are fatal through ktlog, as the
+// reference treats its own unrecoverable states.
+//
+// Contract differences, all documented in INTEGRATION.md:
+//   * with $KTPLACE_B200_HOST_CSR=0 buildB2B fills only diag and rhs on the
+//     host and leaves rowPtr/col/val empty; solveBothAxes then uses the device
+//     copy. By default the whole CSR is copied back, as the reference fills it.
+//   * the IterateObserver is replayed after the device solve with each
+//     iterate's residuals; x and y already hold the final solution then.
+#include "globalPlacer/simpl/simpl_lss.h"
+#include "util/kt_log.h"
+
+#include "ktplace_b200.h"
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace ktplace::simpl {
+namespace {
+
+struct GpuState {
+    ktg_ctx *ctx = nullptr;
+    const Netlist *netlist = nullptr;
+    std::size_t netlistMovable = 0;
+    std::size_t netlistNets = 0;
+    // The SparseSystem objects whose device copy is current.
+    const SparseSystem *devX = nullptr;
+    const SparseSystem *devY = nullptr;
+    std::size_t devRows = 0;
+    bool hostCsr = true;
+    std::vector<double> histX, histY;
+};
+
+GpuState &state() {
+    static GpuState s;
+    return s;
+}
+
+[[noreturn]] void fail(const char *what, int rc) {
+    const ktg_ctx *c = state().ctx;
+    ktlog.fatal("ktplace_b200: {} failed ({}): {}", what, rc, c ? ktg_last_error(c) : "");
+}
+
+void check(const char *what, int rc) {
+    if (rc != KTG_OK) fail(what, rc);
+}
+
+ktg_ctx *context() {
+    GpuState &s = state();
+    if (s.ctx == nullptr) {
+        const char *dev = std::getenv("KTPLACE_B200_DEVICE");
+        const char *csr = std::getenv("KTPLACE_B200_HOST_CSR");
+        s.hostCsr = !(csr != nullptr && std::string(csr) == "0");
+        check("ktg_create", ktg_create(dev ? std::atoi(dev) : 0, &s.ctx));
+    }
+    return s.ctx;
+}
+
+// SimPL's Netlist as the C ABI's structure of arrays (one-time per design).
+void ensureNetlist(const Netlist &nl) {
+    GpuState &s = state();
+    ktg_ctx *c = context();
+    if (s.netlist == &nl && s.netlistMovable == nl.numMovable && s.netlistNets == nl.nets.size())
+        return;
+    const std::size_t V = nl.varOfVertex.size();
+    const std::size_t n = nl.numMovable;
+    std::vector<int32_t> movVertex(nl.movVertex.begin(), nl.movVertex.end());
+    std::vector<int32_t> varOf(V);
+    for (std::size_t v = 0; v < V; ++v)
+        varOf[v] = nl.varOfVertex[v] == noVar ? -1 : static_cast<int32_t>(nl.varOfVertex[v]);
+    std::vector<int64_t> netStart(nl.nets.size() + 1, 0);
+    for (std::size_t k = 0; k < nl.nets.size(); ++k)
+        netStart[k + 1] = netStart[k] + static_cast<int64_t>(nl.nets[k].cells.size());
+    std::vector<int32_t> pinCell(netStart.back());
+    std::vector<double> offX(netStart.back()), offY(netStart.back()), weight(nl.nets.size());
+    for (std::size_t k = 0; k < nl.nets.size(); ++k) {
+        const NetPins &np = nl.nets[k];
+        weight[k] = np.weight;
+        for (std::size_t q = 0; q < np.cells.size(); ++q) {
+            pinCell[netStart[k] + q] = static_cast<int32_t>(np.cells[q]);
+            offX[netStart[k] + q] = np.offX[q];
+            offY[netStart[k] + q] = np.offY[q];
+        }
+    }
+    std::vector<int64_t> pinStart(nl.pinStart.begin(), nl.pinStart.end());
+    std::vector<int32_t> pinNet(nl.pinsOfCell.size()), pinQ(nl.pinsOfCell.size());
+    for (std::size_t e = 0; e < nl.pinsOfCell.size(); ++e) {
+        pinNet[e] = static_cast<int32_t>(nl.pinsOfCell[e].net);
+        pinQ[e] = static_cast<int32_t>(nl.pinsOfCell[e].pin);
+    }
+    // Cell sizes are not part of Netlist; the density entry points take them
+    // from the placer's Design. Unit sizes keep the
+    // upload valid for the assembly and solve.
+    std::vector<double> ones(std::max<std::size_t>(n, 1), 1.0);
+    ktg_netlist_view view{static_cast<int64_t>(V), static_cast<int64_t>(n),
+                          static_cast<int64_t>(nl.nets.size()), movVertex.data(), varOf.data(),
+                          nl.fixedX.data(), nl.fixedY.data(), netStart.data(), pinCell.data(),
+                          offX.data(), offY.data(), weight.data(), pinStart.data(), pinNet.data(),
+                          pinQ.data(), ones.data(), ones.data()};
+    check("ktg_upload_netlist", ktg_upload_netlist(c, &view));
+    s.netlist = &nl;
+    s.netlistMovable = n;
+    s.netlistNets = nl.nets.size();
+    s.devX = s.devY = nullptr;
+}
+
+void download(ktg_ctx *c, int axis, SparseSystem &sys, bool hostCsr) {
+    int64_t n = 0, m = 0;
+    check("ktg_system_info", ktg_system_info(c, axis, &n, &m));
+    sys.diag.resize(n);
+    sys.rhs.resize(n);
+    if (hostCsr) {
+        std::vector<int64_t> rp(n + 1);
+        std::vector<int32_t> col(m);
+        sys.val.resize(m);
+        check("ktg_download_system", ktg_download_system(c, axis, rp.data(), col.data(),
+                                                         sys.val.data(), sys.diag.data(),
+                                                         sys.rhs.data()));
+        sys.rowPtr.assign(rp.begin(), rp.end());
+        sys.col.assign(col.begin(), col.end());
+    } else {
+        check("ktg_download_system", ktg_download_system(c, axis, nullptr, nullptr, nullptr,
+                                                         sys.diag.data(), sys.rhs.data()));
+        sys.rowPtr.clear();
+        sys.col.clear();
+        sys.val.clear();
+    }
+}
+
+void upload(ktg_ctx *c, int axis, const SparseSystem &sys) {
+    const std::size_t n = sys.size();
+    if (sys.rowPtr.size() != n + 1)
+        ktlog.fatal("ktplace_b200: system of axis {} has no CSR on the host", axis);
+    std::vector<int64_t> rp(sys.rowPtr.begin(), sys.rowPtr.end());
+    std::vector<int32_t> col(sys.col.begin(), sys.col.end());
+    check("ktg_upload_system",
+          ktg_upload_system(c, axis, static_cast<int64_t>(n), rp.data(), col.data(),
+                            sys.val.data(), sys.diag.data(), sys.rhs.data()));
+}
+
+}  // namespace
+
+void LinearSystems::buildB2B(const std::vector<double> &x, const std::vector<double> &y,
+                             double alpha, const std::vector<double> &anchorX,
+                             const std::vector<double> &anchorY) const {
+    ensureNetlist(netlist);
+    GpuState &s = state();
+    ktg_ctx *c = s.ctx;
+    check("ktg_set_pointer_mode", ktg_set_pointer_mode(c, KTG_PTR_HOST));
+    const bool anchored = alpha > 0.0;
+    check("ktg_build_b2b",
+          ktg_build_b2b(c, x.data(), y.data(), alpha, anchored ? anchorX.data() : nullptr,
+                        anchored ? anchorY.data() : nullptr, floorX, floorY));
+    download(c, KTG_AXIS_X, sysX, s.hostCsr);
+    download(c, KTG_AXIS_Y, sysY, s.hostCsr);
+    s.devX = &sysX;
+    s.devY = &sysY;
+    s.devRows = sysX.size();
+}
+
+// Star model (simpl_lss.cc:116-201): each net of three or more pins with a
+// movable pin gets a star variable after the movable cells; two-pin nets
+// connect their pins directly; springs add w to the diagonal of each movable
+// end, -w off the diagonal towards a movable other end, and the offset (or the
+// fixed position plus offset) to the right-hand side. Assembled on the host;
+// the systems are solved on the GPU by solveBothAxes.
+std::size_t LinearSystems::buildStar() const {
+    const std::size_t numNets = netlist.nets.size();
+    std::vector<std::uint32_t> star(numNets, noVar);
+    std::size_t size = netlist.numMovable;
+    for (std::size_t k = 0; k < numNets; ++k) {
+        const auto &cells = netlist.nets[k].cells;
+        bool anyMovable = false;
+        for (const std::uint32_t v : cells) anyMovable = anyMovable || netlist.varOfVertex[v] != noVar;
+        if (cells.size() >= 3 && anyMovable) star[k] = static_cast<std::uint32_t>(size++);
+    }
+    for (int axis = 0; axis < 2; ++axis) {
+        SparseSystem &sys = axis == 0 ? sysX : sysY;
+        const bool vertical = axis == 0;
+        std::vector<std::vector<std::pair<std::uint32_t, double>>> rows(size);
+        sys.diag.assign(size, 0.0);
+        sys.rhs.assign(size, 0.0);
+        struct End {
+            std::uint32_t var;
+            double offset;
+            double fixed;
+        };
+        auto pull = [&](const End &self, const End &other, double w) {
+            if (self.var == noVar) return;
+            sys.diag[self.var] += w;
+            if (other.var != noVar) {
+                rows[self.var].emplace_back(other.var, -w);
+                sys.rhs[self.var] += w * (other.offset - self.offset);
+            } else {
+                sys.rhs[self.var] += w * (other.fixed + other.offset - self.offset);
+            }
+        };
+        for (std::size_t k = 0; k < numNets; ++k) {
+            const NetPins &net = netlist.nets[k];
+            const std::size_t p = net.cells.size();
+            if (p < 2) continue;
+            auto end = [&](std::size_t q) {
+                const std::uint32_t v = net.cells[q];
+                return End{netlist.varOfVertex[v], vertical ? net.offX[q] : net.offY[q],
+                           vertical ? netlist.fixedX[v] : netlist.fixedY[v]};
+            };
+            if (p == 2) {
+                const End a = end(0), b = end(1);
+                pull(a, b, net.weight);
+                pull(b, a, net.weight);
+            } else if (star[k] != noVar) {
+                const End hub{star[k], 0.0, 0.0};
+                const double w = net.weight * static_cast<double>(p) / static_cast<double>(p - 1);
+                for (std::size_t q = 0; q < p; ++q) {
+                    const End a = end(q);
+                    pull(a, hub, w);
+                    pull(hub, a, w);
+                }
+            }
+        }
+        sys.rowPtr.assign(size + 1, 0);
+        for (std::size_t i = 0; i < size; ++i) {
+            sys.rowPtr[i + 1] = sys.rowPtr[i] + rows[i].size();
+            sys.diag[i] = std::max(sys.diag[i], 1e-12);
+        }
+        sys.col.resize(sys.rowPtr.back());
+        sys.val.resize(sys.rowPtr.back());
+        for (std::size_t i = 0; i < size; ++i) {
+            std::size_t slot = sys.rowPtr[i];
+            for (const auto &[col, v] : rows[i]) {
+                sys.col[slot] = col;
+                sys.val[slot] = v;
+                ++slot;
+            }
+        }
+    }
+    GpuState &s = state();
+    if (s.devX == &sysX || s.devY == &sysY) s.devX = s.devY = nullptr;
+    return size;
+}
+
+Residuals solveBothAxes(const SparseSystem &sysX, std::vector<double> &x, const SparseSystem &sysY,
+                        std::vector<double> &y, double tolerance, std::size_t maxIterations,
+                        const IterateObserver &observe) {
+    GpuState &s = state();
+    ktg_ctx *c = context();
+    check("ktg_set_pointer_mode", ktg_set_pointer_mode(c, KTG_PTR_HOST));
+    const bool current = s.devX == &sysX && s.devY == &sysY && s.devRows == sysX.size() &&
+                         sysY.size() == sysX.size();
+    if (!current) {
+        upload(c, KTG_AXIS_X, sysX);
+        upload(c, KTG_AXIS_Y, sysY);
+        s.devX = &sysX;
+        s.devY = &sysY;
+        s.devRows = sysX.size();
+    }
+    const int64_t cap = observe ? static_cast<int64_t>(std::min<std::size_t>(maxIterations, 1u << 20)) : 0;
+    s.histX.resize(cap);
+    s.histY.resize(cap);
+    ktg_solve_info info{};
+    check("ktg_solve", ktg_solve(c, x.data(), y.data(), tolerance, static_cast<int64_t>(maxIterations),
+                                 &info, cap ? s.histX.data() : nullptr,
+                                 cap ? s.histY.data() : nullptr, cap));
+    if (observe) {
+        const std::size_t k = static_cast<std::size_t>(std::min<int64_t>(info.iters, cap));
+        for (std::size_t it = 1; it <= k; ++it)
+            observe(it, Residuals(s.histX[it - 1], s.histY[it - 1]), it == k && info.live == 0);
+    }
+    return Residuals(info.resid_x, info.resid_y);
+}
+
+}  // namespace ktplace::simpl

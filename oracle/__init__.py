@@ -22,6 +22,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libktref.so")
+# The reference's SimPL linked with the ktplace_b200 drop-in (GPU path).
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libktref_gpu.so")
 PORT_LIB = os.path.join(HERE, "_build", "libktp_oracle.so")
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -42,17 +44,16 @@ def _c(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
-_ref = None
+_refs = {}
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_LIB)
+def ref_available(variant: str = "cpu") -> bool:
+    return os.path.exists(REF_LIB if variant == "cpu" else REF_GPU_LIB)
 
 
-def load_ref():
-    global _ref
-    if _ref is None:
-        lib = ctypes.CDLL(REF_LIB)
+def load_ref(variant: str = "cpu"):
+    if variant not in _refs:
+        lib = ctypes.CDLL(REF_LIB if variant == "cpu" else REF_GPU_LIB)
         lib.ref_set_threads.argtypes = [ctypes.c_int]
         lib.ref_set_threads.restype = ctypes.c_int
         lib.ref_last_error.argtypes = [_vp]
@@ -83,22 +84,23 @@ def load_ref():
         lib.ref_hpwl.restype = ctypes.c_double
         lib.ref_grid.argtypes = [_vp, ctypes.c_uint64, ctypes.c_double, _f64p, _f64p]
         lib.ref_occupancy.argtypes = [_vp, _f64p, _f64p, _f64p, _f64p]
+        lib.ref_run_simpl.argtypes = [_vp, _f64p, ctypes.c_char_p, _f64p, _f64p]
         for f in ("ref_netlist_sizes", "ref_netlist_export", "ref_floors", "ref_build_b2b",
                   "ref_build_star", "ref_system_sizes", "ref_system_export",
-                  "ref_system_import", "ref_solve", "ref_grid", "ref_occupancy"):
+                  "ref_system_import", "ref_solve", "ref_grid", "ref_occupancy", "ref_run_simpl"):
             getattr(lib, f).restype = ctypes.c_int
-        _ref = lib
-    return _ref
+        _refs[variant] = lib
+    return _refs[variant]
 
 
 class RefDesign:
     """One design inside the reference's SimPL data structures."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, variant: str = "cpu"):
         if not handle:
             raise RuntimeError("reference design could not be created")
         self.h = handle
-        self.lib = load_ref()
+        self.lib = load_ref(variant)
         s = (ctypes.c_uint64 * 8)()
         self.lib.ref_netlist_sizes(self.h, s)
         (self.V, self.n, self.N, self.P, self.Pm, self.num_fixed, self.num_obstacles,
@@ -110,13 +112,13 @@ class RefDesign:
             self.h = None
 
     @classmethod
-    def from_bookshelf(cls, directory: str) -> "RefDesign":
-        lib = load_ref()
-        return cls(lib.ref_design_load_bookshelf(directory.encode()))
+    def from_bookshelf(cls, directory: str, variant: str = "cpu") -> "RefDesign":
+        lib = load_ref(variant)
+        return cls(lib.ref_design_load_bookshelf(directory.encode()), variant)
 
     @classmethod
-    def from_netlist(cls, nl) -> "RefDesign":
-        lib = load_ref()
+    def from_netlist(cls, nl, variant: str = "cpu") -> "RefDesign":
+        lib = load_ref(variant)
         mv = _c(nl.mov_vertex, np.uint32)
         fx, fy = _c(nl.fixed_x, np.float64), _c(nl.fixed_y, np.float64)
         ns = _c(nl.net_start, np.uint64)
@@ -132,7 +134,7 @@ class RefDesign:
             nl.num_nets, _p(ns, _u64p), _p(pc, _u32p), _p(ox, _f64p), _p(oy, _f64p),
             _p(w, _f64p), _p(cw, _f64p), _p(ch, _f64p), nl.obstacles.shape[0], _p(ob, _f64p),
             nl.rows.shape[0], _p(rw, _f64p), _p(die, _f64p))
-        return cls(h)
+        return cls(h, variant)
 
     def export(self) -> dict:
         o = dict(
@@ -229,8 +231,22 @@ class RefDesign:
         return occ, float(ov.value)
 
 
-def set_ref_threads(n: int) -> int:
-    return int(load_ref().ref_set_threads(n))
+    def run_simpl(self, cg_tol=1e-4, cg_max_iter=60, max_iters=100, init_iters=15,
+                  seed=20240607, alpha_base=0.02, bins=0, density=1.0, refine_iters=10,
+                  init_net="star"):
+        """Full SimPL (simplDM::run) on a copy of this design; returns the
+        final look-ahead-legalized positions."""
+        o = np.array([cg_tol, cg_max_iter, max_iters, init_iters, seed, alpha_base, bins,
+                      density, refine_iters], dtype=np.float64)
+        x = np.zeros(self.n)
+        y = np.zeros(self.n)
+        self._check(self.lib.ref_run_simpl(self.h, _p(o, _f64p), init_net.encode(),
+                                           _p(x, _f64p), _p(y, _f64p)))
+        return x, y
+
+
+def set_ref_threads(n: int, variant: str = "cpu") -> int:
+    return int(load_ref(variant).ref_set_threads(n))
 
 
 # ---- the C restatement ---------------------------------------------------------

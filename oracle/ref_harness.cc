@@ -441,6 +441,37 @@ int ref_grid(void *hp, uint64_t perAxis, double densityLimit, double *info, doub
     });
 }
 
+// Full SimPL run (simplDM::run, simpl_dm.cc:245-248) on a copy of the design.
+// opts: cgTol, cgMaxIter, maxIters, initMaxIters, seed, alphaBase,
+// binsPerAxis, densityLimit, refineIters; initNet: "star" | "b2b" |
+// "star_b2b". Final (look-ahead legalized) positions go to x, y.
+int ref_run_simpl(void *hp, const double *opts, const char *initNet, double *x, double *y) {
+    auto *h = static_cast<Handle *>(hp);
+    return guarded(h, [&] {
+        SimplOptions o;
+        o.cgTol = opts[0];
+        o.cgMaxIter = static_cast<std::size_t>(opts[1]);
+        o.maxIters = static_cast<std::size_t>(opts[2]);
+        o.initMaxIters = static_cast<std::size_t>(opts[3]);
+        o.seed = static_cast<std::size_t>(opts[4]);
+        o.alphaBase = opts[5];
+        o.binsPerAxis = static_cast<std::size_t>(opts[6]);
+        o.densityLimit = opts[7];
+        o.refineIters = static_cast<std::size_t>(opts[8]);
+        o.initialNetModel = initNet;
+        o.fences = false;
+        o.reportEvery = 0;
+        o.traceEvery = 0;
+        o.cgEvery = 0;
+        o.initCgEvery = 0;
+        simplDM dm(h->design, o);
+        dm.run();
+        const Design &d = dm.getDesign();
+        std::copy(d.x.begin(), d.x.end(), x);
+        std::copy(d.y.begin(), d.y.end(), y);
+    });
+}
+
 // Impl::getOccupancy then Impl::getOverflow on the grid of the last ref_grid.
 int ref_occupancy(void *hp, const double *x, const double *y, double *occ, double *overflow) {
     auto *h = static_cast<Handle *>(hp);

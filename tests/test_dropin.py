@@ -1,0 +1,82 @@
+"""The C++ drop-in (ktplace_b200/dropin/simpl_lss_b200.cc) inside the
+reference's own, unmodified SimPL code.
+
+oracle/_ref/libktref_gpu.so is the reference's SimPL compiled from its sources
+with the drop-in linked in place of simpl_lss.o; oracle/_ref/libktref.so is the
+same code with the reference's simpl_lss.o. The reference interface
+(LinearSystems::buildB2B, solveBothAxes) must give the same systems and
+solutions, and a whole SimPL run must land on the same placement quality.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import oracle  # noqa: E402
+from cases import build_case, TOL, MAX_ITER  # noqa: E402
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (oracle.ref_available("gpu") and oracle.ref_available()),
+                                 reason="oracle/_ref drop-in build not present")]
+
+
+@pytest.mark.parametrize("name", ["tiny_macros", "edge_alpha", "small12k"])
+def test_dropin_interface_matches_reference(name):
+    raw, nl, x, y, ax, ay, alpha, _ = build_case(name)
+    cpu = oracle.RefDesign.from_netlist(nl, "cpu")
+    gpu = oracle.RefDesign.from_netlist(nl, "gpu")
+    a = ax if alpha > 0 else None
+    b = ay if alpha > 0 else None
+    cpu.build_b2b(x, y, alpha, a, b)
+    gpu.build_b2b(x, y, alpha, a, b)
+    for axis in (0, 1):
+        s, t = cpu.system(axis), gpu.system(axis)
+        for k in ("row_ptr", "col", "val", "diag", "rhs"):
+            assert np.array_equal(s[k], t[k]), (axis, k)
+    r = cpu.solve(x, y, TOL, MAX_ITER, hist_cap=MAX_ITER)
+    g = gpu.solve(x, y, TOL, MAX_ITER, hist_cap=MAX_ITER)
+    assert g["iters"] == r["iters"]
+    for k in ("x", "y"):
+        assert np.linalg.norm(g[k] - r[k]) <= 1e-9 * np.linalg.norm(r[k])
+    for k in ("hist_x", "hist_y"):
+        assert np.linalg.norm(g[k] - r[k]) <= 1e-6 * np.linalg.norm(r[k])
+
+
+def test_star_systems_solve_on_gpu():
+    raw, nl, x, y, *_ = build_case("tiny_macros")
+    cpu = oracle.RefDesign.from_netlist(nl, "cpu")
+    gpu = oracle.RefDesign.from_netlist(nl, "gpu")
+    assert cpu.build_star() == gpu.build_star()
+    for axis in (0, 1):
+        s, t = cpu.system(axis), gpu.system(axis)
+        for k in ("row_ptr", "col", "val", "diag", "rhs"):
+            assert np.array_equal(s[k], t[k]), (axis, k)
+    size = cpu.system(0)["diag"].shape[0]
+    ext = np.concatenate([x, np.full(size - x.shape[0], x.mean())])
+    eyt = np.concatenate([y, np.full(size - y.shape[0], y.mean())])
+    r = cpu.solve(ext, eyt, 1e-6, 1000)
+    g = gpu.solve(ext, eyt, 1e-6, 1000)
+    assert g["iters"] == r["iters"]
+    assert np.linalg.norm(g["x"] - r["x"]) <= 1e-9 * np.linalg.norm(r["x"])
+
+
+def test_full_simpl_run_matches_reference():
+    """Whole SimPL flow (star init, B2B rounds, LAL, refinement) with the
+    solve on the GPU: the final HPWL and overflow stay within 0.5% of the
+    CPU run (the trajectories differ only by round-off in the solves)."""
+    raw, nl, *_ = build_case("small12k")
+    cpu = oracle.RefDesign.from_netlist(nl, "cpu")
+    gpu = oracle.RefDesign.from_netlist(nl, "gpu")
+    cx, cy = cpu.run_simpl()
+    gx, gy = gpu.run_simpl()
+    hc, hg = cpu.hpwl(cx, cy), cpu.hpwl(gx, gy)
+    assert abs(hg - hc) <= 5e-3 * hc, (hg, hc)
+    nb = 64 * 64
+    cpu.grid(64, 1.0)
+    _, oc = cpu.occupancy_map(cx, cy, nb)
+    _, og = cpu.occupancy_map(gx, gy, nb)
+    assert abs(og - oc) <= 0.05
