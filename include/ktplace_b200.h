@@ -194,6 +194,8 @@ int ktg_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ,
 /* Sets a kernel-shape option of this context (no reference counterpart; the
  * values are what the project autotuner chooses between):
  *   "pcg_lanes"  1 or 4: threads per matrix row in the PCG SpMV (0 = default)
+ *   "pcg_form"   0: textbook PCG (three grid barriers per iteration),
+ *                1: Chronopoulos-Gear form (two), -1 = default (1)
  * Returns KTG_ERR_ARG for an unknown key or value. */
 int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
 

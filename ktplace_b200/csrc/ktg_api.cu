@@ -107,6 +107,7 @@ void free_systems(ktg_ctx *c) {
         dev_free(s.z);
         dev_free(s.p);
         dev_free(s.ap);
+        dev_free(s.s);
     }
     dev_free(c->x);
     dev_free(c->y);
@@ -132,6 +133,7 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
             if ((rc = dev_alloc(c, &s.z, rows))) return rc;
             if ((rc = dev_alloc(c, &s.p, rows))) return rc;
             if ((rc = dev_alloc(c, &s.ap, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.s, rows))) return rc;
         }
         if ((rc = dev_alloc(c, &c->x, rows))) return rc;
         if ((rc = dev_alloc(c, &c->y, rows))) return rc;
@@ -254,6 +256,11 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         if (value != 0 && value != 1 && value != 4)
             return set_error(c, KTG_ERR_ARG, "pcg_lanes must be 0, 1 or 4");
         c->pcg_lanes = static_cast<int>(value);
+        return KTG_OK;
+    }
+    if (k == "pcg_form") {
+        if (value < -1 || value > 1) return set_error(c, KTG_ERR_ARG, "pcg_form must be -1, 0 or 1");
+        c->pcg_form = static_cast<int>(value);
         return KTG_OK;
     }
     return set_error(c, KTG_ERR_ARG, "unknown option " + k);

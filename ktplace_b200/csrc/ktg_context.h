@@ -29,7 +29,7 @@ struct AxisSystem {
     double *rhs = nullptr;       // [n]
     uint32_t *lo = nullptr;      // [N]
     uint32_t *hi = nullptr;      // [N]
-    double *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;  // [n]
+    double *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr, *s = nullptr;  // [n]
 };
 
 }  // namespace ktg
@@ -43,6 +43,7 @@ struct ktg_ctx {
     std::string err;
     int64_t launches = 0;
     int pcg_lanes = 0;  // 0: library default; 1 or 4 lanes per row in the PCG SpMV
+    int pcg_form = -1;  // -1: library default; 0 textbook PCG, 1 Chronopoulos-Gear
 
     // netlist sizes
     bool have_netlist = false;

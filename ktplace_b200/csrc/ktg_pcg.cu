@@ -50,6 +50,7 @@ struct PcgAxis {
     double *z;
     double *p;
     double *ap;
+    double *s;
     int32_t n;
 };
 
@@ -172,9 +173,6 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
         axis = c >= n0 ? 1 : 0;
         i = c - (axis ? n0 : 0);
     };
-    // Vector accessors: shared-memory slice or global array.
-#define KTG_V(sm, field) (Smem ? sm[l] : sax[axis].field[i])
-
     if (Smem) {
         for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
             int axis;
@@ -415,6 +413,291 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     }
 }
 
+// Chronopoulos-Gear form of the same Jacobi-PCG: the SpMV runs on z
+// (w = A z) and A p is carried by the recurrence s = w + beta s, so r.z, r.r
+// and w.z of one iteration need only two grid barriers instead of three, and
+// the vector updates fuse into one pass:
+//   barrier A -> gamma = r.z, |r|^2: residual, live test, r.z > 0 test
+//   SpMV w = A z, delta = w.z       -> barrier B
+//   pAp = delta - beta gamma / alpha_prev (= p.Ap in exact arithmetic),
+//   pAp > 0 test, alpha; p = z + beta p, s = w + beta s, x += alpha p,
+//   r -= alpha s, z = r / diag, partials of the next gamma and |r|^2.
+// Every test and counter is applied at the same point of the reference's
+// step (simpl_lss.cc:241-262), so iteration counts and observer histories
+// match; p and x round exactly as in the reference, r through s.
+template <bool Smem, int Lanes>
+__global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
+    extern __shared__ double dyn[];
+    __shared__ double scratch[33 * 4];
+    __shared__ PcgAxis sax[2];
+    if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
+    const uint64_t t_start = global_timer_ns();
+    const uint64_t total_deadline = t_start + A.total_timeout_ns;
+    const int32_t r0 = blockIdx.x * A.rows_per_block;
+    const int32_t r1 = min(r0 + A.rows_per_block, A.total_rows);
+    const int32_t R = max(r1 - r0, 0);
+    const int32_t cap = A.rows_per_block;
+    double *sx = dyn, *sr = dyn + cap, *sz = dyn + 2 * cap, *sp = dyn + 3 * cap;
+    double *ss = dyn + 4 * cap, *sw = dyn + 5 * cap, *sd = dyn + 6 * cap;
+    __syncthreads();
+    const int32_t n0 = sax[0].n;
+    auto deadline = [&]() {
+        const uint64_t d = global_timer_ns() + A.barrier_timeout_ns;
+        return d < total_deadline ? d : total_deadline;
+    };
+    auto locate = [&](int32_t l, int &axis, int32_t &i) {
+        const int32_t c = r0 + l;
+        axis = c >= n0 ? 1 : 0;
+        i = c - (axis ? n0 : 0);
+    };
+    // Global homes when the slices do not fit in shared memory:
+    // x -> x, r -> r, z -> z (also the gathered vector), p -> p, s -> s, w -> ap.
+#define KTG_V(sm, field) (Smem ? sm[l] : sax[axis].field[i])
+
+    if (Smem) {
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            sx[l] = sax[axis].x[i];
+            sd[l] = __ldg(sax[axis].diag + i);
+        }
+        __syncthreads();
+    }
+
+    auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
+        if (Lanes == 1) {
+            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(l, axis, i);
+                if (live && !live[axis]) continue;
+                const PcgAxis &S = sax[axis];
+                const double d = Smem ? sd[l] : __ldg(S.diag + i);
+                const double v = own(l, axis, i);
+                const double s = row_offdiag_seq(S, i, d * v, in_of(axis));
+                emit(l, axis, i, v, s);
+            }
+        } else {
+            const int32_t groups = blockDim.x / 4;
+            const int32_t g = threadIdx.x / 4;
+            for (int32_t base = 0; base < R; base += groups) {
+                const int32_t l = base + g;
+                int axis = 0;
+                int32_t i = 0;
+                bool valid = l < R;
+                if (valid) locate(l, axis, i);
+                if (valid && live && !live[axis]) valid = false;
+                const PcgAxis &S = sax[axis];
+                const double s = row_offdiag_vec4(S, i, valid, in_of(axis));
+                if (valid && (threadIdx.x & 3) == 0) {
+                    const double d = Smem ? sd[l] : __ldg(S.diag + i);
+                    const double v = own(l, axis, i);
+                    emit(l, axis, i, v, d * v + s);
+                }
+            }
+        }
+    };
+
+    // ---- start: Ap = A x, r = b - Ap, z = r / diag --------------------------
+    {
+        double acc[6] = {0, 0, 0, 0, 0, 0};  // bb, rz, rr for x then y
+        spmv([&](int32_t l, int axis, int32_t i) { return KTG_V(sx, x); },
+             [&](int axis) -> const double * { return sax[axis].x; },
+             [&](int32_t l, int axis, int32_t i, double, double ap) {
+                 const PcgAxis &S = sax[axis];
+                 const double b = __ldg(S.rhs + i);
+                 const double r = b - ap;
+                 const double d = Smem ? sd[l] : __ldg(S.diag + i);
+                 const double z = r / d;
+                 if (Smem) {
+                     sr[l] = r;
+                     sz[l] = z;
+                 } else {
+                     S.r[i] = r;
+                 }
+                 __stcg(S.z + i, z);
+                 acc[axis * 3 + 0] += b * b;
+                 acc[axis * 3 + 1] += r * z;
+                 acc[axis * 3 + 2] += r * r;
+             },
+             nullptr);
+        double v0[3] = {acc[0], acc[1], acc[2]};
+        double v1[3] = {acc[3], acc[4], acc[5]};
+        const int sl[3] = {kBB, kRZ0, kRR0};
+        const int a0[3] = {0, 0, 0};
+        const int a1[3] = {1, 1, 1};
+        store_partials<3>(A, v0, sl, a0, scratch);
+        store_partials<3>(A, v1, sl, a1, scratch);
+    }
+    if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+
+    double b_norm[2], rho[2], rho_prev[2] = {0.0, 0.0}, alpha_prev[2] = {0.0, 0.0}, resid[2];
+    bool active[2], first[2] = {true, true}, stepped[2] = {false, false};
+    int64_t steps[2] = {0, 0};
+    {
+        double s[4];
+        const int sl[4] = {kBB, kRZ0, kRR0, kBB};
+        const int ax[4] = {0, 0, 0, 1};
+        reduce_partials<4>(A, s, sl, ax, scratch);
+        double t[2];
+        const int sl2[2] = {kRZ0, kRR0};
+        const int ax2[2] = {1, 1};
+        reduce_partials<2>(A, t, sl2, ax2, scratch);
+        const double bb[2] = {s[0], s[3]};
+        const double rz[2] = {s[1], t[0]};
+        const double rr[2] = {s[2], t[1]};
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            b_norm[a] = sqrt(bb[a]);
+            active[a] = b_norm[a] > 0.0;
+            rho[a] = active[a] ? rz[a] : 0.0;
+            resid[a] = active[a] ? sqrt(rr[a]) / b_norm[a] : 0.0;
+        }
+    }
+
+    int64_t it = 0;
+    for (;;) {
+        if (it > 0) {
+            // ---- after barrier A: results of the previous update ---------
+            double s[4];
+            const int sl[4] = {kRR, kRZ, kRR, kRZ};
+            const int ax[4] = {0, 0, 1, 1};
+            reduce_partials<4>(A, s, sl, ax, scratch);
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                if (!stepped[a]) continue;
+                resid[a] = sqrt(s[a * 2 + 0]) / b_norm[a];
+                const double rz = s[a * 2 + 1];
+                if (rz > 0.0) {
+                    rho_prev[a] = rho[a];
+                    rho[a] = rz;
+                } else {
+                    active[a] = false;
+                }
+            }
+            if (blockIdx.x == 0 && threadIdx.x == 0 && it - 1 < A.hist_cap) {
+                if (A.hist_x) A.hist_x[it - 1] = resid[0];
+                if (A.hist_y) A.hist_y[it - 1] = resid[1];
+            }
+        }
+        bool live[2];
+        live[0] = active[0] && resid[0] > A.tol;
+        live[1] = active[1] && resid[1] > A.tol;
+        if (it >= A.max_iter || !(live[0] || live[1])) break;
+
+        // ---- SpMV: w = A z, w.z ---------------------------------------------
+        double wz[2] = {0.0, 0.0};
+        spmv([&](int32_t l, int axis, int32_t i) {
+                 return Smem ? sz[l] : __ldcg(sax[axis].z + i);
+             },
+             [&](int axis) -> const double * { return sax[axis].z; },
+             [&](int32_t l, int axis, int32_t i, double zi, double w) {
+                 if (Smem)
+                     sw[l] = w;
+                 else
+                     sax[axis].ap[i] = w;
+                 wz[axis] += w * zi;
+             },
+             live);
+        {
+            const int sl[2] = {kPAP, kPAP};
+            const int ax[2] = {0, 1};
+            store_partials<2>(A, wz, sl, ax, scratch);
+        }
+        if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+
+        double alpha[2] = {0.0, 0.0}, beta[2] = {0.0, 0.0};
+        bool ok[2];
+        {
+            double delta[2];
+            const int sl[2] = {kPAP, kPAP};
+            const int ax[2] = {0, 1};
+            reduce_partials<2>(A, delta, sl, ax, scratch);
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                ok[a] = false;
+                if (!live[a]) continue;
+                double pap = delta[a];
+                if (!first[a]) {
+                    beta[a] = rho[a] / rho_prev[a];
+                    pap = delta[a] - beta[a] * rho[a] / alpha_prev[a];
+                }
+                ok[a] = pap > 0.0;
+                if (ok[a]) alpha[a] = rho[a] / pap;
+            }
+        }
+
+        // ---- fused update ------------------------------------------------
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rr x, rz x, rr y, rz y
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            if (!ok[axis]) continue;
+            const PcgAxis &S = sax[axis];
+            const double zi = KTG_V(sz, z);
+            const double wi = Smem ? sw[l] : S.ap[i];
+            const bool f = first[axis];
+            const double pn = f ? zi : zi + beta[axis] * KTG_V(sp, p);
+            const double sn = f ? wi : wi + beta[axis] * KTG_V(ss, s);
+            KTG_V(sp, p) = pn;
+            KTG_V(ss, s) = sn;
+            const double a = alpha[axis];
+            KTG_V(sx, x) += a * pn;
+            const double r = KTG_V(sr, r) - a * sn;
+            const double d = Smem ? sd[l] : __ldg(S.diag + i);
+            const double z = r / d;
+            KTG_V(sr, r) = r;
+            if (Smem) sz[l] = z;
+            __stcg(S.z + i, z);
+            acc[axis * 2 + 0] += r * r;
+            acc[axis * 2 + 1] += r * z;
+        }
+        {
+            const int sl[4] = {kRR, kRZ, kRR, kRZ};
+            const int ax[4] = {0, 0, 1, 1};
+            store_partials<4>(A, acc, sl, ax, scratch);
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            stepped[a] = ok[a];
+            if (!live[a]) continue;
+            ++steps[a];
+            if (!ok[a]) {
+                active[a] = false;
+                continue;
+            }
+            alpha_prev[a] = alpha[a];
+            first[a] = false;
+        }
+        ++it;
+        if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+    }
+#undef KTG_V
+
+    if (Smem) {
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            sax[axis].x[i] = sx[l];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ktg_solve_info inf;
+        inf.resid_x = resid[0];
+        inf.resid_y = resid[1];
+        inf.iters = it;
+        inf.iters_x = steps[0];
+        inf.iters_y = steps[1];
+        inf.status = kStatusOk;
+        inf.live = ((active[0] && resid[0] > A.tol) ? 1 : 0) |
+                   ((active[1] && resid[1] > A.tol) ? 2 : 0);
+        *A.info = inf;
+    }
+}
+
 __global__ void k_solve_status(const int *status, ktg_solve_info *info) {
     if (*status != kStatusOk) info->status = *status;
 }
@@ -423,18 +706,23 @@ using PcgKernel = void (*)(PcgArgs);
 
 struct Variant {
     PcgKernel fn;
-    bool smem;
-    int lanes;
+    int vecs_per_row;
 };
 
-Variant pick_variant(bool smem, int lanes) {
-    if (smem) return lanes == 4 ? Variant{k_pcg<true, 4>, true, 4} : Variant{k_pcg<true, 1>, true, 1};
-    return lanes == 4 ? Variant{k_pcg<false, 4>, false, 4} : Variant{k_pcg<false, 1>, false, 1};
+// form 0: textbook three-barrier PCG; form 1: Chronopoulos-Gear two-barrier.
+Variant pick_variant(int form, bool smem, int lanes) {
+    if (form == 1) {
+        if (smem) return {lanes == 4 ? k_pcg_cg<true, 4> : k_pcg_cg<true, 1>, 7};
+        return {lanes == 4 ? k_pcg_cg<false, 4> : k_pcg_cg<false, 1>, 7};
+    }
+    if (smem) return {lanes == 4 ? k_pcg<true, 4> : k_pcg<true, 1>, kVecsPerRow};
+    return {lanes == 4 ? k_pcg<false, 4> : k_pcg<false, 1>, kVecsPerRow};
 }
 
 }  // namespace
 
-int pcg_lanes_default = 4;
+int pcg_lanes_default = 1;
+int pcg_form_default = 1;
 
 int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
                  ktg_solve_info *info_dev, double *hist_x, double *hist_y, int64_t hist_cap) {
@@ -443,7 +731,7 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     for (int a = 0; a < 2; ++a) {
         ktg::AxisSystem &s = c->sys[a];
         A.ax[a] = PcgAxis{s.row_ptr, s.col, s.val, s.diag, s.rhs, a ? y : x,
-                          s.r, s.z, s.p, s.ap, static_cast<int32_t>(nsys)};
+                          s.r, s.z, s.p, s.ap, s.s, static_cast<int32_t>(nsys)};
     }
     A.total_rows = static_cast<int32_t>(2 * nsys);
     // One 1024-thread block per SM; small systems use fewer blocks so each
@@ -452,13 +740,15 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(c->num_sms, want)));
     A.rows_per_block = static_cast<int32_t>((A.total_rows + grid - 1) / grid);
     if (A.rows_per_block == 0) A.rows_per_block = 1;
-    const size_t smem = sizeof(double) * kVecsPerRow * static_cast<size_t>(A.rows_per_block);
-    const bool use_smem = smem <= static_cast<size_t>(kPcgSmemBytes);
     const int lanes = c->pcg_lanes > 0 ? c->pcg_lanes : pcg_lanes_default;
-    const Variant v = pick_variant(use_smem, lanes);
+    const int form = c->pcg_form >= 0 ? c->pcg_form : pcg_form_default;
+    const int vecs = pick_variant(form, true, lanes).vecs_per_row;
+    const size_t smem = sizeof(double) * vecs * static_cast<size_t>(A.rows_per_block);
+    const bool use_smem = smem <= static_cast<size_t>(kPcgSmemBytes);
+    const Variant v = pick_variant(form, use_smem, lanes);
     const size_t dyn = use_smem ? smem : 0;
-    static bool attr_set[2][2] = {{false, false}, {false, false}};
-    bool &done = attr_set[use_smem][lanes == 4];
+    static bool attr_set[2][2][2] = {};
+    bool &done = attr_set[form][use_smem][lanes == 4];
     if (!done) {
         KTG_CUDA(c, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kPcgSmemBytes));
