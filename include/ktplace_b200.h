@@ -174,6 +174,38 @@ int ktg_upload_system(ktg_ctx *ctx, int axis, int64_t n, const int64_t *row_ptr,
 int ktg_solve(ktg_ctx *ctx, double *x, double *y, double tol, int64_t max_iter,
               ktg_solve_info *info, double *hist_x, double *hist_y, int64_t hist_cap);
 
+/* Result of ktg_solve_mixed. resid_* is the true relative residual
+ * ||b - A x|| / ||b|| in FP64 at exit. */
+typedef struct {
+    double resid_x;
+    double resid_y;
+    int64_t inner_x;               /* FP32 inner PCG iterations per axis       */
+    int64_t inner_y;
+    int32_t outer_x;               /* FP64 refinement rounds per axis          */
+    int32_t outer_y;
+    int32_t status;                /* KTG_OK or KTG_ERR_TIMEOUT                */
+    int32_t stalled;               /* bit 0 / bit 1: x / y refinement stalled  */
+    int64_t fp64_iters_x;          /* iterations of the FP64 fallback per axis */
+    int64_t fp64_iters_y;
+} ktg_mixed_info;
+
+/* Mixed-precision variant of ktg_solve (no reference counterpart; the
+ * reference solves in FP64 only, simpl_lss.cc:203-290): FP64 iterative
+ * refinement around an FP32 Jacobi-PCG. Each round computes r = b - A x in
+ * FP64, stops an axis once ||r|| / ||b|| <= tol (the true residual), and
+ * otherwise solves A d = r with FP32 values and vectors (FP64 dot products
+ * and alpha/beta) until the inner residual falls below inner_tol * ||r||,
+ * then x += d. max_inner caps the FP32 iterations per axis (and the
+ * iterations of the FP64 fallback below) and max_outer the rounds per axis. A round that does not halve the true residual marks the axis as
+ * stalled; the solve is then finished by the FP64 kernel of ktg_solve from
+ * the current x (in device pointer mode that FP64 pass always follows and
+ * returns at once when both axes have converged). hist_x/hist_y receive the
+ * true residual after each round. Pointer mode applies to x, y, info and
+ * the histories. */
+int ktg_solve_mixed(ktg_ctx *ctx, double *x, double *y, double tol, double inner_tol,
+                    int64_t max_inner, int32_t max_outer, ktg_mixed_info *info,
+                    double *hist_x, double *hist_y, int64_t hist_cap);
+
 /* ---- HPWL and density ---------------------------------------------------- */
 
 /* simplPlacer::Impl::getHpwl (simpl_placer.cc:256-275). */

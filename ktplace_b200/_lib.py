@@ -52,6 +52,14 @@ class SolveInfo(ctypes.Structure):
                 ("live", ctypes.c_int32)]
 
 
+class MixedInfo(ctypes.Structure):
+    _fields_ = [("resid_x", ctypes.c_double), ("resid_y", ctypes.c_double),
+                ("inner_x", ctypes.c_int64), ("inner_y", ctypes.c_int64),
+                ("outer_x", ctypes.c_int32), ("outer_y", ctypes.c_int32),
+                ("status", ctypes.c_int32), ("stalled", ctypes.c_int32),
+                ("fp64_iters_x", ctypes.c_int64), ("fp64_iters_y", ctypes.c_int64)]
+
+
 # (name, restype, argtypes) of every entry point in include/ktplace_b200.h
 SIGNATURES = [
     ("ktg_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
@@ -72,6 +80,9 @@ SIGNATURES = [
                                          _f64p, _f64p, _f64p]),
     ("ktg_solve", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int64, _vp, _vp, _vp,
                                  ctypes.c_int64]),
+    ("ktg_solve_mixed", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int64, ctypes.c_int32, _vp, _vp, _vp,
+                                       ctypes.c_int64]),
     ("ktg_hpwl", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("ktg_set_grid", ctypes.c_int, [_vp, ctypes.POINTER(GridView)]),
     ("ktg_occupancy", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),

@@ -108,6 +108,12 @@ void free_systems(ktg_ctx *c) {
         dev_free(s.p);
         dev_free(s.ap);
         dev_free(s.s);
+        dev_free(s.val32);
+        dev_free(s.d32);
+        dev_free(s.r32);
+        dev_free(s.z32);
+        dev_free(s.p32);
+        dev_free(s.ap32);
     }
     dev_free(c->x);
     dev_free(c->y);
@@ -134,6 +140,11 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
             if ((rc = dev_alloc(c, &s.p, rows))) return rc;
             if ((rc = dev_alloc(c, &s.ap, rows))) return rc;
             if ((rc = dev_alloc(c, &s.s, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.d32, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.r32, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.z32, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.p32, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.ap32, rows))) return rc;
         }
         if ((rc = dev_alloc(c, &c->x, rows))) return rc;
         if ((rc = dev_alloc(c, &c->y, rows))) return rc;
@@ -146,7 +157,9 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
         for (auto &s : c->sys) {
             if ((rc = dev_alloc(c, &s.col, nnz))) return rc;
             if ((rc = dev_alloc(c, &s.val, nnz))) return rc;
+            if ((rc = dev_alloc(c, &s.val32, nnz))) return rc;
         }
+        c->val32_valid = false;
         c->sys_cap_nnz = nnz;
     }
     return KTG_OK;
@@ -197,6 +210,8 @@ int ktg_create(int device, ktg_ctx **out) {
     if ((rc = dev_alloc(c, &c->status, 1))) return fail(rc);
     if ((rc = dev_alloc(c, &c->scalars, 8))) return fail(rc);
     if ((rc = dev_alloc(c, &c->info_dev, 1))) return fail(rc);
+    if ((rc = dev_alloc(c, &c->minfo_dev, 1))) return fail(rc);
+    if (cudaMallocHost(&c->h_minfo, sizeof(ktg_mixed_info)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
     if ((rc = dev_alloc(c, &c->nnz_dev, 2))) return fail(rc);
     if ((rc = reserve_partials(c, 16384))) return fail(rc);
     if (cudaMemset(c->counters, 0, 8 * sizeof(unsigned)) != cudaSuccess) return fail(KTG_ERR_CUDA);
@@ -220,6 +235,8 @@ void ktg_destroy(ktg_ctx *c) {
     dev_free(c->status);
     dev_free(c->scalars);
     dev_free(c->info_dev);
+    dev_free(c->minfo_dev);
+    if (c->h_minfo) cudaFreeHost(c->h_minfo);
     dev_free(c->hist_dev);
     dev_free(c->nnz_dev);
     dev_free(c->avail);
@@ -427,6 +444,7 @@ int ktg_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha, co
     c->sys_n = c->n;
     c->have_system = true;
     c->axis_valid[0] = c->axis_valid[1] = true;
+    c->val32_valid = false;
     if (c->ptr_mode == KTG_PTR_HOST) {
         const int st = device_status(c);
         if (st < 0) return st;
@@ -525,6 +543,7 @@ int ktg_upload_system(ktg_ctx *c, int axis, int64_t n, const int64_t *row_ptr, c
     if ((rc = sync(c))) return rc;
     if (n != c->sys_n) c->axis_valid[1 - axis] = false;
     c->axis_valid[axis] = true;
+    c->val32_valid = false;
     c->sys_n = n;
     c->have_system = c->axis_valid[0] && c->axis_valid[1];
     return KTG_OK;
@@ -566,6 +585,85 @@ int ktg_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter, kt
     if (inf.status != KTG_OK) return set_error(c, inf.status, "PCG barrier wait timed out");
     if (hist_cap > 0) {
         const int64_t k = std::min<int64_t>(inf.iters, hist_cap);
+        if (hist_x && k)
+            KTG_CUDA(c, cudaMemcpy(hist_x, c->hist_dev, sizeof(double) * k, cudaMemcpyDeviceToHost));
+        if (hist_y && k)
+            KTG_CUDA(c, cudaMemcpy(hist_y, c->hist_dev + hist_cap, sizeof(double) * k,
+                                   cudaMemcpyDeviceToHost));
+    }
+    return KTG_OK;
+}
+
+namespace {
+__global__ void k_copy_fp64_iters(const ktg_solve_info *s, ktg_mixed_info *m) {
+    m->fp64_iters_x = s->iters_x;
+    m->fp64_iters_y = s->iters_y;
+    if (s->status != KTG_OK) m->status = s->status;
+    m->resid_x = s->iters_x > 0 ? s->resid_x : m->resid_x;
+    m->resid_y = s->iters_y > 0 ? s->resid_y : m->resid_y;
+}
+}  // namespace
+
+int ktg_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inner_tol,
+                    int64_t max_inner, int32_t max_outer, ktg_mixed_info *info, double *hist_x,
+                    double *hist_y, int64_t hist_cap) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no system to solve");
+    if (c->sys_n > 0 && (!x || !y)) return set_error(c, KTG_ERR_ARG, "null positions");
+    if (!(inner_tol > 0.0 && inner_tol < 1.0) || max_inner < 0 || max_outer < 0 || hist_cap < 0)
+        return set_error(c, KTG_ERR_ARG, "bad mixed-precision parameters");
+    if (hist_cap > 0 && !hist_x && !hist_y) hist_cap = 0;
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int64_t n = c->sys_n;
+    if (c->ptr_mode == KTG_PTR_DEVICE) {
+        ktg_mixed_info *mi = info ? info : c->minfo_dev;
+        if ((rc = ktg::launch_solve_mixed(c, x, y, tol, inner_tol, max_inner, max_outer, mi,
+                                          hist_x, hist_y, hist_cap)))
+            return rc;
+        // FP64 pass: finishes a stalled axis, returns at once otherwise.
+        if ((rc = ktg::launch_solve(c, x, y, tol, max_inner, c->info_dev, nullptr, nullptr, 0)))
+            return rc;
+        k_copy_fp64_iters<<<1, 1, 0, c->stream>>>(c->info_dev, mi);
+        ++c->launches;
+        KTG_CUDA(c, cudaGetLastError());
+        return KTG_OK;
+    }
+    if (hist_cap > c->hist_cap_dev) {
+        if ((rc = dev_alloc(c, &c->hist_dev, 2 * hist_cap))) return rc;
+        c->hist_cap_dev = hist_cap;
+    }
+    if ((rc = upload(c, c->x, x, n))) return rc;
+    if ((rc = upload(c, c->y, y, n))) return rc;
+    if ((rc = ktg::launch_solve_mixed(c, c->x, c->y, tol, inner_tol, max_inner, max_outer,
+                                      c->minfo_dev, hist_x ? c->hist_dev : nullptr,
+                                      hist_y ? c->hist_dev + hist_cap : nullptr, hist_cap)))
+        return rc;
+    KTG_CUDA(c, cudaMemcpyAsync(c->h_minfo, c->minfo_dev, sizeof(ktg_mixed_info),
+                                cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    ktg_mixed_info inf = *c->h_minfo;
+    if (inf.status != KTG_OK) return set_error(c, inf.status, "mixed PCG barrier wait timed out");
+    const bool unfinished = (inf.stalled != 0) || inf.resid_x > tol || inf.resid_y > tol;
+    if (unfinished) {
+        if ((rc = ktg::launch_solve(c, c->x, c->y, tol, max_inner, c->info_dev, nullptr, nullptr, 0)))
+            return rc;
+        KTG_CUDA(c, cudaMemcpyAsync(c->h_info, c->info_dev, sizeof(ktg_solve_info),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        if ((rc = sync(c))) return rc;
+        const ktg_solve_info s = *c->h_info;
+        if (s.status != KTG_OK) return set_error(c, s.status, "PCG barrier wait timed out");
+        inf.fp64_iters_x = s.iters_x;
+        inf.fp64_iters_y = s.iters_y;
+        if (s.iters_x > 0) inf.resid_x = s.resid_x;
+        if (s.iters_y > 0) inf.resid_y = s.resid_y;
+    }
+    KTG_CUDA(c, cudaMemcpyAsync(x, c->x, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    KTG_CUDA(c, cudaMemcpyAsync(y, c->y, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    if (info) *info = inf;
+    if (hist_cap > 0) {
+        const int64_t k = std::min<int64_t>(std::max(inf.outer_x, inf.outer_y), hist_cap);
         if (hist_x && k)
             KTG_CUDA(c, cudaMemcpy(hist_x, c->hist_dev, sizeof(double) * k, cudaMemcpyDeviceToHost));
         if (hist_y && k)

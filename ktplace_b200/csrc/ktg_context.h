@@ -30,6 +30,9 @@ struct AxisSystem {
     uint32_t *lo = nullptr;      // [N]
     uint32_t *hi = nullptr;      // [N]
     double *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr, *s = nullptr;  // [n]
+    // mixed precision: FP32 copy of val and the inner vectors
+    float *val32 = nullptr;                                                 // [cap]
+    float *d32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr;  // [n]
 };
 
 }  // namespace ktg
@@ -65,6 +68,7 @@ struct ktg_ctx {
     ktg::AxisSystem sys[2];
     bool have_system = false;  // both axes valid with sys_n rows
     bool axis_valid[2] = {false, false};
+    bool val32_valid = false;  // sys[*].val32 mirrors sys[*].val
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
     int64_t sys_cap_nnz = 0;  // allocated entries for col/val
@@ -81,6 +85,8 @@ struct ktg_ctx {
     int *status = nullptr;           // [1]
     double *scalars = nullptr;       // [8] hpwl of build, hpwl, overflow, ...
     ktg_solve_info *info_dev = nullptr;
+    ktg_mixed_info *minfo_dev = nullptr;
+    ktg_mixed_info *h_minfo = nullptr;
     double *hist_dev = nullptr;      // [2 * hist_cap_dev]
     int64_t hist_cap_dev = 0;
 
@@ -111,6 +117,9 @@ int launch_solve(ktg_ctx *ctx, double *x, double *y, double tol, int64_t max_ite
                  ktg_solve_info *info_dev, double *hist_x, double *hist_y, int64_t hist_cap);
 int launch_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ_dev,
                      double *overflow_dev);
+int launch_solve_mixed(ktg_ctx *ctx, double *x, double *y, double tol, double inner_tol,
+                       int64_t max_inner, int32_t max_outer, ktg_mixed_info *info_dev,
+                       double *hist_x, double *hist_y, int64_t hist_cap);
 
 int set_error(ktg_ctx *ctx, int code, const std::string &msg);
 int cuda_check(ktg_ctx *ctx, cudaError_t e, const char *what);

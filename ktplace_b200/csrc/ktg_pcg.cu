@@ -173,6 +173,9 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
         axis = c >= n0 ? 1 : 0;
         i = c - (axis ? n0 : 0);
     };
+    // Vector accessors: shared-memory slice or global array.
+#define KTG_V(sm, field) (Smem ? sm[l] : sax[axis].field[i])
+
     if (Smem) {
         for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
             int axis;

@@ -1,0 +1,416 @@
+// Mixed-precision Jacobi-PCG with FP64 iterative refinement (sm_100a).
+//
+// Same systems and stopping rule as solveBothAxes (globalPlacer/simpl/
+// simpl_lss.cc:203-290) but the work is split by precision:
+//   FP64: the outer residual r = b - A x (FP64 values), the true relative
+//         residual ||b - A x|| / ||b|| used as the convergence test, every dot
+//         product (accumulated in double) and the alpha/beta scalars;
+//   FP32: the CSR values, the inner vectors (d, r, z, p, Ap) and the SpMV
+//         inside the correction solve A d = r.
+// One persistent cooperative launch runs all refinement rounds of both axes:
+//   outer: r = b - A x, test ||r|| / ||b|| <= tol, then solve A d = r in FP32
+//          with Jacobi-PCG until ||r_inner|| <= inner_tol * ||r||, x += d.
+// A round that fails to halve the true residual is reported as a stall; the
+// C ABI then finishes the solve with the FP64 kernel from the current x.
+#include "ktg_common.cuh"
+#include "ktg_context.h"
+
+#include <algorithm>
+
+namespace ktg {
+namespace {
+
+constexpr int kMixThreads = 1024;
+
+struct MixAxis {
+    const int32_t *rp;
+    const int32_t *col;
+    const double *val;
+    const float *val32;
+    const double *diag;
+    const double *rhs;
+    double *x;
+    double *r;    // outer residual (FP64)
+    float *d;     // correction
+    float *ri;    // inner residual
+    float *z;
+    float *p;
+    float *ap;
+    int32_t n;
+};
+
+struct MixArgs {
+    MixAxis ax[2];
+    int32_t total_rows;
+    int32_t rows_per_block;
+    double tol;
+    double inner_tol;
+    int64_t max_inner;
+    int32_t max_outer;
+    double *part;  // [8 slots][2 axes][grid]
+    unsigned *bar_count;
+    unsigned *bar_gen;
+    int *status;
+    ktg_mixed_info *info;
+    double *hist_x;  // true residual after each refinement round
+    double *hist_y;
+    int64_t hist_cap;
+    uint64_t barrier_timeout_ns;
+    uint64_t total_timeout_ns;
+};
+
+enum MixSlot { kTRR = 0, kTBB = 1, kIRZ0 = 2, kIPAP = 3, kIRR = 4, kIRZ = 5 };
+
+__device__ __forceinline__ double *mslot(const MixArgs &A, int slot, int axis) {
+    return A.part + (static_cast<size_t>(slot) * 2 + axis) * gridDim.x;
+}
+
+template <int K>
+__device__ __forceinline__ void mstore(const MixArgs &A, double (&v)[K], const int (&slot)[K],
+                                       const int (&axis)[K], double *scratch) {
+    block_sum_k<K>(v, scratch);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) __stcg(mslot(A, slot[k], axis[k]) + blockIdx.x, v[k]);
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void mreduce(const MixArgs &A, double (&out)[K], const int (&slot)[K],
+                                        const int (&axis)[K], double *scratch) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = 0.0;
+    for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) out[k] += __ldcg(mslot(A, slot[k], axis[k]) + b);
+    }
+    block_sum_k<K>(out, scratch);
+}
+
+__global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
+    __shared__ double scratch[33 * 4];
+    __shared__ MixAxis sax[2];
+    if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
+    __syncthreads();
+    const uint64_t total_deadline = global_timer_ns() + A.total_timeout_ns;
+    auto deadline = [&]() {
+        const uint64_t d = global_timer_ns() + A.barrier_timeout_ns;
+        return d < total_deadline ? d : total_deadline;
+    };
+    const int32_t r0 = blockIdx.x * A.rows_per_block;
+    const int32_t r1 = min(r0 + A.rows_per_block, A.total_rows);
+    const int32_t n0 = sax[0].n;
+    auto locate = [&](int32_t c, int &axis, int32_t &i) {
+        axis = c >= n0 ? 1 : 0;
+        i = c - (axis ? n0 : 0);
+    };
+    auto sync = [&]() { return grid_barrier(A.bar_count, A.bar_gen, A.status, deadline()); };
+
+    double b_norm[2] = {0.0, 0.0}, true_resid[2] = {0.0, 0.0}, prev_resid[2] = {0.0, 0.0};
+    bool active[2] = {false, false}, stalled[2] = {false, false};
+    int32_t outer[2] = {0, 0};
+    int64_t inner[2] = {0, 0};
+
+    for (int round = 0;; ++round) {
+        // ---- FP64 residual r = b - A x -------------------------------------
+        {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rr x, bb x, rr y, bb y
+            for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(c, axis, i);
+                const MixAxis &S = sax[axis];
+                double s = __ldg(S.diag + i) * __ldcg(S.x + i);
+                const int32_t e1 = __ldg(S.rp + i + 1);
+                for (int32_t e = __ldg(S.rp + i); e < e1; ++e)
+                    s += __ldg(S.val + e) * __ldcg(S.x + __ldg(S.col + e));
+                const double b = __ldg(S.rhs + i);
+                const double r = b - s;
+                S.r[i] = r;
+                acc[axis * 2 + 0] += r * r;
+                acc[axis * 2 + 1] += b * b;
+            }
+            const int sl[4] = {kTRR, kTBB, kTRR, kTBB};
+            const int ax[4] = {0, 0, 1, 1};
+            mstore<4>(A, acc, sl, ax, scratch);
+        }
+        if (!sync()) return;
+        bool live[2];
+        double r_norm[2];
+        {
+            double s[4];
+            const int sl[4] = {kTRR, kTBB, kTRR, kTBB};
+            const int ax[4] = {0, 0, 1, 1};
+            mreduce<4>(A, s, sl, ax, scratch);
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                if (round == 0) {
+                    b_norm[a] = sqrt(s[a * 2 + 1]);
+                    active[a] = b_norm[a] > 0.0;
+                }
+                r_norm[a] = sqrt(s[a * 2 + 0]);
+                if (active[a]) {
+                    prev_resid[a] = true_resid[a];
+                    true_resid[a] = r_norm[a] / b_norm[a];
+                    // a round must at least halve the true residual
+                    if (round > 0 && outer[a] > 0 && !(true_resid[a] < 0.5 * prev_resid[a]) &&
+                        true_resid[a] > A.tol)
+                        stalled[a] = true;
+                }
+                live[a] = active[a] && !stalled[a] && true_resid[a] > A.tol &&
+                          outer[a] < A.max_outer && inner[a] < A.max_inner;
+            }
+            if (blockIdx.x == 0 && threadIdx.x == 0 && round > 0 && round - 1 < A.hist_cap) {
+                if (A.hist_x) A.hist_x[round - 1] = true_resid[0];
+                if (A.hist_y) A.hist_y[round - 1] = true_resid[1];
+            }
+        }
+        if (!(live[0] || live[1])) break;
+
+        // ---- inner FP32 Jacobi-PCG on A d = r ---------------------------------
+        {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rz x, rr x, rz y, rr y
+            for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(c, axis, i);
+                if (!live[axis]) continue;
+                const MixAxis &S = sax[axis];
+                const float r = static_cast<float>(S.r[i]);
+                const float z = r / static_cast<float>(__ldg(S.diag + i));
+                S.ri[i] = r;
+                S.d[i] = 0.0f;
+                S.z[i] = z;
+                __stcg(S.p + i, z);
+                acc[axis * 2 + 0] += static_cast<double>(r) * static_cast<double>(z);
+                acc[axis * 2 + 1] += static_cast<double>(r) * static_cast<double>(r);
+            }
+            const int sl[4] = {kIRZ0, kIRR, kIRZ0, kIRR};
+            const int ax[4] = {0, 0, 1, 1};
+            mstore<4>(A, acc, sl, ax, scratch);
+        }
+        if (!sync()) return;
+        double rho[2] = {0.0, 0.0}, in_resid[2] = {0.0, 0.0}, target[2] = {0.0, 0.0};
+        bool in_live[2];
+        {
+            double s[4];
+            const int sl[4] = {kIRZ0, kIRR, kIRZ0, kIRR};
+            const int ax[4] = {0, 0, 1, 1};
+            mreduce<4>(A, s, sl, ax, scratch);
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                rho[a] = s[a * 2 + 0];
+                in_resid[a] = sqrt(s[a * 2 + 1]);
+                target[a] = A.inner_tol * r_norm[a];
+                in_live[a] = live[a] && rho[a] > 0.0;
+            }
+        }
+        for (;;) {
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+                in_live[a] = in_live[a] && in_resid[a] > target[a] && inner[a] < A.max_inner;
+            if (!(in_live[0] || in_live[1])) break;
+            double pap_acc[2] = {0.0, 0.0};
+            for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(c, axis, i);
+                if (!in_live[axis]) continue;
+                const MixAxis &S = sax[axis];
+                const float pi = __ldcg(S.p + i);
+                float s = static_cast<float>(__ldg(S.diag + i)) * pi;
+                int32_t e = __ldg(S.rp + i);
+                const int32_t e1 = __ldg(S.rp + i + 1);
+                for (; e + 4 <= e1; e += 4) {
+                    const int32_t c0 = __ldg(S.col + e), c1 = __ldg(S.col + e + 1);
+                    const int32_t c2 = __ldg(S.col + e + 2), c3 = __ldg(S.col + e + 3);
+                    const float g0 = __ldcg(S.p + c0), g1 = __ldcg(S.p + c1);
+                    const float g2 = __ldcg(S.p + c2), g3 = __ldcg(S.p + c3);
+                    s += __ldg(S.val32 + e) * g0;
+                    s += __ldg(S.val32 + e + 1) * g1;
+                    s += __ldg(S.val32 + e + 2) * g2;
+                    s += __ldg(S.val32 + e + 3) * g3;
+                }
+                for (; e < e1; ++e) s += __ldg(S.val32 + e) * __ldcg(S.p + __ldg(S.col + e));
+                S.ap[i] = s;
+                pap_acc[axis] += static_cast<double>(pi) * static_cast<double>(s);
+            }
+            {
+                const int sl[2] = {kIPAP, kIPAP};
+                const int ax[2] = {0, 1};
+                mstore<2>(A, pap_acc, sl, ax, scratch);
+            }
+            if (!sync()) return;
+            bool ok[2];
+            float alpha[2] = {0.0f, 0.0f};
+            {
+                double pap[2];
+                const int sl[2] = {kIPAP, kIPAP};
+                const int ax[2] = {0, 1};
+                mreduce<2>(A, pap, sl, ax, scratch);
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    ok[a] = in_live[a] && pap[a] > 0.0;
+                    if (ok[a]) alpha[a] = static_cast<float>(rho[a] / pap[a]);
+                }
+            }
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(c, axis, i);
+                if (!ok[axis]) continue;
+                const MixAxis &S = sax[axis];
+                const float a = alpha[axis];
+                S.d[i] += a * __ldcg(S.p + i);
+                const float r = S.ri[i] - a * S.ap[i];
+                const float z = r / static_cast<float>(__ldg(S.diag + i));
+                S.ri[i] = r;
+                S.z[i] = z;
+                acc[axis * 2 + 0] += static_cast<double>(r) * static_cast<double>(r);
+                acc[axis * 2 + 1] += static_cast<double>(r) * static_cast<double>(z);
+            }
+            {
+                const int sl[4] = {kIRR, kIRZ, kIRR, kIRZ};
+                const int ax[4] = {0, 0, 1, 1};
+                mstore<4>(A, acc, sl, ax, scratch);
+            }
+            if (!sync()) return;
+            float beta[2] = {0.0f, 0.0f};
+            bool ok2[2] = {false, false};
+            {
+                double s[4];
+                const int sl[4] = {kIRR, kIRZ, kIRR, kIRZ};
+                const int ax[4] = {0, 0, 1, 1};
+                mreduce<4>(A, s, sl, ax, scratch);
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    if (!ok[a]) continue;
+                    in_resid[a] = sqrt(s[a * 2 + 0]);
+                    const double rn = s[a * 2 + 1];
+                    ok2[a] = rn > 0.0;
+                    if (ok2[a]) {
+                        beta[a] = static_cast<float>(rn / rho[a]);
+                        rho[a] = rn;
+                    }
+                }
+            }
+            for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(c, axis, i);
+                if (!ok2[axis]) continue;
+                const MixAxis &S = sax[axis];
+                __stcg(S.p + i, S.z[i] + beta[axis] * __ldcg(S.p + i));
+            }
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                if (!in_live[a]) continue;
+                ++inner[a];
+                if (!ok[a] || !ok2[a]) in_live[a] = false;
+            }
+            if (!sync()) return;
+        }
+        // ---- x += d ------------------------------------------------------------
+        for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(c, axis, i);
+            if (!live[axis]) continue;
+            const MixAxis &S = sax[axis];
+            S.x[i] += static_cast<double>(S.d[i]);
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+            if (live[a]) ++outer[a];
+        if (!sync()) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ktg_mixed_info inf;
+        inf.resid_x = true_resid[0];
+        inf.resid_y = true_resid[1];
+        inf.inner_x = inner[0];
+        inf.inner_y = inner[1];
+        inf.outer_x = outer[0];
+        inf.outer_y = outer[1];
+        inf.status = kStatusOk;
+        inf.stalled = (stalled[0] ? 1 : 0) | (stalled[1] ? 2 : 0);
+        inf.fp64_iters_x = 0;
+        inf.fp64_iters_y = 0;
+        *A.info = inf;
+    }
+}
+
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        b[i] = static_cast<float>(a[i]);
+}
+
+__global__ void k_mixed_status(const int *status, ktg_mixed_info *info) {
+    if (*status != kStatusOk) info->status = *status;
+}
+
+}  // namespace
+
+int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inner_tol,
+                       int64_t max_inner, int32_t max_outer, ktg_mixed_info *info_dev,
+                       double *hist_x, double *hist_y, int64_t hist_cap) {
+    const int64_t nsys = c->sys_n;
+    if (!c->val32_valid) {
+        for (int a = 0; a < 2; ++a) {
+            int32_t m = 0;
+            KTG_CUDA(c, cudaMemcpyAsync(&m, c->sys[a].row_ptr + nsys, sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+            if (m > 0) {
+                const int blocks = static_cast<int>(std::min<int64_t>((m + 255) / 256, 4096));
+                k_to_f32<<<blocks, 256, 0, c->stream>>>(c->sys[a].val, c->sys[a].val32, m);
+                ++c->launches;
+            }
+        }
+        c->val32_valid = true;
+    }
+    MixArgs A;
+    for (int a = 0; a < 2; ++a) {
+        ktg::AxisSystem &s = c->sys[a];
+        A.ax[a] = MixAxis{s.row_ptr, s.col, s.val, s.val32, s.diag, s.rhs, a ? y : x, s.r,
+                          s.d32, s.r32, s.z32, s.p32, s.ap32, static_cast<int32_t>(nsys)};
+    }
+    A.total_rows = static_cast<int32_t>(2 * nsys);
+    const int64_t want = (A.total_rows + 1023) / 1024;
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(c->num_sms, want)));
+    A.rows_per_block = static_cast<int32_t>((A.total_rows + grid - 1) / grid);
+    if (A.rows_per_block == 0) A.rows_per_block = 1;
+    int per_sm = 0;
+    KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_mixed, kMixThreads, 0));
+    if (per_sm < 1 || grid > per_sm * c->num_sms)
+        return set_error(c, KTG_ERR_CUDA, "mixed PCG blocks cannot all be resident");
+    if (c->partials_cap < 12 * static_cast<int64_t>(grid))
+        return set_error(c, KTG_ERR_STATE, "partials buffer too small");
+    A.tol = tol;
+    A.inner_tol = inner_tol;
+    A.max_inner = max_inner;
+    A.max_outer = max_outer;
+    A.part = c->partials;
+    A.bar_count = c->counters + 2;
+    A.bar_gen = c->counters + 3;
+    A.status = c->status;
+    A.info = info_dev;
+    A.hist_x = hist_x;
+    A.hist_y = hist_y;
+    A.hist_cap = hist_cap;
+    A.barrier_timeout_ns = 2000000000ull;
+    A.total_timeout_ns = 120000000000ull;
+    KTG_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+    KTG_CUDA(c, cudaMemsetAsync(c->counters + 2, 0, sizeof(unsigned), c->stream));
+    void *args[] = {&A};
+    KTG_CUDA(c, cudaLaunchCooperativeKernel((void *)k_pcg_mixed, dim3(grid), dim3(kMixThreads),
+                                            args, 0, c->stream));
+    k_mixed_status<<<1, 1, 0, c->stream>>>(c->status, info_dev);
+    c->launches += 2;
+    KTG_CUDA(c, cudaGetLastError());
+    return KTG_OK;
+}
+
+}  // namespace ktg

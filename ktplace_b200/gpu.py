@@ -12,7 +12,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import KtgError, NetlistView, GridView, SolveInfo
+from ._lib import KtgError, NetlistView, GridView, SolveInfo, MixedInfo
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -194,6 +194,32 @@ class Context:
         self._set_mode(_lib.KTG_PTR_DEVICE)
         self._check(self.lib.ktg_solve(self.h, _tptr(x), _tptr(y), tol, max_iter, _tptr(info),
                                        _tptr(hist_x), _tptr(hist_y), hist_cap))
+
+    def solve_mixed(self, x, y, tol: float, inner_tol: float = 1e-3, max_inner: int = 100000,
+                    max_outer: int = 50, hist_cap: int = 0, inplace: bool = False) -> dict:
+        """FP32 Jacobi-PCG inside FP64 iterative refinement (host mode)."""
+        self._set_mode(_lib.KTG_PTR_HOST)
+        if not inplace:
+            x, y = _c(x, np.float64).copy(), _c(y, np.float64).copy()
+        info = MixedInfo()
+        hx = np.zeros(hist_cap) if hist_cap else None
+        hy = np.zeros(hist_cap) if hist_cap else None
+        self._check(self.lib.ktg_solve_mixed(self.h, _ptr(x), _ptr(y), tol, inner_tol, max_inner,
+                                             max_outer, ctypes.byref(info), _ptr(hx), _ptr(hy),
+                                             hist_cap))
+        k = max(info.outer_x, info.outer_y)
+        return dict(x=x, y=y, resid=(info.resid_x, info.resid_y),
+                    inner=(int(info.inner_x), int(info.inner_y)),
+                    outer=(int(info.outer_x), int(info.outer_y)), stalled=int(info.stalled),
+                    fp64_iters=(int(info.fp64_iters_x), int(info.fp64_iters_y)),
+                    hist_x=None if hx is None else hx[:min(k, hist_cap)],
+                    hist_y=None if hy is None else hy[:min(k, hist_cap)])
+
+    def solve_mixed_dev(self, x, y, tol: float, inner_tol: float = 1e-3,
+                        max_inner: int = 100000, max_outer: int = 50, info=None):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_solve_mixed(self.h, _tptr(x), _tptr(y), tol, inner_tol,
+                                             max_inner, max_outer, _tptr(info), None, None, 0))
 
     # -- HPWL / density ------------------------------------------------------------
     def hpwl(self, x, y) -> float:
