@@ -39,6 +39,7 @@ ALPHA = 0.2
 TOL = 1e-6
 MAX_ITER = 100000
 GRID = 512
+MIXED_INNER_TOL = 1e-3
 WORKLOAD = ("simpl-global-iteration on synth211k (adaptec1-shaped): B2B build x+y (alpha 0.2), "
             "FP64 Jacobi-PCG x+y warm-start to rtol 1e-6, HPWL, 512x512 density+overflow")
 
@@ -46,11 +47,14 @@ WORKLOAD = ("simpl-global-iteration on synth211k (adaptec1-shaped): B2B build x+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-once", action="store_true",
+                    help="run the workload once (build, FP64 and mixed solves, HPWL, "
+                         "density) for an ncu capture; prints no bench line")
     return ap.parse_args()
 
 
@@ -150,7 +154,7 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -193,6 +197,11 @@ def pcg_bytes(n: int, m: int, iters: int) -> float:
     it = 12.0 * m + 4.0 * (n + 1) + 8.0 * n * 14
     start = 12.0 * m + 4.0 * (n + 1) + 8.0 * n * 6
     return start + iters * it
+
+
+# DRAM bytes (read + write) per launch of the dominant kernel on this
+# workload, from the ncu capture summarised in profiles/k_pcg_synth211k.md.
+NCU_TRAFFIC_BYTES = {"k_pcg_cg": 174.537728e6 + 108.409344e6}
 
 
 def measured_peak():
@@ -288,6 +297,24 @@ def run_ours(args):
     sx_n, sx_m = ctx.system_info(0)
     _, sy_m = ctx.system_info(1)
 
+    # ---- mixed precision on the same systems (breakdown only) --------------
+    from ktplace_b200._lib import MixedInfo
+    minfo = torch.zeros(ctypes.sizeof(MixedInfo), dtype=torch.uint8, device=dev)
+    mixed_ms = []
+    with torch.cuda.stream(stream):
+        ctx.build_b2b_dev(dx, dy, ALPHA, dax, day, fx, fy)
+        for k in range(max(args.steps // 2, 3) + 1):
+            wx.copy_(dx)
+            wy.copy_(dy)
+            flush.zero_()
+            s_starts[0].record(stream)
+            ctx.solve_mixed_dev(wx, wy, TOL, MIXED_INNER_TOL, MAX_ITER, 50, minfo)
+            s_ends[0].record(stream)
+            s_ends[0].synchronize()
+            if k > 0:
+                mixed_ms.append(s_starts[0].elapsed_time(s_ends[0]))
+    mi = MixedInfo.from_buffer_copy(bytes(minfo.cpu().numpy()))
+
     # ---- e2e: host buffers through the C ABI, copies included --------------
     pinned = [torch.tensor(a).pin_memory() for a in (x, y, ax, ay, x, y)]
     hx, hy, hax, hay, px, py = (t.numpy() for t in pinned)
@@ -348,11 +375,18 @@ def run_ours(args):
                        "cg_iters": int(inf.iters), "l2": "flushed between steps",
                        "parallelism": f"replicas x{world} (independent netlists)"},
             "breakdown": {"solve_ms": solve_med, "solve_ms_per_cg_iter": solve_med / inf.iters,
-                          "other_ms": statistics.median(step_ms) - solve_med},
-            "roofline": {"kernel": "k_pcg (persistent cooperative PCG, x+y)", "bound": "hbm",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                          "other_ms": statistics.median(step_ms) - solve_med,
+                          "mixed_solve_ms": statistics.median(mixed_ms),
+                          "mixed_inner_iters": [int(mi.inner_x), int(mi.inner_y)],
+                          "mixed_outer_rounds": [int(mi.outer_x), int(mi.outer_y)],
+                          "mixed_true_resid": [mi.resid_x, mi.resid_y],
+                          "mixed_fp64_fallback_iters": [int(mi.fp64_iters_x),
+                                                        int(mi.fp64_iters_y)]},
+            "roofline": {"kernel": "k_pcg_cg (persistent cooperative PCG, x+y)",
+                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": None, "algorithmic_bytes": byts},
+                         "traffic": NCU_TRAFFIC_BYTES["k_pcg_cg"], "algorithmic_bytes": byts,
+                         "note": "working set is L2-resident: traffic << algorithmic bytes"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -367,8 +401,31 @@ def run_ours(args):
     return 0
 
 
+def profile_once():
+    """The capture workload of profiles/*_synth211k.md: one build, one FP64
+    and one mixed solve, HPWL and the 512x512 density map."""
+    from ktplace_b200.gpu import Context
+    from ktplace_b200 import grid as kgrid
+    raw, nl, x, y, ax, ay = make_workload(1)
+    fx, fy = nl.floors()
+    ctx = Context(0)
+    ctx.upload_netlist(nl)
+    ctx.set_grid(kgrid.build_grid(nl, GRID, 1.0))
+    ctx.build_b2b(x, y, ALPHA, ax, ay, fx, fy)
+    r = ctx.solve(x, y, TOL, MAX_ITER)
+    m = ctx.solve_mixed(x, y, TOL, MIXED_INNER_TOL)
+    h = ctx.hpwl(r["x"], r["y"])
+    _, ov = ctx.occupancy(r["x"], r["y"])
+    print(f"profile-once: {r['iters']} FP64 iterations, mixed inner {m['inner']}, "
+          f"HPWL {h:.6e}, overflow {ov:.4f}")
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile_once:
+        return profile_once()
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
