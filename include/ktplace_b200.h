@@ -221,6 +221,57 @@ int ktg_set_grid(ktg_ctx *ctx, const ktg_grid_view *grid);
 int ktg_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ,
                   double *overflow);
 
+/* ---- batched solves ---------------------------------------------------------- */
+
+/* Many independent systems (the x and y systems of many netlists, of uneven
+ * sizes) solved in one persistent launch of thread-block clusters: one
+ * cluster per system at a time, systems taken from a device work queue
+ * largest first, captured once in a CUDA graph and replayed. Each system is
+ * solved like ktg_solve (precision 0: FP64 Jacobi-PCG, recursive residual)
+ * or like ktg_solve_mixed without the FP64 fallback (precision 1: FP32 PCG in
+ * FP64 refinement, true residual; a stalled system reports status 1). No
+ * reference counterpart: the reference solves one netlist at a time
+ * (simpl_lss.cc:203-290). */
+typedef struct ktg_batch ktg_batch;
+
+typedef struct {
+    int64_t iters;                 /* FP64 iterations, or FP32 inner ones      */
+    int32_t outer;                 /* refinement rounds (precision 1)          */
+    int32_t status;                /* KTG_OK, KTG_ERR_TIMEOUT, or 1 = stalled  */
+    double resid;                  /* final relative residual                  */
+    int64_t latency_ns;            /* device time from dequeue to done         */
+} ktg_batch_result;
+
+int ktg_batch_create(int device, ktg_batch **out);
+void ktg_batch_destroy(ktg_batch *b);
+const char *ktg_batch_last_error(const ktg_batch *b);
+int ktg_batch_set_stream(ktg_batch *b, void *stream);
+int64_t ktg_batch_size(const ktg_batch *b);
+/* Appends one system (host CSR in SparseSystem's layout, start vector x0);
+ * *id receives its index. */
+int ktg_batch_add_system(ktg_batch *b, int64_t n, const int64_t *row_ptr, const int32_t *col,
+                         const double *val, const double *diag, const double *rhs,
+                         const double *x0, int64_t *id);
+/* Appends the x and y systems a context built last (ids first, first+1);
+ * x0/y0 are host start vectors. */
+int ktg_batch_add_from_context(ktg_batch *b, ktg_ctx *ctx, const double *x0, const double *y0,
+                               int64_t *first_id);
+/* Cluster size (1, 2, 4, 8, 16 CTAs) and threads per CTA. */
+int ktg_batch_set_shape(ktg_batch *b, int cluster, int threads);
+int ktg_batch_get_shape(const ktg_batch *b, int *cluster, int *threads);
+/* Times every launchable shape on this batch with an iteration cap of
+ * probe_iter and keeps the fastest (the project autotuner). Resets x. */
+int ktg_batch_autotune(ktg_batch *b, double tol, int precision, double inner_tol,
+                       int64_t probe_iter, int *cluster, int *threads, float *best_ms);
+/* Restores every system's start vector. */
+int ktg_batch_reset_x(ktg_batch *b);
+/* Enqueues the solve of every system on the batch's stream (graph replay). */
+int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, double inner_tol);
+/* Per-system results ([ktg_batch_size]); synchronises the stream. */
+int ktg_batch_results(ktg_batch *b, ktg_batch_result *out);
+int ktg_batch_get_x(ktg_batch *b, int64_t id, double *x);
+int64_t ktg_batch_launch_count(const ktg_batch *b);
+
 /* ---- tuning and introspection ------------------------------------------- */
 
 /* Sets a kernel-shape option of this context (no reference counterpart; the

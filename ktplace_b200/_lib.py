@@ -60,6 +60,11 @@ class MixedInfo(ctypes.Structure):
                 ("fp64_iters_x", ctypes.c_int64), ("fp64_iters_y", ctypes.c_int64)]
 
 
+class BatchResult(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int64), ("outer", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("resid", ctypes.c_double), ("latency_ns", ctypes.c_int64)]
+
+
 # (name, restype, argtypes) of every entry point in include/ktplace_b200.h
 SIGNATURES = [
     ("ktg_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
@@ -88,6 +93,27 @@ SIGNATURES = [
     ("ktg_occupancy", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("ktg_launch_count", ctypes.c_int64, [_vp]),
     ("ktg_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
+    ("ktg_batch_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ktg_batch_destroy", None, [_vp]),
+    ("ktg_batch_last_error", ctypes.c_char_p, [_vp]),
+    ("ktg_batch_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("ktg_batch_size", ctypes.c_int64, [_vp]),
+    ("ktg_batch_add_system", ctypes.c_int, [_vp, ctypes.c_int64, _i64p, _i32p, _f64p, _f64p,
+                                            _f64p, _f64p, _i64p]),
+    ("ktg_batch_add_from_context", ctypes.c_int, [_vp, _vp, _f64p, _f64p, _i64p]),
+    ("ktg_batch_set_shape", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("ktg_batch_get_shape", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int)]),
+    ("ktg_batch_autotune", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_float)]),
+    ("ktg_batch_reset_x", ctypes.c_int, [_vp]),
+    ("ktg_batch_solve", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int64, ctypes.c_int,
+                                       ctypes.c_double]),
+    ("ktg_batch_results", ctypes.c_int, [_vp, _vp]),
+    ("ktg_batch_get_x", ctypes.c_int, [_vp, ctypes.c_int64, _f64p]),
+    ("ktg_batch_launch_count", ctypes.c_int64, [_vp]),
     ("ktg_hpwl_noalloc", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                         ctypes.c_int64, _vp, _vp]),
 ]

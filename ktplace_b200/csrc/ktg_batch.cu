@@ -1,0 +1,757 @@
+// Batched Jacobi-PCG over many independent systems (sm_100a).
+//
+// The solves of solveBothAxes (globalPlacer/simpl/simpl_lss.cc:203-290) for
+// many netlists at once -- x and y of each, of uneven sizes -- in one
+// persistent launch of thread-block clusters:
+//   * one cluster (2-16 CTAs on as many SMs) solves one system at a time; its
+//     CTAs split the rows, meet at hardware cluster barriers, and combine
+//     their dot-product partials through distributed shared memory in a
+//     fixed order (deterministic, identical in every CTA);
+//   * clusters take systems from an atomic work queue ordered largest first,
+//     so uneven sizes balance without any grid-wide synchronisation;
+//   * FP64 Jacobi-PCG (the reference's method), or FP32 Jacobi-PCG inside FP64
+//     iterative refinement (true FP64 residual as the convergence test);
+//   * per system the device records iterations, the final residual and the
+//     solve latency (%globaltimer from dequeue to done).
+// The launch only enqueues work, so the whole batch solve is captured once
+// in a CUDA graph and replayed.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "ktg_common.cuh"
+#include "ktg_context.h"
+#include "ktplace_b200.h"
+
+namespace cg = cooperative_groups;
+
+namespace ktg {
+namespace {
+
+struct SysDesc {
+    int64_t row_base;  // first row in the concatenated vectors
+    int64_t nnz_base;  // first entry in col/val
+    int32_t n;
+    int32_t pad;
+};
+
+struct BatchArgs {
+    const SysDesc *sys;
+    const int32_t *order;  // solve order (largest first)
+    int32_t num_sys;
+    const int32_t *rp;     // system k's row_ptr (local offsets) at row_base + k
+    const int32_t *col;
+    const double *val;
+    const float *val32;
+    const double *diag;
+    const double *rhs;
+    double *x;
+    double *r;
+    double *z;
+    double *p;
+    double *ap;
+    float *d32;
+    float *ri32;
+    float *z32;
+    float *p32;
+    float *ap32;
+    unsigned *queue;
+    ktg_batch_result *results;
+    double tol;
+    double inner_tol;
+    int64_t max_iter;
+    int32_t max_outer;
+    int32_t mixed;
+    uint64_t total_timeout_ns;
+};
+
+// Cluster-wide deterministic sum of K values per thread. Partials are double
+// buffered in shared memory so one cluster barrier per reduction suffices.
+template <int K>
+__device__ __forceinline__ void cluster_sum(double (&v)[K], double *part, int &buf,
+                                            double *scratch, cg::cluster_group &cl) {
+    block_sum_k<K>(v, scratch);
+    double *mine = part + buf * 4;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) mine[k] = v[k];
+    }
+    cl.sync();
+    const unsigned nb = cl.num_blocks();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double t = 0.0;
+        for (unsigned q = 0; q < nb; ++q) t += *cl.map_shared_rank(mine + k, q);
+        v[k] = t;
+    }
+    buf ^= 1;
+}
+
+template <typename T, typename V>
+__device__ __forceinline__ T row_dot(const int32_t *rp, const int32_t *col, const V *val,
+                                     const T *in, int32_t i, T acc) {
+    int32_t e = rp[i];
+    const int32_t e1 = rp[i + 1];
+    for (; e + 4 <= e1; e += 4) {
+        const int32_t c0 = __ldg(col + e), c1 = __ldg(col + e + 1);
+        const int32_t c2 = __ldg(col + e + 2), c3 = __ldg(col + e + 3);
+        const T g0 = __ldcg(in + c0), g1 = __ldcg(in + c1);
+        const T g2 = __ldcg(in + c2), g3 = __ldcg(in + c3);
+        acc += static_cast<T>(__ldg(val + e)) * g0;
+        acc += static_cast<T>(__ldg(val + e + 1)) * g1;
+        acc += static_cast<T>(__ldg(val + e + 2)) * g2;
+        acc += static_cast<T>(__ldg(val + e + 3)) * g3;
+    }
+    for (; e < e1; ++e) acc += static_cast<T>(__ldg(val + e)) * __ldcg(in + __ldg(col + e));
+    return acc;
+}
+
+__global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ double scratch[33 * 4];
+    __shared__ double part[2 * 4];
+    __shared__ int s_job;
+    __shared__ int s_stop;
+    int buf = 0;
+    const unsigned rank = cl.block_rank();
+    const unsigned nb = cl.num_blocks();
+    const uint64_t deadline = global_timer_ns() + A.total_timeout_ns;
+    cl.sync();  // every CTA of the cluster is running before DSMEM is touched
+
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) {
+            s_job = static_cast<int>(atomicAdd(A.queue, 1u));
+            s_stop = global_timer_ns() > deadline ? 1 : 0;
+        }
+        cl.sync();
+        const int job = *cl.map_shared_rank(&s_job, 0);
+        const bool late = *cl.map_shared_rank(&s_stop, 0) != 0;
+        if (job >= A.num_sys) break;
+        const int sid = A.order[job];
+        const SysDesc S = A.sys[sid];
+        const uint64_t t0 = global_timer_ns();
+        const int32_t n = S.n;
+        const int32_t a = static_cast<int32_t>((static_cast<int64_t>(n) * rank) / nb);
+        const int32_t b = static_cast<int32_t>((static_cast<int64_t>(n) * (rank + 1)) / nb);
+        const int32_t *rp = A.rp + S.row_base + sid;
+        const int32_t *col = A.col + S.nnz_base;
+        const double *val = A.val + S.nnz_base;
+        const float *val32 = A.val32 + S.nnz_base;
+        const double *dg = A.diag + S.row_base;
+        const double *rhs = A.rhs + S.row_base;
+        double *x = A.x + S.row_base;
+        double *r = A.r + S.row_base;
+
+        ktg_batch_result res;
+        res.iters = 0;
+        res.outer = 0;
+        res.status = late ? KTG_ERR_TIMEOUT : KTG_OK;
+        double resid = 0.0;
+
+        if (!A.mixed) {
+            double *z = A.z + S.row_base;
+            double *p = A.p + S.row_base;
+            double *ap = A.ap + S.row_base;
+            double v[3] = {0.0, 0.0, 0.0};  // bb, rz, rr
+            for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+                const double s = row_dot<double, double>(rp, col, val, x, i, dg[i] * x[i]);
+                const double bi = rhs[i];
+                const double ri = bi - s;
+                const double zi = ri / dg[i];
+                r[i] = ri;
+                z[i] = zi;
+                __stcg(p + i, zi);
+                v[0] += bi * bi;
+                v[1] += ri * zi;
+                v[2] += ri * ri;
+            }
+            cluster_sum<3>(v, part, buf, scratch, cl);
+            const double bnorm = sqrt(v[0]);
+            bool active = bnorm > 0.0 && !late;
+            double rho = v[1];
+            resid = bnorm > 0.0 ? sqrt(v[2]) / bnorm : 0.0;
+            int64_t it = 0;
+            for (;;) {
+                if (!(active && resid > A.tol && it < A.max_iter)) break;
+                if (rank == 0 && threadIdx.x == 0) s_stop = global_timer_ns() > deadline ? 1 : 0;
+                double w[1] = {0.0};
+                for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+                    const double pi = __ldcg(p + i);
+                    const double s = row_dot<double, double>(rp, col, val, p, i, dg[i] * pi);
+                    ap[i] = s;
+                    w[0] += pi * s;
+                }
+                cluster_sum<1>(w, part, buf, scratch, cl);
+                if (*cl.map_shared_rank(&s_stop, 0)) {
+                    res.status = KTG_ERR_TIMEOUT;
+                    break;
+                }
+                const bool ok = w[0] > 0.0;
+                const double alpha = ok ? rho / w[0] : 0.0;
+                double u[2] = {0.0, 0.0};  // rr, rz
+                if (ok) {
+                    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+                        x[i] += alpha * __ldcg(p + i);
+                        const double ri = r[i] - alpha * ap[i];
+                        const double zi = ri / dg[i];
+                        r[i] = ri;
+                        z[i] = zi;
+                        u[0] += ri * ri;
+                        u[1] += ri * zi;
+                    }
+                }
+                cluster_sum<2>(u, part, buf, scratch, cl);
+                ++it;
+                if (!ok) {
+                    active = false;
+                    continue;
+                }
+                resid = sqrt(u[0]) / bnorm;
+                if (!(u[1] > 0.0)) {
+                    active = false;
+                    continue;
+                }
+                const double beta = u[1] / rho;
+                rho = u[1];
+                for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x)
+                    __stcg(p + i, z[i] + beta * __ldcg(p + i));
+                cl.sync();
+            }
+            res.iters = it;
+        } else {
+            float *d = A.d32 + S.row_base;
+            float *ri = A.ri32 + S.row_base;
+            float *z = A.z32 + S.row_base;
+            float *p = A.p32 + S.row_base;
+            float *ap = A.ap32 + S.row_base;
+            double bnorm = 0.0, prev = 0.0;
+            int64_t inner = 0;
+            int32_t outer = 0;
+            for (int round = 0;; ++round) {
+                double v[2] = {0.0, 0.0};  // rr, bb
+                for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+                    const double s = row_dot<double, double>(rp, col, val, x, i, dg[i] * __ldcg(x + i));
+                    const double bi = rhs[i];
+                    const double rr = bi - s;
+                    r[i] = rr;
+                    v[0] += rr * rr;
+                    v[1] += bi * bi;
+                }
+                cluster_sum<2>(v, part, buf, scratch, cl);
+                if (round == 0) bnorm = sqrt(v[1]);
+                const double rnorm = sqrt(v[0]);
+                prev = resid;
+                resid = bnorm > 0.0 ? rnorm / bnorm : 0.0;
+                const bool stalled = round > 0 && !(resid < 0.5 * prev);
+                if (!(bnorm > 0.0) || late || resid <= A.tol || outer >= A.max_outer ||
+                    inner >= A.max_iter || stalled) {
+                    if (stalled && resid > A.tol) res.status = 1;  // stalled: caller may retry in FP64
+                    break;
+                }
+                double q[2] = {0.0, 0.0};  // rz, rr (inner)
+                for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+                    const float rf = static_cast<float>(r[i]);
+                    const float zf = rf / static_cast<float>(dg[i]);
+                    ri[i] = rf;
+                    d[i] = 0.0f;
+                    z[i] = zf;
+                    __stcg(p + i, zf);
+                    q[0] += static_cast<double>(rf) * zf;
+                    q[1] += static_cast<double>(rf) * rf;
+                }
+                cluster_sum<2>(q, part, buf, scratch, cl);
+                double rho = q[0];
+                double iresid = sqrt(q[1]);
+                const double target = A.inner_tol * rnorm;
+                bool live = rho > 0.0;
+                while (live && iresid > target && inner < A.max_iter) {
+                    double w[1] = {0.0};
+                    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+                        const float pi = __ldcg(p + i);
+                        const float s = row_dot<float, float>(rp, col, val32, p, i,
+                                                              static_cast<float>(dg[i]) * pi);
+                        ap[i] = s;
+                        w[0] += static_cast<double>(pi) * s;
+                    }
+                    cluster_sum<1>(w, part, buf, scratch, cl);
+                    ++inner;
+                    if (!(w[0] > 0.0)) break;
+                    const float alpha = static_cast<float>(rho / w[0]);
+                    double u[2] = {0.0, 0.0};
+                    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+                        d[i] += alpha * __ldcg(p + i);
+                        const float rr = ri[i] - alpha * ap[i];
+                        const float zz = rr / static_cast<float>(dg[i]);
+                        ri[i] = rr;
+                        z[i] = zz;
+                        u[0] += static_cast<double>(rr) * rr;
+                        u[1] += static_cast<double>(rr) * zz;
+                    }
+                    cluster_sum<2>(u, part, buf, scratch, cl);
+                    iresid = sqrt(u[0]);
+                    if (!(u[1] > 0.0)) break;
+                    const float beta = static_cast<float>(u[1] / rho);
+                    rho = u[1];
+                    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x)
+                        __stcg(p + i, z[i] + beta * __ldcg(p + i));
+                    cl.sync();
+                }
+                for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) x[i] += d[i];
+                ++outer;
+                cl.sync();
+            }
+            res.iters = inner;
+            res.outer = outer;
+        }
+        if (rank == 0 && threadIdx.x == 0) {
+            res.resid = resid;
+            res.latency_ns = static_cast<int64_t>(global_timer_ns() - t0);
+            A.results[sid] = res;
+        }
+        cl.sync();  // the job word may be rewritten only after every CTA read it
+    }
+    cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+}  // namespace
+}  // namespace ktg
+
+struct ktg_batch {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    // host mirror of the descriptors
+    std::vector<ktg::SysDesc> sys;
+    std::vector<int64_t> cost;
+    int64_t rows = 0, nnz = 0;     // used
+    int64_t cap_rows = 0, cap_nnz = 0, cap_sys = 0, cap_rp = 0;
+    // device arrays
+    ktg::SysDesc *d_sys = nullptr;
+    int32_t *d_order = nullptr;
+    int32_t *rp = nullptr;  // rows + num_sys entries
+    int32_t *col = nullptr;
+    double *val = nullptr;
+    float *val32 = nullptr;
+    double *diag = nullptr, *rhs = nullptr, *x = nullptr, *x0 = nullptr;
+    double *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
+    float *d32 = nullptr, *ri32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
+    unsigned *queue = nullptr;
+    ktg_batch_result *results = nullptr;
+    bool dirty = true;  // descriptors / order need upload
+    // launch shape
+    int cluster = 8;
+    int threads = 512;
+    // graph cache
+    cudaGraphExec_t graph = nullptr;
+    double g_tol = -1, g_inner = -1;
+    int64_t g_max_iter = -1;
+    int g_mixed = -1, g_cluster = -1, g_threads = -1;
+};
+
+namespace {
+
+int berr(ktg_batch *b, int code, const std::string &m) {
+    if (b) b->err = m;
+    return code;
+}
+
+#define KTG_BCUDA(b, call)                                                          \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess)                                                      \
+            return berr((b), KTG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int grow(ktg_batch *b, T **ptr, int64_t used, int64_t cap) {
+    T *np = nullptr;
+    KTG_BCUDA(b, cudaMalloc(reinterpret_cast<void **>(&np), sizeof(T) * std::max<int64_t>(cap, 1)));
+    if (*ptr && used > 0)
+        KTG_BCUDA(b, cudaMemcpyAsync(np, *ptr, sizeof(T) * used, cudaMemcpyDeviceToDevice, b->stream));
+    KTG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    if (*ptr) cudaFree(*ptr);
+    *ptr = np;
+    return KTG_OK;
+}
+
+// Room for `rows` vector rows, `nnz` entries and `nsys` systems in total.
+int reserve(ktg_batch *b, int64_t rows, int64_t nnz, int64_t nsys) {
+    int rc;
+    if (rows > b->cap_rows) {
+        const int64_t cap = std::max(rows, 2 * b->cap_rows);
+        const int64_t used = b->rows;
+        if ((rc = grow(b, &b->diag, used, cap)) || (rc = grow(b, &b->rhs, used, cap)) ||
+            (rc = grow(b, &b->x, used, cap)) || (rc = grow(b, &b->x0, used, cap)) ||
+            (rc = grow(b, &b->r, 0, cap)) || (rc = grow(b, &b->z, 0, cap)) ||
+            (rc = grow(b, &b->p, 0, cap)) || (rc = grow(b, &b->ap, 0, cap)) ||
+            (rc = grow(b, &b->d32, 0, cap)) || (rc = grow(b, &b->ri32, 0, cap)) ||
+            (rc = grow(b, &b->z32, 0, cap)) || (rc = grow(b, &b->p32, 0, cap)) ||
+            (rc = grow(b, &b->ap32, 0, cap)))
+            return rc;
+        b->cap_rows = cap;
+    }
+    if (rows + nsys > b->cap_rp) {
+        const int64_t cap = std::max(rows + nsys, 2 * b->cap_rp);
+        if ((rc = grow(b, &b->rp, b->rows + static_cast<int64_t>(b->sys.size()), cap))) return rc;
+        b->cap_rp = cap;
+    }
+    if (nsys > b->cap_sys) {
+        const int64_t cap = std::max<int64_t>(nsys, 2 * b->cap_sys);
+        if ((rc = grow(b, &b->d_sys, 0, cap)) || (rc = grow(b, &b->d_order, 0, cap)) ||
+            (rc = grow(b, &b->results, static_cast<int64_t>(b->sys.size()), cap)))
+            return rc;
+        b->cap_sys = cap;
+    }
+    if (nnz > b->cap_nnz) {
+        const int64_t cap = std::max(nnz, 2 * b->cap_nnz);
+        if ((rc = grow(b, &b->col, b->nnz, cap)) || (rc = grow(b, &b->val, b->nnz, cap)) ||
+            (rc = grow(b, &b->val32, b->nnz, cap)))
+            return rc;
+        b->cap_nnz = cap;
+    }
+    return KTG_OK;
+}
+
+__global__ void k_batch_f32(const double *a, float *b, int64_t n) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        b[i] = static_cast<float>(a[i]);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ktg_batch_create(int device, ktg_batch **out) {
+    if (!out) return KTG_ERR_ARG;
+    *out = nullptr;
+    ktg_batch *b = new (std::nothrow) ktg_batch();
+    if (!b) return KTG_ERR_NOMEM;
+    b->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&b->queue, sizeof(unsigned)) != cudaSuccess) {
+        ktg_batch_destroy(b);
+        return KTG_ERR_CUDA;
+    }
+    b->stream = b->own_stream;
+    *out = b;
+    return KTG_OK;
+}
+
+void ktg_batch_destroy(ktg_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    void *ptrs[] = {b->d_sys, b->d_order, b->rp, b->col, b->val, b->val32, b->diag, b->rhs,
+                    b->x, b->x0, b->r, b->z, b->p, b->ap, b->d32, b->ri32, b->z32, b->p32,
+                    b->ap32, b->queue, b->results};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    delete b;
+}
+
+const char *ktg_batch_last_error(const ktg_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int ktg_batch_set_stream(ktg_batch *b, void *stream) {
+    if (!b) return KTG_ERR_ARG;
+    b->stream = stream ? static_cast<cudaStream_t>(stream) : b->own_stream;
+    return KTG_OK;
+}
+
+int64_t ktg_batch_size(const ktg_batch *b) { return b ? static_cast<int64_t>(b->sys.size()) : 0; }
+
+int ktg_batch_add_system(ktg_batch *b, int64_t n, const int64_t *row_ptr, const int32_t *col,
+                         const double *val, const double *diag, const double *rhs,
+                         const double *x0, int64_t *id) {
+    if (!b || n < 0 || !row_ptr || (n > 0 && (!diag || !rhs || !x0))) return KTG_ERR_ARG;
+    const int64_t m = row_ptr[n];
+    if (m < 0 || (m > 0 && (!col || !val))) return KTG_ERR_ARG;
+    if (n > 0x3fffffffll || m > 0x7fffffffll || b->rows + n > 0x7fffffffll ||
+        b->nnz + m > 0x7fffffffll)
+        return berr(b, KTG_ERR_RANGE, "batch exceeds 32-bit indices");
+    std::vector<int32_t> rp(n + 1);
+    for (int64_t i = 0; i <= n; ++i) {
+        if (row_ptr[i] < 0 || (i > 0 && row_ptr[i] < row_ptr[i - 1]))
+            return berr(b, KTG_ERR_ARG, "row_ptr not monotone");
+        rp[i] = static_cast<int32_t>(row_ptr[i]);
+    }
+    for (int64_t e = 0; e < m; ++e)
+        if (col[e] < 0 || col[e] >= n) return berr(b, KTG_ERR_ARG, "col out of range");
+    if (cudaSetDevice(b->device) != cudaSuccess) return KTG_ERR_CUDA;
+    const int64_t nsys = static_cast<int64_t>(b->sys.size()) + 1;
+    int rc = reserve(b, b->rows + n, b->nnz + m, nsys);
+    if (rc) return rc;
+    const int64_t base = b->rows, ebase = b->nnz, k = nsys - 1;
+    KTG_BCUDA(b, cudaMemcpyAsync(b->rp + base + k, rp.data(), sizeof(int32_t) * (n + 1),
+                                 cudaMemcpyHostToDevice, b->stream));
+    if (m) {
+        KTG_BCUDA(b, cudaMemcpyAsync(b->col + ebase, col, sizeof(int32_t) * m, cudaMemcpyHostToDevice, b->stream));
+        KTG_BCUDA(b, cudaMemcpyAsync(b->val + ebase, val, sizeof(double) * m, cudaMemcpyHostToDevice, b->stream));
+    }
+    if (n) {
+        KTG_BCUDA(b, cudaMemcpyAsync(b->diag + base, diag, sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
+        KTG_BCUDA(b, cudaMemcpyAsync(b->rhs + base, rhs, sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
+        KTG_BCUDA(b, cudaMemcpyAsync(b->x + base, x0, sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
+        KTG_BCUDA(b, cudaMemcpyAsync(b->x0 + base, x0, sizeof(double) * n, cudaMemcpyHostToDevice, b->stream));
+    }
+    if (m) {
+        k_batch_f32<<<static_cast<int>(std::min<int64_t>((m + 255) / 256, 4096)), 256, 0, b->stream>>>(
+            b->val + ebase, b->val32 + ebase, m);
+        ++b->launches;
+    }
+    KTG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->sys.push_back(ktg::SysDesc{base, ebase, static_cast<int32_t>(n), 0});
+    b->cost.push_back(m + n);
+    b->rows += n;
+    b->nnz += m;
+    b->dirty = true;
+    if (id) *id = k;
+    return KTG_OK;
+}
+
+int ktg_batch_add_from_context(ktg_batch *b, ktg_ctx *c, const double *x0, const double *y0,
+                               int64_t *first_id) {
+    if (!b || !c || !x0 || !y0) return KTG_ERR_ARG;
+    if (!c->have_system) return berr(b, KTG_ERR_STATE, "context has no systems");
+    int64_t first = -1;
+    for (int axis = 0; axis < 2; ++axis) {
+        int64_t n = 0, m = 0;
+        int rc = ktg_system_info(c, axis, &n, &m);
+        if (rc) return berr(b, rc, "ktg_system_info failed");
+        std::vector<int64_t> rp(n + 1);
+        std::vector<int32_t> col(m);
+        std::vector<double> val(m), dg(n), rhs(n);
+        if ((rc = ktg_download_system(c, axis, rp.data(), col.data(), val.data(), dg.data(), rhs.data())))
+            return berr(b, rc, "ktg_download_system failed");
+        int64_t id = -1;
+        if ((rc = ktg_batch_add_system(b, n, rp.data(), col.data(), val.data(), dg.data(), rhs.data(),
+                                       axis ? y0 : x0, &id)))
+            return rc;
+        if (axis == 0) first = id;
+    }
+    if (first_id) *first_id = first;
+    return KTG_OK;
+}
+
+int ktg_batch_set_shape(ktg_batch *b, int cluster, int threads) {
+    if (!b) return KTG_ERR_ARG;
+    if (!(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8 || cluster == 16))
+        return berr(b, KTG_ERR_ARG, "cluster must be 1, 2, 4, 8 or 16");
+    if (!(threads == 128 || threads == 256 || threads == 512 || threads == 1024))
+        return berr(b, KTG_ERR_ARG, "threads must be 128, 256, 512 or 1024");
+    b->cluster = cluster;
+    b->threads = threads;
+    return KTG_OK;
+}
+
+int ktg_batch_get_shape(const ktg_batch *b, int *cluster, int *threads) {
+    if (!b) return KTG_ERR_ARG;
+    if (cluster) *cluster = b->cluster;
+    if (threads) *threads = b->threads;
+    return KTG_OK;
+}
+
+int ktg_batch_reset_x(ktg_batch *b) {
+    if (!b) return KTG_ERR_ARG;
+    if (b->rows)
+        KTG_BCUDA(b, cudaMemcpyAsync(b->x, b->x0, sizeof(double) * b->rows, cudaMemcpyDeviceToDevice,
+                                     b->stream));
+    return KTG_OK;
+}
+
+// How many clusters of the current shape can be resident at once.
+static int resident_clusters(ktg_batch *b, int *out) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = b->cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(b->threads);
+    cfg.gridDim = dim3(b->cluster);
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (b->cluster > 8)
+        KTG_BCUDA(b, cudaFuncSetAttribute(ktg::k_batch_pcg,
+                                          cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    KTG_BCUDA(b, cudaOccupancyMaxActiveClusters(out, ktg::k_batch_pcg, &cfg));
+    if (*out < 1) return berr(b, KTG_ERR_CUDA, "cluster shape cannot be resident");
+    return KTG_OK;
+}
+
+static int batch_enqueue(ktg_batch *b, double tol, int64_t max_iter, int mixed, double inner_tol,
+                         int max_clusters, cudaStream_t st) {
+    const int ns = static_cast<int>(b->sys.size());
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = b->cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(b->threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int clusters = std::min(max_clusters, std::max(ns, 1));
+    cfg.gridDim = dim3(clusters * b->cluster);
+    ktg::BatchArgs A{b->d_sys, b->d_order, ns, b->rp, b->col, b->val, b->val32, b->diag,
+                     b->rhs, b->x, b->r, b->z, b->p, b->ap, b->d32, b->ri32, b->z32, b->p32,
+                     b->ap32, b->queue, b->results, tol, inner_tol, max_iter, 50, mixed,
+                     120000000000ull};
+    KTG_BCUDA(b, cudaMemsetAsync(b->queue, 0, sizeof(unsigned), st));
+    KTG_BCUDA(b, cudaLaunchKernelEx(&cfg, ktg::k_batch_pcg, A));
+    ++b->launches;
+    return KTG_OK;
+}
+
+int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, double inner_tol) {
+    if (!b) return KTG_ERR_ARG;
+    if (precision != 0 && precision != 1) return berr(b, KTG_ERR_ARG, "precision must be 0 or 1");
+    if (precision == 1 && !(inner_tol > 0.0 && inner_tol < 1.0))
+        return berr(b, KTG_ERR_ARG, "inner_tol must be in (0, 1)");
+    if (max_iter < 0) return berr(b, KTG_ERR_ARG, "negative max_iter");
+    if (b->sys.empty()) return KTG_OK;
+    if (cudaSetDevice(b->device) != cudaSuccess) return KTG_ERR_CUDA;
+    if (b->dirty) {
+        std::vector<int32_t> order(b->sys.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int32_t p, int32_t q) { return b->cost[p] > b->cost[q]; });
+        KTG_BCUDA(b, cudaMemcpyAsync(b->d_sys, b->sys.data(), sizeof(ktg::SysDesc) * b->sys.size(),
+                                     cudaMemcpyHostToDevice, b->stream));
+        KTG_BCUDA(b, cudaMemcpyAsync(b->d_order, order.data(), sizeof(int32_t) * order.size(),
+                                     cudaMemcpyHostToDevice, b->stream));
+        KTG_BCUDA(b, cudaStreamSynchronize(b->stream));
+        b->dirty = false;
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+    }
+    const bool same = b->graph && b->g_tol == tol && b->g_max_iter == max_iter &&
+                      b->g_mixed == precision && b->g_inner == inner_tol &&
+                      b->g_cluster == b->cluster && b->g_threads == b->threads;
+    if (!same) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        int max_clusters = 0;
+        int rc0 = resident_clusters(b, &max_clusters);
+        if (rc0) return rc0;
+        // Capture the whole batch solve once on a private stream.
+        cudaStream_t cap;
+        KTG_BCUDA(b, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        int rc = KTG_OK;
+        if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaStreamDestroy(cap);
+            return berr(b, KTG_ERR_CUDA, "stream capture failed to start");
+        }
+        rc = batch_enqueue(b, tol, max_iter, precision, inner_tol, max_clusters, cap);
+        const cudaError_t ec = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ec != cudaSuccess) return berr(b, KTG_ERR_CUDA, "stream capture failed");
+        const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return berr(b, KTG_ERR_CUDA, "graph instantiation failed");
+        b->g_tol = tol;
+        b->g_max_iter = max_iter;
+        b->g_mixed = precision;
+        b->g_inner = inner_tol;
+        b->g_cluster = b->cluster;
+        b->g_threads = b->threads;
+    }
+    KTG_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
+    ++b->launches;
+    return KTG_OK;
+}
+
+int ktg_batch_results(ktg_batch *b, ktg_batch_result *out) {
+    if (!b || !out) return KTG_ERR_ARG;
+    if (b->sys.empty()) return KTG_OK;
+    KTG_BCUDA(b, cudaMemcpyAsync(out, b->results, sizeof(ktg_batch_result) * b->sys.size(),
+                                 cudaMemcpyDeviceToHost, b->stream));
+    KTG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return KTG_OK;
+}
+
+int ktg_batch_get_x(ktg_batch *b, int64_t id, double *x) {
+    if (!b || !x || id < 0 || id >= static_cast<int64_t>(b->sys.size())) return KTG_ERR_ARG;
+    const ktg::SysDesc &s = b->sys[id];
+    KTG_BCUDA(b, cudaMemcpyAsync(x, b->x + s.row_base, sizeof(double) * s.n, cudaMemcpyDeviceToHost,
+                                 b->stream));
+    KTG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return KTG_OK;
+}
+
+int64_t ktg_batch_launch_count(const ktg_batch *b) { return b ? b->launches : 0; }
+
+int ktg_batch_autotune(ktg_batch *b, double tol, int precision, double inner_tol,
+                       int64_t probe_iter, int *cluster, int *threads, float *best_ms) {
+    if (!b || probe_iter <= 0) return KTG_ERR_ARG;
+    if (b->sys.empty()) return berr(b, KTG_ERR_STATE, "empty batch");
+    static const int kClusters[] = {2, 4, 8, 16};
+    static const int kThreads[] = {256, 512, 1024};
+    cudaEvent_t e0, e1;
+    KTG_BCUDA(b, cudaEventCreate(&e0));
+    KTG_BCUDA(b, cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bc = b->cluster, bt = b->threads;
+    int rc = KTG_OK;
+    for (int c : kClusters) {
+        for (int t : kThreads) {
+            if ((rc = ktg_batch_set_shape(b, c, t))) break;
+            int resident = 0;
+            if (resident_clusters(b, &resident) != KTG_OK) {
+                b->err.clear();
+                continue;  // shape not launchable on this device
+            }
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2 && rc == KTG_OK; ++rep) {
+                if ((rc = ktg_batch_reset_x(b))) break;
+                if (cudaEventRecord(e0, b->stream) != cudaSuccess) rc = KTG_ERR_CUDA;
+                if (!rc) rc = ktg_batch_solve(b, tol, probe_iter, precision, inner_tol);
+                if (!rc && cudaEventRecord(e1, b->stream) != cudaSuccess) rc = KTG_ERR_CUDA;
+                if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = KTG_ERR_CUDA;
+                if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (rc) break;
+            if (ms < best) {
+                best = ms;
+                bc = c;
+                bt = t;
+            }
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    ktg_batch_set_shape(b, bc, bt);
+    if ((rc = ktg_batch_reset_x(b))) return rc;
+    if (cluster) *cluster = bc;
+    if (threads) *threads = bt;
+    if (best_ms) *best_ms = best;
+    return KTG_OK;
+}
+
+}  // extern "C"

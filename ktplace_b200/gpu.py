@@ -253,3 +253,106 @@ class Context:
         self._set_mode(_lib.KTG_PTR_DEVICE)
         self._check(self.lib.ktg_occupancy(self.h, _tptr(x), _tptr(y), _tptr(occ),
                                            _tptr(overflow)))
+
+
+class Batch:
+    """Owns a ``ktg_batch``: many independent systems solved in one
+    persistent cluster launch (see include/ktplace_b200.h)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self.lib.ktg_batch_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise KtgError(rc, f"ktg_batch_create(device={device}) failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ktg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise KtgError(rc, self.lib.ktg_batch_last_error(self.h).decode())
+
+    def __len__(self):
+        return int(self.lib.ktg_batch_size(self.h))
+
+    def set_stream(self, stream_handle: int):
+        self._check(self.lib.ktg_batch_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def add_system(self, s: dict, x0) -> int:
+        rp = _c(s["row_ptr"], np.int64)
+        col = _c(s["col"], np.int32)
+        val, diag, rhs = (_c(s[k], np.float64) for k in ("val", "diag", "rhs"))
+        x0 = _c(x0, np.float64)
+        P = ctypes.POINTER
+        sid = ctypes.c_int64()
+        self._check(self.lib.ktg_batch_add_system(
+            self.h, diag.shape[0], rp.ctypes.data_as(P(ctypes.c_int64)),
+            col.ctypes.data_as(P(ctypes.c_int32)), val.ctypes.data_as(P(ctypes.c_double)),
+            diag.ctypes.data_as(P(ctypes.c_double)), rhs.ctypes.data_as(P(ctypes.c_double)),
+            x0.ctypes.data_as(P(ctypes.c_double)), ctypes.byref(sid)))
+        return int(sid.value)
+
+    def add_from_context(self, ctx: Context, x0, y0) -> int:
+        x0, y0 = _c(x0, np.float64), _c(y0, np.float64)
+        P = ctypes.POINTER(ctypes.c_double)
+        sid = ctypes.c_int64()
+        self._check(self.lib.ktg_batch_add_from_context(self.h, ctx.h, x0.ctypes.data_as(P),
+                                                        y0.ctypes.data_as(P), ctypes.byref(sid)))
+        return int(sid.value)
+
+    def set_shape(self, cluster: int, threads: int):
+        self._check(self.lib.ktg_batch_set_shape(self.h, cluster, threads))
+
+    def shape(self):
+        c, t = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.ktg_batch_get_shape(self.h, ctypes.byref(c), ctypes.byref(t)))
+        return int(c.value), int(t.value)
+
+    def autotune(self, tol: float, precision: int = 1, inner_tol: float = 1e-3,
+                 probe_iter: int = 40):
+        c, t, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        self._check(self.lib.ktg_batch_autotune(self.h, tol, precision, inner_tol, probe_iter,
+                                                ctypes.byref(c), ctypes.byref(t),
+                                                ctypes.byref(ms)))
+        return int(c.value), int(t.value), float(ms.value)
+
+    def reset_x(self):
+        self._check(self.lib.ktg_batch_reset_x(self.h))
+
+    def solve(self, tol: float, max_iter: int = 100000, precision: int = 0,
+              inner_tol: float = 1e-3):
+        """Enqueues the batch solve (asynchronous)."""
+        self._check(self.lib.ktg_batch_solve(self.h, tol, max_iter, precision, inner_tol))
+
+    def results(self):
+        n = len(self)
+        arr = (_lib.BatchResult * max(n, 1))()
+        self._check(self.lib.ktg_batch_results(self.h, ctypes.cast(arr, ctypes.c_void_p)))
+        return [dict(iters=int(r.iters), outer=int(r.outer), status=int(r.status),
+                     resid=float(r.resid), latency_ns=int(r.latency_ns)) for r in arr[:n]]
+
+    def get_x(self, sid: int, n: int) -> np.ndarray:
+        x = np.zeros(max(n, 1))
+        self._check(self.lib.ktg_batch_get_x(self.h, sid,
+                                             x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return x[:n]
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.ktg_batch_launch_count(self.h))

@@ -1,0 +1,91 @@
+"""Batched cluster solver against the oracle.
+
+FP64: every system of a batch of uneven sizes (a 12k-cell design's systems
+next to tiny and corner-case ones) matches the oracle's PCG: same iteration
+count, solution within 1e-9 relative. Mixed: every system meets the
+tolerance on its true FP64 residual. Also: each cluster shape gives the same
+FP64 answer, the autotuner picks a launchable shape, results carry
+latencies, and repeated graph replays are identical.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import oracle  # noqa: E402
+from cases import build_case, TOL, MAX_ITER  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def true_resid(s, x):
+    n = s["diag"].shape[0]
+    rows = np.repeat(np.arange(n), np.diff(s["row_ptr"]))
+    ax = s["diag"] * x
+    np.add.at(ax, rows, s["val"] * x[s["col"]])
+    nb = np.linalg.norm(s["rhs"])
+    return np.linalg.norm(s["rhs"] - ax) / nb if nb > 0 else 0.0
+
+
+@pytest.fixture(scope="module")
+def systems(port_built):
+    out = []
+    for name in ("small12k", "tiny_macros", "edge_alpha", "edge_alpha0"):
+        raw, nl, x, y, ax, ay, alpha, _ = build_case(name)
+        port = oracle.PortNetlist(nl)
+        fx, fy = nl.floors()
+        sx = port.b2b_axis(True, x, fx, alpha, ax if alpha > 0 else None)
+        sy = port.b2b_axis(False, y, fy, alpha, ay if alpha > 0 else None)
+        out += [(sx, x), (sy, y)]
+    return out
+
+
+def make_batch(systems):
+    from ktplace_b200.gpu import Batch
+    b = Batch(0)
+    ids = [b.add_system(s, x0) for s, x0 in systems]
+    return b, ids
+
+
+@pytest.mark.parametrize("cluster,threads", [(2, 256), (8, 512), (16, 1024)])
+def test_batch_fp64_matches_oracle(systems, cluster, threads):
+    b, ids = make_batch(systems)
+    b.set_shape(cluster, threads)
+    b.solve(TOL, MAX_ITER, precision=0)
+    res = b.results()
+    for (s, x0), sid in zip(systems, ids):
+        ref = oracle.port_pcg_axis(s, x0, TOL, MAX_ITER)
+        got = b.get_x(sid, s["diag"].shape[0])
+        assert res[sid]["status"] == 0
+        assert res[sid]["iters"] == ref["iters"], (sid, res[sid], ref["iters"])
+        assert np.linalg.norm(got - ref["x"]) <= 1e-9 * np.linalg.norm(ref["x"])
+        assert res[sid]["latency_ns"] > 0
+    b.close()
+
+
+def test_batch_mixed_meets_true_residual(systems):
+    b, ids = make_batch(systems)
+    b.solve(TOL, MAX_ITER, precision=1, inner_tol=1e-3)
+    res = b.results()
+    for (s, x0), sid in zip(systems, ids):
+        got = b.get_x(sid, s["diag"].shape[0])
+        assert res[sid]["status"] == 0, res[sid]
+        assert true_resid(s, got) <= TOL * 1.0001
+    b.close()
+
+
+def test_batch_autotune_and_replay(systems):
+    b, ids = make_batch(systems)
+    c, t, ms = b.autotune(TOL, precision=0, probe_iter=20)
+    assert c in (2, 4, 8, 16) and t in (256, 512, 1024) and ms > 0
+    b.solve(TOL, MAX_ITER, precision=0)
+    first = [b.get_x(i, s["diag"].shape[0]).copy() for (s, _), i in zip(systems, ids)]
+    b.reset_x()
+    b.solve(TOL, MAX_ITER, precision=0)
+    for (s, _), i, a in zip(systems, ids, first):
+        assert np.array_equal(b.get_x(i, s["diag"].shape[0]), a)
+    b.close()
