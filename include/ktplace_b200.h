@@ -272,6 +272,37 @@ int ktg_batch_results(ktg_batch *b, ktg_batch_result *out);
 int ktg_batch_get_x(ktg_batch *b, int64_t id, double *x);
 int64_t ktg_batch_launch_count(const ktg_batch *b);
 
+/* ---- learned preconditioner ------------------------------------------------ */
+
+/* A learned sparse approximate inverse for ktg_solve_mixed (no reference
+ * counterpart; the reference uses Jacobi only, simpl_lss.cc:203-290):
+ *   M = D^-1/2 (I + S) D^-1/2,  s_e = tanh(<p_i, p_j> / 4) |a_e| / max(d_i, d_j)
+ * on A's own pattern (SPD for any network output, since sum_j |s_ij| <= 1),
+ * where p comes from a 3-layer message-passing network over the cell-net
+ * graph (hidden 64, BF16 tensor-core dense layers, FP32 accumulation).
+ * Training minimises mean ||M A v - v||^2 / n over Rademacher probes v. */
+typedef struct ktg_learned ktg_learned;
+
+int64_t ktg_learned_num_params(void);
+int ktg_learned_create(int device, uint64_t seed, ktg_learned **out);
+void ktg_learned_destroy(ktg_learned *h);
+const char *ktg_learned_last_error(const ktg_learned *h);
+/* "tensor_cores" (1: BF16 mma, 0: FP32 CUDA cores), "lr", "probes", "clip". */
+int ktg_learned_set_option(ktg_learned *h, const char *key, double value);
+/* FP32 parameters in the layout of oracle/learned_ref.py (host memory). */
+int ktg_learned_get_params(ktg_learned *h, float *out);
+int ktg_learned_set_params(ktg_learned *h, const float *in);
+/* Loss and parameter gradient on the current B2B system of one axis of ctx
+ * (probe seed `seed`); grad may be NULL. */
+int ktg_learned_loss_grad(ktg_learned *h, ktg_ctx *ctx, int axis, uint64_t seed, double *loss,
+                          float *grad);
+/* One Adam step (global-norm clipped) on that system. */
+int ktg_learned_train_step(ktg_learned *h, ktg_ctx *ctx, int axis, uint64_t seed, double *loss);
+/* Computes M for both axes of ctx's current systems; ktg_solve_mixed uses it
+ * when ktg_set_option(ctx, "precond", 1). A new build invalidates it. */
+int ktg_learned_prepare(ktg_learned *h, ktg_ctx *ctx);
+int64_t ktg_learned_launch_count(const ktg_learned *h);
+
 /* ---- tuning and introspection ------------------------------------------- */
 
 /* Sets a kernel-shape option of this context (no reference counterpart; the
@@ -279,6 +310,8 @@ int64_t ktg_batch_launch_count(const ktg_batch *b);
  *   "pcg_lanes"  1 or 4: threads per matrix row in the PCG SpMV (0 = default)
  *   "pcg_form"   0: textbook PCG (three grid barriers per iteration),
  *                1: Chronopoulos-Gear form (two), -1 = default (1)
+ *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare) in
+ *                ktg_solve_mixed
  * Returns KTG_ERR_ARG for an unknown key or value. */
 int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
 

@@ -114,6 +114,19 @@ SIGNATURES = [
     ("ktg_batch_results", ctypes.c_int, [_vp, _vp]),
     ("ktg_batch_get_x", ctypes.c_int, [_vp, ctypes.c_int64, _f64p]),
     ("ktg_batch_launch_count", ctypes.c_int64, [_vp]),
+    ("ktg_learned_num_params", ctypes.c_int64, []),
+    ("ktg_learned_create", ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    ("ktg_learned_destroy", None, [_vp]),
+    ("ktg_learned_last_error", ctypes.c_char_p, [_vp]),
+    ("ktg_learned_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_double]),
+    ("ktg_learned_get_params", ctypes.c_int, [_vp, _vp]),
+    ("ktg_learned_set_params", ctypes.c_int, [_vp, _vp]),
+    ("ktg_learned_loss_grad", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint64,
+                                             ctypes.POINTER(ctypes.c_double), _vp]),
+    ("ktg_learned_train_step", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint64,
+                                              ctypes.POINTER(ctypes.c_double)]),
+    ("ktg_learned_prepare", ctypes.c_int, [_vp, _vp]),
+    ("ktg_learned_launch_count", ctypes.c_int64, [_vp]),
     ("ktg_hpwl_noalloc", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                         ctypes.c_int64, _vp, _vp]),
 ]

@@ -114,6 +114,8 @@ void free_systems(ktg_ctx *c) {
         dev_free(s.z32);
         dev_free(s.p32);
         dev_free(s.ap32);
+        dev_free(s.s32);
+        dev_free(s.rs32);
     }
     dev_free(c->x);
     dev_free(c->y);
@@ -145,6 +147,7 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
             if ((rc = dev_alloc(c, &s.z32, rows))) return rc;
             if ((rc = dev_alloc(c, &s.p32, rows))) return rc;
             if ((rc = dev_alloc(c, &s.ap32, rows))) return rc;
+            if ((rc = dev_alloc(c, &s.rs32, rows))) return rc;
         }
         if ((rc = dev_alloc(c, &c->x, rows))) return rc;
         if ((rc = dev_alloc(c, &c->y, rows))) return rc;
@@ -158,8 +161,10 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
             if ((rc = dev_alloc(c, &s.col, nnz))) return rc;
             if ((rc = dev_alloc(c, &s.val, nnz))) return rc;
             if ((rc = dev_alloc(c, &s.val32, nnz))) return rc;
+            if ((rc = dev_alloc(c, &s.s32, nnz))) return rc;
         }
         c->val32_valid = false;
+        c->precond_ready = false;
         c->sys_cap_nnz = nnz;
     }
     return KTG_OK;
@@ -273,6 +278,11 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         if (value != 0 && value != 1 && value != 4)
             return set_error(c, KTG_ERR_ARG, "pcg_lanes must be 0, 1 or 4");
         c->pcg_lanes = static_cast<int>(value);
+        return KTG_OK;
+    }
+    if (k == "precond") {
+        if (value != 0 && value != 1) return set_error(c, KTG_ERR_ARG, "precond must be 0 or 1");
+        c->precond = static_cast<int>(value);
         return KTG_OK;
     }
     if (k == "pcg_form") {
@@ -445,6 +455,7 @@ int ktg_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha, co
     c->have_system = true;
     c->axis_valid[0] = c->axis_valid[1] = true;
     c->val32_valid = false;
+    c->precond_ready = false;
     if (c->ptr_mode == KTG_PTR_HOST) {
         const int st = device_status(c);
         if (st < 0) return st;
@@ -544,6 +555,7 @@ int ktg_upload_system(ktg_ctx *c, int axis, int64_t n, const int64_t *row_ptr, c
     if (n != c->sys_n) c->axis_valid[1 - axis] = false;
     c->axis_valid[axis] = true;
     c->val32_valid = false;
+    c->precond_ready = false;
     c->sys_n = n;
     c->have_system = c->axis_valid[0] && c->axis_valid[1];
     return KTG_OK;

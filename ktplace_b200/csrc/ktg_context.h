@@ -33,6 +33,9 @@ struct AxisSystem {
     // mixed precision: FP32 copy of val and the inner vectors
     float *val32 = nullptr;                                                 // [cap]
     float *d32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr;  // [n]
+    // learned preconditioner: S values on A's pattern and D^-1/2 r scratch
+    float *s32 = nullptr;   // [cap]
+    float *rs32 = nullptr;  // [n]
 };
 
 }  // namespace ktg
@@ -69,6 +72,8 @@ struct ktg_ctx {
     bool have_system = false;  // both axes valid with sys_n rows
     bool axis_valid[2] = {false, false};
     bool val32_valid = false;  // sys[*].val32 mirrors sys[*].val
+    bool precond_ready = false;  // sys[*].s32 holds learned values for the current systems
+    int precond = 0;             // 0 Jacobi, 1 learned (ktg_set_option "precond")
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
     int64_t sys_cap_nnz = 0;  // allocated entries for col/val

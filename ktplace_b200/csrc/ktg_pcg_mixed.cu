@@ -36,6 +36,8 @@ struct MixAxis {
     float *z;
     float *p;
     float *ap;
+    const float *s32;  // learned preconditioner values on A's pattern (null: Jacobi)
+    float *rs;         // D^-1/2 r_inner, published for the preconditioner's gathers
     int32_t n;
 };
 
@@ -85,6 +87,16 @@ __device__ __forceinline__ void mreduce(const MixArgs &A, double (&out)[K], cons
         for (int k = 0; k < K; ++k) out[k] += __ldcg(mslot(A, slot[k], axis[k]) + b);
     }
     block_sum_k<K>(out, scratch);
+}
+
+// z_i = r_i / d_i + d_i^-1/2 sum_e s_e rs_j   (M = D^-1/2 (I + S) D^-1/2)
+__device__ __forceinline__ float apply_m_row(const MixAxis &S, int32_t i, float r) {
+    const float dis = rsqrtf(static_cast<float>(__ldg(S.diag + i)));
+    float acc = 0.0f;
+    const int32_t e1 = __ldg(S.rp + i + 1);
+    for (int32_t e = __ldg(S.rp + i); e < e1; ++e)
+        acc += __ldg(S.s32 + e) * __ldcg(S.rs + __ldg(S.col + e));
+    return r / static_cast<float>(__ldg(S.diag + i)) + dis * acc;
 }
 
 __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
@@ -168,6 +180,22 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
         if (!(live[0] || live[1])) break;
 
         // ---- inner FP32 Jacobi-PCG on A d = r ---------------------------------
+        const bool pre = sax[0].s32 != nullptr;
+        if (pre) {
+            // publish D^-1/2 r before the preconditioner gathers it
+            for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(c, axis, i);
+                if (!live[axis]) continue;
+                const MixAxis &S = sax[axis];
+                const float r = static_cast<float>(S.r[i]);
+                S.ri[i] = r;
+                S.d[i] = 0.0f;
+                __stcg(S.rs + i, r * rsqrtf(static_cast<float>(__ldg(S.diag + i))));
+            }
+            if (!sync()) return;
+        }
         {
             double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rz x, rr x, rz y, rr y
             for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
@@ -177,9 +205,11 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
                 if (!live[axis]) continue;
                 const MixAxis &S = sax[axis];
                 const float r = static_cast<float>(S.r[i]);
-                const float z = r / static_cast<float>(__ldg(S.diag + i));
-                S.ri[i] = r;
-                S.d[i] = 0.0f;
+                const float z = pre ? apply_m_row(S, i, r) : r / static_cast<float>(__ldg(S.diag + i));
+                if (!pre) {
+                    S.ri[i] = r;
+                    S.d[i] = 0.0f;
+                }
                 S.z[i] = z;
                 __stcg(S.p + i, z);
                 acc[axis * 2 + 0] += static_cast<double>(r) * static_cast<double>(z);
@@ -264,11 +294,29 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
                 const float a = alpha[axis];
                 S.d[i] += a * __ldcg(S.p + i);
                 const float r = S.ri[i] - a * S.ap[i];
-                const float z = r / static_cast<float>(__ldg(S.diag + i));
                 S.ri[i] = r;
-                S.z[i] = z;
                 acc[axis * 2 + 0] += static_cast<double>(r) * static_cast<double>(r);
-                acc[axis * 2 + 1] += static_cast<double>(r) * static_cast<double>(z);
+                if (pre) {
+                    __stcg(S.rs + i, r * rsqrtf(static_cast<float>(__ldg(S.diag + i))));
+                } else {
+                    const float z = r / static_cast<float>(__ldg(S.diag + i));
+                    S.z[i] = z;
+                    acc[axis * 2 + 1] += static_cast<double>(r) * static_cast<double>(z);
+                }
+            }
+            if (pre) {
+                if (!sync()) return;
+                for (int32_t c = r0 + threadIdx.x; c < r1; c += blockDim.x) {
+                    int axis;
+                    int32_t i;
+                    locate(c, axis, i);
+                    if (!ok[axis]) continue;
+                    const MixAxis &S = sax[axis];
+                    const float r = S.ri[i];
+                    const float z = apply_m_row(S, i, r);
+                    S.z[i] = z;
+                    acc[axis * 2 + 1] += static_cast<double>(r) * static_cast<double>(z);
+                }
             }
             {
                 const int sl[4] = {kIRR, kIRZ, kIRR, kIRZ};
@@ -374,8 +422,10 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     MixArgs A;
     for (int a = 0; a < 2; ++a) {
         ktg::AxisSystem &s = c->sys[a];
+        const bool pre = c->precond == 1 && c->precond_ready;
         A.ax[a] = MixAxis{s.row_ptr, s.col, s.val, s.val32, s.diag, s.rhs, a ? y : x, s.r,
-                          s.d32, s.r32, s.z32, s.p32, s.ap32, static_cast<int32_t>(nsys)};
+                          s.d32, s.r32, s.z32, s.p32, s.ap32, pre ? s.s32 : nullptr, s.rs32,
+                          static_cast<int32_t>(nsys)};
     }
     A.total_rows = static_cast<int32_t>(2 * nsys);
     const int64_t want = (A.total_rows + 1023) / 1024;

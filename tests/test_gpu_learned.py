@@ -1,0 +1,113 @@
+"""Learned preconditioner on the GPU.
+
+* Gradients of the hand-written training kernels against the float64 CPU
+  oracle (oracle/learned_ref.py) on the same parameters: FP32 CUDA-core path
+  within 2e-3 relative, BF16 tensor-core path within 3e-2 of the FP32 path.
+* M keeps the solve exact: the learned-preconditioned mixed solve meets the
+  true FP64 residual.
+* What training buys: after training on SimPL-style systems of a few small
+  netlists, held-out systems need fewer PCG iterations than with Jacobi.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import oracle  # noqa: E402
+from oracle import learned_ref as lr  # noqa: E402
+from cases import build_case, TOL  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def tiny(port_built):
+    raw, nl, x, y, ax, ay, alpha, _ = build_case("tiny_macros")
+    return raw, nl, x, y, ax, ay, alpha
+
+
+def test_gradients_match_cpu_oracle(tiny, gpu_ctx):
+    from ktplace_b200.learned import Learned
+    raw, nl, x, y, ax, ay, alpha = tiny
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, alpha, ax, ay, fx, fy)
+    params = lr.init_params(7)
+    params["P"] *= 20.0
+    flat = lr.flatten(params).astype(np.float32)
+    learned = Learned(0, seed=1)
+    learned.set_params(flat)
+    learned.set_option("probes", 3)
+    learned.set_option("tensor_cores", 0)
+    s = gpu_ctx.system(0)
+    p32 = lr.unflatten(flat.astype(np.float64))
+    L_ref, g_ref, _ = lr.loss_and_grad(p32, s, nl, k=3, seed=11)
+    L_gpu, g_gpu = learned.loss_grad(gpu_ctx, 0, seed=11)
+    assert abs(L_gpu - L_ref) <= 1e-4 * abs(L_ref)
+    gr = lr.flatten(g_ref)
+    assert rel(g_gpu.astype(np.float64), gr) <= 2e-3
+    for name, shape in lr.PARAM_SHAPES:
+        a = lr.unflatten(g_gpu.astype(np.float64))[name]
+        b = g_ref[name]
+        if np.linalg.norm(b) > 1e-6 * np.linalg.norm(gr):
+            assert rel(a, b) <= 1e-2, name
+    learned.set_option("tensor_cores", 1)
+    L_tc, g_tc = learned.loss_grad(gpu_ctx, 0, seed=11)
+    assert abs(L_tc - L_gpu) <= 3e-2 * abs(L_gpu)
+    assert rel(g_tc, g_gpu) <= 3e-2
+    learned.close()
+
+
+def test_learned_preconditioner_solves_exactly(tiny, gpu_ctx):
+    from ktplace_b200.learned import Learned
+    raw, nl, x, y, ax, ay, alpha = tiny
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, alpha, ax, ay, fx, fy)
+    params = lr.init_params(3)
+    params["P"] *= 30.0
+    learned = Learned(0)
+    learned.set_params(lr.flatten(params).astype(np.float32))
+    learned.prepare(gpu_ctx)
+    gpu_ctx.set_option("precond", 1)
+    r = gpu_ctx.solve_mixed(x, y, TOL, 1e-3)
+    gpu_ctx.set_option("precond", 0)
+    sx = gpu_ctx.system(0)
+    n = sx["diag"].shape[0]
+    rows = np.repeat(np.arange(n), np.diff(sx["row_ptr"]))
+    axv = sx["diag"] * r["x"]
+    np.add.at(axv, rows, sx["val"] * r["x"][sx["col"]])
+    assert np.linalg.norm(sx["rhs"] - axv) / np.linalg.norm(sx["rhs"]) <= TOL * 1.0001
+    learned.close()
+
+
+def test_training_reduces_iterations(gpu_ctx):
+    from ktplace_b200 import synth, netlist
+    from ktplace_b200.learned import Learned, train, compare_solvers
+    designs = []
+    for k in range(4):
+        raw = synth.generate(synth.spec_tiny(seed=60 + k, cells=3000, nets=3300, pads=60, rows=40))
+        nl = netlist.flatten(raw)
+        x0, y0 = synth.seed_positions(raw, nl.num_movable, 5 + k)
+        designs.append((nl, x0, y0))
+    learned = Learned(0, seed=2)
+    learned.set_option("lr", 3e-3)
+    losses = train(learned, designs[:3], iters=6, epochs=3, ctx=gpu_ctx)
+    assert np.mean(losses[-6:]) < np.mean(losses[:6])
+    nl, x0, y0 = designs[3]
+    gpu_ctx.upload_netlist(nl)
+    rows = compare_solvers(learned, gpu_ctx, nl, x0, y0, iters=6)
+    jac = sum(sum(r["jacobi"]["inner"]) for r in rows)
+    lrn = sum(sum(r["learned"]["inner"]) for r in rows)
+    for r in rows:
+        assert max(r["learned"]["resid"]) <= TOL * 1.0001
+    assert lrn < jac, (lrn, jac)
+    learned.close()
