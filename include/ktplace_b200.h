@@ -136,6 +136,13 @@ int ktg_upload_netlist(ktg_ctx *ctx, const ktg_netlist_view *nl);
 int ktg_build_b2b(ktg_ctx *ctx, const double *x, const double *y, double alpha,
                   const double *ax, const double *ay, double floor_x, double floor_y);
 
+/* LinearSystems::buildStar (simpl_lss.cc:116-201) for both axes: the star
+ * model of SimPL's initial rounds, with a star variable after the movable
+ * cells for every net of three or more pins that has a movable pin. *size
+ * receives the number of rows (movable cells + stars); the systems stay on
+ * the device for ktg_solve, bit-identical to the reference's. */
+int ktg_build_star(ktg_ctx *ctx, int64_t *size);
+
 /* HPWL of the positions given to the last ktg_build_b2b, equal to
  * simplPlacer::Impl::getHpwl on those positions (simpl_placer.cc:256-275).
  * Pointer mode applies to `out`. */
@@ -318,6 +325,13 @@ int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
 /* Number of kernels this context has launched since creation (all entry
  * points). */
 int64_t ktg_launch_count(const ktg_ctx *ctx);
+
+/* Test of the bounded device waits: a cooperative launch in which one block
+ * never arrives at a grid barrier, so the other's wait gives up after
+ * timeout_ns (at most 1 s) and reports through the status word; *status_out
+ * receives that status (KTG_ERR_TIMEOUT). Nothing faults and the context
+ * stays usable. No reference counterpart (the reference has no device). */
+int ktg_selftest_wait_timeout(ktg_ctx *ctx, int64_t timeout_ns, int *status_out);
 
 /* ---- allocation-free HPWL ------------------------------------------------ */
 

@@ -77,6 +77,7 @@ SIGNATURES = [
     ("ktg_build_b2b", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _vp, _vp, ctypes.c_double,
                                      ctypes.c_double]),
     ("ktg_build_hpwl", ctypes.c_int, [_vp, _vp]),
+    ("ktg_build_star", ctypes.c_int, [_vp, _i64p]),
     ("ktg_system_info", ctypes.c_int, [_vp, ctypes.c_int, _i64p, _i64p]),
     ("ktg_download_system", ctypes.c_int, [_vp, ctypes.c_int, _i64p, _i32p, _f64p, _f64p,
                                            _f64p]),
@@ -92,6 +93,8 @@ SIGNATURES = [
     ("ktg_set_grid", ctypes.c_int, [_vp, ctypes.POINTER(GridView)]),
     ("ktg_occupancy", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("ktg_launch_count", ctypes.c_int64, [_vp]),
+    ("ktg_selftest_wait_timeout", ctypes.c_int, [_vp, ctypes.c_int64,
+                                                 ctypes.POINTER(ctypes.c_int)]),
     ("ktg_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
     ("ktg_batch_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ktg_batch_destroy", None, [_vp]),

@@ -83,6 +83,7 @@ void free_netlist(ktg_ctx *c) {
     dev_free(c->off_x);
     dev_free(c->off_y);
     dev_free(c->net_base);
+    dev_free(c->net_weight);
     dev_free(c->net_mov);
     dev_free(c->pin_start);
     dev_free(c->pin_ref);
@@ -391,6 +392,7 @@ int ktg_upload_netlist(ktg_ctx *c, const ktg_netlist_view *nl) {
     if ((rc = dev_alloc(c, &c->off_x, P))) return rc;
     if ((rc = dev_alloc(c, &c->off_y, P))) return rc;
     if ((rc = dev_alloc(c, &c->net_base, N))) return rc;
+    if ((rc = dev_alloc(c, &c->net_weight, N))) return rc;
     if ((rc = dev_alloc(c, &c->net_mov, N))) return rc;
     if ((rc = dev_alloc(c, &c->pin_start, n + 1))) return rc;
     if ((rc = dev_alloc(c, &c->pin_ref, Pm))) return rc;
@@ -415,6 +417,7 @@ int ktg_upload_netlist(ktg_ctx *c, const ktg_netlist_view *nl) {
     if ((rc = upload(c, c->off_x, nl->off_x, P))) return rc;
     if ((rc = upload(c, c->off_y, nl->off_y, P))) return rc;
     if ((rc = upload(c, c->net_base, net_base.data(), N))) return rc;
+    if ((rc = upload(c, c->net_weight, nl->net_weight, N))) return rc;
     if ((rc = upload(c, c->net_mov, net_mov.data(), N))) return rc;
     if ((rc = upload(c, c->pin_start, pin_start32.data(), n + 1))) return rc;
     if ((rc = upload(c, c->pin_ref, pin_ref.data(), Pm))) return rc;
@@ -461,6 +464,22 @@ int ktg_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha, co
         if (st < 0) return st;
         if (st != 0) return set_error(c, st, "B2B system exceeds its capacity");
     }
+    return KTG_OK;
+}
+
+int ktg_build_star(ktg_ctx *c, int64_t *size) {
+    if (!c || !size) return KTG_ERR_ARG;
+    if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");
+    int rc = set_device(c);
+    if (rc) return rc;
+    int64_t rows = 0;
+    if ((rc = ktg::build_star(c, &rows, reserve_systems))) return rc;
+    c->sys_n = rows;
+    c->have_system = true;
+    c->axis_valid[0] = c->axis_valid[1] = true;
+    c->val32_valid = false;
+    c->precond_ready = false;
+    *size = rows;
     return KTG_OK;
 }
 

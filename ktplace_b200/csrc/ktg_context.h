@@ -61,7 +61,7 @@ struct ktg_ctx {
     int32_t *var_of_vertex = nullptr;
     double *fixed_x = nullptr, *fixed_y = nullptr;
     int32_t *net_start = nullptr, *pin_cell = nullptr, *pin_var = nullptr;
-    double *off_x = nullptr, *off_y = nullptr, *net_base = nullptr;
+    double *off_x = nullptr, *off_y = nullptr, *net_base = nullptr, *net_weight = nullptr;
     int32_t *net_mov = nullptr;
     int32_t *pin_start = nullptr;
     int2 *pin_ref = nullptr;
@@ -125,6 +125,8 @@ int launch_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ
 int launch_solve_mixed(ktg_ctx *ctx, double *x, double *y, double tol, double inner_tol,
                        int64_t max_inner, int32_t max_outer, ktg_mixed_info *info_dev,
                        double *hist_x, double *hist_y, int64_t hist_cap);
+
+int build_star(ktg_ctx *ctx, int64_t *size_out, int (*reserve)(ktg_ctx *, int64_t, int64_t));
 
 int set_error(ktg_ctx *ctx, int code, const std::string &msg);
 int cuda_check(ktg_ctx *ctx, cudaError_t e, const char *what);

@@ -115,6 +115,12 @@ class Context:
         self._check(self.lib.ktg_build_b2b(self.h, _tptr(x), _tptr(y), alpha, _tptr(ax),
                                            _tptr(ay), floor_x, floor_y))
 
+    def build_star(self) -> int:
+        """LinearSystems::buildStar on the GPU; returns the system size."""
+        size = ctypes.c_int64()
+        self._check(self.lib.ktg_build_star(self.h, ctypes.byref(size)))
+        return int(size.value)
+
     def build_hpwl(self) -> float:
         self._set_mode(_lib.KTG_PTR_HOST)
         out = ctypes.c_double()

@@ -80,3 +80,18 @@ def test_full_simpl_run_matches_reference():
     _, oc = cpu.occupancy_map(cx, cy, nb)
     _, og = cpu.occupancy_map(gx, gy, nb)
     assert abs(og - oc) <= 0.05
+
+
+def test_gpu_star_build_bit_exact(gpu_ctx):
+    """ktg_build_star against the reference's buildStar: same size, same CSR,
+    values, diagonal and right-hand sides, bit for bit."""
+    for name in ("tiny_macros", "edge_alpha", "small12k"):
+        raw, nl, *_ = build_case(name)
+        cpu = oracle.RefDesign.from_netlist(nl, "cpu")
+        size = cpu.build_star()
+        gpu_ctx.upload_netlist(nl)
+        assert gpu_ctx.build_star() == size
+        for axis in (0, 1):
+            s, t = cpu.system(axis), gpu_ctx.system(axis)
+            for k in ("row_ptr", "col", "val", "diag", "rhs"):
+                assert np.array_equal(s[k].astype(np.float64), t[k].astype(np.float64)), (name, axis, k)
