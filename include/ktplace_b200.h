@@ -283,8 +283,10 @@ int64_t ktg_batch_launch_count(const ktg_batch *b);
 
 /* A learned sparse approximate inverse for ktg_solve_mixed (no reference
  * counterpart; the reference uses Jacobi only, simpl_lss.cc:203-290):
- *   M = D^-1/2 (I + S) D^-1/2,  s_e = tanh(<p_i, p_j> / 4) |a_e| / max(d_i, d_j)
- * on A's own pattern (SPD for any network output, since sum_j |s_ij| <= 1),
+ *   M = D^-1/2 (I + S) D^-1/2,  s_e = t_e |a_e| / sqrt(d_i d_j),
+ *   t_e = clamp(tanh(<p_i, p_j> / 4), -0.999, 0.999)
+ * on A's own pattern (SPD for any network output on diagonally dominant
+ * M-matrices such as the B2B systems, since rho(S) < 1),
  * where p comes from a 3-layer message-passing network over the cell-net
  * graph (hidden 64, BF16 tensor-core dense layers, FP32 accumulation).
  * Training minimises mean ||M A v - v||^2 / n over Rademacher probes v. */
@@ -319,6 +321,8 @@ int64_t ktg_learned_launch_count(const ktg_learned *h);
  *                1: Chronopoulos-Gear form (two), -1 = default (1)
  *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare) in
  *                ktg_solve_mixed
+ *   "mixed_form" 1 (default): Chronopoulos-Gear mixed solve with per-block
+ *                shared-memory slices; 0: textbook mixed solve
  * Returns KTG_ERR_ARG for an unknown key or value. */
 int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
 

@@ -281,6 +281,11 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         c->pcg_lanes = static_cast<int>(value);
         return KTG_OK;
     }
+    if (k == "mixed_form") {
+        if (value != 0 && value != 1) return set_error(c, KTG_ERR_ARG, "mixed_form must be 0 or 1");
+        c->mixed_form = static_cast<int>(value);
+        return KTG_OK;
+    }
     if (k == "precond") {
         if (value != 0 && value != 1) return set_error(c, KTG_ERR_ARG, "precond must be 0 or 1");
         c->precond = static_cast<int>(value);

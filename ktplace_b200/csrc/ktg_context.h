@@ -50,6 +50,7 @@ struct ktg_ctx {
     int64_t launches = 0;
     int pcg_lanes = 0;  // 0: library default; 1 or 4 lanes per row in the PCG SpMV
     int pcg_form = -1;  // -1: library default; 0 textbook PCG, 1 Chronopoulos-Gear
+    int mixed_form = 1; // mixed solve: 0 textbook (global vectors), 1 Chronopoulos-Gear
 
     // netlist sizes
     bool have_netlist = false;

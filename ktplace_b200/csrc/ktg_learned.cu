@@ -3,8 +3,11 @@
 // preconditioner values, all in hand-written kernels.
 //
 // Preconditioner (SPD by construction, on A's own sparsity pattern):
-//   M = D^-1/2 (I + S) D^-1/2,  s_e = tanh(<p_i, p_j> / 4) |a_e| / max(d_i, d_j)
-// so sum_j |s_ij| <= 1 and I + S is diagonally dominant. p (16 per cell)
+//   M = D^-1/2 (I + S) D^-1/2,  s_e = t_e |a_e| / sqrt(d_i d_j),
+//   t_e = clamp(tanh(<p_i, p_j> / 4), -0.999, 0.999)
+// |S| <= 0.999 D^-1/2 |A_off| D^-1/2 entrywise, whose spectral radius is at
+// most 1 for the diagonally dominant M-matrices B2B builds, so I + S is SPD
+// (t = 1 would be the first-order Neumann preconditioner). p (16 per cell)
 // comes from a 3-layer message-passing network over the cell-net bipartite
 // graph (hidden width 64, mean aggregation, ReLU):
 //   h0 = relu(x W_in + b_in),  x = 8 per-cell features of the system
@@ -399,7 +402,9 @@ __device__ __forceinline__ int32_t row_of_entry(const int32_t *rp, int32_t n, in
     return lo;
 }
 
-// s_e = tanh(<p_i, p_j>/4) |a_e| / max(d_i, d_j); also stores t_e.
+constexpr float kTMax = 0.999f;
+
+// s_e = clamp(tanh(<p_i, p_j>/4)) |a_e| / sqrt(d_i d_j); also stores t_e.
 __global__ void k_head(const int32_t *rp, const int32_t *col, const double *val,
                        const double *diag, int32_t n, int32_t m, const float *p, float *t_out,
                        float *s_out) {
@@ -415,10 +420,11 @@ __global__ void k_head(const int32_t *rp, const int32_t *col, const double *val,
         const float4 a = pi[q], b = pj[q];
         phi += a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
     }
-    const float t = tanhf(phi * 0.25f);
-    const double dm = diag[i] > diag[j] ? diag[i] : diag[j];
-    const float c = static_cast<float>(fabs(val[e]) / dm);
-    if (t_out) t_out[e] = t;
+    const float th = tanhf(phi * 0.25f);
+    const float t = fminf(fmaxf(th, -kTMax), kTMax);
+    const float c = static_cast<float>(fabs(val[e]) / sqrt(diag[i] * diag[j]));
+    // t_out keeps tanh itself (its clamped slope is zero past the bound)
+    if (t_out) t_out[e] = th;
     s_out[e] = t * c;
 }
 
@@ -501,7 +507,7 @@ __global__ void k_probe_ds(const int32_t *rp, const int32_t *col, const double *
     ds[e] = first ? static_cast<float>(v) : ds[e] + static_cast<float>(v);
 }
 
-// dphi_e = ds_e c_e (1 - t_e^2)
+// dphi_e = ds_e c_e dt/dphi, with dt/dphi = 1 - tanh^2 inside the clamp, 0 outside
 __global__ void k_dphi(const int32_t *rp, const int32_t *col, const double *val,
                        const double *diag, int32_t n, int32_t m, const float *t, const float *ds,
                        float *dphi) {
@@ -509,9 +515,9 @@ __global__ void k_dphi(const int32_t *rp, const int32_t *col, const double *val,
     if (e >= m) return;
     const int32_t i = row_of_entry(rp, n, e);
     const int32_t j = col[e];
-    const double dm = diag[i] > diag[j] ? diag[i] : diag[j];
-    const float c = static_cast<float>(fabs(val[e]) / dm);
-    dphi[e] = ds[e] * c * (1.0f - t[e] * t[e]);
+    const float c = static_cast<float>(fabs(val[e]) / sqrt(diag[i] * diag[j]));
+    const float th = t[e];
+    dphi[e] = fabsf(th) < kTMax ? ds[e] * c * (1.0f - th * th) : 0.0f;
 }
 
 // dp_i = sum over entries e=(i,j) of (dphi_e + dphi_tr(e)) p_j / 4

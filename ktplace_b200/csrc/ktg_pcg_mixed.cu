@@ -21,6 +21,7 @@ namespace ktg {
 namespace {
 
 constexpr int kMixThreads = 1024;
+constexpr int kMixSmemBytes = 216 * 1024;
 
 struct MixAxis {
     const int32_t *rp;
@@ -389,6 +390,288 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
     }
 }
 
+// Chronopoulos-Gear form of the mixed solve, with the block's vector slices
+// in shared memory (x, diag in FP64; r, u, w, p, s, d in FP32). Per inner
+// iteration: w = A u (gather u) and the partials of gamma = r.u, delta = w.u
+// and |r|^2 -> barrier -> alpha, beta (FP64) -> p = u + beta p,
+// s = w + beta s, d += alpha p, r -= alpha s, u = M r -> barrier. With the
+// learned M, u = M r gathers D^-1/2 r of other rows, which adds one barrier.
+__global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
+    extern __shared__ double dyn[];
+    __shared__ double scratch[33 * 4];
+    __shared__ MixAxis sax[2];
+    if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
+    __syncthreads();
+    const uint64_t total_deadline = global_timer_ns() + A.total_timeout_ns;
+    auto deadline = [&]() {
+        const uint64_t d = global_timer_ns() + A.barrier_timeout_ns;
+        return d < total_deadline ? d : total_deadline;
+    };
+    const int32_t r0 = blockIdx.x * A.rows_per_block;
+    const int32_t r1 = min(r0 + A.rows_per_block, A.total_rows);
+    const int32_t R = max(r1 - r0, 0);
+    const int32_t cap = A.rows_per_block;
+    double *sx = dyn, *sd = dyn + cap;
+    float *sr = reinterpret_cast<float *>(dyn + 2 * cap);
+    float *su = sr + cap, *sw = su + cap, *sp = sw + cap, *ss = sp + cap, *sdd = ss + cap;
+    const int32_t n0 = sax[0].n;
+    auto locate = [&](int32_t l, int &axis, int32_t &i) {
+        const int32_t c = r0 + l;
+        axis = c >= n0 ? 1 : 0;
+        i = c - (axis ? n0 : 0);
+    };
+    auto sync = [&]() { return grid_barrier(A.bar_count, A.bar_gen, A.status, deadline()); };
+    const bool pre = sax[0].s32 != nullptr;
+    for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+        int axis;
+        int32_t i;
+        locate(l, axis, i);
+        sx[l] = sax[axis].x[i];
+        sd[l] = __ldg(sax[axis].diag + i);
+    }
+    __syncthreads();
+
+    // u = M r for own rows (learned M), reading the published D^-1/2 r.
+    auto apply_m = [&](const bool *live) {
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            if (!live[axis]) continue;
+            const MixAxis &S = sax[axis];
+            const float u = apply_m_row(S, i, sr[l]);
+            su[l] = u;
+            __stcg(S.z + i, u);
+        }
+    };
+
+    double b_norm[2] = {0.0, 0.0}, true_resid[2] = {0.0, 0.0}, prev_resid[2] = {0.0, 0.0};
+    bool active[2] = {false, false}, stalled[2] = {false, false};
+    int32_t outer[2] = {0, 0};
+    int64_t inner[2] = {0, 0};
+
+    for (int round = 0;; ++round) {
+        // ---- FP64 residual r = b - A x; r32, and u (Jacobi) or D^-1/2 r -----
+        {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rr x, bb x, rr y, bb y
+            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(l, axis, i);
+                const MixAxis &S = sax[axis];
+                double s = sd[l] * sx[l];
+                int32_t e = __ldg(S.rp + i);
+                const int32_t e1 = __ldg(S.rp + i + 1);
+                for (; e + 4 <= e1; e += 4) {
+                    const int32_t c0 = __ldg(S.col + e), c1 = __ldg(S.col + e + 1);
+                    const int32_t c2 = __ldg(S.col + e + 2), c3 = __ldg(S.col + e + 3);
+                    const double g0 = __ldcg(S.x + c0), g1 = __ldcg(S.x + c1);
+                    const double g2 = __ldcg(S.x + c2), g3 = __ldcg(S.x + c3);
+                    s += __ldg(S.val + e) * g0;
+                    s += __ldg(S.val + e + 1) * g1;
+                    s += __ldg(S.val + e + 2) * g2;
+                    s += __ldg(S.val + e + 3) * g3;
+                }
+                for (; e < e1; ++e) s += __ldg(S.val + e) * __ldcg(S.x + __ldg(S.col + e));
+                const double b = __ldg(S.rhs + i);
+                const double r = b - s;
+                const float rf = static_cast<float>(r);
+                sr[l] = rf;
+                sdd[l] = 0.0f;
+                if (pre) {
+                    __stcg(S.rs + i, rf * rsqrtf(static_cast<float>(sd[l])));
+                } else {
+                    const float u = rf / static_cast<float>(sd[l]);
+                    su[l] = u;
+                    __stcg(S.z + i, u);
+                }
+                acc[axis * 2 + 0] += r * r;
+                acc[axis * 2 + 1] += b * b;
+            }
+            const int sl[4] = {kTRR, kTBB, kTRR, kTBB};
+            const int ax[4] = {0, 0, 1, 1};
+            mstore<4>(A, acc, sl, ax, scratch);
+        }
+        if (!sync()) return;
+        bool live[2];
+        double r_norm[2];
+        {
+            double s[4];
+            const int sl[4] = {kTRR, kTBB, kTRR, kTBB};
+            const int ax[4] = {0, 0, 1, 1};
+            mreduce<4>(A, s, sl, ax, scratch);
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                if (round == 0) {
+                    b_norm[a] = sqrt(s[a * 2 + 1]);
+                    active[a] = b_norm[a] > 0.0;
+                }
+                r_norm[a] = sqrt(s[a * 2 + 0]);
+                if (active[a]) {
+                    prev_resid[a] = true_resid[a];
+                    true_resid[a] = r_norm[a] / b_norm[a];
+                    if (round > 0 && outer[a] > 0 && !(true_resid[a] < 0.5 * prev_resid[a]) &&
+                        true_resid[a] > A.tol)
+                        stalled[a] = true;
+                }
+                live[a] = active[a] && !stalled[a] && true_resid[a] > A.tol &&
+                          outer[a] < A.max_outer && inner[a] < A.max_inner;
+            }
+            if (blockIdx.x == 0 && threadIdx.x == 0 && round > 0 && round - 1 < A.hist_cap) {
+                if (A.hist_x) A.hist_x[round - 1] = true_resid[0];
+                if (A.hist_y) A.hist_y[round - 1] = true_resid[1];
+            }
+        }
+        if (!(live[0] || live[1])) break;
+        if (pre) {
+            apply_m(live);
+            if (!sync()) return;
+        }
+        // ---- inner FP32 PCG (Chronopoulos-Gear) -------------------------------
+        bool in_live[2] = {live[0], live[1]}, first[2] = {true, true};
+        double gamma_prev[2] = {0.0, 0.0}, alpha_prev[2] = {0.0, 0.0};
+        const double target[2] = {A.inner_tol * r_norm[0], A.inner_tol * r_norm[1]};
+        for (;;) {
+            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // gamma, delta, rr per axis
+            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(l, axis, i);
+                if (!in_live[axis]) continue;
+                const MixAxis &S = sax[axis];
+                const float ui = su[l];
+                float w = static_cast<float>(sd[l]) * ui;
+                int32_t e = __ldg(S.rp + i);
+                const int32_t e1 = __ldg(S.rp + i + 1);
+                for (; e + 4 <= e1; e += 4) {
+                    const int32_t c0 = __ldg(S.col + e), c1 = __ldg(S.col + e + 1);
+                    const int32_t c2 = __ldg(S.col + e + 2), c3 = __ldg(S.col + e + 3);
+                    const float g0 = __ldcg(S.z + c0), g1 = __ldcg(S.z + c1);
+                    const float g2 = __ldcg(S.z + c2), g3 = __ldcg(S.z + c3);
+                    w += __ldg(S.val32 + e) * g0;
+                    w += __ldg(S.val32 + e + 1) * g1;
+                    w += __ldg(S.val32 + e + 2) * g2;
+                    w += __ldg(S.val32 + e + 3) * g3;
+                }
+                for (; e < e1; ++e) w += __ldg(S.val32 + e) * __ldcg(S.z + __ldg(S.col + e));
+                sw[l] = w;
+                const float r = sr[l];
+                acc[axis * 3 + 0] += static_cast<double>(r) * ui;
+                acc[axis * 3 + 1] += static_cast<double>(w) * ui;
+                acc[axis * 3 + 2] += static_cast<double>(r) * r;
+            }
+            {
+                double v0[3] = {acc[0], acc[1], acc[2]};
+                double v1[3] = {acc[3], acc[4], acc[5]};
+                const int sl[3] = {kIRZ, kIPAP, kIRR};
+                const int a0[3] = {0, 0, 0};
+                const int a1[3] = {1, 1, 1};
+                mstore<3>(A, v0, sl, a0, scratch);
+                mstore<3>(A, v1, sl, a1, scratch);
+            }
+            if (!sync()) return;
+            float alpha[2] = {0.0f, 0.0f}, beta[2] = {0.0f, 0.0f};
+            bool ok[2] = {false, false};
+            {
+                double s[4], t[2];
+                const int sl[4] = {kIRZ, kIPAP, kIRR, kIRZ};
+                const int ax[4] = {0, 0, 0, 1};
+                mreduce<4>(A, s, sl, ax, scratch);
+                const int sl2[2] = {kIPAP, kIRR};
+                const int ax2[2] = {1, 1};
+                mreduce<2>(A, t, sl2, ax2, scratch);
+                const double gamma[2] = {s[0], s[3]}, delta[2] = {s[1], t[0]};
+                const double rr[2] = {s[2], t[1]};
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    if (!in_live[a]) continue;
+                    const double res = sqrt(rr[a]);
+                    if (!(res > target[a]) || inner[a] >= A.max_inner || !(gamma[a] > 0.0)) {
+                        in_live[a] = false;
+                        continue;
+                    }
+                    double b = 0.0, pap = delta[a];
+                    if (!first[a]) {
+                        b = gamma[a] / gamma_prev[a];
+                        pap = delta[a] - b * gamma[a] / alpha_prev[a];
+                    }
+                    if (!(pap > 0.0)) {
+                        in_live[a] = false;
+                        continue;
+                    }
+                    const double al = gamma[a] / pap;
+                    ok[a] = true;
+                    alpha[a] = static_cast<float>(al);
+                    beta[a] = static_cast<float>(b);
+                    gamma_prev[a] = gamma[a];
+                    alpha_prev[a] = al;
+                }
+            }
+            if (!(ok[0] || ok[1])) break;
+            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(l, axis, i);
+                if (!ok[axis]) continue;
+                const MixAxis &S = sax[axis];
+                const bool f = first[axis];
+                const float pn = f ? su[l] : su[l] + beta[axis] * sp[l];
+                const float sn = f ? sw[l] : sw[l] + beta[axis] * ss[l];
+                sp[l] = pn;
+                ss[l] = sn;
+                sdd[l] += alpha[axis] * pn;
+                const float r = sr[l] - alpha[axis] * sn;
+                sr[l] = r;
+                if (pre) {
+                    __stcg(S.rs + i, r * rsqrtf(static_cast<float>(sd[l])));
+                } else {
+                    const float u = r / static_cast<float>(sd[l]);
+                    su[l] = u;
+                    __stcg(S.z + i, u);
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                if (!ok[a]) continue;
+                ++inner[a];
+                first[a] = false;
+            }
+            if (!sync()) return;
+            if (pre) {
+                apply_m(ok);
+                if (!sync()) return;
+            }
+        }
+        // ---- x += d, published for the next residual -------------------------
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            if (!live[axis]) continue;
+            sx[l] += static_cast<double>(sdd[l]);
+            sax[axis].x[i] = sx[l];
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+            if (live[a]) ++outer[a];
+        if (!sync()) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ktg_mixed_info inf;
+        inf.resid_x = true_resid[0];
+        inf.resid_y = true_resid[1];
+        inf.inner_x = inner[0];
+        inf.inner_y = inner[1];
+        inf.outer_x = outer[0];
+        inf.outer_y = outer[1];
+        inf.status = kStatusOk;
+        inf.stalled = (stalled[0] ? 1 : 0) | (stalled[1] ? 2 : 0);
+        inf.fp64_iters_x = 0;
+        inf.fp64_iters_y = 0;
+        *A.info = inf;
+    }
+}
+
 __global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -432,8 +715,20 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(c->num_sms, want)));
     A.rows_per_block = static_cast<int32_t>((A.total_rows + grid - 1) / grid);
     if (A.rows_per_block == 0) A.rows_per_block = 1;
+    // Chronopoulos-Gear kernel with shared-memory slices when they fit
+    // (40 bytes per row), else the textbook kernel on global vectors.
+    const size_t smem = 40 * static_cast<size_t>(A.rows_per_block);
+    const bool cg_form = c->mixed_form != 0 && smem <= kMixSmemBytes;
+    void (*fn)(MixArgs) = cg_form ? k_pcg_mixed_cg : k_pcg_mixed;
+    const size_t dyn = cg_form ? smem : 0;
+    static bool attr_set = false;
+    if (cg_form && !attr_set) {
+        KTG_CUDA(c, cudaFuncSetAttribute(k_pcg_mixed_cg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMixSmemBytes));
+        attr_set = true;
+    }
     int per_sm = 0;
-    KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_mixed, kMixThreads, 0));
+    KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMixThreads, dyn));
     if (per_sm < 1 || grid > per_sm * c->num_sms)
         return set_error(c, KTG_ERR_CUDA, "mixed PCG blocks cannot all be resident");
     if (c->partials_cap < 12 * static_cast<int64_t>(grid))
@@ -455,8 +750,8 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     KTG_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
     KTG_CUDA(c, cudaMemsetAsync(c->counters + 2, 0, sizeof(unsigned), c->stream));
     void *args[] = {&A};
-    KTG_CUDA(c, cudaLaunchCooperativeKernel((void *)k_pcg_mixed, dim3(grid), dim3(kMixThreads),
-                                            args, 0, c->stream));
+    KTG_CUDA(c, cudaLaunchCooperativeKernel((void *)fn, dim3(grid), dim3(kMixThreads), args, dyn,
+                                            c->stream));
     k_mixed_status<<<1, 1, 0, c->stream>>>(c->status, info_dev);
     c->launches += 2;
     KTG_CUDA(c, cudaGetLastError());

@@ -5,8 +5,7 @@
 // runs them on a B200 through the ktplace_b200 C ABI:
 //
 //   LinearSystems::buildB2B  (reference: simpl_lss.cc:11-114)  -> ktg_build_b2b
-//   LinearSystems::buildStar (reference: simpl_lss.cc:116-201) -> host assembly,
-//                            solved on the GPU like any other system
+//   LinearSystems::buildStar (reference: simpl_lss.cc:116-201) -> ktg_build_star
 //   solveBothAxes            (reference: simpl_lss.cc:203-290) -> ktg_solve
 //
 // Link this object instead of simpl_lss.o. One GPU
@@ -176,85 +175,20 @@ void LinearSystems::buildB2B(const std::vector<double> &x, const std::vector<dou
     s.devRows = sysX.size();
 }
 
-// Star model (simpl_lss.cc:116-201): each net of three or more pins with a
-// movable pin gets a star variable after the movable cells; two-pin nets
-// connect their pins directly; springs add w to the diagonal of each movable
-// end, -w off the diagonal towards a movable other end, and the offset (or the
-// fixed position plus offset) to the right-hand side. Assembled on the host;
-// the systems are solved on the GPU by solveBothAxes.
+// Star model (simpl_lss.cc:116-201): assembled on the GPU by ktg_build_star
+// (bit-identical to the reference) and copied into sysX/sysY like buildB2B.
 std::size_t LinearSystems::buildStar() const {
-    const std::size_t numNets = netlist.nets.size();
-    std::vector<std::uint32_t> star(numNets, noVar);
-    std::size_t size = netlist.numMovable;
-    for (std::size_t k = 0; k < numNets; ++k) {
-        const auto &cells = netlist.nets[k].cells;
-        bool anyMovable = false;
-        for (const std::uint32_t v : cells) anyMovable = anyMovable || netlist.varOfVertex[v] != noVar;
-        if (cells.size() >= 3 && anyMovable) star[k] = static_cast<std::uint32_t>(size++);
-    }
-    for (int axis = 0; axis < 2; ++axis) {
-        SparseSystem &sys = axis == 0 ? sysX : sysY;
-        const bool vertical = axis == 0;
-        std::vector<std::vector<std::pair<std::uint32_t, double>>> rows(size);
-        sys.diag.assign(size, 0.0);
-        sys.rhs.assign(size, 0.0);
-        struct End {
-            std::uint32_t var;
-            double offset;
-            double fixed;
-        };
-        auto pull = [&](const End &self, const End &other, double w) {
-            if (self.var == noVar) return;
-            sys.diag[self.var] += w;
-            if (other.var != noVar) {
-                rows[self.var].emplace_back(other.var, -w);
-                sys.rhs[self.var] += w * (other.offset - self.offset);
-            } else {
-                sys.rhs[self.var] += w * (other.fixed + other.offset - self.offset);
-            }
-        };
-        for (std::size_t k = 0; k < numNets; ++k) {
-            const NetPins &net = netlist.nets[k];
-            const std::size_t p = net.cells.size();
-            if (p < 2) continue;
-            auto end = [&](std::size_t q) {
-                const std::uint32_t v = net.cells[q];
-                return End{netlist.varOfVertex[v], vertical ? net.offX[q] : net.offY[q],
-                           vertical ? netlist.fixedX[v] : netlist.fixedY[v]};
-            };
-            if (p == 2) {
-                const End a = end(0), b = end(1);
-                pull(a, b, net.weight);
-                pull(b, a, net.weight);
-            } else if (star[k] != noVar) {
-                const End hub{star[k], 0.0, 0.0};
-                const double w = net.weight * static_cast<double>(p) / static_cast<double>(p - 1);
-                for (std::size_t q = 0; q < p; ++q) {
-                    const End a = end(q);
-                    pull(a, hub, w);
-                    pull(hub, a, w);
-                }
-            }
-        }
-        sys.rowPtr.assign(size + 1, 0);
-        for (std::size_t i = 0; i < size; ++i) {
-            sys.rowPtr[i + 1] = sys.rowPtr[i] + rows[i].size();
-            sys.diag[i] = std::max(sys.diag[i], 1e-12);
-        }
-        sys.col.resize(sys.rowPtr.back());
-        sys.val.resize(sys.rowPtr.back());
-        for (std::size_t i = 0; i < size; ++i) {
-            std::size_t slot = sys.rowPtr[i];
-            for (const auto &[col, v] : rows[i]) {
-                sys.col[slot] = col;
-                sys.val[slot] = v;
-                ++slot;
-            }
-        }
-    }
+    ensureNetlist(netlist);
     GpuState &s = state();
-    if (s.devX == &sysX || s.devY == &sysY) s.devX = s.devY = nullptr;
-    return size;
+    ktg_ctx *c = s.ctx;
+    int64_t size = 0;
+    check("ktg_build_star", ktg_build_star(c, &size));
+    download(c, KTG_AXIS_X, sysX, s.hostCsr);
+    download(c, KTG_AXIS_Y, sysY, s.hostCsr);
+    s.devX = &sysX;
+    s.devY = &sysY;
+    s.devRows = static_cast<std::size_t>(size);
+    return static_cast<std::size_t>(size);
 }
 
 Residuals solveBothAxes(const SparseSystem &sysX, std::vector<double> &x, const SparseSystem &sysY,
