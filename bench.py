@@ -301,23 +301,8 @@ def run_ours(args):
     sx_n, sx_m = ctx.system_info(0)
     _, sy_m = ctx.system_info(1)
 
-    # ---- mixed precision on the same systems (breakdown only) --------------
-    from ktplace_b200._lib import MixedInfo
-    minfo = torch.zeros(ctypes.sizeof(MixedInfo), dtype=torch.uint8, device=dev)
-    mixed_ms = []
-    with torch.cuda.stream(stream):
-        ctx.build_b2b_dev(dx, dy, ALPHA, dax, day, fx, fy)
-        for k in range(max(args.steps // 2, 3) + 1):
-            wx.copy_(dx)
-            wy.copy_(dy)
-            flush.zero_()
-            s_starts[0].record(stream)
-            ctx.solve_mixed_dev(wx, wy, TOL, MIXED_INNER_TOL, MAX_ITER, 50, minfo)
-            s_ends[0].record(stream)
-            s_ends[0].synchronize()
-            if k > 0:
-                mixed_ms.append(s_starts[0].elapsed_time(s_ends[0]))
-    mi = MixedInfo.from_buffer_copy(bytes(minfo.cpu().numpy()))
+    variants = solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, info, scal,
+                              flush, max(args.steps // 2, 3))
 
     # ---- e2e: host buffers through the C ABI, copies included --------------
     pinned = [torch.tensor(a).pin_memory() for a in (x, y, ax, ay, x, y)]
@@ -383,13 +368,8 @@ def run_ours(args):
                        "cg_iters": int(inf.iters), "l2": "flushed between steps",
                        "parallelism": f"replicas x{world} (independent netlists)"},
             "breakdown": {"solve_ms": solve_med, "solve_ms_per_cg_iter": solve_med / inf.iters,
-                          "other_ms": statistics.median(step_ms) - solve_med,
-                          "mixed_solve_ms": statistics.median(mixed_ms),
-                          "mixed_inner_iters": [int(mi.inner_x), int(mi.inner_y)],
-                          "mixed_outer_rounds": [int(mi.outer_x), int(mi.outer_y)],
-                          "mixed_true_resid": [mi.resid_x, mi.resid_y],
-                          "mixed_fp64_fallback_iters": [int(mi.fp64_iters_x),
-                                                        int(mi.fp64_iters_y)]},
+                          "other_ms": statistics.median(step_ms) - solve_med},
+            "solve_variants": variants,
             "roofline": {"kernel": "k_pcg_cg (persistent cooperative PCG, x+y)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
@@ -408,6 +388,82 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, info, scal, flush,
+                   reps: int) -> dict:
+    """The x+y solve of the same systems to the same true residual (rtol
+    1e-6) by each method, per-system set-up included (aggregation build,
+    network inference), B2B build excluded: plain FP64 Jacobi-PCG (the
+    drop-in), and FP32 PCG inside FP64 refinement with Jacobi, the learned
+    preconditioner and the aggregation preconditioner. Reports the median
+    device ms, iterations and the HPWL of the solution relative to FP64."""
+    from ktplace_b200._lib import MixedInfo, SolveInfo
+    from ktplace_b200.learned import Learned
+    minfo = torch.zeros(ctypes.sizeof(MixedInfo), dtype=torch.uint8, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    weights = os.path.join(ROOT, "ktplace_b200", "weights", "learned_precond.npy")
+    learned = None
+    if os.path.exists(weights):
+        learned = Learned(dev.index or 0)
+        learned.load(weights)
+    out = {}
+    hpwl_ref = None
+    for name, pre in (("fp64_jacobi", None), ("fp32_jacobi", 0), ("fp32_learned", 1),
+                      ("fp32_aggregation", 2)):
+        if pre == 1 and learned is None:
+            continue
+        if pre is not None:
+            ctx.set_option("precond", pre)
+        ms = []
+        host_ms = 0.0
+        for k in range(reps + 1):
+            with torch.cuda.stream(stream):
+                ctx.build_b2b_dev(dx, dy, ALPHA, dax, day, fx, fy)
+                wx.copy_(dx)
+                wy.copy_(dy)
+                flush.zero_()
+            torch.cuda.synchronize(dev)
+            host_ms = 0.0
+            if pre == 1:
+                t0 = time.perf_counter()
+                learned.prepare(ctx)  # synchronous: network inference for x and y
+                host_ms = 1000.0 * (time.perf_counter() - t0)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                if pre is None:
+                    ctx.solve_dev(wx, wy, TOL, MAX_ITER, info)
+                else:
+                    ctx.solve_mixed_dev(wx, wy, TOL, MIXED_INNER_TOL, MAX_ITER, 50, minfo)
+                e1.record(stream)
+                ctx.hpwl_dev(wx, wy, scal[2:3])
+            e1.synchronize()
+            if k > 0:
+                ms.append(e0.elapsed_time(e1) + host_ms)
+        h = float(scal[2].item())
+        if pre is None:
+            inf = SolveInfo.from_buffer_copy(bytes(info.cpu().numpy()))
+            hpwl_ref = h
+            row = {"ms": statistics.median(ms), "iters": [int(inf.iters_x), int(inf.iters_y)],
+                   "true_resid": [inf.resid_x, inf.resid_y]}
+        else:
+            mi = MixedInfo.from_buffer_copy(bytes(minfo.cpu().numpy()))
+            row = {"ms": statistics.median(ms), "iters": [int(mi.inner_x), int(mi.inner_y)],
+                   "outer_rounds": [int(mi.outer_x), int(mi.outer_y)],
+                   "true_resid": [mi.resid_x, mi.resid_y],
+                   "fp64_fallback_iters": [int(mi.fp64_iters_x), int(mi.fp64_iters_y)]}
+            if pre == 1:
+                row["inference_ms_host_timed"] = host_ms
+        row["hpwl_rel_vs_fp64"] = (h - hpwl_ref) / hpwl_ref if hpwl_ref else 0.0
+        out[name] = row
+    ctx.set_option("precond", 0)
+    if learned is not None:
+        learned.close()
+    base = out["fp64_jacobi"]["ms"]
+    for row in out.values():
+        row["speedup_vs_fp64"] = base / row["ms"]
+    return out
 
 
 def batch_workload(count: int = 64):

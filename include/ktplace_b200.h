@@ -312,6 +312,26 @@ int ktg_learned_train_step(ktg_learned *h, ktg_ctx *ctx, int axis, uint64_t seed
 int ktg_learned_prepare(ktg_learned *h, ktg_ctx *ctx);
 int64_t ktg_learned_launch_count(const ktg_learned *h);
 
+/* ---- aggregation preconditioner (no reference counterpart) ---------------
+ * With ktg_set_option(ctx, "precond", 2), ktg_solve_mixed preconditions its
+ * FP32 inner PCG with the exact inverses of A's diagonal blocks over
+ * aggregates of at most 8 rows, found by three levels of pairwise handshake
+ * matching on the strength -a_ij / sqrt(a_ii a_jj) with Galerkin coarsening.
+ * The rows are renumbered so that each aggregate is contiguous and lies in
+ * one thread block of the solve, which applies M from shared memory. The
+ * aggregates are built on the device (no host synchronisation) at the first
+ * mixed solve after each build or upload of the systems.
+ *
+ * ktg_download_aggregates builds them now if needed and copies out, for the
+ * 2n rows of the combined system (x rows 0..n-1, y rows n..2n-1):
+ *   order[k]   combined row placed at position k (x rows come first),
+ *   meta[k]    (first position of k's aggregate within its axis) * 8 +
+ *              (aggregate size - 1),
+ *   minv[8k+j] row k of its aggregate's block inverse, column j (FP32,
+ *              zero beyond the aggregate's size).
+ * Any of the three pointers may be NULL. Host memory. */
+int ktg_download_aggregates(ktg_ctx *ctx, int32_t *order, int32_t *meta, float *minv);
+
 /* ---- tuning and introspection ------------------------------------------- */
 
 /* Sets a kernel-shape option of this context (no reference counterpart; the
@@ -319,8 +339,8 @@ int64_t ktg_learned_launch_count(const ktg_learned *h);
  *   "pcg_lanes"  1 or 4: threads per matrix row in the PCG SpMV (0 = default)
  *   "pcg_form"   0: textbook PCG (three grid barriers per iteration),
  *                1: Chronopoulos-Gear form (two), -1 = default (1)
- *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare) in
- *                ktg_solve_mixed
+ *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare),
+ *                2: aggregation block-Jacobi, in ktg_solve_mixed
  *   "mixed_form" 1 (default): Chronopoulos-Gear mixed solve with per-block
  *                shared-memory slices; 0: textbook mixed solve
  * Returns KTG_ERR_ARG for an unknown key or value. */

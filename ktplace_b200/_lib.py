@@ -26,6 +26,7 @@ _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _f64p = ctypes.POINTER(ctypes.c_double)
+_f32p = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
 
 
@@ -96,6 +97,7 @@ SIGNATURES = [
     ("ktg_selftest_wait_timeout", ctypes.c_int, [_vp, ctypes.c_int64,
                                                  ctypes.POINTER(ctypes.c_int)]),
     ("ktg_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
+    ("ktg_download_aggregates", ctypes.c_int, [_vp, _i32p, _i32p, _f32p]),
     ("ktg_batch_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ktg_batch_destroy", None, [_vp]),
     ("ktg_batch_last_error", ctypes.c_char_p, [_vp]),

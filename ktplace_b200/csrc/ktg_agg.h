@@ -1,0 +1,41 @@
+// Buffers of the aggregation preconditioner (built by ktg_agg.cu, read by
+// the mixed-precision solve).
+#pragma once
+
+#include <cstdint>
+
+namespace ktg {
+
+struct AggState {
+    int64_t cap_rows = 0;  // 2n capacity
+    int64_t cap_nnz = 0;   // nnz(x) + nnz(y) capacity
+    int grid_cap = 0;
+    // level work
+    int32_t *mate = nullptr, *pick = nullptr, *flag = nullptr, *cid = nullptr;
+    int32_t *child0 = nullptr, *child1 = nullptr, *size_a = nullptr, *size_b = nullptr;
+    int32_t *cur = nullptr, *pos = nullptr;
+    int32_t *cstart[2] = {nullptr, nullptr};
+    int32_t *clen[2] = {nullptr, nullptr};
+    int32_t *ccol[2] = {nullptr, nullptr};
+    double *cval[2] = {nullptr, nullptr};
+    double *cdiag[2] = {nullptr, nullptr};
+    int32_t *counts = nullptr;     // [8] node counts per level, totals
+    int32_t *tile_sum = nullptr;   // scan tiles
+    int64_t tiles_cap = 0;
+    // result
+    int32_t *agg_start = nullptr;  // [2n + 1]
+    int32_t *order = nullptr, *newpos = nullptr;  // [2n]
+    int32_t *prp = nullptr;        // [2n + 1] combined offsets
+    int32_t *pcol = nullptr;       // [nnz] per-axis local columns
+    double *pval = nullptr;        // [nnz]
+    float *pval32 = nullptr;       // [nnz]
+    double *pdiag = nullptr, *prhs = nullptr, *px = nullptr;  // [2n]
+    float *minv = nullptr;         // [2n * 8]
+    int32_t *meta = nullptr;       // [2n] per-axis first * 8 + size - 1
+    int32_t *blk_start = nullptr;  // [grid + 1]
+    double *gslice = nullptr;      // per-block slices when shared memory is too small
+    int64_t gslice_cap = 0;
+    int blk_grid = 0;              // grid the blk_start array was built for
+};
+
+}  // namespace ktg

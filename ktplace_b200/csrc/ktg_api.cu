@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "ktg_agg.h"
 #include "ktg_context.h"
 #include "ktplace_b200.h"
 
@@ -166,6 +167,7 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
         }
         c->val32_valid = false;
         c->precond_ready = false;
+        c->agg_ready = false;
         c->sys_cap_nnz = nnz;
     }
     return KTG_OK;
@@ -236,6 +238,7 @@ void ktg_destroy(ktg_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_netlist(c);
     free_systems(c);
+    ktg::free_agg(c);
     dev_free(c->partials);
     dev_free(c->counters);
     dev_free(c->status);
@@ -287,7 +290,8 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         return KTG_OK;
     }
     if (k == "precond") {
-        if (value != 0 && value != 1) return set_error(c, KTG_ERR_ARG, "precond must be 0 or 1");
+        if (value != 0 && value != 1 && value != 2)
+            return set_error(c, KTG_ERR_ARG, "precond must be 0, 1 or 2");
         c->precond = static_cast<int>(value);
         return KTG_OK;
     }
@@ -464,6 +468,7 @@ int ktg_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha, co
     c->axis_valid[0] = c->axis_valid[1] = true;
     c->val32_valid = false;
     c->precond_ready = false;
+    c->agg_ready = false;
     if (c->ptr_mode == KTG_PTR_HOST) {
         const int st = device_status(c);
         if (st < 0) return st;
@@ -484,6 +489,7 @@ int ktg_build_star(ktg_ctx *c, int64_t *size) {
     c->axis_valid[0] = c->axis_valid[1] = true;
     c->val32_valid = false;
     c->precond_ready = false;
+    c->agg_ready = false;
     *size = rows;
     return KTG_OK;
 }
@@ -580,6 +586,7 @@ int ktg_upload_system(ktg_ctx *c, int axis, int64_t n, const int64_t *row_ptr, c
     c->axis_valid[axis] = true;
     c->val32_valid = false;
     c->precond_ready = false;
+    c->agg_ready = false;
     c->sys_n = n;
     c->have_system = c->axis_valid[0] && c->axis_valid[1];
     return KTG_OK;
@@ -707,6 +714,28 @@ int ktg_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inner_t
                                    cudaMemcpyDeviceToHost));
     }
     return KTG_OK;
+}
+
+int ktg_download_aggregates(ktg_ctx *c, int32_t *order, int32_t *meta, float *minv) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no system to aggregate");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (!c->agg_ready && (rc = ktg::build_agg(c))) return rc;
+    const int64_t rows = 2 * c->sys_n;
+    const ktg::AggState *g = c->agg;
+    if (rows > 0) {
+        if (order)
+            KTG_CUDA(c, cudaMemcpyAsync(order, g->order, sizeof(int32_t) * rows,
+                                        cudaMemcpyDeviceToHost, c->stream));
+        if (meta)
+            KTG_CUDA(c, cudaMemcpyAsync(meta, g->meta, sizeof(int32_t) * rows,
+                                        cudaMemcpyDeviceToHost, c->stream));
+        if (minv)
+            KTG_CUDA(c, cudaMemcpyAsync(minv, g->minv, sizeof(float) * 8 * rows,
+                                        cudaMemcpyDeviceToHost, c->stream));
+    }
+    return sync(c);
 }
 
 int ktg_hpwl(ktg_ctx *c, const double *x, const double *y, double *out) {

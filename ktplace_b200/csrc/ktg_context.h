@@ -21,6 +21,8 @@
 
 namespace ktg {
 
+struct AggState;  // aggregation preconditioner buffers (ktg_agg.cu)
+
 struct AxisSystem {
     int32_t *row_ptr = nullptr;  // [n+1]
     int32_t *col = nullptr;      // [cap]
@@ -74,7 +76,9 @@ struct ktg_ctx {
     bool axis_valid[2] = {false, false};
     bool val32_valid = false;  // sys[*].val32 mirrors sys[*].val
     bool precond_ready = false;  // sys[*].s32 holds learned values for the current systems
-    int precond = 0;             // 0 Jacobi, 1 learned (ktg_set_option "precond")
+    int precond = 0;             // 0 Jacobi, 1 learned, 2 aggregation (ktg_set_option "precond")
+    ktg::AggState *agg = nullptr;  // aggregation preconditioner of the current systems
+    bool agg_ready = false;        // agg holds aggregates of the current systems
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
     int64_t sys_cap_nnz = 0;  // allocated entries for col/val
@@ -128,6 +132,14 @@ int launch_solve_mixed(ktg_ctx *ctx, double *x, double *y, double tol, double in
                        double *hist_x, double *hist_y, int64_t hist_cap);
 
 int build_star(ktg_ctx *ctx, int64_t *size_out, int (*reserve)(ktg_ctx *, int64_t, int64_t));
+
+// Aggregation preconditioner (ktg_agg.cu): build for the current systems,
+// per-solve set-up (block row ranges, permuted positions) and write-back.
+int build_agg(ktg_ctx *ctx);
+int agg_prepare_solve(ktg_ctx *ctx, int grid, const double *x, const double *y, int32_t *rows_cap);
+int agg_finish_solve(ktg_ctx *ctx, double *x, double *y);
+double *agg_global_slices(ktg_ctx *ctx, int64_t doubles);
+void free_agg(ktg_ctx *ctx);
 
 int set_error(ktg_ctx *ctx, int code, const std::string &msg);
 int cuda_check(ktg_ctx *ctx, cudaError_t e, const char *what);

@@ -12,6 +12,7 @@
 //          with Jacobi-PCG until ||r_inner|| <= inner_tol * ||r||, x += d.
 // A round that fails to halve the true residual is reported as a stall; the
 // C ABI then finishes the solve with the FP64 kernel from the current x.
+#include "ktg_agg.h"
 #include "ktg_common.cuh"
 #include "ktg_context.h"
 
@@ -39,6 +40,8 @@ struct MixAxis {
     float *ap;
     const float *s32;  // learned preconditioner values on A's pattern (null: Jacobi)
     float *rs;         // D^-1/2 r_inner, published for the preconditioner's gathers
+    const float *minv;     // aggregation: 8 block-inverse entries per row
+    const int32_t *meta;   // aggregation: first row of the aggregate * 8 + size - 1
     int32_t n;
 };
 
@@ -60,6 +63,8 @@ struct MixArgs {
     int64_t hist_cap;
     uint64_t barrier_timeout_ns;
     uint64_t total_timeout_ns;
+    const int32_t *blk_start;  // aggregation: block row ranges aligned to aggregates
+    double *gslice;            // per-block slices in global memory (null: shared memory)
 };
 
 enum MixSlot { kTRR = 0, kTBB = 1, kIRZ0 = 2, kIPAP = 3, kIRR = 4, kIRZ = 5 };
@@ -390,12 +395,21 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
     }
 }
 
+// Preconditioners of the mixed solve.
+enum MixPre { kPreJacobi = 0, kPreLearned = 1, kPreAgg = 2 };
+
 // Chronopoulos-Gear form of the mixed solve, with the block's vector slices
-// in shared memory (x, diag in FP64; r, u, w, p, s, d in FP32). Per inner
+// in shared memory (x, diag in FP64; r, u, w, p, s, d in FP32), or in a
+// per-block region of global memory when they do not fit. Per inner
 // iteration: w = A u (gather u) and the partials of gamma = r.u, delta = w.u
 // and |r|^2 -> barrier -> alpha, beta (FP64) -> p = u + beta p,
-// s = w + beta s, d += alpha p, r -= alpha s, u = M r -> barrier. With the
-// learned M, u = M r gathers D^-1/2 r of other rows, which adds one barrier.
+// s = w + beta s, d += alpha p, r -= alpha s, u = M r -> barrier.
+//   Jacobi:  u = r / d, row-local.
+//   learned: u = M r gathers D^-1/2 r of other rows, which adds one barrier.
+//   aggregation: the system is renumbered so that every aggregate lies in
+//     one block's rows; u = (block inverse) r reads the block's own slice
+//     after a __syncthreads, with no extra grid barrier.
+template <int PRE>
 __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     extern __shared__ double dyn[];
     __shared__ double scratch[33 * 4];
@@ -407,12 +421,19 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         const uint64_t d = global_timer_ns() + A.barrier_timeout_ns;
         return d < total_deadline ? d : total_deadline;
     };
-    const int32_t r0 = blockIdx.x * A.rows_per_block;
-    const int32_t r1 = min(r0 + A.rows_per_block, A.total_rows);
+    int32_t r0, r1;
+    if (PRE == kPreAgg) {
+        r0 = __ldg(A.blk_start + blockIdx.x);
+        r1 = __ldg(A.blk_start + blockIdx.x + 1);
+    } else {
+        r0 = blockIdx.x * A.rows_per_block;
+        r1 = min(r0 + A.rows_per_block, A.total_rows);
+    }
     const int32_t R = max(r1 - r0, 0);
     const int32_t cap = A.rows_per_block;
-    double *sx = dyn, *sd = dyn + cap;
-    float *sr = reinterpret_cast<float *>(dyn + 2 * cap);
+    double *base = A.gslice ? A.gslice + static_cast<size_t>(blockIdx.x) * cap * 5 : dyn;
+    double *sx = base, *sd = base + cap;
+    float *sr = reinterpret_cast<float *>(base + 2 * cap);
     float *su = sr + cap, *sw = su + cap, *sp = sw + cap, *ss = sp + cap, *sdd = ss + cap;
     const int32_t n0 = sax[0].n;
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
@@ -421,7 +442,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         i = c - (axis ? n0 : 0);
     };
     auto sync = [&]() { return grid_barrier(A.bar_count, A.bar_gen, A.status, deadline()); };
-    const bool pre = sax[0].s32 != nullptr;
+    constexpr bool pre = PRE == kPreLearned;
     for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
         int axis;
         int32_t i;
@@ -430,6 +451,31 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         sd[l] = __ldg(sax[axis].diag + i);
     }
     __syncthreads();
+
+    // u = M r for own rows with the aggregation preconditioner: the block
+    // inverse row of each row times r over its aggregate (own slice).
+    auto apply_blocks = [&](const bool *live) {
+        __syncthreads();
+        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+            int axis;
+            int32_t i;
+            locate(l, axis, i);
+            if (!live[axis]) continue;
+            const MixAxis &S = sax[axis];
+            const int32_t meta = __ldg(S.meta + i);
+            const int k = (meta & 7) + 1;
+            const int32_t lf = (meta >> 3) + (axis ? n0 : 0) - r0;
+            const float4 m0 = __ldg(reinterpret_cast<const float4 *>(S.minv) + 2 * static_cast<size_t>(i));
+            const float4 m1 = __ldg(reinterpret_cast<const float4 *>(S.minv) + 2 * static_cast<size_t>(i) + 1);
+            const float mm[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+            float u = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (q < k) u += mm[q] * sr[lf + q];
+            su[l] = u;
+            __stcg(S.z + i, u);
+        }
+    };
 
     // u = M r for own rows (learned M), reading the published D^-1/2 r.
     auto apply_m = [&](const bool *live) {
@@ -480,13 +526,17 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 sdd[l] = 0.0f;
                 if (pre) {
                     __stcg(S.rs + i, rf * rsqrtf(static_cast<float>(sd[l])));
-                } else {
+                } else if (PRE == kPreJacobi) {
                     const float u = rf / static_cast<float>(sd[l]);
                     su[l] = u;
                     __stcg(S.z + i, u);
                 }
                 acc[axis * 2 + 0] += r * r;
                 acc[axis * 2 + 1] += b * b;
+            }
+            if (PRE == kPreAgg) {
+                const bool all[2] = {true, true};
+                apply_blocks(all);
             }
             const int sl[4] = {kTRR, kTBB, kTRR, kTBB};
             const int ax[4] = {0, 0, 1, 1};
@@ -624,12 +674,13 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 sr[l] = r;
                 if (pre) {
                     __stcg(S.rs + i, r * rsqrtf(static_cast<float>(sd[l])));
-                } else {
+                } else if (PRE == kPreJacobi) {
                     const float u = r / static_cast<float>(sd[l]);
                     su[l] = u;
                     __stcg(S.z + i, u);
                 }
             }
+            if (PRE == kPreAgg) apply_blocks(ok);
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
                 if (!ok[a]) continue;
@@ -688,7 +739,11 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
                        int64_t max_inner, int32_t max_outer, ktg_mixed_info *info_dev,
                        double *hist_x, double *hist_y, int64_t hist_cap) {
     const int64_t nsys = c->sys_n;
-    if (!c->val32_valid) {
+    const bool agg = c->precond == 2;
+    const bool learned = c->precond == 1 && c->precond_ready;
+    int rc = KTG_OK;
+    if (agg && !c->agg_ready && (rc = build_agg(c))) return rc;
+    if (!agg && !c->val32_valid) {
         for (int a = 0; a < 2; ++a) {
             int32_t m = 0;
             KTG_CUDA(c, cudaMemcpyAsync(&m, c->sys[a].row_ptr + nsys, sizeof(int32_t),
@@ -703,28 +758,53 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
         c->val32_valid = true;
     }
     MixArgs A;
-    for (int a = 0; a < 2; ++a) {
-        ktg::AxisSystem &s = c->sys[a];
-        const bool pre = c->precond == 1 && c->precond_ready;
-        A.ax[a] = MixAxis{s.row_ptr, s.col, s.val, s.val32, s.diag, s.rhs, a ? y : x, s.r,
-                          s.d32, s.r32, s.z32, s.p32, s.ap32, pre ? s.s32 : nullptr, s.rs32,
-                          static_cast<int32_t>(nsys)};
-    }
     A.total_rows = static_cast<int32_t>(2 * nsys);
     const int64_t want = (A.total_rows + 1023) / 1024;
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(c->num_sms, want)));
     A.rows_per_block = static_cast<int32_t>((A.total_rows + grid - 1) / grid);
     if (A.rows_per_block == 0) A.rows_per_block = 1;
-    // Chronopoulos-Gear kernel with shared-memory slices when they fit
-    // (40 bytes per row), else the textbook kernel on global vectors.
-    const size_t smem = 40 * static_cast<size_t>(A.rows_per_block);
-    const bool cg_form = c->mixed_form != 0 && smem <= kMixSmemBytes;
-    void (*fn)(MixArgs) = cg_form ? k_pcg_mixed_cg : k_pcg_mixed;
-    const size_t dyn = cg_form ? smem : 0;
+    A.blk_start = nullptr;
+    A.gslice = nullptr;
+    AggState *g = nullptr;
+    if (agg) {
+        if ((rc = agg_prepare_solve(c, grid, x, y, &A.rows_per_block))) return rc;
+        g = c->agg;
+        A.blk_start = g->blk_start;
+    }
+    for (int a = 0; a < 2; ++a) {
+        ktg::AxisSystem &s = c->sys[a];
+        if (agg) {
+            const int64_t o = a * nsys;
+            A.ax[a] = MixAxis{g->prp + o, g->pcol, g->pval, g->pval32, g->pdiag + o, g->prhs + o,
+                              g->px + o, s.r, s.d32, s.r32, s.z32, s.p32, s.ap32, nullptr,
+                              s.rs32, g->minv + o * 8, g->meta + o, static_cast<int32_t>(nsys)};
+        } else {
+            A.ax[a] = MixAxis{s.row_ptr, s.col, s.val, s.val32, s.diag, s.rhs, a ? y : x, s.r,
+                              s.d32, s.r32, s.z32, s.p32, s.ap32, learned ? s.s32 : nullptr,
+                              s.rs32, nullptr, nullptr, static_cast<int32_t>(nsys)};
+        }
+    }
+    // Chronopoulos-Gear kernel (always for the aggregation preconditioner),
+    // with shared-memory slices of 40 bytes per row when they fit, else
+    // global ones; the textbook kernel on global vectors when asked for.
+    const size_t slice = 40 * static_cast<size_t>(A.rows_per_block);
+    const bool cg_form = agg || c->mixed_form != 0;
+    const bool in_smem = slice <= kMixSmemBytes;
+    if (cg_form && !in_smem) {
+        A.gslice = agg_global_slices(c, static_cast<int64_t>(grid) * A.rows_per_block * 5);
+        if (!A.gslice) return KTG_ERR_NOMEM;
+    }
+    void (*fn)(MixArgs) = !cg_form ? k_pcg_mixed
+                          : agg    ? k_pcg_mixed_cg<kPreAgg>
+                          : learned ? k_pcg_mixed_cg<kPreLearned>
+                                    : k_pcg_mixed_cg<kPreJacobi>;
+    const size_t dyn = cg_form && in_smem ? slice : 0;
     static bool attr_set = false;
-    if (cg_form && !attr_set) {
-        KTG_CUDA(c, cudaFuncSetAttribute(k_pcg_mixed_cg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kMixSmemBytes));
+    if (!attr_set) {
+        for (void (*f)(MixArgs) : {k_pcg_mixed_cg<kPreJacobi>, k_pcg_mixed_cg<kPreLearned>,
+                                   k_pcg_mixed_cg<kPreAgg>})
+            KTG_CUDA(c, cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             kMixSmemBytes));
         attr_set = true;
     }
     int per_sm = 0;
@@ -755,6 +835,7 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     k_mixed_status<<<1, 1, 0, c->stream>>>(c->status, info_dev);
     c->launches += 2;
     KTG_CUDA(c, cudaGetLastError());
+    if (agg && (rc = agg_finish_solve(c, x, y))) return rc;
     return KTG_OK;
 }
 

@@ -136,6 +136,19 @@ class Context:
         self._check(self.lib.ktg_system_info(self.h, axis, ctypes.byref(n), ctypes.byref(m)))
         return int(n.value), int(m.value)
 
+    def aggregates(self) -> dict:
+        """Aggregation preconditioner of the current systems (built if needed):
+        order [2n], meta [2n] and the block-inverse rows minv [2n, 8]."""
+        n, _ = self.system_info(0)
+        out = dict(order=np.zeros(max(2 * n, 1), np.int32), meta=np.zeros(max(2 * n, 1), np.int32),
+                   minv=np.zeros((max(2 * n, 1), 8), np.float32))
+        P = ctypes.POINTER
+        self._check(self.lib.ktg_download_aggregates(
+            self.h, out["order"].ctypes.data_as(P(ctypes.c_int32)),
+            out["meta"].ctypes.data_as(P(ctypes.c_int32)),
+            out["minv"].ctypes.data_as(P(ctypes.c_float))))
+        return {k: v[:2 * n] for k, v in out.items()}
+
     def system(self, axis: int) -> dict:
         n, m = self.system_info(axis)
         s = dict(row_ptr=np.zeros(n + 1, np.int64), col=np.zeros(max(m, 1), np.int32),
