@@ -56,6 +56,9 @@ def parse():
                     help="skip the batched-solve leg (64 netlists, 128 systems)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="run the batched-solve workload once for an ncu capture")
+    ap.add_argument("--profile-agg", action="store_true",
+                    help="build the 211k systems twice, each followed by a mixed solve with "
+                         "the aggregation preconditioner (set-up included), for ncu captures")
     ap.add_argument("--profile-once", action="store_true",
                     help="run the workload once (build, FP64 and mixed solves, HPWL, "
                          "density) for an ncu capture; prints no bench line")
@@ -549,10 +552,30 @@ def profile_once():
     return 0
 
 
+def profile_agg():
+    """The capture workload of profiles/agg_*_synth211k.md: two B2B builds of
+    the 211k-cell workload, each followed by a mixed solve with the
+    aggregation preconditioner (which rebuilds the aggregates)."""
+    from ktplace_b200.gpu import Context
+    raw, nl, x, y, ax, ay = make_workload(1)
+    fx, fy = nl.floors()
+    ctx = Context(0)
+    ctx.upload_netlist(nl)
+    ctx.set_option("precond", 2)
+    for _ in range(2):
+        ctx.build_b2b(x, y, ALPHA, ax, ay, fx, fy)
+        m = ctx.solve_mixed(x, y, TOL, MIXED_INNER_TOL)
+    print(f"profile-agg: inner {m['inner']}, outer {m['outer']}, resid {m['resid']}")
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_once:
         return profile_once()
+    if args.profile_agg:
+        return profile_agg()
     if args.profile_batch:
         batch, rows = batch_workload(16)
         batch.solve(TOL, MAX_ITER, precision=1, inner_tol=MIXED_INNER_TOL)

@@ -110,24 +110,13 @@ __global__ void k_init(int32_t rows, int32_t *cur, int32_t *pos, int32_t *size, 
     mate[c] = -1;
 }
 
-// One thread per node, four entries of its row fetched at a time so that
-// their gathers (mate and diag of the neighbour) are in flight together. Rows
-// longer than kPickShort are queued in shared memory and scanned afterwards
-// by a whole warp each, so the long tail of row lengths does not set the
-// kernel's time. The result (largest strength, ties to the smaller J) does
-// not depend on the order of the scan.
-constexpr int kPickShort = 16;
-constexpr int kPickThreads = 256;
-
-__device__ __forceinline__ void pick_consider(int32_t I, int32_t J, double v, double dI,
-                                              double dJ, int32_t mJ, double &best, int32_t &bj) {
-    if (J == I || mJ >= 0) return;
-    const double s = -v / sqrt(dI * dJ);
-    if (s > 0.0 && (s > best || (s == best && J < bj))) {
-        best = s;
-        bj = J;
-    }
-}
+// One warp per 32 consecutive nodes (CSR-vector form): the lanes walk the
+// flattened entries of the warp's unmatched rows 32 at a time, so every
+// lane's gathers (mate and diag of the neighbour) are in flight together
+// whatever the row lengths; a segmented shuffle reduction gives each row's
+// best entry in the chunk, merged into a per-row slot in shared memory. The
+// result (largest strength, ties to the smaller J) is order-free.
+constexpr int kPickWarps = 8;
 
 __device__ __forceinline__ void pick_merge(double ob, int32_t oj, double &best, int32_t &bj) {
     if (oj >= 0 && (bj < 0 || ob > best || (ob == best && oj < bj))) {
@@ -136,70 +125,96 @@ __device__ __forceinline__ void pick_merge(double ob, int32_t oj, double &best, 
     }
 }
 
-__global__ void __launch_bounds__(kPickThreads) k_pick(LevelView L, const int32_t *count,
-                                                       const int32_t *mate, int32_t *pick) {
-    __shared__ int32_t queue[kPickThreads];
-    __shared__ int qn;
-    if (threadIdx.x == 0) qn = 0;
-    __syncthreads();
-    const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
+// kFirst (first round of a level: nothing is matched yet): computes every
+// entry's strength and stores it in sbuf (y rows of level 0 at offset yoff);
+// later rounds read it back and gather only the neighbour's mate.
+template <bool kFirst>
+__global__ void __launch_bounds__(32 * kPickWarps) k_pick(LevelView L, const int32_t *count,
+                                                          const int32_t *mate, int32_t *pick,
+                                                          double *sbuf, int64_t yoff) {
+    __shared__ double best_s[kPickWarps][32];
+    __shared__ int32_t best_j[kPickWarps][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int32_t cnt = *count;
-    if (I < cnt) {
-        if (mate[I] >= 0) {
-            pick[I] = -1;
-        } else {
-            const RowRef r = row_of(L, I);
-            if (r.e1 - r.e0 > kPickShort) {
-                queue[atomicAdd(&qn, 1)] = I;
+    const int32_t base = (blockIdx.x * kPickWarps + w) * 32;
+    if (base >= cnt) return;  // whole warp
+    const int32_t I = base + lane;
+    bool act = false, yax = false;
+    int32_t e0 = 0, len = 0;
+    double dI = 1.0;
+    if (I < cnt && (kFirst || mate[I] < 0)) {
+        act = true;
+        const RowRef r = row_of(L, I);
+        e0 = r.e0;
+        len = r.e1 - r.e0;
+        yax = r.off != 0;
+        if (kFirst) dI = diag_of(L, I);
+    }
+    int32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int32_t excl = incl - len;
+    const int32_t T = __shfl_sync(0xffffffffu, incl, 31);
+    best_s[w][lane] = 0.0;
+    best_j[w][lane] = -1;
+    __syncwarp();
+    for (int32_t t0 = 0; t0 < T; t0 += 32) {
+        const int32_t t = t0 + lane;
+        // row of entry t: the last lane whose exclusive offset is <= t
+        int row = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cand = row + step;
+            const int32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+            if (cand < 32 && ex <= t) row = cand;
+        }
+        const int32_t re0 = __shfl_sync(0xffffffffu, e0, row);
+        const int32_t rex = __shfl_sync(0xffffffffu, excl, row);
+        const bool ry = __shfl_sync(0xffffffffu, yax, row);
+        const double rd = __shfl_sync(0xffffffffu, dI, row);
+        double sv = 0.0;
+        int32_t sj = -1;
+        if (t < T) {
+            const int32_t e = re0 + (t - rex);
+            const int32_t *col = L.fine ? (ry ? L.col1 : L.col0) : L.ccol;
+            const int32_t J = __ldg(col + e) + (ry ? L.n : 0);
+            double *sp = sbuf + (ry ? yoff : 0) + e;
+            double st;
+            if (kFirst) {
+                const double *val = L.fine ? (ry ? L.val1 : L.val0) : L.cval;
+                st = -__ldg(val + e) / sqrt(rd * diag_of(L, J));
+                *sp = st;
             } else {
-                const double dI = diag_of(L, I);
-                double best = 0.0;
-                int32_t bj = -1;
-                int32_t e = r.e0;
-                for (; e + 4 <= r.e1; e += 4) {
-                    int32_t J[4], mJ[4];
-                    double v[4], dJ[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        J[q] = __ldg(r.col + e + q) + r.off;
-                        v[q] = __ldg(r.val + e + q);
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        mJ[q] = mate[J[q]];
-                        dJ[q] = diag_of(L, J[q]);
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) pick_consider(I, J[q], v[q], dI, dJ[q], mJ[q], best, bj);
-                }
-                for (; e < r.e1; ++e) {
-                    const int32_t J = __ldg(r.col + e) + r.off;
-                    pick_consider(I, J, __ldg(r.val + e), dI, diag_of(L, J), mate[J], best, bj);
-                }
-                pick[I] = bj;
+                st = *sp;
+            }
+            if (J != base + row && st > 0.0 && (kFirst || mate[J] < 0)) {
+                sv = st;
+                sj = J;
             }
         }
-    }
-    __syncthreads();
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int q = w; q < qn; q += kPickThreads / 32) {
-        const int32_t node = queue[q];
-        const RowRef r = row_of(L, node);
-        const double dI = diag_of(L, node);
-        double best = 0.0;
-        int32_t bj = -1;
-        for (int32_t e = r.e0 + lane; e < r.e1; e += 32) {
-            const int32_t J = __ldg(r.col + e) + r.off;
-            pick_consider(node, J, __ldg(r.val + e), dI, diag_of(L, J), mate[J], best, bj);
-        }
+        // segmented max over lanes of the same row (contiguous in the chunk)
+        const int rowv = t < T ? row : -1;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int32_t oj = __shfl_xor_sync(0xffffffffu, bj, o);
-            pick_merge(ob, oj, best, bj);
+        for (int o = 1; o < 32; o <<= 1) {
+            const double os = __shfl_down_sync(0xffffffffu, sv, o);
+            const int32_t oj = __shfl_down_sync(0xffffffffu, sj, o);
+            const int orow = __shfl_down_sync(0xffffffffu, rowv, o);
+            if (lane + o < 32 && orow == rowv) pick_merge(os, oj, sv, sj);
         }
-        if (lane == 0) pick[node] = bj;
+        const int prow = __shfl_up_sync(0xffffffffu, rowv, 1);
+        if (rowv >= 0 && (lane == 0 || prow != rowv)) {
+            double b = best_s[w][rowv];
+            int32_t bj = best_j[w][rowv];
+            pick_merge(sv, sj, b, bj);
+            best_s[w][rowv] = b;
+            best_j[w][rowv] = bj;
+        }
+        __syncwarp();
     }
+    if (I < cnt) pick[I] = act ? best_j[w][lane] : -1;
 }
 
 __global__ void k_handshake(const int32_t *count, const int32_t *pick, int32_t *mate) {
@@ -325,46 +340,56 @@ __global__ void k_reset_mate(const int32_t *count, int32_t *mate) {
     if (I < *count) mate[I] = -1;
 }
 
+// Raw length of every coarse row, and where its children's rows start
+// (row a at ea[J] with la[J] entries, row b at eb[J]), so that the coarse
+// kernels fetch all of a row's metadata in one round of independent loads.
 __global__ void k_rawlen(LevelView L, const int32_t *count, const int32_t *child0,
-                         const int32_t *child1, int32_t *rawlen) {
+                         const int32_t *child1, int32_t *rawlen, int32_t *ea, int32_t *eb,
+                         int32_t *la_out) {
     const int32_t J = blockIdx.x * blockDim.x + threadIdx.x;
     if (J >= *count) return;
     const RowRef ra = row_of(L, child0[J]);
-    int32_t len = ra.e1 - ra.e0;
+    const int32_t la = ra.e1 - ra.e0;
+    int32_t len = la, e0b = ra.e0;
     const int32_t b = child1[J];
     if (b >= 0) {
         const RowRef rb = row_of(L, b);
         len += rb.e1 - rb.e0;
+        e0b = rb.e0;
     }
     rawlen[J] = len;
+    ea[J] = ra.e0;
+    eb[J] = e0b;
+    la_out[J] = la;
 }
 
 // Coarse row J = (a, b): the raw entries (row a's, then row b's) mapped to
 // coarse ids; ids equal to J fold into the diagonal in raw order
 // (d_a, a's entries, d_b, b's entries); the others are summed per id in raw
 // order and stored with the ids ascending. Two persistent grid-stride kernels:
-//   k_coarse_light: one thread per row of raw length R <= kLight, sorted
-//     insertion into a per-thread list in shared memory, entries fetched
-//     eight at a time; longer rows are appended to a list (order free: each
-//     row is processed on its own);
-//   k_coarse_heavy: one warp per listed row: bitonic sort of (id, raw index)
-//     in shared memory for R <= kHeavyMax, else sorted insertion by one lane
-//     directly in the output row (rare: rows that long need nets of hundreds
-//     of pins).
-constexpr int kLight = 32;
-constexpr int kLightThreads = 128;
-constexpr int kHeavyMax = 1024;
-constexpr int kHeavyWarps = 4;
-constexpr size_t kHeavySmem = static_cast<size_t>(kHeavyWarps) * kHeavyMax * 16;
+//   k_coarse_warp: one warp per row of raw length R <= kWarpRaw, two raw
+//     entries per lane in registers; for every entry the warp walks all R
+//     entries by shuffles to find whether it is the first of its id, its
+//     rank among the distinct ids and its raw-order sum; longer rows are
+//     appended to a list (order free: each row is processed on its own);
+//   k_coarse_heavy: one block per listed row: bitonic sort of (id, raw
+//     index) in shared memory for R <= kHeavyMax, output ranks by a block
+//     scan; longer rows by sorted insertion in one thread directly in the
+//     output row (rare: rows that long need nets of hundreds of pins).
+constexpr int kWarpRaw = 64;
+constexpr int kWarpWarps = 8;
+constexpr int kHeavyMax = 2048;
+constexpr int kHeavyThreads = 256;
 
 struct CoarseArgs {
     LevelView L;
     const int32_t *count;
     const int32_t *child0, *child1, *cid, *start, *rawlen;
+    const int32_t *ea, *eb, *la;  // children's row starts and row a's length
     int32_t *out_len, *out_col;
     double *out_val, *out_diag;
-    int32_t *heavy;        // rows with R > kLight
-    int32_t *heavy_count;  // zero before k_coarse_light
+    int32_t *heavy;        // rows with R > kWarpRaw
+    int32_t *heavy_count;  // zero before k_coarse_warp
 };
 
 // Sorted insertion of (K, v) into keys/sums[0..k) (stride apart).
@@ -386,95 +411,192 @@ __device__ __forceinline__ void sorted_add(KeyPtr keys, SumPtr sums, int stride,
     ++k;
 }
 
-__global__ void __launch_bounds__(kLightThreads) k_coarse_light(CoarseArgs A) {
-    __shared__ int32_t keys_s[kLight * kLightThreads];
-    __shared__ double sums_s[kLight * kLightThreads];
-    constexpr int T = kLightThreads;
-    int32_t *keys = keys_s + threadIdx.x;  // entry q at keys[q * T]
-    double *sums = sums_s + threadIdx.x;
+// Row references of coarse row J's children from the precomputed starts
+// (both children are rows of the same axis at level 0).
+__device__ __forceinline__ void child_rows(const CoarseArgs &A, int32_t J, int32_t a, RowRef &ra,
+                                           RowRef &rb, int &la) {
     const LevelView &L = A.L;
-    const int32_t cnt = *A.count;
-    for (int32_t J = blockIdx.x * blockDim.x + threadIdx.x; J < cnt; J += gridDim.x * blockDim.x) {
-        const int32_t R = A.rawlen[J];
-        if (R > kLight) {
-            A.heavy[atomicAdd(A.heavy_count, 1)] = J;
-            continue;
-        }
-        const int32_t a = A.child0[J], b = A.child1[J];
-        const RowRef ra = row_of(L, a);
-        const int la = ra.e1 - ra.e0;
-        RowRef rb = ra;
-        if (b >= 0) rb = row_of(L, b);
-        double dacc = diag_of(L, a);
-        int k = 0;
-        for (int e0 = 0; e0 < R; e0 += 8) {
-            int32_t K[8];
-            double v[8];
+    la = A.la[J];
+    const bool y = L.fine && a >= L.n;
+    ra.e0 = A.ea[J];
+    ra.e1 = ra.e0 + la;
+    ra.off = y ? L.n : 0;
+    ra.col = L.fine ? (y ? L.col1 : L.col0) : L.ccol;
+    ra.val = L.fine ? (y ? L.val1 : L.val0) : L.cval;
+    rb = ra;
+    rb.e0 = A.eb[J];
+    rb.e1 = rb.e0;  // unused: raw index e >= la selects row b
+}
+
+// Raw entry e of coarse row (a, b): its coarse id and value.
+__device__ __forceinline__ void raw_entry(const CoarseArgs &A, const RowRef &ra, const RowRef &rb,
+                                          int la, int e, int32_t &K, double &v) {
+    const bool in_a = e < la;
+    const int32_t idx = in_a ? ra.e0 + e : rb.e0 + (e - la);
+    K = A.cid[__ldg((in_a ? ra.col : rb.col) + idx) + (in_a ? ra.off : rb.off)];
+    v = __ldg((in_a ? ra.val : rb.val) + idx);
+}
+
+// Compare-exchange of a bitonic network: keep the smaller key when this
+// position should hold the smaller one.
+template <typename KeyT>
+__device__ __forceinline__ KeyT bitonic_keep(KeyT mine, KeyT other, bool keep_small) {
+    const bool less = mine < other;
+    return (less == keep_small) ? mine : other;
+}
+
+// Bitonic sort of P keys held two per lane (positions 2 * lane and
+// 2 * lane + 1), ascending; fully unrolled so every direction mask is a
+// constant. Positions at or beyond P (lanes >= P / 2) are left alone.
+template <int P, typename KeyT>
+__device__ __forceinline__ void bitonic_pairs(KeyT &k0, KeyT &k1, int lane) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int e = e0 + q;
-                K[q] = -1;
-                v[q] = 0.0;
-                if (e < R) {
-                    const bool in_a = e < la;
-                    const int32_t idx = in_a ? ra.e0 + e : rb.e0 + (e - la);
-                    const int32_t c = __ldg((in_a ? ra.col : rb.col) + idx) + (in_a ? ra.off : rb.off);
-                    v[q] = __ldg((in_a ? ra.val : rb.val) + idx);
-                    K[q] = c;
-                }
+    for (int kk = 2; kk <= P; kk <<= 1) {
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            const int p0 = 2 * lane;
+            const bool asc = (p0 & kk) == 0;  // the same for p0 and p0 + 1
+            if (j == 1) {
+                const KeyT lo = k0 < k1 ? k0 : k1, hi = k0 < k1 ? k1 : k0;
+                k0 = asc ? lo : hi;
+                k1 = asc ? hi : lo;
+            } else {
+                const KeyT o0 = __shfl_xor_sync(0xffffffffu, k0, j >> 1);
+                const KeyT o1 = __shfl_xor_sync(0xffffffffu, k1, j >> 1);
+                const bool keep_small = ((p0 & j) == 0) == asc;  // p0 + 1 has the same bit j
+                k0 = bitonic_keep(k0, o0, keep_small);
+                k1 = bitonic_keep(k1, o1, keep_small);
             }
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (e0 + q < R) K[q] = A.cid[K[q]];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int e = e0 + q;
-                if (e >= R) break;
-                if (e == la) dacc += diag_of(L, b);
-                if (K[q] == J) dacc += v[q];
-                else sorted_add(keys, sums, T, k, K[q], v[q]);
-            }
         }
-        if (la == R && b >= 0) dacc += diag_of(L, b);
-        int32_t *oc = A.out_col + A.start[J];
-        double *ov = A.out_val + A.start[J];
-        for (int q = 0; q < k; ++q) {
-            oc[q] = keys[q * T];
-            ov[q] = sums[q * T];
-        }
-        A.out_len[J] = k;
-        A.out_diag[J] = dacc;
     }
 }
 
-__global__ void __launch_bounds__(32 * kHeavyWarps) k_coarse_heavy(CoarseArgs A) {
-    extern __shared__ unsigned long long heavy_smem[];
+// Keys are (coarse id << kShift) | raw index: 32-bit when the ids fit in
+// 26 bits, else 64-bit.
+template <typename KeyT>
+__global__ void __launch_bounds__(32 * kWarpWarps) k_coarse_warp(CoarseArgs A) {
+    constexpr int kShift = sizeof(KeyT) == 8 ? 32 : 6;
+    constexpr KeyT kPad = ~KeyT(0);
+    // per warp: the sorted (key, value) sequence, for the segment folds
+    __shared__ KeyT skey_s[kWarpWarps][kWarpRaw];
+    __shared__ double sval_s[kWarpWarps][kWarpRaw];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned long long *key = heavy_smem + static_cast<size_t>(w) * kHeavyMax * 2;
-    double *vr = reinterpret_cast<double *>(key + kHeavyMax);
+    KeyT *skey = skey_s[w];
+    double *sval = sval_s[w];
     const LevelView &L = A.L;
+    const int32_t cnt = *A.count;
+    const int32_t warps = gridDim.x * kWarpWarps;
+    for (int32_t J = blockIdx.x * kWarpWarps + w; J < cnt; J += warps) {
+        const int32_t R = A.rawlen[J];
+        if (R > kWarpRaw) {
+            if (lane == 0) A.heavy[atomicAdd(A.heavy_count, 1)] = J;
+            continue;
+        }
+        const int32_t a = A.child0[J], b = A.child1[J];
+        RowRef ra, rb;
+        int la;
+        child_rows(A, J, a, ra, rb, la);
+        // positions p = 2 * lane + r hold raw entries e = p (r = 0, 1)
+        KeyT k0 = kPad, k1 = kPad;
+        double v0 = 0.0, v1 = 0.0;
+        {
+            const int e0 = 2 * lane, e1 = 2 * lane + 1;
+            int32_t K;
+            if (e0 < R) {
+                raw_entry(A, ra, rb, la, e0, K, v0);
+                k0 = (static_cast<KeyT>(static_cast<uint32_t>(K)) << kShift) | KeyT(e0);
+            }
+            if (e1 < R) {
+                raw_entry(A, ra, rb, la, e1, K, v1);
+                k1 = (static_cast<KeyT>(static_cast<uint32_t>(K)) << kShift) | KeyT(e1);
+            }
+        }
+        // raw values by raw index, for the folds after the sort
+        sval[2 * lane] = v0;
+        sval[2 * lane + 1] = v1;
+        // bitonic sort of the keys over P = 32 or 64 positions
+        if (R <= 32) bitonic_pairs<32>(k0, k1, lane);
+        else bitonic_pairs<64>(k0, k1, lane);
+        skey[2 * lane] = k0;
+        skey[2 * lane + 1] = k1;
+        __syncwarp();
+        // segment heads: first position of each id; ids != J are output rows
+        const uint32_t uJ = static_cast<uint32_t>(J);
+        const uint32_t K0 = static_cast<uint32_t>(k0 >> kShift), K1 = static_cast<uint32_t>(k1 >> kShift);
+        const uint32_t Kprev = lane == 0 ? 0xffffffffu
+                                         : static_cast<uint32_t>(skey[2 * lane - 1] >> kShift);
+        const bool in0 = 2 * lane < R, in1 = 2 * lane + 1 < R;
+        const bool first0 = in0 && (lane == 0 || Kprev != K0);
+        const bool first1 = in1 && K1 != K0;
+        const bool h0 = first0 && K0 != uJ, h1 = first1 && K1 != uJ;
+        const unsigned b0 = __ballot_sync(0xffffffffu, h0), b1 = __ballot_sync(0xffffffffu, h1);
+        const unsigned below = (1u << lane) - 1u;
+        const int rank0 = __popc(b0 & below) + __popc(b1 & below);
+        const int rank1 = rank0 + (h0 ? 1 : 0);
+        const int32_t st = A.start[J];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const bool h = r == 0 ? h0 : h1;
+            const bool dh = (r == 0 ? first0 : first1) && (r == 0 ? K0 : K1) == uJ;
+            const int p = 2 * lane + r;
+            const uint32_t K = r == 0 ? K0 : K1;
+            if (h) {
+                double sum = sval[static_cast<uint32_t>(skey[p] & ((KeyT(1) << kShift) - 1))];
+                for (int q = p + 1; q < R && static_cast<uint32_t>(skey[q] >> kShift) == K; ++q)
+                    sum += sval[static_cast<uint32_t>(skey[q] & ((KeyT(1) << kShift) - 1))];
+                const int rank = r == 0 ? rank0 : rank1;
+                A.out_col[st + rank] = static_cast<int32_t>(K);
+                A.out_val[st + rank] = sum;
+            }
+            if (dh) {
+                double dacc = diag_of(L, a);
+                bool added_b = false;
+                for (int q = p; q < R && static_cast<uint32_t>(skey[q] >> kShift) == K; ++q) {
+                    const uint32_t idx = static_cast<uint32_t>(skey[q] & ((KeyT(1) << kShift) - 1));
+                    if (!added_b && static_cast<int>(idx) >= la) {
+                        dacc += diag_of(L, b);
+                        added_b = true;
+                    }
+                    dacc += sval[idx];
+                }
+                if (!added_b && b >= 0) dacc += diag_of(L, b);
+                A.out_diag[J] = dacc;
+            }
+        }
+        const bool any_diag = __any_sync(0xffffffffu, (first0 && K0 == uJ) || (first1 && K1 == uJ));
+        if (lane == 0) {
+            A.out_len[J] = __popc(b0) + __popc(b1);
+            if (!any_diag) A.out_diag[J] = b >= 0 ? diag_of(L, a) + diag_of(L, b) : diag_of(L, a);
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kHeavyThreads) k_coarse_heavy(CoarseArgs A) {
+    __shared__ unsigned long long key[kHeavyMax];
+    __shared__ double vr[kHeavyMax];
+    __shared__ int32_t warp_tot[33];
+    const LevelView &L = A.L;
+    const int tid = threadIdx.x;
     const int32_t nh = *A.heavy_count;
-    for (int32_t h = blockIdx.x * kHeavyWarps + w; h < nh; h += gridDim.x * kHeavyWarps) {
+    for (int32_t h = blockIdx.x; h < nh; h += gridDim.x) {
         const int32_t J = A.heavy[h];
         const int32_t R = A.rawlen[J];
         const int32_t a = A.child0[J], b = A.child1[J];
-        const RowRef ra = row_of(L, a);
-        const int la = ra.e1 - ra.e0;
-        RowRef rb = ra;
-        if (b >= 0) rb = row_of(L, b);
+        RowRef ra, rb;
+        int la;
+        child_rows(A, J, a, ra, rb, la);
         if (R > kHeavyMax) {
-            if (lane == 0) {
+            if (tid == 0) {
                 int32_t *keys = A.out_col + A.start[J];
                 double *sums = A.out_val + A.start[J];
                 int k = 0;
                 double dacc = diag_of(L, a);
                 for (int e = 0; e < R; ++e) {
                     if (e == la) dacc += diag_of(L, b);
-                    const bool in_a = e < la;
-                    const int32_t idx = in_a ? ra.e0 + e : rb.e0 + (e - la);
-                    const int32_t K =
-                        A.cid[__ldg((in_a ? ra.col : rb.col) + idx) + (in_a ? ra.off : rb.off)];
-                    const double v = __ldg((in_a ? ra.val : rb.val) + idx);
+                    int32_t K;
+                    double v;
+                    raw_entry(A, ra, rb, la, e, K, v);
                     if (K == J) dacc += v;
                     else sorted_add(keys, sums, 1, k, K, v);
                 }
@@ -482,28 +604,27 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) k_coarse_heavy(CoarseArgs A)
                 A.out_len[J] = k;
                 A.out_diag[J] = dacc;
             }
-            __syncwarp();
+            __syncthreads();
             continue;
         }
         int P = 1;
         while (P < R) P <<= 1;
-        for (int e = lane; e < P; e += 32) {
+        for (int e = tid; e < P; e += kHeavyThreads) {
             if (e < R) {
-                const bool in_a = e < la;
-                const int32_t idx = in_a ? ra.e0 + e : rb.e0 + (e - la);
-                const int32_t K =
-                    A.cid[__ldg((in_a ? ra.col : rb.col) + idx) + (in_a ? ra.off : rb.off)];
+                int32_t K;
+                double v;
+                raw_entry(A, ra, rb, la, e, K, v);
                 key[e] = (static_cast<unsigned long long>(static_cast<uint32_t>(K)) << 32) |
                          static_cast<uint32_t>(e);
-                vr[e] = __ldg((in_a ? ra.val : rb.val) + idx);
+                vr[e] = v;
             } else {
                 key[e] = ~0ull;
             }
         }
-        __syncwarp();
+        __syncthreads();
         for (int kk = 2; kk <= P; kk <<= 1) {
             for (int j = kk >> 1; j > 0; j >>= 1) {
-                for (int i = lane; i < P; i += 32) {
+                for (int i = tid; i < P; i += kHeavyThreads) {
                     const int ixj = i ^ j;
                     if (ixj > i) {
                         const unsigned long long x = key[i], y = key[ixj];
@@ -513,15 +634,15 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) k_coarse_heavy(CoarseArgs A)
                         }
                     }
                 }
-                __syncwarp();
+                __syncthreads();
             }
         }
-        // segment heads (ids != J) in ascending order, numbered by a warp scan
+        // segment heads (ids != J) in ascending order, ranked by a block scan
         const uint32_t uJ = static_cast<uint32_t>(J);
-        int base = 0;
-        bool any_diag = false;
-        for (int i0 = 0; i0 < R; i0 += 32) {
-            const int i = i0 + lane;
+        int32_t running = 0;
+        int any_diag = 0;
+        for (int i0 = 0; i0 < R; i0 += kHeavyThreads) {
+            const int i = i0 + tid;
             bool head = false, dhead = false;
             uint32_t K = 0;
             if (i < R) {
@@ -530,21 +651,20 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) k_coarse_heavy(CoarseArgs A)
                 head = first && K != uJ;
                 dhead = first && K == uJ;
             }
-            const unsigned hm = __ballot_sync(0xffffffffu, head);
-            any_diag = any_diag || __any_sync(0xffffffffu, dhead);
+            int32_t tot;
+            const int32_t ex = block_excl_scan(head ? 1 : 0, warp_tot, tot);
             if (head) {
-                const int pos = base + __popc(hm & ((1u << lane) - 1u));
                 double sum = vr[static_cast<uint32_t>(key[i])];
-                for (int j = i + 1; j < R && static_cast<uint32_t>(key[j] >> 32) == K; ++j)
-                    sum += vr[static_cast<uint32_t>(key[j])];
-                A.out_col[A.start[J] + pos] = static_cast<int32_t>(K);
-                A.out_val[A.start[J] + pos] = sum;
+                for (int q = i + 1; q < R && static_cast<uint32_t>(key[q] >> 32) == K; ++q)
+                    sum += vr[static_cast<uint32_t>(key[q])];
+                A.out_col[A.start[J] + running + ex] = static_cast<int32_t>(K);
+                A.out_val[A.start[J] + running + ex] = sum;
             }
             if (dhead) {
                 double dacc = diag_of(L, a);
                 bool added_b = false;
-                for (int j = i; j < R && static_cast<uint32_t>(key[j] >> 32) == K; ++j) {
-                    const uint32_t idx = static_cast<uint32_t>(key[j]);
+                for (int q = i; q < R && static_cast<uint32_t>(key[q] >> 32) == K; ++q) {
+                    const uint32_t idx = static_cast<uint32_t>(key[q]);
                     if (!added_b && static_cast<int>(idx) >= la) {
                         dacc += diag_of(L, b);
                         added_b = true;
@@ -554,13 +674,14 @@ __global__ void __launch_bounds__(32 * kHeavyWarps) k_coarse_heavy(CoarseArgs A)
                 if (!added_b && b >= 0) dacc += diag_of(L, b);
                 A.out_diag[J] = dacc;
             }
-            base += __popc(hm);
+            any_diag |= __syncthreads_or(dhead ? 1 : 0);
+            running += tot;
         }
-        if (lane == 0) {
-            A.out_len[J] = base;
+        if (tid == 0) {
+            A.out_len[J] = running;
             if (!any_diag) A.out_diag[J] = b >= 0 ? diag_of(L, a) + diag_of(L, b) : diag_of(L, a);
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 
@@ -629,8 +750,8 @@ __global__ void k_pfill(LevelView L, int32_t rows, const int32_t *order, const i
 
 // Eight lanes per aggregate, lane m owning row m of the block: the block
 // row from the permuted CSR, a row-oriented Cholesky B = L L^T in FP64 with
-// the finished rows broadcast by shuffles, L^-1 by forward substitution and
-// inv = L^-T L^-1, written as 8 floats per row. All arrays are indexed by
+// the finished rows broadcast by shuffles (one division per pivot), L^-1 by
+// forward substitution and inv = L^-T L^-1, written as 8 floats per row. All arrays are indexed by
 // compile-time constants, so they stay in registers.
 __global__ void __launch_bounds__(256) k_blockinv(const int32_t *count, const int32_t *agg_start,
                                                   const int32_t *size, int32_t n,
@@ -683,8 +804,10 @@ __global__ void __launch_bounds__(256) k_blockinv(const int32_t *count, const in
             for (int q = 0; q < kAggMax; ++q) l[q] += q == qq ? v : 0.0;
         }
     }
-    // Cholesky: after step j, lane j holds L[j][0..j] and lanes i > j hold L[i][j].
+    // Cholesky: after step j, lane j holds L[j][0..j] and lanes i > j hold L[i][j];
+    // one reciprocal per pivot (rinv = 1 / L[m][m] kept by lane m).
     bool ok = true;
+    double rinv = 1.0;
 #pragma unroll
     for (int j = 0; j < kAggMax; ++j) {
         if (m == j && act) {
@@ -693,15 +816,17 @@ __global__ void __launch_bounds__(256) k_blockinv(const int32_t *count, const in
             for (int q = 0; q < j; ++q) s -= l[q] * l[q];
             ok = s > 0.0;
             l[j] = ok ? sqrt(s) : 1.0;
+            rinv = 1.0 / l[j];
         }
         double rj[kAggMax];
 #pragma unroll
-        for (int q = 0; q <= j; ++q) rj[q] = __shfl_sync(0xffffffffu, l[q], j, kAggMax);
+        for (int q = 0; q < j; ++q) rj[q] = __shfl_sync(0xffffffffu, l[q], j, kAggMax);
+        const double rjinv = __shfl_sync(0xffffffffu, rinv, j, kAggMax);
         if (act && m > j && j < k) {
             double u = l[j];
 #pragma unroll
             for (int q = 0; q < j; ++q) u -= l[q] * rj[q];
-            l[j] = u / rj[j];
+            l[j] = u * rjinv;
         }
     }
     const unsigned bad = __ballot_sync(0xffffffffu, !ok);
@@ -717,7 +842,7 @@ __global__ void __launch_bounds__(256) k_blockinv(const int32_t *count, const in
     for (int r = 0; r < kAggMax; ++r) {
         if (m == r && act) {
 #pragma unroll
-            for (int c = 0; c <= r; ++c) li[c] = ((c == r ? 1.0 : 0.0) - acc[c]) / l[r];
+            for (int c = 0; c <= r; ++c) li[c] = ((c == r ? 1.0 : 0.0) - acc[c]) * rinv;
         }
         double rt[kAggMax];
 #pragma unroll
@@ -747,7 +872,7 @@ __global__ void __launch_bounds__(256) k_blockinv(const int32_t *count, const in
     }
     if (!act) return;
     float *dst = minv + static_cast<size_t>(first + m) * kAggMax;
-    const double dm = 1.0 / pdiag[first + m];
+    const double dm = group_ok ? 0.0 : 1.0 / pdiag[first + m];
 #pragma unroll
     for (int q = 0; q < kAggMax; ++q) {
         const double v = group_ok ? inv[q] : (q == m ? dm : 0.0);
@@ -805,7 +930,8 @@ int reserve(ktg_ctx *c, AggState *s, int64_t rows, int64_t nnz) {
     if (rows > s->cap_rows) {
         for (int32_t **p : {&s->mate, &s->pick, &s->flag, &s->cid, &s->child0, &s->child1,
                             &s->size_a, &s->size_b, &s->cur, &s->pos, &s->cstart[0], &s->cstart[1],
-                            &s->clen[0], &s->clen[1], &s->order, &s->newpos, &s->meta})
+                            &s->clen[0], &s->clen[1], &s->order, &s->newpos, &s->meta, &s->ea,
+                            &s->eb, &s->la})
             if ((rc = grow(c, p, rows))) return rc;
         if ((rc = grow(c, &s->agg_start, rows + 1))) return rc;
         if ((rc = grow(c, &s->prp, rows + 1))) return rc;
@@ -858,7 +984,8 @@ void free_agg(ktg_ctx *c) {
                     (void *)s->agg_start, (void *)s->order, (void *)s->newpos, (void *)s->prp,
                     (void *)s->pcol, (void *)s->pval, (void *)s->pval32, (void *)s->pdiag,
                     (void *)s->prhs, (void *)s->px, (void *)s->minv, (void *)s->meta,
-                    (void *)s->blk_start, (void *)s->gslice})
+                    (void *)s->blk_start, (void *)s->gslice, (void *)s->ea, (void *)s->eb,
+                    (void *)s->la})
         if (p) cudaFree(p);
     delete s;
     c->agg = nullptr;
@@ -877,12 +1004,6 @@ int build_agg(ktg_ctx *c) {
     const int64_t nnz_cap = 2 * c->sys_cap_nnz;
     int rc = reserve(c, s, rows, nnz_cap);
     if (rc) return rc;
-    static bool attr_set = false;
-    if (!attr_set) {
-        KTG_CUDA(c, cudaFuncSetAttribute(k_coarse_heavy, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kHeavySmem)));
-        attr_set = true;
-    }
     const int32_t R = static_cast<int32_t>(rows);
     if (rows == 0) {  // counts all zero: empty row ranges for the solve
         k_init<<<1, kT, 0, c->stream>>>(0, s->cur, s->pos, s->size_a, s->mate, s->counts);
@@ -911,9 +1032,17 @@ int build_agg(ktg_ctx *c) {
     LevelView L = L0;
     for (int level = 0; level < kLevels; ++level) {
         const int32_t *count = cnt + level;
+        // strengths of this level's entries live in cval[level & 1] until this
+        // level's coarsening overwrites that buffer (level 0 reads the axis
+        // CSRs, level l > 0 reads cval[(l - 1) & 1])
+        double *sbuf = s->cval[level & 1];
+        const int64_t yoff = c->sys_cap_nnz;
+        const int gP = blocks_for(rows, 32 * kPickWarps);
         for (int round = 0; round < kRounds; ++round) {
-            k_pick<<<blocks_for(rows, kPickThreads), kPickThreads, 0, c->stream>>>(L, count, s->mate,
-                                                                                   s->pick);
+            if (round == 0)
+                k_pick<true><<<gP, 32 * kPickWarps, 0, c->stream>>>(L, count, s->mate, s->pick, sbuf, yoff);
+            else
+                k_pick<false><<<gP, 32 * kPickWarps, 0, c->stream>>>(L, count, s->mate, s->pick, sbuf, yoff);
             k_handshake<<<gR, kT, 0, c->stream>>>(count, s->pick, s->mate);
             c->launches += 2;
         }
@@ -929,15 +1058,19 @@ int build_agg(ktg_ctx *c) {
             const int32_t *next = cnt + level + 1;
             // raw lengths in s->pick (free until the next level's matching);
             // the heavy-row list in s->flag (its scan was used by k_number)
-            k_rawlen<<<gR, kT, 0, c->stream>>>(L, next, s->child0, s->child1, s->pick);
+            k_rawlen<<<gR, kT, 0, c->stream>>>(L, next, s->child0, s->child1, s->pick, s->ea,
+                                               s->eb, s->la);
             scan(c, s, s->pick, s->cstart[t], next, rows, cnt + 4);
             KTG_CUDA(c, cudaMemsetAsync(cnt + 7, 0, sizeof(int32_t), c->stream));
-            const CoarseArgs CA{L,          next,        s->child0,   s->child1,
-                                s->cid,     s->cstart[t], s->pick,    s->clen[t],
-                                s->ccol[t], s->cval[t],  s->cdiag[t], s->flag,
+            const CoarseArgs CA{L,          next,         s->child0, s->child1,  s->cid,
+                                s->cstart[t], s->pick,    s->ea,     s->eb,      s->la,
+                                s->clen[t], s->ccol[t],   s->cval[t], s->cdiag[t], s->flag,
                                 cnt + 7};
-            k_coarse_light<<<4 * c->num_sms, kLightThreads, 0, c->stream>>>(CA);
-            k_coarse_heavy<<<3 * c->num_sms, 32 * kHeavyWarps, kHeavySmem, c->stream>>>(CA);
+            if (rows < (1ll << 26))
+                k_coarse_warp<uint32_t><<<8 * c->num_sms, 32 * kWarpWarps, 0, c->stream>>>(CA);
+            else
+                k_coarse_warp<unsigned long long><<<8 * c->num_sms, 32 * kWarpWarps, 0, c->stream>>>(CA);
+            k_coarse_heavy<<<4 * c->num_sms, kHeavyThreads, 0, c->stream>>>(CA);
             k_reset_mate<<<gR, kT, 0, c->stream>>>(next, s->mate);
             c->launches += 4;
             LevelView C{};

@@ -14,6 +14,7 @@ struct AggState {
     int32_t *mate = nullptr, *pick = nullptr, *flag = nullptr, *cid = nullptr;
     int32_t *child0 = nullptr, *child1 = nullptr, *size_a = nullptr, *size_b = nullptr;
     int32_t *cur = nullptr, *pos = nullptr;
+    int32_t *ea = nullptr, *eb = nullptr, *la = nullptr;  // coarse rows' children row starts
     int32_t *cstart[2] = {nullptr, nullptr};
     int32_t *clen[2] = {nullptr, nullptr};
     int32_t *ccol[2] = {nullptr, nullptr};
