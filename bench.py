@@ -331,6 +331,11 @@ def run_ours(args):
     h2d = 8 * n * (4 + 2 + 2 + 2)
     d2h = 8 * n * 2 + 8 * GRID * GRID + 8 * 3 + ctypes.sizeof(SolveInfo)
 
+    kw2_line = None
+    if world == 1:
+        kw2_line = kraftwerk2_leg(torch, dev, stream, raw, max(3, args.steps // 10),
+                                  cpu=not args.no_cpu_baseline)
+
     batch_line = None
     if world == 1 and not args.no_batch:
         batch_line = run_batch_leg(torch, dev, stream, max(3, args.steps // 10))
@@ -383,6 +388,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "batch": batch_line,
+            "kraftwerk2": kw2_line,
             "clocks": clk,
         }
         print(json.dumps(line))
@@ -466,6 +472,73 @@ def solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, in
     base = out["fp64_jacobi"]["ms"]
     for row in out.values():
         row["speedup_vs_fp64"] = base / row["ms"]
+    return out
+
+
+def kraftwerk2_leg(torch, dev, stream, raw, reps: int, cpu: bool) -> dict:
+    """Kraftwerk2's initial-placement step on the same 211k-cell netlist
+    (Kraftwerk2Placer::Impl::placeInitially, kraftwerk2_placer.cc:422-453):
+    buildSystem with rhs for x and y, diag floor 1e-12, CG to its default
+    tolerance 1e-5 with at most 150 iterations, from the bench positions. GPU:
+    ktg_build_b2b_kraftwerk2 + ktg_kraftwerk2_adjust + ktg_solve (CUDA events).
+    Beside it, the reference's own buildSystem and solve (oracle/_ref) on the
+    host cores, when the reference library is present."""
+    from ktplace_b200 import netlist
+    from ktplace_b200.gpu import Context
+    from ktplace_b200._lib import SolveInfo
+    nl = netlist.flatten(raw, kraftwerk2=True)
+    n = nl.num_movable
+    fx, fy = nl.floors()
+    rng = np.random.default_rng(5)
+    lx, ly, ux, uy = nl.die
+    x0 = rng.uniform(lx, ux - nl.width)
+    y0 = rng.uniform(ly, uy - nl.height)
+    ctx = Context(dev.index or 0)
+    ctx.upload_netlist(nl)
+    ctx.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        dx = torch.tensor(x0, device=dev)
+        dy = torch.tensor(y0, device=dev)
+        wx = torch.empty_like(dx)
+        wy = torch.empty_like(dy)
+        info = torch.zeros(ctypes.sizeof(SolveInfo), dtype=torch.uint8, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ms = []
+    for k in range(reps + 1):
+        with torch.cuda.stream(stream):
+            wx.copy_(dx)
+            wy.copy_(dy)
+            e0.record(stream)
+            ctx.build_kraftwerk2_dev(wx, wy, True, fx, fy)
+            ctx.kraftwerk2_adjust_dev(None, None, None, 1e-12)
+            ctx.solve_dev(wx, wy, 1e-5, 150, info)
+            e1.record(stream)
+        e1.synchronize()
+        if k > 0:
+            ms.append(e0.elapsed_time(e1))
+    inf = SolveInfo.from_buffer_copy(bytes(info.cpu().numpy()))
+    out = {"workload": "Kraftwerk2 initial-placement step on synth211k: buildSystem x+y with rhs, "
+                       "diag floor 1e-12, Jacobi-PCG to 1e-5 (max 150)",
+           "gpu_ms": statistics.median(ms), "iters": [int(inf.iters_x), int(inf.iters_y)]}
+    ctx.close()
+    if cpu:
+        import oracle
+        if oracle.ref_available():
+            threads = os.cpu_count() or 1
+            oracle.set_ref_threads(threads)
+            ref = oracle.Kraftwerk2Ref(nl)
+            t = []
+            for k in range(2):
+                t0 = time.perf_counter()
+                for axis, p in ((0, x0), (1, y0)):
+                    r = ref.build(x0, y0, axis == 0, True, fx, fy)
+                    ref.set_diag_rhs(np.maximum(r["diag"], 1e-12), r["rhs"])
+                    ref.solve(p, 1e-5, 150)
+                t.append(1000.0 * (time.perf_counter() - t0))
+            out["reference_cpu_ms"] = min(t)
+            out["reference_cpu_cores"] = threads
+            out["speedup_vs_reference"] = out["reference_cpu_ms"] / out["gpu_ms"]
     return out
 
 

@@ -136,6 +136,25 @@ int ktg_upload_netlist(ktg_ctx *ctx, const ktg_netlist_view *nl);
 int ktg_build_b2b(ktg_ctx *ctx, const double *x, const double *y, double alpha,
                   const double *ax, const double *ay, double floor_x, double floor_y);
 
+/* Kraftwerk2Placer::Impl::buildSystem (globalPlacer/kraftwerk2/
+ * kraftwerk2_placer.cc:328-410) for both axes on the uploaded netlist (the
+ * Kraftwerk2 Design's cells as the movable vertices, each fixed pin as a
+ * fixed vertex at its fixedPosition with zero offset; nets may list a cell
+ * more than once). with_rhs = withRhs. Kraftwerk2's rules: the high bound
+ * pin is the last maximum, base = 2 w / (p - 1), edges to the row's own cell
+ * are skipped, no anchor term, no diagonal floor. floor_x/floor_y are
+ * Impl::floorX/floorY. The systems are then solved by ktg_solve, whose
+ * per-axis iteration is Kraftwerk2's solve (kraftwerk2_placer.cc:86-126). */
+int ktg_build_b2b_kraftwerk2(ktg_ctx *ctx, const double *x, const double *y, int with_rhs,
+                             double floor_x, double floor_y);
+
+/* Kraftwerk2's adjustments of the built systems: with move_weight (n values)
+ * diag += move_weight and rhs = -move_weight * toward (kraftwerk2_placer.cc:
+ * 716-721); then, when diag_floor > 0, diag = max(diag, diag_floor)
+ * (kraftwerk2_placer.cc:433-437, floor 1e-12). move_weight may be NULL. */
+int ktg_kraftwerk2_adjust(ktg_ctx *ctx, const double *move_weight, const double *toward_x,
+                          const double *toward_y, double diag_floor);
+
 /* LinearSystems::buildStar (simpl_lss.cc:116-201) for both axes: the star
  * model of SimPL's initial rounds, with a star variable after the movable
  * cells for every net of three or more pins that has a movable pin. *size

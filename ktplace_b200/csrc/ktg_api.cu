@@ -477,6 +477,63 @@ int ktg_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha, co
     return KTG_OK;
 }
 
+int ktg_build_b2b_kraftwerk2(ktg_ctx *c, const double *x, const double *y, int with_rhs,
+                             double floor_x, double floor_y) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");
+    if (c->n > 0 && (!x || !y)) return set_error(c, KTG_ERR_ARG, "null positions");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = reserve_systems(c, c->n, c->cap_nnz))) return rc;
+    const double *dx = x, *dy = y;
+    if (c->ptr_mode == KTG_PTR_HOST) {
+        if ((rc = upload(c, c->x, x, c->n))) return rc;
+        if ((rc = upload(c, c->y, y, c->n))) return rc;
+        dx = c->x;
+        dy = c->y;
+    }
+    if ((rc = ktg::launch_build_kraftwerk2(c, dx, dy, with_rhs != 0, floor_x, floor_y))) return rc;
+    c->sys_n = c->n;
+    c->have_system = true;
+    c->axis_valid[0] = c->axis_valid[1] = true;
+    c->val32_valid = false;
+    c->precond_ready = false;
+    c->agg_ready = false;
+    if (c->ptr_mode == KTG_PTR_HOST) {
+        const int st = device_status(c);
+        if (st < 0) return st;
+        if (st != 0) return set_error(c, st, "Kraftwerk2 system exceeds its capacity");
+    }
+    return KTG_OK;
+}
+
+int ktg_kraftwerk2_adjust(ktg_ctx *c, const double *move_weight, const double *toward_x,
+                          const double *toward_y, double diag_floor) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no system to adjust");
+    if (move_weight && (!toward_x || !toward_y))
+        return set_error(c, KTG_ERR_ARG, "move_weight needs toward_x and toward_y");
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int64_t n = c->sys_n;
+    const double *mw = move_weight, *tx = toward_x, *ty = toward_y;
+    if (move_weight && c->ptr_mode == KTG_PTR_HOST) {
+        // staging: ax / ay hold the two toward vectors, x holds the weights
+        if ((rc = upload(c, c->ax, toward_x, n))) return rc;
+        if ((rc = upload(c, c->ay, toward_y, n))) return rc;
+        if ((rc = upload(c, c->x, move_weight, n))) return rc;
+        mw = c->x;
+        tx = c->ax;
+        ty = c->ay;
+    }
+    if ((rc = ktg::launch_kraftwerk2_adjust(c, mw, tx, ty, diag_floor))) return rc;
+    c->val32_valid = false;
+    c->precond_ready = false;
+    c->agg_ready = false;
+    if (c->ptr_mode == KTG_PTR_HOST) return sync(c);
+    return KTG_OK;
+}
+
 int ktg_build_star(ktg_ctx *c, int64_t *size) {
     if (!c || !size) return KTG_ERR_ARG;
     if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");

@@ -20,6 +20,14 @@
 // Bit-exactness: the library is compiled with -fmad=false (no FMA
 // contraction, like the reference's -ffp-contract=off) and CUDA's IEEE
 // double division, so every w, val, diag and rhs equals the reference's.
+//
+// The same kernels also build Kraftwerk2's systems
+// (Kraftwerk2Placer::Impl::buildSystem, globalPlacer/kraftwerk2/
+// kraftwerk2_placer.cc:328-410) under its own rules (Rules = kKraftwerk2):
+// the high bound pin is the last maximum (>=), the edge weight base is
+// 2 w / (p - 1), nets may list a cell twice and edges to the row's own cell
+// are skipped, the right-hand side uses the raw pin offsets, and there is
+// neither an anchor term nor a diagonal floor (the caller applies them).
 #include "ktg_common.cuh"
 #include "ktg_context.h"
 
@@ -27,6 +35,7 @@ namespace ktg {
 namespace {
 
 constexpr int kBuildThreads = 256;
+enum Rules { kSimpl = 0, kKraftwerk2 = 1 };
 
 struct NetlistDev {
     const int32_t *var_of_vertex;
@@ -60,7 +69,7 @@ __device__ __forceinline__ double cell_pos(const double *pos, const double *fixe
 }
 
 // One thread per net. WithBounds: also choose the bound pins of both axes.
-template <bool WithBounds>
+template <bool WithBounds, int R = kSimpl>
 __global__ void __launch_bounds__(kBuildThreads)
     k_bound_pins(NetlistDev nl, const double *__restrict__ x, const double *__restrict__ y,
                  uint32_t *__restrict__ lo_x, uint32_t *__restrict__ hi_x,
@@ -91,11 +100,12 @@ __global__ void __launch_bounds__(kBuildThreads)
                     vlx = vhx = px;
                     vly = vhy = py;
                 } else {
-                    // lo = pinAt(q) < pinAt(lo) ? q : lo (simpl_lss.cc:41-42)
+                    // lo = pinAt(q) < pinAt(lo) ? q : lo (simpl_lss.cc:41-42);
+                    // Kraftwerk2: hi = at[q] >= at[hi] ? q : hi (kraftwerk2_placer.cc:341-342)
                     if (px < vlx) { lx = q; vlx = px; }
-                    if (px > vhx) { hx = q; vhx = px; }
+                    if (R == kKraftwerk2 ? px >= vhx : px > vhx) { hx = q; vhx = px; }
                     if (py < vly) { ly = q; vly = py; }
-                    if (py > vhy) { hy = q; vhy = py; }
+                    if (R == kKraftwerk2 ? py >= vhy : py > vhy) { hy = q; vhy = py; }
                 }
             }
             bx0 = ref_min(bx0, px);
@@ -121,8 +131,9 @@ __global__ void __launch_bounds__(kBuildThreads)
 }
 
 // Edges of movable cell i's row on one axis, in the reference's order.
-// Visit(cell_var, other_pos_of_cell, there, own_offset, w) for every edge.
-template <typename Visit>
+// Visit(cell_var, other_pos_of_cell, there, own_offset, w, raw own offset,
+// raw other offset) for every edge.
+template <int R = kSimpl, typename Visit>
 __device__ __forceinline__ void for_each_edge(const NetlistDev &nl, const double *pos,
                                               const double *fixed, const double *off,
                                               const uint32_t *lo, const uint32_t *hi,
@@ -138,16 +149,19 @@ __device__ __forceinline__ void for_each_edge(const NetlistDev &nl, const double
         const uint32_t h = hi[k];
         if (l == h) continue;
         const int32_t s = nl.net_start[k];
-        const double base = nl.net_base[k];
-        const double own = own_pos + off[s + q];
+        // Kraftwerk2's base, w * 2 / (p - 1), is exactly twice w / (p - 1)
+        const double base = R == kKraftwerk2 ? 2.0 * nl.net_base[k] : nl.net_base[k];
+        const double own_raw = off[s + q];
+        const double own = own_pos + own_raw;
         const double own_offset = own - own_pos;
         auto edge = [&](uint32_t t) {
             const int32_t p = s + static_cast<int32_t>(t);
             const int32_t var = nl.pin_var[p];
+            if (R == kKraftwerk2 && var == i) return;  // a second pin of the row's own cell
             const double cp = cell_pos(pos, fixed, var, nl.pin_cell[p]);
             const double there = cp + off[p];
             const double w = base / ref_max(fabs(own - there), floor_len);
-            visit(var, cp, there, own_offset, w);
+            visit(var, cp, there, own_offset, w, own_raw, off[p]);
         };
         if (q == l || q == h) {
             const int32_t deg = nl.net_start[k + 1] - s;
@@ -176,6 +190,7 @@ struct AxisArgs {
 };
 
 // Count of movable other ends per row; per-block totals for the scan.
+template <int R = kSimpl>
 __global__ void __launch_bounds__(kBuildThreads)
     k_row_count(NetlistDev nl, AxisArgs ax, AxisArgs ay, int32_t blocks_per_axis,
                 int32_t *__restrict__ row_cnt, int64_t *__restrict__ block_sum_out) {
@@ -194,10 +209,23 @@ __global__ void __launch_bounds__(kBuildThreads)
             const uint32_t l = a.lo[k];
             const uint32_t h = a.hi[k];
             if (l == h) continue;
-            if (q == l || q == h) {
+            const int32_t s = nl.net_start[k];
+            if (R == kKraftwerk2) {
+                // movable other ends that are not the row's own cell
+                const auto other = [&](uint32_t t) {
+                    const int32_t v = nl.pin_var[s + static_cast<int32_t>(t)];
+                    return v >= 0 && v != i ? 1 : 0;
+                };
+                if (q == l || q == h) {
+                    const int32_t deg = nl.net_start[k + 1] - s;
+                    for (int32_t t = 0; t < deg; ++t)
+                        if (static_cast<uint32_t>(t) != q) cnt += other(static_cast<uint32_t>(t));
+                } else {
+                    cnt += other(l) + other(h);
+                }
+            } else if (q == l || q == h) {
                 cnt += nl.net_mov[k] - 1;  // every other movable pin of the net
             } else {
-                const int32_t s = nl.net_start[k];
                 cnt += (nl.pin_var[s + l] >= 0 ? 1 : 0) + (nl.pin_var[s + h] >= 0 ? 1 : 0);
             }
         }
@@ -275,6 +303,8 @@ __global__ void __launch_bounds__(1024)
 }
 
 // Row pointers from a block scan of the counts, then the row's entries.
+// Kraftwerk2: alpha < 0 leaves the right-hand side at zero (withRhs false).
+template <int R = kSimpl>
 __global__ void __launch_bounds__(kBuildThreads)
     k_fill(NetlistDev nl, AxisArgs ax, AxisArgs ay, int32_t blocks_per_axis, double alpha,
            const int32_t *__restrict__ row_cnt, const int64_t *__restrict__ block_first,
@@ -311,20 +341,30 @@ __global__ void __launch_bounds__(kBuildThreads)
     a.row_ptr[i] = static_cast<int32_t>(slot);
     double dg = 0.0;
     double rh = 0.0;
-    for_each_edge(nl, a.pos, a.fixed, a.off, a.lo, a.hi, a.floor_len, i,
-                  [&](int32_t var, double cp, double there, double own_offset, double w) {
-                      dg += w;
-                      if (var >= 0) {
-                          if (slot < cap) {
-                              a.col[slot] = var;
-                              a.val[slot] = -w;
-                          }
-                          ++slot;
-                          rh += w * ((there - cp) - own_offset);
-                      } else {
-                          rh += w * (there - own_offset);
-                      }
-                  });
+    for_each_edge<R>(nl, a.pos, a.fixed, a.off, a.lo, a.hi, a.floor_len, i,
+                     [&](int32_t var, double cp, double there, double own_offset, double w,
+                         double own_raw, double other_raw) {
+                         dg += w;
+                         if (var >= 0) {
+                             if (slot < cap) {
+                                 a.col[slot] = var;
+                                 a.val[slot] = -w;
+                             }
+                             ++slot;
+                             // Kraftwerk2: w * (otherOffset - ownOffset)
+                             rh += R == kKraftwerk2 ? w * (other_raw - own_raw)
+                                                    : w * ((there - cp) - own_offset);
+                         } else {
+                             // Kraftwerk2: w * (at[other] - ownOffset)
+                             rh += R == kKraftwerk2 ? w * (there - own_raw)
+                                                    : w * (there - own_offset);
+                         }
+                     });
+    if (R == kKraftwerk2) {
+        a.diag[i] = dg;
+        a.rhs[i] = alpha < 0.0 ? 0.0 : rh;
+        return;
+    }
     if (alpha > 0.0) {
         const double p = a.pos[i];
         const double w = alpha / ref_max(fabs(p - a.anchor[i]), a.floor_len);
@@ -335,17 +375,40 @@ __global__ void __launch_bounds__(kBuildThreads)
     a.rhs[i] = rh;
 }
 
-}  // namespace
+// Kraftwerk2's adjustments after buildSystem: diag += move_weight and
+// rhs = -move_weight * toward (kraftwerk2_placer.cc:716-721) when
+// move_weight is given, then diag = max(diag, floor) when floor > 0
+// (kraftwerk2_placer.cc:433-437).
+__global__ void k_kw2_adjust(int32_t n, double *dx, double *rx, double *dy, double *ry,
+                             const double *mw, const double *tx, const double *ty, double floor) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = dx[i], b = dy[i];
+    if (mw) {
+        a += mw[i];
+        b += mw[i];
+        rx[i] = -mw[i] * tx[i];
+        ry[i] = -mw[i] * ty[i];
+    }
+    if (floor > 0.0) {
+        a = ref_max(a, floor);
+        b = ref_max(b, floor);
+    }
+    dx[i] = a;
+    dy[i] = b;
+}
 
-int launch_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha,
-                     const double *ax, const double *ay, double floor_x, double floor_y) {
+
+template <int R>
+int launch_build(ktg_ctx *c, const double *x, const double *y, double alpha, const double *ax,
+                 const double *ay, double floor_x, double floor_y) {
     const NetlistDev nl = view_of(c);
     const int32_t n = static_cast<int32_t>(c->n);
     const int net_blocks = static_cast<int>((c->N + kBuildThreads - 1) / kBuildThreads);
     const int32_t bpa = static_cast<int32_t>((c->n + kBuildThreads - 1) / kBuildThreads);
     KTG_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
     if (c->N > 0) {
-        k_bound_pins<true><<<net_blocks, kBuildThreads, 0, c->stream>>>(
+        k_bound_pins<true, R><<<net_blocks, kBuildThreads, 0, c->stream>>>(
             nl, x, y, c->sys[0].lo, c->sys[0].hi, c->sys[1].lo, c->sys[1].hi, c->partials,
             c->counters + 0, c->scalars + 0);
         ++c->launches;
@@ -360,19 +423,46 @@ int launch_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha,
                            s.row_ptr, s.col, s.val, s.diag, s.rhs};
     }
     if (n > 0) {
-        k_row_count<<<2 * bpa, kBuildThreads, 0, c->stream>>>(nl, a[0], a[1], bpa, c->row_cnt,
-                                                              c->block_sum);
+        k_row_count<R><<<2 * bpa, kBuildThreads, 0, c->stream>>>(nl, a[0], a[1], bpa,
+                                                                 c->row_cnt, c->block_sum);
         k_scan_blocks<<<1, 1024, 0, c->stream>>>(c->block_sum, bpa, n, c->cap_nnz,
                                                  c->sys[0].row_ptr, c->sys[1].row_ptr,
                                                  c->nnz_dev, c->status);
-        k_fill<<<2 * bpa, kBuildThreads, 0, c->stream>>>(nl, a[0], a[1], bpa, alpha, c->row_cnt,
-                                                         c->block_sum, c->cap_nnz, c->status);
+        k_fill<R><<<2 * bpa, kBuildThreads, 0, c->stream>>>(nl, a[0], a[1], bpa, alpha,
+                                                            c->row_cnt, c->block_sum, c->cap_nnz,
+                                                            c->status);
         c->launches += 3;
     } else {
         KTG_CUDA(c, cudaMemsetAsync(c->sys[0].row_ptr, 0, sizeof(int32_t), c->stream));
         KTG_CUDA(c, cudaMemsetAsync(c->sys[1].row_ptr, 0, sizeof(int32_t), c->stream));
         KTG_CUDA(c, cudaMemsetAsync(c->nnz_dev, 0, 2 * sizeof(int64_t), c->stream));
     }
+    KTG_CUDA(c, cudaGetLastError());
+    return KTG_OK;
+}
+
+}  // namespace
+
+int launch_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha,
+                     const double *ax, const double *ay, double floor_x, double floor_y) {
+    return launch_build<kSimpl>(c, x, y, alpha, ax, ay, floor_x, floor_y);
+}
+
+int launch_build_kraftwerk2(ktg_ctx *c, const double *x, const double *y, bool with_rhs,
+                            double floor_x, double floor_y) {
+    return launch_build<kKraftwerk2>(c, x, y, with_rhs ? 0.0 : -1.0, nullptr, nullptr, floor_x,
+                                     floor_y);
+}
+
+int launch_kraftwerk2_adjust(ktg_ctx *c, const double *move_weight, const double *toward_x,
+                             const double *toward_y, double diag_floor) {
+    const int32_t n = static_cast<int32_t>(c->sys_n);
+    if (n == 0) return KTG_OK;
+    k_kw2_adjust<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->sys[0].diag, c->sys[0].rhs,
+                                                        c->sys[1].diag, c->sys[1].rhs,
+                                                        move_weight, toward_x, toward_y,
+                                                        diag_floor);
+    ++c->launches;
     KTG_CUDA(c, cudaGetLastError());
     return KTG_OK;
 }

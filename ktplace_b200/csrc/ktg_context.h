@@ -123,6 +123,10 @@ namespace ktg {
 int launch_build_b2b(ktg_ctx *ctx, const double *x, const double *y, double alpha,
                      const double *ax, const double *ay, double floor_x, double floor_y);
 int launch_hpwl(ktg_ctx *ctx, const double *x, const double *y, double *out_dev);
+int launch_build_kraftwerk2(ktg_ctx *ctx, const double *x, const double *y, bool with_rhs,
+                            double floor_x, double floor_y);
+int launch_kraftwerk2_adjust(ktg_ctx *ctx, const double *move_weight, const double *toward_x,
+                             const double *toward_y, double diag_floor);
 int launch_solve(ktg_ctx *ctx, double *x, double *y, double tol, int64_t max_iter,
                  ktg_solve_info *info_dev, double *hist_x, double *hist_y, int64_t hist_cap);
 int launch_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ_dev,

@@ -110,6 +110,33 @@ class Context:
         self._check(self.lib.ktg_build_b2b(self.h, _ptr(x), _ptr(y), alpha, _ptr(ax), _ptr(ay),
                                            floor_x, floor_y))
 
+    def build_kraftwerk2(self, x, y, with_rhs: bool, floor_x: float, floor_y: float):
+        """Kraftwerk2's buildSystem for both axes (host mode)."""
+        self._set_mode(_lib.KTG_PTR_HOST)
+        x, y = _c(x, np.float64), _c(y, np.float64)
+        self._check(self.lib.ktg_build_b2b_kraftwerk2(self.h, _ptr(x), _ptr(y), int(with_rhs),
+                                                      floor_x, floor_y))
+
+    def build_kraftwerk2_dev(self, x, y, with_rhs: bool, floor_x: float, floor_y: float):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_build_b2b_kraftwerk2(self.h, _tptr(x), _tptr(y), int(with_rhs),
+                                                      floor_x, floor_y))
+
+    def kraftwerk2_adjust_dev(self, move_weight=None, toward_x=None, toward_y=None,
+                              diag_floor: float = 0.0):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_kraftwerk2_adjust(self.h, _tptr(move_weight), _tptr(toward_x),
+                                                   _tptr(toward_y), diag_floor))
+
+    def kraftwerk2_adjust(self, move_weight=None, toward_x=None, toward_y=None,
+                          diag_floor: float = 0.0):
+        self._set_mode(_lib.KTG_PTR_HOST)
+        mw = None if move_weight is None else _c(move_weight, np.float64)
+        tx = None if toward_x is None else _c(toward_x, np.float64)
+        ty = None if toward_y is None else _c(toward_y, np.float64)
+        self._check(self.lib.ktg_kraftwerk2_adjust(self.h, _ptr(mw), _ptr(tx), _ptr(ty),
+                                                   diag_floor))
+
     def build_b2b_dev(self, x, y, alpha, ax=None, ay=None, floor_x=1.0, floor_y=1.0):
         self._set_mode(_lib.KTG_PTR_DEVICE)
         self._check(self.lib.ktg_build_b2b(self.h, _tptr(x), _tptr(y), alpha, _tptr(ax),

@@ -73,8 +73,12 @@ class Netlist:
         return fx / n, fy / n
 
 
-def flatten(d: RawDesign) -> Netlist:
-    """Flatten a raw design the way SimPL's buildSimplDM does."""
+def flatten(d: RawDesign, kraftwerk2: bool = False) -> Netlist:
+    """Flatten a raw design the way SimPL's buildSimplDM does.
+
+    kraftwerk2=True keeps every pin in its listed order instead, duplicates
+    of a cell within a net included, as Kraftwerk2's collectNets does
+    (globalPlacer/kraftwerk2/kraftwerk2_dm.cc:34-54)."""
     V = d.num_vertices
     movable = ~d.fixed
     mov_vertex = np.nonzero(movable)[0].astype(np.int32)
@@ -87,12 +91,16 @@ def flatten(d: RawDesign) -> Netlist:
     net_of = np.repeat(np.arange(N, dtype=np.int64), deg_raw)
     P_raw = int(d.net_start[-1])
     # Stable sort by cell id within each net (lexsort keys: last is primary).
-    order = np.lexsort((np.arange(P_raw), d.pin_cell, net_of))
-    cells_sorted = d.pin_cell[order]
-    nets_sorted = net_of[order]
-    keep = np.ones(P_raw, dtype=bool)
-    keep[1:] = ~((nets_sorted[1:] == nets_sorted[:-1]) & (cells_sorted[1:] == cells_sorted[:-1]))
-    sel = order[keep]
+    if kraftwerk2:
+        sel = np.arange(P_raw)
+    else:
+        order = np.lexsort((np.arange(P_raw), d.pin_cell, net_of))
+        cells_sorted = d.pin_cell[order]
+        nets_sorted = net_of[order]
+        keep = np.ones(P_raw, dtype=bool)
+        keep[1:] = ~((nets_sorted[1:] == nets_sorted[:-1]) &
+                     (cells_sorted[1:] == cells_sorted[:-1]))
+        sel = order[keep]
     pin_cell = d.pin_cell[sel].astype(np.int32)
     pin_net_all = net_of[sel]
     # Lower-left relative offsets, as bookshelfToKTAdaptor.cc:430 forms them.

@@ -407,3 +407,71 @@ def port_overflow(occ, avail, density_limit: float, total_avail: float) -> float
 def port_dot(a, b) -> float:
     a, b = _c(a, np.float64), _c(b, np.float64)
     return float(load_port().kto_dot(a.shape[0], _p(a, _f64p), _p(b, _f64p)))
+
+
+class Kraftwerk2Ref:
+    """The reference's Kraftwerk2 buildSystem / solve on a Design filled from a
+    Netlist (oracle/ref_kraftwerk2.cc): movable cells as slots, each net's
+    pins as (slot or none, offset, fixedPosition = fixed position + offset)."""
+
+    def __init__(self, nl):
+        lib = load_ref("cpu")
+        if not hasattr(lib, "_kw2_ready"):
+            lib.kw2_create.argtypes = [ctypes.c_int64, _f64p, _f64p, ctypes.c_int64, _i64p, _i64p,
+                                       _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double]
+            lib.kw2_create.restype = _vp
+            lib.kw2_destroy.argtypes = [_vp]
+            lib.kw2_build.argtypes = [_vp, _f64p, _f64p, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double]
+            lib.kw2_build.restype = ctypes.c_int64
+            lib.kw2_get_system.argtypes = [_vp, _i64p, _i32p, _f64p, _f64p, _f64p]
+            lib.kw2_set_diag_rhs.argtypes = [_vp, _f64p, _f64p]
+            lib.kw2_solve.argtypes = [_vp, _f64p, ctypes.c_double, ctypes.c_int64]
+            lib._kw2_ready = True
+        self.lib = lib
+        self.n = nl.num_movable
+        slot = nl.var_of_vertex[nl.pin_cell].astype(np.int64)
+        fixed = slot < 0
+        fx = np.where(fixed, nl.fixed_x[nl.pin_cell] + nl.off_x, 0.0)
+        fy = np.where(fixed, nl.fixed_y[nl.pin_cell] + nl.off_y, 0.0)
+        k = dict(w=_c(nl.width, np.float64), h=_c(nl.height, np.float64),
+                 ns=_c(nl.net_start, np.int64), slot=_c(slot, np.int64),
+                 ox=_c(nl.off_x, np.float64), oy=_c(nl.off_y, np.float64),
+                 fx=_c(fx, np.float64), fy=_c(fy, np.float64),
+                 wt=_c(nl.net_weight, np.float64))
+        self._keep = k
+        lx, ly, ux, uy = nl.die
+        self.h = lib.kw2_create(self.n, _p(k["w"], _f64p), _p(k["h"], _f64p), nl.num_nets,
+                                _p(k["ns"], _i64p), _p(k["slot"], _i64p), _p(k["ox"], _f64p),
+                                _p(k["oy"], _f64p), _p(k["fx"], _f64p), _p(k["fy"], _f64p),
+                                _p(k["wt"], _f64p), lx, ly, ux, uy)
+        if not self.h:
+            raise RuntimeError("kw2_create failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.kw2_destroy(self.h)
+            self.h = None
+
+    def build(self, x, y, horizontal: bool, with_rhs: bool, floor_x: float, floor_y: float) -> dict:
+        x, y = _c(x, np.float64), _c(y, np.float64)
+        m = int(self.lib.kw2_build(self.h, _p(x, _f64p), _p(y, _f64p), int(horizontal),
+                                   int(with_rhs), floor_x, floor_y))
+        s = dict(row_ptr=np.zeros(self.n + 1, np.int64), col=np.zeros(max(m, 1), np.int32),
+                 val=np.zeros(max(m, 1)), diag=np.zeros(max(self.n, 1)),
+                 rhs=np.zeros(max(self.n, 1)))
+        self.lib.kw2_get_system(self.h, _p(s["row_ptr"], _i64p), _p(s["col"], _i32p),
+                                _p(s["val"], _f64p), _p(s["diag"], _f64p), _p(s["rhs"], _f64p))
+        s["col"], s["val"] = s["col"][:m], s["val"][:m]
+        s["diag"], s["rhs"] = s["diag"][:self.n], s["rhs"][:self.n]
+        return s
+
+    def set_diag_rhs(self, diag, rhs):
+        d, r = _c(diag, np.float64), _c(rhs, np.float64)
+        self.lib.kw2_set_diag_rhs(self.h, _p(d, _f64p), _p(r, _f64p))
+
+    def solve(self, x, tol: float, max_iter: int):
+        x = _c(x, np.float64).copy()
+        self.lib.kw2_solve(self.h, _p(x, _f64p), tol, max_iter)
+        return x
