@@ -336,6 +336,10 @@ def run_ours(args):
         kw2_line = kraftwerk2_leg(torch, dev, stream, raw, max(3, args.steps // 10),
                                   cpu=not args.no_cpu_baseline)
 
+    bs_line = None
+    if world == 1:
+        bs_line = bookshelf_leg(raw, cpu=not args.no_cpu_baseline)
+
     batch_line = None
     if world == 1 and not args.no_batch:
         batch_line = run_batch_leg(torch, dev, stream, max(3, args.steps // 10))
@@ -389,6 +393,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "batch": batch_line,
             "kraftwerk2": kw2_line,
+            "bookshelf": bs_line,
             "clocks": clk,
         }
         print(json.dumps(line))
@@ -539,6 +544,45 @@ def kraftwerk2_leg(torch, dev, stream, raw, reps: int, cpu: bool) -> dict:
             out["reference_cpu_ms"] = min(t)
             out["reference_cpu_cores"] = threads
             out["speedup_vs_reference"] = out["reference_cpu_ms"] / out["gpu_ms"]
+    return out
+
+
+def bookshelf_leg(raw, cpu: bool) -> dict:
+    """Load time of the 211k-cell workload written as a Bookshelf directory:
+    ktg_bookshelf_read (read + flatten, all host threads) beside the
+    reference's BookshelfInputAdapter + buildSimplDM (oracle/_ref, same
+    threads; it needs more than the default 8 MiB of main-thread stack at this
+    size, so the soft stack limit is raised first)."""
+    import resource
+    import tempfile
+    from ktplace_b200 import bookshelf, synth
+    threads = os.cpu_count() or 1
+    out = {"workload": "Bookshelf read + SimPL flattening of synth211k (nodes/nets/wts/pl/scl)",
+           "threads": threads}
+    with tempfile.TemporaryDirectory() as tmp:
+        d = os.path.join(tmp, raw.name)
+        synth.write_bookshelf(raw, d)
+        t = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            nl = bookshelf.read(d, threads)
+            t.append(1000.0 * (time.perf_counter() - t0))
+        out["ms"] = statistics.median(t)
+        out["phases_ms"] = nl.read_ms
+        if cpu:
+            import oracle
+            if oracle.ref_available():
+                try:
+                    resource.setrlimit(resource.RLIMIT_STACK,
+                                       (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+                except (ValueError, OSError):
+                    pass
+                oracle.set_ref_threads(threads)
+                t0 = time.perf_counter()
+                ref = oracle.RefDesign.from_bookshelf(d)
+                out["reference_ms"] = 1000.0 * (time.perf_counter() - t0)
+                out["speedup_vs_reference"] = out["reference_ms"] / out["ms"]
+                del ref
     return out
 
 

@@ -351,6 +351,34 @@ int64_t ktg_learned_launch_count(const ktg_learned *h);
  * Any of the three pointers may be NULL. Host memory. */
 int ktg_download_aggregates(ktg_ctx *ctx, int32_t *order, int32_t *meta, float *minv);
 
+/* ---- Bookshelf reader ----------------------------------------------------
+ * Reads a Bookshelf design directory <dir>/<name>.{nodes,wts,nets,pl,scl}
+ * (name = the directory's own name, ".gz" variants read through zlib) with
+ * the rules of BookshelfInputAdapter (adaptor/bookshelfToKTAdaptor.cc:137-672)
+ * and flattens it like buildSimplDM (globalPlacer/simpl/simpl_dm.cc:16-85,
+ * 262-279; die as getPlacementDieBox, datamodel/kt_die.cc:45-105). Host code;
+ * line parsing on `threads` host threads (0 = all). The netlist view points
+ * into the reader's arrays (valid until ktg_bookshelf_free) and goes straight
+ * to ktg_upload_netlist. Status codes as elsewhere; the message of a failed
+ * read is ktg_bookshelf_last_error() (per calling thread). */
+typedef struct ktg_bookshelf ktg_bookshelf;
+
+int ktg_bookshelf_read(const char *dir, int threads, ktg_bookshelf **out);
+void ktg_bookshelf_free(ktg_bookshelf *b);
+const char *ktg_bookshelf_last_error(void);
+/* sizes[9]: vertices, movable, nets, pins, movable pins, fixed cells,
+ * obstacles, rows, subrows. */
+int ktg_bookshelf_sizes(const ktg_bookshelf *b, int64_t *sizes);
+int ktg_bookshelf_view(const ktg_bookshelf *b, ktg_netlist_view *view);
+/* Wall milliseconds of the read's phases (the reference times each file the
+ * same way): ms[6] = nodes, wts, nets, pl, scl, flattening. */
+int ktg_bookshelf_times(const ktg_bookshelf *b, double *ms);
+/* die4 = (lx, ly, ux, uy); obstacles [K*4] (lx, ly, ux, uy) of the fixed
+ * cells with area; rows [R*5] (coordinate, height, pitch, first subrow's xlo,
+ * last subrow's xhi); subrows [S*3] (row index, xlo, xhi). NULL skips. */
+int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacles, double *rows,
+                           double *subrows);
+
 /* ---- tuning and introspection ------------------------------------------- */
 
 /* Sets a kernel-shape option of this context (no reference counterpart; the

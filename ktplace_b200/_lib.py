@@ -98,6 +98,13 @@ SIGNATURES = [
                                                  ctypes.POINTER(ctypes.c_int)]),
     ("ktg_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
     ("ktg_download_aggregates", ctypes.c_int, [_vp, _i32p, _i32p, _f32p]),
+    ("ktg_bookshelf_read", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ktg_bookshelf_free", None, [_vp]),
+    ("ktg_bookshelf_last_error", ctypes.c_char_p, []),
+    ("ktg_bookshelf_sizes", ctypes.c_int, [_vp, _i64p]),
+    ("ktg_bookshelf_view", ctypes.c_int, [_vp, ctypes.POINTER(NetlistView)]),
+    ("ktg_bookshelf_times", ctypes.c_int, [_vp, _f64p]),
+    ("ktg_bookshelf_geometry", ctypes.c_int, [_vp, _f64p, _f64p, _f64p, _f64p]),
     ("ktg_build_b2b_kraftwerk2", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_double,
                                                 ctypes.c_double]),
     ("ktg_kraftwerk2_adjust", ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double]),
