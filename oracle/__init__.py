@@ -222,6 +222,37 @@ class RefDesign:
         return dict(origin=(info[0], info[1]), dx=info[2], dy=info[3], nx=nx, ny=ny,
                     total_avail=info[6], avail=avail)
 
+    def lal(self, x, y):
+        """The reference's look-ahead legalization on the grid of the last
+        grid() call; returns the new (x, y)."""
+        lib = self.lib
+        if not hasattr(lib, "_lal_ready"):
+            lib.ref_lal.argtypes = [_vp, _f64p, _f64p]
+            lib.ref_lal.restype = ctypes.c_int
+            lib.ref_free_space.argtypes = [_vp, _u64p, _f64p, _u64p, _f64p]
+            lib.ref_free_space.restype = ctypes.c_int
+            lib._lal_ready = True
+        x, y = _c(x, np.float64).copy(), _c(y, np.float64).copy()
+        self._check(lib.ref_lal(self.h, _p(x, _f64p), _p(y, _f64p)))
+        return x, y
+
+    def free_space(self):
+        """FreeSpace rows of the last grid() call: rows [R, 2] (y0, y1),
+        row_span [R + 1], spans [S, 2] (x0, x1)."""
+        self.lal.__func__  # argtypes are set up by lal()
+        lib = self.lib
+        if not hasattr(lib, "_lal_ready"):
+            self.lal(np.zeros(self.n), np.zeros(self.n))
+        counts = np.zeros(2, np.uint64)
+        self._check(lib.ref_free_space(self.h, _p(counts, _u64p), None, None, None))
+        R, S = int(counts[0]), int(counts[1])
+        rows = np.zeros((max(R, 1), 2))
+        rs = np.zeros(R + 1, np.uint64)
+        spans = np.zeros((max(S, 1), 2))
+        self._check(lib.ref_free_space(self.h, _p(counts, _u64p), _p(rows, _f64p), _p(rs, _u64p),
+                                       _p(spans, _f64p)))
+        return rows[:R], rs.astype(np.int64), spans[:S]
+
     def occupancy_map(self, x, y, nbins: int):
         x, y = _c(x, np.float64), _c(y, np.float64)
         occ = np.zeros(nbins)

@@ -13,6 +13,9 @@
 //   * ref_occupancy   -> Impl::getOccupancy + getOverflow (simpl_placer.cc:282-297)
 //   * ref_grid        -> Impl::buildGrid            (simpl_placer.cc:190-224)
 //   * ref_floors      -> Impl::collect              (simpl_placer.cc:169-179)
+//   * ref_lal         -> Impl::lookAheadLegalize (simpl_placer.cc:299-310,
+//                        LookAheadLegalizer::legalize, simpl_lal.cc:43-123)
+//   * ref_free_space  -> the FreeSpace rows Impl::buildGrid made (simpl_grid.h:130-173)
 //   * ref_design_load_bookshelf -> BookshelfInputAdapter + buildSimplDM
 //     (adaptor/bookshelfToKTAdaptor.cc, simpl_dm.cc:16-85,262-279)
 //
@@ -69,6 +72,8 @@ struct GridTag { friend auto reach(GridTag); };
 struct FloorXTag { friend auto reach(FloorXTag); };
 struct FloorYTag { friend auto reach(FloorYTag); };
 struct DieTag { friend auto reach(DieTag); };
+struct LalTag { friend auto reach(LalTag); };
+struct FreeTag { friend auto reach(FreeTag); };
 
 }  // namespace
 
@@ -83,6 +88,8 @@ template struct Grant<GridTag, &simplPlacer::Impl::grid>;
 template struct Grant<FloorXTag, &simplPlacer::Impl::floorX>;
 template struct Grant<FloorYTag, &simplPlacer::Impl::floorY>;
 template struct Grant<DieTag, &simplPlacer::Impl::die>;
+template struct Grant<LalTag, &simplPlacer::Impl::lookAheadLegalize>;
+template struct Grant<FreeTag, &simplPlacer::Impl::freeSpace>;
 
 namespace {
 
@@ -469,6 +476,49 @@ int ref_run_simpl(void *hp, const double *opts, const char *initNet, double *x, 
         const Design &d = dm.getDesign();
         std::copy(d.x.begin(), d.x.end(), x);
         std::copy(d.y.begin(), d.y.end(), y);
+    });
+}
+
+// Impl::lookAheadLegalize on the grid of the last ref_grid (default
+// SimplOptions: maxLevel 20, minCellsToSplit 4, stripeAreaFraction 0.1), in
+// place on x, y.
+int ref_lal(void *hp, double *x, double *y) {
+    auto *h = static_cast<Handle *>(hp);
+    return guarded(h, [&] {
+        const std::size_t n = h->design.netlist.numMovable;
+        std::vector<double> vx(x, x + n), vy(y, y + n);
+        auto &im = h->impl();
+        (im.*reach(LalTag{}))(vx, vy);
+        std::copy(vx.begin(), vx.end(), x);
+        std::copy(vy.begin(), vy.end(), y);
+    });
+}
+
+// The FreeSpace rows of the last ref_grid: counts[0] = rows, counts[1] =
+// spans; rows [R*2] (y start, y end), row_span [R+1] offsets, spans [S*2].
+// Pointers may be null to query the counts.
+int ref_free_space(void *hp, uint64_t *counts, double *rows, uint64_t *row_span, double *spans) {
+    auto *h = static_cast<Handle *>(hp);
+    return guarded(h, [&] {
+        const FreeSpace &fs = h->impl().*reach(FreeTag{});
+        uint64_t s = 0;
+        for (std::size_t r = 0; r < fs.rows.size(); ++r) {
+            if (rows) {
+                rows[2 * r] = fs.rows[r].y.start;
+                rows[2 * r + 1] = fs.rows[r].y.end;
+            }
+            if (row_span) row_span[r] = s;
+            for (const Interval &sp : fs.rows[r].spans) {
+                if (spans) {
+                    spans[2 * s] = sp.start;
+                    spans[2 * s + 1] = sp.end;
+                }
+                ++s;
+            }
+        }
+        if (row_span) row_span[fs.rows.size()] = s;
+        counts[0] = fs.rows.size();
+        counts[1] = s;
     });
 }
 
