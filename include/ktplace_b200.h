@@ -247,6 +247,38 @@ int ktg_set_grid(ktg_ctx *ctx, const ktg_grid_view *grid);
 int ktg_occupancy(ktg_ctx *ctx, const double *x, const double *y, double *occ,
                   double *overflow);
 
+/* ---- look-ahead legalization ---------------------------------------------- */
+
+/* Installs the free space, obstacles and die of LookAheadLegalizer
+ * (globalPlacer/simpl/simpl_lal.h; FreeSpace of simpl_grid.h:130-232), host
+ * memory, copied:
+ *   row_y     [2*num_rows]  per row y start, y end; rows sorted by y start
+ *   row_span  [num_rows+1]  row r's free spans are spans[row_span[r] ..
+ *                           row_span[r+1]), row_span[0] = 0
+ *   spans     [2*S]         x start, x end (spans already cut by the
+ *                           obstacles, as FreeSpace::build leaves them)
+ *   obstacles [4*num_obstacles]  lx ly ux uy of the fixed blocks
+ *   die       [4]           lx ly ux uy
+ * KTG_ERR_ARG on unsorted rows or a row_span that is not ascending. */
+int ktg_set_free_space(ktg_ctx *ctx, int64_t num_rows, const double *row_y,
+                       const int64_t *row_span, const double *spans, int64_t num_obstacles,
+                       const double *obstacles, const double *die);
+
+/* LookAheadLegalizer::legalize (globalPlacer/simpl/simpl_lal.cc:43-121, with
+ * split :213-264, getStripes :266-312, nonlinearScale :314-363 and
+ * clampToDie :365-372) in place
+ * on x, y: overfilled clusters of the installed grid (ktg_set_grid, whose
+ * density limit it uses) grown and legalized in batches by recursive
+ * bisection with free-space-aware cutlines and stripe scaling, then clamped
+ * to the die. Options as in simpl_options.h:24-26: maxLevel,
+ * minCellsToSplit, stripeAreaFraction (defaults 20, 4, 0.1).
+ * Positions are bit-identical to the reference when the cell areas are
+ * multiples of 2^-s (s the occupancy's fixed-point shift; integer site
+ * areas qualify): the bin occupancies it grows clusters from are exact then.
+ * The cluster/grow/batch loop runs on the host between batches. */
+int ktg_lal(ktg_ctx *ctx, double *x, double *y, int32_t max_level, int32_t min_cells_to_split,
+            double stripe_area_fraction);
+
 /* ---- batched solves ---------------------------------------------------------- */
 
 /* Many independent systems (the x and y systems of many netlists, of uneven

@@ -239,6 +239,7 @@ void ktg_destroy(ktg_ctx *c) {
     free_netlist(c);
     free_systems(c);
     ktg::free_agg(c);
+    ktg::free_lal(c);
     dev_free(c->partials);
     dev_free(c->counters);
     dev_free(c->status);
@@ -832,6 +833,9 @@ int ktg_set_grid(ktg_ctx *c, const ktg_grid_view *g) {
     if ((rc = reserve_partials(c, (bins + 255) / 256 + 64))) return rc;
     KTG_CUDA(c, cudaMemsetAsync(c->occ_fx, 0, sizeof(unsigned long long) * bins, c->stream));
     if ((rc = upload(c, c->avail, g->avail, bins))) return rc;
+    c->avail_host.resize(static_cast<size_t>(bins));
+    KTG_CUDA(c, cudaMemcpyAsync(c->avail_host.data(), c->avail, sizeof(double) * bins,
+                                cudaMemcpyDeviceToHost, c->stream));
     if ((rc = sync(c))) return rc;
     c->nx = g->nx;
     c->ny = g->ny;
@@ -866,6 +870,63 @@ int ktg_occupancy(ktg_ctx *c, const double *x, const double *y, double *occ, dou
                                 cudaMemcpyDeviceToHost, c->stream));
     if ((rc = sync(c))) return rc;
     *overflow = c->h_scalars[2];
+    return KTG_OK;
+}
+
+int ktg_set_free_space(ktg_ctx *c, int64_t num_rows, const double *row_y,
+                       const int64_t *row_span, const double *spans, int64_t num_obstacles,
+                       const double *obstacles, const double *die) {
+    if (!c || !die || num_rows < 0 || num_obstacles < 0) return KTG_ERR_ARG;
+    if (num_rows > 0 && (!row_y || !row_span)) return set_error(c, KTG_ERR_ARG, "null rows");
+    if (num_obstacles > 0 && !obstacles) return set_error(c, KTG_ERR_ARG, "null obstacles");
+    if (num_rows > 0x7fffffffll || num_obstacles > 0x7fffffffll)
+        return set_error(c, KTG_ERR_RANGE, "free space exceeds 32-bit indices");
+    const int64_t zero = 0;
+    const int64_t *rs = num_rows > 0 ? row_span : &zero;
+    if (rs[0] != 0) return set_error(c, KTG_ERR_ARG, "row_span[0] must be 0");
+    for (int64_t r = 0; r < num_rows; ++r) {
+        if (rs[r + 1] < rs[r]) return set_error(c, KTG_ERR_ARG, "row_span not ascending");
+        if (r > 0 && row_y[2 * r] < row_y[2 * r - 2])
+            return set_error(c, KTG_ERR_ARG, "rows not sorted by their bottom edge");
+    }
+    if (rs[num_rows] > 0 && !spans) return set_error(c, KTG_ERR_ARG, "null spans");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = sync(c))) return rc;
+    if ((rc = ktg::set_free_space(c, num_rows, row_y, rs, spans, num_obstacles, obstacles, die)))
+        return rc;
+    c->have_free_space = true;
+    return KTG_OK;
+}
+
+int ktg_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_cells_to_split,
+            double stripe_area_fraction) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_netlist) return set_error(c, KTG_ERR_STATE, "no netlist uploaded");
+    if (!c->have_grid) return set_error(c, KTG_ERR_STATE, "no grid installed");
+    if (!c->have_free_space) return set_error(c, KTG_ERR_STATE, "no free space installed");
+    if (c->n > 0 && (!x || !y)) return set_error(c, KTG_ERR_ARG, "null positions");
+    if (max_level < 1 || min_cells_to_split < 0 || !(stripe_area_fraction > 0.0))
+        return set_error(c, KTG_ERR_ARG, "bad legalization options");
+    int rc = set_device(c);
+    if (rc) return rc;
+    double *dx = x, *dy = y;
+    if (c->ptr_mode == KTG_PTR_HOST) {
+        if ((rc = reserve_systems(c, c->n, 0))) return rc;
+        if ((rc = upload(c, c->x, x, c->n))) return rc;
+        if ((rc = upload(c, c->y, y, c->n))) return rc;
+        dx = c->x;
+        dy = c->y;
+    }
+    if ((rc = ktg::launch_lal(c, dx, dy, max_level, min_cells_to_split, stripe_area_fraction)))
+        return rc;
+    if (c->ptr_mode == KTG_PTR_HOST && c->n > 0) {
+        KTG_CUDA(c, cudaMemcpyAsync(x, dx, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+        KTG_CUDA(c, cudaMemcpyAsync(y, dy, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    const int st = device_status(c);
+    if (st < 0) return st;
+    if (st != 0) return set_error(c, st, "legalization stripes exceed their capacity");
     return KTG_OK;
 }
 

@@ -16,12 +16,14 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "ktplace_b200.h"
 
 namespace ktg {
 
 struct AggState;  // aggregation preconditioner buffers (ktg_agg.cu)
+struct LalState;  // free space and scratch of the look-ahead legalizer (ktg_lal.cu)
 
 struct AxisSystem {
     int32_t *row_ptr = nullptr;  // [n+1]
@@ -111,9 +113,14 @@ struct ktg_ctx {
     int64_t nx = 0, ny = 0;
     double origin_x = 0, origin_y = 0, dx = 1, dy = 1, total_avail = 0, density_limit = 1;
     double *avail = nullptr;         // [bins]
+    std::vector<double> avail_host;  // [bins] host copy (the legalizer's cluster loop)
     unsigned long long *occ_fx = nullptr;  // [bins] two's-complement fixed point
     double *occ = nullptr;           // [bins] staging for host mode
     int64_t bins_cap = 0;
+
+    // look-ahead legalization
+    ktg::LalState *lal = nullptr;
+    bool have_free_space = false;
 };
 
 namespace ktg {
@@ -144,6 +151,14 @@ int agg_prepare_solve(ktg_ctx *ctx, int grid, const double *x, const double *y, 
 int agg_finish_solve(ktg_ctx *ctx, double *x, double *y);
 double *agg_global_slices(ktg_ctx *ctx, int64_t doubles);
 void free_agg(ktg_ctx *ctx);
+
+// Look-ahead legalization (ktg_lal.cu): free space (host arrays) and the
+// legalizer on device positions.
+int set_free_space(ktg_ctx *ctx, int64_t nrows, const double *row_y, const int64_t *row_span,
+                   const double *spans, int64_t nobst, const double *obst, const double *die4);
+int launch_lal(ktg_ctx *ctx, double *x, double *y, int32_t max_level, int32_t min_cells,
+               double stripe_fraction);
+void free_lal(ktg_ctx *ctx);
 
 int set_error(ktg_ctx *ctx, int code, const std::string &msg);
 int cuda_check(ktg_ctx *ctx, cudaError_t e, const char *what);

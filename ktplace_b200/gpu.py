@@ -300,6 +300,33 @@ class Context:
         self._check(self.lib.ktg_occupancy(self.h, _tptr(x), _tptr(y), _tptr(occ),
                                            _tptr(overflow)))
 
+    def set_free_space(self, fs):
+        """Installs a ``grid.FreeSpace`` (rows, spans, obstacles, die) for
+        ``lal``."""
+        self._fs = (_c(fs.row_y, np.float64), _c(fs.row_span, np.int64),
+                    _c(fs.spans, np.float64), _c(fs.obstacles, np.float64),
+                    _c(np.asarray(fs.die, np.float64), np.float64))
+        ry, rs, sp, ob, die = self._fs
+        self._check(self.lib.ktg_set_free_space(self.h, ry.shape[0], _ptr(ry), _ptr(rs), _ptr(sp),
+                                                ob.shape[0], _ptr(ob), _ptr(die)))
+
+    def lal(self, x, y, max_level: int = 20, min_cells_to_split: int = 4,
+            stripe_area_fraction: float = 0.1):
+        """LookAheadLegalizer::legalize on host positions; returns new (x, y)."""
+        self._set_mode(_lib.KTG_PTR_HOST)
+        x = _c(x, np.float64).copy()
+        y = _c(y, np.float64).copy()
+        self._check(self.lib.ktg_lal(self.h, _ptr(x), _ptr(y), max_level, min_cells_to_split,
+                                     stripe_area_fraction))
+        return x, y
+
+    def lal_dev(self, x, y, max_level: int = 20, min_cells_to_split: int = 4,
+                stripe_area_fraction: float = 0.1):
+        """In place on device tensors x, y."""
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_lal(self.h, _tptr(x), _tptr(y), max_level, min_cells_to_split,
+                                     stripe_area_fraction))
+
 
 class Batch:
     """Owns a ``ktg_batch``: many independent systems solved in one

@@ -85,6 +85,30 @@ def free_spans(rows: np.ndarray, obstacles: np.ndarray):
     return out, smallest
 
 
+@dataclasses.dataclass
+class FreeSpace:
+    """FreeSpace (simpl_grid.h:130-177) flattened for ktg_set_free_space:
+    row r spans y in row_y[r] and holds spans[row_span[r]:row_span[r+1]]."""
+    row_y: np.ndarray       # [R, 2] y start, y end (sorted by y start)
+    row_span: np.ndarray    # [R + 1] int64
+    spans: np.ndarray       # [S, 2] x start, x end
+    obstacles: np.ndarray   # [K, 4] lx ly ux uy
+    die: tuple
+
+
+def build_free_space(nl) -> FreeSpace:
+    """The free space LookAheadLegalizer works in: the design's rows cut by its
+    obstacles (free_spans), the same obstacles and the die."""
+    rows, _ = free_spans(nl.rows, nl.obstacles)
+    row_y = np.array([(r[0], r[1]) for r in rows], np.float64).reshape(-1, 2)
+    counts = np.array([len(r[2]) for r in rows], np.int64)
+    row_span = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    spans = np.array([sp for r in rows for sp in r[2]], np.float64).reshape(-1, 2)
+    obst = np.asarray(nl.obstacles, np.float64).reshape(-1, 4)
+    return FreeSpace(row_y=row_y, row_span=row_span, spans=spans, obstacles=obst,
+                     die=tuple(float(v) for v in nl.die))
+
+
 def build_grid(nl, per_axis: int, density_limit: float = 1.0) -> BinGrid:
     lx, ly, ux, uy = nl.die
     nx = ny = int(per_axis)

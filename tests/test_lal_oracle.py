@@ -8,7 +8,7 @@ import pytest
 
 import oracle
 from oracle import lal_ref
-from ktplace_b200 import synth, netlist
+from ktplace_b200 import grid, netlist, synth
 
 pytestmark = pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
 
@@ -38,3 +38,43 @@ def test_restatement_matches_reference(seed, cells, macros, bins):
         assert np.array_equal(np.array(px), rx)
         assert np.array_equal(np.array(py), ry)
         assert np.mean(rx != x) > 0.1  # legalization did move cells
+
+
+def _clustered(raw, n, seed, spread):
+    rng = np.random.default_rng(seed)
+    lx, ly, ux, uy = raw.die
+    return (0.5 * (lx + ux) + spread * (ux - lx) * rng.standard_normal(n),
+            0.5 * (ly + uy) + spread * (uy - ly) * rng.standard_normal(n))
+
+
+@pytest.mark.parametrize("seed,cells,macros,bins,density", [(5, 900, 4, 24, 1.0), (9, 700, 2, 12, 0.9),
+                                                            (7, 600, 0, 8, 0.8)])
+def test_restatement_clustered_and_density(seed, cells, macros, bins, density):
+    """Cells started in a tight cluster (one region, deep bisection) and
+    density limits below 1, on the host free space the GPU path installs."""
+    raw = synth.generate(synth.spec_tiny(seed=seed, macros=macros, cells=cells, nets=cells + 30))
+    nl = netlist.flatten(raw)
+    x, y = _clustered(raw, nl.num_movable, seed + 10, 0.08)
+    ref = oracle.RefDesign.from_netlist(nl)
+    g = ref.grid(bins, density)
+    rx, ry = ref.lal(x, y)
+    fs = grid.build_free_space(nl)
+    L = lal_ref.LAL(nl.width, nl.height, g, lal_ref.free_rows(fs.row_y, fs.row_span, fs.spans),
+                    fs.obstacles, fs.die, density)
+    px, py = L.legalize(x, y)
+    assert np.array_equal(np.array(px), rx) and np.array_equal(np.array(py), ry)
+
+
+@pytest.mark.parametrize("seed,cells,macros", [(2, 400, 3), (5, 900, 4), (7, 600, 0)])
+def test_host_free_space_matches_reference(seed, cells, macros):
+    """grid.build_free_space (what ktg_set_free_space receives) equals the
+    reference's FreeSpace rows and spans."""
+    raw = synth.generate(synth.spec_tiny(seed=seed, macros=macros, cells=cells, nets=cells + 30))
+    nl = netlist.flatten(raw)
+    ref = oracle.RefDesign.from_netlist(nl)
+    ref.grid(16, 1.0)
+    rows, rs, spans = ref.free_space()
+    fs = grid.build_free_space(nl)
+    assert np.array_equal(rows, fs.row_y)
+    assert np.array_equal(rs, fs.row_span)
+    assert np.array_equal(spans, fs.spans)
