@@ -340,6 +340,11 @@ def run_ours(args):
     if world == 1:
         bs_line = bookshelf_leg(raw, cpu=not args.no_cpu_baseline)
 
+    lal_line = None
+    if world == 1:
+        lal_line = lal_leg(torch, dev, stream, nl, wx.cpu().numpy(), wy.cpu().numpy(),
+                           max(3, args.steps // 10), cpu=not args.no_cpu_baseline)
+
     batch_line = None
     if world == 1 and not args.no_batch:
         batch_line = run_batch_leg(torch, dev, stream, max(3, args.steps // 10))
@@ -394,6 +399,7 @@ def run_ours(args):
             "batch": batch_line,
             "kraftwerk2": kw2_line,
             "bookshelf": bs_line,
+            "lal": lal_line,
             "clocks": clk,
         }
         print(json.dumps(line))
@@ -544,6 +550,81 @@ def kraftwerk2_leg(torch, dev, stream, raw, reps: int, cpu: bool) -> dict:
             out["reference_cpu_ms"] = min(t)
             out["reference_cpu_cores"] = threads
             out["speedup_vs_reference"] = out["reference_cpu_ms"] / out["gpu_ms"]
+    return out
+
+
+def lal_leg(torch, dev, stream, nl, x0, y0, reps: int, cpu: bool) -> dict:
+    """SimPL's look-ahead legalization (LookAheadLegalizer::legalize,
+    simpl_lal.cc:43-123) of the bench step's solved positions on the 211k-cell
+    netlist, SimPL's default grid (getDefaultBinsPerAxis) at density 1.0 and
+    the default options (20 levels, 4 cells, stripe fraction 0.1). GPU:
+    ktg_lal on device positions (host wall clock around the call, which ends
+    synchronised) and through the host-pointer C ABI (copies included).
+    Beside it, the reference's own legalizer (oracle/_ref) on all host cores,
+    with a bit-identity check of the two results."""
+    from ktplace_b200 import grid
+    from ktplace_b200.gpu import Context
+    bins = grid.default_bins_per_axis(nl.num_movable)
+    g = grid.build_grid(nl, bins, 1.0)
+    fs = grid.build_free_space(nl)
+    ctx = Context(dev.index or 0)
+    ctx.upload_netlist(nl)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_grid(g)
+    ctx.set_free_space(fs)
+    with torch.cuda.stream(stream):
+        bx = torch.tensor(x0, device=dev)
+        by = torch.tensor(y0, device=dev)
+        wx = torch.empty_like(bx)
+        wy = torch.empty_like(by)
+    ms, e2e = [], []
+    for k in range(reps + 1):
+        with torch.cuda.stream(stream):
+            wx.copy_(bx)
+            wy.copy_(by)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        ctx.lal_dev(wx, wy)
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        if k > 0:
+            ms.append(1000.0 * (t1 - t0))
+    stats = ctx.lal_stats()
+    for k in range(reps):
+        t0 = time.perf_counter()
+        gx, gy = ctx.lal(x0, y0)
+        e2e.append(1000.0 * (time.perf_counter() - t0))
+    out = {"workload": f"look-ahead legalization of the bench step's solved positions on "
+                       f"synth211k, {bins}x{bins} bins, density 1.0, options 20/4/0.1",
+           "gpu_ms": statistics.median(ms), "e2e_ms": statistics.median(e2e),
+           "h2d_bytes": 16 * nl.num_movable, "d2h_bytes": 16 * nl.num_movable,
+           "moved_fraction": float(np.mean((gx != x0) | (gy != y0))),
+           "batches": int(stats["batches"]), "regions": int(stats["regions"]),
+           "host_syncs": int(stats["syncs"])}
+    ctx.close()
+    if cpu:
+        import oracle
+        if oracle.ref_available():
+            import resource
+            try:  # the reference's recursion wants more than the default 8 MiB stack
+                resource.setrlimit(resource.RLIMIT_STACK,
+                                   (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+            except (ValueError, OSError):
+                pass
+            threads = os.cpu_count() or 1
+            oracle.set_ref_threads(threads)
+            ref = oracle.RefDesign.from_netlist(nl)
+            ref.grid(bins, 1.0)
+            t = []
+            for k in range(3):
+                t0 = time.perf_counter()
+                rx, ry = ref.lal(x0, y0)
+                t.append(1000.0 * (time.perf_counter() - t0))
+            out["reference_cpu_ms"] = min(t)
+            out["reference_cpu_cores"] = threads
+            out["bit_identical"] = bool(np.array_equal(rx, gx) and np.array_equal(ry, gy))
+            out["speedup_vs_reference"] = out["reference_cpu_ms"] / out["gpu_ms"]
+            out["e2e_speedup_vs_reference"] = out["reference_cpu_ms"] / out["e2e_ms"]
     return out
 
 

@@ -422,12 +422,30 @@ int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacl
  *                2: aggregation block-Jacobi, in ktg_solve_mixed
  *   "mixed_form" 1 (default): Chronopoulos-Gear mixed solve with per-block
  *                shared-memory slices; 0: textbook mixed solve
+ *   "lal_subtree_cells"  ktg_lal: blocks of at most this many cells (0 to
+ *                2048, default 2048) finish their bisection in one CTA;
+ *                larger ones go level by level (0: always level by level).
+ *                Results are identical either way.
+ *   "lal_exact_sums"  ktg_lal: 1 (default) reads the area sums of split and
+ *                nonlinearScale off integer prefix sums when every cell area
+ *                is a multiple of 2^-q with the total below 2^52 (so the
+ *                reference's sequential double sums are exact); 0 always
+ *                sums sequentially in the reference's order.
  * Returns KTG_ERR_ARG for an unknown key or value. */
 int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
 
 /* Number of kernels this context has launched since creation (all entry
  * points). */
 int64_t ktg_launch_count(const ktg_ctx *ctx);
+
+/* Counters of the last ktg_lal call, up to `count` (at most 12) of:
+ * batches, regions, bisection rounds (one-CTA launches and level-by-level
+ * levels, summed over batches), host synchronisations, blocks (summed over
+ * rounds), ms in the batches' bisection, ms in the occupancy refreshes, ms
+ * in total, ms in the one-CTA subtree launches, level-by-level levels,
+ * one-CTA blocks, one-CTA blocks handed back (host wall clock). No
+ * reference counterpart. */
+int ktg_lal_stats(ktg_ctx *ctx, double *out, int32_t count);
 
 /* Test of the bounded device waits: a cooperative launch in which one block
  * never arrives at a grid barrier, so the other's wait gives up after

@@ -96,6 +96,7 @@ SIGNATURES = [
     ("ktg_set_free_space", ctypes.c_int, [_vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int64,
                                           _vp, _vp]),
     ("ktg_lal", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double]),
+    ("ktg_lal_stats", ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     ("ktg_launch_count", ctypes.c_int64, [_vp]),
     ("ktg_selftest_wait_timeout", ctypes.c_int, [_vp, ctypes.c_int64,
                                                  ctypes.POINTER(ctypes.c_int)]),

@@ -301,6 +301,17 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         c->pcg_form = static_cast<int>(value);
         return KTG_OK;
     }
+    if (k == "lal_subtree_cells") {
+        if (value < 0 || value > 2048)
+            return set_error(c, KTG_ERR_ARG, "lal_subtree_cells must be in [0, 2048]");
+        c->lal_subtree_cells = static_cast<int>(value);
+        return KTG_OK;
+    }
+    if (k == "lal_exact_sums") {
+        if (value != 0 && value != 1) return set_error(c, KTG_ERR_ARG, "lal_exact_sums must be 0 or 1");
+        c->lal_exact_sums = static_cast<int>(value);
+        return KTG_OK;
+    }
     return set_error(c, KTG_ERR_ARG, "unknown option " + k);
 }
 
@@ -383,6 +394,24 @@ int ktg_upload_netlist(ktg_ctx *c, const ktg_netlist_view *nl) {
     if (total_area > 0.0) s = std::min(60, 61 - static_cast<int>(std::ceil(std::log2(total_area + 1.0))));
     s = std::max(s, 0);
     c->fx_scale = std::ldexp(1.0, s);
+    // Exact-sum shift of the legalizer: the least q with every area * 2^q an
+    // integer and the total * 2^q below 2^52, so that every partial sum of
+    // areas, in any order, is exact in double (-1: no such q).
+    {
+        int q = 0;  // the lowest set bit of every area's significand sets q
+        bool ok = true;
+        for (int64_t i = 0; ok && i < n; ++i) {
+            const double a = area[i];
+            if (!(a >= 0.0) || !std::isfinite(a)) ok = false;
+            if (!ok || a == 0.0) continue;
+            int e;
+            const double f = std::frexp(a, &e);  // a = f * 2^e, f in [0.5, 1)
+            const auto m = static_cast<uint64_t>(std::ldexp(f, 53));
+            const int low_bit = e - 53 + __builtin_ctzll(m);
+            q = std::max(q, -low_bit);
+        }
+        c->area_shift = ok && q <= 60 && std::ldexp(total_area, q) < 4503599627370496.0 ? q : -1;
+    }
 
     KTG_CUDA(c, cudaStreamSynchronize(c->stream));
     free_netlist(c);
@@ -928,6 +957,11 @@ int ktg_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_cel
     if (st < 0) return st;
     if (st != 0) return set_error(c, st, "legalization stripes exceed their capacity");
     return KTG_OK;
+}
+
+int ktg_lal_stats(ktg_ctx *c, double *out, int32_t count) {
+    if (!c || !out || count < 0) return KTG_ERR_ARG;
+    return ktg::lal_stats(c, out, count);
 }
 
 }  // extern "C"

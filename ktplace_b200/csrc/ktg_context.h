@@ -61,6 +61,7 @@ struct ktg_ctx {
     int64_t V = 0, n = 0, N = 0, P = 0, Pm = 0;
     int64_t cap_nnz = 0;  // col/val capacity per axis (upper bound on nnz)
     double fx_scale = 1.0;
+    int area_shift = -1;  // areas are multiples of 2^-area_shift with exact sums (-1: not)
 
     // netlist arrays
     int32_t *var_of_vertex = nullptr;
@@ -121,6 +122,8 @@ struct ktg_ctx {
     // look-ahead legalization
     ktg::LalState *lal = nullptr;
     bool have_free_space = false;
+    int lal_subtree_cells = 2048;  // blocks up to this many cells finish in one CTA
+    int lal_exact_sums = 1;        // area sums from integer prefixes when exact
 };
 
 namespace ktg {
@@ -159,6 +162,7 @@ int set_free_space(ktg_ctx *ctx, int64_t nrows, const double *row_y, const int64
 int launch_lal(ktg_ctx *ctx, double *x, double *y, int32_t max_level, int32_t min_cells,
                double stripe_fraction);
 void free_lal(ktg_ctx *ctx);
+int lal_stats(ktg_ctx *ctx, double *out, int count);
 
 int set_error(ktg_ctx *ctx, int code, const std::string &msg);
 int cuda_check(ktg_ctx *ctx, cudaError_t e, const char *what);

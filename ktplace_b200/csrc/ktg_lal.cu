@@ -37,6 +37,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <limits>
 #include <vector>
@@ -238,22 +239,58 @@ __device__ __forceinline__ void profile_bound(const Free &F, const double *box, 
     edges = (vertical ? 2 * sp : 2 * static_cast<int64_t>(r1 - r0)) + 2;
 }
 
-// Vertical profile steps of `box` (unsorted), returns the count.
-__device__ int64_t profile_steps(const Free &F, const double *box, Key *out) {
+// Vertical profile steps of `box` (unsorted), handed to sink(at, dh) in
+// row and span order; returns the count.
+// First span of row r ending after x (spans of a row ascend and are
+// disjoint, FreeSpace::build).
+__device__ __forceinline__ int64_t first_span(const Free &F, int32_t r, double x) {
+    int64_t lo = F.rowspan[r], hi = F.rowspan[r + 1];
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (F.spans[2 * mid + 1] > x) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// Vertical profile steps of `box` (unsorted), handed to sink(at, dh) in
+// row and span order; returns the count. Only spans overlapping the box's x
+// range can give a step (z > a), so each row starts at its first such span.
+template <typename Sink>
+__device__ int64_t emit_steps(const Free &F, const double *box, Sink sink) {
     const double lx = box[0], ly = box[1], ux = box[2], uy = box[3];
     int64_t k = 0;
     for (int32_t r = first_row(F, ly); r < F.R && F.rowy[2 * r] < uy; ++r) {
         const double h = ref_min(uy, F.rowy[2 * r + 1]) - ref_max(ly, F.rowy[2 * r]);
-        for (int64_t s = F.rowspan[r]; s < F.rowspan[r + 1]; ++s) {
+        if (!(h > 0.0)) continue;
+        const int64_t end = F.rowspan[r + 1];
+        for (int64_t s = first_span(F, r, lx); s < end && F.spans[2 * s] < ux; ++s) {
             const double a = ref_max(F.spans[2 * s], lx);
             const double z = ref_min(F.spans[2 * s + 1], ux);
-            if (h > 0.0 && z > a) {
-                out[k++] = Key{ord(a), ord(h)};
-                out[k++] = Key{ord(z), ord(-h)};
+            if (z > a) {
+                sink(k, a, h);
+                sink(k + 1, z, -h);
+                k += 2;
             }
         }
     }
     return k;
+}
+
+__device__ int64_t profile_steps(const Free &F, const double *box, Key *out) {
+    return emit_steps(F, box, [&](int64_t k, double at, double dh) { out[k] = Key{ord(at), ord(dh)}; });
+}
+
+__device__ int64_t count_steps(const Free &F, const double *box) {
+    return emit_steps(F, box, [](int64_t, double, double) {});
+}
+
+// Rows overlapping `box` (the horizontal profile's extent).
+__device__ __forceinline__ int32_t count_rows(const Free &F, const double *box) {
+    const int32_t r0 = first_row(F, box[1]);
+    int32_t r1 = r0;
+    while (r1 < F.R && F.rowy[2 * r1] < box[3]) ++r1;
+    return r1 - r0;
 }
 
 // AxisProfile (simpl_grid.h:29-65, getProfile :179-232) stored as edges /
@@ -293,10 +330,12 @@ struct Prof {
     }
 };
 
-// Builds the profile of `box` into e/p from its sorted steps (vertical) or
-// the rows (horizontal); returns the number of edges.
-__device__ int64_t build_profile(const Free &F, const double *box, bool vertical, const Key *steps,
-                                 int64_t nsteps, double *e, double *p) {
+// Builds the profile of `box` into e/p from its sorted steps (vertical;
+// step(k, at, dh) reads the k-th) or the rows (horizontal); returns the
+// number of edges.
+template <typename Step>
+__device__ int64_t build_profile_from(const Free &F, const double *box, bool vertical, Step step,
+                                      int64_t nsteps, double *e, double *p) {
     const double lx = box[0], ly = box[1], ux = box[2], uy = box[3];
     const double lo = vertical ? lx : ly, hi = vertical ? ux : uy;
     int64_t n = 1;
@@ -312,7 +351,8 @@ __device__ int64_t build_profile(const Free &F, const double *box, bool vertical
     if (vertical) {
         double height = 0.0;
         for (int64_t k = 0; k < nsteps; ++k) {
-            const double at = unord(steps[k].a), dh = unord(steps[k].b);
+            double at, dh;
+            step(k, at, dh);
             extend(at, height * (at - e[n - 1]));
             height += dh;
         }
@@ -322,8 +362,10 @@ __device__ int64_t build_profile(const Free &F, const double *box, bool vertical
             const double z = ref_min(hi, F.rowy[2 * r + 1]);
             if (z > a) {
                 extend(a, 0.0);
-                double total = 0.0;  // Row::getLength(b.getX())
-                for (int64_t s = F.rowspan[r]; s < F.rowspan[r + 1]; ++s)
+                // Row::getLength(b.getX()); spans outside [lx, ux] add +0.0
+                double total = 0.0;
+                const int64_t end = F.rowspan[r + 1];
+                for (int64_t s = first_span(F, r, lx); s < end && F.spans[2 * s] < ux; ++s)
                     total += ref_max(0.0, ref_min(ux, F.spans[2 * s + 1]) - ref_max(lx, F.spans[2 * s]));
                 extend(z, total * (z - a));
             }
@@ -336,6 +378,123 @@ __device__ int64_t build_profile(const Free &F, const double *box, bool vertical
         n = 2;
     }
     return n;
+}
+
+__device__ int64_t build_profile(const Free &F, const double *box, bool vertical, const Key *steps,
+                                 int64_t nsteps, double *e, double *p) {
+    return build_profile_from(
+        F, box, vertical,
+        [&](int64_t k, double &at, double &dh) {
+            at = unord(steps[k].a);
+            dh = unord(steps[k].b);
+        },
+        nsteps, e, p);
+}
+
+// getStripes (simpl_lal.cc:266-312) for one half box, then the stable sort
+// of nonlinearScale (:325-328) by distance from the cutline, farthest first.
+// The reference inserts each midpoint split into its cut list and steps on;
+// that visits the intervals depth first, which a small stack does here with
+// the same operations (room.getBetween(a, b) = before(b) - before(a), each
+// before() computed once). The stripes come out in ascending position, so
+// their distance from the cut is monotone: below the cut the stable
+// descending order is the order itself, above it the runs of equal distance
+// in reverse with each run kept in order. `cuts` is scratch of `cap` doubles;
+// the stripes' spans and capacities go to sa/sb/scap. Returns the number of
+// stripes, or -1 when `cap` (or the split depth) is exceeded.
+__device__ int64_t make_stripes(const Prof &room, const double *box, bool v, double cell_area,
+                                double region_room, double frac, double limit_density,
+                                const double *obst, int32_t K, double cutline, bool below,
+                                double *cuts, int64_t cap, double *sa, double *sb, double *scap) {
+    constexpr int kLocalCuts = 64;
+    constexpr int kDepth = 64;
+    const double lo = v ? box[0] : box[1], hi = v ? box[2] : box[3];
+    double lc[kLocalCuts];  // small cut lists are sorted in (L1-resident) local memory
+    int64_t nc = 0;
+    bool local = true;
+    auto put = [&](double x) {
+        if (local && nc < kLocalCuts) {
+            lc[nc++] = x;
+            return;
+        }
+        if (local) {
+            for (int64_t i = 0; i < nc; ++i) cuts[i] = lc[i];
+            local = false;
+        }
+        cuts[nc++] = x;
+    };
+    put(lo);
+    put(hi);
+    for (int32_t o = 0; o < K; ++o) {
+        const double *ob = obst + 4 * o;
+        if (ob[2] <= box[0] || ob[0] >= box[2] || ob[3] <= box[1] || ob[1] >= box[3]) continue;
+        const double e0 = v ? ob[0] : ob[1], e1 = v ? ob[2] : ob[3];
+        if (nc + 2 > cap) return -1;
+        if (e0 > lo && e0 < hi) put(e0);
+        if (e1 > lo && e1 < hi) put(e1);
+    }
+    double *c = local ? lc : cuts;
+    for (int64_t i = 1; i < nc; ++i) {  // insertion sort (stable)
+        const double t = c[i];
+        int64_t j = i - 1;
+        while (j >= 0 && t < c[j]) {
+            c[j + 1] = c[j];
+            --j;
+        }
+        c[j + 1] = t;
+    }
+    int64_t u = 0;
+    for (int64_t i = 0; i < nc; ++i)
+        if (u == 0 || !(c[u - 1] == c[i])) c[u++] = c[i];
+    nc = u;
+    const double limit = frac * (region_room > 0.0 ? region_room : room.total());
+    const double fill = room.total() > 0.0 ? ref_min(limit_density, cell_area / room.total())
+                                           : limit_density;
+    int64_t ns = 0;
+    double a = c[0], ba = room.before(a);
+    double stk[kDepth], stkb[kDepth];
+    for (int64_t i = 1; i < nc; ++i) {
+        int top = 0;
+        stk[top] = c[i];
+        stkb[top] = room.before(c[i]);
+        ++top;
+        while (top > 0) {
+            const double b = stk[top - 1], bb = stkb[top - 1];
+            const double here = bb - ba;
+            const double mid = room.coordinate_at(ba + 0.5 * here);
+            if (here > limit && mid > a && mid < b) {
+                if (top == kDepth || ns + top + 1 > cap) return -1;
+                stk[top] = mid;
+                stkb[top] = room.before(mid);
+                ++top;
+            } else {
+                if (ns >= cap) return -1;
+                sa[ns] = a;
+                sb[ns] = b;
+                scap[ns] = fill * here;
+                ++ns;
+                --top;
+                a = b;
+                ba = bb;
+            }
+        }
+    }
+    if (!below) {
+        auto swap_at = [&](int64_t i, int64_t j) {
+            double t = sa[i]; sa[i] = sa[j]; sa[j] = t;
+            t = sb[i]; sb[i] = sb[j]; sb[j] = t;
+            t = scap[i]; scap[i] = scap[j]; scap[j] = t;
+        };
+        for (int64_t i = 0, j = ns - 1; i < j; ++i, --j) swap_at(i, j);
+        for (int64_t r = 0; r < ns;) {  // restore the original order inside each run
+            const double f = 0.5 * (sa[r] + sb[r]) - cutline;
+            int64_t e = r + 1;
+            while (e < ns && 0.5 * (sa[e] + sb[e]) - cutline == f) ++e;
+            for (int64_t i = r, j = e - 1; i < j; ++i, --j) swap_at(i, j);
+            r = e;
+        }
+    }
+    return ns;
 }
 
 // ---- per-level kernels --------------------------------------------------------------
@@ -384,18 +543,131 @@ __global__ void k_keys_to_cells(Level L, const Key *keys, int32_t *cells) {
 
 // One thread per block: areas and median in the reference's order, and the
 // block profile's bound.
-__global__ void k_block_split(Level L, CellsDev C, Free F, const int32_t *cells) {
+// ---- exact area sums ------------------------------------------------------------
+//
+// When every cell area is a multiple of 2^-q and the total times 2^q stays
+// below 2^52, every partial sum the reference forms (cellArea, lowArea, a
+// stripe's used area) is exact in double, whatever the order. The sums are
+// then read off an integer prefix over the positions: pre[p] = fixed-point
+// area of positions [0, p).
+
+constexpr int kScanTile = 2048;  // positions per tile: kT threads x 8
+
+__device__ __forceinline__ long long area_fx(const double *area, int32_t i, double scale) {
+    return __double2ll_rn(area[i] * scale);
+}
+
+__device__ __forceinline__ long long warp_incl64(long long v) {
+    const int lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Exclusive block scan of one value per thread (blockDim.x == kT); returns
+// the exclusive prefix and sets `total`.
+__device__ long long block_excl64(long long v, long long &total) {
+    __shared__ long long ws[kT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const long long inc = warp_incl64(v);
+    if (lane == 31) ws[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        long long w = lane < kT / 32 ? ws[lane] : 0;
+        w = warp_incl64(w);
+        if (lane < kT / 32) ws[lane] = w;
+    }
+    __syncthreads();
+    const long long out = inc - v + (wid > 0 ? ws[wid - 1] : 0);
+    total = ws[kT / 32 - 1];
+    __syncthreads();
+    return out;
+}
+
+__global__ void __launch_bounds__(kT) k_fx_tile_sums(const int32_t *cells, const double *area,
+                                                     int32_t n, double scale, long long *tile) {
+    const int32_t base = blockIdx.x * kScanTile;
+    long long v = 0;
+    for (int k = threadIdx.x; k < kScanTile; k += kT)
+        if (base + k < n) v += area_fx(area, cells[base + k], scale);
+    long long total;
+    block_excl64(v, total);
+    if (threadIdx.x == 0) tile[blockIdx.x] = total;
+}
+
+// Exclusive scan of the tile sums in place (one block).
+__global__ void __launch_bounds__(kT) k_fx_tile_scan(long long *tile, int32_t ntiles) {
+    const int per = (ntiles + kT - 1) / kT;
+    const int beg = threadIdx.x * per, end = min(beg + per, ntiles);
+    long long v = 0;
+    for (int i = beg; i < end; ++i) v += tile[i];
+    long long total;
+    long long run = block_excl64(v, total);
+    for (int i = beg; i < end; ++i) {
+        const long long t = tile[i];
+        tile[i] = run;
+        run += t;
+    }
+}
+
+// pre[p + 1] = fixed-point area of positions [0, p]; pre[0] = 0.
+__global__ void __launch_bounds__(kT) k_fx_prefix(const int32_t *cells, const double *area,
+                                                  int32_t n, double scale, const long long *tile,
+                                                  long long *pre) {
+    const int32_t base = blockIdx.x * kScanTile + threadIdx.x * (kScanTile / kT);
+    long long v[kScanTile / kT];
+    long long sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanTile / kT; ++k) {
+        v[k] = base + k < n ? area_fx(area, cells[base + k], scale) : 0;
+        sum += v[k];
+    }
+    long long total;
+    long long run = block_excl64(sum, total) + tile[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanTile / kT; ++k) {
+        run += v[k];
+        if (base + k < n) pre[base + k + 1] = run;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) pre[0] = 0;
+}
+
+// Median split from the prefix: the least m >= 1 with 2 * low(m) >= total,
+// at most size - 1 (the loop of split, simpl_lal.cc:230-233).
+__device__ __forceinline__ int32_t median_fx(const long long *pre, int32_t b, int32_t size) {
+    if (size <= 1) return 0;
+    const long long tot = pre[b + size] - pre[b];
+    int32_t lo = 1, hi = size - 1;  // answer in [lo, hi]
+    while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (2 * (pre[b + mid] - pre[b]) >= tot) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// One thread per block: areas and median in the reference's order (or from
+// the exact prefix when `pre` is set), and the block profile's bound.
+__global__ void k_block_split(Level L, CellsDev C, Free F, const int32_t *cells,
+                              const long long *pre, double inv_scale) {
     const int32_t blk = blockIdx.x * blockDim.x + threadIdx.x;
     if (blk >= L.na) return;
     const int32_t b = L.b[blk], e = L.e[blk];
     const int32_t size = e - b;
-    double cell_area = 0.0;
-    for (int32_t p = b; p < e; ++p) cell_area += C.area[cells[p]];
+    double cell_area = 0.0, low = 0.0, high = 0.0;
     int32_t m = 0;
-    double low = 0.0;
-    while (m + 1 < size && (m == 0 || low < 0.5 * cell_area)) low += C.area[cells[b + m++]];
-    double high = 0.0;
-    for (int32_t p = b + m; p < e; ++p) high += C.area[cells[p]];
+    if (pre) {
+        m = median_fx(pre, b, size);
+        cell_area = static_cast<double>(pre[e] - pre[b]) * inv_scale;
+        low = static_cast<double>(pre[b + m] - pre[b]) * inv_scale;
+        high = static_cast<double>(pre[e] - pre[b + m]) * inv_scale;
+    } else {
+        for (int32_t p = b; p < e; ++p) cell_area += C.area[cells[p]];
+        while (m + 1 < size && (m == 0 || low < 0.5 * cell_area)) low += C.area[cells[b + m++]];
+        for (int32_t p = b + m; p < e; ++p) high += C.area[cells[p]];
+    }
     L.m[blk] = m;
     L.low_area[blk] = low;
     L.high_area[blk] = high;
@@ -444,7 +716,7 @@ __global__ void k_block_cut(Level L, Free F, const int64_t *soff, const Key *ste
             ++k;
         }
         hbound[4 * blk + 2 * side] = st;
-        hbound[4 * blk + 2 * side + 1] = ed + 2 * k + 2 + 256;  // profile edges, then cuts
+        hbound[4 * blk + 2 * side + 1] = ed + 2 * k + 2;  // profile edges, obstacle cuts
     }
 }
 
@@ -478,80 +750,14 @@ __global__ void k_half_stripes(Level L, Free F, const int64_t *soff, const Key *
     const int64_t n = build_profile(F, box, v, steps + soff[h], nsteps[h], e, p);
     const Prof room{e, p, n};
     const double cell_area = side ? L.high_area[blk] : L.low_area[blk];
-    const double region_room = L.room[blk];
-    const double lo = v ? box[0] : box[1], hi = v ? box[2] : box[3];
-    // cuts live after the profile in the same scratch
-    double *cuts = p + n;
-    const int64_t cap = cap_over[h];  // cuts (and stripes) the half may hold
-    int64_t nc = 0;
-    cuts[nc++] = lo;
-    cuts[nc++] = hi;
-    for (int32_t o = 0; o < F.K; ++o) {
-        const double *ob = F.obst + 4 * o;
-        if (ob[2] <= box[0] || ob[0] >= box[2] || ob[3] <= box[1] || ob[1] >= box[3]) continue;
-        const double e0 = v ? ob[0] : ob[1], e1 = v ? ob[2] : ob[3];
-        if (e0 > lo && e0 < hi) cuts[nc++] = e0;
-        if (e1 > lo && e1 < hi) cuts[nc++] = e1;
-    }
-    for (int64_t i = 1; i < nc; ++i) {  // insertion sort (stable)
-        const double t = cuts[i];
-        int64_t j = i - 1;
-        while (j >= 0 && t < cuts[j]) {
-            cuts[j + 1] = cuts[j];
-            --j;
-        }
-        cuts[j + 1] = t;
-    }
-    int64_t u = 0;
-    for (int64_t i = 0; i < nc; ++i)
-        if (u == 0 || !(cuts[u - 1] == cuts[i])) cuts[u++] = cuts[i];
-    nc = u;
-    const double limit = frac * (region_room > 0.0 ? region_room : room.total());
-    const double fill = room.total() > 0.0 ? ref_min(limit_density, cell_area / room.total())
-                                           : limit_density;
-    for (int64_t s = 0; s + 1 < nc;) {
-        const double a = cuts[s], b = cuts[s + 1];
-        const double here = room.between(a, b);
-        const double mid = room.coordinate_at(room.before(a) + 0.5 * here);
-        if (here > limit && mid > a && mid < b) {
-            if (nc + 1 > cap) {
-                atomicCAS(status, kStatusOk, kStatusCapacity);
-                break;
-            }
-            for (int64_t q = nc; q > s + 1; --q) cuts[q] = cuts[q - 1];
-            cuts[s + 1] = mid;
-            ++nc;
-        } else {
-            ++s;
-        }
-    }
-    const int64_t ns = nc - 1;
     const int64_t so = S.off[h];
-    const double cutline = L.cut[blk];
-    const bool below = side == 0;
-    for (int64_t s = 0; s < ns; ++s) {
-        S.a[so + s] = cuts[s];
-        S.b[so + s] = cuts[s + 1];
-        S.cap[so + s] = fill * room.between(cuts[s], cuts[s + 1]);
-    }
-    // stable sort by fromCut(center) descending (insertion sort on the arrays)
-    for (int64_t i = 1; i < ns; ++i) {
-        const double ta = S.a[so + i], tb = S.b[so + i], tc = S.cap[so + i];
-        const double cc = 0.5 * (ta + tb);
-        const double fc = below ? cutline - cc : cc - cutline;
-        int64_t j = i - 1;
-        while (j >= 0) {
-            const double cj = 0.5 * (S.a[so + j] + S.b[so + j]);
-            const double fj = below ? cutline - cj : cj - cutline;
-            if (!(fc > fj)) break;
-            S.a[so + j + 1] = S.a[so + j];
-            S.b[so + j + 1] = S.b[so + j];
-            S.cap[so + j + 1] = S.cap[so + j];
-            --j;
-        }
-        S.a[so + j + 1] = ta;
-        S.b[so + j + 1] = tb;
-        S.cap[so + j + 1] = tc;
+    // cuts live after the profile in the same scratch
+    int64_t ns = make_stripes(room, box, v, cell_area, L.room[blk], frac, limit_density, F.obst,
+                              F.K, L.cut[blk], side == 0, p + n, cap_over[h], S.a + so,
+                              S.b + so, S.cap + so);
+    if (ns < 0) {
+        atomicCAS(status, kStatusOk, kStatusCapacity);
+        ns = 0;
     }
     for (int64_t s = 0; s < ns; ++s) {
         S.used[so + s] = 0.0;
@@ -598,6 +804,59 @@ __global__ void k_fill(Level L, CellsDev C, const int32_t *cells, Stripes S, int
     }
 }
 
+// Greedy fill from the exact prefix (fill order): stripe s of a half takes
+// positions [start_s, start_{s+1}), start_{s+1} the least position whose
+// preceding area in the stripe reaches its capacity. One thread per half;
+// the starts go to `sbeg`.
+__global__ void k_fill_fx(Level L, Stripes S, const long long *pre, double inv_scale,
+                          int32_t *sbeg) {
+    const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2 * L.na) return;
+    const int32_t blk = h >> 1;
+    const int32_t b = L.b[blk], e = L.e[blk], mid = b + L.m[blk];
+    const int32_t p0 = (h & 1) ? mid : b, p1 = (h & 1) ? e : mid;
+    const int64_t so = S.off[h];
+    const int32_t ns = S.count[h];
+    int32_t at = p0;
+    for (int32_t s = 0; s < ns; ++s) {
+        sbeg[so + s] = at;
+        if (s + 1 == ns) break;
+        const double cap = S.cap[so + s];
+        int32_t lo = at, hi = p1;  // least k in [at, p1] with used(k) >= cap, else p1
+        while (lo < hi) {
+            const int32_t k = (lo + hi) >> 1;
+            if (static_cast<double>(pre[k] - pre[at]) * inv_scale >= cap) hi = k;
+            else lo = k + 1;
+        }
+        at = lo;
+    }
+}
+
+// Stripe of every position: the last stripe of its half starting at or
+// before it.
+__global__ void k_assign_fx(Level L, const int32_t *cells, Stripes S, const int32_t *sbeg,
+                            int32_t *stripe_of) {
+    for (int32_t blk = blockIdx.y; blk < L.na; blk += gridDim.y) {
+        const int32_t b = L.b[blk], e = L.e[blk], mid = b + L.m[blk];
+        for (int32_t p = b + blockIdx.x * blockDim.x + threadIdx.x; p < e; p += gridDim.x * blockDim.x) {
+            const int32_t h = 2 * blk + (p < mid ? 0 : 1);
+            const int64_t so = S.off[h];
+            const int32_t ns = S.count[h];
+            int32_t s = -1;
+            if (ns > 0) {
+                int32_t lo = 0, hi = ns - 1;  // last s with sbeg[s] <= p (sbeg[0] <= p)
+                while (lo < hi) {
+                    const int32_t k = (lo + hi + 1) >> 1;
+                    if (sbeg[so + k] <= p) lo = k;
+                    else hi = k - 1;
+                }
+                s = static_cast<int32_t>(so + lo);
+            }
+            stripe_of[cells[p]] = s;
+        }
+    }
+}
+
 __global__ void k_stripe_minmax(Level L, CellsDev C, const int32_t *cells, Stripes S,
                                 const int32_t *stripe_of) {
     for (int32_t blk = blockIdx.y; blk < L.na; blk += gridDim.y) {
@@ -634,6 +893,724 @@ __global__ void k_new_pos(Level L, CellsDev C, const int32_t *cells, Stripes S,
         np = np < a ? a : (lim < np ? lim : np);  // std::clamp
         (v ? C.x : C.y)[i] = np;
     }
+    }
+}
+
+// ---- small blocks: one CTA finishes a block's whole subtree ------------------------
+//
+// A block of at most kSub cells is handed to one CTA, which runs every
+// remaining level of its bisection out of shared memory: the cells' ids,
+// positions, sizes and areas, the CTA-wide sort buffer (three key words per
+// entry, compared as (k2, k0, k1)) and the per-level scans. The level's
+// sub-blocks, their profiles and stripes live in a per-CTA slice of global
+// scratch. A block whose needs exceed a capacity (sort buffer, profile or
+// stripe slots, sub-blocks per level, local obstacles) is left untouched
+// and flagged; the caller runs it level by level instead.
+
+constexpr int kSub = 2048;
+constexpr int kSubThreads = 512;
+constexpr int kSortCap = 4096;      // entries of the sort buffer (steps and profiles)
+constexpr int kMaxSub = 1024;       // sub-blocks of one level
+constexpr int kObstLocal = 256;     // obstacles overlapping the block
+constexpr int64_t kStripeCap = 8192;
+constexpr int kRowsLocal = 512;     // free-space rows staged in shared memory
+constexpr int kSpansLocal = 1280;   // and their spans
+constexpr int kSmallSeg = 48;       // segments up to this long: one thread sorts each
+constexpr size_t kSubSmem = sizeof(unsigned long long) * 2 * kSortCap +
+                            sizeof(uint32_t) * kSortCap + sizeof(long long) * (kSub + 2) +
+                            sizeof(double) * (3 * kSub + 4 * kObstLocal) +
+                            sizeof(double) * (2 * kRowsLocal + 2 * kSpansLocal) +
+                            sizeof(int64_t) * (kRowsLocal + 2) +
+                            sizeof(int32_t) * (3 * kSub + 2 * kMaxSub) + sizeof(int16_t) * kSub;
+
+struct SubTask {
+    double box[4];
+    double room;
+    int32_t b, e, level, vert;
+};
+
+struct SubDesc {
+    double box[4];
+    double hbox[8];
+    double cell_area, low_area, high_area, cut;
+    int32_t b, e, level, vert, m, act, rank;
+    int32_t soff, scnt, slen;                     // block profile region in the sort buffer
+    int32_t hsoff[2], hscnt[2], hslen[2];         // the halves' regions
+    int32_t stoff[2], stcap[2], stcnt[2];         // the halves' stripes
+};
+
+struct SubArgs {
+    const SubTask *tasks;
+    int32_t ntasks;
+    int32_t *fail;           // [ntasks] 1: left for the level-by-level path
+    const int32_t *cells;    // position -> cell id
+    CellsDev C;
+    Free F;
+    SubDesc *desc;           // [grid * 2 * kMaxSub]
+    double *strp;            // [grid * 4 * kStripeCap] cuts, start, end, capacity
+    unsigned long long *strlh;  // [grid * 2 * kStripeCap] lowest / highest centre
+    int32_t max_level, min_cells, stripe_extra;
+    double frac, limit_density;
+    int32_t exact;           // areas sum exactly: prefix sums and binary searches
+    double scale, inv_scale; // 2^q, 2^-q
+};
+
+__device__ __forceinline__ bool sub_less(uint32_t a2, unsigned long long a0, unsigned long long a1,
+                                         uint32_t b2, unsigned long long b0, unsigned long long b1) {
+    return a2 < b2 || (a2 == b2 && (a0 < b0 || (a0 == b0 && a1 < b1)));
+}
+
+// Bitonic sort of entries [0, n) of the CTA buffer (padded to the power of
+// two P >= n with entries above every key).
+__device__ void cta_sort(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int n) {
+    int P = 1;
+    while (P < n) P <<= 1;
+    for (int i = n + threadIdx.x; i < P; i += blockDim.x) {
+        k2[i] = 0xffffffffu;
+        k0[i] = ~0ull;
+        k1[i] = ~0ull;
+    }
+    __syncthreads();
+    if (n <= 1) return;
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
+                const int i = 2 * j * (t / j) + (t % j);
+                const int q = i + j;
+                const bool up = (i & k) == 0;
+                const uint32_t a2 = k2[i], b2 = k2[q];
+                const unsigned long long a0 = k0[i], b0 = k0[q], a1 = k1[i], b1 = k1[q];
+                if (sub_less(b2, b0, b1, a2, a0, a1) == up) {
+                    k2[i] = b2; k0[i] = b0; k1[i] = b1;
+                    k2[q] = a2; k0[q] = a0; k1[q] = a1;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Stable insertion sort of entries [b, e) by one thread.
+__device__ void seg_sort1(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int b,
+                          int e) {
+    for (int i = b + 1; i < e; ++i) {
+        const unsigned long long a0 = k0[i], a1 = k1[i];
+        const uint32_t a2 = k2[i];
+        int j = i - 1;
+        while (j >= b && sub_less(a2, a0, a1, k2[j], k0[j], k1[j])) {
+            k0[j + 1] = k0[j];
+            k1[j + 1] = k1[j];
+            k2[j + 1] = k2[j];
+            --j;
+        }
+        k0[j + 1] = a0;
+        k1[j + 1] = a1;
+        k2[j + 1] = a2;
+    }
+}
+
+// Exclusive scan of buf[0, n) in place; returns the total to every thread.
+__device__ int32_t cta_scan(int32_t *buf, int n, int32_t *warp_tmp) {
+    const int nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int per = (n + nt - 1) / nt;
+    const int beg = min(tid * per, n), end = min(beg + per, n);
+    int32_t local = 0;
+    for (int i = beg; i < end; ++i) local += buf[i];
+    int32_t v = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_tmp[wid] = v;
+    __syncthreads();
+    const int nw = nt >> 5;
+    if (wid == 0) {
+        int32_t w = lane < nw ? warp_tmp[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) warp_tmp[lane] = w;
+    }
+    __syncthreads();
+    int32_t run = v - local + (wid > 0 ? warp_tmp[wid - 1] : 0);
+    const int32_t total = warp_tmp[nw - 1];
+    for (int i = beg; i < end; ++i) {
+        const int32_t t = buf[i];
+        buf[i] = run;
+        run += t;
+    }
+    __syncthreads();
+    return total;
+}
+
+// pre[p + 1] = fixed-point area of positions [0, p] (cell at[p], area sa);
+// pre[0] = 0.
+__device__ void cta_prefix64(const int32_t *at, const double *sa, int n, double scale,
+                             long long *pre, long long *w64) {
+    const int nt = blockDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int per = (n + nt - 1) / nt;
+    const int beg = min(tid * per, n), end = min(beg + per, n);
+    long long local = 0;
+    for (int p = beg; p < end; ++p) local += __double2ll_rn(sa[at[p]] * scale);
+    long long v = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) w64[wid] = v;
+    __syncthreads();
+    const int nw = nt >> 5;
+    if (wid == 0) {
+        long long w = lane < nw ? w64[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) w64[lane] = w;
+    }
+    __syncthreads();
+    long long run = v - local + (wid > 0 ? w64[wid - 1] : 0);
+    for (int p = beg; p < end; ++p) {
+        run += __double2ll_rn(sa[at[p]] * scale);
+        pre[p + 1] = run;
+    }
+    if (tid == 0) pre[0] = 0;
+    __syncthreads();
+}
+
+// Index of the sub-block holding position p: the last with b <= p.
+__device__ __forceinline__ int find_desc(const SubDesc *cur, int ncur, int p) {
+    int lo = 0, hi = ncur;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (cur[mid].b <= p) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// A region of the sort buffer holding a profile: two leading pads, then the
+// sorted steps (vertical) or nothing (horizontal); the profile is written
+// over it in place (edge n lands at slot n, the step read last sits at slot
+// >= n + 1).
+__device__ int64_t build_profile_inplace(const Free &F, const double *box, bool v,
+                                         unsigned long long *k0, unsigned long long *k1, int o,
+                                         int nsteps) {
+    double *e = reinterpret_cast<double *>(k0 + o);
+    double *p = reinterpret_cast<double *>(k1 + o);
+    return build_profile_from(
+        F, box, v,
+        [&](int64_t k, double &x, double &dh) {
+            x = unord(k0[o + 2 + k]);
+            dh = unord(k1[o + 2 + k]);
+        },
+        nsteps, e, p);
+}
+
+// Writes a profile region: pads over [o, o + len), then the box's steps
+// from o + 2 (vertical).
+__device__ void emit_region(const Free &F, const double *box, bool v, uint32_t tag,
+                            unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int o,
+                            int len) {
+    for (int q = 0; q < len; ++q) {
+        k2[o + q] = tag;
+        k0[o + q] = 0ull;
+        k1[o + q] = 0ull;
+    }
+    if (v)
+        emit_steps(F, box, [&](int64_t k, double x, double dh) {
+            k0[o + 2 + k] = ord(x);
+            k1[o + 2 + k] = ord(dh);
+        });
+}
+
+__global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long *k0 = reinterpret_cast<unsigned long long *>(smem);
+    unsigned long long *k1 = k0 + kSortCap;
+    long long *pre = reinterpret_cast<long long *>(k1 + kSortCap);  // [kSub + 1]
+    double *sx = reinterpret_cast<double *>(pre + kSub + 2);
+    double *sy = sx + kSub, *sa = sy + kSub;
+    double *obst = sa + kSub;
+    double *lrowy = obst + 4 * kObstLocal, *lspans = lrowy + 2 * kRowsLocal;
+    int64_t *lrowspan = reinterpret_cast<int64_t *>(lspans + 2 * kSpansLocal);
+    uint32_t *k2 = reinterpret_cast<uint32_t *>(lrowspan + kRowsLocal + 2);
+    int32_t *gid = reinterpret_cast<int32_t *>(k2 + kSortCap);
+    int32_t *at = gid + kSub, *sof = at + kSub, *scan = sof + kSub;
+    int16_t *dof = reinterpret_cast<int16_t *>(scan + 2 * kMaxSub);
+    __shared__ int32_t warp_tmp[32];
+    __shared__ long long w64[32];
+    __shared__ int s_fail, s_nobst, s_ncur, s_maxlen, s_maxsteps;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    SubDesc *const cur0 = A.desc + static_cast<size_t>(blockIdx.x) * 2 * kMaxSub;
+    double *const scut = A.strp + static_cast<size_t>(blockIdx.x) * 4 * kStripeCap;
+    double *const sta = scut + kStripeCap, *const stb = sta + kStripeCap;
+    double *const stc = stb + kStripeCap;
+    unsigned long long *const slo = A.strlh + static_cast<size_t>(blockIdx.x) * 2 * kStripeCap;
+    unsigned long long *const shi = slo + kStripeCap;
+    const CellsDev &C = A.C;
+    auto centre = [&](int j, bool v) {
+        return v ? sx[j] + 0.5 * C.w[gid[j]] : sy[j] + 0.5 * C.h[gid[j]];
+    };
+
+    for (int task = blockIdx.x; task < A.ntasks; task += gridDim.x) {
+        const SubTask T = A.tasks[task];
+        const int size = T.e - T.b;
+        if (tid == 0) {
+            s_fail = size > kSub ? 1 : 0;
+            s_nobst = 0;
+            s_maxlen = 0;
+            s_maxsteps = 0;
+        }
+        __syncthreads();
+        if (s_fail) {
+            if (tid == 0) A.fail[task] = 1;
+            __syncthreads();
+            continue;
+        }
+        for (int j = tid; j < size; j += nt) {
+            const int32_t g = A.cells[T.b + j];
+            gid[j] = g;
+            sx[j] = C.x[g];
+            sy[j] = C.y[g];
+            sa[j] = C.area[g];
+            at[j] = j;
+        }
+        for (int o = tid; o < A.F.K; o += nt) {
+            const double *ob = A.F.obst + 4 * o;
+            if (ob[2] <= T.box[0] || ob[0] >= T.box[2] || ob[3] <= T.box[1] || ob[1] >= T.box[3])
+                continue;
+            const int k = atomicAdd(&s_nobst, 1);
+            if (k < kObstLocal)
+                for (int q = 0; q < 4; ++q) obst[4 * k + q] = ob[q];
+        }
+        if (tid == 0) {
+            SubDesc &d = cur0[0];
+            for (int q = 0; q < 4; ++q) d.box[q] = T.box[q];
+            d.b = 0;
+            d.e = size;
+            d.level = T.level;
+            d.vert = T.vert;
+            s_ncur = 1;
+        }
+        Free FL = A.F;
+        {  // the rows overlapping the block, with their spans overlapping its x
+           // range, into shared memory (the only spans its sub-boxes can meet)
+            const int32_t r0 = first_row(A.F, T.box[1]);
+            int32_t lo = r0, hi = A.F.R;  // first row from r0 with y start >= uy
+            while (lo < hi) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (A.F.rowy[2 * mid] < T.box[3]) lo = mid + 1;
+                else hi = mid;
+            }
+            const int32_t nr = lo - r0;
+            if (nr <= kRowsLocal) {
+                for (int i = tid; i < nr; i += nt) {
+                    const int64_t f = first_span(A.F, r0 + i, T.box[0]);
+                    int64_t e = f;
+                    while (e < A.F.rowspan[r0 + i + 1] && A.F.spans[2 * e] < T.box[2]) ++e;
+                    scan[i] = static_cast<int32_t>(e - f);
+                    lrowspan[i] = f;  // first span, global index (rebased below)
+                }
+                __syncthreads();
+                const int32_t ns = cta_scan(scan, nr, warp_tmp);
+                if (ns <= kSpansLocal) {
+                    for (int i = tid; i < nr; i += nt) {
+                        const int64_t f = lrowspan[i];
+                        const int32_t o = scan[i];
+                        const int32_t cnt = (i + 1 < nr ? scan[i + 1] : ns) - o;
+                        for (int32_t q = 0; q < cnt; ++q) {
+                            lspans[2 * (o + q)] = A.F.spans[2 * (f + q)];
+                            lspans[2 * (o + q) + 1] = A.F.spans[2 * (f + q) + 1];
+                        }
+                        lrowy[2 * i] = A.F.rowy[2 * (r0 + i)];
+                        lrowy[2 * i + 1] = A.F.rowy[2 * (r0 + i) + 1];
+                    }
+                    __syncthreads();
+                    for (int i = tid; i <= nr; i += nt) lrowspan[i] = i < nr ? scan[i] : ns;
+                    FL.rowy = lrowy;
+                    FL.rowspan = lrowspan;
+                    FL.spans = lspans;
+                    FL.R = nr;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_nobst > kObstLocal && tid == 0) s_fail = 1;
+        FL.obst = obst;
+        FL.K = min(s_nobst, kObstLocal);
+        SubDesc *cur = cur0, *nxt = cur0 + kMaxSub;
+        for (;;) {
+            __syncthreads();
+            const int ncur = s_ncur;
+            if (s_fail || ncur == 0) break;
+            // A. which sub-blocks split at this level, their rank, the longest
+            for (int i = tid; i < ncur; i += nt) {
+                const int len = cur[i].e - cur[i].b;
+                const int act = cur[i].level < A.max_level && len > A.min_cells;
+                cur[i].act = act;
+                scan[i] = act;
+                if (act) atomicMax(&s_maxlen, len);
+            }
+            __syncthreads();
+            const int nact = cta_scan(scan, ncur, warp_tmp);
+            if (nact == 0) break;
+            if (2 * nact > kMaxSub) {
+                if (tid == 0) s_fail = 1;
+                break;
+            }
+            const bool small_cells = s_maxlen <= kSmallSeg;
+            for (int i = tid; i < ncur; i += nt) cur[i].rank = scan[i];
+            // B. each position's sub-block; cells of each splitting sub-block by
+            // (centre, id), ties by cell id as the reference's sortCells
+            for (int p = tid; p < size; p += nt) {
+                const int i = find_desc(cur, ncur, p);
+                const bool in = p >= cur[i].b && p < cur[i].e && cur[i].act;
+                dof[p] = static_cast<int16_t>(in ? i : -1);
+                const int j = at[p];
+                if (in) {
+                    k2[p] = static_cast<uint32_t>(cur[i].b);
+                    k0[p] = ord(centre(j, cur[i].vert != 0));
+                } else {
+                    k2[p] = static_cast<uint32_t>(p);
+                    k0[p] = 0ull;
+                }
+                k1[p] = (static_cast<unsigned long long>(gid[j]) << 32) | static_cast<unsigned>(j);
+            }
+            __syncthreads();
+            if (small_cells) {
+                for (int i = tid; i < ncur; i += nt)
+                    if (cur[i].act) seg_sort1(k0, k1, k2, cur[i].b, cur[i].e);
+                __syncthreads();
+            } else {
+                cta_sort(k0, k1, k2, size);
+            }
+            for (int p = tid; p < size; p += nt) at[p] = static_cast<int32_t>(k1[p] & 0xffffffffull);
+            __syncthreads();
+            if (A.exact) cta_prefix64(at, sa, size, A.scale, pre, w64);
+            // C. areas and median in sorted order; the block profile's region
+            for (int i = tid; i < ncur; i += nt) {
+                SubDesc &d = cur[i];
+                int32_t steps = 0, len = 0;
+                if (d.act) {
+                    const int b = d.b, e = d.e, n = e - b;
+                    double cell_area = 0.0, low = 0.0, high = 0.0;
+                    int m = 0;
+                    if (A.exact) {
+                        m = median_fx(pre, b, n);
+                        cell_area = static_cast<double>(pre[e] - pre[b]) * A.inv_scale;
+                        low = static_cast<double>(pre[b + m] - pre[b]) * A.inv_scale;
+                        high = static_cast<double>(pre[e] - pre[b + m]) * A.inv_scale;
+                    } else {
+                        for (int p = b; p < e; ++p) cell_area += sa[at[p]];
+                        while (m + 1 < n && (m == 0 || low < 0.5 * cell_area))
+                            low += sa[at[b + m++]];
+                        for (int p = b + m; p < e; ++p) high += sa[at[p]];
+                    }
+                    d.m = m;
+                    d.cell_area = cell_area;
+                    d.low_area = low;
+                    d.high_area = high;
+                    const bool v = d.vert != 0;
+                    steps = v ? static_cast<int32_t>(count_steps(FL, d.box)) : 0;
+                    len = (v ? steps : 2 * count_rows(FL, d.box)) + 2;
+                    atomicMax(&s_maxsteps, steps);
+                }
+                d.scnt = steps;
+                d.slen = len;
+                scan[i] = len;
+            }
+            __syncthreads();
+            const int tot = cta_scan(scan, ncur, warp_tmp);
+            if (tot > kSortCap) {
+                if (tid == 0) s_fail = 1;
+                break;
+            }
+            const bool small_steps = s_maxsteps <= kSmallSeg;
+            for (int i = tid; i < ncur; i += nt) cur[i].soff = scan[i];
+            __syncthreads();  // every thread has read s_maxsteps before it is reset
+            if (tid == 0) s_maxsteps = 0;
+            // D. the block profiles' regions: pads, then the steps sorted by (x, dh)
+            for (int i = tid; i < ncur; i += nt) {
+                const SubDesc &d = cur[i];
+                if (!d.act) continue;
+                emit_region(FL, d.box, d.vert != 0, static_cast<uint32_t>(i), k0, k1, k2,
+                            d.soff, d.slen);
+                if (small_steps && d.vert) seg_sort1(k0, k1, k2, d.soff + 2, d.soff + 2 + d.scnt);
+            }
+            __syncthreads();
+            if (!small_steps) cta_sort(k0, k1, k2, tot);
+            // E. profile, cutline, half boxes, the halves' regions and stripe room
+            for (int i = tid; i < ncur; i += nt) {
+                SubDesc &d = cur[i];
+                if (!d.act) {
+                    for (int side = 0; side < 2; ++side) d.hslen[side] = d.stcap[side] = 0;
+                    continue;
+                }
+                const bool v = d.vert != 0;
+                const int64_t n = build_profile_inplace(FL, d.box, v, k0, k1, d.soff, d.scnt);
+                const Prof room{reinterpret_cast<const double *>(k0 + d.soff),
+                                reinterpret_cast<const double *>(k1 + d.soff), n};
+                const double share = d.cell_area > 0.0 ? d.low_area / d.cell_area : 0.5;
+                const double lo = v ? d.box[0] : d.box[1], hi = v ? d.box[2] : d.box[3];
+                const double cut = room.total() > 0.0 ? room.coordinate_at(share * room.total())
+                                                      : lo + share * (hi - lo);
+                d.cut = cut;
+                for (int q = 0; q < 4; ++q) d.hbox[q] = d.hbox[4 + q] = d.box[q];
+                d.hbox[v ? 2 : 3] = cut;
+                d.hbox[4 + (v ? 0 : 1)] = cut;
+                const double r_lo = room.before(cut);
+                for (int side = 0; side < 2; ++side) {
+                    const double *bx = d.hbox + 4 * side;
+                    const int32_t st = v ? static_cast<int32_t>(count_steps(FL, bx)) : 0;
+                    d.hscnt[side] = st;
+                    d.hslen[side] = (v ? st : 2 * count_rows(FL, bx)) + 2;
+                    atomicMax(&s_maxsteps, st);
+                    int32_t k = 0;
+                    for (int32_t ob = 0; ob < FL.K; ++ob) {
+                        const double *q = FL.obst + 4 * ob;
+                        if (q[2] <= bx[0] || q[0] >= bx[2] || q[3] <= bx[1] || q[1] >= bx[3]) continue;
+                        ++k;
+                    }
+                    // stripes from midpoint splits hold more than half the split
+                    // limit each: at most 2 room / limit of them (+ margin)
+                    const double r_h = side ? ref_max(0.0, room.total() - r_lo) : r_lo;
+                    const double lim = A.frac * (T.room > 0.0 ? T.room : r_h);
+                    int32_t extra = A.stripe_extra;
+                    if (T.room > 0.0 && lim > 0.0)
+                        extra = static_cast<int32_t>(ref_min(static_cast<double>(A.stripe_extra),
+                                                             ceil(2.02 * r_h / lim) + 4.0));
+                    d.stcap[side] = 2 * k + 2 + extra;
+                }
+            }
+            __syncthreads();
+            for (int h = tid; h < 2 * ncur; h += nt) scan[h] = cur[h >> 1].hslen[h & 1];
+            __syncthreads();
+            const int htot = cta_scan(scan, 2 * ncur, warp_tmp);
+            for (int h = tid; h < 2 * ncur; h += nt) {
+                cur[h >> 1].hsoff[h & 1] = scan[h];
+                scan[h] = cur[h >> 1].stcap[h & 1];
+            }
+            __syncthreads();
+            const int stot = cta_scan(scan, 2 * ncur, warp_tmp);
+            if (htot > kSortCap || stot > kStripeCap) {
+                if (tid == 0) s_fail = 1;
+                break;
+            }
+            const bool small_hsteps = s_maxsteps <= kSmallSeg;
+            for (int h = tid; h < 2 * ncur; h += nt) cur[h >> 1].stoff[h & 1] = scan[h];
+            __syncthreads();
+            // F. the halves' profile regions
+            for (int h = tid; h < 2 * ncur; h += nt) {
+                const SubDesc &d = cur[h >> 1];
+                const int side = h & 1;
+                if (!d.act) continue;
+                const int o = d.hsoff[side];
+                emit_region(FL, d.hbox + 4 * side, d.vert != 0, static_cast<uint32_t>(h), k0, k1, k2,
+                            o, d.hslen[side]);
+                if (small_hsteps && d.vert) seg_sort1(k0, k1, k2, o + 2, o + 2 + d.hscnt[side]);
+            }
+            __syncthreads();
+            if (tid == 0) s_maxsteps = 0;
+            if (!small_hsteps) cta_sort(k0, k1, k2, htot);
+            // G. the halves' profiles and stripes
+            for (int h = tid; h < 2 * ncur; h += nt) {
+                SubDesc &d = cur[h >> 1];
+                const int side = h & 1;
+                if (!d.act) continue;
+                const bool v = d.vert != 0;
+                const int o = d.hsoff[side];
+                const int64_t n =
+                    build_profile_inplace(FL, d.hbox + 4 * side, v, k0, k1, o, d.hscnt[side]);
+                const Prof room{reinterpret_cast<const double *>(k0 + o),
+                                reinterpret_cast<const double *>(k1 + o), n};
+                const int so = d.stoff[side];
+                const int64_t ns = make_stripes(
+                    room, d.hbox + 4 * side, v, side ? d.high_area : d.low_area, T.room, A.frac,
+                    A.limit_density, FL.obst, FL.K, d.cut, side == 0, scut + so, d.stcap[side],
+                    sta + so, stb + so, stc + so);
+                if (ns < 0) {
+                    atomicExch(&s_fail, 1);
+                    d.stcnt[side] = 0;
+                    continue;
+                }
+                d.stcnt[side] = static_cast<int32_t>(ns);
+                for (int64_t q = 0; q < ns; ++q) {
+                    slo[so + q] = ~0ull;
+                    shi[so + q] = 0ull;
+                }
+            }
+            __syncthreads();
+            if (s_fail) break;
+            // H. cells of each half by (-distance from the cut, id)
+            for (int p = tid; p < size; p += nt) {
+                const int i = dof[p];
+                const int j = at[p];
+                if (i >= 0) {
+                    const SubDesc &d = cur[i];
+                    const int mid = d.b + d.m;
+                    const double c = centre(j, d.vert != 0);
+                    const double from = p < mid ? d.cut - c : c - d.cut;
+                    k2[p] = static_cast<uint32_t>(p < mid ? d.b : mid);
+                    k0[p] = ord(-from);
+                } else {
+                    k2[p] = static_cast<uint32_t>(p);
+                    k0[p] = 0ull;
+                }
+                k1[p] = (static_cast<unsigned long long>(gid[j]) << 32) | static_cast<unsigned>(j);
+            }
+            __syncthreads();
+            if (small_cells) {
+                for (int h = tid; h < 2 * ncur; h += nt) {
+                    const SubDesc &d = cur[h >> 1];
+                    if (!d.act) continue;
+                    const int mid = d.b + d.m;
+                    if (h & 1) seg_sort1(k0, k1, k2, mid, d.e);
+                    else seg_sort1(k0, k1, k2, d.b, mid);
+                }
+                __syncthreads();
+            } else {
+                cta_sort(k0, k1, k2, size);
+            }
+            for (int p = tid; p < size; p += nt) at[p] = static_cast<int32_t>(k1[p] & 0xffffffffull);
+            __syncthreads();
+            // I. greedy fill (exact areas: stripe starts by binary search on the
+            // prefix, then each position looks its stripe up; else one thread
+            // per half in the reference's order)
+            if (A.exact) {
+                cta_prefix64(at, sa, size, A.scale, pre, w64);
+                for (int h = tid; h < 2 * ncur; h += nt) {
+                    const SubDesc &d = cur[h >> 1];
+                    if (!d.act) continue;
+                    const int side = h & 1;
+                    const int mid = d.b + d.m;
+                    const int p0 = side ? mid : d.b, p1 = side ? d.e : mid;
+                    const int ns = d.stcnt[side], so = d.stoff[side];
+                    int q0 = p0;
+                    for (int q = 0; q < ns; ++q) {
+                        scut[so + q] = static_cast<double>(q0);  // stripe starts
+                        if (q + 1 == ns) break;
+                        const double cap = stc[so + q];
+                        int lo = q0, hi = p1;
+                        while (lo < hi) {
+                            const int k = (lo + hi) >> 1;
+                            if (static_cast<double>(pre[k] - pre[q0]) * A.inv_scale >= cap) hi = k;
+                            else lo = k + 1;
+                        }
+                        q0 = lo;
+                    }
+                }
+                __syncthreads();
+                for (int p = tid; p < size; p += nt) {
+                    const int i = dof[p];
+                    if (i < 0) continue;
+                    const SubDesc &d = cur[i];
+                    const int side = p < d.b + d.m ? 0 : 1;
+                    const int ns = d.stcnt[side], so = d.stoff[side];
+                    int q = -1;
+                    if (ns > 0) {
+                        int lo = 0, hi = ns - 1;
+                        while (lo < hi) {
+                            const int k = (lo + hi + 1) >> 1;
+                            if (scut[so + k] <= static_cast<double>(p)) lo = k;
+                            else hi = k - 1;
+                        }
+                        q = so + lo;
+                    }
+                    sof[at[p]] = q;
+                }
+            } else {
+                for (int h = tid; h < 2 * ncur; h += nt) {
+                    const SubDesc &d = cur[h >> 1];
+                    if (!d.act) continue;
+                    const int side = h & 1;
+                    const int mid = d.b + d.m;
+                    const int p0 = side ? mid : d.b, p1 = side ? d.e : mid;
+                    const int ns = d.stcnt[side], so = d.stoff[side];
+                    if (ns == 0) {
+                        for (int p = p0; p < p1; ++p) sof[at[p]] = -1;
+                        continue;
+                    }
+                    int q = 0;
+                    double used = 0.0;
+                    for (int p = p0; p < p1; ++p) {
+                        while (q + 1 < ns && used >= stc[so + q]) {
+                            ++q;
+                            used = 0.0;
+                        }
+                        const int j = at[p];
+                        sof[j] = so + q;
+                        used += sa[j];
+                    }
+                }
+            }
+            __syncthreads();
+            // J. lowest and highest centre per stripe
+            for (int p = tid; p < size; p += nt) {
+                const int i = dof[p];
+                if (i < 0) continue;
+                const int j = at[p];
+                const int q = sof[j];
+                if (q < 0) continue;
+                const unsigned long long o = ord(centre(j, cur[i].vert != 0));
+                atomicMin(slo + q, o);
+                atomicMax(shi + q, o);
+            }
+            __syncthreads();
+            // K. new positions
+            for (int p = tid; p < size; p += nt) {
+                const int i = dof[p];
+                if (i < 0) continue;
+                const int j = at[p];
+                const int q = sof[j];
+                if (q < 0) continue;
+                const bool v = cur[i].vert != 0;
+                const double lo = unord(slo[q]), hi = unord(shi[q]);
+                const double c0 = centre(j, v);
+                const double t = hi > lo ? (c0 - lo) / (hi - lo) : 0.5;
+                const double sz = v ? C.w[gid[j]] : C.h[gid[j]];
+                const double a = sta[q], bb = stb[q];
+                const double c = a + t * (bb - a);
+                const double lim = ref_max(a, bb - sz);
+                double np = c - 0.5 * sz;
+                np = np < a ? a : (lim < np ? lim : np);
+                (v ? sx : sy)[j] = np;
+            }
+            __syncthreads();
+            // L. children: low and high halves, next axis
+            for (int i = tid; i < ncur; i += nt) {
+                const SubDesc &d = cur[i];
+                if (!d.act) continue;
+                for (int side = 0; side < 2; ++side) {
+                    SubDesc &c = nxt[2 * d.rank + side];
+                    for (int q = 0; q < 4; ++q) c.box[q] = d.hbox[4 * side + q];
+                    c.b = side ? d.b + d.m : d.b;
+                    c.e = side ? d.e : d.b + d.m;
+                    c.level = d.level + 1;
+                    c.vert = d.vert ? 0 : 1;
+                }
+            }
+            if (tid == 0) {
+                s_ncur = 2 * nact;
+                s_maxlen = 0;
+                s_maxsteps = 0;
+            }
+            SubDesc *t = cur;
+            cur = nxt;
+            nxt = t;
+        }
+        __syncthreads();
+        if (s_fail) {
+            if (tid == 0) A.fail[task] = 1;
+        } else {
+            for (int j = tid; j < size; j += nt) {
+                C.x[gid[j]] = sx[j];
+                C.y[gid[j]] = sy[j];
+            }
+            if (tid == 0) A.fail[task] = 0;
+        }
+        __syncthreads();
     }
 }
 
@@ -735,6 +1712,16 @@ struct LalState {
     DevBuf<double> sa, sb, scap, sused;
     DevBuf<unsigned long long> slo, shi;
     DevBuf<double> overflow;
+    DevBuf<long long> pre, tile;
+    DevBuf<int32_t> sbeg;
+    DevBuf<SubTask> tasks;
+    DevBuf<int32_t> tfail;
+    DevBuf<SubDesc> sdesc;
+    DevBuf<double> sstrp;
+    DevBuf<unsigned long long> sstrlh;
+    bool subtree_attr = false;
+    // counters of the last ktg_lal call (ktg_lal_stats)
+    double stats[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 void free_lal(ktg_ctx *c) {
@@ -756,6 +1743,14 @@ void free_lal(ktg_ctx *c) {
     s->steps_tmp.release();
     s->slo.release();
     s->shi.release();
+    s->pre.release();
+    s->tile.release();
+    s->sbeg.release();
+    s->tasks.release();
+    s->tfail.release();
+    s->sdesc.release();
+    s->sstrp.release();
+    s->sstrlh.release();
     delete s;
     c->lal = nullptr;
 }
@@ -789,6 +1784,16 @@ int set_free_space(ktg_ctx *c, int64_t nrows, const double *rowy, const int64_t 
 }
 
 namespace {
+
+cudaError_t lal_sync(ktg_ctx *c) {
+    c->lal->stats[3] += 1;
+    return cudaStreamSynchronize(c->stream);
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 // ---- host side: clusters and growth exactly as the reference sums them ---------------
 
@@ -886,6 +1891,8 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         (rc = s->keys.ensure(c, n + 1)) || (rc = s->keys_tmp.ensure(c, n + 1)))
         return rc;
     KTG_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+    std::fill(s->stats, s->stats + 12, 0.0);
+    const double t_start = now_ms();
     CellsDev C{x, y, c->width, c->height, c->area};
     const GridDev G{c->origin_x, c->origin_y, c->dx, c->dy, nx, ny};
     Free F{s->d_rowy.p, s->d_rowspan.p, s->d_spans.p, s->d_obst.p,
@@ -893,6 +1900,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
     const HostGrid HG{nx, ny, &c->avail_host, c->density_limit};
     std::vector<double> occ(nbins);
     auto refresh = [&]() -> int {  // bins and occupancy of the current positions
+        const double t0 = now_ms();
         if (n > 0) {
             k_bins<<<blocks_for(n), kT, 0, c->stream>>>(C, n, G, s->binof.p);
             ++c->launches;
@@ -901,7 +1909,8 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         if (r2) return r2;
         KTG_CUDA(c, cudaMemcpyAsync(occ.data(), s->occ.p, sizeof(double) * nbins,
                                     cudaMemcpyDeviceToHost, c->stream));
-        KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+        KTG_CUDA(c, lal_sync(c));
+        s->stats[6] += now_ms() - t0;
         return KTG_OK;
     };
     if ((rc = refresh())) return rc;
@@ -914,10 +1923,71 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         return a[0] <= b[1] && b[0] <= a[1] && a[2] <= b[3] && b[2] <= a[3];
     };
     std::vector<std::array<int32_t, 4>> batch, batch_reach;
+    const int32_t stripe_extra =
+        64 + static_cast<int32_t>(std::min(1048576.0, std::ceil(4.0 / frac)));
+    const bool exact = c->area_shift >= 0 && c->lal_exact_sums != 0;
+    const double scale = exact ? std::ldexp(1.0, c->area_shift) : 1.0;
+    const double inv_scale = exact ? std::ldexp(1.0, -c->area_shift) : 1.0;
+
+    // pre[p] = fixed-point area of cell positions [0, p), p <= count.
+    auto fx_prefix = [&](int32_t count) -> int {
+        const int32_t tiles = std::max(1, (count + kScanTile - 1) / kScanTile);
+        int r2;
+        if ((r2 = s->pre.ensure(c, static_cast<int64_t>(count) + 1)) ||
+            (r2 = s->tile.ensure(c, tiles)))
+            return r2;
+        k_fx_tile_sums<<<tiles, kT, 0, c->stream>>>(s->cells.p, c->area, count, scale, s->tile.p);
+        k_fx_tile_scan<<<1, kT, 0, c->stream>>>(s->tile.p, tiles);
+        k_fx_prefix<<<tiles, kT, 0, c->stream>>>(s->cells.p, c->area, count, scale, s->tile.p,
+                                                 s->pre.p);
+        c->launches += 3;
+        KTG_CUDA(c, cudaGetLastError());
+        return KTG_OK;
+    };
+
+    // Blocks of at most kSub cells: one CTA each runs the rest of the
+    // bisection; failed[t] = 1 for a block left for the level-by-level path.
+    auto run_subtree = [&](const std::vector<SubTask> &tasks, std::vector<int32_t> &failed) -> int {
+        const int32_t nt = static_cast<int32_t>(tasks.size());
+        const int grid = std::max(1, std::min<int>(nt, c->num_sms));
+        const double t0 = now_ms();
+        int r2;
+        if ((r2 = s->tasks.ensure(c, nt)) || (r2 = s->tfail.ensure(c, nt)) ||
+            (r2 = s->sdesc.ensure(c, static_cast<int64_t>(grid) * 2 * kMaxSub)) ||
+            (r2 = s->sstrp.ensure(c, static_cast<int64_t>(grid) * 4 * kStripeCap)) ||
+            (r2 = s->sstrlh.ensure(c, static_cast<int64_t>(grid) * 2 * kStripeCap)))
+            return r2;
+        if (!s->subtree_attr) {
+            KTG_CUDA(c, cudaFuncSetAttribute(k_subtree, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(kSubSmem)));
+            s->subtree_attr = true;
+        }
+        KTG_CUDA(c, cudaMemcpyAsync(s->tasks.p, tasks.data(), sizeof(SubTask) * nt,
+                                    cudaMemcpyHostToDevice, c->stream));
+        SubArgs A{s->tasks.p, nt, s->tfail.p, s->cells.p, C, F, s->sdesc.p,
+                  s->sstrp.p, s->sstrlh.p, max_level, min_cells, stripe_extra, frac,
+                  c->density_limit, exact ? 1 : 0, scale, inv_scale};
+        k_subtree<<<grid, kSubThreads, kSubSmem, c->stream>>>(A);
+        ++c->launches;
+        KTG_CUDA(c, cudaGetLastError());
+        failed.assign(nt, 0);
+        KTG_CUDA(c, cudaMemcpyAsync(failed.data(), s->tfail.p, sizeof(int32_t) * nt,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        KTG_CUDA(c, lal_sync(c));
+        s->stats[2] += 1;
+        s->stats[4] += nt;
+        s->stats[8] += now_ms() - t0;
+        s->stats[10] += nt;
+        for (int32_t t = 0; t < nt; ++t) s->stats[11] += failed[t] != 0;
+        return KTG_OK;
+    };
 
     auto run_batch = [&]() -> int {
         const int32_t nreg = static_cast<int32_t>(batch.size());
         if (nreg == 0) return KTG_OK;
+        const double t0 = now_ms();
+        s->stats[0] += 1;
+        s->stats[1] += nreg;
         int r2;
         std::vector<int32_t> rects(4 * nreg);
         std::vector<double> box(4 * nreg), room(nreg);
@@ -940,9 +2010,9 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         std::vector<int32_t> cnt(nreg);
         KTG_CUDA(c, cudaMemcpyAsync(cnt.data(), s->cnt.p, sizeof(int32_t) * nreg,
                                     cudaMemcpyDeviceToHost, c->stream));
-        KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+        KTG_CUDA(c, lal_sync(c));
         // level-1 blocks: one per region
-        std::vector<int32_t> hb(nreg), he(nreg), hv(nreg, 1);
+        std::vector<int32_t> hb(nreg), he(nreg), hv(nreg, 1), hl(nreg, 1);
         int32_t run = 0;
         for (int32_t r = 0; r < nreg; ++r) {
             hb[r] = run;
@@ -960,20 +2030,48 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         ++c->launches;
         // host copies of the current level's blocks
         std::vector<double> hbox = box, hroom = room;
-        for (int32_t level = 1; level < max_level; ++level) {
-            // active blocks: more than min_cells cells
-            std::vector<int32_t> ab, ae, av;
+        for (;;) {
+            // blocks that split: more than min_cells cells, below max_level;
+            // small ones finish in the subtree kernel, the rest go level by level
+            std::vector<int32_t> ab, ae, av, al;
             std::vector<double> abox, aroom;
-            for (size_t k = 0; k < hb.size(); ++k) {
-                if (he[k] - hb[k] <= min_cells) continue;
+            std::vector<SubTask> tasks;
+            std::vector<size_t> task_src;
+            auto take = [&](size_t k) {
                 ab.push_back(hb[k]);
                 ae.push_back(he[k]);
                 av.push_back(hv[k]);
+                al.push_back(hl[k]);
                 for (int q = 0; q < 4; ++q) abox.push_back(hbox[4 * k + q]);
                 aroom.push_back(hroom[k]);
+            };
+            for (size_t k = 0; k < hb.size(); ++k) {
+                if (he[k] - hb[k] <= min_cells || hl[k] >= max_level) continue;
+                if (he[k] - hb[k] <= c->lal_subtree_cells) {
+                    SubTask t;
+                    for (int q = 0; q < 4; ++q) t.box[q] = hbox[4 * k + q];
+                    t.room = hroom[k];
+                    t.b = hb[k];
+                    t.e = he[k];
+                    t.level = hl[k];
+                    t.vert = hv[k];
+                    tasks.push_back(t);
+                    task_src.push_back(k);
+                } else {
+                    take(k);
+                }
+            }
+            if (!tasks.empty()) {
+                std::vector<int32_t> failed;
+                if ((r2 = run_subtree(tasks, failed))) return r2;
+                for (size_t t = 0; t < tasks.size(); ++t)
+                    if (failed[t]) take(task_src[t]);
             }
             const int32_t na = static_cast<int32_t>(ab.size());
             if (na == 0) break;
+            s->stats[2] += 1;
+            s->stats[4] += na;
+            s->stats[9] += 1;
             if ((r2 = s->lb.ensure(c, na)) || (r2 = s->le.ensure(c, na)) ||
                 (r2 = s->lvert.ensure(c, na)) || (r2 = s->lbox.ensure(c, 4 * na)) ||
                 (r2 = s->lroom.ensure(c, na)) || (r2 = s->m.ensure(c, na)) ||
@@ -1006,13 +2104,16 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             ++c->launches;
             if ((r2 = seg_sort(c, s->keys.p, s->keys_tmp.p, segs, s->seg.p))) return r2;
             k_keys_to_cells<<<gcell, kT, 0, c->stream>>>(L, s->keys.p, s->cells.p);
+            ++c->launches;
             // 2. areas, median, block profile bounds
-            k_block_split<<<blocks_for(na), kT, 0, c->stream>>>(L, C, F, s->cells.p);
-            c->launches += 2;
+            if (exact && (r2 = fx_prefix(run))) return r2;
+            k_block_split<<<blocks_for(na), kT, 0, c->stream>>>(L, C, F, s->cells.p,
+                                                              exact ? s->pre.p : nullptr, inv_scale);
+            ++c->launches;
             std::vector<int64_t> bound(2 * na);
             KTG_CUDA(c, cudaMemcpyAsync(bound.data(), s->bound.p, sizeof(int64_t) * 2 * na,
                                         cudaMemcpyDeviceToHost, c->stream));
-            KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+            KTG_CUDA(c, lal_sync(c));
             std::vector<int64_t> soff(na), eoff(na);
             int64_t st = 0, ed = 0;
             for (int32_t k = 0; k < na; ++k) {
@@ -1031,7 +2132,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             std::vector<int64_t> nst(na);
             KTG_CUDA(c, cudaMemcpyAsync(nst.data(), s->nsteps.p, sizeof(int64_t) * na,
                                         cudaMemcpyDeviceToHost, c->stream));
-            KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+            KTG_CUDA(c, lal_sync(c));
             std::vector<int64_t> ssegs;
             for (int32_t k = 0; k < na; ++k) {
                 ssegs.push_back(soff[k]);
@@ -1045,7 +2146,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             std::vector<int64_t> hbound(4 * na);
             KTG_CUDA(c, cudaMemcpyAsync(hbound.data(), s->hbound.p, sizeof(int64_t) * 4 * na,
                                         cudaMemcpyDeviceToHost, c->stream));
-            KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+            KTG_CUDA(c, lal_sync(c));
             std::vector<int64_t> hsoff(2 * na), heoff(2 * na), hcap(2 * na), stoff(2 * na);
             st = ed = 0;
             int64_t stripes = 0;
@@ -1054,7 +2155,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
                 st += hbound[2 * h];
                 heoff[h] = ed;
                 // pe: the profile edges; pp: the prefix, then up to `edges` cuts
-                const int64_t edges = hbound[2 * h + 1];
+                const int64_t edges = hbound[2 * h + 1] + stripe_extra;
                 hcap[h] = edges;
                 ed += 2 * edges;
                 stoff[h] = stripes;
@@ -1077,7 +2178,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             std::vector<int64_t> hnst(2 * na);
             KTG_CUDA(c, cudaMemcpyAsync(hnst.data(), s->hnsteps.p, sizeof(int64_t) * 2 * na,
                                         cudaMemcpyDeviceToHost, c->stream));
-            KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+            KTG_CUDA(c, lal_sync(c));
             ssegs.clear();
             for (int32_t h = 0; h < 2 * na; ++h) {
                 ssegs.push_back(hsoff[h]);
@@ -1098,7 +2199,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             std::vector<double> cuth(na);
             KTG_CUDA(c, cudaMemcpyAsync(cuth.data(), s->cut.p, sizeof(double) * na,
                                         cudaMemcpyDeviceToHost, c->stream));
-            KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+            KTG_CUDA(c, lal_sync(c));
             std::vector<int64_t> fsegs;
             for (int32_t k = 0; k < na; ++k) {
                 fsegs.push_back(ab[k]);
@@ -1108,19 +2209,32 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             }
             if ((r2 = seg_sort(c, s->keys.p, s->keys_tmp.p, fsegs, s->seg.p))) return r2;
             k_keys_to_cells<<<gcell, kT, 0, c->stream>>>(L, s->keys.p, s->cells.p);
-            k_fill<<<blocks_for(2 * na), kT, 0, c->stream>>>(L, C, s->cells.p, S, s->stripe_of.p);
+            ++c->launches;
+            if (exact) {
+                if ((r2 = fx_prefix(run)) || (r2 = s->sbeg.ensure(c, stripes + 1))) return r2;
+                k_fill_fx<<<blocks_for(2 * na), kT, 0, c->stream>>>(L, S, s->pre.p, inv_scale,
+                                                                   s->sbeg.p);
+                k_assign_fx<<<gcell, kT, 0, c->stream>>>(L, s->cells.p, S, s->sbeg.p,
+                                                         s->stripe_of.p);
+                c->launches += 2;
+            } else {
+                k_fill<<<blocks_for(2 * na), kT, 0, c->stream>>>(L, C, s->cells.p, S,
+                                                                 s->stripe_of.p);
+                ++c->launches;
+            }
             k_stripe_minmax<<<gcell, kT, 0, c->stream>>>(L, C, s->cells.p, S, s->stripe_of.p);
             k_new_pos<<<gcell, kT, 0, c->stream>>>(L, C, s->cells.p, S, s->stripe_of.p);
-            c->launches += 4;
+            c->launches += 2;
             KTG_CUDA(c, cudaGetLastError());
             // children
             std::vector<double> halfbox(8 * na);
             KTG_CUDA(c, cudaMemcpyAsync(halfbox.data(), s->half_box.p, sizeof(double) * 8 * na,
                                         cudaMemcpyDeviceToHost, c->stream));
-            KTG_CUDA(c, cudaStreamSynchronize(c->stream));
+            KTG_CUDA(c, lal_sync(c));
             hb.clear();
             he.clear();
             hv.clear();
+            hl.clear();
             hbox.clear();
             hroom.clear();
             for (int32_t k = 0; k < na; ++k) {
@@ -1128,6 +2242,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
                     hb.push_back(side ? ab[k] + mh[k] : ab[k]);
                     he.push_back(side ? ae[k] : ab[k] + mh[k]);
                     hv.push_back(av[k] ? 0 : 1);
+                    hl.push_back(al[k] + 1);
                     for (int q = 0; q < 4; ++q) hbox.push_back(halfbox[8 * k + 4 * side + q]);
                     hroom.push_back(aroom[k]);
                 }
@@ -1135,6 +2250,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         }
         batch.clear();
         batch_reach.clear();
+        s->stats[5] += now_ms() - t0;
         return refresh();
     };
 
@@ -1158,6 +2274,12 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         ++c->launches;
     }
     KTG_CUDA(c, cudaGetLastError());
+    s->stats[7] = now_ms() - t_start;
+    return KTG_OK;
+}
+
+int lal_stats(ktg_ctx *c, double *out, int count) {
+    for (int k = 0; k < count && k < 12; ++k) out[k] = c->lal ? c->lal->stats[k] : 0.0;
     return KTG_OK;
 }
 

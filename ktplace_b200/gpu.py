@@ -320,6 +320,13 @@ class Context:
                                      stripe_area_fraction))
         return x, y
 
+    def lal_stats(self) -> dict:
+        out = np.zeros(12)
+        self._check(self.lib.ktg_lal_stats(self.h, _ptr(out), 12))
+        keys = ("batches", "regions", "levels", "syncs", "blocks", "ms_bisect", "ms_refresh",
+                "ms_total", "ms_subtree", "big_levels", "subtree_blocks", "subtree_handed_back")
+        return dict(zip(keys, out.tolist()))
+
     def lal_dev(self, x, y, max_level: int = 20, min_cells_to_split: int = 4,
                 stripe_area_fraction: float = 0.1):
         """In place on device tensors x, y."""
