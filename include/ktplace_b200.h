@@ -438,13 +438,15 @@ int ktg_set_option(ktg_ctx *ctx, const char *key, int64_t value);
  * points). */
 int64_t ktg_launch_count(const ktg_ctx *ctx);
 
-/* Counters of the last ktg_lal call, up to `count` (at most 12) of:
+/* Counters of the last ktg_lal call, up to `count` (at most 16) of:
  * batches, regions, bisection rounds (one-CTA launches and level-by-level
  * levels, summed over batches), host synchronisations, blocks (summed over
  * rounds), ms in the batches' bisection, ms in the occupancy refreshes, ms
  * in total, ms in the one-CTA subtree launches, level-by-level levels,
- * one-CTA blocks, one-CTA blocks handed back (host wall clock). No
- * reference counterpart. */
+ * one-CTA blocks, one-CTA blocks handed back, and of those the ones with too
+ * many cells or obstacles, too many sub-blocks at one level, a full sort
+ * buffer, full stripe storage (host wall clock). No reference
+ * counterpart. */
 int ktg_lal_stats(ktg_ctx *ctx, double *out, int32_t count);
 
 /* Test of the bounded device waits: a cooperative launch in which one block

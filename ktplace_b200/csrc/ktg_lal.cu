@@ -232,8 +232,13 @@ __device__ __forceinline__ int32_t first_row(const Free &F, double ly) {
 __device__ __forceinline__ void profile_bound(const Free &F, const double *box, bool vertical,
                                               int64_t &steps, int64_t &edges) {
     const int32_t r0 = first_row(F, box[1]);
-    int32_t r1 = r0;
-    while (r1 < F.R && F.rowy[2 * r1] < box[3]) ++r1;
+    int32_t lo = r0, hi = F.R;  // first row from r0 with y start >= uy
+    while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (F.rowy[2 * mid] < box[3]) lo = mid + 1;
+        else hi = mid;
+    }
+    const int32_t r1 = lo;
     const int64_t sp = F.rowspan[r1] - F.rowspan[r0];
     steps = vertical ? 2 * sp : 0;
     edges = (vertical ? 2 * sp : 2 * static_cast<int64_t>(r1 - r0)) + 2;
@@ -253,44 +258,39 @@ __device__ __forceinline__ int64_t first_span(const Free &F, int32_t r, double x
     return lo;
 }
 
-// Vertical profile steps of `box` (unsorted), handed to sink(at, dh) in
-// row and span order; returns the count. Only spans overlapping the box's x
-// range can give a step (z > a), so each row starts at its first such span.
+// Rows [r0, r1) a box's row loops visit (rows sorted by y start).
+__device__ __forceinline__ void box_rows(const Free &F, const double *box, int32_t &r0,
+                                         int32_t &r1) {
+    r0 = first_row(F, box[1]);
+    int32_t lo = r0, hi = F.R;
+    while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (F.rowy[2 * mid] < box[3]) lo = mid + 1;
+        else hi = mid;
+    }
+    r1 = lo;
+}
+
+// Steps of row r inside box (emit_steps restricted to one row), written
+// through sink(k + i, x, dh); returns their count.
 template <typename Sink>
-__device__ int64_t emit_steps(const Free &F, const double *box, Sink sink) {
+__device__ __forceinline__ int64_t row_steps(const Free &F, int32_t r, const double *box, Sink sink,
+                                             int64_t k) {
     const double lx = box[0], ly = box[1], ux = box[2], uy = box[3];
-    int64_t k = 0;
-    for (int32_t r = first_row(F, ly); r < F.R && F.rowy[2 * r] < uy; ++r) {
-        const double h = ref_min(uy, F.rowy[2 * r + 1]) - ref_max(ly, F.rowy[2 * r]);
-        if (!(h > 0.0)) continue;
-        const int64_t end = F.rowspan[r + 1];
-        for (int64_t s = first_span(F, r, lx); s < end && F.spans[2 * s] < ux; ++s) {
-            const double a = ref_max(F.spans[2 * s], lx);
-            const double z = ref_min(F.spans[2 * s + 1], ux);
-            if (z > a) {
-                sink(k, a, h);
-                sink(k + 1, z, -h);
-                k += 2;
-            }
+    const double h = ref_min(uy, F.rowy[2 * r + 1]) - ref_max(ly, F.rowy[2 * r]);
+    if (!(h > 0.0)) return 0;
+    const int64_t end = F.rowspan[r + 1];
+    int64_t c = 0;
+    for (int64_t s = first_span(F, r, lx); s < end && F.spans[2 * s] < ux; ++s) {
+        const double a = ref_max(F.spans[2 * s], lx);
+        const double z = ref_min(F.spans[2 * s + 1], ux);
+        if (z > a) {
+            sink(k + c, a, h);
+            sink(k + c + 1, z, -h);
+            c += 2;
         }
     }
-    return k;
-}
-
-__device__ int64_t profile_steps(const Free &F, const double *box, Key *out) {
-    return emit_steps(F, box, [&](int64_t k, double at, double dh) { out[k] = Key{ord(at), ord(dh)}; });
-}
-
-__device__ int64_t count_steps(const Free &F, const double *box) {
-    return emit_steps(F, box, [](int64_t, double, double) {});
-}
-
-// Rows overlapping `box` (the horizontal profile's extent).
-__device__ __forceinline__ int32_t count_rows(const Free &F, const double *box) {
-    const int32_t r0 = first_row(F, box[1]);
-    int32_t r1 = r0;
-    while (r1 < F.R && F.rowy[2 * r1] < box[3]) ++r1;
-    return r1 - r0;
+    return c;
 }
 
 // AxisProfile (simpl_grid.h:29-65, getProfile :179-232) stored as edges /
@@ -378,17 +378,6 @@ __device__ int64_t build_profile_from(const Free &F, const double *box, bool ver
         n = 2;
     }
     return n;
-}
-
-__device__ int64_t build_profile(const Free &F, const double *box, bool vertical, const Key *steps,
-                                 int64_t nsteps, double *e, double *p) {
-    return build_profile_from(
-        F, box, vertical,
-        [&](int64_t k, double &at, double &dh) {
-            at = unord(steps[k].a);
-            dh = unord(steps[k].b);
-        },
-        nsteps, e, p);
 }
 
 // getStripes (simpl_lal.cc:266-312) for one half box, then the stable sort
@@ -678,55 +667,7 @@ __global__ void k_block_split(Level L, CellsDev C, Free F, const int32_t *cells,
     L.bound[2 * blk + 1] = ed;
 }
 
-__global__ void k_block_steps(Level L, Free F, const int64_t *soff, Key *steps, int64_t *nsteps) {
-    const int32_t blk = blockIdx.x * blockDim.x + threadIdx.x;
-    if (blk >= L.na) return;
-    nsteps[blk] = L.vert[blk] ? profile_steps(F, L.box + 4 * blk, steps + soff[blk]) : 0;
-}
-
 // One thread per block: profile, cutline, half boxes, half bounds.
-__global__ void k_block_cut(Level L, Free F, const int64_t *soff, const Key *steps,
-                            const int64_t *nsteps, const int64_t *eoff, double *pe, double *pp,
-                            int64_t *hbound) {
-    const int32_t blk = blockIdx.x * blockDim.x + threadIdx.x;
-    if (blk >= L.na) return;
-    const bool v = L.vert[blk] != 0;
-    const double *box = L.box + 4 * blk;
-    double *e = pe + eoff[blk], *p = pp + eoff[blk];
-    const int64_t n = build_profile(F, box, v, steps + soff[blk], nsteps[blk], e, p);
-    const Prof room{e, p, n};
-    const double cell_area = L.cut[blk];
-    const double share = cell_area > 0.0 ? L.low_area[blk] / cell_area : 0.5;
-    const double lo = v ? box[0] : box[1], hi = v ? box[2] : box[3];
-    const double cut = room.total() > 0.0 ? room.coordinate_at(share * room.total())
-                                          : lo + share * (hi - lo);
-    L.cut[blk] = cut;
-    double *lb = L.half_box + 8 * blk, *hb = lb + 4;
-    for (int k = 0; k < 4; ++k) lb[k] = hb[k] = box[k];
-    (v ? lb[2] : lb[3]) = cut;
-    (v ? hb[0] : hb[1]) = cut;
-    for (int side = 0; side < 2; ++side) {
-        const double *bx = side ? hb : lb;
-        int64_t st, ed;
-        profile_bound(F, bx, v, st, ed);
-        int64_t k = 0;  // obstacles overlapping the half box
-        for (int32_t o = 0; o < F.K; ++o) {
-            const double *ob = F.obst + 4 * o;
-            if (ob[2] <= bx[0] || ob[0] >= bx[2] || ob[3] <= bx[1] || ob[1] >= bx[3]) continue;
-            ++k;
-        }
-        hbound[4 * blk + 2 * side] = st;
-        hbound[4 * blk + 2 * side + 1] = ed + 2 * k + 2;  // profile edges, obstacle cuts
-    }
-}
-
-__global__ void k_half_steps(Level L, Free F, const int64_t *soff, Key *steps, int64_t *nsteps) {
-    const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= 2 * L.na) return;
-    const int32_t blk = h >> 1;
-    nsteps[h] = L.vert[blk] ? profile_steps(F, L.half_box + 4 * h, steps + soff[h]) : 0;
-}
-
 struct Stripes {
     int64_t *off;    // [2 na] first stripe of the half (into the arrays below)
     int32_t *count;  // [2 na]
@@ -734,37 +675,195 @@ struct Stripes {
     unsigned long long *lo, *hi;
 };
 
-// One thread per half: profile, stripes (getStripes, simpl_lal.cc:265-308),
-// ordered by distance from the cut (stable, farthest first).
-__global__ void k_half_stripes(Level L, Free F, const int64_t *soff, const Key *steps,
-                               const int64_t *nsteps, const int64_t *eoff, double *pe, double *pp,
-                               int64_t *cap_over, double frac, double limit_density, Stripes S,
-                               int *status) {
-    const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= 2 * L.na) return;
-    const int32_t blk = h >> 1;
-    const int side = h & 1;
+// ---- one CTA per block (or half) for the level-by-level path ------------------------
+//
+// Blocks too large for the one-CTA subtree have die-sized boxes: their row
+// loops are split over the CTA's threads and the profile is built by thread 0
+// from chunks staged in shared memory (the order of its sums is the
+// reference's).
+
+constexpr int kStage = 1024;
+
+// Builds the profile of `box` into e/p (global). Returns the edge count on
+// thread 0.
+__device__ int64_t cta_build_profile(const Free &F, const double *box, bool v, const Key *steps,
+                                     int64_t nsteps, double *e, double *p, double *stage) {
+    const double lx = box[0], ly = box[1], ux = box[2], uy = box[3];
+    const double lo = v ? lx : ly, hi = v ? ux : uy;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int64_t n = 1;
+    double elast = lo, plast = 0.0, height = 0.0;
+    auto extend = [&](double to, double area) {
+        if (to > elast) {
+            plast = plast + area;
+            elast = to;
+            e[n] = to;
+            p[n] = plast;
+            ++n;
+        }
+    };
+    if (tid == 0) {
+        e[0] = lo;
+        p[0] = 0.0;
+    }
+    if (v) {
+        for (int64_t c0 = 0; c0 < nsteps; c0 += kStage) {
+            const int cnt = static_cast<int>(nsteps - c0 < kStage ? nsteps - c0 : kStage);
+            for (int i = tid; i < cnt; i += nt) {
+                stage[2 * i] = unord(steps[c0 + i].a);
+                stage[2 * i + 1] = unord(steps[c0 + i].b);
+            }
+            __syncthreads();
+            if (tid == 0)
+                for (int i = 0; i < cnt; ++i) {
+                    const double at = stage[2 * i], dh = stage[2 * i + 1];
+                    extend(at, height * (at - elast));
+                    height += dh;
+                }
+            __syncthreads();
+        }
+    } else {
+        int32_t r0, r1;
+        box_rows(F, box, r0, r1);
+        for (int32_t c0 = r0; c0 < r1; c0 += kStage) {
+            const int cnt = min(kStage, r1 - c0);
+            for (int i = tid; i < cnt; i += nt) {  // Row::getLength(b.getX())
+                const int32_t r = c0 + i;
+                double total = 0.0;
+                const int64_t end = F.rowspan[r + 1];
+                for (int64_t q = first_span(F, r, lx); q < end && F.spans[2 * q] < ux; ++q)
+                    total += ref_max(0.0, ref_min(ux, F.spans[2 * q + 1]) - ref_max(lx, F.spans[2 * q]));
+                stage[i] = total;
+            }
+            __syncthreads();
+            if (tid == 0)
+                for (int i = 0; i < cnt; ++i) {
+                    const int32_t r = c0 + i;
+                    const double a = ref_max(lo, F.rowy[2 * r]);
+                    const double z = ref_min(hi, F.rowy[2 * r + 1]);
+                    if (z > a) {
+                        extend(a, 0.0);
+                        extend(z, stage[i] * (z - a));
+                    }
+                }
+            __syncthreads();
+        }
+    }
+    if (tid == 0) {
+        extend(hi, 0.0);
+        if (n == 1) {
+            e[1] = hi;
+            p[1] = 0.0;
+            n = 2;
+        }
+    }
+    return n;
+}
+
+// Profile steps of each block (half = 0) or half box (half = 1), one CTA
+// each, rows split over the threads.
+__global__ void __launch_bounds__(kT) k_steps_cta(Level L, Free F, int half, const int64_t *soff,
+                                                  Key *steps, int64_t *nsteps) {
+    const int item = blockIdx.x;
+    const int blk = half ? item >> 1 : item;
+    const double *box = half ? L.half_box + 4 * item : L.box + 4 * item;
+    if (!L.vert[blk]) {
+        if (threadIdx.x == 0) nsteps[item] = 0;
+        return;
+    }
+    int32_t r0, r1;
+    box_rows(F, box, r0, r1);
+    long long c = 0;
+    for (int32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+        c += row_steps(F, r, box, [](int64_t, double, double) {}, 0);
+    long long total;
+    int64_t k = block_excl64(c, total);
+    Key *out = steps + soff[item];
+    auto sink = [&](int64_t q, double x, double dh) { out[q] = Key{ord(x), ord(dh)}; };
+    for (int32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) k += row_steps(F, r, box, sink, k);
+    if (threadIdx.x == 0) nsteps[item] = total;
+}
+
+// One CTA per block: profile, cutline, half boxes, half bounds.
+__global__ void __launch_bounds__(kT) k_block_cut_cta(Level L, Free F, const int64_t *soff,
+                                                      const Key *steps, const int64_t *nsteps,
+                                                      const int64_t *eoff, double *pe, double *pp,
+                                                      int64_t *hbound) {
+    __shared__ double stage[2 * kStage];
+    const int blk = blockIdx.x;
+    const bool v = L.vert[blk] != 0;
+    const double *box = L.box + 4 * blk;
+    double *e = pe + eoff[blk], *p = pp + eoff[blk];
+    const int64_t n = cta_build_profile(F, box, v, steps + soff[blk], nsteps[blk], e, p, stage);
+    if (threadIdx.x == 0) {
+        const Prof room{e, p, n};
+        const double cell_area = L.cut[blk];
+        const double share = cell_area > 0.0 ? L.low_area[blk] / cell_area : 0.5;
+        const double lo = v ? box[0] : box[1], hi = v ? box[2] : box[3];
+        const double cut = room.total() > 0.0 ? room.coordinate_at(share * room.total())
+                                              : lo + share * (hi - lo);
+        L.cut[blk] = cut;
+        double *lb = L.half_box + 8 * blk, *hb = lb + 4;
+        for (int k = 0; k < 4; ++k) lb[k] = hb[k] = box[k];
+        (v ? lb[2] : lb[3]) = cut;
+        (v ? hb[0] : hb[1]) = cut;
+    }
+    __syncthreads();
+    for (int side = 0; side < 2; ++side) {
+        const double *bx = L.half_box + 8 * blk + 4 * side;
+        long long k = 0;  // obstacles overlapping the half box
+        for (int32_t o = threadIdx.x; o < F.K; o += blockDim.x) {
+            const double *ob = F.obst + 4 * o;
+            if (ob[2] <= bx[0] || ob[0] >= bx[2] || ob[3] <= bx[1] || ob[1] >= bx[3]) continue;
+            ++k;
+        }
+        long long total;
+        block_excl64(k, total);
+        if (threadIdx.x == 0) {
+            int64_t st, ed;
+            profile_bound(F, bx, v, st, ed);
+            hbound[4 * blk + 2 * side] = st;
+            hbound[4 * blk + 2 * side + 1] = ed + 2 * total + 2;  // profile edges, obstacle cuts
+        }
+    }
+}
+
+// One CTA per half: profile, stripes (getStripes), fill state.
+__global__ void __launch_bounds__(kT) k_half_stripes_cta(Level L, Free F, const int64_t *soff,
+                                                         const Key *steps, const int64_t *nsteps,
+                                                         const int64_t *eoff, double *pe, double *pp,
+                                                         const int64_t *cap_over, double frac,
+                                                         double limit_density, Stripes S,
+                                                         int *status) {
+    __shared__ double stage[2 * kStage];
+    __shared__ long long s_ns;
+    const int h = blockIdx.x;
+    const int blk = h >> 1, side = h & 1;
     const bool v = L.vert[blk] != 0;
     const double *box = L.half_box + 4 * h;
     double *e = pe + eoff[h], *p = pp + eoff[h];
-    const int64_t n = build_profile(F, box, v, steps + soff[h], nsteps[h], e, p);
-    const Prof room{e, p, n};
-    const double cell_area = side ? L.high_area[blk] : L.low_area[blk];
+    const int64_t n = cta_build_profile(F, box, v, steps + soff[h], nsteps[h], e, p, stage);
     const int64_t so = S.off[h];
-    // cuts live after the profile in the same scratch
-    int64_t ns = make_stripes(room, box, v, cell_area, L.room[blk], frac, limit_density, F.obst,
-                              F.K, L.cut[blk], side == 0, p + n, cap_over[h], S.a + so,
-                              S.b + so, S.cap + so);
-    if (ns < 0) {
-        atomicCAS(status, kStatusOk, kStatusCapacity);
-        ns = 0;
+    if (threadIdx.x == 0) {
+        const Prof room{e, p, n};
+        const double cell_area = side ? L.high_area[blk] : L.low_area[blk];
+        // cuts live after the profile in the same scratch
+        int64_t ns = make_stripes(room, box, v, cell_area, L.room[blk], frac, limit_density,
+                                  F.obst, F.K, L.cut[blk], side == 0, p + n, cap_over[h],
+                                  S.a + so, S.b + so, S.cap + so);
+        if (ns < 0) {
+            atomicCAS(status, kStatusOk, kStatusCapacity);
+            ns = 0;
+        }
+        S.count[h] = static_cast<int32_t>(ns);
+        s_ns = ns;
     }
-    for (int64_t s = 0; s < ns; ++s) {
-        S.used[so + s] = 0.0;
-        S.lo[so + s] = ~0ull;
-        S.hi[so + s] = 0ull;
+    __syncthreads();
+    for (int64_t q = threadIdx.x; q < s_ns; q += blockDim.x) {
+        S.used[so + q] = 0.0;
+        S.lo[so + q] = ~0ull;
+        S.hi[so + q] = 0ull;
     }
-    S.count[h] = static_cast<int32_t>(ns);
 }
 
 __global__ void k_fill_keys(Level L, CellsDev C, const int32_t *cells, Key *keys) {
@@ -921,7 +1020,7 @@ constexpr size_t kSubSmem = sizeof(unsigned long long) * 2 * kSortCap +
                             sizeof(double) * (3 * kSub + 4 * kObstLocal) +
                             sizeof(double) * (2 * kRowsLocal + 2 * kSpansLocal) +
                             sizeof(int64_t) * (kRowsLocal + 2) +
-                            sizeof(int32_t) * (3 * kSub + 2 * kMaxSub) + sizeof(int16_t) * kSub;
+                            sizeof(int32_t) * (3 * kSub + 2 * kMaxSub + 2) + sizeof(int16_t) * kSub;
 
 struct SubTask {
     double box[4];
@@ -960,36 +1059,6 @@ __device__ __forceinline__ bool sub_less(uint32_t a2, unsigned long long a0, uns
     return a2 < b2 || (a2 == b2 && (a0 < b0 || (a0 == b0 && a1 < b1)));
 }
 
-// Bitonic sort of entries [0, n) of the CTA buffer (padded to the power of
-// two P >= n with entries above every key).
-__device__ void cta_sort(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int n) {
-    int P = 1;
-    while (P < n) P <<= 1;
-    for (int i = n + threadIdx.x; i < P; i += blockDim.x) {
-        k2[i] = 0xffffffffu;
-        k0[i] = ~0ull;
-        k1[i] = ~0ull;
-    }
-    __syncthreads();
-    if (n <= 1) return;
-    for (int k = 2; k <= P; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
-                const int i = 2 * j * (t / j) + (t % j);
-                const int q = i + j;
-                const bool up = (i & k) == 0;
-                const uint32_t a2 = k2[i], b2 = k2[q];
-                const unsigned long long a0 = k0[i], b0 = k0[q], a1 = k1[i], b1 = k1[q];
-                if (sub_less(b2, b0, b1, a2, a0, a1) == up) {
-                    k2[i] = b2; k0[i] = b0; k1[i] = b1;
-                    k2[q] = a2; k0[q] = a0; k1[q] = a1;
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
 // Stable insertion sort of entries [b, e) by one thread.
 __device__ void seg_sort1(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int b,
                           int e) {
@@ -1007,6 +1076,77 @@ __device__ void seg_sort1(unsigned long long *k0, unsigned long long *k1, uint32
         k1[j + 1] = a1;
         k2[j + 1] = a2;
     }
+}
+
+// In-place sort of entries [b, b + n) by `nthreads` cooperating threads
+// (index `me`), for any n: every merge of two sorted halves starts with the
+// mirrored comparators (i, k - 1 - i) and continues with half-cleaners, all
+// ascending, so positions past n act as +inf and their comparators are
+// skipped. `sync` separates the steps (a warp or the whole block).
+template <typename Sync>
+__device__ void net_sort(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int b, int n,
+                         int me, int nthreads, Sync sync) {
+    if (n <= 1) return;
+    int P = 1;
+    while (P < n) P <<= 1;
+    auto cas = [&](int i, int q) {
+        const uint32_t a2 = k2[b + i], b2 = k2[b + q];
+        const unsigned long long a0 = k0[b + i], b0 = k0[b + q], a1 = k1[b + i], b1 = k1[b + q];
+        if (sub_less(b2, b0, b1, a2, a0, a1)) {
+            k2[b + i] = b2; k0[b + i] = b0; k1[b + i] = b1;
+            k2[b + q] = a2; k0[b + q] = a0; k1[b + q] = a1;
+        }
+    };
+    for (int k = 2; k <= P; k <<= 1) {
+        const int h = k >> 1;
+        for (int t = me; t < (P >> 1); t += nthreads) {
+            const int base = (t / h) * k, off = t % h;
+            const int q = base + k - 1 - off;
+            if (q < n) cas(base + off, q);
+        }
+        sync();
+        for (int j = k >> 2; j > 0; j >>= 1) {
+            for (int t = me; t < (P >> 1); t += nthreads) {
+                const int i = 2 * j * (t / j) + (t % j);
+                if (i + j < n) cas(i, i + j);
+            }
+            sync();
+        }
+    }
+}
+
+__device__ __forceinline__ void named_barrier(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Sorts each segment [b, e) = seg(g) of g < nseg: the whole block for one
+// segment, equal groups of warps (each on its own named barrier) for up to
+// 15, one warp per segment beyond. Ends with a block barrier.
+template <typename Seg>
+__device__ void sort_segments(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int nseg,
+                              Seg seg) {
+    const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (nseg == 1) {
+        int b, e;
+        seg(0, b, e);
+        net_sort(k0, k1, k2, b, e - b, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+    } else if (nseg < 16 && nw / nseg >= 2) {
+        const int W = nw / nseg;  // warps per group
+        const int g = w / W;
+        if (g < nseg) {
+            int b, e;
+            seg(g, b, e);
+            const int me = (w - g * W) * 32 + lane, n = W * 32;
+            net_sort(k0, k1, k2, b, e - b, me, n, [g, n] { named_barrier(1 + g, n); });
+        }
+    } else {
+        for (int g = w; g < nseg; g += nw) {
+            int b, e;
+            seg(g, b, e);
+            net_sort(k0, k1, k2, b, e - b, lane, 32, [] { __syncwarp(); });
+        }
+    }
+    __syncthreads();
 }
 
 // Exclusive scan of buf[0, n) in place; returns the total to every thread.
@@ -1079,17 +1219,6 @@ __device__ void cta_prefix64(const int32_t *at, const double *sa, int n, double 
     __syncthreads();
 }
 
-// Index of the sub-block holding position p: the last with b <= p.
-__device__ __forceinline__ int find_desc(const SubDesc *cur, int ncur, int p) {
-    int lo = 0, hi = ncur;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (cur[mid].b <= p) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
 // A region of the sort buffer holding a profile: two leading pads, then the
 // sorted steps (vertical) or nothing (horizontal); the profile is written
 // over it in place (edge n lands at slot n, the step read last sits at slot
@@ -1108,21 +1237,147 @@ __device__ int64_t build_profile_inplace(const Free &F, const double *box, bool 
         nsteps, e, p);
 }
 
-// Writes a profile region: pads over [o, o + len), then the box's steps
-// from o + 2 (vertical).
-__device__ void emit_region(const Free &F, const double *box, bool v, uint32_t tag,
-                            unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int o,
-                            int len) {
-    for (int q = 0; q < len; ++q) {
+// A team of T lanes (a power of two up to 32, aligned inside a warp) that
+// works on one sub-block: few sub-blocks at a level get wide teams, many get
+// one thread each. Row loops are split over the lanes; everything whose
+// floating-point order matters runs on lane 0.
+struct Team {
+    int T, lane, team, nteams;
+    unsigned mask;
+    __device__ explicit Team(int items) {
+        const int per = kSubThreads / max(items, 1);
+        T = per >= 32 ? 32 : per >= 16 ? 16 : per >= 8 ? 8 : per >= 4 ? 4 : per >= 2 ? 2 : 1;
+        lane = threadIdx.x & (T - 1);
+        team = threadIdx.x / T;
+        nteams = blockDim.x / T;
+        const int wl = threadIdx.x & 31;
+        mask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << (wl & ~(T - 1)));
+    }
+    template <typename V>
+    __device__ V sum(V v) const {
+        for (int o = T >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+        return v;
+    }
+    template <typename V>
+    __device__ V excl(V v) const {
+        V inc = v;
+        for (int o = 1; o < T; o <<= 1) {
+            const V t = __shfl_up_sync(mask, inc, o, T);
+            if (lane >= o) inc += t;
+        }
+        return inc - v;
+    }
+    template <typename V>
+    __device__ V bcast(V v) const { return __shfl_sync(mask, v, 0, T); }
+    __device__ void sync() const { __syncwarp(mask); }
+};
+
+__device__ int32_t team_count_steps(const Team &tm, const Free &F, const double *box) {
+    int32_t r0, r1;
+    box_rows(F, box, r0, r1);
+    int32_t c = 0;
+    for (int32_t r = r0 + tm.lane; r < r1; r += tm.T)
+        c += static_cast<int32_t>(row_steps(F, r, box, [](int64_t, double, double) {}, 0));
+    return tm.sum(c);
+}
+
+__device__ int32_t team_count_obstacles(const Team &tm, const Free &F, const double *bx) {
+    int32_t k = 0;
+    for (int32_t ob = tm.lane; ob < F.K; ob += tm.T) {
+        const double *q = F.obst + 4 * ob;
+        if (q[2] <= bx[0] || q[0] >= bx[2] || q[3] <= bx[1] || q[1] >= bx[3]) continue;
+        ++k;
+    }
+    return tm.sum(k);
+}
+
+// Writes a profile region: pads over [o, o + len), then (vertical) the box's
+// steps from o + 2, the rows split over the team (step order inside the
+// region does not matter: it is sorted next).
+__device__ void team_emit_region(const Team &tm, const Free &F, const double *box, bool v,
+                                 uint32_t tag, unsigned long long *k0, unsigned long long *k1,
+                                 uint32_t *k2, int o, int len) {
+    for (int q = tm.lane; q < len; q += tm.T) {
         k2[o + q] = tag;
         k0[o + q] = 0ull;
         k1[o + q] = 0ull;
     }
-    if (v)
-        emit_steps(F, box, [&](int64_t k, double x, double dh) {
-            k0[o + 2 + k] = ord(x);
-            k1[o + 2 + k] = ord(dh);
-        });
+    tm.sync();
+    if (!v) return;
+    int32_t r0, r1;
+    box_rows(F, box, r0, r1);
+    int32_t c = 0;
+    for (int32_t r = r0 + tm.lane; r < r1; r += tm.T)
+        c += static_cast<int32_t>(row_steps(F, r, box, [](int64_t, double, double) {}, 0));
+    int64_t k = o + 2 + tm.excl(c);
+    auto sink = [&](int64_t q, double x, double dh) {
+        k0[q] = ord(x);
+        k1[q] = ord(dh);
+    };
+    for (int32_t r = r0 + tm.lane; r < r1; r += tm.T) k += row_steps(F, r, box, sink, k);
+    tm.sync();
+}
+
+// build_profile_inplace with a team: horizontal boxes get their per-row
+// lengths (Row::getLength, each row's spans summed in order by one lane)
+// from the lanes first, parked at the top of the region (slots the profile
+// reaches only after it has read them); the profile itself is built by lane
+// 0. Returns the edge count to every lane.
+__device__ int64_t team_build_profile(const Team &tm, const Free &F, const double *box, bool v,
+                                      unsigned long long *k0, unsigned long long *k1, int o,
+                                      int nsteps, int len) {
+    int64_t n = 0;
+    if (v) {
+        if (tm.lane == 0) n = build_profile_inplace(F, box, v, k0, k1, o, nsteps);
+        return tm.bcast(n);
+    }
+    const double lx = box[0], ly = box[1], ux = box[2], uy = box[3];
+    int32_t r0, r1;
+    box_rows(F, box, r0, r1);
+    const int32_t nr = r1 - r0;
+    double *tot = reinterpret_cast<double *>(k1 + o + len - nr);
+    for (int32_t i = tm.lane; i < nr; i += tm.T) {
+        const int32_t r = r0 + i;
+        double total = 0.0;
+        const int64_t end = F.rowspan[r + 1];
+        for (int64_t s = first_span(F, r, lx); s < end && F.spans[2 * s] < ux; ++s)
+            total += ref_max(0.0, ref_min(ux, F.spans[2 * s + 1]) - ref_max(lx, F.spans[2 * s]));
+        tot[i] = total;
+    }
+    tm.sync();
+    if (tm.lane == 0) {
+        double *e = reinterpret_cast<double *>(k0 + o);
+        double *p = reinterpret_cast<double *>(k1 + o);
+        n = 1;
+        e[0] = ly;
+        p[0] = 0.0;
+        auto extend = [&](double to, double area) {
+            if (to > e[n - 1]) {
+                e[n] = to;
+                p[n] = p[n - 1] + area;
+                ++n;
+            }
+        };
+        for (int32_t i = 0; i < nr; ++i) {
+            const int32_t r = r0 + i;
+            const double a = ref_max(ly, F.rowy[2 * r]);
+            const double z = ref_min(uy, F.rowy[2 * r + 1]);
+            if (z > a) {
+                const double total = tot[i];
+                extend(a, 0.0);
+                extend(z, total * (z - a));
+            }
+        }
+        extend(uy, 0.0);
+        if (n == 1) {
+            e[1] = uy;
+            p[1] = 0.0;
+            n = 2;
+        }
+    }
+    n = tm.bcast(n);
+    tm.sync();
+    return n;
 }
 
 __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
@@ -1138,10 +1393,10 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
     uint32_t *k2 = reinterpret_cast<uint32_t *>(lrowspan + kRowsLocal + 2);
     int32_t *gid = reinterpret_cast<int32_t *>(k2 + kSortCap);
     int32_t *at = gid + kSub, *sof = at + kSub, *scan = sof + kSub;
-    int16_t *dof = reinterpret_cast<int16_t *>(scan + 2 * kMaxSub);
+    int16_t *dof = reinterpret_cast<int16_t *>(scan + 2 * kMaxSub + 2);
     __shared__ int32_t warp_tmp[32];
     __shared__ long long w64[32];
-    __shared__ int s_fail, s_nobst, s_ncur, s_maxlen, s_maxsteps;
+    __shared__ int s_fail, s_nobst, s_ncur, s_maxlen, s_maxsteps, s_c1;
     const int tid = threadIdx.x, nt = blockDim.x;
     SubDesc *const cur0 = A.desc + static_cast<size_t>(blockIdx.x) * 2 * kMaxSub;
     double *const scut = A.strp + static_cast<size_t>(blockIdx.x) * 4 * kStripeCap;
@@ -1237,7 +1492,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
             }
         }
         __syncthreads();
-        if (s_nobst > kObstLocal && tid == 0) s_fail = 1;
+        if (s_nobst > kObstLocal && tid == 0) s_fail = 1;  // too many obstacles
         FL.obst = obst;
         FL.K = min(s_nobst, kObstLocal);
         SubDesc *cur = cur0, *nxt = cur0 + kMaxSub;
@@ -1257,21 +1512,36 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
             const int nact = cta_scan(scan, ncur, warp_tmp);
             if (nact == 0) break;
             if (2 * nact > kMaxSub) {
-                if (tid == 0) s_fail = 1;
+                if (tid == 0) s_fail = 2;  // too many sub-blocks
                 break;
             }
             const bool small_cells = s_maxlen <= kSmallSeg;
             for (int i = tid; i < ncur; i += nt) cur[i].rank = scan[i];
+            __syncthreads();
+            // the sub-blocks' starts, and ends with the split and axis flags,
+            // in shared memory for the position lookups
+            for (int i = tid; i < ncur; i += nt) {
+                scan[i] = cur[i].b;
+                scan[kMaxSub + i] = cur[i].e | (cur[i].act << 30) | (cur[i].vert << 29);
+            }
+            __syncthreads();
             // B. each position's sub-block; cells of each splitting sub-block by
             // (centre, id), ties by cell id as the reference's sortCells
             for (int p = tid; p < size; p += nt) {
-                const int i = find_desc(cur, ncur, p);
-                const bool in = p >= cur[i].b && p < cur[i].e && cur[i].act;
+                int lo = 0, hi = ncur;  // last sub-block with b <= p
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (scan[mid] <= p) lo = mid;
+                    else hi = mid;
+                }
+                const int i = lo;
+                const int ev = scan[kMaxSub + i];
+                const bool in = p >= scan[i] && p < (ev & 0x1fffffff) && ((ev >> 30) & 1);
                 dof[p] = static_cast<int16_t>(in ? i : -1);
                 const int j = at[p];
                 if (in) {
-                    k2[p] = static_cast<uint32_t>(cur[i].b);
-                    k0[p] = ord(centre(j, cur[i].vert != 0));
+                    k2[p] = static_cast<uint32_t>(scan[i]);
+                    k0[p] = ord(centre(j, ((ev >> 29) & 1) != 0));
                 } else {
                     k2[p] = static_cast<uint32_t>(p);
                     k0[p] = 0ull;
@@ -1284,164 +1554,266 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                     if (cur[i].act) seg_sort1(k0, k1, k2, cur[i].b, cur[i].e);
                 __syncthreads();
             } else {
-                cta_sort(k0, k1, k2, size);
+                // the active sub-blocks in rank order: nxt is free until phase L
+                for (int i = tid; i < ncur; i += nt)
+                    if (cur[i].act) {
+                        nxt[cur[i].rank].b = cur[i].b;
+                        nxt[cur[i].rank].e = cur[i].e;
+                    }
+                __syncthreads();
+                sort_segments(k0, k1, k2, nact, [&](int g, int &b, int &e) {
+                    b = nxt[g].b;
+                    e = nxt[g].e;
+                });
             }
             for (int p = tid; p < size; p += nt) at[p] = static_cast<int32_t>(k1[p] & 0xffffffffull);
             __syncthreads();
             if (A.exact) cta_prefix64(at, sa, size, A.scale, pre, w64);
             // C. areas and median in sorted order; the block profile's region
-            for (int i = tid; i < ncur; i += nt) {
-                SubDesc &d = cur[i];
-                int32_t steps = 0, len = 0;
-                if (d.act) {
-                    const int b = d.b, e = d.e, n = e - b;
-                    double cell_area = 0.0, low = 0.0, high = 0.0;
-                    int m = 0;
-                    if (A.exact) {
-                        m = median_fx(pre, b, n);
-                        cell_area = static_cast<double>(pre[e] - pre[b]) * A.inv_scale;
-                        low = static_cast<double>(pre[b + m] - pre[b]) * A.inv_scale;
-                        high = static_cast<double>(pre[e] - pre[b + m]) * A.inv_scale;
-                    } else {
-                        for (int p = b; p < e; ++p) cell_area += sa[at[p]];
-                        while (m + 1 < n && (m == 0 || low < 0.5 * cell_area))
-                            low += sa[at[b + m++]];
-                        for (int p = b + m; p < e; ++p) high += sa[at[p]];
+            {
+                const Team tm(nact);
+                for (int i = tm.team; i < ncur; i += tm.nteams) {
+                    SubDesc &d = cur[i];
+                    int32_t steps = 0, len = 0;
+                    if (d.act) {
+                        const bool v = d.vert != 0;
+                        steps = v ? team_count_steps(tm, FL, d.box) : 0;
+                        int32_t r0, r1;
+                        box_rows(FL, d.box, r0, r1);
+                        len = (v ? steps : 2 * (r1 - r0)) + 2;
+                        if (tm.lane == 0) {
+                            const int b = d.b, e = d.e, n = e - b;
+                            double cell_area = 0.0, low = 0.0, high = 0.0;
+                            int m = 0;
+                            if (A.exact) {
+                                m = median_fx(pre, b, n);
+                                cell_area = static_cast<double>(pre[e] - pre[b]) * A.inv_scale;
+                                low = static_cast<double>(pre[b + m] - pre[b]) * A.inv_scale;
+                                high = static_cast<double>(pre[e] - pre[b + m]) * A.inv_scale;
+                            } else {
+                                for (int p = b; p < e; ++p) cell_area += sa[at[p]];
+                                while (m + 1 < n && (m == 0 || low < 0.5 * cell_area))
+                                    low += sa[at[b + m++]];
+                                for (int p = b + m; p < e; ++p) high += sa[at[p]];
+                            }
+                            d.m = m;
+                            d.cell_area = cell_area;
+                            d.low_area = low;
+                            d.high_area = high;
+                            atomicMax(&s_maxsteps, steps);
+                        }
                     }
-                    d.m = m;
-                    d.cell_area = cell_area;
-                    d.low_area = low;
-                    d.high_area = high;
-                    const bool v = d.vert != 0;
-                    steps = v ? static_cast<int32_t>(count_steps(FL, d.box)) : 0;
-                    len = (v ? steps : 2 * count_rows(FL, d.box)) + 2;
-                    atomicMax(&s_maxsteps, steps);
+                    if (tm.lane == 0) {
+                        d.scnt = steps;
+                        d.slen = len;
+                        scan[i] = len;
+                    }
                 }
-                d.scnt = steps;
-                d.slen = len;
-                scan[i] = len;
             }
             __syncthreads();
             const int tot = cta_scan(scan, ncur, warp_tmp);
-            if (tot > kSortCap) {
-                if (tid == 0) s_fail = 1;
-                break;
-            }
             const bool small_steps = s_maxsteps <= kSmallSeg;
             for (int i = tid; i < ncur; i += nt) cur[i].soff = scan[i];
             __syncthreads();  // every thread has read s_maxsteps before it is reset
-            if (tid == 0) s_maxsteps = 0;
-            // D. the block profiles' regions: pads, then the steps sorted by (x, dh)
-            for (int i = tid; i < ncur; i += nt) {
-                const SubDesc &d = cur[i];
-                if (!d.act) continue;
-                emit_region(FL, d.box, d.vert != 0, static_cast<uint32_t>(i), k0, k1, k2,
-                            d.soff, d.slen);
-                if (small_steps && d.vert) seg_sort1(k0, k1, k2, d.soff + 2, d.soff + 2 + d.scnt);
+            if (tid == 0) {
+                s_maxsteps = 0;
+                scan[ncur] = tot;
             }
-            __syncthreads();
-            if (!small_steps) cta_sort(k0, k1, k2, tot);
-            // E. profile, cutline, half boxes, the halves' regions and stripe room
-            for (int i = tid; i < ncur; i += nt) {
-                SubDesc &d = cur[i];
-                if (!d.act) {
-                    for (int side = 0; side < 2; ++side) d.hslen[side] = d.stcap[side] = 0;
-                    continue;
-                }
-                const bool v = d.vert != 0;
-                const int64_t n = build_profile_inplace(FL, d.box, v, k0, k1, d.soff, d.scnt);
-                const Prof room{reinterpret_cast<const double *>(k0 + d.soff),
-                                reinterpret_cast<const double *>(k1 + d.soff), n};
-                const double share = d.cell_area > 0.0 ? d.low_area / d.cell_area : 0.5;
-                const double lo = v ? d.box[0] : d.box[1], hi = v ? d.box[2] : d.box[3];
-                const double cut = room.total() > 0.0 ? room.coordinate_at(share * room.total())
-                                                      : lo + share * (hi - lo);
-                d.cut = cut;
-                for (int q = 0; q < 4; ++q) d.hbox[q] = d.hbox[4 + q] = d.box[q];
-                d.hbox[v ? 2 : 3] = cut;
-                d.hbox[4 + (v ? 0 : 1)] = cut;
-                const double r_lo = room.before(cut);
-                for (int side = 0; side < 2; ++side) {
-                    const double *bx = d.hbox + 4 * side;
-                    const int32_t st = v ? static_cast<int32_t>(count_steps(FL, bx)) : 0;
-                    d.hscnt[side] = st;
-                    d.hslen[side] = (v ? st : 2 * count_rows(FL, bx)) + 2;
-                    atomicMax(&s_maxsteps, st);
-                    int32_t k = 0;
-                    for (int32_t ob = 0; ob < FL.K; ++ob) {
-                        const double *q = FL.obst + 4 * ob;
-                        if (q[2] <= bx[0] || q[0] >= bx[2] || q[3] <= bx[1] || q[1] >= bx[3]) continue;
-                        ++k;
+            // D + E, in chunks of consecutive sub-blocks whose profile regions fit
+            // the sort buffer together (scan[] holds the regions' offsets)
+            for (int c0 = 0; c0 < ncur;) {
+                if (tid == 0) {
+                    int lo = c0 + 1, hi = ncur;  // the last end offset within reach
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (scan[mid] - scan[c0] <= kSortCap) lo = mid;
+                        else hi = mid - 1;
                     }
-                    // stripes from midpoint splits hold more than half the split
-                    // limit each: at most 2 room / limit of them (+ margin)
-                    const double r_h = side ? ref_max(0.0, room.total() - r_lo) : r_lo;
-                    const double lim = A.frac * (T.room > 0.0 ? T.room : r_h);
-                    int32_t extra = A.stripe_extra;
-                    if (T.room > 0.0 && lim > 0.0)
-                        extra = static_cast<int32_t>(ref_min(static_cast<double>(A.stripe_extra),
-                                                             ceil(2.02 * r_h / lim) + 4.0));
-                    d.stcap[side] = 2 * k + 2 + extra;
+                    int c1 = lo;
+                    if (scan[c1] - scan[c0] > kSortCap) c1 = c0;  // one region too long
+                    if (c1 == c0) s_fail = 3;  // sort buffer
+                    s_c1 = c1;
                 }
+                __syncthreads();
+                if (s_fail) break;
+                const int c1 = s_c1, base = scan[c0];
+                // D. the block profiles' regions: pads, then the steps sorted by (x, dh)
+                {
+                    const Team tm(nact);
+                    for (int i = c0 + tm.team; i < c1; i += tm.nteams) {
+                        const SubDesc &d = cur[i];
+                        if (!d.act) continue;
+                        const int o = d.soff - base;
+                        team_emit_region(tm, FL, d.box, d.vert != 0, static_cast<uint32_t>(i), k0,
+                                         k1, k2, o, d.slen);
+                        if (small_steps && d.vert && tm.lane == 0) seg_sort1(k0, k1, k2, o + 2, o + 2 + d.scnt);
+                        tm.sync();
+                    }
+                }
+                __syncthreads();
+                if (!small_steps)
+                    sort_segments(k0, k1, k2, c1 - c0, [&](int g, int &b, int &e) {
+                        const SubDesc &d = cur[c0 + g];
+                        const bool on = d.act && d.vert;
+                        b = on ? d.soff - base + 2 : 0;
+                        e = on ? d.soff - base + 2 + d.scnt : 0;
+                    });
+                // E. profile, cutline, half boxes, the halves' regions and stripe room
+                {
+                    const Team tm(nact);
+                    for (int i = c0 + tm.team; i < c1; i += tm.nteams) {
+                        SubDesc &d = cur[i];
+                        if (!d.act) {
+                            if (tm.lane == 0)
+                                for (int side = 0; side < 2; ++side) d.hslen[side] = d.stcap[side] = 0;
+                            continue;
+                        }
+                        const bool v = d.vert != 0;
+                        const int o = d.soff - base;
+                        const int64_t n = team_build_profile(tm, FL, d.box, v, k0, k1, o, d.scnt, d.slen);
+                        const Prof room{reinterpret_cast<const double *>(k0 + o),
+                                        reinterpret_cast<const double *>(k1 + o), n};
+                        const double share = d.cell_area > 0.0 ? d.low_area / d.cell_area : 0.5;
+                        const double lo = v ? d.box[0] : d.box[1], hi = v ? d.box[2] : d.box[3];
+                        const double cut = room.total() > 0.0 ? room.coordinate_at(share * room.total())
+                                                              : lo + share * (hi - lo);
+                        double hb[8];
+                        for (int q = 0; q < 4; ++q) hb[q] = hb[4 + q] = d.box[q];
+                        hb[v ? 2 : 3] = cut;
+                        hb[4 + (v ? 0 : 1)] = cut;
+                        const double r_lo = room.before(cut);
+                        int32_t hsc[2], hsl[2], cap[2];
+                        for (int side = 0; side < 2; ++side) {
+                            const double *bx = hb + 4 * side;
+                            hsc[side] = v ? team_count_steps(tm, FL, bx) : 0;
+                            int32_t r0, r1;
+                            box_rows(FL, bx, r0, r1);
+                            hsl[side] = (v ? hsc[side] : 2 * (r1 - r0)) + 2;
+                            const int32_t k = team_count_obstacles(tm, FL, bx);
+                            // stripes from midpoint splits hold more than half the split
+                            // limit each: at most 2 room / limit of them (+ margin)
+                            const double r_h = side ? ref_max(0.0, room.total() - r_lo) : r_lo;
+                            const double lim = A.frac * (T.room > 0.0 ? T.room : r_h);
+                            int32_t extra = A.stripe_extra;
+                            if (T.room > 0.0 && lim > 0.0)
+                                extra = static_cast<int32_t>(ref_min(static_cast<double>(A.stripe_extra),
+                                                                     ceil(2.02 * r_h / lim) + 4.0));
+                            cap[side] = 2 * k + 2 + extra;
+                        }
+                        tm.sync();  // every lane has read the profile and the box
+                        if (tm.lane == 0) {
+                            d.cut = cut;
+                            for (int q = 0; q < 8; ++q) d.hbox[q] = hb[q];
+                            for (int side = 0; side < 2; ++side) {
+                                d.hscnt[side] = hsc[side];
+                                d.hslen[side] = hsl[side];
+                                d.stcap[side] = cap[side];
+                                atomicMax(&s_maxsteps, hsc[side]);
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+                c0 = c1;
             }
-            __syncthreads();
-            for (int h = tid; h < 2 * ncur; h += nt) scan[h] = cur[h >> 1].hslen[h & 1];
-            __syncthreads();
-            const int htot = cta_scan(scan, 2 * ncur, warp_tmp);
-            for (int h = tid; h < 2 * ncur; h += nt) {
-                cur[h >> 1].hsoff[h & 1] = scan[h];
-                scan[h] = cur[h >> 1].stcap[h & 1];
-            }
+            if (s_fail) break;
+            // the halves' stripe offsets, then their profile regions' offsets
+            for (int h = tid; h < 2 * ncur; h += nt) scan[h] = cur[h >> 1].stcap[h & 1];
             __syncthreads();
             const int stot = cta_scan(scan, 2 * ncur, warp_tmp);
-            if (htot > kSortCap || stot > kStripeCap) {
-                if (tid == 0) s_fail = 1;
+            if (stot > kStripeCap) {
+                if (tid == 0) s_fail = 4;  // stripes
                 break;
             }
+            for (int h = tid; h < 2 * ncur; h += nt) {
+                cur[h >> 1].stoff[h & 1] = scan[h];
+                scan[h] = cur[h >> 1].hslen[h & 1];
+            }
+            __syncthreads();
+            const int htot = cta_scan(scan, 2 * ncur, warp_tmp);
             const bool small_hsteps = s_maxsteps <= kSmallSeg;
-            for (int h = tid; h < 2 * ncur; h += nt) cur[h >> 1].stoff[h & 1] = scan[h];
+            for (int h = tid; h < 2 * ncur; h += nt) cur[h >> 1].hsoff[h & 1] = scan[h];
             __syncthreads();
-            // F. the halves' profile regions
-            for (int h = tid; h < 2 * ncur; h += nt) {
-                const SubDesc &d = cur[h >> 1];
-                const int side = h & 1;
-                if (!d.act) continue;
-                const int o = d.hsoff[side];
-                emit_region(FL, d.hbox + 4 * side, d.vert != 0, static_cast<uint32_t>(h), k0, k1, k2,
-                            o, d.hslen[side]);
-                if (small_hsteps && d.vert) seg_sort1(k0, k1, k2, o + 2, o + 2 + d.hscnt[side]);
+            if (tid == 0) {
+                s_maxsteps = 0;
+                scan[2 * ncur] = htot;
             }
-            __syncthreads();
-            if (tid == 0) s_maxsteps = 0;
-            if (!small_hsteps) cta_sort(k0, k1, k2, htot);
-            // G. the halves' profiles and stripes
-            for (int h = tid; h < 2 * ncur; h += nt) {
-                SubDesc &d = cur[h >> 1];
-                const int side = h & 1;
-                if (!d.act) continue;
-                const bool v = d.vert != 0;
-                const int o = d.hsoff[side];
-                const int64_t n =
-                    build_profile_inplace(FL, d.hbox + 4 * side, v, k0, k1, o, d.hscnt[side]);
-                const Prof room{reinterpret_cast<const double *>(k0 + o),
-                                reinterpret_cast<const double *>(k1 + o), n};
-                const int so = d.stoff[side];
-                const int64_t ns = make_stripes(
-                    room, d.hbox + 4 * side, v, side ? d.high_area : d.low_area, T.room, A.frac,
-                    A.limit_density, FL.obst, FL.K, d.cut, side == 0, scut + so, d.stcap[side],
-                    sta + so, stb + so, stc + so);
-                if (ns < 0) {
-                    atomicExch(&s_fail, 1);
-                    d.stcnt[side] = 0;
-                    continue;
+            // F + G, in chunks of consecutive halves
+            for (int c0 = 0; c0 < 2 * ncur;) {
+                if (tid == 0) {
+                    const int nh = 2 * ncur;
+                    int lo = c0 + 1, hi = nh;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (scan[mid] - scan[c0] <= kSortCap) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    int c1 = lo;
+                    if (scan[c1] - scan[c0] > kSortCap) c1 = c0;  // one region too long
+                    if (c1 == c0) s_fail = 3;  // sort buffer
+                    s_c1 = c1;
                 }
-                d.stcnt[side] = static_cast<int32_t>(ns);
-                for (int64_t q = 0; q < ns; ++q) {
-                    slo[so + q] = ~0ull;
-                    shi[so + q] = 0ull;
+                __syncthreads();
+                if (s_fail) break;
+                const int c1 = s_c1, base = scan[c0];
+                // F. the halves' profile regions
+                {
+                    const Team tm(2 * nact);
+                    for (int h = c0 + tm.team; h < c1; h += tm.nteams) {
+                        const SubDesc &d = cur[h >> 1];
+                        const int side = h & 1;
+                        if (!d.act) continue;
+                        const int o = d.hsoff[side] - base;
+                        team_emit_region(tm, FL, d.hbox + 4 * side, d.vert != 0, static_cast<uint32_t>(h),
+                                         k0, k1, k2, o, d.hslen[side]);
+                        if (small_hsteps && d.vert && tm.lane == 0)
+                            seg_sort1(k0, k1, k2, o + 2, o + 2 + d.hscnt[side]);
+                        tm.sync();
+                    }
                 }
+                __syncthreads();
+                if (!small_hsteps)
+                    sort_segments(k0, k1, k2, c1 - c0, [&](int g, int &b, int &e) {
+                        const int h = c0 + g;
+                        const SubDesc &d = cur[h >> 1];
+                        const bool on = d.act && d.vert;
+                        b = on ? d.hsoff[h & 1] - base + 2 : 0;
+                        e = on ? d.hsoff[h & 1] - base + 2 + d.hscnt[h & 1] : 0;
+                    });
+                // G. the halves' profiles and stripes
+                {
+                    const Team tm(2 * nact);
+                    for (int h = c0 + tm.team; h < c1; h += tm.nteams) {
+                        SubDesc &d = cur[h >> 1];
+                        const int side = h & 1;
+                        if (!d.act) continue;
+                        const bool v = d.vert != 0;
+                        const int o = d.hsoff[side] - base;
+                        const int64_t n = team_build_profile(tm, FL, d.hbox + 4 * side, v, k0, k1, o,
+                                                             d.hscnt[side], d.hslen[side]);
+                        const int so = d.stoff[side];
+                        int64_t ns = 0;
+                        if (tm.lane == 0) {
+                            const Prof room{reinterpret_cast<const double *>(k0 + o),
+                                            reinterpret_cast<const double *>(k1 + o), n};
+                            ns = make_stripes(room, d.hbox + 4 * side, v, side ? d.high_area : d.low_area,
+                                              T.room, A.frac, A.limit_density, FL.obst, FL.K, d.cut,
+                                              side == 0, scut + so, d.stcap[side], sta + so, stb + so,
+                                              stc + so);
+                            if (ns < 0) atomicExch(&s_fail, 4);
+                            d.stcnt[side] = static_cast<int32_t>(ns < 0 ? 0 : ns);
+                        }
+                        ns = tm.bcast(ns);
+                        for (int64_t q = tm.lane; q < ns; q += tm.T) {
+                            slo[so + q] = ~0ull;
+                            shi[so + q] = 0ull;
+                        }
+                    }
+                }
+                __syncthreads();
+                if (s_fail) break;
+                c0 = c1;
             }
-            __syncthreads();
             if (s_fail) break;
             // H. cells of each half by (-distance from the cut, id)
             for (int p = tid; p < size; p += nt) {
@@ -1471,7 +1843,18 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                 }
                 __syncthreads();
             } else {
-                cta_sort(k0, k1, k2, size);
+                for (int i = tid; i < ncur; i += nt)
+                    if (cur[i].act) {
+                        nxt[cur[i].rank].b = cur[i].b;
+                        nxt[cur[i].rank].e = cur[i].e;
+                        nxt[cur[i].rank].m = cur[i].m;
+                    }
+                __syncthreads();
+                sort_segments(k0, k1, k2, 2 * nact, [&](int g, int &b, int &e) {
+                    const SubDesc &d = nxt[g >> 1];
+                    b = (g & 1) ? d.b + d.m : d.b;
+                    e = (g & 1) ? d.e : d.b + d.m;
+                });
             }
             for (int p = tid; p < size; p += nt) at[p] = static_cast<int32_t>(k1[p] & 0xffffffffull);
             __syncthreads();
@@ -1602,7 +1985,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
         }
         __syncthreads();
         if (s_fail) {
-            if (tid == 0) A.fail[task] = 1;
+            if (tid == 0) A.fail[task] = s_fail;
         } else {
             for (int j = tid; j < size; j += nt) {
                 C.x[gid[j]] = sx[j];
@@ -1721,7 +2104,7 @@ struct LalState {
     DevBuf<unsigned long long> sstrlh;
     bool subtree_attr = false;
     // counters of the last ktg_lal call (ktg_lal_stats)
-    double stats[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double stats[16] = {};
 };
 
 void free_lal(ktg_ctx *c) {
@@ -1891,7 +2274,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         (rc = s->keys.ensure(c, n + 1)) || (rc = s->keys_tmp.ensure(c, n + 1)))
         return rc;
     KTG_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
-    std::fill(s->stats, s->stats + 12, 0.0);
+    std::fill(s->stats, s->stats + 16, 0.0);
     const double t_start = now_ms();
     CellsDev C{x, y, c->width, c->height, c->area};
     const GridDev G{c->origin_x, c->origin_y, c->dx, c->dy, nx, ny};
@@ -1978,7 +2361,10 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
         s->stats[4] += nt;
         s->stats[8] += now_ms() - t0;
         s->stats[10] += nt;
-        for (int32_t t = 0; t < nt; ++t) s->stats[11] += failed[t] != 0;
+        for (int32_t t = 0; t < nt; ++t) {
+            s->stats[11] += failed[t] != 0;
+            if (failed[t] >= 1 && failed[t] <= 4) s->stats[11 + failed[t]] += 1;
+        }
         return KTG_OK;
     };
 
@@ -2127,7 +2513,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
                 return r2;
             KTG_CUDA(c, cudaMemcpyAsync(s->soff.p, soff.data(), sizeof(int64_t) * na, cudaMemcpyHostToDevice, c->stream));
             KTG_CUDA(c, cudaMemcpyAsync(s->eoff.p, eoff.data(), sizeof(int64_t) * na, cudaMemcpyHostToDevice, c->stream));
-            k_block_steps<<<blocks_for(na), kT, 0, c->stream>>>(L, F, s->soff.p, s->steps.p, s->nsteps.p);
+            k_steps_cta<<<na, kT, 0, c->stream>>>(L, F, 0, s->soff.p, s->steps.p, s->nsteps.p);
             ++c->launches;
             std::vector<int64_t> nst(na);
             KTG_CUDA(c, cudaMemcpyAsync(nst.data(), s->nsteps.p, sizeof(int64_t) * na,
@@ -2140,8 +2526,8 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             }
             if ((r2 = seg_sort(c, s->steps.p, s->steps_tmp.p, ssegs, s->seg.p))) return r2;
             // 3. profile, cutline, half boxes and bounds
-            k_block_cut<<<blocks_for(na), kT, 0, c->stream>>>(L, F, s->soff.p, s->steps.p, s->nsteps.p,
-                                                            s->eoff.p, s->pe.p, s->pp.p, s->hbound.p);
+            k_block_cut_cta<<<na, kT, 0, c->stream>>>(L, F, s->soff.p, s->steps.p, s->nsteps.p,
+                                                      s->eoff.p, s->pe.p, s->pp.p, s->hbound.p);
             ++c->launches;
             std::vector<int64_t> hbound(4 * na);
             KTG_CUDA(c, cudaMemcpyAsync(hbound.data(), s->hbound.p, sizeof(int64_t) * 4 * na,
@@ -2171,9 +2557,9 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             KTG_CUDA(c, cudaMemcpyAsync(s->hsoff.p, hsoff.data(), sizeof(int64_t) * 2 * na, cudaMemcpyHostToDevice, c->stream));
             KTG_CUDA(c, cudaMemcpyAsync(s->heoff.p, heoff.data(), sizeof(int64_t) * 2 * na, cudaMemcpyHostToDevice, c->stream));
             KTG_CUDA(c, cudaMemcpyAsync(s->stoff.p, stoff.data(), sizeof(int64_t) * 2 * na, cudaMemcpyHostToDevice, c->stream));
-            // cut capacity per half, read by k_half_stripes
+            // cut capacity per half, read by k_half_stripes_cta
             KTG_CUDA(c, cudaMemcpyAsync(s->hbound.p, hcap.data(), sizeof(int64_t) * 2 * na, cudaMemcpyHostToDevice, c->stream));
-            k_half_steps<<<blocks_for(2 * na), kT, 0, c->stream>>>(L, F, s->hsoff.p, s->steps.p, s->hnsteps.p);
+            k_steps_cta<<<2 * na, kT, 0, c->stream>>>(L, F, 1, s->hsoff.p, s->steps.p, s->hnsteps.p);
             ++c->launches;
             std::vector<int64_t> hnst(2 * na);
             KTG_CUDA(c, cudaMemcpyAsync(hnst.data(), s->hnsteps.p, sizeof(int64_t) * 2 * na,
@@ -2187,7 +2573,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             if ((r2 = seg_sort(c, s->steps.p, s->steps_tmp.p, ssegs, s->seg.p))) return r2;
             // 4. stripes per half (profile arrays: e in pe, p and the cuts in pp)
             Stripes S{s->stoff.p, s->scount.p, s->sa.p, s->sb.p, s->scap.p, s->sused.p, s->slo.p, s->shi.p};
-            k_half_stripes<<<blocks_for(2 * na), kT, 0, c->stream>>>(
+            k_half_stripes_cta<<<2 * na, kT, 0, c->stream>>>(
                 L, F, s->hsoff.p, s->steps.p, s->hnsteps.p, s->heoff.p, s->pe.p, s->pp.p,
                 s->hbound.p, frac, c->density_limit, S, c->status);
             // 5. fill order, fill, stripe ranges, positions
@@ -2279,7 +2665,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
 }
 
 int lal_stats(ktg_ctx *c, double *out, int count) {
-    for (int k = 0; k < count && k < 12; ++k) out[k] = c->lal ? c->lal->stats[k] : 0.0;
+    for (int k = 0; k < count && k < 16; ++k) out[k] = c->lal ? c->lal->stats[k] : 0.0;
     return KTG_OK;
 }
 

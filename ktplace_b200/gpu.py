@@ -321,10 +321,11 @@ class Context:
         return x, y
 
     def lal_stats(self) -> dict:
-        out = np.zeros(12)
-        self._check(self.lib.ktg_lal_stats(self.h, _ptr(out), 12))
+        out = np.zeros(16)
+        self._check(self.lib.ktg_lal_stats(self.h, _ptr(out), 16))
         keys = ("batches", "regions", "levels", "syncs", "blocks", "ms_bisect", "ms_refresh",
-                "ms_total", "ms_subtree", "big_levels", "subtree_blocks", "subtree_handed_back")
+                "ms_total", "ms_subtree", "big_levels", "subtree_blocks", "subtree_handed_back",
+                "back_size_or_obstacles", "back_sub_blocks", "back_sort_buffer", "back_stripes")
         return dict(zip(keys, out.tolist()))
 
     def lal_dev(self, x, y, max_level: int = 20, min_cells_to_split: int = 4,
