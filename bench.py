@@ -56,6 +56,9 @@ def parse():
                     help="skip the batched-solve leg (64 netlists, 128 systems)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="run the batched-solve workload once for an ncu capture")
+    ap.add_argument("--profile-lal", action="store_true",
+                    help="run only the look-ahead legalization of the step's solved positions "
+                         "twice (the capture workload of profiles/lal_*)")
     ap.add_argument("--profile-agg", action="store_true",
                     help="build the 211k systems twice, each followed by a mixed solve with "
                          "the aggregation preconditioner (set-up included), for ncu captures")
@@ -768,10 +771,37 @@ def profile_agg():
     return 0
 
 
+def profile_lal():
+    """The capture workload of profiles/lal_*_synth211k.md: one B2B build and
+    FP64 PCG solve of the 211k-cell workload from its seed positions, then
+    the look-ahead legalization of the solved positions, twice."""
+    from ktplace_b200 import grid
+    from ktplace_b200.gpu import Context
+    raw, nl, x, y, ax, ay = make_workload(1)
+    fx, fy = nl.floors()
+    ctx = Context(0)
+    ctx.upload_netlist(nl)
+    ctx.build_b2b(x, y, ALPHA, ax, ay, fx, fy)
+    px, py = np.array(x, dtype=np.float64), np.array(y, dtype=np.float64)
+    ctx.solve(px, py, TOL, MAX_ITER, inplace=True)
+    bins = grid.default_bins_per_axis(nl.num_movable)
+    ctx.set_grid(grid.build_grid(nl, bins, 1.0))
+    ctx.set_free_space(grid.build_free_space(nl))
+    for _ in range(2):
+        lx, ly = ctx.lal(px, py)
+    st = ctx.lal_stats()
+    print(f"profile-lal: {int(st['batches'])} batches, {int(st['regions'])} regions, "
+          f"{st['ms_total']:.1f} ms, moved {float(np.mean((lx != px) | (ly != py))):.3f}")
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_once:
         return profile_once()
+    if args.profile_lal:
+        return profile_lal()
     if args.profile_agg:
         return profile_agg()
     if args.profile_batch:

@@ -101,11 +101,38 @@ __global__ void __launch_bounds__(kT) k_sort_small(Key *keys, const int64_t *seg
     for (int i = threadIdx.x; i < len; i += kT) keys[b + i] = s[i];
 }
 
-// Chunks of kSortSmall keys of one long segment, each sorted in shared memory.
-__global__ void __launch_bounds__(kT) k_sort_chunks(Key *keys, int64_t b, int64_t e) {
+int blocks_for(int64_t items, int threads = kT) {
+    return static_cast<int>(std::max<int64_t>(1, (items + threads - 1) / threads));
+}
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    int64_t cap = 0;
+    int ensure(ktg_ctx *c, int64_t n) {
+        if (n <= cap) return KTG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const int64_t want = std::max<int64_t>(n + n / 4, 64);
+        if (cudaMalloc(&p, sizeof(T) * want) != cudaSuccess)
+            return set_error(c, KTG_ERR_NOMEM, "out of device memory (legalization)");
+        cap = want;
+        return KTG_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// Chunks [b, e) of at most kSortSmall keys, one per block, sorted in shared
+// memory; the chunk list holds (b, e) pairs.
+__global__ void __launch_bounds__(kT) k_sort_chunks_multi(Key *keys, const int64_t *chunks) {
     __shared__ Key s[kSortSmall];
-    const int64_t c0 = b + static_cast<int64_t>(blockIdx.x) * kSortSmall;
-    const int len = static_cast<int>(std::min<int64_t>(kSortSmall, e - c0));
+    const int64_t c0 = chunks[2 * blockIdx.x], c1 = chunks[2 * blockIdx.x + 1];
+    const int len = static_cast<int>(c1 - c0);
     for (int i = threadIdx.x; i < kSortSmall; i += kT)
         s[i] = i < len ? keys[c0 + i] : Key{~0ull, ~0ull};
     __syncthreads();
@@ -127,16 +154,33 @@ __global__ void __launch_bounds__(kT) k_sort_chunks(Key *keys, int64_t b, int64_
     for (int i = threadIdx.x; i < len; i += kT) keys[c0 + i] = s[i];
 }
 
-// One merge pass over a long segment: runs of `run` keys pairwise, stable
-// (keys of the first run go before equal keys of the second).
-__global__ void k_merge_pass(const Key *src, Key *dst, int64_t b, int64_t e, int64_t run) {
-    const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int64_t len = e - b;
-    if (r >= len) return;
-    const int64_t pair = r / (2 * run);
-    const int64_t a0 = pair * 2 * run;
-    const int64_t a1 = std::min(a0 + run, len);
-    const int64_t b1 = std::min(a0 + 2 * run, len);
+// Segment of global position g among the segments whose lengths prefix
+// `pref` (nseg + 1 entries): the last s with pref[s] <= g.
+__device__ __forceinline__ int seg_of(const int64_t *pref, int nseg, int64_t g) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pref[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One merge pass over every long segment at once: runs of `run` keys merged
+// pairwise (stable); a segment no longer than `run` is copied across.
+__global__ void k_merge_pass_multi(const Key *src, Key *dst, const int64_t *segs,
+                                   const int64_t *pref, int nseg, int64_t run) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= pref[nseg]) return;
+    const int sg = seg_of(pref, nseg, g);
+    const int64_t b = segs[2 * sg], len = segs[2 * sg + 1] - b, r = g - pref[sg];
+    if (run >= len) {
+        dst[b + r] = src[b + r];
+        return;
+    }
+    const int64_t a0 = (r / (2 * run)) * 2 * run;
+    const int64_t a1 = min(a0 + run, len);
+    const int64_t b1 = min(a0 + 2 * run, len);
     const Key k = src[b + r];
     int64_t out;
     if (r < a1) {  // in the first run: count second-run keys strictly below
@@ -159,21 +203,24 @@ __global__ void k_merge_pass(const Key *src, Key *dst, int64_t b, int64_t e, int
     dst[b + out] = k;
 }
 
-__global__ void k_copy_keys(const Key *src, Key *dst, int64_t b, int64_t e) {
-    const int64_t i = b + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < e) dst[i] = src[i];
+__global__ void k_copy_multi(const Key *src, Key *dst, const int64_t *segs, const int64_t *pref,
+                             int nseg) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= pref[nseg]) return;
+    const int sg = seg_of(pref, nseg, g);
+    const int64_t q = segs[2 * sg] + g - pref[sg];
+    dst[q] = src[q];
 }
 
-int blocks_for(int64_t items, int threads = kT) {
-    return static_cast<int>(std::max<int64_t>(1, (items + threads - 1) / threads));
-}
-
-// Sorts keys[b, e) of every segment (host list, device copy in dseg).
-int seg_sort(ktg_ctx *c, Key *keys, Key *tmp, const std::vector<int64_t> &hseg, int64_t *dseg) {
+// Sorts keys[b, e) of every segment (host list of (b, e) pairs): segments of
+// up to kSortSmall keys one block each; longer ones in chunks, then merge
+// passes over all of them together. `dseg` holds the device descriptors.
+int seg_sort(ktg_ctx *c, Key *keys, Key *tmp, const std::vector<int64_t> &hseg,
+             DevBuf<int64_t> &dseg) {
     const int nseg = static_cast<int>(hseg.size() / 2);
     if (nseg == 0) return KTG_OK;
-    std::vector<int64_t> small;
-    small.reserve(hseg.size());
+    std::vector<int64_t> small, chunks, large, pref(1, 0);
+    int64_t maxlen = 0;
     for (int s = 0; s < nseg; ++s) {
         const int64_t b = hseg[2 * s], e = hseg[2 * s + 1];
         if (e - b <= 1) continue;
@@ -182,26 +229,52 @@ int seg_sort(ktg_ctx *c, Key *keys, Key *tmp, const std::vector<int64_t> &hseg, 
             small.push_back(e);
             continue;
         }
-        k_sort_chunks<<<blocks_for(e - b, kSortSmall), kT, 0, c->stream>>>(keys, b, e);
+        for (int64_t q = b; q < e; q += kSortSmall) {
+            chunks.push_back(q);
+            chunks.push_back(std::min(e, q + kSortSmall));
+        }
+        large.push_back(b);
+        large.push_back(e);
+        pref.push_back(pref.back() + (e - b));
+        maxlen = std::max(maxlen, e - b);
+    }
+    // descriptors: small pairs, chunk pairs, long segments, their prefix
+    std::vector<int64_t> all;
+    all.reserve(small.size() + chunks.size() + large.size() + pref.size());
+    all.insert(all.end(), small.begin(), small.end());
+    all.insert(all.end(), chunks.begin(), chunks.end());
+    all.insert(all.end(), large.begin(), large.end());
+    all.insert(all.end(), pref.begin(), pref.end());
+    int rc;
+    if ((rc = dseg.ensure(c, static_cast<int64_t>(all.size()) + 1))) return rc;
+    KTG_CUDA(c, cudaMemcpyAsync(dseg.p, all.data(), sizeof(int64_t) * all.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    const int64_t *d_small = dseg.p;
+    const int64_t *d_chunks = d_small + small.size();
+    const int64_t *d_large = d_chunks + chunks.size();
+    const int64_t *d_pref = d_large + large.size();
+    if (!small.empty()) {
+        k_sort_small<<<static_cast<int>(small.size() / 2), kT, 0, c->stream>>>(
+            keys, d_small, static_cast<int>(small.size() / 2));
         ++c->launches;
-        Key *src = keys;
-        Key *dst = tmp;
-        for (int64_t run = kSortSmall; run < e - b; run *= 2) {
-            k_merge_pass<<<blocks_for(e - b), kT, 0, c->stream>>>(src, dst, b, e, run);
+    }
+    if (!large.empty()) {
+        const int nl = static_cast<int>(large.size() / 2);
+        const int64_t total = pref.back();
+        k_sort_chunks_multi<<<static_cast<int>(chunks.size() / 2), kT, 0, c->stream>>>(keys,
+                                                                                     d_chunks);
+        ++c->launches;
+        Key *src = keys, *dst = tmp;
+        for (int64_t run = kSortSmall; run < maxlen; run *= 2) {
+            k_merge_pass_multi<<<blocks_for(total), kT, 0, c->stream>>>(src, dst, d_large, d_pref,
+                                                                       nl, run);
             ++c->launches;
             std::swap(src, dst);
         }
         if (src != keys) {
-            k_copy_keys<<<blocks_for(e - b), kT, 0, c->stream>>>(src, keys, b, e);
+            k_copy_multi<<<blocks_for(total), kT, 0, c->stream>>>(src, keys, d_large, d_pref, nl);
             ++c->launches;
         }
-    }
-    if (!small.empty()) {
-        KTG_CUDA(c, cudaMemcpyAsync(dseg, small.data(), sizeof(int64_t) * small.size(),
-                                    cudaMemcpyHostToDevice, c->stream));
-        k_sort_small<<<static_cast<int>(small.size() / 2), kT, 0, c->stream>>>(
-            keys, dseg, static_cast<int>(small.size() / 2));
-        ++c->launches;
     }
     KTG_CUDA(c, cudaGetLastError());
     return KTG_OK;
@@ -905,12 +978,13 @@ __global__ void k_fill(Level L, CellsDev C, const int32_t *cells, Stripes S, int
 
 // Greedy fill from the exact prefix (fill order): stripe s of a half takes
 // positions [start_s, start_{s+1}), start_{s+1} the least position whose
-// preceding area in the stripe reaches its capacity. One thread per half;
-// the starts go to `sbeg`.
-__global__ void k_fill_fx(Level L, Stripes S, const long long *pre, double inv_scale,
-                          int32_t *sbeg) {
-    const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= 2 * L.na) return;
+// preceding area in the stripe reaches its capacity. One CTA per half; each
+// start is found by rounds of kT-way probing of the (monotone) prefix. The
+// starts go to `sbeg`.
+__global__ void __launch_bounds__(kT) k_fill_fx(Level L, Stripes S, const long long *pre,
+                                                double inv_scale, int32_t *sbeg) {
+    __shared__ int32_t s_lo, s_hi, s_first;
+    const int32_t h = blockIdx.x;
     const int32_t blk = h >> 1;
     const int32_t b = L.b[blk], e = L.e[blk], mid = b + L.m[blk];
     const int32_t p0 = (h & 1) ? mid : b, p1 = (h & 1) ? e : mid;
@@ -918,16 +992,36 @@ __global__ void k_fill_fx(Level L, Stripes S, const long long *pre, double inv_s
     const int32_t ns = S.count[h];
     int32_t at = p0;
     for (int32_t s = 0; s < ns; ++s) {
-        sbeg[so + s] = at;
+        if (threadIdx.x == 0) sbeg[so + s] = at;
         if (s + 1 == ns) break;
         const double cap = S.cap[so + s];
-        int32_t lo = at, hi = p1;  // least k in [at, p1] with used(k) >= cap, else p1
-        while (lo < hi) {
-            const int32_t k = (lo + hi) >> 1;
-            if (static_cast<double>(pre[k] - pre[at]) * inv_scale >= cap) hi = k;
-            else lo = k + 1;
+        const long long base = pre[at];
+        // least k in [at, p1] with used(k) >= cap, p1 counting as true
+        auto hit = [&](int32_t k) {
+            return k >= p1 || static_cast<double>(pre[k] - base) * inv_scale >= cap;
+        };
+        int32_t lo = at, hi = p1;
+        while (hi - lo + 1 > kT) {
+            const int32_t step = (hi - lo + kT) / kT;  // ceil((hi - lo + 1) / kT)
+            if (threadIdx.x == 0) s_first = kT;
+            __syncthreads();
+            const int32_t k = min(hi, lo + (threadIdx.x + 1) * step - 1);
+            if (hit(k)) atomicMin(&s_first, static_cast<int32_t>(threadIdx.x));
+            __syncthreads();
+            const int32_t f = s_first;
+            const int32_t nlo = f == 0 ? lo : min(hi, lo + f * step - 1) + 1;
+            const int32_t nhi = min(hi, lo + (f + 1) * step - 1);
+            __syncthreads();
+            lo = nlo;
+            hi = nhi;
         }
-        at = lo;
+        if (threadIdx.x == 0) s_first = hi;
+        __syncthreads();
+        if (lo + static_cast<int32_t>(threadIdx.x) <= hi && hit(lo + threadIdx.x))
+            atomicMin(&s_first, lo + static_cast<int32_t>(threadIdx.x));
+        __syncthreads();
+        at = s_first;
+        __syncthreads();
     }
 }
 
@@ -2054,28 +2148,6 @@ __global__ void k_clamp_die(CellsDev C, int32_t n, double lx, double ly, double 
     C.y[i] = y;
 }
 
-template <typename T>
-struct DevBuf {
-    T *p = nullptr;
-    int64_t cap = 0;
-    int ensure(ktg_ctx *c, int64_t n) {
-        if (n <= cap) return KTG_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        const int64_t want = std::max<int64_t>(n + n / 4, 64);
-        if (cudaMalloc(&p, sizeof(T) * want) != cudaSuccess)
-            return set_error(c, KTG_ERR_NOMEM, "out of device memory (legalization)");
-        cap = want;
-        return KTG_OK;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
 }  // namespace
 
 // Free space, obstacles and die for the legalizer, and its scratch.
@@ -2488,7 +2560,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             // 1. cells by centre
             k_centre_keys<<<gcell, kT, 0, c->stream>>>(L, C, s->cells.p, s->keys.p);
             ++c->launches;
-            if ((r2 = seg_sort(c, s->keys.p, s->keys_tmp.p, segs, s->seg.p))) return r2;
+            if ((r2 = seg_sort(c, s->keys.p, s->keys_tmp.p, segs, s->seg))) return r2;
             k_keys_to_cells<<<gcell, kT, 0, c->stream>>>(L, s->keys.p, s->cells.p);
             ++c->launches;
             // 2. areas, median, block profile bounds
@@ -2524,7 +2596,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
                 ssegs.push_back(soff[k]);
                 ssegs.push_back(soff[k] + nst[k]);
             }
-            if ((r2 = seg_sort(c, s->steps.p, s->steps_tmp.p, ssegs, s->seg.p))) return r2;
+            if ((r2 = seg_sort(c, s->steps.p, s->steps_tmp.p, ssegs, s->seg))) return r2;
             // 3. profile, cutline, half boxes and bounds
             k_block_cut_cta<<<na, kT, 0, c->stream>>>(L, F, s->soff.p, s->steps.p, s->nsteps.p,
                                                       s->eoff.p, s->pe.p, s->pp.p, s->hbound.p);
@@ -2570,7 +2642,7 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
                 ssegs.push_back(hsoff[h]);
                 ssegs.push_back(hsoff[h] + hnst[h]);
             }
-            if ((r2 = seg_sort(c, s->steps.p, s->steps_tmp.p, ssegs, s->seg.p))) return r2;
+            if ((r2 = seg_sort(c, s->steps.p, s->steps_tmp.p, ssegs, s->seg))) return r2;
             // 4. stripes per half (profile arrays: e in pe, p and the cuts in pp)
             Stripes S{s->stoff.p, s->scount.p, s->sa.p, s->sb.p, s->scap.p, s->sused.p, s->slo.p, s->shi.p};
             k_half_stripes_cta<<<2 * na, kT, 0, c->stream>>>(
@@ -2593,13 +2665,12 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
                 fsegs.push_back(ab[k] + mh[k]);
                 fsegs.push_back(ae[k]);
             }
-            if ((r2 = seg_sort(c, s->keys.p, s->keys_tmp.p, fsegs, s->seg.p))) return r2;
+            if ((r2 = seg_sort(c, s->keys.p, s->keys_tmp.p, fsegs, s->seg))) return r2;
             k_keys_to_cells<<<gcell, kT, 0, c->stream>>>(L, s->keys.p, s->cells.p);
             ++c->launches;
             if (exact) {
                 if ((r2 = fx_prefix(run)) || (r2 = s->sbeg.ensure(c, stripes + 1))) return r2;
-                k_fill_fx<<<blocks_for(2 * na), kT, 0, c->stream>>>(L, S, s->pre.p, inv_scale,
-                                                                   s->sbeg.p);
+                k_fill_fx<<<2 * na, kT, 0, c->stream>>>(L, S, s->pre.p, inv_scale, s->sbeg.p);
                 k_assign_fx<<<gcell, kT, 0, c->stream>>>(L, s->cells.p, S, s->sbeg.p,
                                                          s->stripe_of.p);
                 c->launches += 2;
