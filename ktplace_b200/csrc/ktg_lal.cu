@@ -1108,7 +1108,6 @@ constexpr int kObstLocal = 256;     // obstacles overlapping the block
 constexpr int64_t kStripeCap = 8192;
 constexpr int kRowsLocal = 512;     // free-space rows staged in shared memory
 constexpr int kSpansLocal = 1280;   // and their spans
-constexpr int kSmallSeg = 48;       // segments up to this long: one thread sorts each
 constexpr size_t kSubSmem = sizeof(unsigned long long) * 2 * kSortCap +
                             sizeof(uint32_t) * kSortCap + sizeof(long long) * (kSub + 2) +
                             sizeof(double) * (3 * kSub + 4 * kObstLocal) +
@@ -1153,25 +1152,6 @@ __device__ __forceinline__ bool sub_less(uint32_t a2, unsigned long long a0, uns
     return a2 < b2 || (a2 == b2 && (a0 < b0 || (a0 == b0 && a1 < b1)));
 }
 
-// Stable insertion sort of entries [b, e) by one thread.
-__device__ void seg_sort1(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int b,
-                          int e) {
-    for (int i = b + 1; i < e; ++i) {
-        const unsigned long long a0 = k0[i], a1 = k1[i];
-        const uint32_t a2 = k2[i];
-        int j = i - 1;
-        while (j >= b && sub_less(a2, a0, a1, k2[j], k0[j], k1[j])) {
-            k0[j + 1] = k0[j];
-            k1[j + 1] = k1[j];
-            k2[j + 1] = k2[j];
-            --j;
-        }
-        k0[j + 1] = a0;
-        k1[j + 1] = a1;
-        k2[j + 1] = a2;
-    }
-}
-
 // In-place sort of entries [b, b + n) by `nthreads` cooperating threads
 // (index `me`), for any n: every merge of two sorted halves starts with the
 // mirrored comparators (i, k - 1 - i) and continues with half-cleaners, all
@@ -1213,18 +1193,24 @@ __device__ __forceinline__ void named_barrier(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Sorts each segment [b, e) = seg(g) of g < nseg: the whole block for one
-// segment, equal groups of warps (each on its own named barrier) for up to
-// 15, one warp per segment beyond. Ends with a block barrier.
+// Sorts each segment [b, e) = seg(g) of g < nseg (none longer than maxlen):
+// the whole block for one segment, equal groups of warps (each on its own
+// named barrier) for a few long ones, else teams of lanes sized to the
+// longest segment (one lane for up to 3 keys, up to a warp), each team
+// taking segments in turn. Ends with a block barrier.
 template <typename Seg>
 __device__ void sort_segments(unsigned long long *k0, unsigned long long *k1, uint32_t *k2, int nseg,
-                              Seg seg) {
+                              int maxlen, Seg seg) {
     const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (nseg <= 0 || maxlen <= 1) {
+        __syncthreads();
+        return;
+    }
     if (nseg == 1) {
         int b, e;
         seg(0, b, e);
         net_sort(k0, k1, k2, b, e - b, threadIdx.x, blockDim.x, [] { __syncthreads(); });
-    } else if (nseg < 16 && nw / nseg >= 2) {
+    } else if (nseg < 16 && nw / nseg >= 2 && maxlen > 256) {
         const int W = nw / nseg;  // warps per group
         const int g = w / W;
         if (g < nseg) {
@@ -1234,10 +1220,14 @@ __device__ void sort_segments(unsigned long long *k0, unsigned long long *k1, ui
             net_sort(k0, k1, k2, b, e - b, me, n, [g, n] { named_barrier(1 + g, n); });
         }
     } else {
-        for (int g = w; g < nseg; g += nw) {
+        int T = 1;  // lanes per team: about half the longest segment, at most a warp
+        while (T < 32 && 2 * T < maxlen) T <<= 1;
+        const int me = threadIdx.x & (T - 1), team = threadIdx.x / T, nteams = blockDim.x / T;
+        const unsigned mask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << (lane & ~(T - 1)));
+        for (int g = team; g < nseg; g += nteams) {
             int b, e;
             seg(g, b, e);
-            net_sort(k0, k1, k2, b, e - b, lane, 32, [] { __syncwarp(); });
+            net_sort(k0, k1, k2, b, e - b, me, T, [mask] { __syncwarp(mask); });
         }
     }
     __syncthreads();
@@ -1609,7 +1599,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                 if (tid == 0) s_fail = 2;  // too many sub-blocks
                 break;
             }
-            const bool small_cells = s_maxlen <= kSmallSeg;
+            const int maxlen = s_maxlen;
             for (int i = tid; i < ncur; i += nt) cur[i].rank = scan[i];
             __syncthreads();
             // the sub-blocks' starts, and ends with the split and axis flags,
@@ -1643,11 +1633,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                 k1[p] = (static_cast<unsigned long long>(gid[j]) << 32) | static_cast<unsigned>(j);
             }
             __syncthreads();
-            if (small_cells) {
-                for (int i = tid; i < ncur; i += nt)
-                    if (cur[i].act) seg_sort1(k0, k1, k2, cur[i].b, cur[i].e);
-                __syncthreads();
-            } else {
+            {
                 // the active sub-blocks in rank order: nxt is free until phase L
                 for (int i = tid; i < ncur; i += nt)
                     if (cur[i].act) {
@@ -1655,7 +1641,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                         nxt[cur[i].rank].e = cur[i].e;
                     }
                 __syncthreads();
-                sort_segments(k0, k1, k2, nact, [&](int g, int &b, int &e) {
+                sort_segments(k0, k1, k2, nact, maxlen, [&](int g, int &b, int &e) {
                     b = nxt[g].b;
                     e = nxt[g].e;
                 });
@@ -1706,7 +1692,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
             }
             __syncthreads();
             const int tot = cta_scan(scan, ncur, warp_tmp);
-            const bool small_steps = s_maxsteps <= kSmallSeg;
+            const int maxsteps = s_maxsteps;
             for (int i = tid; i < ncur; i += nt) cur[i].soff = scan[i];
             __syncthreads();  // every thread has read s_maxsteps before it is reset
             if (tid == 0) {
@@ -1740,13 +1726,10 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                         const int o = d.soff - base;
                         team_emit_region(tm, FL, d.box, d.vert != 0, static_cast<uint32_t>(i), k0,
                                          k1, k2, o, d.slen);
-                        if (small_steps && d.vert && tm.lane == 0) seg_sort1(k0, k1, k2, o + 2, o + 2 + d.scnt);
-                        tm.sync();
                     }
                 }
                 __syncthreads();
-                if (!small_steps)
-                    sort_segments(k0, k1, k2, c1 - c0, [&](int g, int &b, int &e) {
+                sort_segments(k0, k1, k2, c1 - c0, maxsteps, [&](int g, int &b, int &e) {
                         const SubDesc &d = cur[c0 + g];
                         const bool on = d.act && d.vert;
                         b = on ? d.soff - base + 2 : 0;
@@ -1825,7 +1808,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
             }
             __syncthreads();
             const int htot = cta_scan(scan, 2 * ncur, warp_tmp);
-            const bool small_hsteps = s_maxsteps <= kSmallSeg;
+            const int maxhsteps = s_maxsteps;
             for (int h = tid; h < 2 * ncur; h += nt) cur[h >> 1].hsoff[h & 1] = scan[h];
             __syncthreads();
             if (tid == 0) {
@@ -1860,14 +1843,10 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                         const int o = d.hsoff[side] - base;
                         team_emit_region(tm, FL, d.hbox + 4 * side, d.vert != 0, static_cast<uint32_t>(h),
                                          k0, k1, k2, o, d.hslen[side]);
-                        if (small_hsteps && d.vert && tm.lane == 0)
-                            seg_sort1(k0, k1, k2, o + 2, o + 2 + d.hscnt[side]);
-                        tm.sync();
                     }
                 }
                 __syncthreads();
-                if (!small_hsteps)
-                    sort_segments(k0, k1, k2, c1 - c0, [&](int g, int &b, int &e) {
+                sort_segments(k0, k1, k2, c1 - c0, maxhsteps, [&](int g, int &b, int &e) {
                         const int h = c0 + g;
                         const SubDesc &d = cur[h >> 1];
                         const bool on = d.act && d.vert;
@@ -1927,16 +1906,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                 k1[p] = (static_cast<unsigned long long>(gid[j]) << 32) | static_cast<unsigned>(j);
             }
             __syncthreads();
-            if (small_cells) {
-                for (int h = tid; h < 2 * ncur; h += nt) {
-                    const SubDesc &d = cur[h >> 1];
-                    if (!d.act) continue;
-                    const int mid = d.b + d.m;
-                    if (h & 1) seg_sort1(k0, k1, k2, mid, d.e);
-                    else seg_sort1(k0, k1, k2, d.b, mid);
-                }
-                __syncthreads();
-            } else {
+            {
                 for (int i = tid; i < ncur; i += nt)
                     if (cur[i].act) {
                         nxt[cur[i].rank].b = cur[i].b;
@@ -1944,7 +1914,7 @@ __global__ void __launch_bounds__(kSubThreads, 1) k_subtree(SubArgs A) {
                         nxt[cur[i].rank].m = cur[i].m;
                     }
                 __syncthreads();
-                sort_segments(k0, k1, k2, 2 * nact, [&](int g, int &b, int &e) {
+                sort_segments(k0, k1, k2, 2 * nact, maxlen, [&](int g, int &b, int &e) {
                     const SubDesc &d = nxt[g >> 1];
                     b = (g & 1) ? d.b + d.m : d.b;
                     e = (g & 1) ? d.e : d.b + d.m;
