@@ -901,7 +901,12 @@ __global__ void __launch_bounds__(kT) k_block_cut_cta(Level L, Free F, const int
     }
 }
 
-// One CTA per half: profile, stripes (getStripes), fill state.
+// One CTA per half: profile, stripes (getStripes), fill state. A profile of
+// up to kProfSmem edges is copied to shared memory before the stripe loop,
+// whose profile lookups are then shared-memory binary searches.
+constexpr int kProfSmem = 6144;
+constexpr size_t kHalfStripesSmem = sizeof(double) * 2 * kProfSmem;
+
 __global__ void __launch_bounds__(kT) k_half_stripes_cta(Level L, Free F, const int64_t *soff,
                                                          const Key *steps, const int64_t *nsteps,
                                                          const int64_t *eoff, double *pe, double *pp,
@@ -909,18 +914,30 @@ __global__ void __launch_bounds__(kT) k_half_stripes_cta(Level L, Free F, const 
                                                          double limit_density, Stripes S,
                                                          int *status) {
     __shared__ double stage[2 * kStage];
-    __shared__ long long s_ns;
+    __shared__ long long s_ns, s_n;
+    extern __shared__ double prof[];  // [2 * kProfSmem]
     const int h = blockIdx.x;
     const int blk = h >> 1, side = h & 1;
     const bool v = L.vert[blk] != 0;
     const double *box = L.half_box + 4 * h;
     double *e = pe + eoff[h], *p = pp + eoff[h];
-    const int64_t n = cta_build_profile(F, box, v, steps + soff[h], nsteps[h], e, p, stage);
+    const int64_t n0 = cta_build_profile(F, box, v, steps + soff[h], nsteps[h], e, p, stage);
+    if (threadIdx.x == 0) s_n = n0;
+    __syncthreads();
+    const int64_t n = s_n;
+    const bool local = n <= kProfSmem;
+    if (local) {
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            prof[i] = e[i];
+            prof[kProfSmem + i] = p[i];
+        }
+        __syncthreads();
+    }
     const int64_t so = S.off[h];
     if (threadIdx.x == 0) {
-        const Prof room{e, p, n};
+        const Prof room{local ? prof : e, local ? prof + kProfSmem : p, n};
         const double cell_area = side ? L.high_area[blk] : L.low_area[blk];
-        // cuts live after the profile in the same scratch
+        // cuts live after the profile in the global scratch
         int64_t ns = make_stripes(room, box, v, cell_area, L.room[blk], frac, limit_density,
                                   F.obst, F.K, L.cut[blk], side == 0, p + n, cap_over[h],
                                   S.a + so, S.b + so, S.cap + so);
@@ -2145,6 +2162,7 @@ struct LalState {
     DevBuf<double> sstrp;
     DevBuf<unsigned long long> sstrlh;
     bool subtree_attr = false;
+    bool half_stripes_attr = false;
     // counters of the last ktg_lal call (ktg_lal_stats)
     double stats[16] = {};
 };
@@ -2615,7 +2633,13 @@ int launch_lal(ktg_ctx *c, double *x, double *y, int32_t max_level, int32_t min_
             if ((r2 = seg_sort(c, s->steps.p, s->steps_tmp.p, ssegs, s->seg))) return r2;
             // 4. stripes per half (profile arrays: e in pe, p and the cuts in pp)
             Stripes S{s->stoff.p, s->scount.p, s->sa.p, s->sb.p, s->scap.p, s->sused.p, s->slo.p, s->shi.p};
-            k_half_stripes_cta<<<2 * na, kT, 0, c->stream>>>(
+            if (!s->half_stripes_attr) {
+                KTG_CUDA(c, cudaFuncSetAttribute(k_half_stripes_cta,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(kHalfStripesSmem)));
+                s->half_stripes_attr = true;
+            }
+            k_half_stripes_cta<<<2 * na, kT, kHalfStripesSmem, c->stream>>>(
                 L, F, s->hsoff.p, s->steps.p, s->hnsteps.p, s->heoff.p, s->pe.p, s->pp.p,
                 s->hbound.p, frac, c->density_limit, S, c->status);
             // 5. fill order, fill, stripe ranges, positions
