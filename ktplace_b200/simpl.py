@@ -9,6 +9,10 @@ so code written against the reference reads the same:
   solveBothAxes        simpl_lss.h:86-88
   getHpwl, getOccupancy, getOverflow
                        simplPlacer::Impl, simpl_placer.cc:256-297
+  SimplOptions         the legalizer's options, simpl_options.h:24-26
+  LookAheadLegalizer   simpl_lal.h:18-60 (legalize), built as
+                       simplPlacer::Impl::lookAheadLegalize does
+                       (simpl_placer.cc:299-310)
 
 All arithmetic runs in the CUDA library through the C ABI; nothing here
 computes a result on the CPU. A SparseSystem produced by buildB2B remembers
@@ -23,7 +27,7 @@ from typing import Callable, Optional
 import numpy as np
 
 from .gpu import Context
-from .grid import BinGrid
+from .grid import BinGrid, FreeSpace
 
 
 @dataclasses.dataclass
@@ -137,3 +141,37 @@ def getOverflowOf(context: Context, grid: BinGrid, x, y) -> float:
         context.set_grid(grid)
     _, ov = context.occupancy(x, y, want_map=False)
     return ov
+
+
+@dataclasses.dataclass
+class SimplOptions:
+    """The look-ahead legalizer's fields of SimplOptions (simpl_options.h:24-26)."""
+    maxLevel: int = 20
+    minCellsToSplit: int = 4
+    stripeAreaFraction: float = 0.1
+
+
+@dataclasses.dataclass
+class LookAheadLegalizer:
+    """LookAheadLegalizer (simpl_lal.h:18-60) on the GPU. The cell widths,
+    heights and areas are those of the netlist uploaded to ``context``;
+    ``freeSpace`` carries the rows, obstacles and die (grid.build_free_space);
+    ``densityLimit`` is the grid's. ``legalize`` updates x and y in place, as
+    the reference's does (ktg_lal: bit-identical positions)."""
+    context: Context
+    grid: BinGrid
+    freeSpace: FreeSpace
+    opts: SimplOptions = dataclasses.field(default_factory=SimplOptions)
+
+    def legalize(self, x: np.ndarray, y: np.ndarray) -> None:
+        ctx = self.context
+        if getattr(ctx, "grid", None) is not self.grid:
+            ctx.set_grid(self.grid)
+        if getattr(ctx, "_fs_obj", None) is not self.freeSpace:
+            ctx.set_free_space(self.freeSpace)
+            ctx._fs_obj = self.freeSpace
+        nx, ny = ctx.lal(x, y, self.opts.maxLevel, self.opts.minCellsToSplit,
+                         self.opts.stripeAreaFraction)
+        x[...] = nx
+        y[...] = ny
+

@@ -158,3 +158,22 @@ def test_lal_requires_free_space(gpu_ctx):
             gpu_ctx.lal(x, y)
     with pytest.raises(KtgError):
         gpu_ctx.lal(x, y, stripe_area_fraction=0.0)
+
+
+def test_simpl_mirror_legalizes_in_place(gpu_ctx):
+    """simpl.LookAheadLegalizer reads like the reference's (simpl_placer.cc:
+    299-310): built from the grid, the free space and the options, legalize()
+    updates x and y in place."""
+    from ktplace_b200 import simpl
+    raw = synth.generate(synth.spec_tiny(seed=5, macros=4, cells=900, nets=930))
+    nl = netlist.flatten(raw)
+    x, y = clustered(raw, nl.num_movable, 15, 0.08)
+    gpu_ctx.set_option("lal_subtree_cells", 2048)
+    gpu_ctx.set_option("lal_exact_sums", 1)
+    gpu_ctx.upload_netlist(nl)
+    legalizer = simpl.LookAheadLegalizer(gpu_ctx, grid.build_grid(nl, 24, 1.0),
+                                         grid.build_free_space(nl), simpl.SimplOptions())
+    px, py = x.copy(), y.copy()
+    legalizer.legalize(px, py)
+    ox, oy = run_oracle(nl, 24, 1.0, x, y)
+    assert np.array_equal(px, ox) and np.array_equal(py, oy)
