@@ -95,3 +95,34 @@ def test_gpu_star_build_bit_exact(gpu_ctx):
             s, t = cpu.system(axis), gpu_ctx.system(axis)
             for k in ("row_ptr", "col", "val", "diag", "rhs"):
                 assert np.array_equal(s[k].astype(np.float64), t[k].astype(np.float64)), (name, axis, k)
+
+
+@pytest.mark.parametrize("name,start", [("tiny_macros", "solved"), ("small12k", "solved"),
+                                        ("small12k", "packed")])
+def test_dropin_legalizer_matches_reference(name, start):
+    """simpl_lal_b200.cc in place of simpl_lal.o: the reference's own
+    simplPlacer::Impl::lookAheadLegalize, called on the same grid and
+    positions, gives bit-identical positions through the GPU legalizer."""
+    import resource
+    try:  # the reference legalizer's recursion wants a large stack
+        resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+    except (ValueError, OSError):
+        pass
+    raw, nl, x, y, ax, ay, alpha, bins = build_case(name)
+    cpu = oracle.RefDesign.from_netlist(nl, "cpu")
+    gpu = oracle.RefDesign.from_netlist(nl, "gpu")
+    if start == "solved":
+        cpu.build_b2b(x, y, alpha, ax if alpha > 0 else None, ay if alpha > 0 else None)
+        r = cpu.solve(x, y, TOL, MAX_ITER)
+        px, py = r["x"], r["y"]
+    else:
+        rng = np.random.default_rng(3)
+        lx, ly, ux, uy = nl.die
+        px = 0.5 * (lx + ux) + 0.03 * (ux - lx) * rng.standard_normal(nl.num_movable)
+        py = 0.5 * (ly + uy) + 0.03 * (uy - ly) * rng.standard_normal(nl.num_movable)
+    cpu.grid(bins, 1.0)
+    gpu.grid(bins, 1.0)
+    cx, cy = cpu.lal(px, py)
+    gx, gy = gpu.lal(px, py)
+    assert np.array_equal(cx, gx) and np.array_equal(cy, gy)
+    assert np.mean(cx != px) > 0.1
