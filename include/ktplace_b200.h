@@ -417,7 +417,13 @@ int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacl
  * values are what the project autotuner chooses between):
  *   "pcg_lanes"  1 or 4: threads per matrix row in the PCG SpMV (0 = default)
  *   "pcg_form"   0: textbook PCG (three grid barriers per iteration),
- *                1: Chronopoulos-Gear form (two), -1 = default (1)
+ *                1: Chronopoulos-Gear form (two), -1 = default (1),
+ *                2: textbook PCG with every dot product summed in the
+ *                reference's order (getDeterministicSum, simpl_parallel.h:
+ *                35-51: 4,096-element chunks left to right, then the chunk
+ *                sums in order) and one thread per matrix row: solutions,
+ *                iteration counts and residual histories are bit-identical
+ *                to solveBothAxes (about 2.4x the time of form 1)
  *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare),
  *                2: aggregation block-Jacobi, in ktg_solve_mixed
  *   "mixed_form" 1 (default): Chronopoulos-Gear mixed solve with per-block

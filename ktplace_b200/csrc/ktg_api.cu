@@ -240,6 +240,8 @@ void ktg_destroy(ktg_ctx *c) {
     free_systems(c);
     ktg::free_agg(c);
     ktg::free_lal(c);
+    dev_free(c->exact_prod);
+    dev_free(c->exact_cpart);
     dev_free(c->partials);
     dev_free(c->counters);
     dev_free(c->status);
@@ -297,7 +299,8 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         return KTG_OK;
     }
     if (k == "pcg_form") {
-        if (value < -1 || value > 1) return set_error(c, KTG_ERR_ARG, "pcg_form must be -1, 0 or 1");
+        if (value < -1 || value > 2)
+            return set_error(c, KTG_ERR_ARG, "pcg_form must be -1, 0, 1 or 2");
         c->pcg_form = static_cast<int>(value);
         return KTG_OK;
     }

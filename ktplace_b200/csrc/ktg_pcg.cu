@@ -70,6 +70,10 @@ struct PcgArgs {
     int64_t hist_cap;
     uint64_t barrier_timeout_ns;
     uint64_t total_timeout_ns;
+    // reference summation order (form 2): products, chunk partials
+    double *prod;     // [3][total_rows], row index axis * n + i
+    double *cpart;    // [6][nchunk]
+    int32_t nchunk;   // ceil(n / kGrain)
 };
 
 enum Slot { kBB = 0, kRZ0 = 1, kRR0 = 2, kPAP = 3, kRR = 4, kRZ = 5 };
@@ -100,6 +104,86 @@ __device__ __forceinline__ void reduce_partials(const PcgArgs &A, double (&out)[
         for (int k = 0; k < K; ++k) out[k] += __ldcg(slot_ptr(A, slot[k], axis[k]) + b);
     }
     block_sum_k<K>(out, scratch);
+}
+
+// ---- dot products in the reference's summation order (form 2) ----------------
+//
+// getDeterministicSum (simpl_parallel.h:35-51): chunks of kGrain elements,
+// each summed left to right from 0.0, then the chunk sums added in order.
+// The products are stored by the phase that computes them; after a grid
+// barrier one block per (dot, chunk) adds its chunk's products in order
+// (staged in shared memory, the next batch loading while thread 0 adds);
+// after a second barrier every block adds the chunk sums in order.
+constexpr int kGrain = 4096;
+constexpr int kStage = 128;  // chunk sums staged per round (fits the block's scratch)
+constexpr int kStageSum = 1024;  // products staged per round (one per thread)
+
+__device__ __forceinline__ double *prod_ptr(const PcgArgs &A, int vec) {
+    return A.prod + static_cast<size_t>(vec) * A.total_rows;
+}
+
+template <int K>
+__device__ bool ref_order_dots(const PcgArgs &A, const int (&vec)[K], const int (&axis)[K],
+                               const bool (&want)[K], double (&out)[K], double *sh, double *stage,
+                               uint64_t deadline_ns) {
+    const int32_t n = A.ax[0].n;
+    const int32_t nc = A.nchunk;
+    const int64_t tasks = static_cast<int64_t>(K) * nc;
+    // one block per (dot, chunk): the products are staged kStageSum at a
+    // time in shared memory (the next batch already in flight in registers)
+    // and thread 0 adds them in index order
+    for (int64_t t = blockIdx.x; t < tasks; t += gridDim.x) {
+        const int k = static_cast<int>(t / nc), c = static_cast<int>(t % nc);
+        bool on = false;
+        int v = 0, a = 0;
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+            if (q == k) {
+                on = want[q];
+                v = vec[q];
+                a = axis[q];
+            }
+        if (!on) continue;
+        const double *pr = prod_ptr(A, v) + (a ? n : 0);
+        const int32_t b = c * kGrain, e = min(n, b + kGrain);
+        double next = static_cast<int32_t>(b + threadIdx.x) < e ? __ldcg(pr + b + threadIdx.x) : 0.0;
+        double sum = 0.0;
+        for (int32_t base = b; base < e; base += kStageSum) {
+            const int32_t cnt = min(kStageSum, e - base);
+            __syncthreads();  // the previous batch is consumed
+            if (static_cast<int32_t>(threadIdx.x) < cnt) stage[threadIdx.x] = next;
+            __syncthreads();
+            const int32_t nb = base + kStageSum + static_cast<int32_t>(threadIdx.x);
+            next = nb < e ? __ldcg(pr + nb) : 0.0;
+            if (threadIdx.x == 0)
+                for (int32_t i = 0; i < cnt; ++i) sum += stage[i];
+        }
+        if (threadIdx.x == 0) __stcg(A.cpart + static_cast<size_t>(k) * nc + c, sum);
+    }
+    if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline_ns)) return false;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (!want[k]) {
+            out[k] = 0.0;
+            continue;
+        }
+        const double *cp = A.cpart + static_cast<size_t>(k) * nc;
+        double s = 0.0;
+        for (int32_t c0 = 0; c0 < nc; c0 += kStage) {  // staged, then added in order
+            const int32_t cnt = min(kStage, nc - c0);
+            __syncthreads();
+            if (static_cast<int32_t>(threadIdx.x) < cnt) sh[threadIdx.x] = __ldcg(cp + c0 + threadIdx.x);
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int32_t c = 0; c < cnt; ++c) s += sh[c];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sh[0] = s;
+        __syncthreads();
+        out[k] = sh[0];
+    }
+    __syncthreads();
+    return true;
 }
 
 // Off-diagonal part of row i of S times `in` (gathered from global memory,
@@ -147,10 +231,11 @@ __device__ __forceinline__ double row_offdiag_vec4(const PcgAxis &S, int32_t i, 
     return s;
 }
 
-template <bool Smem, int Lanes>
+template <bool Smem, int Lanes, bool Exact = false>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     extern __shared__ double dyn[];
     __shared__ double scratch[33 * 4];
+    __shared__ double exstage[Exact ? kStageSum : 1];  // reference-order sums
     __shared__ PcgAxis sax[2];
     if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
     const uint64_t t_start = global_timer_ns();
@@ -244,25 +329,47 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                      S.z[i] = z;
                  }
                  __stcg(S.p + i, z);
-                 acc[axis * 3 + 0] += b * b;
-                 acc[axis * 3 + 1] += r * z;
-                 acc[axis * 3 + 2] += r * r;
+                 if constexpr (Exact) {
+                     const int32_t ci = axis ? n0 + i : i;
+                     __stcg(prod_ptr(A, 0) + ci, b * b);
+                     __stcg(prod_ptr(A, 1) + ci, r * z);
+                     __stcg(prod_ptr(A, 2) + ci, r * r);
+                 } else {
+                     acc[axis * 3 + 0] += b * b;
+                     acc[axis * 3 + 1] += r * z;
+                     acc[axis * 3 + 2] += r * r;
+                 }
              },
              nullptr);
-        double v0[3] = {acc[0], acc[1], acc[2]};
-        double v1[3] = {acc[3], acc[4], acc[5]};
-        const int sl[3] = {kBB, kRZ0, kRR0};
-        const int a0[3] = {0, 0, 0};
-        const int a1[3] = {1, 1, 1};
-        store_partials<3>(A, v0, sl, a0, scratch);
-        store_partials<3>(A, v1, sl, a1, scratch);
+        if constexpr (!Exact) {
+            double v0[3] = {acc[0], acc[1], acc[2]};
+            double v1[3] = {acc[3], acc[4], acc[5]};
+            const int sl[3] = {kBB, kRZ0, kRR0};
+            const int a0[3] = {0, 0, 0};
+            const int a1[3] = {1, 1, 1};
+            store_partials<3>(A, v0, sl, a0, scratch);
+            store_partials<3>(A, v1, sl, a1, scratch);
+        }
     }
     if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
 
     double b_norm[2], rho[2], resid[2];
     bool active[2];
     int64_t steps[2] = {0, 0};
-    {
+    if constexpr (Exact) {
+        double s[6];
+        const int vec[6] = {0, 1, 2, 0, 1, 2};
+        const int ax[6] = {0, 0, 0, 1, 1, 1};
+        const bool want[6] = {true, true, true, true, true, true};
+        if (!ref_order_dots<6>(A, vec, ax, want, s, scratch, exstage, deadline())) return;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            b_norm[a] = sqrt(s[3 * a]);
+            active[a] = b_norm[a] > 0.0;
+            rho[a] = active[a] ? s[3 * a + 1] : 0.0;
+            resid[a] = active[a] ? sqrt(s[3 * a + 2]) / b_norm[a] : 0.0;
+        }
+    } else {
         double s[4];
         const int sl[4] = {kBB, kRZ0, kRR0, kBB};
         const int ax[4] = {0, 0, 0, 1};
@@ -299,10 +406,13 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                      sap[l] = ap;
                  else
                      sax[axis].ap[i] = ap;
-                 pap_acc[axis] += pi * ap;
+                 if constexpr (Exact)
+                     __stcg(prod_ptr(A, 0) + (axis ? n0 + i : i), pi * ap);
+                 else
+                     pap_acc[axis] += pi * ap;
              },
              live);
-        {
+        if constexpr (!Exact) {
             const int sl[2] = {kPAP, kPAP};
             const int ax[2] = {0, 1};
             store_partials<2>(A, pap_acc, sl, ax, scratch);
@@ -313,9 +423,16 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
         bool ok[2];
         {
             double pap[2];
-            const int sl[2] = {kPAP, kPAP};
-            const int ax[2] = {0, 1};
-            reduce_partials<2>(A, pap, sl, ax, scratch);
+            if constexpr (Exact) {
+                const int vec[2] = {0, 0};
+                const int ax[2] = {0, 1};
+                const bool want[2] = {live[0], live[1]};
+                if (!ref_order_dots<2>(A, vec, ax, want, pap, scratch, exstage, deadline())) return;
+            } else {
+                const int sl[2] = {kPAP, kPAP};
+                const int ax[2] = {0, 1};
+                reduce_partials<2>(A, pap, sl, ax, scratch);
+            }
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
                 ok[a] = live[a] && pap[a] > 0.0;
@@ -340,10 +457,16 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             const double z = r / d;
             KTG_V(sr, r) = r;
             KTG_V(sz, z) = z;
-            acc[axis * 2 + 0] += r * r;
-            acc[axis * 2 + 1] += r * z;
+            if constexpr (Exact) {
+                const int32_t ci = axis ? n0 + i : i;
+                __stcg(prod_ptr(A, 1) + ci, r * r);
+                __stcg(prod_ptr(A, 2) + ci, r * z);
+            } else {
+                acc[axis * 2 + 0] += r * r;
+                acc[axis * 2 + 1] += r * z;
+            }
         }
-        {
+        if constexpr (!Exact) {
             const int sl[4] = {kRR, kRZ, kRR, kRZ};
             const int ax[4] = {0, 0, 1, 1};
             store_partials<4>(A, acc, sl, ax, scratch);
@@ -355,9 +478,16 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
         double rho_next[2] = {0.0, 0.0};
         {
             double s[4];
-            const int sl[4] = {kRR, kRZ, kRR, kRZ};
-            const int ax[4] = {0, 0, 1, 1};
-            reduce_partials<4>(A, s, sl, ax, scratch);
+            if constexpr (Exact) {
+                const int vec[4] = {1, 2, 1, 2};
+                const int ax[4] = {0, 0, 1, 1};
+                const bool want[4] = {ok[0], ok[0], ok[1], ok[1]};
+                if (!ref_order_dots<4>(A, vec, ax, want, s, scratch, exstage, deadline())) return;
+            } else {
+                const int sl[4] = {kRR, kRZ, kRR, kRZ};
+                const int ax[4] = {0, 0, 1, 1};
+                reduce_partials<4>(A, s, sl, ax, scratch);
+            }
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
                 if (!ok[a]) continue;
@@ -712,8 +842,11 @@ struct Variant {
     int vecs_per_row;
 };
 
-// form 0: textbook three-barrier PCG; form 1: Chronopoulos-Gear two-barrier.
+// form 0: textbook three-barrier PCG; form 1: Chronopoulos-Gear two-barrier;
+// form 2: textbook PCG with the reference's summation order everywhere (one
+// thread per row; bit-identical to the reference's solve).
 Variant pick_variant(int form, bool smem, int lanes) {
+    if (form == 2) return {smem ? k_pcg<true, 1, true> : k_pcg<false, 1, true>, kVecsPerRow};
     if (form == 1) {
         if (smem) return {lanes == 4 ? k_pcg_cg<true, 4> : k_pcg_cg<true, 1>, 7};
         return {lanes == 4 ? k_pcg_cg<false, 4> : k_pcg_cg<false, 1>, 7};
@@ -750,7 +883,7 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     const bool use_smem = smem <= static_cast<size_t>(kPcgSmemBytes);
     const Variant v = pick_variant(form, use_smem, lanes);
     const size_t dyn = use_smem ? smem : 0;
-    static bool attr_set[2][2][2] = {};
+    static bool attr_set[3][2][2] = {};
     bool &done = attr_set[form][use_smem][lanes == 4];
     if (!done) {
         KTG_CUDA(c, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -773,6 +906,29 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     A.hist_x = hist_x;
     A.hist_y = hist_y;
     A.hist_cap = hist_cap;
+    A.prod = nullptr;
+    A.cpart = nullptr;
+    A.nchunk = static_cast<int32_t>((nsys + kGrain - 1) / kGrain);
+    if (form == 2) {  // products and chunk sums of the reference-order dots
+        const int64_t need_prod = 3 * std::max<int64_t>(2 * nsys, 1);
+        const int64_t need_cpart = 6 * std::max<int64_t>(A.nchunk, 1);
+        if (need_prod > c->exact_prod_cap) {
+            if (c->exact_prod) cudaFree(c->exact_prod);
+            c->exact_prod = nullptr;
+            c->exact_prod_cap = 0;
+            KTG_CUDA(c, cudaMalloc(&c->exact_prod, sizeof(double) * need_prod));
+            c->exact_prod_cap = need_prod;
+        }
+        if (need_cpart > c->exact_cpart_cap) {
+            if (c->exact_cpart) cudaFree(c->exact_cpart);
+            c->exact_cpart = nullptr;
+            c->exact_cpart_cap = 0;
+            KTG_CUDA(c, cudaMalloc(&c->exact_cpart, sizeof(double) * need_cpart));
+            c->exact_cpart_cap = need_cpart;
+        }
+        A.prod = c->exact_prod;
+        A.cpart = c->exact_cpart;
+    }
     A.barrier_timeout_ns = 2000000000ull;   // 2 s for any single barrier
     A.total_timeout_ns = 120000000000ull;   // 120 s for the whole solve
     KTG_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));

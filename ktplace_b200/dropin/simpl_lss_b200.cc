@@ -20,6 +20,10 @@
 //     copy. By default the whole CSR is copied back, as the reference fills it.
 //   * the IterateObserver is replayed after the device solve with each
 //     iterate's residuals; x and y already hold the final solution then.
+//   * solveBothAxes sums its dot products in the reference's order
+//     (pcg_form 2), so solutions, iteration counts and residuals are the
+//     reference's bit for bit; $KTPLACE_B200_PCG_FORM=1 selects the faster
+//     two-barrier form, whose results agree to about 1e-9 relative.
 #include "globalPlacer/simpl/simpl_lss.h"
 #include "util/kt_log.h"
 
@@ -67,8 +71,10 @@ ktg_ctx *context() {
     if (s.ctx == nullptr) {
         const char *dev = std::getenv("KTPLACE_B200_DEVICE");
         const char *csr = std::getenv("KTPLACE_B200_HOST_CSR");
+        const char *form = std::getenv("KTPLACE_B200_PCG_FORM");
         s.hostCsr = !(csr != nullptr && std::string(csr) == "0");
         check("ktg_create", ktg_create(dev ? std::atoi(dev) : 0, &s.ctx));
+        check("ktg_set_option", ktg_set_option(s.ctx, "pcg_form", form ? std::atoi(form) : 2));
     }
     return s.ctx;
 }

@@ -1,11 +1,12 @@
-"""The C++ drop-in (ktplace_b200/dropin/simpl_lss_b200.cc) inside the
-reference's own, unmodified SimPL code.
+"""The C++ drop-ins (ktplace_b200/dropin/simpl_lss_b200.cc and
+simpl_lal_b200.cc) inside the reference's own, unmodified SimPL code.
 
 oracle/_ref/libktref_gpu.so is the reference's SimPL compiled from its sources
-with the drop-in linked in place of simpl_lss.o; oracle/_ref/libktref.so is the
-same code with the reference's simpl_lss.o. The reference interface
-(LinearSystems::buildB2B, solveBothAxes) must give the same systems and
-solutions, and a whole SimPL run must land on the same placement quality.
+with the drop-ins linked in place of simpl_lss.o and simpl_lal.o;
+oracle/_ref/libktref.so is the same code with the reference's objects. The
+reference interface (LinearSystems::buildB2B, solveBothAxes,
+LookAheadLegalizer::legalize) must give the same systems, solutions and
+positions, and a whole SimPL run must land on the same placement.
 """
 import os
 import sys
@@ -65,14 +66,21 @@ def test_star_systems_solve_on_gpu():
 
 
 def test_full_simpl_run_matches_reference():
-    """Whole SimPL flow (star init, B2B rounds, LAL, refinement) with the
-    solve on the GPU: the final HPWL and overflow stay within 0.5% of the
-    CPU run (the trajectories differ only by round-off in the solves)."""
+    """Whole SimPL flow (star init, B2B rounds, LAL, refinement) with both
+    drop-ins: the solve sums in the reference's order (the drop-in's default)
+    and the legalizer is exact, so the final placement is the CPU run's, bit
+    for bit."""
+    import resource
+    try:  # the reference legalizer's recursion wants a large stack
+        resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+    except (ValueError, OSError):
+        pass
     raw, nl, *_ = build_case("small12k")
     cpu = oracle.RefDesign.from_netlist(nl, "cpu")
     gpu = oracle.RefDesign.from_netlist(nl, "gpu")
     cx, cy = cpu.run_simpl()
     gx, gy = gpu.run_simpl()
+    assert np.array_equal(cx, gx) and np.array_equal(cy, gy)
     hc, hg = cpu.hpwl(cx, cy), cpu.hpwl(gx, gy)
     assert abs(hg - hc) <= 5e-3 * hc, (hg, hc)
     nb = 64 * 64
