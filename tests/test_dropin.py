@@ -134,3 +134,21 @@ def test_dropin_legalizer_matches_reference(name, start):
     gx, gy = gpu.lal(px, py)
     assert np.array_equal(cx, gx) and np.array_equal(cy, gy)
     assert np.mean(cx != px) > 0.1
+
+
+def test_full_simpl_run_211k_identical():
+    """The same at 211k cells (the bench netlist, 550 macros): the reference's
+    SimPL with both drop-ins ends on the CPU run's placement, bit for bit."""
+    import resource
+    try:
+        resource.setrlimit(resource.RLIMIT_STACK, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+    except (ValueError, OSError):
+        pass
+    from ktplace_b200 import netlist, synth
+    nl = netlist.flatten(synth.generate(synth.spec_adaptec1_like(seed=1)))
+    threads = os.cpu_count() or 1
+    oracle.set_ref_threads(threads, "cpu")
+    oracle.set_ref_threads(threads, "gpu")
+    cx, cy = oracle.RefDesign.from_netlist(nl, "cpu").run_simpl()
+    gx, gy = oracle.RefDesign.from_netlist(nl, "gpu").run_simpl()
+    assert np.array_equal(cx, gx) and np.array_equal(cy, gy)
