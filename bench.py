@@ -56,6 +56,9 @@ def parse():
                     help="skip the batched-solve leg (64 netlists, 128 systems)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="run the batched-solve workload once for an ncu capture")
+    ap.add_argument("--config4", action="store_true",
+                    help="only the solve comparison (FP64, FP32 with Jacobi / learned / "
+                         "aggregation) on the 2.2M-cell design; prints one JSON line")
     ap.add_argument("--profile-lal", action="store_true",
                     help="run only the look-ahead legalization of the step's solved positions "
                          "twice (the capture workload of profiles/lal_*)")
@@ -796,8 +799,47 @@ def profile_lal():
     return 0
 
 
+def run_config4(args) -> int:
+    """The solve comparison of `solve_variants` on the 2.2M-cell design (2.25M
+    nets, 8,000 macros; seed positions and anchors), the configuration the
+    learned preconditioner is specified at. One GPU; not part of the default
+    run (the design alone takes tens of seconds to generate)."""
+    import torch
+    from ktplace_b200 import netlist, synth
+    from ktplace_b200.gpu import Context
+    from ktplace_b200._lib import SolveInfo
+    raw = synth.generate(synth.spec_2m(4))
+    nl = netlist.flatten(raw)
+    x, y = synth.seed_positions(raw, nl.num_movable, 104)
+    ax, ay = synth.seed_positions(raw, nl.num_movable, 204)
+    fx, fy = nl.floors()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    ctx = Context(0)
+    ctx.upload_netlist(nl)
+    ctx.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        dx, dy = torch.tensor(x, device=dev), torch.tensor(y, device=dev)
+        dax, day = torch.tensor(ax, device=dev), torch.tensor(ay, device=dev)
+        wx, wy = torch.empty_like(dx), torch.empty_like(dy)
+        info = torch.zeros(ctypes.sizeof(SolveInfo), dtype=torch.uint8, device=dev)
+        scal = torch.zeros(8, dtype=torch.float64, device=dev)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(dev)
+    variants = solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, info,
+                              scal, flush, max(3, args.steps // 20))
+    print(json.dumps({"config": "2.2M cells, 2.25M nets, 8,000 macros (seed 4), positions seed "
+                                "104, anchors seed 204, alpha 0.2, rtol 1e-6",
+                      "cells": nl.num_movable, "nets": nl.num_nets, "pins": nl.num_pins,
+                      "solve_variants": variants}))
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.config4:
+        return run_config4(args)
     if args.profile_once:
         return profile_once()
     if args.profile_lal:

@@ -96,3 +96,34 @@ def test_hpwl_density_and_legalization_2m(design, built):
     lx, ly = ref.lal(px, py)
     assert np.array_equal(gx, lx) and np.array_equal(gy, ly)
     assert np.mean(gx != px) > 0.1
+
+
+@pytest.mark.parametrize("precond", [0, 2, 1])
+def test_mixed_solves_2m(precond, design, built):
+    """Mixed precision at 2.2M cells (FP32 PCG inside FP64 refinement) with
+    the Jacobi, aggregation and learned preconditioners: true residual at the
+    tolerance and HPWL within 0.1% of the FP64 solve's."""
+    nl, x, y, ax, ay, ref = design
+    ctx = built
+    d = ctx.solve(x, y, 1e-6, 100000)
+    h64 = ctx.hpwl(d["x"], d["y"])
+    learned = None
+    try:
+        if precond == 1:
+            from ktplace_b200.learned import Learned
+            w = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                             "ktplace_b200", "weights", "learned_precond.npy")
+            if not os.path.exists(w):
+                pytest.skip("no trained weights")
+            learned = Learned(0)
+            learned.load(w)
+            learned.prepare(ctx)
+        ctx.set_option("precond", precond)
+        m = ctx.solve_mixed(x, y, 1e-6, 1e-3)
+    finally:
+        ctx.set_option("precond", 0)
+        if learned is not None:
+            learned.close()
+    assert max(m["resid"]) <= 1e-6
+    h = ctx.hpwl(m["x"], m["y"])
+    assert abs(h - h64) <= 1e-3 * h64
