@@ -56,6 +56,11 @@ def parse():
                     help="skip the batched-solve leg (64 netlists, 128 systems)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="run the batched-solve workload once for an ncu capture")
+    ap.add_argument("--profile-pcg", type=int, default=0, metavar="CELLS",
+                    help="only one B2B build and FP64 solve of a synthetic design with CELLS "
+                         "movable cells (scaled from the 211k design), timed, with its "
+                         "algorithmic bytes per second; the capture workload of "
+                         "profiles/k_pcg_cg_beyond_l2.md")
     ap.add_argument("--config4", action="store_true",
                     help="only the solve comparison (FP64, FP32 with Jacobi / learned / "
                          "aggregation) on the 2.2M-cell design; prints one JSON line")
@@ -799,6 +804,65 @@ def profile_lal():
     return 0
 
 
+def profile_pcg(cells: int) -> int:
+    """A design of `cells` movable cells with the 211k design's proportions
+    (nets 1.05x, rows and pads by the square root, macros by the cell count),
+    seed 7: one B2B build (alpha 0.2, anchors) and three FP64 solves to rtol
+    1e-6 from the same start, timed with CUDA events; prints the median time,
+    iterations and the algorithmic bytes per second of the solve (pcg_bytes)."""
+    import math
+    import torch
+    from ktplace_b200 import netlist, synth
+    from ktplace_b200.gpu import Context
+    from ktplace_b200._lib import SolveInfo
+    k = cells / 211_000
+    spec = synth.SynthSpec(num_movable=cells, num_nets=int(round(1.0474 * cells)),
+                           num_pads=int(round(1000 * math.sqrt(k))),
+                           num_rows=int(round(890 * math.sqrt(k))), utilization=0.6,
+                           num_macros=int(round(550 * k)), seed=7, name=f"synth{cells}")
+    raw = synth.generate(spec)
+    nl = netlist.flatten(raw)
+    x, y = synth.seed_positions(raw, nl.num_movable, 107)
+    ax, ay = synth.seed_positions(raw, nl.num_movable, 207)
+    fx, fy = nl.floors()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    ctx = Context(0)
+    ctx.upload_netlist(nl)
+    ctx.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        dx, dy = torch.tensor(x, device=dev), torch.tensor(y, device=dev)
+        dax, day = torch.tensor(ax, device=dev), torch.tensor(ay, device=dev)
+        wx, wy = torch.empty_like(dx), torch.empty_like(dy)
+        info = torch.zeros(ctypes.sizeof(SolveInfo), dtype=torch.uint8, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(3):
+        with torch.cuda.stream(stream):
+            ctx.build_b2b_dev(dx, dy, ALPHA, dax, day, fx, fy)
+            wx.copy_(dx)
+            wy.copy_(dy)
+            e0.record(stream)
+            ctx.solve_dev(wx, wy, TOL, MAX_ITER, info)
+            e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    inf = SolveInfo.from_buffer_copy(bytes(info.cpu().numpy()))
+    _, mx = ctx.system_info(0)
+    _, my = ctx.system_info(1)
+    n = nl.num_movable
+    byts = pcg_bytes(n, mx, inf.iters_x) + pcg_bytes(n, my, inf.iters_y)
+    t = statistics.median(ms)
+    peak, kind = measured_peak()
+    print(json.dumps({"cells": n, "nnz": [mx, my], "iters": [int(inf.iters_x), int(inf.iters_y)],
+                      "solve_ms": t, "algorithmic_bytes": byts,
+                      "achieved_gbs": byts / (t * 1e-3) / 1e9, "peak_gbs": peak,
+                      "peak_kind": kind, "frac": byts / (t * 1e-3) / 1e9 / peak}))
+    ctx.close()
+    return 0
+
+
 def run_config4(args) -> int:
     """The solve comparison of `solve_variants` on the 2.2M-cell design (2.25M
     nets, 8,000 macros; seed positions and anchors), the configuration the
@@ -838,6 +902,8 @@ def run_config4(args) -> int:
 
 def main():
     args = parse()
+    if args.profile_pcg:
+        return profile_pcg(args.profile_pcg)
     if args.config4:
         return run_config4(args)
     if args.profile_once:
