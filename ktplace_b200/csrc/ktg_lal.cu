@@ -780,21 +780,38 @@ __device__ int64_t cta_build_profile(const Free &F, const double *box, bool v, c
         p[0] = 0.0;
     }
     if (v) {
+        // chunk c + 1 is loaded into registers while thread 0 walks chunk c
+        constexpr int kPer = kStage / kT;
+        Key nxt[kPer];
+        auto fetch = [&](int64_t c0) {
+#pragma unroll
+            for (int u = 0; u < kPer; ++u) {
+                const int64_t k = c0 + u * nt + tid;
+                nxt[u] = k < nsteps ? steps[k] : Key{0ull, 0ull};
+            }
+        };
+        fetch(0);
         for (int64_t c0 = 0; c0 < nsteps; c0 += kStage) {
             const int cnt = static_cast<int>(nsteps - c0 < kStage ? nsteps - c0 : kStage);
-            for (int i = tid; i < cnt; i += nt) {
-                stage[2 * i] = unord(steps[c0 + i].a);
-                stage[2 * i + 1] = unord(steps[c0 + i].b);
+            __syncthreads();  // the previous chunk is consumed
+#pragma unroll
+            for (int u = 0; u < kPer; ++u) {
+                const int i = u * nt + tid;
+                if (i < cnt) {
+                    stage[2 * i] = unord(nxt[u].a);
+                    stage[2 * i + 1] = unord(nxt[u].b);
+                }
             }
             __syncthreads();
+            fetch(c0 + kStage);
             if (tid == 0)
                 for (int i = 0; i < cnt; ++i) {
                     const double at = stage[2 * i], dh = stage[2 * i + 1];
                     extend(at, height * (at - elast));
                     height += dh;
                 }
-            __syncthreads();
         }
+        __syncthreads();
     } else {
         int32_t r0, r1;
         box_rows(F, box, r0, r1);
