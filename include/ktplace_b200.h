@@ -275,7 +275,9 @@ int ktg_set_free_space(ktg_ctx *ctx, int64_t num_rows, const double *row_y,
  * Positions are bit-identical to the reference when the cell areas are
  * multiples of 2^-s (s the occupancy's fixed-point shift; integer site
  * areas qualify): the bin occupancies it grows clusters from are exact then.
- * The cluster/grow/batch loop runs on the host between batches. */
+ * The cluster/grow/batch loop runs on the host between batches, so the call
+ * synchronises with the context's stream and returns after the positions are
+ * final in both pointer modes (device pointers are updated in place). */
 int ktg_lal(ktg_ctx *ctx, double *x, double *y, int32_t max_level, int32_t min_cells_to_split,
             double stripe_area_fraction);
 
