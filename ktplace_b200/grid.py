@@ -54,17 +54,28 @@ def default_bins_per_axis(num_movable: int) -> int:
     return int(min(max(v, 16.0), 256.0))
 
 
-def free_spans(rows: np.ndarray, obstacles: np.ndarray):
-    """FreeSpace::build: per row (sorted by bottom edge) the free x spans."""
+def free_spans(rows: np.ndarray, obstacles: np.ndarray, subrows=None):
+    """FreeSpace::build: per row (sorted by bottom edge) the free x spans.
+
+    A row's spans are its subrows' x intervals (buildGrid, simpl_placer.cc:
+    199-212) when `subrows` ([S, 3]: row index, x start, x end, as the
+    Bookshelf reader returns them) is given, else the row's one span
+    (xlo, xhi)."""
     out = []
     smallest = math.inf
     raw = []
-    for r in rows:
+    per_row = None
+    if subrows is not None and len(subrows):
+        per_row = {}
+        for sr in np.asarray(subrows, np.float64).reshape(-1, 3):
+            per_row.setdefault(int(sr[0]), []).append((float(sr[1]), float(sr[2])))
+    for ri, r in enumerate(rows):
         coord, height, pitch, xlo, xhi = (float(v) for v in r)
         if not (height > 0.0) or not (pitch > 0.0):
             continue
         smallest = min(smallest, pitch * height)
-        raw.append((coord, coord + height, [(xlo, xhi)]))
+        spans = [(xlo, xhi)] if per_row is None else per_row.get(ri, [])
+        raw.append((coord, coord + height, spans))
     raw.sort(key=lambda t: t[0])  # stable
     for y0, y1, spans in raw:
         cuts = sorted((float(o[0]), float(o[2])) for o in obstacles
@@ -99,7 +110,7 @@ class FreeSpace:
 def build_free_space(nl) -> FreeSpace:
     """The free space LookAheadLegalizer works in: the design's rows cut by its
     obstacles (free_spans), the same obstacles and the die."""
-    rows, _ = free_spans(nl.rows, nl.obstacles)
+    rows, _ = free_spans(nl.rows, nl.obstacles, getattr(nl, "subrows", None))
     row_y = np.array([(r[0], r[1]) for r in rows], np.float64).reshape(-1, 2)
     counts = np.array([len(r[2]) for r in rows], np.int64)
     row_span = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
@@ -115,7 +126,7 @@ def build_grid(nl, per_axis: int, density_limit: float = 1.0) -> BinGrid:
     dx = _max(ux - lx, 1e-9) / float(per_axis)
     dy = _max(uy - ly, 1e-9) / float(per_axis)
     avail = np.zeros(nx * ny)
-    rows, smallest = free_spans(nl.rows, nl.obstacles)
+    rows, smallest = free_spans(nl.rows, nl.obstacles, getattr(nl, "subrows", None))
 
     def col(x):
         return _clamp_index((x - lx) / dx, nx)

@@ -175,3 +175,34 @@ def test_missing_nodes_is_an_error(tmp_path):
     from ktplace_b200._lib import KtgError
     with pytest.raises(KtgError):
         bookshelf.read(d)
+
+
+def test_grid_and_free_space_follow_subrows(tmp_path):
+    """A row split into subrows with a gap that no obstacle covers: the bin
+    grid's free area and the legalizer's free space come from the subrows,
+    as the reference's buildGrid takes them, and match the reference."""
+    if not oracle.ref_available():
+        pytest.skip("reference library not built")
+    from ktplace_b200 import grid
+    scl = SCL.replace("""  Sitespacing : 0
+  SubrowOrigin : 0 NumSites : 60
+End""", """  Sitespacing : 0
+  SubrowOrigin : 0 NumSites : 15
+  SubrowOrigin : 70 NumSites : 25
+End""")
+    d = os.path.join(str(tmp_path), "gapped")
+    os.makedirs(d)
+    for ext, text in ((".nodes", NODES), (".wts", WTS), (".nets", NETS), (".pl", PL), (".scl", scl)):
+        with open(os.path.join(d, "gapped" + ext), "w", newline="") as f:
+            f.write(text)
+    nl = bookshelf.read(d)
+    ref = oracle.RefDesign.from_bookshelf(d)
+    for bins in (4, 8):
+        g = ref.grid(bins, 1.0)
+        mine = grid.build_grid(nl, bins, 1.0)
+        assert np.array_equal(mine.avail, g["avail"]) and mine.total_avail == g["total_avail"]
+    rows, rs, spans = ref.free_space()
+    fs = grid.build_free_space(nl)
+    assert np.array_equal(rows, fs.row_y) and np.array_equal(rs, fs.row_span)
+    assert np.array_equal(spans, fs.spans)
+    assert [30.0, 70.0] in [[a, b] for a, b in zip(spans[:-1, 1], spans[1:, 0])]  # the gap
