@@ -417,15 +417,19 @@ int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacl
 
 /* Sets a kernel-shape option of this context (no reference counterpart; the
  * values are what the project autotuner chooses between):
- *   "pcg_lanes"  1 or 4: threads per matrix row in the PCG SpMV (0 = default)
+ *   "pcg_lanes"  SpMV shape in the PCG: 32 = warp tiles (a warp streams the
+ *                nonzeros of 32 consecutive rows, each lane adding its row's
+ *                products in storage order), 1 = one thread per row (the
+ *                same row sums, so the same solve bit for bit), 4 = four
+ *                lanes per row; 0 = default (32)
  *   "pcg_form"   0: textbook PCG (three grid barriers per iteration),
- *                1: Chronopoulos-Gear form (two), -1 = default (1),
+ *                1: Chronopoulos-Gear form (two), -1 = default (0),
  *                2: textbook PCG with every dot product summed in the
  *                reference's order (getDeterministicSum, simpl_parallel.h:
  *                35-51: 4,096-element chunks left to right, then the chunk
- *                sums in order) and one thread per matrix row: solutions,
- *                iteration counts and residual histories are bit-identical
- *                to solveBothAxes (about 2.4x the time of form 1)
+ *                sums in order): solutions, iteration counts and residual
+ *                histories are bit-identical to solveBothAxes (about 2.6x
+ *                the time of form 0)
  *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare),
  *                2: aggregation block-Jacobi, in ktg_solve_mixed
  *   "mixed_form" 1 (default): Chronopoulos-Gear mixed solve with per-block
@@ -459,9 +463,11 @@ int ktg_lal_stats(ktg_ctx *ctx, double *out, int32_t count);
 
 /* Test of the bounded device waits: a cooperative launch in which one block
  * never arrives at a grid barrier, so the other's wait gives up after
- * timeout_ns (at most 1 s) and reports through the status word; *status_out
- * receives that status (KTG_ERR_TIMEOUT). Nothing faults and the context
- * stays usable. No reference counterpart (the reference has no device). */
+ * timeout_ns (at most 1 s) and reports through the status word; run once
+ * with each of the library's two grid barriers. *status_out receives
+ * KTG_ERR_TIMEOUT when both gave up as they should, else the first other
+ * status. Nothing faults and the context stays usable. No reference
+ * counterpart (the reference has no device). */
 int ktg_selftest_wait_timeout(ktg_ctx *ctx, int64_t timeout_ns, int *status_out);
 
 /* ---- allocation-free HPWL ------------------------------------------------ */

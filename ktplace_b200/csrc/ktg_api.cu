@@ -282,8 +282,8 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
     if (!c || !key) return KTG_ERR_ARG;
     const std::string k(key);
     if (k == "pcg_lanes") {
-        if (value != 0 && value != 1 && value != 4)
-            return set_error(c, KTG_ERR_ARG, "pcg_lanes must be 0, 1 or 4");
+        if (value != 0 && value != 1 && value != 4 && value != 32)
+            return set_error(c, KTG_ERR_ARG, "pcg_lanes must be 0, 1, 4 or 32");
         c->pcg_lanes = static_cast<int>(value);
         return KTG_OK;
     }

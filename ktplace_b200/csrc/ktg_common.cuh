@@ -168,4 +168,55 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, int
     return ok != 0;
 }
 
+// Grid barrier for the persistent solvers, with grid_barrier's contract but
+// fewer round trips to L2 on the critical path: the generation a block waits
+// on is kept in a register of thread 0 (read once by grid_sync_init, before
+// the first arrival, when every block sees the same value), arriving is one
+// acq_rel atomic (its release half publishes the block's writes, ordered
+// before it by __syncthreads) and waiting is one acquire load per poll (its
+// acquire half orders the block's later reads). Other blocks' errors are
+// seen while polling; a block that passes a barrier another block gave up
+// on stops at its next one.
+struct GridSync {
+    unsigned *count;
+    unsigned *gen;
+    int *status;
+    unsigned open_gen;  // meaningful in thread 0 only
+};
+
+__device__ __forceinline__ GridSync grid_sync_init(unsigned *count, unsigned *gen, int *status) {
+    GridSync g{count, gen, status, 0u};
+    if (threadIdx.x == 0) g.open_gen = ld_acquire_gpu(gen);
+    return g;
+}
+
+__device__ __forceinline__ bool grid_sync(GridSync &g, uint64_t deadline_ns) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int good = 1;
+        const unsigned arrived = atom_add_acq_rel_gpu(g.count, 1u);
+        if (arrived == gridDim.x - 1) {
+            *g.count = 0u;
+            red_add_release_gpu(g.gen, 1u);
+        } else {
+            uint32_t spins = 0;
+            while (ld_acquire_gpu(g.gen) == g.open_gen) {
+                if ((++spins & 63u) == 0u) {
+                    if (ld_relaxed_gpu(g.status) != kStatusOk || global_timer_ns() > deadline_ns) {
+                        atomicCAS(g.status, kStatusOk, kStatusTimeout);
+                        good = 0;
+                        break;
+                    }
+                }
+                __nanosleep(20);
+            }
+        }
+        g.open_gen += 1u;
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
 }  // namespace ktg

@@ -52,7 +52,7 @@ struct ktg_ctx {
     int ptr_mode = KTG_PTR_HOST;
     std::string err;
     int64_t launches = 0;
-    int pcg_lanes = 0;  // 0: library default; 1 or 4 lanes per row in the PCG SpMV
+    int pcg_lanes = 0;  // 0: library default; 32 warp tiles, 1 or 4 lanes per row in the PCG SpMV
     int pcg_form = -1;  // -1: library default; 0 textbook PCG, 1 Chronopoulos-Gear,
                         // 2 textbook PCG in the reference's summation order
     double *exact_prod = nullptr;   // form 2: products of the dots [3 * 2n]

@@ -13,9 +13,11 @@
 // When a block's rows fit, its slices of x, r, z, p, diag and Ap live in
 // shared memory for the whole solve, so phases B and C never leave the SM
 // and only p is published to global memory for the other blocks' gathers.
-// SpMV runs either one thread per row with four independent gathers in
-// flight (the row sum then adds terms in the reference's order) or four lanes
-// per row; the launcher picks by problem size.
+// SpMV runs in one of three shapes (option "pcg_lanes"): warp tiles (the
+// default: a warp streams the nonzeros of 32 consecutive rows with coalesced
+// loads and each lane adds its row's products in storage order), one thread
+// per row (same row sums, four gathers in flight), or four lanes per row.
+// The first two give bit-identical solves.
 // Scalars (alpha, beta, residuals, live flags) are recomputed identically by
 // every block from the same partials in a fixed order, so all blocks take the
 // same branch and the result is identical from run to run.
@@ -38,6 +40,7 @@ constexpr int kPcgThreads = 1024;
 // Shared-memory budget for the per-block vector slices (6 doubles per row).
 constexpr int kPcgSmemBytes = 216 * 1024;
 constexpr int kVecsPerRow = 6;
+constexpr int kCgVecsPerRow = 7;  // the two-barrier form also keeps s
 
 struct PcgAxis {
     const int32_t *rp;
@@ -125,7 +128,7 @@ __device__ __forceinline__ double *prod_ptr(const PcgArgs &A, int vec) {
 template <int K>
 __device__ bool ref_order_dots(const PcgArgs &A, const int (&vec)[K], const int (&axis)[K],
                                const bool (&want)[K], double (&out)[K], double *sh, double *stage,
-                               uint64_t deadline_ns) {
+                               GridSync &gs, uint64_t deadline_ns) {
     const int32_t n = A.ax[0].n;
     const int32_t nc = A.nchunk;
     const int64_t tasks = static_cast<int64_t>(K) * nc;
@@ -160,7 +163,7 @@ __device__ bool ref_order_dots(const PcgArgs &A, const int (&vec)[K], const int 
         }
         if (threadIdx.x == 0) __stcg(A.cpart + static_cast<size_t>(k) * nc + c, sum);
     }
-    if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline_ns)) return false;
+    if (!grid_sync(gs, deadline_ns)) return false;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         if (!want[k]) {
@@ -231,6 +234,82 @@ __device__ __forceinline__ double row_offdiag_vec4(const PcgAxis &S, int32_t i, 
     return s;
 }
 
+// Warp tiles: each warp takes 32 consecutive rows of the block and streams
+// their (contiguous) nonzeros in chunks of kTileChunk, every lane loading
+// consecutive entries (coalesced column and value loads, kTileQ independent
+// gathers in flight per lane). The products go to the warp's slice of shared
+// memory and each lane adds its own row's products in storage order onto
+// diag * own, carrying the running sum across chunks, so every row sum is the
+// same sequence of roundings as a row-per-thread loop (and as the
+// reference's SparseSystem::multiply, simpl_lss.h:49-57).
+constexpr int kTileQ = 4;
+constexpr int kTileChunk = 32 * kTileQ;
+constexpr int kTileWarps = kPcgThreads / 32;
+
+template <bool Smem, class Own, class InOf, class Emit>
+__device__ __forceinline__ void spmv_warp_tiles(const PcgAxis *sax, int32_t r0, int32_t n0,
+                                                int32_t R, const double *sd, const bool *live,
+                                                double *tilebuf, Own own, InOf in_of, Emit emit) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    double *buf = tilebuf + warp * kTileChunk;
+    for (int32_t t0 = warp * 32; t0 < R; t0 += nw * 32) {
+        const int32_t l = t0 + lane;
+        const int32_t c = r0 + l;
+        const int axis = c >= n0 ? 1 : 0;
+        const int32_t i = c - (axis ? n0 : 0);
+        const bool mine = l < R && (!live || live[axis]);
+        // a tile that straddles the x|y boundary takes one pass per axis
+#pragma unroll 1
+        for (int pass = 0; pass < 2; ++pass) {
+            const bool part = mine && axis == pass;
+            const unsigned m = __ballot_sync(0xffffffffu, part);
+            if (!m) continue;
+            const PcgAxis &S = sax[pass];
+            int32_t rs = 0, re = 0;
+            double v = 0.0, sum = 0.0;
+            if (part) {
+                rs = __ldg(S.rp + i);
+                re = __ldg(S.rp + i + 1);
+                const double d = Smem ? sd[l] : __ldg(S.diag + i);
+                v = own(l, pass, i);
+                sum = d * v;
+            }
+            // the participating rows are consecutive: their entries are
+            // [rs of the first, re of the last)
+            const int32_t k_begin = __shfl_sync(0xffffffffu, rs, __ffs(m) - 1);
+            const int32_t k_end = __shfl_sync(0xffffffffu, re, 31 - __clz(m));
+            const double *in = in_of(pass);
+#pragma unroll 1
+            for (int32_t k0 = k_begin; k0 < k_end; k0 += kTileChunk) {
+                int32_t cl[kTileQ];
+#pragma unroll
+                for (int q = 0; q < kTileQ; ++q) {
+                    const int32_t k = k0 + lane + 32 * q;
+                    cl[q] = k < k_end ? __ldg(S.col + k) : -1;
+                }
+                double pr[kTileQ];
+#pragma unroll
+                for (int q = 0; q < kTileQ; ++q) {
+                    const int32_t k = k0 + lane + 32 * q;
+                    pr[q] = cl[q] >= 0 ? __ldg(S.val + k) * __ldcg(in + cl[q]) : 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < kTileQ; ++q) buf[lane + 32 * q] = pr[q];
+                __syncwarp();
+                if (part) {
+                    const int32_t lo = rs > k0 ? rs : k0;
+                    const int32_t hi = re < k0 + kTileChunk ? re : k0 + kTileChunk;
+                    for (int32_t k = lo; k < hi; ++k) sum += buf[k - k0];
+                }
+                __syncwarp();
+            }
+            if (part) emit(l, pass, i, v, sum);
+        }
+    }
+}
+
 template <bool Smem, int Lanes, bool Exact = false>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     extern __shared__ double dyn[];
@@ -246,12 +325,14 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     const int32_t cap = A.rows_per_block;
     double *sx = dyn, *sr = dyn + cap, *sz = dyn + 2 * cap;
     double *sp = dyn + 3 * cap, *sd = dyn + 4 * cap, *sap = dyn + 5 * cap;
+    double *tilebuf = dyn + (Smem ? kVecsPerRow * cap : 0);  // after the vector slices
     __syncthreads();
     const int32_t n0 = sax[0].n;
     auto deadline = [&]() {
         const uint64_t d = global_timer_ns() + A.barrier_timeout_ns;
         return d < total_deadline ? d : total_deadline;
     };
+    GridSync gs = grid_sync_init(A.bar_count, A.bar_gen, A.status);
     // Row l of this block: axis and row index inside that axis.
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
         const int32_t c = r0 + l;
@@ -276,7 +357,9 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     // `own` reads the row's own input element, `in` selects the gathered
     // vector per axis.
     auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
-        if (Lanes == 1) {
+        if (Lanes == 32) {
+            spmv_warp_tiles<Smem>(sax, r0, n0, R, sd, live, tilebuf, own, in_of, emit);
+        } else if (Lanes == 1) {
             for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
                 int axis;
                 int32_t i;
@@ -351,7 +434,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             store_partials<3>(A, v1, sl, a1, scratch);
         }
     }
-    if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+    if (!grid_sync(gs, deadline())) return;
 
     double b_norm[2], rho[2], resid[2];
     bool active[2];
@@ -361,7 +444,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
         const int vec[6] = {0, 1, 2, 0, 1, 2};
         const int ax[6] = {0, 0, 0, 1, 1, 1};
         const bool want[6] = {true, true, true, true, true, true};
-        if (!ref_order_dots<6>(A, vec, ax, want, s, scratch, exstage, deadline())) return;
+        if (!ref_order_dots<6>(A, vec, ax, want, s, scratch, exstage, gs, deadline())) return;
 #pragma unroll
         for (int a = 0; a < 2; ++a) {
             b_norm[a] = sqrt(s[3 * a]);
@@ -417,7 +500,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             const int ax[2] = {0, 1};
             store_partials<2>(A, pap_acc, sl, ax, scratch);
         }
-        if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+        if (!grid_sync(gs, deadline())) return;
 
         double alpha[2] = {0.0, 0.0};
         bool ok[2];
@@ -427,7 +510,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                 const int vec[2] = {0, 0};
                 const int ax[2] = {0, 1};
                 const bool want[2] = {live[0], live[1]};
-                if (!ref_order_dots<2>(A, vec, ax, want, pap, scratch, exstage, deadline())) return;
+                if (!ref_order_dots<2>(A, vec, ax, want, pap, scratch, exstage, gs, deadline())) return;
             } else {
                 const int sl[2] = {kPAP, kPAP};
                 const int ax[2] = {0, 1};
@@ -471,7 +554,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             const int ax[4] = {0, 0, 1, 1};
             store_partials<4>(A, acc, sl, ax, scratch);
         }
-        if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+        if (!grid_sync(gs, deadline())) return;
 
         double beta[2] = {0.0, 0.0};
         bool ok2[2] = {false, false};
@@ -482,7 +565,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                 const int vec[4] = {1, 2, 1, 2};
                 const int ax[4] = {0, 0, 1, 1};
                 const bool want[4] = {ok[0], ok[0], ok[1], ok[1]};
-                if (!ref_order_dots<4>(A, vec, ax, want, s, scratch, exstage, deadline())) return;
+                if (!ref_order_dots<4>(A, vec, ax, want, s, scratch, exstage, gs, deadline())) return;
             } else {
                 const int sl[4] = {kRR, kRZ, kRR, kRZ};
                 const int ax[4] = {0, 0, 1, 1};
@@ -520,7 +603,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             if (A.hist_y) A.hist_y[it] = resid[1];
         }
         ++it;
-        if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+        if (!grid_sync(gs, deadline())) return;
     }
 #undef KTG_V
 
@@ -572,12 +655,14 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
     const int32_t cap = A.rows_per_block;
     double *sx = dyn, *sr = dyn + cap, *sz = dyn + 2 * cap, *sp = dyn + 3 * cap;
     double *ss = dyn + 4 * cap, *sw = dyn + 5 * cap, *sd = dyn + 6 * cap;
+    double *tilebuf = dyn + (Smem ? kCgVecsPerRow * cap : 0);  // after the vector slices
     __syncthreads();
     const int32_t n0 = sax[0].n;
     auto deadline = [&]() {
         const uint64_t d = global_timer_ns() + A.barrier_timeout_ns;
         return d < total_deadline ? d : total_deadline;
     };
+    GridSync gs = grid_sync_init(A.bar_count, A.bar_gen, A.status);
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
         const int32_t c = r0 + l;
         axis = c >= n0 ? 1 : 0;
@@ -599,7 +684,9 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
     }
 
     auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
-        if (Lanes == 1) {
+        if (Lanes == 32) {
+            spmv_warp_tiles<Smem>(sax, r0, n0, R, sd, live, tilebuf, own, in_of, emit);
+        } else if (Lanes == 1) {
             for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
                 int axis;
                 int32_t i;
@@ -663,7 +750,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
         store_partials<3>(A, v0, sl, a0, scratch);
         store_partials<3>(A, v1, sl, a1, scratch);
     }
-    if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+    if (!grid_sync(gs, deadline())) return;
 
     double b_norm[2], rho[2], rho_prev[2] = {0.0, 0.0}, alpha_prev[2] = {0.0, 0.0}, resid[2];
     bool active[2], first[2] = {true, true}, stepped[2] = {false, false};
@@ -738,7 +825,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
             const int ax[2] = {0, 1};
             store_partials<2>(A, wz, sl, ax, scratch);
         }
-        if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+        if (!grid_sync(gs, deadline())) return;
 
         double alpha[2] = {0.0, 0.0}, beta[2] = {0.0, 0.0};
         bool ok[2];
@@ -805,7 +892,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
             first[a] = false;
         }
         ++it;
-        if (!grid_barrier(A.bar_count, A.bar_gen, A.status, deadline())) return;
+        if (!grid_sync(gs, deadline())) return;
     }
 #undef KTG_V
 
@@ -846,19 +933,27 @@ struct Variant {
 // form 2: textbook PCG with the reference's summation order everywhere (one
 // thread per row; bit-identical to the reference's solve).
 Variant pick_variant(int form, bool smem, int lanes) {
-    if (form == 2) return {smem ? k_pcg<true, 1, true> : k_pcg<false, 1, true>, kVecsPerRow};
-    if (form == 1) {
-        if (smem) return {lanes == 4 ? k_pcg_cg<true, 4> : k_pcg_cg<true, 1>, 7};
-        return {lanes == 4 ? k_pcg_cg<false, 4> : k_pcg_cg<false, 1>, 7};
+    if (form == 2) {
+        if (lanes == 32)
+            return {smem ? k_pcg<true, 32, true> : k_pcg<false, 32, true>, kVecsPerRow};
+        return {smem ? k_pcg<true, 1, true> : k_pcg<false, 1, true>, kVecsPerRow};
     }
+    if (form == 1) {
+        if (lanes == 32) return {smem ? k_pcg_cg<true, 32> : k_pcg_cg<false, 32>, kCgVecsPerRow};
+        if (smem) return {lanes == 4 ? k_pcg_cg<true, 4> : k_pcg_cg<true, 1>, kCgVecsPerRow};
+        return {lanes == 4 ? k_pcg_cg<false, 4> : k_pcg_cg<false, 1>, kCgVecsPerRow};
+    }
+    if (lanes == 32) return {smem ? k_pcg<true, 32> : k_pcg<false, 32>, kVecsPerRow};
     if (smem) return {lanes == 4 ? k_pcg<true, 4> : k_pcg<true, 1>, kVecsPerRow};
     return {lanes == 4 ? k_pcg<false, 4> : k_pcg<false, 1>, kVecsPerRow};
 }
 
+int lanes_index(int lanes) { return lanes == 4 ? 1 : lanes == 32 ? 2 : 0; }
+
 }  // namespace
 
-int pcg_lanes_default = 1;
-int pcg_form_default = 1;
+int pcg_lanes_default = 32;
+int pcg_form_default = 0;
 
 int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
                  ktg_solve_info *info_dev, double *hist_x, double *hist_y, int64_t hist_cap) {
@@ -878,16 +973,33 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     if (A.rows_per_block == 0) A.rows_per_block = 1;
     const int lanes = c->pcg_lanes > 0 ? c->pcg_lanes : pcg_lanes_default;
     const int form = c->pcg_form >= 0 ? c->pcg_form : pcg_form_default;
+    // Dynamic shared memory for the vector slices: what the block may opt in
+    // to, less the kernel's static arrays, capped at kPcgSmemBytes.
+    static size_t budget[3][3] = {};
+    size_t &bud = budget[form][lanes_index(lanes)];
+    if (bud == 0) {
+        int optin = 0;
+        KTG_CUDA(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                           c->device));
+        cudaFuncAttributes fa;
+        KTG_CUDA(c, cudaFuncGetAttributes(&fa, pick_variant(form, true, lanes).fn));
+        const size_t room = optin > static_cast<int>(fa.sharedSizeBytes)
+                                ? static_cast<size_t>(optin) - fa.sharedSizeBytes
+                                : 0;
+        bud = std::min(room, static_cast<size_t>(kPcgSmemBytes));
+        if (bud == 0) bud = 1;
+    }
     const int vecs = pick_variant(form, true, lanes).vecs_per_row;
-    const size_t smem = sizeof(double) * vecs * static_cast<size_t>(A.rows_per_block);
-    const bool use_smem = smem <= static_cast<size_t>(kPcgSmemBytes);
+    const size_t tile = lanes == 32 ? sizeof(double) * kTileWarps * kTileChunk : 0;
+    const size_t smem = sizeof(double) * vecs * static_cast<size_t>(A.rows_per_block) + tile;
+    const bool use_smem = smem <= bud;
     const Variant v = pick_variant(form, use_smem, lanes);
-    const size_t dyn = use_smem ? smem : 0;
-    static bool attr_set[3][2][2] = {};
-    bool &done = attr_set[form][use_smem][lanes == 4];
+    const size_t dyn = use_smem ? smem : tile;
+    static bool attr_set[3][2][3] = {};
+    bool &done = attr_set[form][use_smem][lanes_index(lanes)];
     if (!done) {
         KTG_CUDA(c, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kPcgSmemBytes));
+                                         static_cast<int>(bud)));
         done = true;
     }
     int per_sm = 0;
