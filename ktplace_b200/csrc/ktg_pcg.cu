@@ -30,6 +30,7 @@
 // summation orders differ.
 #include "ktg_common.cuh"
 #include "ktg_context.h"
+#include "ktg_spmv.cuh"
 
 #include <algorithm>
 
@@ -234,85 +235,11 @@ __device__ __forceinline__ double row_offdiag_vec4(const PcgAxis &S, int32_t i, 
     return s;
 }
 
-// Warp tiles: each warp takes 32 consecutive rows of the block and streams
-// their (contiguous) nonzeros in chunks of kTileChunk, every lane loading
-// consecutive entries (coalesced column and value loads, kTileQ independent
-// gathers in flight per lane). The products go to the warp's slice of shared
-// memory and each lane adds its own row's products in storage order onto
-// diag * own, carrying the running sum across chunks, so every row sum is the
-// same sequence of roundings as a row-per-thread loop (and as the
-// reference's SparseSystem::multiply, simpl_lss.h:49-57).
-constexpr int kTileQ = 4;
-constexpr int kTileChunk = 32 * kTileQ;
 constexpr int kTileWarps = kPcgThreads / 32;
-
-template <bool Smem, class Own, class InOf, class Emit>
-__device__ __forceinline__ void spmv_warp_tiles(const PcgAxis *sax, int32_t r0, int32_t n0,
-                                                int32_t R, const double *sd, const bool *live,
-                                                double *tilebuf, Own own, InOf in_of, Emit emit) {
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int nw = blockDim.x >> 5;
-    double *buf = tilebuf + warp * kTileChunk;
-    for (int32_t t0 = warp * 32; t0 < R; t0 += nw * 32) {
-        const int32_t l = t0 + lane;
-        const int32_t c = r0 + l;
-        const int axis = c >= n0 ? 1 : 0;
-        const int32_t i = c - (axis ? n0 : 0);
-        const bool mine = l < R && (!live || live[axis]);
-        // a tile that straddles the x|y boundary takes one pass per axis
-#pragma unroll 1
-        for (int pass = 0; pass < 2; ++pass) {
-            const bool part = mine && axis == pass;
-            const unsigned m = __ballot_sync(0xffffffffu, part);
-            if (!m) continue;
-            const PcgAxis &S = sax[pass];
-            int32_t rs = 0, re = 0;
-            double v = 0.0, sum = 0.0;
-            if (part) {
-                rs = __ldg(S.rp + i);
-                re = __ldg(S.rp + i + 1);
-                const double d = Smem ? sd[l] : __ldg(S.diag + i);
-                v = own(l, pass, i);
-                sum = d * v;
-            }
-            // the participating rows are consecutive: their entries are
-            // [rs of the first, re of the last)
-            const int32_t k_begin = __shfl_sync(0xffffffffu, rs, __ffs(m) - 1);
-            const int32_t k_end = __shfl_sync(0xffffffffu, re, 31 - __clz(m));
-            const double *in = in_of(pass);
-#pragma unroll 1
-            for (int32_t k0 = k_begin; k0 < k_end; k0 += kTileChunk) {
-                int32_t cl[kTileQ];
-#pragma unroll
-                for (int q = 0; q < kTileQ; ++q) {
-                    const int32_t k = k0 + lane + 32 * q;
-                    cl[q] = k < k_end ? __ldg(S.col + k) : -1;
-                }
-                double pr[kTileQ];
-#pragma unroll
-                for (int q = 0; q < kTileQ; ++q) {
-                    const int32_t k = k0 + lane + 32 * q;
-                    pr[q] = cl[q] >= 0 ? __ldg(S.val + k) * __ldcg(in + cl[q]) : 0.0;
-                }
-#pragma unroll
-                for (int q = 0; q < kTileQ; ++q) buf[lane + 32 * q] = pr[q];
-                __syncwarp();
-                if (part) {
-                    const int32_t lo = rs > k0 ? rs : k0;
-                    const int32_t hi = re < k0 + kTileChunk ? re : k0 + kTileChunk;
-                    for (int32_t k = lo; k < hi; ++k) sum += buf[k - k0];
-                }
-                __syncwarp();
-            }
-            if (part) emit(l, pass, i, v, sum);
-        }
-    }
-}
 
 template <bool Smem, int Lanes, bool Exact = false>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
-    extern __shared__ double dyn[];
+    extern __shared__ __align__(16) double dyn[];
     __shared__ double scratch[33 * 4];
     __shared__ double exstage[Exact ? kStageSum : 1];  // reference-order sums
     __shared__ PcgAxis sax[2];
@@ -325,7 +252,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     const int32_t cap = A.rows_per_block;
     double *sx = dyn, *sr = dyn + cap, *sz = dyn + 2 * cap;
     double *sp = dyn + 3 * cap, *sd = dyn + 4 * cap, *sap = dyn + 5 * cap;
-    double *tilebuf = dyn + (Smem ? kVecsPerRow * cap : 0);  // after the vector slices
+    double *tilebuf = dyn + (Smem ? (kVecsPerRow * cap + 1) / 2 * 2 : 0);  // 16-byte aligned
     __syncthreads();
     const int32_t n0 = sax[0].n;
     auto deadline = [&]() {
@@ -358,7 +285,22 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     // vector per axis.
     auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
         if (Lanes == 32) {
-            spmv_warp_tiles<Smem>(sax, r0, n0, R, sd, live, tilebuf, own, in_of, emit);
+            double vcur = 0.0;
+            warp_tile_spmv<double>(
+                r0, n0, R, live, tilebuf,
+                [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
+                    const double *&in) {
+                    rp = sax[pass].rp;
+                    col = sax[pass].col;
+                    val = sax[pass].val;
+                    in = in_of(pass);
+                },
+                [&](int32_t l, int pass, int32_t i) {
+                    const double d = Smem ? sd[l] : __ldg(sax[pass].diag + i);
+                    vcur = own(l, pass, i);
+                    return d * vcur;
+                },
+                [&](int32_t l, int pass, int32_t i, double s) { emit(l, pass, i, vcur, s); });
         } else if (Lanes == 1) {
             for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
                 int axis;
@@ -643,7 +585,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
 // match; p and x round exactly as in the reference, r through s.
 template <bool Smem, int Lanes>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
-    extern __shared__ double dyn[];
+    extern __shared__ __align__(16) double dyn[];
     __shared__ double scratch[33 * 4];
     __shared__ PcgAxis sax[2];
     if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
@@ -655,7 +597,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
     const int32_t cap = A.rows_per_block;
     double *sx = dyn, *sr = dyn + cap, *sz = dyn + 2 * cap, *sp = dyn + 3 * cap;
     double *ss = dyn + 4 * cap, *sw = dyn + 5 * cap, *sd = dyn + 6 * cap;
-    double *tilebuf = dyn + (Smem ? kCgVecsPerRow * cap : 0);  // after the vector slices
+    double *tilebuf = dyn + (Smem ? (kCgVecsPerRow * cap + 1) / 2 * 2 : 0);  // 16-byte aligned
     __syncthreads();
     const int32_t n0 = sax[0].n;
     auto deadline = [&]() {
@@ -685,7 +627,22 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
 
     auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
         if (Lanes == 32) {
-            spmv_warp_tiles<Smem>(sax, r0, n0, R, sd, live, tilebuf, own, in_of, emit);
+            double vcur = 0.0;
+            warp_tile_spmv<double>(
+                r0, n0, R, live, tilebuf,
+                [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
+                    const double *&in) {
+                    rp = sax[pass].rp;
+                    col = sax[pass].col;
+                    val = sax[pass].val;
+                    in = in_of(pass);
+                },
+                [&](int32_t l, int pass, int32_t i) {
+                    const double d = Smem ? sd[l] : __ldg(sax[pass].diag + i);
+                    vcur = own(l, pass, i);
+                    return d * vcur;
+                },
+                [&](int32_t l, int pass, int32_t i, double s) { emit(l, pass, i, vcur, s); });
         } else if (Lanes == 1) {
             for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
                 int axis;
@@ -991,7 +948,8 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     }
     const int vecs = pick_variant(form, true, lanes).vecs_per_row;
     const size_t tile = lanes == 32 ? sizeof(double) * kTileWarps * kTileChunk : 0;
-    const size_t smem = sizeof(double) * vecs * static_cast<size_t>(A.rows_per_block) + tile;
+    const size_t smem =
+        sizeof(double) * ((vecs * static_cast<size_t>(A.rows_per_block) + 1) / 2 * 2) + tile;
     const bool use_smem = smem <= bud;
     const Variant v = pick_variant(form, use_smem, lanes);
     const size_t dyn = use_smem ? smem : tile;

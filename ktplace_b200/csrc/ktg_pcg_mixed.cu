@@ -15,6 +15,7 @@
 #include "ktg_agg.h"
 #include "ktg_common.cuh"
 #include "ktg_context.h"
+#include "ktg_spmv.cuh"
 
 #include <algorithm>
 
@@ -122,7 +123,8 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
         axis = c >= n0 ? 1 : 0;
         i = c - (axis ? n0 : 0);
     };
-    auto sync = [&]() { return grid_barrier(A.bar_count, A.bar_gen, A.status, deadline()); };
+    GridSync gs = grid_sync_init(A.bar_count, A.bar_gen, A.status);
+    auto sync = [&]() { return grid_sync(gs, deadline()); };
 
     double b_norm[2] = {0.0, 0.0}, true_resid[2] = {0.0, 0.0}, prev_resid[2] = {0.0, 0.0};
     bool active[2] = {false, false}, stalled[2] = {false, false};
@@ -411,7 +413,7 @@ enum MixPre { kPreJacobi = 0, kPreLearned = 1, kPreAgg = 2 };
 //     after a __syncthreads, with no extra grid barrier.
 template <int PRE>
 __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
-    extern __shared__ double dyn[];
+    extern __shared__ __align__(16) double dyn[];
     __shared__ double scratch[33 * 4];
     __shared__ MixAxis sax[2];
     if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
@@ -432,6 +434,9 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     const int32_t R = max(r1 - r0, 0);
     const int32_t cap = A.rows_per_block;
     double *base = A.gslice ? A.gslice + static_cast<size_t>(blockIdx.x) * cap * 5 : dyn;
+    // warp-tile buffer after the shared slices (16-byte aligned)
+    double *tile64 = A.gslice ? dyn : dyn + (5 * static_cast<size_t>(cap) + 1) / 2 * 2;
+    float *tile32 = reinterpret_cast<float *>(tile64);
     double *sx = base, *sd = base + cap;
     float *sr = reinterpret_cast<float *>(base + 2 * cap);
     float *su = sr + cap, *sw = su + cap, *sp = sw + cap, *ss = sp + cap, *sdd = ss + cap;
@@ -441,7 +446,8 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         axis = c >= n0 ? 1 : 0;
         i = c - (axis ? n0 : 0);
     };
-    auto sync = [&]() { return grid_barrier(A.bar_count, A.bar_gen, A.status, deadline()); };
+    GridSync gs = grid_sync_init(A.bar_count, A.bar_gen, A.status);
+    auto sync = [&]() { return grid_sync(gs, deadline()); };
     constexpr bool pre = PRE == kPreLearned;
     for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
         int axis;
@@ -500,40 +506,33 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         // ---- FP64 residual r = b - A x; r32, and u (Jacobi) or D^-1/2 r -----
         {
             double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rr x, bb x, rr y, bb y
-            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
-                int axis;
-                int32_t i;
-                locate(l, axis, i);
-                const MixAxis &S = sax[axis];
-                double s = sd[l] * sx[l];
-                int32_t e = __ldg(S.rp + i);
-                const int32_t e1 = __ldg(S.rp + i + 1);
-                for (; e + 4 <= e1; e += 4) {
-                    const int32_t c0 = __ldg(S.col + e), c1 = __ldg(S.col + e + 1);
-                    const int32_t c2 = __ldg(S.col + e + 2), c3 = __ldg(S.col + e + 3);
-                    const double g0 = __ldcg(S.x + c0), g1 = __ldcg(S.x + c1);
-                    const double g2 = __ldcg(S.x + c2), g3 = __ldcg(S.x + c3);
-                    s += __ldg(S.val + e) * g0;
-                    s += __ldg(S.val + e + 1) * g1;
-                    s += __ldg(S.val + e + 2) * g2;
-                    s += __ldg(S.val + e + 3) * g3;
-                }
-                for (; e < e1; ++e) s += __ldg(S.val + e) * __ldcg(S.x + __ldg(S.col + e));
-                const double b = __ldg(S.rhs + i);
-                const double r = b - s;
-                const float rf = static_cast<float>(r);
-                sr[l] = rf;
-                sdd[l] = 0.0f;
-                if (pre) {
-                    __stcg(S.rs + i, rf * rsqrtf(static_cast<float>(sd[l])));
-                } else if (PRE == kPreJacobi) {
-                    const float u = rf / static_cast<float>(sd[l]);
-                    su[l] = u;
-                    __stcg(S.z + i, u);
-                }
-                acc[axis * 2 + 0] += r * r;
-                acc[axis * 2 + 1] += b * b;
-            }
+            warp_tile_spmv<double>(
+                r0, n0, R, nullptr, tile64,
+                [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
+                    const double *&in) {
+                    rp = sax[pass].rp;
+                    col = sax[pass].col;
+                    val = sax[pass].val;
+                    in = sax[pass].x;
+                },
+                [&](int32_t l, int, int32_t) { return sd[l] * sx[l]; },
+                [&](int32_t l, int axis, int32_t i, double s) {
+                    const MixAxis &S = sax[axis];
+                    const double b = __ldg(S.rhs + i);
+                    const double r = b - s;
+                    const float rf = static_cast<float>(r);
+                    sr[l] = rf;
+                    sdd[l] = 0.0f;
+                    if (pre) {
+                        __stcg(S.rs + i, rf * rsqrtf(static_cast<float>(sd[l])));
+                    } else if (PRE == kPreJacobi) {
+                        const float u = rf / static_cast<float>(sd[l]);
+                        su[l] = u;
+                        __stcg(S.z + i, u);
+                    }
+                    acc[axis * 2 + 0] += r * r;
+                    acc[axis * 2 + 1] += b * b;
+                });
             if (PRE == kPreAgg) {
                 const bool all[2] = {true, true};
                 apply_blocks(all);
@@ -583,33 +582,24 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         const double target[2] = {A.inner_tol * r_norm[0], A.inner_tol * r_norm[1]};
         for (;;) {
             double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // gamma, delta, rr per axis
-            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
-                int axis;
-                int32_t i;
-                locate(l, axis, i);
-                if (!in_live[axis]) continue;
-                const MixAxis &S = sax[axis];
-                const float ui = su[l];
-                float w = static_cast<float>(sd[l]) * ui;
-                int32_t e = __ldg(S.rp + i);
-                const int32_t e1 = __ldg(S.rp + i + 1);
-                for (; e + 4 <= e1; e += 4) {
-                    const int32_t c0 = __ldg(S.col + e), c1 = __ldg(S.col + e + 1);
-                    const int32_t c2 = __ldg(S.col + e + 2), c3 = __ldg(S.col + e + 3);
-                    const float g0 = __ldcg(S.z + c0), g1 = __ldcg(S.z + c1);
-                    const float g2 = __ldcg(S.z + c2), g3 = __ldcg(S.z + c3);
-                    w += __ldg(S.val32 + e) * g0;
-                    w += __ldg(S.val32 + e + 1) * g1;
-                    w += __ldg(S.val32 + e + 2) * g2;
-                    w += __ldg(S.val32 + e + 3) * g3;
-                }
-                for (; e < e1; ++e) w += __ldg(S.val32 + e) * __ldcg(S.z + __ldg(S.col + e));
-                sw[l] = w;
-                const float r = sr[l];
-                acc[axis * 3 + 0] += static_cast<double>(r) * ui;
-                acc[axis * 3 + 1] += static_cast<double>(w) * ui;
-                acc[axis * 3 + 2] += static_cast<double>(r) * r;
-            }
+            warp_tile_spmv<float>(
+                r0, n0, R, in_live, tile32,
+                [&](int pass, const int32_t *&rp, const int32_t *&col, const float *&val,
+                    const float *&in) {
+                    rp = sax[pass].rp;
+                    col = sax[pass].col;
+                    val = sax[pass].val32;
+                    in = sax[pass].z;
+                },
+                [&](int32_t l, int, int32_t) { return static_cast<float>(sd[l]) * su[l]; },
+                [&](int32_t l, int axis, int32_t, float w) {
+                    const float ui = su[l];
+                    sw[l] = w;
+                    const float r = sr[l];
+                    acc[axis * 3 + 0] += static_cast<double>(r) * ui;
+                    acc[axis * 3 + 1] += static_cast<double>(w) * ui;
+                    acc[axis * 3 + 2] += static_cast<double>(r) * r;
+                });
             {
                 double v0[3] = {acc[0], acc[1], acc[2]};
                 double v1[3] = {acc[3], acc[4], acc[5]};
@@ -787,9 +777,10 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     // Chronopoulos-Gear kernel (always for the aggregation preconditioner),
     // with shared-memory slices of 40 bytes per row when they fit, else
     // global ones; the textbook kernel on global vectors when asked for.
-    const size_t slice = 40 * static_cast<size_t>(A.rows_per_block);
+    const size_t slice = 40 * static_cast<size_t>(A.rows_per_block) + 8;  // + alignment
+    const size_t tile = sizeof(double) * kTileChunk * (kMixThreads / 32);
     const bool cg_form = agg || c->mixed_form != 0;
-    const bool in_smem = slice <= kMixSmemBytes;
+    const bool in_smem = slice + tile <= kMixSmemBytes;
     if (cg_form && !in_smem) {
         A.gslice = agg_global_slices(c, static_cast<int64_t>(grid) * A.rows_per_block * 5);
         if (!A.gslice) return KTG_ERR_NOMEM;
@@ -798,7 +789,7 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
                           : agg    ? k_pcg_mixed_cg<kPreAgg>
                           : learned ? k_pcg_mixed_cg<kPreLearned>
                                     : k_pcg_mixed_cg<kPreJacobi>;
-    const size_t dyn = cg_form && in_smem ? slice : 0;
+    const size_t dyn = !cg_form ? 0 : in_smem ? slice + tile : tile;
     static bool attr_set = false;
     if (!attr_set) {
         for (void (*f)(MixArgs) : {k_pcg_mixed_cg<kPreJacobi>, k_pcg_mixed_cg<kPreLearned>,

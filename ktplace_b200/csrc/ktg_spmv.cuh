@@ -1,0 +1,111 @@
+// Warp-tile sparse row sums for the persistent solvers (sm_100a).
+//
+// Each warp takes 32 consecutive rows of its block and streams their
+// (contiguous) nonzeros in chunks of kTileChunk, every lane loading
+// consecutive entries: coalesced column and value loads and kTileQ
+// independent gathers in flight per lane. The products go to the warp's
+// slice of shared memory and each lane adds its own row's products in
+// storage order onto the row's first term, carrying the running sum across
+// chunks, so every row sum is the same sequence of roundings as a
+// row-per-thread loop (and, in FP64, as the reference's
+// SparseSystem::multiply, simpl_lss.h:49-57). Where a lane's run of
+// products is 16-byte aligned it reads two per shared load.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ktg {
+
+constexpr int kTileQ = 4;
+constexpr int kTileChunk = 32 * kTileQ;
+
+template <typename T>
+struct TilePair;
+template <>
+struct TilePair<double> {
+    using type = double2;
+};
+template <>
+struct TilePair<float> {
+    using type = float2;
+};
+
+// Rows [r0, r0 + R) of a block's slice of the combined row space
+// [axis 0 rows | axis 1 rows] (axis 1 starts at row n0); rows of an axis
+// with live[axis] false are skipped (live may be null). All threads of the
+// block call it.
+//   csr(pass, rp, col, val, in): the axis's CSR arrays and gathered vector;
+//   start(l, pass, i) -> T: the row's first term (diag * own value);
+//   emit(l, pass, i, sum): the finished row sum.
+// tilebuf holds kTileChunk elements per warp, 16-byte aligned.
+template <typename T, class Csr, class Start, class Emit>
+__device__ __forceinline__ void warp_tile_spmv(int32_t r0, int32_t n0, int32_t R, const bool *live,
+                                               T *tilebuf, Csr csr, Start start, Emit emit) {
+    using P2 = typename TilePair<T>::type;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    T *buf = tilebuf + warp * kTileChunk;
+    for (int32_t t0 = warp * 32; t0 < R; t0 += nw * 32) {
+        const int32_t l = t0 + lane;
+        const int32_t c = r0 + l;
+        const int axis = c >= n0 ? 1 : 0;
+        const int32_t i = c - (axis ? n0 : 0);
+        const bool mine = l < R && (!live || live[axis]);
+        // a tile that straddles the axis boundary takes one pass per axis
+#pragma unroll 1
+        for (int pass = 0; pass < 2; ++pass) {
+            const bool part = mine && axis == pass;
+            const unsigned m = __ballot_sync(0xffffffffu, part);
+            if (!m) continue;
+            const int32_t *rp, *col;
+            const T *val, *in;
+            csr(pass, rp, col, val, in);
+            int32_t rs = 0, re = 0;
+            T sum = T(0);
+            if (part) {
+                rs = __ldg(rp + i);
+                re = __ldg(rp + i + 1);
+                sum = start(l, pass, i);
+            }
+            // the participating rows are consecutive: their entries are
+            // [rs of the first, re of the last)
+            const int32_t k_begin = __shfl_sync(0xffffffffu, rs, __ffs(m) - 1);
+            const int32_t k_end = __shfl_sync(0xffffffffu, re, 31 - __clz(m));
+#pragma unroll 1
+            for (int32_t k0 = k_begin; k0 < k_end; k0 += kTileChunk) {
+                int32_t cl[kTileQ];
+#pragma unroll
+                for (int q = 0; q < kTileQ; ++q) {
+                    const int32_t k = k0 + lane + 32 * q;
+                    cl[q] = k < k_end ? __ldg(col + k) : -1;
+                }
+                T pr[kTileQ];
+#pragma unroll
+                for (int q = 0; q < kTileQ; ++q) {
+                    const int32_t k = k0 + lane + 32 * q;
+                    pr[q] = cl[q] >= 0 ? __ldg(val + k) * __ldcg(in + cl[q]) : T(0);
+                }
+#pragma unroll
+                for (int q = 0; q < kTileQ; ++q) buf[lane + 32 * q] = pr[q];
+                __syncwarp();
+                if (part) {
+                    int32_t j = (rs > k0 ? rs : k0) - k0;
+                    const int32_t je = (re < k0 + kTileChunk ? re : k0 + kTileChunk) - k0;
+                    if ((j & 1) && j < je) sum += buf[j++];
+                    for (; j + 1 < je; j += 2) {
+                        const P2 t = *reinterpret_cast<const P2 *>(buf + j);
+                        sum += t.x;
+                        sum += t.y;
+                    }
+                    if (j < je) sum += buf[j];
+                }
+                __syncwarp();
+            }
+            if (part) emit(l, pass, i, sum);
+        }
+    }
+}
+
+}  // namespace ktg
