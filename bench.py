@@ -60,7 +60,7 @@ def parse():
                     help="only one B2B build and FP64 solve of a synthetic design with CELLS "
                          "movable cells (scaled from the 211k design), timed, with its "
                          "algorithmic bytes per second; the capture workload of "
-                         "profiles/k_pcg_cg_beyond_l2.md")
+                         "profiles/k_pcg_beyond_l2.md")
     ap.add_argument("--config4", action="store_true",
                     help="only the solve comparison (FP64, FP32 with Jacobi / learned / "
                          "aggregation) on the 2.2M-cell design; prints one JSON line")
@@ -219,7 +219,7 @@ def pcg_bytes(n: int, m: int, iters: int) -> float:
 
 # DRAM bytes (read + write) per launch of the dominant kernel on this
 # workload, from the ncu capture summarised in profiles/k_pcg_synth211k.md.
-NCU_TRAFFIC_BYTES = {"k_pcg_cg": 174.537728e6 + 108.409344e6}
+NCU_TRAFFIC_BYTES = {"k_pcg": 188.578560e6 + 46.643712e6}
 
 
 def measured_peak():
@@ -398,10 +398,11 @@ def run_ours(args):
             "breakdown": {"solve_ms": solve_med, "solve_ms_per_cg_iter": solve_med / inf.iters,
                           "other_ms": statistics.median(step_ms) - solve_med},
             "solve_variants": variants,
-            "roofline": {"kernel": "k_pcg_cg (persistent cooperative PCG, x+y)",
+            "roofline": {"kernel": "k_pcg<1, 32, 0, 1> (persistent cooperative PCG, x+y, "
+                                   "warp-tile SpMV, two grid barriers per iteration)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": NCU_TRAFFIC_BYTES["k_pcg_cg"], "algorithmic_bytes": byts,
+                         "traffic": NCU_TRAFFIC_BYTES["k_pcg"], "algorithmic_bytes": byts,
                          "note": "working set is L2-resident: traffic << algorithmic bytes"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,

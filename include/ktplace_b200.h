@@ -423,13 +423,16 @@ int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacl
  *                same row sums, so the same solve bit for bit), 4 = four
  *                lanes per row; 0 = default (32)
  *   "pcg_form"   0: textbook PCG (three grid barriers per iteration),
- *                1: Chronopoulos-Gear form (two), -1 = default (0),
+ *                1: Chronopoulos-Gear form (two),
+ *                3: textbook PCG with A p = A z + beta A p_prev by recurrence
+ *                (two barriers; the same iterates to rounding), -1 = default
+ *                (3),
  *                2: textbook PCG with every dot product summed in the
  *                reference's order (getDeterministicSum, simpl_parallel.h:
  *                35-51: 4,096-element chunks left to right, then the chunk
  *                sums in order): solutions, iteration counts and residual
- *                histories are bit-identical to solveBothAxes (about 2.6x
- *                the time of form 0)
+ *                histories are bit-identical to solveBothAxes (about 3x the
+ *                time of form 3)
  *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare),
  *                2: aggregation block-Jacobi, in ktg_solve_mixed
  *   "mixed_form" 1 (default): Chronopoulos-Gear mixed solve with per-block

@@ -299,8 +299,8 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         return KTG_OK;
     }
     if (k == "pcg_form") {
-        if (value < -1 || value > 2)
-            return set_error(c, KTG_ERR_ARG, "pcg_form must be -1, 0, 1 or 2");
+        if (value < -1 || value > 3)
+            return set_error(c, KTG_ERR_ARG, "pcg_form must be -1, 0, 1, 2 or 3");
         c->pcg_form = static_cast<int>(value);
         return KTG_OK;
     }

@@ -54,7 +54,8 @@ struct ktg_ctx {
     int64_t launches = 0;
     int pcg_lanes = 0;  // 0: library default; 32 warp tiles, 1 or 4 lanes per row in the PCG SpMV
     int pcg_form = -1;  // -1: library default; 0 textbook PCG, 1 Chronopoulos-Gear,
-                        // 2 textbook PCG in the reference's summation order
+                        // 2 textbook PCG in the reference's summation order,
+                        // 3 textbook PCG with A p by recurrence
     double *exact_prod = nullptr;   // form 2: products of the dots [3 * 2n]
     double *exact_cpart = nullptr;  // form 2: chunk sums [6 * chunks]
     int64_t exact_prod_cap = 0, exact_cpart_cap = 0;

@@ -5,11 +5,13 @@
 // SparseSystem::multiply (simpl_lss.h:49-57). The whole solve -- warm start,
 // every iteration, the stopping test -- runs inside one kernel, so there is no
 // host round trip per iteration. Each block owns a contiguous slice of the
-// combined row space [x rows | y rows] (one 1024-thread block per SM); three
-// grid barriers per iteration separate
+// combined row space [x rows | y rows] (one 1024-thread block per SM); in
+// the textbook form three grid barriers per iteration separate
 //   A: Ap = A p and p.Ap partials
 //   B: x += a p, r -= a Ap, z = r / diag, and r.r, r.z partials
 //   C: p = z + b p
+// and the default form (3) folds C into A, gathering z and updating p and
+// A p = A z + b A p there, for two barriers per iteration.
 // When a block's rows fit, its slices of x, r, z, p, diag and Ap live in
 // shared memory for the whole solve, so phases B and C never leave the SM
 // and only p is published to global memory for the other blocks' gathers.
@@ -237,7 +239,12 @@ __device__ __forceinline__ double row_offdiag_vec4(const PcgAxis &S, int32_t i, 
 
 constexpr int kTileWarps = kPcgThreads / 32;
 
-template <bool Smem, int Lanes, bool Exact = false>
+// Rec (form 3): A p by the recurrence A p = A z + beta A p_prev, so each
+// iteration's SpMV gathers z, published by the update phase before the
+// second barrier, and p and A p are updated in the SpMV phase; the third
+// barrier (and the phase that published p) goes away. Rounding differs from
+// the direct product; iterates agree to rounding.
+template <bool Smem, int Lanes, bool Exact = false, bool Rec = false>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     extern __shared__ __align__(16) double dyn[];
     __shared__ double scratch[33 * 4];
@@ -349,6 +356,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                      sr[l] = r;
                      sz[l] = z;
                      sp[l] = z;
+                     if (Rec) __stcg(S.z + i, z);
                  } else {
                      S.r[i] = r;
                      S.z[i] = z;
@@ -416,6 +424,8 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     }
 
     int64_t it = 0;
+    double beta_rec[2] = {0.0, 0.0};  // Rec: beta of the previous iteration
+    bool first_rec[2] = {true, true};
     for (;;) {
         bool live[2];
         live[0] = active[0] && resid[0] > A.tol;
@@ -424,19 +434,40 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
 
         // ---- A: Ap = A p, p.Ap ------------------------------------------
         double pap_acc[2] = {0.0, 0.0};
-        spmv([&](int32_t l, int axis, int32_t i) { return Smem ? sp[l] : __ldcg(sax[axis].p + i); },
-             [&](int axis) -> const double * { return sax[axis].p; },
-             [&](int32_t l, int axis, int32_t i, double pi, double ap) {
-                 if (Smem)
-                     sap[l] = ap;
-                 else
-                     sax[axis].ap[i] = ap;
-                 if constexpr (Exact)
-                     __stcg(prod_ptr(A, 0) + (axis ? n0 + i : i), pi * ap);
-                 else
-                     pap_acc[axis] += pi * ap;
-             },
-             live);
+        if constexpr (Rec) {
+            // w = A z; p = z + beta p, Ap = w + beta Ap (p = z, Ap = w at first)
+            spmv([&](int32_t l, int axis, int32_t i) {
+                     return Smem ? sz[l] : __ldcg(sax[axis].z + i);
+                 },
+                 [&](int axis) -> const double * { return sax[axis].z; },
+                 [&](int32_t l, int axis, int32_t i, double zi, double w) {
+                     double pn = zi, apn = w;
+                     if (!first_rec[axis]) {
+                         pn = zi + beta_rec[axis] * KTG_V(sp, p);
+                         apn = w + beta_rec[axis] * KTG_V(sap, ap);
+                     }
+                     KTG_V(sp, p) = pn;
+                     KTG_V(sap, ap) = apn;
+                     pap_acc[axis] += pn * apn;
+                 },
+                 live);
+        } else {
+            spmv([&](int32_t l, int axis, int32_t i) {
+                     return Smem ? sp[l] : __ldcg(sax[axis].p + i);
+                 },
+                 [&](int axis) -> const double * { return sax[axis].p; },
+                 [&](int32_t l, int axis, int32_t i, double pi, double ap) {
+                     if (Smem)
+                         sap[l] = ap;
+                     else
+                         sax[axis].ap[i] = ap;
+                     if constexpr (Exact)
+                         __stcg(prod_ptr(A, 0) + (axis ? n0 + i : i), pi * ap);
+                     else
+                         pap_acc[axis] += pi * ap;
+                 },
+                 live);
+        }
         if constexpr (!Exact) {
             const int sl[2] = {kPAP, kPAP};
             const int ax[2] = {0, 1};
@@ -482,6 +513,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             const double z = r / d;
             KTG_V(sr, r) = r;
             KTG_V(sz, z) = z;
+            if (Rec && Smem) __stcg(S.z + i, z);  // gathered by the next SpMV
             if constexpr (Exact) {
                 const int32_t ci = axis ? n0 + i : i;
                 __stcg(prod_ptr(A, 1) + ci, r * r);
@@ -523,15 +555,24 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             }
         }
 
-        // ---- C: p = z + beta p -------------------------------------------
-        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
-            int axis;
-            int32_t i;
-            locate(l, axis, i);
-            if (!ok2[axis]) continue;
-            const double pn = KTG_V(sz, z) + beta[axis] * KTG_V(sp, p);
-            if (Smem) sp[l] = pn;
-            __stcg(sax[axis].p + i, pn);
+        // ---- C: p = z + beta p (Rec: done by the next SpMV phase) -----------
+        if constexpr (!Rec) {
+            for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
+                int axis;
+                int32_t i;
+                locate(l, axis, i);
+                if (!ok2[axis]) continue;
+                const double pn = KTG_V(sz, z) + beta[axis] * KTG_V(sp, p);
+                if (Smem) sp[l] = pn;
+                __stcg(sax[axis].p + i, pn);
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                if (!live[a]) continue;
+                beta_rec[a] = beta[a];
+                first_rec[a] = false;
+            }
         }
 #pragma unroll
         for (int a = 0; a < 2; ++a) {
@@ -545,7 +586,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             if (A.hist_y) A.hist_y[it] = resid[1];
         }
         ++it;
-        if (!grid_sync(gs, deadline())) return;
+        if (!Rec && !grid_sync(gs, deadline())) return;
     }
 #undef KTG_V
 
@@ -887,9 +928,19 @@ struct Variant {
 };
 
 // form 0: textbook three-barrier PCG; form 1: Chronopoulos-Gear two-barrier;
-// form 2: textbook PCG with the reference's summation order everywhere (one
-// thread per row; bit-identical to the reference's solve).
+// form 2: textbook PCG with the reference's summation order everywhere
+// (bit-identical to the reference's solve); form 3: textbook PCG with A p by
+// recurrence, two barriers.
 Variant pick_variant(int form, bool smem, int lanes) {
+    if (form == 3) {
+        if (lanes == 32)
+            return {smem ? k_pcg<true, 32, false, true> : k_pcg<false, 32, false, true>,
+                    kVecsPerRow};
+        if (smem) return {lanes == 4 ? k_pcg<true, 4, false, true> : k_pcg<true, 1, false, true>,
+                          kVecsPerRow};
+        return {lanes == 4 ? k_pcg<false, 4, false, true> : k_pcg<false, 1, false, true>,
+                kVecsPerRow};
+    }
     if (form == 2) {
         if (lanes == 32)
             return {smem ? k_pcg<true, 32, true> : k_pcg<false, 32, true>, kVecsPerRow};
@@ -910,7 +961,7 @@ int lanes_index(int lanes) { return lanes == 4 ? 1 : lanes == 32 ? 2 : 0; }
 }  // namespace
 
 int pcg_lanes_default = 32;
-int pcg_form_default = 0;
+int pcg_form_default = 3;
 
 int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
                  ktg_solve_info *info_dev, double *hist_x, double *hist_y, int64_t hist_cap) {
@@ -932,7 +983,7 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     const int form = c->pcg_form >= 0 ? c->pcg_form : pcg_form_default;
     // Dynamic shared memory for the vector slices: what the block may opt in
     // to, less the kernel's static arrays, capped at kPcgSmemBytes.
-    static size_t budget[3][3] = {};
+    static size_t budget[4][3] = {};
     size_t &bud = budget[form][lanes_index(lanes)];
     if (bud == 0) {
         int optin = 0;
@@ -953,7 +1004,7 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     const bool use_smem = smem <= bud;
     const Variant v = pick_variant(form, use_smem, lanes);
     const size_t dyn = use_smem ? smem : tile;
-    static bool attr_set[3][2][3] = {};
+    static bool attr_set[4][2][3] = {};
     bool &done = attr_set[form][use_smem][lanes_index(lanes)];
     if (!done) {
         KTG_CUDA(c, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
