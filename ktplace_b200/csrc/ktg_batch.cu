@@ -27,6 +27,7 @@
 
 #include "ktg_common.cuh"
 #include "ktg_context.h"
+#include "ktg_spmv.cuh"
 #include "ktplace_b200.h"
 
 namespace cg = cooperative_groups;
@@ -116,6 +117,7 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
     cg::cluster_group cl = cg::this_cluster();
     __shared__ double scratch[33 * 4];
     __shared__ double part[2 * 4];
+    __shared__ __align__(16) double tilebuf[32 * kTileChunk];  // warp tiles, <= 32 warps
     __shared__ int s_job;
     __shared__ int s_stop;
     int buf = 0;
@@ -181,12 +183,24 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
                 if (!(active && resid > A.tol && it < A.max_iter)) break;
                 if (rank == 0 && threadIdx.x == 0) s_stop = global_timer_ns() > deadline ? 1 : 0;
                 double w[1] = {0.0};
-                for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-                    const double pi = __ldcg(p + i);
-                    const double s = row_dot<double, double>(rp, col, val, p, i, dg[i] * pi);
-                    ap[i] = s;
-                    w[0] += pi * s;
-                }
+                double pcur = 0.0;
+                warp_tile_spmv<double>(
+                    a, INT32_MAX, b - a, nullptr, tilebuf,
+                    [&](int, const int32_t *&trp, const int32_t *&tcol, const double *&tval,
+                        const double *&tin) {
+                        trp = rp;
+                        tcol = col;
+                        tval = val;
+                        tin = p;
+                    },
+                    [&](int32_t, int, int32_t i) {
+                        pcur = __ldcg(p + i);
+                        return dg[i] * pcur;
+                    },
+                    [&](int32_t, int, int32_t i, double s) {
+                        ap[i] = s;
+                        w[0] += pcur * s;
+                    });
                 cluster_sum<1>(w, part, buf, scratch, cl);
                 if (*cl.map_shared_rank(&s_stop, 0)) {
                     res.status = KTG_ERR_TIMEOUT;
@@ -272,13 +286,24 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
                 bool live = rho > 0.0;
                 while (live && iresid > target && inner < A.max_iter) {
                     double w[1] = {0.0};
-                    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-                        const float pi = __ldcg(p + i);
-                        const float s = row_dot<float, float>(rp, col, val32, p, i,
-                                                              static_cast<float>(dg[i]) * pi);
-                        ap[i] = s;
-                        w[0] += static_cast<double>(pi) * s;
-                    }
+                    float pcur = 0.0f;
+                    warp_tile_spmv<float>(
+                        a, INT32_MAX, b - a, nullptr, reinterpret_cast<float *>(tilebuf),
+                        [&](int, const int32_t *&trp, const int32_t *&tcol, const float *&tval,
+                            const float *&tin) {
+                            trp = rp;
+                            tcol = col;
+                            tval = val32;
+                            tin = p;
+                        },
+                        [&](int32_t, int, int32_t i) {
+                            pcur = __ldcg(p + i);
+                            return static_cast<float>(dg[i]) * pcur;
+                        },
+                        [&](int32_t, int, int32_t i, float s) {
+                            ap[i] = s;
+                            w[0] += static_cast<double>(pcur) * s;
+                        });
                     cluster_sum<1>(w, part, buf, scratch, cl);
                     ++inner;
                     if (!(w[0] > 0.0)) break;

@@ -483,18 +483,27 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         }
     };
 
-    // u = M r for own rows (learned M), reading the published D^-1/2 r.
+    // u = M r for own rows (learned M), reading the published D^-1/2 r: the
+    // sum over A's pattern runs as warp tiles, adding in the order and with
+    // the roundings of apply_m_row.
     auto apply_m = [&](const bool *live) {
-        for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
-            int axis;
-            int32_t i;
-            locate(l, axis, i);
-            if (!live[axis]) continue;
-            const MixAxis &S = sax[axis];
-            const float u = apply_m_row(S, i, sr[l]);
-            su[l] = u;
-            __stcg(S.z + i, u);
-        }
+        warp_tile_spmv<float>(
+            r0, n0, R, live, tile32,
+            [&](int pass, const int32_t *&rp, const int32_t *&col, const float *&val,
+                const float *&in) {
+                rp = sax[pass].rp;
+                col = sax[pass].col;
+                val = sax[pass].s32;
+                in = sax[pass].rs;
+            },
+            [&](int32_t, int, int32_t) { return 0.0f; },
+            [&](int32_t l, int axis, int32_t i, float acc) {
+                const MixAxis &S = sax[axis];
+                const float d = static_cast<float>(__ldg(S.diag + i));
+                const float u = sr[l] / d + rsqrtf(d) * acc;
+                su[l] = u;
+                __stcg(S.z + i, u);
+            });
     };
 
     double b_norm[2] = {0.0, 0.0}, true_resid[2] = {0.0, 0.0}, prev_resid[2] = {0.0, 0.0};
