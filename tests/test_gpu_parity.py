@@ -75,6 +75,39 @@ def test_pcg_matches_reference(name, gpu_ctx):
         assert abs(r["resid"][a] - g["resid"][a]) <= HIST_RTOL * max(g["resid"][a], TOL)
 
 
+@pytest.mark.parametrize("name", ["tiny_macros", "edge_alpha", "small12k"])
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
+def test_pcg_forms_and_spmv_shapes(name, form, gpu_ctx):
+    """Every solve form against the reference, in every SpMV shape. Warp tiles
+    (32) and one thread per row (1) add each row's terms in the same order,
+    so their solves are bit-identical in every form; form 2 (the reference's
+    summation order) equals the reference's solution bit for bit."""
+    g, meta = gold(name)
+    raw, nl, x, y, ax, ay, alpha, _ = build_case(name)
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, alpha, ax if alpha > 0 else None, ay if alpha > 0 else None, fx, fy)
+    got = {}
+    try:
+        gpu_ctx.set_option("pcg_form", form)
+        for lanes in (32, 1, 4):
+            gpu_ctx.set_option("pcg_lanes", lanes)
+            r = gpu_ctx.solve(x, y, TOL, MAX_ITER, hist_cap=MAX_ITER)
+            assert r["iters"] == meta["iters"], (form, lanes)
+            assert rel(r["hist_x"], g["hist_x"]) <= HIST_RTOL, (form, lanes)
+            assert rel(r["x"], g["x"]) <= SOL_RTOL, (form, lanes)
+            assert rel(r["y"], g["y"]) <= SOL_RTOL, (form, lanes)
+            got[lanes] = r
+    finally:
+        gpu_ctx.set_option("pcg_form", -1)
+        gpu_ctx.set_option("pcg_lanes", 0)
+    for k in ("x", "y", "hist_x", "hist_y"):
+        assert np.array_equal(got[32][k], got[1][k]), (form, k)
+    if form == 2:
+        for lanes in (32, 1):
+            assert np.array_equal(got[lanes]["x"], g["x"]) and np.array_equal(got[lanes]["y"], g["y"])
+
+
 @pytest.mark.parametrize("name", list(CASES))
 def test_hpwl_and_density(name, gpu_ctx):
     from ktplace_b200 import grid as kgrid
