@@ -417,11 +417,12 @@ int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacl
 
 /* Sets a kernel-shape option of this context (no reference counterpart; the
  * values are what the project autotuner chooses between):
- *   "pcg_lanes"  SpMV shape in the PCG: 32 = warp tiles (a warp streams the
- *                nonzeros of 32 consecutive rows, each lane adding its row's
- *                products in storage order), 1 = one thread per row (the
- *                same row sums, so the same solve bit for bit), 4 = four
- *                lanes per row; 0 = default (32)
+ *   "pcg_lanes"  SpMV shape in the PCG: 32 = warp tiles (each warp streams
+ *                the nonzeros of its range of rows 32 rows at a time, each
+ *                lane adding its row's products in storage order; the ranges
+ *                are balanced by nonzeros), 1 = one thread per row (the same
+ *                row sums: the same solve bit for bit in form 2, to rounding
+ *                in the others), 4 = four lanes per row; 0 = default (32)
  *   "pcg_form"   0: textbook PCG (three grid barriers per iteration),
  *                1: Chronopoulos-Gear form (two),
  *                3: textbook PCG with A p = A z + beta A p_prev by recurrence

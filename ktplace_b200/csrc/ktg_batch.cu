@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
     __shared__ double scratch[33 * 4];
     __shared__ double part[2 * 4];
     __shared__ __align__(16) double tilebuf[32 * kTileChunk];  // warp tiles, <= 32 warps
+    __shared__ int32_t wb[32 + 1];
     __shared__ int s_job;
     __shared__ int s_stop;
     int buf = 0;
@@ -149,6 +150,11 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
         const double *rhs = A.rhs + S.row_base;
         double *x = A.x + S.row_base;
         double *r = A.r + S.row_base;
+
+        // per-warp row ranges of the warp tiles, balanced by nonzeros
+        warp_row_bounds(b - a, wb, [&](int32_t l) {
+            return int64_t(__ldg(rp + a + l)) - __ldg(rp + a) + int64_t(kRowCost) * l;
+        });
 
         ktg_batch_result res;
         res.iters = 0;
@@ -185,7 +191,7 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
                 double w[1] = {0.0};
                 double pcur = 0.0;
                 warp_tile_spmv<double>(
-                    a, INT32_MAX, b - a, nullptr, tilebuf,
+                    a, INT32_MAX, b - a, nullptr, wb, tilebuf,
                     [&](int, const int32_t *&trp, const int32_t *&tcol, const double *&tval,
                         const double *&tin) {
                         trp = rp;
@@ -288,7 +294,7 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
                     double w[1] = {0.0};
                     float pcur = 0.0f;
                     warp_tile_spmv<float>(
-                        a, INT32_MAX, b - a, nullptr, reinterpret_cast<float *>(tilebuf),
+                        a, INT32_MAX, b - a, nullptr, wb, reinterpret_cast<float *>(tilebuf),
                         [&](int, const int32_t *&trp, const int32_t *&tcol, const float *&tval,
                             const float *&tin) {
                             trp = rp;

@@ -267,6 +267,19 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
         return d < total_deadline ? d : total_deadline;
     };
     GridSync gs = grid_sync_init(A.bar_count, A.bar_gen, A.status);
+    // warp tiles: per-warp row ranges balanced by nonzeros, fixed for the solve
+    __shared__ int32_t wb[kTileWarps + 1];
+    if (Lanes == 32) {
+        const PcgAxis X = A.ax[0], Y = A.ax[1];
+        auto prefix = [&](int32_t c) -> int64_t {  // work of combined rows [0, c)
+            const int64_t e = c <= X.n ? int64_t(__ldg(X.rp + c))
+                                       : int64_t(__ldg(X.rp + X.n)) + __ldg(Y.rp + (c - X.n));
+            return e + int64_t(kRowCost) * c;
+        };
+        const int32_t rb = min(r0, A.total_rows);  // R == 0 past the last row
+        const int64_t base = prefix(rb);
+        warp_row_bounds(R, wb, [&](int32_t l) { return prefix(rb + l) - base; });
+    }
     // Row l of this block: axis and row index inside that axis.
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
         const int32_t c = r0 + l;
@@ -294,7 +307,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
         if (Lanes == 32) {
             double vcur = 0.0;
             warp_tile_spmv<double>(
-                r0, n0, R, live, tilebuf,
+                r0, n0, R, live, wb, tilebuf,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
                     const double *&in) {
                     rp = sax[pass].rp;
@@ -646,6 +659,19 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
         return d < total_deadline ? d : total_deadline;
     };
     GridSync gs = grid_sync_init(A.bar_count, A.bar_gen, A.status);
+    // warp tiles: per-warp row ranges balanced by nonzeros, fixed for the solve
+    __shared__ int32_t wb[kTileWarps + 1];
+    if (Lanes == 32) {
+        const PcgAxis X = A.ax[0], Y = A.ax[1];
+        auto prefix = [&](int32_t c) -> int64_t {  // work of combined rows [0, c)
+            const int64_t e = c <= X.n ? int64_t(__ldg(X.rp + c))
+                                       : int64_t(__ldg(X.rp + X.n)) + __ldg(Y.rp + (c - X.n));
+            return e + int64_t(kRowCost) * c;
+        };
+        const int32_t rb = min(r0, A.total_rows);  // R == 0 past the last row
+        const int64_t base = prefix(rb);
+        warp_row_bounds(R, wb, [&](int32_t l) { return prefix(rb + l) - base; });
+    }
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
         const int32_t c = r0 + l;
         axis = c >= n0 ? 1 : 0;
@@ -670,7 +696,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
         if (Lanes == 32) {
             double vcur = 0.0;
             warp_tile_spmv<double>(
-                r0, n0, R, live, tilebuf,
+                r0, n0, R, live, wb, tilebuf,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
                     const double *&in) {
                     rp = sax[pass].rp;

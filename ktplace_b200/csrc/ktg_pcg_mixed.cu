@@ -449,6 +449,21 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     GridSync gs = grid_sync_init(A.bar_count, A.bar_gen, A.status);
     auto sync = [&]() { return grid_sync(gs, deadline()); };
     constexpr bool pre = PRE == kPreLearned;
+    // per-warp row ranges of the warp tiles, balanced by nonzeros (the axes'
+    // row pointers may start anywhere in a shared column array)
+    __shared__ int32_t wb[kMixThreads / 32 + 1];
+    {
+        const MixAxis X = A.ax[0], Y = A.ax[1];
+        const int64_t x0 = __ldg(X.rp), xn = __ldg(X.rp + X.n), y0 = __ldg(Y.rp);
+        auto prefix = [&](int32_t c) -> int64_t {  // work of combined rows [0, c)
+            const int64_t e = c <= X.n ? int64_t(__ldg(X.rp + c)) - x0
+                                       : (xn - x0) + (int64_t(__ldg(Y.rp + (c - X.n))) - y0);
+            return e + int64_t(kRowCost) * c;
+        };
+        const int32_t rb = min(r0, A.total_rows);
+        const int64_t basec = prefix(rb);
+        warp_row_bounds(R, wb, [&](int32_t l) { return prefix(rb + l) - basec; });
+    }
     for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
         int axis;
         int32_t i;
@@ -488,7 +503,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     // the roundings of apply_m_row.
     auto apply_m = [&](const bool *live) {
         warp_tile_spmv<float>(
-            r0, n0, R, live, tile32,
+            r0, n0, R, live, wb, tile32,
             [&](int pass, const int32_t *&rp, const int32_t *&col, const float *&val,
                 const float *&in) {
                 rp = sax[pass].rp;
@@ -516,7 +531,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         {
             double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rr x, bb x, rr y, bb y
             warp_tile_spmv<double>(
-                r0, n0, R, nullptr, tile64,
+                r0, n0, R, nullptr, wb, tile64,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
                     const double *&in) {
                     rp = sax[pass].rp;
@@ -592,7 +607,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         for (;;) {
             double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // gamma, delta, rr per axis
             warp_tile_spmv<float>(
-                r0, n0, R, in_live, tile32,
+                r0, n0, R, in_live, wb, tile32,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const float *&val,
                     const float *&in) {
                     rp = sax[pass].rp;

@@ -31,28 +31,68 @@ struct TilePair<float> {
     using type = float2;
 };
 
+// Work per row when the block's rows are split between its warps: the row's
+// nonzeros plus this many (row pointers, the row's own terms, the emit);
+// 2 measured best of {2, 8, 24} on the 211k and 1M systems.
+constexpr int32_t kRowCost = 2;
+
+// Contiguous row ranges of the block's warps, balanced by kRowCost plus the
+// nonzeros of each row: warp w takes rows [wb[w], wb[w+1]) of [0, R).
+// cost(l) is the (nondecreasing) work of rows [0, l). Every row sum stays
+// the same; only which lane adds it changes, and that depends on the matrix
+// pattern alone, so results are still the same from run to run. All threads
+// of the block call it; wb has room for the warp count + 1.
+template <class Cost>
+__device__ __forceinline__ void warp_row_bounds(int32_t R, int32_t *wb, Cost cost) {
+    const int nw = blockDim.x >> 5;
+    const int w = threadIdx.x;
+    if (w <= nw) {
+        int32_t res = w == 0 ? 0 : R;
+        if (w > 0 && w < nw) {
+            const int64_t target = cost(R) * w / nw;
+            int32_t lo = 0, hi = R;  // smallest l with cost(l) >= target
+            while (lo < hi) {
+                const int32_t mid = lo + (hi - lo) / 2;
+                if (cost(mid) >= target)
+                    hi = mid;
+                else
+                    lo = mid + 1;
+            }
+            res = lo;
+        }
+        wb[w] = res;
+    }
+    __syncthreads();
+}
+
 // Rows [r0, r0 + R) of a block's slice of the combined row space
 // [axis 0 rows | axis 1 rows] (axis 1 starts at row n0); rows of an axis
 // with live[axis] false are skipped (live may be null). All threads of the
 // block call it.
+//   wb: per-warp row ranges from warp_row_bounds, or null for tiles dealt
+//       to the warps in turn (warp w takes tiles w, w + nw, ...);
 //   csr(pass, rp, col, val, in): the axis's CSR arrays and gathered vector;
 //   start(l, pass, i) -> T: the row's first term (diag * own value);
 //   emit(l, pass, i, sum): the finished row sum.
 // tilebuf holds kTileChunk elements per warp, 16-byte aligned.
 template <typename T, class Csr, class Start, class Emit>
 __device__ __forceinline__ void warp_tile_spmv(int32_t r0, int32_t n0, int32_t R, const bool *live,
-                                               T *tilebuf, Csr csr, Start start, Emit emit) {
+                                               const int32_t *wb, T *tilebuf, Csr csr, Start start,
+                                               Emit emit) {
     using P2 = typename TilePair<T>::type;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int nw = blockDim.x >> 5;
     T *buf = tilebuf + warp * kTileChunk;
-    for (int32_t t0 = warp * 32; t0 < R; t0 += nw * 32) {
+    const int32_t first = wb ? wb[warp] : warp * 32;
+    const int32_t end = wb ? wb[warp + 1] : R;
+    const int32_t step = wb ? 32 : nw * 32;
+    for (int32_t t0 = first; t0 < end; t0 += step) {
         const int32_t l = t0 + lane;
         const int32_t c = r0 + l;
         const int axis = c >= n0 ? 1 : 0;
         const int32_t i = c - (axis ? n0 : 0);
-        const bool mine = l < R && (!live || live[axis]);
+        const bool mine = l < end && (!live || live[axis]);
         // a tile that straddles the axis boundary takes one pass per axis
 #pragma unroll 1
         for (int pass = 0; pass < 2; ++pass) {

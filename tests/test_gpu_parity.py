@@ -79,9 +79,11 @@ def test_pcg_matches_reference(name, gpu_ctx):
 @pytest.mark.parametrize("form", [0, 1, 2, 3])
 def test_pcg_forms_and_spmv_shapes(name, form, gpu_ctx):
     """Every solve form against the reference, in every SpMV shape. Warp tiles
-    (32) and one thread per row (1) add each row's terms in the same order,
-    so their solves are bit-identical in every form; form 2 (the reference's
-    summation order) equals the reference's solution bit for bit."""
+    (32) and one thread per row (1) add each row's terms in the same order;
+    they differ only in which thread's partial of a dot product a row lands
+    in, so their solves agree to rounding in forms 0, 1 and 3, and are
+    bit-identical in form 2 (the reference's summation order), which equals
+    the reference's solution bit for bit."""
     g, meta = gold(name)
     raw, nl, x, y, ax, ay, alpha, _ = build_case(name)
     gpu_ctx.upload_netlist(nl)
@@ -102,7 +104,10 @@ def test_pcg_forms_and_spmv_shapes(name, form, gpu_ctx):
         gpu_ctx.set_option("pcg_form", -1)
         gpu_ctx.set_option("pcg_lanes", 0)
     for k in ("x", "y", "hist_x", "hist_y"):
-        assert np.array_equal(got[32][k], got[1][k]), (form, k)
+        if form == 2:
+            assert np.array_equal(got[32][k], got[1][k]), (form, k)
+        else:
+            assert rel(got[32][k], got[1][k]) <= 1e-12, (form, k)
     if form == 2:
         for lanes in (32, 1):
             assert np.array_equal(got[lanes]["x"], g["x"]) and np.array_equal(got[lanes]["y"], g["y"])
