@@ -435,10 +435,10 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     const int32_t cap = A.rows_per_block;
     double *base = A.gslice ? A.gslice + static_cast<size_t>(blockIdx.x) * cap * 5 : dyn;
     // warp-tile buffer after the shared slices (16-byte aligned)
-    double *tile64 = A.gslice ? dyn : dyn + (5 * static_cast<size_t>(cap) + 1) / 2 * 2;
+    double *tile64 = A.gslice ? dyn : dyn + (4 * static_cast<size_t>(cap) + 1) / 2 * 2;
     float *tile32 = reinterpret_cast<float *>(tile64);
-    double *sx = base, *sd = base + cap;
-    float *sr = reinterpret_cast<float *>(base + 2 * cap);
+    double *sx = base;  // diag is read through L1 (shared memory comes out of L1)
+    float *sr = reinterpret_cast<float *>(base + cap);
     float *su = sr + cap, *sw = su + cap, *sp = sw + cap, *ss = sp + cap, *sdd = ss + cap;
     const int32_t n0 = sax[0].n;
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
@@ -469,7 +469,6 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         int32_t i;
         locate(l, axis, i);
         sx[l] = sax[axis].x[i];
-        sd[l] = __ldg(sax[axis].diag + i);
     }
     __syncthreads();
 
@@ -539,7 +538,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     val = sax[pass].val;
                     in = sax[pass].x;
                 },
-                [&](int32_t l, int, int32_t) { return sd[l] * sx[l]; },
+                [&](int32_t l, int pass, int32_t i) { return __ldg(sax[pass].diag + i) * sx[l]; },
                 [&](int32_t l, int axis, int32_t i, double s) {
                     const MixAxis &S = sax[axis];
                     const double b = __ldg(S.rhs + i);
@@ -548,9 +547,9 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     sr[l] = rf;
                     sdd[l] = 0.0f;
                     if (pre) {
-                        __stcg(S.rs + i, rf * rsqrtf(static_cast<float>(sd[l])));
+                        __stcg(S.rs + i, rf * rsqrtf(static_cast<float>(__ldg(S.diag + i))));
                     } else if (PRE == kPreJacobi) {
-                        const float u = rf / static_cast<float>(sd[l]);
+                        const float u = rf / static_cast<float>(__ldg(S.diag + i));
                         su[l] = u;
                         __stcg(S.z + i, u);
                     }
@@ -615,7 +614,9 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     val = sax[pass].val32;
                     in = sax[pass].z;
                 },
-                [&](int32_t l, int, int32_t) { return static_cast<float>(sd[l]) * su[l]; },
+                [&](int32_t l, int pass, int32_t i) {
+                    return static_cast<float>(__ldg(sax[pass].diag + i)) * su[l];
+                },
                 [&](int32_t l, int axis, int32_t, float w) {
                     const float ui = su[l];
                     sw[l] = w;
@@ -687,9 +688,9 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 const float r = sr[l] - alpha[axis] * sn;
                 sr[l] = r;
                 if (pre) {
-                    __stcg(S.rs + i, r * rsqrtf(static_cast<float>(sd[l])));
+                    __stcg(S.rs + i, r * rsqrtf(static_cast<float>(__ldg(S.diag + i))));
                 } else if (PRE == kPreJacobi) {
-                    const float u = r / static_cast<float>(sd[l]);
+                    const float u = r / static_cast<float>(__ldg(S.diag + i));
                     su[l] = u;
                     __stcg(S.z + i, u);
                 }
@@ -799,9 +800,9 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
         }
     }
     // Chronopoulos-Gear kernel (always for the aggregation preconditioner),
-    // with shared-memory slices of 40 bytes per row when they fit, else
+    // with shared-memory slices of 32 bytes per row when they fit, else
     // global ones; the textbook kernel on global vectors when asked for.
-    const size_t slice = 40 * static_cast<size_t>(A.rows_per_block) + 8;  // + alignment
+    const size_t slice = 32 * static_cast<size_t>(A.rows_per_block) + 8;  // + alignment
     const size_t tile = sizeof(double) * kTileChunk * (kMixThreads / 32);
     const bool cg_form = agg || c->mixed_form != 0;
     const bool in_smem = slice + tile <= kMixSmemBytes;
