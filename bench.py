@@ -219,7 +219,7 @@ def pcg_bytes(n: int, m: int, iters: int) -> float:
 
 # DRAM bytes (read + write) per launch of the dominant kernel on this
 # workload, from the ncu capture summarised in profiles/k_pcg_synth211k.md.
-NCU_TRAFFIC_BYTES = {"k_pcg": 188.578560e6 + 46.643712e6}
+NCU_TRAFFIC_BYTES = {"k_pcg": 111.045376e6 + 41.966848e6}
 
 
 def measured_peak():

@@ -73,8 +73,8 @@ __device__ __forceinline__ double block_sum(double v, double *scratch) {
     return scratch[32];
 }
 
-// Deterministic block sum of K values per thread (K <= 4). scratch holds
-// >= 33*K doubles.
+// Deterministic block sum of K values per thread; each value is summed with
+// the same tree whatever K is. scratch holds >= 33*K doubles.
 template <int K>
 __device__ __forceinline__ void block_sum_k(double (&v)[K], double *scratch) {
     const int lane = threadIdx.x & 31;

@@ -414,7 +414,7 @@ enum MixPre { kPreJacobi = 0, kPreLearned = 1, kPreAgg = 2 };
 template <int PRE>
 __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     extern __shared__ __align__(16) double dyn[];
-    __shared__ double scratch[33 * 4];
+    __shared__ double scratch[33 * 6];  // block sums of up to 6 values
     __shared__ MixAxis sax[2];
     if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
     __syncthreads();
@@ -625,28 +625,21 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     acc[axis * 3 + 1] += static_cast<double>(w) * ui;
                     acc[axis * 3 + 2] += static_cast<double>(r) * r;
                 });
-            {
-                double v0[3] = {acc[0], acc[1], acc[2]};
-                double v1[3] = {acc[3], acc[4], acc[5]};
-                const int sl[3] = {kIRZ, kIPAP, kIRR};
-                const int a0[3] = {0, 0, 0};
-                const int a1[3] = {1, 1, 1};
-                mstore<3>(A, v0, sl, a0, scratch);
-                mstore<3>(A, v1, sl, a1, scratch);
+            {  // one block sum for both axes (each value summed as alone)
+                const int sl[6] = {kIRZ, kIPAP, kIRR, kIRZ, kIPAP, kIRR};
+                const int ax[6] = {0, 0, 0, 1, 1, 1};
+                mstore<6>(A, acc, sl, ax, scratch);
             }
             if (!sync()) return;
             float alpha[2] = {0.0f, 0.0f}, beta[2] = {0.0f, 0.0f};
             bool ok[2] = {false, false};
             {
-                double s[4], t[2];
-                const int sl[4] = {kIRZ, kIPAP, kIRR, kIRZ};
-                const int ax[4] = {0, 0, 0, 1};
-                mreduce<4>(A, s, sl, ax, scratch);
-                const int sl2[2] = {kIPAP, kIRR};
-                const int ax2[2] = {1, 1};
-                mreduce<2>(A, t, sl2, ax2, scratch);
-                const double gamma[2] = {s[0], s[3]}, delta[2] = {s[1], t[0]};
-                const double rr[2] = {s[2], t[1]};
+                double s[6];
+                const int sl[6] = {kIRZ, kIPAP, kIRR, kIRZ, kIPAP, kIRR};
+                const int ax[6] = {0, 0, 0, 1, 1, 1};
+                mreduce<6>(A, s, sl, ax, scratch);
+                const double gamma[2] = {s[0], s[3]}, delta[2] = {s[1], s[4]};
+                const double rr[2] = {s[2], s[5]};
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
                     if (!in_live[a]) continue;
