@@ -22,8 +22,8 @@
 //     iterate's residuals; x and y already hold the final solution then.
 //   * solveBothAxes sums its dot products in the reference's order
 //     (pcg_form 2), so solutions, iteration counts and residuals are the
-//     reference's bit for bit; $KTPLACE_B200_PCG_FORM=1 selects the faster
-//     two-barrier form, whose results agree to about 1e-9 relative.
+//     reference's bit for bit; $KTPLACE_B200_PCG_FORM=3 selects the library's
+//     default (faster) form, whose results agree to about 1e-9 relative.
 #include "globalPlacer/simpl/simpl_lss.h"
 #include "util/kt_log.h"
 
