@@ -403,7 +403,10 @@ def run_ours(args):
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": NCU_TRAFFIC_BYTES["k_pcg"], "algorithmic_bytes": byts,
-                         "note": "working set is L2-resident: traffic << algorithmic bytes"},
+                         "note": "working set is L2-resident: traffic << algorithmic bytes",
+                         "limiter": "L1TEX data pipe: 56% of peak over the whole solve in the ncu "
+                                    "capture (random 8-byte gathers, one LSU wavefront each); "
+                                    "L2 39%, DRAM 0.2% (profiles/k_pcg_synth211k.md)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
