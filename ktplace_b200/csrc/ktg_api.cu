@@ -92,6 +92,7 @@ void free_netlist(ktg_ctx *c) {
     dev_free(c->height);
     dev_free(c->area);
     dev_free(c->row_cnt);
+    dev_free(c->heavy_rows);
     dev_free(c->block_sum);
     c->have_netlist = false;
 }
@@ -443,6 +444,7 @@ int ktg_upload_netlist(ktg_ctx *c, const ktg_netlist_view *nl) {
     if ((rc = dev_alloc(c, &c->area, n))) return rc;
     const int64_t bpa = (n + 255) / 256;
     if ((rc = dev_alloc(c, &c->row_cnt, 2 * n))) return rc;
+    if ((rc = dev_alloc(c, &c->heavy_rows, 1 + 2 * n))) return rc;
     if ((rc = dev_alloc(c, &c->block_sum, 2 * bpa))) return rc;
     if ((rc = reserve_systems(c, n, c->cap_nnz))) return rc;
     for (auto &s2 : c->sys) {

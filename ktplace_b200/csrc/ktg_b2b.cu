@@ -2,7 +2,7 @@
 //
 // Replaces LinearSystems::buildB2B / buildB2BAxis (globalPlacer/simpl/
 // simpl_lss.cc:11-114) and simplPlacer::Impl::getHpwl (simpl_placer.cc:
-// 256-275). Four launches build both axes at once:
+// 256-275). Five launches build both axes at once:
 //
 //   k_bound_pins  one thread per net: first-index argmin/argmax of the pin
 //                 coordinate for x and y (simpl_lss.cc:32-45) and, from the
@@ -15,7 +15,9 @@
 //   k_fill        one thread per (axis, movable cell): block scan of the row
 //                 counts -> row_ptr, then the row's edges in the reference's
 //                 order (simpl_lss.cc:47-73, 89-113) so that diag and rhs are
-//                 summed exactly as the reference sums them.
+//                 summed exactly as the reference sums them; rows with many
+//                 movable other ends go to k_fill_heavy (a warp per row,
+//                 the same edges, sums and roundings).
 //
 // Bit-exactness: the library is compiled with -fmad=false (no FMA
 // contraction, like the reference's -ffp-contract=off) and CUDA's IEEE
@@ -304,11 +306,17 @@ __global__ void __launch_bounds__(1024)
 
 // Row pointers from a block scan of the counts, then the row's entries.
 // Kraftwerk2: alpha < 0 leaves the right-hand side at zero (withRhs false).
+// Rows with at least this many movable other ends (the bound pins of large
+// nets) are filled by k_fill_heavy, one warp per row, instead of by one
+// thread: their edges are the long serial chains of dependent gathers that
+// would otherwise set the kernel's time.
+constexpr int32_t kHeavyRow = 32;
+
 template <int R = kSimpl>
 __global__ void __launch_bounds__(kBuildThreads)
     k_fill(NetlistDev nl, AxisArgs ax, AxisArgs ay, int32_t blocks_per_axis, double alpha,
            const int32_t *__restrict__ row_cnt, const int64_t *__restrict__ block_first,
-           int64_t cap, const int *__restrict__ status) {
+           int64_t cap, const int *__restrict__ status, int32_t *__restrict__ heavy) {
     __shared__ int32_t warp_tot[kBuildThreads / kWarp];
     const int axis = blockIdx.x >= blocks_per_axis ? 1 : 0;
     const AxisArgs &a = axis ? ay : ax;
@@ -339,6 +347,10 @@ __global__ void __launch_bounds__(kBuildThreads)
     if (*status != kStatusOk) return;  // capacity exceeded: leave the buffers alone
     int64_t slot = block_first[blockIdx.x] + warp_tot[threadIdx.x >> 5] + (incl - cnt);
     a.row_ptr[i] = static_cast<int32_t>(slot);
+    if (cnt >= kHeavyRow) {  // left for k_fill_heavy (the order of the list is free)
+        heavy[1 + atomicAdd(heavy, 1)] = axis * nl.n + i;
+        return;
+    }
     double dg = 0.0;
     double rh = 0.0;
     for_each_edge<R>(nl, a.pos, a.fixed, a.off, a.lo, a.hi, a.floor_len, i,
@@ -373,6 +385,105 @@ __global__ void __launch_bounds__(kBuildThreads)
     }
     a.diag[i] = ref_max(dg, 1e-12);
     a.rhs[i] = rh;
+}
+
+// One warp per heavy row: the same edges in the same order as for_each_edge,
+// 32 at a time. Each lane computes one edge (gathers, weight, the rhs term)
+// and, when the other end is movable, writes its CSR entry at its rank among
+// this chunk's entries; then every lane adds the chunk's w and rhs terms in
+// edge order, so diag and rhs round exactly as in k_fill.
+template <int R = kSimpl>
+__global__ void __launch_bounds__(kBuildThreads)
+    k_fill_heavy(NetlistDev nl, AxisArgs ax, AxisArgs ay, double alpha, int64_t cap,
+                 const int *__restrict__ status, const int32_t *__restrict__ heavy) {
+    const int lane = threadIdx.x & 31;
+    const int32_t warps = static_cast<int32_t>((gridDim.x * blockDim.x) >> 5);
+    const int32_t count = heavy[0];
+    if (*status != kStatusOk) return;
+    for (int32_t h = static_cast<int32_t>((blockIdx.x * blockDim.x + threadIdx.x) >> 5); h < count;
+         h += warps) {
+        const int32_t code = heavy[1 + h];
+        const int axis = code >= nl.n ? 1 : 0;
+        const int32_t i = code - (axis ? nl.n : 0);
+        const AxisArgs &a = axis ? ay : ax;
+        const double own_pos = a.pos[i];
+        int64_t slot = a.row_ptr[i];
+        double dg = 0.0, rh = 0.0;
+        const int32_t e0 = nl.pin_start[i], e1 = nl.pin_start[i + 1];
+        for (int32_t e = e0; e < e1; ++e) {
+            const int2 ref = nl.pin_ref[e];
+            const int32_t k = ref.x;
+            const uint32_t q = static_cast<uint32_t>(ref.y);
+            const uint32_t l = a.lo[k], hb = a.hi[k];
+            if (l == hb) continue;
+            const int32_t s0 = nl.net_start[k];
+            const double base = R == kKraftwerk2 ? 2.0 * nl.net_base[k] : nl.net_base[k];
+            const double own_raw = a.off[s0 + q];
+            const double own = own_pos + own_raw;
+            const double own_offset = own - own_pos;
+            const bool bound = q == l || q == hb;
+            // the pin's edges: every other pin t of the net, or its lo and hi
+            const int32_t ne = bound ? nl.net_start[k + 1] - s0 : 2;
+            for (int32_t t0 = 0; t0 < ne; t0 += 32) {
+                const int32_t j = t0 + lane;
+                bool has = false, entry = false;
+                int32_t var = -1;
+                double w = 0.0, term = 0.0;
+                if (j < ne) {
+                    const uint32_t t = bound ? static_cast<uint32_t>(j) : (j == 0 ? l : hb);
+                    if (!bound || t != q) {
+                        const int32_t p = s0 + static_cast<int32_t>(t);
+                        var = nl.pin_var[p];
+                        if (!(R == kKraftwerk2 && var == i)) {
+                            has = true;
+                            const double cp = cell_pos(a.pos, a.fixed, var, nl.pin_cell[p]);
+                            const double other_raw = a.off[p];
+                            const double there = cp + other_raw;
+                            w = base / ref_max(fabs(own - there), a.floor_len);
+                            if (var >= 0) {
+                                entry = true;
+                                term = R == kKraftwerk2 ? w * (other_raw - own_raw)
+                                                        : w * ((there - cp) - own_offset);
+                            } else {
+                                term = R == kKraftwerk2 ? w * (there - own_raw)
+                                                        : w * (there - own_offset);
+                            }
+                        }
+                    }
+                }
+                const unsigned em = __ballot_sync(0xffffffffu, entry);
+                if (entry) {
+                    const int64_t at = slot + __popc(em & ((1u << lane) - 1u));
+                    if (at < cap) {
+                        a.col[at] = var;
+                        a.val[at] = -w;
+                    }
+                }
+                slot += __popc(em);
+                const unsigned hm = __ballot_sync(0xffffffffu, has);
+                for (unsigned m = hm; m; m &= m - 1) {  // edge order = lane order
+                    const int src = __ffs(m) - 1;
+                    dg += __shfl_sync(0xffffffffu, w, src);
+                    rh += __shfl_sync(0xffffffffu, term, src);
+                }
+            }
+        }
+        if (lane == 0) {
+            if (R == kKraftwerk2) {
+                a.diag[i] = dg;
+                a.rhs[i] = alpha < 0.0 ? 0.0 : rh;
+            } else {
+                if (alpha > 0.0) {
+                    const double p = a.pos[i];
+                    const double wa = alpha / ref_max(fabs(p - a.anchor[i]), a.floor_len);
+                    dg += wa;
+                    rh += wa * a.anchor[i];
+                }
+                a.diag[i] = ref_max(dg, 1e-12);
+                a.rhs[i] = rh;
+            }
+        }
+    }
 }
 
 // Kraftwerk2's adjustments after buildSystem: diag += move_weight and
@@ -428,10 +539,13 @@ int launch_build(ktg_ctx *c, const double *x, const double *y, double alpha, con
         k_scan_blocks<<<1, 1024, 0, c->stream>>>(c->block_sum, bpa, n, c->cap_nnz,
                                                  c->sys[0].row_ptr, c->sys[1].row_ptr,
                                                  c->nnz_dev, c->status);
+        KTG_CUDA(c, cudaMemsetAsync(c->heavy_rows, 0, sizeof(int32_t), c->stream));
         k_fill<R><<<2 * bpa, kBuildThreads, 0, c->stream>>>(nl, a[0], a[1], bpa, alpha,
                                                             c->row_cnt, c->block_sum, c->cap_nnz,
-                                                            c->status);
-        c->launches += 3;
+                                                            c->status, c->heavy_rows);
+        k_fill_heavy<R><<<8 * c->num_sms, kBuildThreads, 0, c->stream>>>(
+            nl, a[0], a[1], alpha, c->cap_nnz, c->status, c->heavy_rows);
+        c->launches += 4;
     } else {
         KTG_CUDA(c, cudaMemsetAsync(c->sys[0].row_ptr, 0, sizeof(int32_t), c->stream));
         KTG_CUDA(c, cudaMemsetAsync(c->sys[1].row_ptr, 0, sizeof(int32_t), c->stream));

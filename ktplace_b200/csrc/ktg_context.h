@@ -95,6 +95,7 @@ struct ktg_ctx {
     double *x = nullptr, *y = nullptr, *ax = nullptr, *ay = nullptr;  // [max(n, sys_cap_n)]
     int64_t stage_cap = 0;
     int32_t *row_cnt = nullptr;      // [2n]
+    int32_t *heavy_rows = nullptr;   // [1 + 2n] B2B rows filled one warp each: count, rows
     int64_t *block_sum = nullptr;    // [2 * blocks]
     int64_t *nnz_dev = nullptr;      // [2]
     double *partials = nullptr;      // reduction partials
