@@ -61,6 +61,10 @@ def parse():
                          "movable cells (scaled from the 211k design), timed, with its "
                          "algorithmic bytes per second; the capture workload of "
                          "profiles/k_pcg_beyond_l2.md")
+    ap.add_argument("--profile-spmv", type=int, default=0, metavar="CELLS",
+                    help="only the standalone SpMV (ktg_spmv) on the scaled design of "
+                         "--profile-pcg, timed, with its algorithmic bytes per second; the "
+                         "capture workload of profiles/k_spmv_beyond_l2.md")
     ap.add_argument("--config4", action="store_true",
                     help="only the solve comparison (FP64, FP32 with Jacobi / learned / "
                          "aggregation) on the 2.2M-cell design; prints one JSON line")
@@ -215,6 +219,13 @@ def pcg_bytes(n: int, m: int, iters: int) -> float:
     it = 12.0 * m + 4.0 * (n + 1) + 8.0 * n * 14
     start = 12.0 * m + 4.0 * (n + 1) + 8.0 * n * 6
     return start + iters * it
+
+
+def spmv_bytes(n: int, m: int) -> float:
+    """Algorithmic bytes of one A v: the CSR (4 B column + 8 B value per
+    entry, 4 B per row pointer), one 8-byte gather of v per entry, and v, diag
+    and the result per row."""
+    return 12.0 * m + 4.0 * (n + 1) + 8.0 * m + 24.0 * n
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel on this
@@ -867,6 +878,63 @@ def profile_pcg(cells: int) -> int:
     return 0
 
 
+def profile_spmv(cells: int) -> int:
+    """Standalone SpMV (ktg_spmv, SparseSystem::multiply's row sums) on the
+    scaled design of --profile-pcg: one B2B build, then 20 timed rounds of
+    A v on both axes with CUDA events; prints ms per SpMV and the
+    algorithmic bytes per second (spmv_bytes) against the measured HBM peak.
+    Inputs larger than L2 (from about 1M cells) need no flush."""
+    import math
+    import torch
+    from ktplace_b200 import netlist, synth
+    from ktplace_b200.gpu import Context
+    k = cells / 211_000
+    spec = synth.SynthSpec(num_movable=cells, num_nets=int(round(1.0474 * cells)),
+                           num_pads=int(round(1000 * math.sqrt(k))),
+                           num_rows=int(round(890 * math.sqrt(k))), utilization=0.6,
+                           num_macros=int(round(550 * k)), seed=7, name=f"synth{cells}")
+    raw = synth.generate(spec)
+    nl = netlist.flatten(raw)
+    x, y = synth.seed_positions(raw, nl.num_movable, 107)
+    ax, ay = synth.seed_positions(raw, nl.num_movable, 207)
+    fx, fy = nl.floors()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    ctx = Context(0)
+    ctx.upload_netlist(nl)
+    ctx.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        dx, dy = torch.tensor(x, device=dev), torch.tensor(y, device=dev)
+        dax, day = torch.tensor(ax, device=dev), torch.tensor(ay, device=dev)
+        ox, oy = torch.empty_like(dx), torch.empty_like(dy)
+        ctx.build_b2b_dev(dx, dy, ALPHA, dax, day, fx, fy)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    rounds = 20
+    with torch.cuda.stream(stream):
+        for _ in range(3):  # warm-up
+            ctx.spmv_dev(0, dx, ox)
+            ctx.spmv_dev(1, dy, oy)
+        e0.record(stream)
+        for _ in range(rounds):
+            ctx.spmv_dev(0, dx, ox)
+            ctx.spmv_dev(1, dy, oy)
+        e1.record(stream)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / (2 * rounds)
+    n = nl.num_movable
+    _, mx = ctx.system_info(0)
+    _, my = ctx.system_info(1)
+    byts = (spmv_bytes(n, mx) + spmv_bytes(n, my)) / 2
+    peak, kind = measured_peak()
+    gbs = byts / (t * 1e-3) / 1e9
+    print(json.dumps({"cells": n, "nnz": [mx, my], "ms_per_spmv": t, "algorithmic_bytes": byts,
+                      "achieved_gbs": gbs, "peak_gbs": peak, "peak_kind": kind,
+                      "frac": gbs / peak}))
+    ctx.close()
+    return 0
+
+
 def run_config4(args) -> int:
     """The solve comparison of `solve_variants` on the 2.2M-cell design (2.25M
     nets, 8,000 macros; seed positions and anchors), the configuration the
@@ -908,6 +976,8 @@ def main():
     args = parse()
     if args.profile_pcg:
         return profile_pcg(args.profile_pcg)
+    if args.profile_spmv:
+        return profile_spmv(args.profile_spmv)
     if args.config4:
         return run_config4(args)
     if args.profile_once:

@@ -232,6 +232,14 @@ int ktg_solve_mixed(ktg_ctx *ctx, double *x, double *y, double tol, double inner
                     int64_t max_inner, int32_t max_outer, ktg_mixed_info *info,
                     double *hist_x, double *hist_y, int64_t hist_cap);
 
+/* out = A in for the system of `axis` (0: x, 1: y) from the last build:
+ * SparseSystem::multiply (simpl_lss.h:49-57). Each row sum starts from
+ * diag * in and adds the row's entries in storage order, so out is
+ * bit-identical to the reference's. Pointer mode applies to in and out
+ * (n doubles each); in device mode the call is asynchronous on the
+ * context's stream. */
+int ktg_spmv(ktg_ctx *ctx, int32_t axis, const double *in, double *out);
+
 /* ---- HPWL and density ---------------------------------------------------- */
 
 /* simplPlacer::Impl::getHpwl (simpl_placer.cc:256-275). */

@@ -85,6 +85,7 @@ SIGNATURES = [
     ("ktg_download_bound_pins", ctypes.c_int, [_vp, ctypes.c_int, _u32p, _u32p]),
     ("ktg_upload_system", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64, _i64p, _i32p,
                                          _f64p, _f64p, _f64p]),
+    ("ktg_spmv", ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp]),
     ("ktg_solve", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int64, _vp, _vp, _vp,
                                  ctypes.c_int64]),
     ("ktg_solve_mixed", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double,

@@ -848,6 +848,23 @@ int ktg_hpwl(ktg_ctx *c, const double *x, const double *y, double *out) {
     return KTG_OK;
 }
 
+int ktg_spmv(ktg_ctx *c, int32_t axis, const double *in, double *out) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no system built");
+    if (axis != 0 && axis != 1) return set_error(c, KTG_ERR_ARG, "axis must be 0 or 1");
+    if (c->sys_n > 0 && (!in || !out)) return set_error(c, KTG_ERR_ARG, "null vector");
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int64_t n = c->sys_n;
+    if (c->ptr_mode == KTG_PTR_DEVICE) return ktg::launch_spmv(c, axis, in, out);
+    if ((rc = upload(c, c->x, in, n))) return rc;
+    if ((rc = ktg::launch_spmv(c, axis, c->x, c->y))) return rc;
+    if (n > 0)
+        KTG_CUDA(c, cudaMemcpyAsync(out, c->y, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    return sync(c);
+}
+
 int ktg_set_grid(ktg_ctx *c, const ktg_grid_view *g) {
     if (!c || !g) return KTG_ERR_ARG;
     if (g->nx <= 0 || g->ny <= 0 || !g->avail || !(g->dx > 0.0) || !(g->dy > 0.0))

@@ -139,6 +139,7 @@ namespace ktg {
 int launch_build_b2b(ktg_ctx *ctx, const double *x, const double *y, double alpha,
                      const double *ax, const double *ay, double floor_x, double floor_y);
 int launch_hpwl(ktg_ctx *ctx, const double *x, const double *y, double *out_dev);
+int launch_spmv(ktg_ctx *ctx, int axis, const double *in, double *out);
 int launch_build_kraftwerk2(ktg_ctx *ctx, const double *x, const double *y, bool with_rhs,
                             double floor_x, double floor_y);
 int launch_kraftwerk2_adjust(ktg_ctx *ctx, const double *move_weight, const double *toward_x,

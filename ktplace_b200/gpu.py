@@ -275,6 +275,19 @@ class Context:
         self._check(self.lib.ktg_hpwl(self.h, _ptr(x), _ptr(y), ctypes.byref(out)))
         return float(out.value)
 
+    def spmv(self, axis: int, v) -> np.ndarray:
+        """A v for the system of `axis` from the last build (host mode):
+        SparseSystem::multiply's row sums, bit for bit."""
+        self._set_mode(_lib.KTG_PTR_HOST)
+        v = _c(v, np.float64)
+        out = np.empty_like(v)
+        self._check(self.lib.ktg_spmv(self.h, axis, _ptr(v), _ptr(out)))
+        return out
+
+    def spmv_dev(self, axis: int, v, out):
+        self._set_mode(_lib.KTG_PTR_DEVICE)
+        self._check(self.lib.ktg_spmv(self.h, axis, _tptr(v), _tptr(out)))
+
     def hpwl_dev(self, x, y, out):
         self._set_mode(_lib.KTG_PTR_DEVICE)
         self._check(self.lib.ktg_hpwl(self.h, _tptr(x), _tptr(y), _tptr(out)))

@@ -114,6 +114,30 @@ def test_pcg_forms_and_spmv_shapes(name, form, gpu_ctx):
 
 
 @pytest.mark.parametrize("name", list(CASES))
+def test_spmv_bit_exact(name, gpu_ctx):
+    """ktg_spmv against SparseSystem::multiply's order (simpl_lss.h:49-57):
+    diag * v first, then the row's entries in storage order."""
+    raw, nl, x, y, ax, ay, alpha, _ = build_case(name)
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, alpha, ax if alpha > 0 else None, ay if alpha > 0 else None, fx, fy)
+    rng = np.random.default_rng(5)
+    for axis in (0, 1):
+        s = gpu_ctx.system(axis)
+        n = len(s["diag"])
+        v = rng.standard_normal(n)
+        rp = s["row_ptr"].astype(np.int64)
+        col, val = s["col"].astype(np.int64), s["val"]
+        want = s["diag"] * v
+        lens = np.diff(rp)
+        for k in range(int(lens.max()) if n else 0):
+            rows = np.nonzero(lens > k)[0]
+            e = rp[rows] + k
+            want[rows] = want[rows] + val[e] * v[col[e]]
+        assert np.array_equal(gpu_ctx.spmv(axis, v), want), (name, axis)
+
+
+@pytest.mark.parametrize("name", list(CASES))
 def test_hpwl_and_density(name, gpu_ctx):
     from ktplace_b200 import grid as kgrid
     g, meta = gold(name)
