@@ -19,10 +19,13 @@
 // SpMV's gathers in flight (a block with 30 KB more shared memory solved
 // the 211k system in 8.6 ms instead of 5.8).
 // SpMV runs in one of three shapes (option "pcg_lanes"): warp tiles (the
-// default: a warp streams the nonzeros of 32 consecutive rows with coalesced
-// loads and each lane adds its row's products in storage order), one thread
+// default: each warp takes a range of the block's rows balanced by
+// nonzeros and streams their nonzeros 32 rows at a time with coalesced
+// loads, each lane adding its row's products in storage order), one thread
 // per row (same row sums, four gathers in flight), or four lanes per row.
-// The first two give bit-identical solves.
+// The first two give the same row sums; their solves are bit-identical in
+// form 2 and agree to rounding in the others (dot-product partials group
+// rows by thread differently).
 // Scalars (alpha, beta, residuals, live flags) are recomputed identically by
 // every block from the same partials in a fixed order, so all blocks take the
 // same branch and the result is identical from run to run.
