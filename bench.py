@@ -59,18 +59,17 @@ def parse():
     ap.add_argument("--profile-pcg", type=int, default=0, metavar="CELLS",
                     help="only one B2B build and FP64 solve of a synthetic design with CELLS "
                          "movable cells (scaled from the 211k design), timed, with its "
-                         "algorithmic bytes per second; the capture workload of "
-                         "profiles/k_pcg_beyond_l2.md")
+                         "algorithmic bytes per second (the PCG capture workload past L2)")
     ap.add_argument("--profile-spmv", type=int, default=0, metavar="CELLS",
                     help="only the standalone SpMV (ktg_spmv) on the scaled design of "
-                         "--profile-pcg, timed, with its algorithmic bytes per second; the "
-                         "capture workload of profiles/k_spmv_beyond_l2.md")
+                         "--profile-pcg, timed, with its algorithmic bytes per second (the "
+                         "SpMV capture workload past L2)")
     ap.add_argument("--config4", action="store_true",
                     help="only the solve comparison (FP64, FP32 with Jacobi / learned / "
                          "aggregation) on the 2.2M-cell design; prints one JSON line")
     ap.add_argument("--profile-lal", action="store_true",
                     help="run only the look-ahead legalization of the step's solved positions "
-                         "twice (the capture workload of profiles/lal_*)")
+                         "twice (the legalizer's capture workload)")
     ap.add_argument("--profile-agg", action="store_true",
                     help="build the 211k systems twice, each followed by a mixed solve with "
                          "the aggregation preconditioner (set-up included), for ncu captures")
@@ -168,7 +167,8 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        import tempfile
+        self.path = os.path.join(tempfile.mkdtemp(prefix="ktg_clocks_"), f"rank{index}.csv")
 
     def start(self):
         try:
@@ -229,7 +229,8 @@ def spmv_bytes(n: int, m: int) -> float:
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel on this
-# workload, from the ncu capture summarised in profiles/k_pcg_synth211k.md.
+# workload, from an ncu capture of bench.py --profile-once (dram__bytes_read.sum +
+# dram__bytes_write.sum of the k_pcg launch).
 NCU_TRAFFIC_BYTES = {"k_pcg": 111.045376e6 + 41.966848e6}
 
 
@@ -417,7 +418,7 @@ def run_ours(args):
                          "note": "working set is L2-resident: traffic << algorithmic bytes",
                          "limiter": "L1TEX data pipe: 56% of peak over the whole solve in the ncu "
                                     "capture (random 8-byte gathers, one LSU wavefront each); "
-                                    "L2 39%, DRAM 0.2% (profiles/k_pcg_synth211k.md)"},
+                                    "L2 39%, DRAM 0.2% (ncu of bench.py --profile-once)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -756,7 +757,7 @@ def run_batch_leg(torch, dev, stream, steps: int):
 
 
 def profile_once():
-    """The capture workload of profiles/*_synth211k.md: one build, one FP64
+    """The capture workload of the 211k kernel profiles: one build, one FP64
     and one mixed solve, HPWL and the 512x512 density map."""
     from ktplace_b200.gpu import Context
     from ktplace_b200 import grid as kgrid
@@ -777,7 +778,7 @@ def profile_once():
 
 
 def profile_agg():
-    """The capture workload of profiles/agg_*_synth211k.md: two B2B builds of
+    """The capture workload of the aggregation profiles: two B2B builds of
     the 211k-cell workload, each followed by a mixed solve with the
     aggregation preconditioner (which rebuilds the aggregates)."""
     from ktplace_b200.gpu import Context
@@ -795,7 +796,7 @@ def profile_agg():
 
 
 def profile_lal():
-    """The capture workload of profiles/lal_*_synth211k.md: one B2B build and
+    """The capture workload of the legalizer profiles: one B2B build and
     FP64 PCG solve of the 211k-cell workload from its seed positions, then
     the look-ahead legalization of the solved positions, twice."""
     from ktplace_b200 import grid

@@ -237,7 +237,8 @@ int ktg_solve_mixed(ktg_ctx *ctx, double *x, double *y, double tol, double inner
  * diag * in and adds the row's entries in storage order, so out is
  * bit-identical to the reference's. Pointer mode applies to in and out
  * (n doubles each); in device mode the call is asynchronous on the
- * context's stream. */
+ * context's stream, and in and out must not overlap (other rows gather `in`
+ * while `out` is written): an overlap returns KTG_ERR_ARG. */
 int ktg_spmv(ktg_ctx *ctx, int32_t axis, const double *in, double *out);
 
 /* ---- HPWL and density ---------------------------------------------------- */
@@ -501,9 +502,12 @@ int ktg_selftest_wait_timeout(ktg_ctx *ctx, int64_t timeout_ns, int *status_out)
  * 128 KiB) is a static device array that every GPU which loads this library
  * holds until the process exits. Limits and caveats:
  *   - num_nets above KTG_NOALLOC_HPWL_MAX_NETS returns KTG_ERR_RANGE;
- *   - the first call with a given device current looks up that device's
- *     scratch address (cudaGetSymbolAddress), so make that first call before
- *     any stream capture begins;
+ *   - the first call made with a given CUDA context current looks up the
+ *     scratch array's address in that context (cudaGetSymbolAddress) and
+ *     keeps it under the context's id, so make that first call before any
+ *     stream capture begins; a context created later (another driver
+ *     context, or the primary one again after cudaDeviceReset) gets its own
+ *     lookup, never a stale address;
  *   - all calls share the one scratch array: calls that overlap on the GPU
  *     (different streams, or host threads without ordering) race and give
  *     wrong sums. Serialise them on one stream.

@@ -853,9 +853,13 @@ int ktg_spmv(ktg_ctx *c, int32_t axis, const double *in, double *out) {
     if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no system built");
     if (axis != 0 && axis != 1) return set_error(c, KTG_ERR_ARG, "axis must be 0 or 1");
     if (c->sys_n > 0 && (!in || !out)) return set_error(c, KTG_ERR_ARG, "null vector");
+    const int64_t n = c->sys_n;
+    // other rows gather `in` while `out` is written: the two may not overlap
+    // on the device (host buffers are staged separately, so they may)
+    if (c->ptr_mode == KTG_PTR_DEVICE && n > 0 && in < out + n && out < in + n)
+        return set_error(c, KTG_ERR_ARG, "ktg_spmv: in and out overlap");
     int rc = set_device(c);
     if (rc) return rc;
-    const int64_t n = c->sys_n;
     if (c->ptr_mode == KTG_PTR_DEVICE) return ktg::launch_spmv(c, axis, in, out);
     if ((rc = upload(c, c->x, in, n))) return rc;
     if ((rc = ktg::launch_spmv(c, axis, c->x, c->y))) return rc;

@@ -22,6 +22,10 @@
 
 namespace ktg {
 
+// Bits of ktg_ctx::attr_bits.
+constexpr unsigned kAttrOccupancy = 1u;  // k_occ_accum<true> opt-in shared memory
+constexpr unsigned kAttrMixed = 2u;      // k_pcg_mixed_cg opt-in shared memory
+
 struct AggState;  // aggregation preconditioner buffers (ktg_agg.cu)
 struct LalState;  // free space and scratch of the look-ahead legalizer (ktg_lal.cu)
 
@@ -60,6 +64,14 @@ struct ktg_ctx {
     double *exact_cpart = nullptr;  // form 2: chunk sums [6 * chunks]
     int64_t exact_prod_cap = 0, exact_cpart_cap = 0;
     int mixed_form = 1; // mixed solve: 0 textbook (global vectors), 1 Chronopoulos-Gear
+    // Per-device launch set-up, done once per context (a context owns one
+    // device): opt-in shared memory attributes set (kAttr* bits and the PCG
+    // variants' bits), the PCG's shared-memory budgets and ktg_spmv's blocks
+    // per SM.
+    unsigned attr_bits = 0;
+    unsigned pcg_attr_bits = 0;
+    size_t pcg_smem_budget[4][3] = {};
+    int spmv_per_sm = 0;
 
     // netlist sizes
     bool have_netlist = false;

@@ -144,13 +144,12 @@ int launch_occupancy(ktg_ctx *c, const double *x, const double *y, double *occ_d
             // Enough blocks to cover the SMs, each privatising the whole map.
             blocks = std::min(blocks, c->num_sms);
             const size_t smem = sizeof(unsigned long long) * static_cast<size_t>(bins);
-            static bool attr_set = false;
-            if (!attr_set) {
+            if (!(c->attr_bits & kAttrOccupancy)) {  // per device: once per context
                 KTG_CUDA(c, cudaFuncSetAttribute(k_occ_accum<true>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  static_cast<int>(sizeof(unsigned long long) *
                                                                   kSmemBins)));
-                attr_set = true;
+                c->attr_bits |= kAttrOccupancy;
             }
             k_occ_accum<true><<<blocks, kOccThreads, smem, c->stream>>>(
                 x, y, c->width, c->height, c->area, n, g, c->occ_fx);

@@ -32,9 +32,28 @@ constexpr int kTicketSlots = 32;
 
 static __device__ __align__(256) double g_hpwl_scratch[kTicketSlots + kMaxBlocks];
 
-constexpr int kMaxDevices = 64;
+// Looked-up scratch addresses, one per CUDA context. A context is named by
+// its process-unique id (cuCtxGetId), never by its handle or by the device
+// ordinal alone: after a context is destroyed (cudaDeviceReset, or a driver
+// context the caller made current and later destroyed) a new context may get
+// the same handle and the same ordinal, but this library's module, and so
+// the scratch array, is loaded into it afresh at a possibly different
+// address. The ids of destroyed contexts are never reused, so a stale entry
+// is never matched.
+struct ScratchEntry {
+    unsigned long long ctx_id;
+    double *addr;
+};
+constexpr int kCacheSize = 64;
 std::mutex g_setup_mutex;
-double *g_scratch_addr[kMaxDevices] = {};
+ScratchEntry g_cache[kCacheSize] = {};
+int g_cache_next = 0;
+
+typedef int (*CtxGetCurrentFn)(void **);
+typedef int (*CtxGetIdFn)(void *, unsigned long long *);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+bool g_driver_looked_up = false;
 
 __global__ void __launch_bounds__(kThreads)
     k_hpwl_noalloc(const int32_t *__restrict__ net_start, const int32_t *__restrict__ pin_cell,
@@ -75,20 +94,47 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-// Address of this device's scratch array, looked up on the first call made
-// with that device current.
-int scratch_for_current_device(double **addr) {
+// Address of the scratch array in the current context, looked up with
+// cudaGetSymbolAddress on the first call made with that context current and
+// cached under the context's id. When no context is current yet (the
+// runtime creates the device's primary context during the lookup) or the
+// driver cannot name contexts (no cuCtxGetId), nothing is cached and the
+// address is looked up again on the next call.
+int scratch_for_current_context(double **addr) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return KTG_ERR_CUDA;
-    if (dev < 0 || dev >= kMaxDevices) return KTG_ERR_RANGE;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (g_scratch_addr[dev] == nullptr) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_hpwl_scratch) != cudaSuccess || p == nullptr)
-            return KTG_ERR_CUDA;
-        g_scratch_addr[dev] = static_cast<double *>(p);
+    if (!g_driver_looked_up) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_id = reinterpret_cast<CtxGetIdFn>(f);
+        g_driver_looked_up = true;
     }
-    *addr = g_scratch_addr[dev];
+    unsigned long long id = 0;
+    void *ctx = nullptr;
+    const bool named = g_ctx_current && g_ctx_id && g_ctx_current(&ctx) == 0 && ctx &&
+                       g_ctx_id(ctx, &id) == 0;
+    if (named) {
+        for (const ScratchEntry &e : g_cache)
+            if (e.addr && e.ctx_id == id) {
+                *addr = e.addr;
+                return KTG_OK;
+            }
+    }
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_hpwl_scratch) != cudaSuccess || p == nullptr)
+        return KTG_ERR_CUDA;
+    if (named) {
+        g_cache[g_cache_next] = ScratchEntry{id, static_cast<double *>(p)};
+        g_cache_next = (g_cache_next + 1) % kCacheSize;
+    }
+    *addr = static_cast<double *>(p);
     return KTG_OK;
 }
 
@@ -105,7 +151,7 @@ extern "C" int ktg_hpwl_noalloc(const int32_t *net_start, const int32_t *pin_cel
                          !fixed_y || !x || !y))
         return KTG_ERR_ARG;
     double *scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
+    int rc = scratch_for_current_context(&scratch);
     if (rc != KTG_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // The ticket must start at zero; the partials are always written before

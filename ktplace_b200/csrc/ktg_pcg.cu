@@ -1014,8 +1014,7 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     const int form = c->pcg_form >= 0 ? c->pcg_form : pcg_form_default;
     // Dynamic shared memory for the vector slices: what the block may opt in
     // to, less the kernel's static arrays, capped at kPcgSmemBytes.
-    static size_t budget[4][3] = {};
-    size_t &bud = budget[form][lanes_index(lanes)];
+    size_t &bud = c->pcg_smem_budget[form][lanes_index(lanes)];  // per context (one device)
     if (bud == 0) {
         int optin = 0;
         KTG_CUDA(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
@@ -1035,12 +1034,11 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     const bool use_smem = smem <= bud;
     const Variant v = pick_variant(form, use_smem, lanes);
     const size_t dyn = use_smem ? smem : tile;
-    static bool attr_set[4][2][3] = {};
-    bool &done = attr_set[form][use_smem][lanes_index(lanes)];
-    if (!done) {
+    const unsigned bit = 1u << ((form * 2 + (use_smem ? 1 : 0)) * 3 + lanes_index(lanes));
+    if (!(c->pcg_attr_bits & bit)) {  // per device: once per context
         KTG_CUDA(c, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bud)));
-        done = true;
+        c->pcg_attr_bits |= bit;
     }
     int per_sm = 0;
     KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, kPcgThreads, dyn));

@@ -808,13 +808,12 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
                           : learned ? k_pcg_mixed_cg<kPreLearned>
                                     : k_pcg_mixed_cg<kPreJacobi>;
     const size_t dyn = !cg_form ? 0 : in_smem ? slice + tile : tile;
-    static bool attr_set = false;
-    if (!attr_set) {
+    if (!(c->attr_bits & kAttrMixed)) {  // per device: once per context
         for (void (*f)(MixArgs) : {k_pcg_mixed_cg<kPreJacobi>, k_pcg_mixed_cg<kPreLearned>,
                                    k_pcg_mixed_cg<kPreAgg>})
             KTG_CUDA(c, cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              kMixSmemBytes));
-        attr_set = true;
+        c->attr_bits |= kAttrMixed;
     }
     int per_sm = 0;
     KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMixThreads, dyn));

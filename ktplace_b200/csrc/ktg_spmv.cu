@@ -56,7 +56,7 @@ int launch_spmv(ktg_ctx *c, int axis, const double *in, double *out) {
     const AxisSystem &s = c->sys[axis];
     // one even wave: as many blocks as fit on the GPU at once, each at least
     // kSpmvMinRows rows (several waves beyond that)
-    static int per_sm = 0;
+    int &per_sm = c->spmv_per_sm;  // once per context (one device)
     if (per_sm == 0) {
         KTG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv, kSpmvThreads,
                                                                   0));

@@ -8,7 +8,7 @@
 //
 // (called from simplPlacer::Impl::lookAheadLegalize, simpl_placer.cc:299-310),
 // and runs it on a B200. Link this object instead of simpl_lal.o, next to
-// simpl_lss_b200.o (see INTEGRATION.md).
+// simpl_lss_b200.o.
 //
 // The legalizer keeps its own GPU context (device $KTPLACE_B200_DEVICE,
 // default 0) holding the cells' sizes as a netlist without nets, the bin grid

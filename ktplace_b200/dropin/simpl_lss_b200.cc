@@ -8,13 +8,13 @@
 //   LinearSystems::buildStar (reference: simpl_lss.cc:116-201) -> ktg_build_star
 //   solveBothAxes            (reference: simpl_lss.cc:203-290) -> ktg_solve
 //
-// Link this object instead of simpl_lss.o (see INTEGRATION.md). One GPU
+// Link this object instead of simpl_lss.o. One GPU
 // context per process (device $KTPLACE_B200_DEVICE, default 0) holds the
 // netlist, uploaded the first time a Netlist is seen and again whenever a
 // different one is. Errors from the GPU are fatal through ktlog, as the
 // reference treats its own unrecoverable states.
 //
-// Contract differences, all documented in INTEGRATION.md:
+// Contract differences from the reference's simpl_lss.cc:
 //   * with $KTPLACE_B200_HOST_CSR=0 buildB2B fills only diag and rhs on the
 //     host and leaves rowPtr/col/val empty; solveBothAxes then uses the device
 //     copy. By default the whole CSR is copied back, as the reference fills it.
@@ -112,7 +112,7 @@ void ensureNetlist(const Netlist &nl) {
         pinQ[e] = static_cast<int32_t>(nl.pinsOfCell[e].pin);
     }
     // Cell sizes are not part of Netlist; the density entry points take them
-    // from the placer's Design. Unit sizes keep the
+    // from the placer's Design (simpl_dm.h), not from here. Unit sizes keep the
     // upload valid for the assembly and solve.
     std::vector<double> ones(std::max<std::size_t>(n, 1), 1.0);
     ktg_netlist_view view{static_cast<int64_t>(V), static_cast<int64_t>(n),

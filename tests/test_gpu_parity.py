@@ -113,6 +113,52 @@ def test_pcg_forms_and_spmv_shapes(name, form, gpu_ctx):
             assert np.array_equal(got[lanes]["x"], g["x"]) and np.array_equal(got[lanes]["y"], g["y"])
 
 
+def _multiply_order(s, v):
+    """SparseSystem::multiply's order (simpl_lss.h:49-57) in numpy: diag * v
+    first, then each row's entries in storage order."""
+    rp = s["row_ptr"].astype(np.int64)
+    col, val = s["col"].astype(np.int64), s["val"]
+    want = s["diag"] * v
+    lens = np.diff(rp)
+    for k in range(int(lens.max()) if len(lens) else 0):
+        rows = np.nonzero(lens > k)[0]
+        e = rp[rows] + k
+        want[rows] = want[rows] + val[e] * v[col[e]]
+    return want
+
+
+@pytest.mark.parametrize("cells", [12_000, 1_000_000])
+def test_spmv_device_mode_bit_exact(cells, gpu_ctx):
+    """ktg_spmv on device pointers: one wave of blocks at 12k rows, more
+    blocks than SMs at 1M rows; bit-identical to the reference's row sums and
+    to the host-pointer call. Overlapping in and out are refused."""
+    import torch
+    from ktplace_b200 import synth, netlist
+    spec = synth.spec_small(0) if cells == 12_000 else synth.SynthSpec(
+        num_movable=cells, num_nets=int(cells * 1.05), num_pads=1_200, num_rows=1_900,
+        utilization=0.6, num_macros=600, seed=9, name="synth1m")
+    raw = synth.generate(spec)
+    nl = netlist.flatten(raw)
+    x, y = synth.seed_positions(raw, nl.num_movable, 21)
+    ax, ay = synth.seed_positions(raw, nl.num_movable, 22)
+    fx, fy = nl.floors()
+    gpu_ctx.upload_netlist(nl)
+    gpu_ctx.build_b2b(x, y, 0.2, ax, ay, fx, fy)
+    rng = np.random.default_rng(6)
+    for axis in (0, 1):
+        s = gpu_ctx.system(axis)
+        v = rng.standard_normal(len(s["diag"]))
+        want = _multiply_order(s, v)
+        dv = torch.tensor(v, device="cuda:0")
+        dout = torch.empty_like(dv)
+        gpu_ctx.spmv_dev(axis, dv, dout)
+        torch.cuda.synchronize()
+        assert np.array_equal(dout.cpu().numpy(), want), (cells, axis)
+        assert np.array_equal(gpu_ctx.spmv(axis, v), want), (cells, axis)
+        with pytest.raises(Exception):
+            gpu_ctx.spmv_dev(axis, dv, dv)
+
+
 @pytest.mark.parametrize("name", list(CASES))
 def test_spmv_bit_exact(name, gpu_ctx):
     """ktg_spmv against SparseSystem::multiply's order (simpl_lss.h:49-57):
@@ -124,17 +170,8 @@ def test_spmv_bit_exact(name, gpu_ctx):
     rng = np.random.default_rng(5)
     for axis in (0, 1):
         s = gpu_ctx.system(axis)
-        n = len(s["diag"])
-        v = rng.standard_normal(n)
-        rp = s["row_ptr"].astype(np.int64)
-        col, val = s["col"].astype(np.int64), s["val"]
-        want = s["diag"] * v
-        lens = np.diff(rp)
-        for k in range(int(lens.max()) if n else 0):
-            rows = np.nonzero(lens > k)[0]
-            e = rp[rows] + k
-            want[rows] = want[rows] + val[e] * v[col[e]]
-        assert np.array_equal(gpu_ctx.spmv(axis, v), want), (name, axis)
+        v = rng.standard_normal(len(s["diag"]))
+        assert np.array_equal(gpu_ctx.spmv(axis, v), _multiply_order(s, v)), (name, axis)
 
 
 @pytest.mark.parametrize("name", list(CASES))
