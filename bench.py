@@ -73,6 +73,11 @@ def parse():
     ap.add_argument("--profile-agg", action="store_true",
                     help="build the 211k systems twice, each followed by a mixed solve with "
                          "the aggregation preconditioner (set-up included), for ncu captures")
+    ap.add_argument("--simpl-report", type=int, default=0, metavar="ITERS",
+                    help="only the mixed-precision study on the systems of ITERS SimPL global "
+                         "iterations of the 211k design (prints one JSON line)")
+    ap.add_argument("--no-simpl-report", action="store_true",
+                    help="skip the 30-iteration SimPL study in the default run")
     ap.add_argument("--profile-once", action="store_true",
                     help="run the workload once (build, FP64 and mixed solves, HPWL, "
                          "density) for an ncu capture; prints no bench line")
@@ -368,6 +373,10 @@ def run_ours(args):
         lal_line = lal_leg(torch, dev, stream, nl, wx.cpu().numpy(), wy.cpu().numpy(),
                            max(3, args.steps // 10), cpu=not args.no_cpu_baseline)
 
+    simpl_line = None
+    if world == 1 and not args.no_simpl_report:
+        simpl_line = simpl_report(torch, dev, stream, nl, x, y, 30)
+
     batch_line = None
     if world == 1 and not args.no_batch:
         batch_line = run_batch_leg(torch, dev, stream, max(3, args.steps // 10))
@@ -423,6 +432,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
+            "simpl_report": simpl_line,
             "batch": batch_line,
             "kraftwerk2": kw2_line,
             "bookshelf": bs_line,
@@ -457,12 +467,15 @@ def solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, in
         learned.load(weights)
     out = {}
     hpwl_ref = None
-    for name, pre in (("fp64_jacobi", None), ("fp32_jacobi", 0), ("fp32_learned", 1),
-                      ("fp32_aggregation", 2)):
+    for name, pre, coarse in (("fp64_jacobi", None, 0), ("fp32_jacobi", 0, 0),
+                              ("fp32_learned", 1, 0), ("fp32_aggregation", 2, 0),
+                              ("fp32_aggregation_coarse_const", 2, 1),
+                              ("fp32_aggregation_coarse_coupling", 2, 2)):
         if pre == 1 and learned is None:
             continue
         if pre is not None:
             ctx.set_option("precond", pre)
+            ctx.set_option("coarse", coarse)
         ms = []
         host_ms = 0.0
         for k in range(reps + 1):
@@ -505,12 +518,119 @@ def solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, in
         row["hpwl_rel_vs_fp64"] = (h - hpwl_ref) / hpwl_ref if hpwl_ref else 0.0
         out[name] = row
     ctx.set_option("precond", 0)
+    ctx.set_option("coarse", 0)
     if learned is not None:
         learned.close()
     base = out["fp64_jacobi"]["ms"]
     for row in out.values():
         row["speedup_vs_fp64"] = base / row["ms"]
     return out
+
+
+SIMPL_VARIANTS = (("fp64_jacobi", None, 0), ("fp32_jacobi", 0, 0), ("fp32_aggregation", 2, 0),
+                  ("fp32_aggregation_coarse_const", 2, 1),
+                  ("fp32_aggregation_coarse_coupling", 2, 2))
+
+
+def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: int = 5,
+                 variants=SIMPL_VARIANTS, learned=None) -> dict:
+    """The mixed-precision study on real SimPL systems: SimPL's B2B initial
+    rounds, then `iters` global iterations (simpl_placer.cc:463-539) on the
+    GPU path with the anchors at the look-ahead-legalized positions (ktg_lal)
+    and the anchor weight rising linearly from 0.01 to 1.0. Every iteration's
+    x+y systems are solved by each variant from the same warm start to the
+    same true residual (rtol 1e-6): FP64 Jacobi-PCG (the drop-in), and FP32
+    PCG in FP64 refinement with Jacobi, aggregation block Jacobi, and
+    aggregation with a coarse vector (constant, coupling share, learned).
+    Per variant and iteration: device ms (CUDA events, L2 flushed, set-up
+    such as the aggregates included, the B2B build excluded), iterations,
+    the true FP64 relative residual, the solution's difference from the FP64
+    solve and its HPWL relative to FP64's. The loop continues from the FP64
+    solution, so every variant sees the same systems."""
+    from ktplace_b200 import grid as kgrid
+    from ktplace_b200 import simpl
+    from ktplace_b200._lib import MixedInfo, SolveInfo
+    from ktplace_b200.gpu import Context
+    ctx = Context(dev.index or 0)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_netlist(nl)
+    g = kgrid.build_grid(nl, kgrid.default_bins_per_axis(nl.num_movable), 1.0)
+    loop = simpl.GlobalLoop(ctx, nl, g, kgrid.build_free_space(nl), tol=TOL, max_iter=MAX_ITER)
+    with torch.cuda.stream(stream):
+        dx = torch.zeros(nl.num_movable, dtype=torch.float64, device=dev)
+        dy = torch.zeros_like(dx)
+        info = torch.zeros(ctypes.sizeof(SolveInfo), dtype=torch.uint8, device=dev)
+        minfo = torch.zeros(ctypes.sizeof(MixedInfo), dtype=torch.uint8, device=dev)
+        hp = torch.zeros(1, dtype=torch.float64, device=dev)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    x, y = loop.initial_rounds(x0, y0, init_rounds)
+    rows = []
+    fx, fy = loop.fx, loop.fy
+    for st in loop.iterations(x, y, iters):
+        row = {"it": st.it, "alpha": st.alpha}
+        ref = None
+        for name, pre, coarse in variants:
+            if coarse == 3 and learned is None:
+                continue
+            ctx.build_b2b(st.x, st.y, st.alpha, st.ux, st.uy, fx, fy)  # fresh systems
+            with torch.cuda.stream(stream):
+                dx.copy_(torch.from_numpy(st.x))
+                dy.copy_(torch.from_numpy(st.y))
+                flush.zero_()
+            torch.cuda.synchronize(dev)
+            if pre is not None:
+                ctx.set_option("precond", pre)
+                ctx.set_option("coarse", coarse)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                if coarse == 3:
+                    learned.prepare_coarse_dev(ctx)
+                if pre is None:
+                    ctx.solve_dev(dx, dy, TOL, MAX_ITER, info)
+                else:
+                    ctx.solve_mixed_dev(dx, dy, TOL, MIXED_INNER_TOL, MAX_ITER, 50, minfo)
+                e1.record(stream)
+                ctx.hpwl_dev(dx, dy, hp)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            ctx.set_option("precond", 0)
+            ctx.set_option("coarse", 0)
+            sol = np.concatenate([dx.cpu().numpy(), dy.cpu().numpy()])
+            h = float(hp.item())
+            if pre is None:
+                inf = SolveInfo.from_buffer_copy(bytes(info.cpu().numpy()))
+                ref = (sol, h)
+                row[name] = {"ms": ms, "iters": [int(inf.iters_x), int(inf.iters_y)],
+                             "resid": [inf.resid_x, inf.resid_y], "hpwl": h}
+            else:
+                mi = MixedInfo.from_buffer_copy(bytes(minfo.cpu().numpy()))
+                row[name] = {"ms": ms, "iters": [int(mi.inner_x), int(mi.inner_y)],
+                             "outer": [int(mi.outer_x), int(mi.outer_y)],
+                             "true_resid": [mi.resid_x, mi.resid_y],
+                             "fp64_fallback_iters": [int(mi.fp64_iters_x), int(mi.fp64_iters_y)],
+                             "sol_rel_vs_fp64": float(np.linalg.norm(sol - ref[0]) /
+                                                      np.linalg.norm(ref[0])),
+                             "hpwl_rel_vs_fp64": (h - ref[1]) / ref[1]}
+        rows.append(row)
+    ctx.close()
+    names = [v[0] for v in variants if v[0] in rows[0]]
+    summary = {}
+    base = sum(r["fp64_jacobi"]["ms"] for r in rows)
+    for nm in names:
+        tot = sum(r[nm]["ms"] for r in rows)
+        d = {"ms_per_iter": tot / len(rows), "speedup_vs_fp64": base / tot,
+             "iters_mean": float(np.mean([sum(r[nm]["iters"]) / 2 for r in rows]))}
+        if nm != "fp64_jacobi":
+            d["max_true_resid"] = max(max(r[nm]["true_resid"]) for r in rows)
+            d["max_abs_hpwl_rel_vs_fp64"] = max(abs(r[nm]["hpwl_rel_vs_fp64"]) for r in rows)
+            d["max_sol_rel_vs_fp64"] = max(r[nm]["sol_rel_vs_fp64"] for r in rows)
+        summary[nm] = d
+    return {"workload": f"{iters} SimPL global iterations on synth211k after {init_rounds} B2B "
+                        "initial rounds: anchors at ktg_lal positions, alpha 0.01 -> 1.0 "
+                        "linear, x+y solved to rtol 1e-6 from the previous FP64 solution",
+            "summary": summary, "iterations": rows}
 
 
 def kraftwerk2_leg(torch, dev, stream, raw, reps: int, cpu: bool) -> dict:
@@ -973,6 +1093,17 @@ def run_config4(args) -> int:
     return 0
 
 
+def run_simpl_report(iters: int) -> int:
+    import torch
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    raw, nl, x, y, ax, ay = make_workload(1)
+    rep = simpl_report(torch, dev, stream, nl, x, y, iters)
+    print(json.dumps(rep))
+    return 0
+
+
 def main():
     args = parse()
     if args.profile_pcg:
@@ -981,6 +1112,8 @@ def main():
         return profile_spmv(args.profile_spmv)
     if args.config4:
         return run_config4(args)
+    if args.simpl_report:
+        return run_simpl_report(args.simpl_report)
     if args.profile_once:
         return profile_once()
     if args.profile_lal:

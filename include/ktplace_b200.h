@@ -394,6 +394,26 @@ int64_t ktg_learned_launch_count(const ktg_learned *h);
  * Any of the three pointers may be NULL. Host memory. */
 int ktg_download_aggregates(ktg_ctx *ctx, int32_t *order, int32_t *meta, float *minv);
 
+/* Coarse correction of the aggregation preconditioner (no reference
+ * counterpart). With ktg_set_option(ctx, "coarse", m) for m > 0 the mixed
+ * solve's preconditioner is the two-level additive
+ *   M r = B^-1 r + z (z^T A z)^-1 z^T r   per axis,
+ * B the aggregates' block diagonal and z one coarse vector per axis:
+ *   m = 1  the constant vector (the rigid motion of all cells, the smooth
+ *          error block Jacobi leaves on SimPL systems);
+ *   m = 2  z_i = sum_j |a_ij| / a_ii, the share of the row coupled to other
+ *          movable cells (cells held only by fixed pins and anchors do not
+ *          take part in the rigid motion);
+ *   m = 3  the learned coarse vector (ktg_learned_prepare_coarse).
+ * M is SPD for any nonzero z. The solve adds the term with no extra grid
+ * barrier: it gathers only the block part B^-1 r, forms A z c from a stored
+ * A z, and carries z^T r by recurrence beside its dot products.
+ * ktg_download_coarse builds the aggregates and the coarse vector if needed
+ * and copies out, in the permuted row order of ktg_download_aggregates,
+ * z[k] and (A z)[k] (FP32, [2n]) and einv[axis] = 1 / (z^T A z) (FP64, [2],
+ * 0 when not positive). Any pointer may be NULL. Host memory. */
+int ktg_download_coarse(ktg_ctx *ctx, float *z, float *az, double *einv);
+
 /* ---- Bookshelf reader ----------------------------------------------------
  * Reads a Bookshelf design directory <dir>/<name>.{nodes,wts,nets,pl,scl}
  * (name = the directory's own name, ".gz" variants read through zlib) with

@@ -915,6 +915,73 @@ __global__ void k_perm_out(int32_t rows, int32_t n, const int32_t *order, const 
     else y[c - n] = px[k];
 }
 
+// ---- coarse correction: z, A z and 1 / (z^T A z) per axis ------------------
+//
+// The smooth error left by block Jacobi on a SimPL system is dominated by one
+// mode: the whole placement moving together (a Laplacian held only by the
+// anchors and the fixed pins). The mixed solve removes it with the additive
+// coarse term z (z^T A z)^-1 z^T r. z per permuted row:
+//   mode 1  the constant 1;
+//   mode 2  the share of the row's weight that couples to other movable
+//           cells, sum_j |a_ij| / a_ii (cells held only by fixed pins and
+//           anchors do not take part in the rigid motion);
+//   mode 3  a caller-provided vector in the combined natural order (the
+//           learned coarse vector).
+__global__ void k_coarse_z(int mode, int32_t rows, const int32_t *prp, const double *pval,
+                           const double *pdiag, const int32_t *order, const float *zin,
+                           float2 *zaz) {
+    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= rows) return;
+    float z = 1.0f;
+    if (mode == 2) {
+        double sabs = 0.0;
+        for (int32_t e = __ldg(prp + k); e < __ldg(prp + k + 1); ++e) sabs += fabs(__ldg(pval + e));
+        z = static_cast<float>(sabs / __ldg(pdiag + k));
+    } else if (mode == 3) {
+        z = __ldg(zin + __ldg(order + k));
+    }
+    zaz[k] = make_float2(z, 0.0f);
+}
+
+// (A z)_k in FP64 (row sums of a Laplacian-like system cancel: the FP32
+// result keeps its relative precision only if it is formed in FP64), stored
+// beside z; block partials of z^T A z per axis, summed in block order by the
+// last block, which writes 1 / (z^T A z) (0 when not positive).
+__global__ void __launch_bounds__(256) k_coarse_az(int32_t rows, int32_t n, const int32_t *prp,
+                                                   const int32_t *pcol, const double *pval,
+                                                   const double *pdiag, float2 *zaz,
+                                                   double *part, unsigned *ticket, double *einv) {
+    __shared__ double red[33 * 2];
+    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    double e[2] = {0.0, 0.0};
+    if (k < rows) {
+        const int32_t off = k >= n ? n : 0;
+        const double zk = zaz[k].x;
+        double az = __ldg(pdiag + k) * zk;
+        for (int32_t q = __ldg(prp + k); q < __ldg(prp + k + 1); ++q)
+            az += __ldg(pval + q) * static_cast<double>(zaz[__ldg(pcol + q) + off].x);
+        zaz[k].y = static_cast<float>(az);
+        e[off ? 1 : 0] = zk * az;
+    }
+    block_sum_k<2>(e, red);
+    if (threadIdx.x == 0) {
+        __stcg(part + 2 * blockIdx.x, e[0]);
+        __stcg(part + 2 * blockIdx.x + 1, e[1]);
+    }
+    if (last_block_done(ticket)) {
+        double t[2] = {0.0, 0.0};
+        for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x) {
+            t[0] += __ldcg(part + 2 * b);
+            t[1] += __ldcg(part + 2 * b + 1);
+        }
+        block_sum_k<2>(t, red);
+        if (threadIdx.x == 0) {
+            einv[0] = t[0] > 0.0 ? 1.0 / t[0] : 0.0;
+            einv[1] = t[1] > 0.0 ? 1.0 / t[1] : 0.0;
+        }
+    }
+}
+
 template <typename T>
 int grow(ktg_ctx *c, T **p, int64_t count) {
     if (*p) cudaFree(*p);
@@ -938,6 +1005,8 @@ int reserve(ktg_ctx *c, AggState *s, int64_t rows, int64_t nnz) {
         for (double **p : {&s->cdiag[0], &s->cdiag[1], &s->pdiag, &s->prhs, &s->px})
             if ((rc = grow(c, p, rows))) return rc;
         if ((rc = grow(c, &s->minv, rows * kAggMax))) return rc;
+        if ((rc = grow(c, &s->zaz, rows))) return rc;
+        if ((rc = grow(c, &s->coarse_part, 2 * ((rows + kT - 1) / kT)))) return rc;
         s->tiles_cap = (std::max(rows, nnz) + kScanTile - 1) / kScanTile + 1;
         if ((rc = grow(c, &s->tile_sum, s->tiles_cap))) return rc;
         s->cap_rows = rows;
@@ -953,6 +1022,11 @@ int reserve(ktg_ctx *c, AggState *s, int64_t rows, int64_t nnz) {
         s->cap_nnz = nnz;
     }
     if (!s->counts && (rc = grow(c, &s->counts, 8))) return rc;
+    if (!s->coarse_einv && (rc = grow(c, &s->coarse_einv, 2))) return rc;
+    if (!s->ticket) {
+        if ((rc = grow(c, &s->ticket, 1))) return rc;
+        KTG_CUDA(c, cudaMemsetAsync(s->ticket, 0, sizeof(unsigned), c->stream));
+    }
     return KTG_OK;
 }
 
@@ -985,7 +1059,8 @@ void free_agg(ktg_ctx *c) {
                     (void *)s->pcol, (void *)s->pval, (void *)s->pval32, (void *)s->pdiag,
                     (void *)s->prhs, (void *)s->px, (void *)s->minv, (void *)s->meta,
                     (void *)s->blk_start, (void *)s->gslice, (void *)s->ea, (void *)s->eb,
-                    (void *)s->la})
+                    (void *)s->la, (void *)s->zaz, (void *)s->coarse_einv,
+                    (void *)s->coarse_part, (void *)s->ticket})
         if (p) cudaFree(p);
     delete s;
     c->agg = nullptr;
@@ -1101,7 +1176,33 @@ int build_agg(ktg_ctx *c) {
     c->launches += 2;
     KTG_CUDA(c, cudaGetLastError());
     s->blk_grid = 0;  // row ranges follow the new aggregates
+    s->coarse_mode = 0;
     c->agg_ready = true;
+    return KTG_OK;
+}
+
+// The coarse vector of `mode` (1, 2, or 3 with zin) for the current
+// aggregates and its A z and 1 / (z^T A z); kept until the next build.
+int agg_coarse_setup(ktg_ctx *c, int mode, const float *zin) {
+    AggState *s = c->agg;
+    const int64_t rows = 2 * c->sys_n;
+    if (!s || !c->agg_ready) return set_error(c, KTG_ERR_STATE, "no aggregates to correct");
+    if (mode == 3 && !zin) return set_error(c, KTG_ERR_STATE, "no learned coarse vector");
+    if (s->coarse_mode == mode && mode != 3) return KTG_OK;
+    if (rows == 0) {
+        KTG_CUDA(c, cudaMemsetAsync(s->coarse_einv, 0, 2 * sizeof(double), c->stream));
+        s->coarse_mode = mode;
+        return KTG_OK;
+    }
+    const int32_t R = static_cast<int32_t>(rows), n = static_cast<int32_t>(c->sys_n);
+    const int g = blocks_for(rows, kT);
+    k_coarse_z<<<g, kT, 0, c->stream>>>(mode, R, s->prp, s->pval, s->pdiag, s->order, zin,
+                                        s->zaz);
+    k_coarse_az<<<g, kT, 0, c->stream>>>(R, n, s->prp, s->pcol, s->pval, s->pdiag, s->zaz,
+                                         s->coarse_part, s->ticket, s->coarse_einv);
+    c->launches += 2;
+    KTG_CUDA(c, cudaGetLastError());
+    s->coarse_mode = mode;
     return KTG_OK;
 }
 

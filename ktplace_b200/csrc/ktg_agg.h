@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector_types.h>
 
 namespace ktg {
 
@@ -37,6 +38,13 @@ struct AggState {
     double *gslice = nullptr;      // per-block slices when shared memory is too small
     int64_t gslice_cap = 0;
     int blk_grid = 0;              // grid the blk_start array was built for
+    // coarse correction (the mixed solve's u = B^-1 r + z c): per permuted row
+    // (z, (A z)) in FP32, per axis 1 / (z^T A z) (0: no correction)
+    float2 *zaz = nullptr;         // [2n]
+    double *coarse_einv = nullptr; // [2]
+    double *coarse_part = nullptr; // [2 * blocks] per-block z^T A z
+    unsigned *ticket = nullptr;    // last-block ticket of the coarse set-up
+    int coarse_mode = 0;           // mode the zaz array holds (0: none built)
 };
 
 }  // namespace ktg

@@ -299,6 +299,11 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         c->precond = static_cast<int>(value);
         return KTG_OK;
     }
+    if (k == "coarse") {
+        if (value < 0 || value > 3) return set_error(c, KTG_ERR_ARG, "coarse must be 0, 1, 2 or 3");
+        c->coarse = static_cast<int>(value);
+        return KTG_OK;
+    }
     if (k == "pcg_form") {
         if (value < -1 || value > 3)
             return set_error(c, KTG_ERR_ARG, "pcg_form must be -1, 0, 1, 2 or 3");
@@ -827,6 +832,34 @@ int ktg_download_aggregates(ktg_ctx *c, int32_t *order, int32_t *meta, float *mi
             KTG_CUDA(c, cudaMemcpyAsync(minv, g->minv, sizeof(float) * 8 * rows,
                                         cudaMemcpyDeviceToHost, c->stream));
     }
+    return sync(c);
+}
+
+int ktg_download_coarse(ktg_ctx *c, float *z, float *az, double *einv) {
+    if (!c) return KTG_ERR_ARG;
+    if (!c->have_system) return set_error(c, KTG_ERR_STATE, "no system to aggregate");
+    if (c->coarse <= 0) return set_error(c, KTG_ERR_STATE, "coarse option is 0");
+    if (c->coarse == 3 && !c->coarse_z_ready)
+        return set_error(c, KTG_ERR_STATE, "learned coarse vector not prepared");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (!c->agg_ready && (rc = ktg::build_agg(c))) return rc;
+    if ((rc = ktg::agg_coarse_setup(c, c->coarse, c->coarse_z))) return rc;
+    const int64_t rows = 2 * c->sys_n;
+    const ktg::AggState *g = c->agg;
+    if (rows > 0 && (z || az)) {
+        std::vector<float2> h(rows);
+        KTG_CUDA(c, cudaMemcpyAsync(h.data(), g->zaz, sizeof(float2) * rows,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        if ((rc = sync(c))) return rc;
+        for (int64_t k = 0; k < rows; ++k) {
+            if (z) z[k] = h[k].x;
+            if (az) az[k] = h[k].y;
+        }
+    }
+    if (einv)
+        KTG_CUDA(c, cudaMemcpyAsync(einv, g->coarse_einv, 2 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c->stream));
     return sync(c);
 }
 

@@ -99,6 +99,10 @@ struct ktg_ctx {
     int precond = 0;             // 0 Jacobi, 1 learned, 2 aggregation (ktg_set_option "precond")
     ktg::AggState *agg = nullptr;  // aggregation preconditioner of the current systems
     bool agg_ready = false;        // agg holds aggregates of the current systems
+    int coarse = 0;                // coarse vector of the aggregation solve: 0 none,
+                                   // 1 constant, 2 coupling share, 3 learned
+    const float *coarse_z = nullptr;  // learned coarse vector [2n] (combined natural order)
+    bool coarse_z_ready = false;      // coarse_z belongs to the current systems
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
     int64_t sys_cap_nnz = 0;  // allocated entries for col/val
@@ -172,6 +176,7 @@ int build_agg(ktg_ctx *ctx);
 int agg_prepare_solve(ktg_ctx *ctx, int grid, const double *x, const double *y, int32_t *rows_cap);
 int agg_finish_solve(ktg_ctx *ctx, double *x, double *y);
 double *agg_global_slices(ktg_ctx *ctx, int64_t doubles);
+int agg_coarse_setup(ktg_ctx *ctx, int mode, const float *zin);
 void free_agg(ktg_ctx *ctx);
 
 // Look-ahead legalization (ktg_lal.cu): free space (host arrays) and the

@@ -66,9 +66,13 @@ struct MixArgs {
     uint64_t total_timeout_ns;
     const int32_t *blk_start;  // aggregation: block row ranges aligned to aggregates
     double *gslice;            // per-block slices in global memory (null: shared memory)
+    // aggregation's coarse correction (null: none): per permuted row (z, (A z)),
+    // and per axis 1 / (z^T A z) (0 turns the axis's correction off)
+    const float2 *zaz;
+    const double *coarse_einv;
 };
 
-enum MixSlot { kTRR = 0, kTBB = 1, kIRZ0 = 2, kIPAP = 3, kIRR = 4, kIRZ = 5 };
+enum MixSlot { kTRR = 0, kTBB = 1, kIRZ0 = 2, kIPAP = 3, kIRR = 4, kIRZ = 5, kIZW = 6, kTZR = 7 };
 
 __device__ __forceinline__ double *mslot(const MixArgs &A, int slot, int axis) {
     return A.part + (static_cast<size_t>(slot) * 2 + axis) * gridDim.x;
@@ -414,7 +418,7 @@ enum MixPre { kPreJacobi = 0, kPreLearned = 1, kPreAgg = 2 };
 template <int PRE>
 __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     extern __shared__ __align__(16) double dyn[];
-    __shared__ double scratch[33 * 6];  // block sums of up to 6 values
+    __shared__ double scratch[33 * 8];  // block sums of up to 8 values
     __shared__ MixAxis sax[2];
     if (threadIdx.x < 2) sax[threadIdx.x] = A.ax[threadIdx.x];
     __syncthreads();
@@ -433,13 +437,21 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     }
     const int32_t R = max(r1 - r0, 0);
     const int32_t cap = A.rows_per_block;
+    // coarse correction of the aggregation preconditioner: u = B^-1 r + z c,
+    // c = (z^T r) / (z^T A z) per axis
+    const bool coarse = PRE == kPreAgg && A.zaz != nullptr;
+    const int slice_doubles = coarse ? 5 : 4;
     double *base = A.gslice ? A.gslice + static_cast<size_t>(blockIdx.x) * cap * 5 : dyn;
     // warp-tile buffer after the shared slices (16-byte aligned)
-    double *tile64 = A.gslice ? dyn : dyn + (4 * static_cast<size_t>(cap) + 1) / 2 * 2;
+    double *tile64 =
+        A.gslice ? dyn : dyn + (slice_doubles * static_cast<size_t>(cap) + 1) / 2 * 2;
     float *tile32 = reinterpret_cast<float *>(tile64);
     double *sx = base;  // diag is read through L1 (shared memory comes out of L1)
     float *sr = reinterpret_cast<float *>(base + cap);
+    // su holds the block part B^-1 r of u (what the SpMV gathers); with the
+    // coarse correction the full u is su + z c
     float *su = sr + cap, *sw = su + cap, *sp = sw + cap, *ss = sp + cap, *sdd = ss + cap;
+    float2 *szaz = reinterpret_cast<float2 *>(sdd + cap);  // (z, A z) per row (coarse only)
     const int32_t n0 = sax[0].n;
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
         const int32_t c = r0 + l;
@@ -469,6 +481,12 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         int32_t i;
         locate(l, axis, i);
         sx[l] = sax[axis].x[i];
+        if (coarse) szaz[l] = __ldg(A.zaz + r0 + l);
+    }
+    double einv[2] = {0.0, 0.0};
+    if (coarse) {
+        einv[0] = __ldg(A.coarse_einv);
+        einv[1] = __ldg(A.coarse_einv + 1);
     }
     __syncthreads();
 
@@ -528,7 +546,8 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     for (int round = 0;; ++round) {
         // ---- FP64 residual r = b - A x; r32, and u (Jacobi) or D^-1/2 r -----
         {
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};  // rr x, bb x, rr y, bb y
+            // rr x, bb x, rr y, bb y, z.r x, z.r y
+            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             warp_tile_spmv<double>(
                 r0, n0, R, nullptr, wb, tile64,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
@@ -555,23 +574,35 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     }
                     acc[axis * 2 + 0] += r * r;
                     acc[axis * 2 + 1] += b * b;
+                    if (coarse) acc[4 + axis] += static_cast<double>(szaz[l].x) * r;
                 });
             if (PRE == kPreAgg) {
                 const bool all[2] = {true, true};
                 apply_blocks(all);
             }
-            const int sl[4] = {kTRR, kTBB, kTRR, kTBB};
-            const int ax[4] = {0, 0, 1, 1};
-            mstore<4>(A, acc, sl, ax, scratch);
+            const int sl[6] = {kTRR, kTBB, kTRR, kTBB, kTZR, kTZR};
+            const int ax[6] = {0, 0, 1, 1, 0, 1};
+            mstore<6>(A, acc, sl, ax, scratch);
         }
         if (!sync()) return;
         bool live[2];
         double r_norm[2];
+        // coarse state per axis: z^T r and z^T s by recurrence, and the
+        // coefficient c of z in the current u
+        double ztr[2] = {0.0, 0.0}, zts[2] = {0.0, 0.0};
+        float cu[2] = {0.0f, 0.0f};
         {
-            double s[4];
-            const int sl[4] = {kTRR, kTBB, kTRR, kTBB};
-            const int ax[4] = {0, 0, 1, 1};
-            mreduce<4>(A, s, sl, ax, scratch);
+            double s[6];
+            const int sl[6] = {kTRR, kTBB, kTRR, kTBB, kTZR, kTZR};
+            const int ax[6] = {0, 0, 1, 1, 0, 1};
+            mreduce<6>(A, s, sl, ax, scratch);
+            if (coarse) {
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    ztr[a] = s[4 + a];
+                    cu[a] = static_cast<float>(einv[a] * ztr[a]);
+                }
+            }
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
                 if (round == 0) {
@@ -604,7 +635,8 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         double gamma_prev[2] = {0.0, 0.0}, alpha_prev[2] = {0.0, 0.0};
         const double target[2] = {A.inner_tol * r_norm[0], A.inner_tol * r_norm[1]};
         for (;;) {
-            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // gamma, delta, rr per axis
+            // gamma, delta, rr, z.w per axis
+            double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             warp_tile_spmv<float>(
                 r0, n0, R, in_live, wb, tile32,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const float *&val,
@@ -618,28 +650,49 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     return static_cast<float>(__ldg(sax[pass].diag + i)) * su[l];
                 },
                 [&](int32_t l, int axis, int32_t, float w) {
-                    const float ui = su[l];
+                    float ui = su[l];
+                    if (coarse) {  // A (u_b + z c) = A u_b + (A z) c
+                        const float2 za = szaz[l];
+                        ui += za.x * cu[axis];
+                        w += za.y * cu[axis];
+                        acc[axis * 4 + 3] += static_cast<double>(za.x) * w;
+                    }
                     sw[l] = w;
                     const float r = sr[l];
-                    acc[axis * 3 + 0] += static_cast<double>(r) * ui;
-                    acc[axis * 3 + 1] += static_cast<double>(w) * ui;
-                    acc[axis * 3 + 2] += static_cast<double>(r) * r;
+                    acc[axis * 4 + 0] += static_cast<double>(r) * ui;
+                    acc[axis * 4 + 1] += static_cast<double>(w) * ui;
+                    acc[axis * 4 + 2] += static_cast<double>(r) * r;
                 });
-            {  // one block sum for both axes (each value summed as alone)
+            if (coarse) {  // one block sum for both axes (each value summed as alone)
+                const int sl[8] = {kIRZ, kIPAP, kIRR, kIZW, kIRZ, kIPAP, kIRR, kIZW};
+                const int ax[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+                mstore<8>(A, acc, sl, ax, scratch);
+            } else {
+                double a6[6] = {acc[0], acc[1], acc[2], acc[4], acc[5], acc[6]};
                 const int sl[6] = {kIRZ, kIPAP, kIRR, kIRZ, kIPAP, kIRR};
                 const int ax[6] = {0, 0, 0, 1, 1, 1};
-                mstore<6>(A, acc, sl, ax, scratch);
+                mstore<6>(A, a6, sl, ax, scratch);
             }
             if (!sync()) return;
             float alpha[2] = {0.0f, 0.0f}, beta[2] = {0.0f, 0.0f};
+            float cu_next[2] = {cu[0], cu[1]};
             bool ok[2] = {false, false};
             {
-                double s[6];
-                const int sl[6] = {kIRZ, kIPAP, kIRR, kIRZ, kIPAP, kIRR};
-                const int ax[6] = {0, 0, 0, 1, 1, 1};
-                mreduce<6>(A, s, sl, ax, scratch);
-                const double gamma[2] = {s[0], s[3]}, delta[2] = {s[1], s[4]};
-                const double rr[2] = {s[2], s[5]};
+                double s[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if (coarse) {
+                    const int sl[8] = {kIRZ, kIPAP, kIRR, kIZW, kIRZ, kIPAP, kIRR, kIZW};
+                    const int ax[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+                    mreduce<8>(A, s, sl, ax, scratch);
+                } else {
+                    double s6[6];
+                    const int sl[6] = {kIRZ, kIPAP, kIRR, kIRZ, kIPAP, kIRR};
+                    const int ax[6] = {0, 0, 0, 1, 1, 1};
+                    mreduce<6>(A, s6, sl, ax, scratch);
+                    s[0] = s6[0], s[1] = s6[1], s[2] = s6[2];
+                    s[4] = s6[3], s[5] = s6[4], s[6] = s6[5];
+                }
+                const double gamma[2] = {s[0], s[4]}, delta[2] = {s[1], s[5]};
+                const double rr[2] = {s[2], s[6]}, zw[2] = {s[3], s[7]};
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
                     if (!in_live[a]) continue;
@@ -663,6 +716,11 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     beta[a] = static_cast<float>(b);
                     gamma_prev[a] = gamma[a];
                     alpha_prev[a] = al;
+                    if (coarse) {  // s = w + beta s, r -= alpha s, projected on z
+                        zts[a] = first[a] ? zw[a] : zw[a] + b * zts[a];
+                        ztr[a] -= al * zts[a];
+                        cu_next[a] = static_cast<float>(einv[a] * ztr[a]);
+                    }
                 }
             }
             if (!(ok[0] || ok[1])) break;
@@ -673,7 +731,8 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 if (!ok[axis]) continue;
                 const MixAxis &S = sax[axis];
                 const bool f = first[axis];
-                const float pn = f ? su[l] : su[l] + beta[axis] * sp[l];
+                const float ui = coarse ? su[l] + szaz[l].x * cu[axis] : su[l];
+                const float pn = f ? ui : ui + beta[axis] * sp[l];
                 const float sn = f ? sw[l] : sw[l] + beta[axis] * ss[l];
                 sp[l] = pn;
                 ss[l] = sn;
@@ -694,6 +753,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 if (!ok[a]) continue;
                 ++inner[a];
                 first[a] = false;
+                cu[a] = cu_next[a];
             }
             if (!sync()) return;
             if (pre) {
@@ -773,11 +833,20 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     if (A.rows_per_block == 0) A.rows_per_block = 1;
     A.blk_start = nullptr;
     A.gslice = nullptr;
+    A.zaz = nullptr;
+    A.coarse_einv = nullptr;
     AggState *g = nullptr;
     if (agg) {
         if ((rc = agg_prepare_solve(c, grid, x, y, &A.rows_per_block))) return rc;
         g = c->agg;
         A.blk_start = g->blk_start;
+        if (c->coarse > 0) {
+            if (c->coarse == 3 && !c->coarse_z_ready)
+                return set_error(c, KTG_ERR_STATE, "learned coarse vector not prepared");
+            if ((rc = agg_coarse_setup(c, c->coarse, c->coarse_z))) return rc;
+            A.zaz = g->zaz;
+            A.coarse_einv = g->coarse_einv;
+        }
     }
     for (int a = 0; a < 2; ++a) {
         ktg::AxisSystem &s = c->sys[a];
@@ -795,7 +864,8 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     // Chronopoulos-Gear kernel (always for the aggregation preconditioner),
     // with shared-memory slices of 32 bytes per row when they fit, else
     // global ones; the textbook kernel on global vectors when asked for.
-    const size_t slice = 32 * static_cast<size_t>(A.rows_per_block) + 8;  // + alignment
+    // 32 bytes per row (x; r, u, w, p, s, d), 40 with the coarse (z, A z)
+    const size_t slice = (A.zaz ? 40 : 32) * static_cast<size_t>(A.rows_per_block) + 8;
     const size_t tile = sizeof(double) * kTileChunk * (kMixThreads / 32);
     const bool cg_form = agg || c->mixed_form != 0;
     const bool in_smem = slice + tile <= kMixSmemBytes;

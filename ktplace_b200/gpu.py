@@ -176,6 +176,19 @@ class Context:
             out["minv"].ctypes.data_as(P(ctypes.c_float))))
         return {k: v[:2 * n] for k, v in out.items()}
 
+    def coarse(self) -> dict:
+        """Coarse correction of the aggregation preconditioner (option
+        "coarse" > 0): z and A z per permuted row [2n], 1 / (z^T A z) per axis."""
+        n, _ = self.system_info(0)
+        z = np.zeros(max(2 * n, 1), np.float32)
+        az = np.zeros(max(2 * n, 1), np.float32)
+        einv = np.zeros(2)
+        P = ctypes.POINTER
+        self._check(self.lib.ktg_download_coarse(self.h, z.ctypes.data_as(P(ctypes.c_float)),
+                                                 az.ctypes.data_as(P(ctypes.c_float)),
+                                                 einv.ctypes.data_as(P(ctypes.c_double))))
+        return dict(z=z[:2 * n], az=az[:2 * n], einv=einv)
+
     def system(self, axis: int) -> dict:
         n, m = self.system_info(axis)
         s = dict(row_ptr=np.zeros(n + 1, np.int64), col=np.zeros(max(m, 1), np.int32),

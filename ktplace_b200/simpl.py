@@ -13,6 +13,11 @@ so code written against the reference reads the same:
   LookAheadLegalizer   simpl_lal.h:18-60 (legalize), built as
                        simplPlacer::Impl::lookAheadLegalize does
                        (simpl_placer.cc:299-310)
+  GlobalLoop           the B2B rounds of getInitialPlacement and the loop of
+                       getGlobalPlacement (simpl_placer.cc:406-448, 463-539):
+                       look-ahead legalization of the lower bound, B2B build
+                       anchored at the legalized (upper-bound) positions,
+                       warm-started solve, on device-resident data
 
 All arithmetic runs in the CUDA library through the C ABI; nothing here
 computes a result on the CPU. A SparseSystem produced by buildB2B remembers
@@ -175,3 +180,74 @@ class LookAheadLegalizer:
         x[...] = nx
         y[...] = ny
 
+
+
+def alpha_linear(it: int, iters: int = 30, first: float = 0.01, last: float = 1.0) -> float:
+    """Anchor weight rising linearly from `first` to `last` over `iters`
+    global iterations (the schedule of the mixed-precision study; the
+    reference's own default is alphaBase * (1 + it), simpl_placer.cc:513)."""
+    return first + (last - first) * min(it, iters - 1) / max(iters - 1, 1)
+
+
+@dataclasses.dataclass
+class GlobalIterate:
+    """State of one global iteration, taken right after its B2B build (the
+    context then holds that iteration's systems): the lower-bound positions
+    the systems were built at (the solve's warm start), the legalized
+    upper-bound positions that anchor them, and the anchor weight."""
+    it: int
+    alpha: float
+    x: np.ndarray
+    y: np.ndarray
+    ux: np.ndarray
+    uy: np.ndarray
+
+
+class GlobalLoop:
+    """SimPL's global placement loop on the GPU path (simpl_placer.cc:463-539).
+
+    Every iteration: upper = lookAheadLegalize(lower) (ktg_lal), then
+    buildB2B(lower, alpha, upper) (ktg_build_b2b) and the warm-started solve
+    of lower (``solve``, by default the FP64 Jacobi-PCG of ktg_solve). The
+    initial placement is SimPL's B2B initial rounds with no anchor
+    (initialRounds with init_net b2b, simpl_placer.cc:406-448: buildB2B with
+    alpha 0 and a solve per round). ``iterations`` yields a GlobalIterate
+    after each build, before the solve, so a caller can solve or inspect the
+    same systems another way; ``solve`` then advances the lower bound.
+    Convergence checks and refinement are the caller's (the iteration count
+    is fixed)."""
+
+    def __init__(self, context: Context, netlist, grid: BinGrid, free_space: FreeSpace,
+                 tol: float = 1e-6, max_iter: int = 100000, opts: Optional[SimplOptions] = None):
+        self.ctx = context
+        self.nl = netlist
+        if context.nl is not netlist:
+            context.upload_netlist(netlist)
+        self.fx, self.fy = netlist.floors()
+        self.lal = LookAheadLegalizer(context, grid, free_space, opts or SimplOptions())
+        self.tol = tol
+        self.max_iter = max_iter
+
+    def solve(self, x, y):
+        r = self.ctx.solve(x, y, self.tol, self.max_iter)
+        return r["x"], r["y"]
+
+    def initial_rounds(self, x, y, rounds: int = 5):
+        x, y = np.array(x, dtype=np.float64), np.array(y, dtype=np.float64)
+        for _ in range(rounds):
+            self.ctx.build_b2b(x, y, 0.0, None, None, self.fx, self.fy)
+            x, y = self.solve(x, y)
+        return x, y
+
+    def iterations(self, x, y, iters: int, alpha=alpha_linear, solve=None):
+        """Yields GlobalIterate k = 0 .. iters-1; between yields the lower
+        bound is solved with ``solve(x, y) -> (x, y)`` (default: FP64)."""
+        solve = solve or self.solve
+        x, y = np.array(x, dtype=np.float64), np.array(y, dtype=np.float64)
+        for it in range(iters):
+            ux, uy = x.copy(), y.copy()
+            self.lal.legalize(ux, uy)
+            a = float(alpha(it))
+            self.ctx.build_b2b(x, y, a, ux, uy, self.fx, self.fy)
+            yield GlobalIterate(it, a, x.copy(), y.copy(), ux, uy)
+            x, y = solve(x, y)
