@@ -374,6 +374,31 @@ int ktg_learned_train_step(ktg_learned *h, ktg_ctx *ctx, int axis, uint64_t seed
 int ktg_learned_prepare(ktg_learned *h, ktg_ctx *ctx);
 int64_t ktg_learned_launch_count(const ktg_learned *h);
 
+/* The learned coarse vector of the two-level aggregation preconditioner
+ * (ktg_download_coarse, "coarse" = 3; no reference counterpart). The same
+ * 3-layer network runs once per netlist on features of the netlist alone
+ * (pins per cell, sizes of its nets, fixed pins on them, area), giving an
+ * embedding p (16 per cell) that is reused for every system of that
+ * netlist; a per-system head (one hidden layer of 16, FP32) maps
+ * (p_i, sum_j |a_ij| / a_ii, log a_ii - mean log a) to z_i = softplus(.) > 0.
+ * An untrained head gives z = 1, the constant coarse vector.
+ * Training minimises, over test vectors e_t of a system (the errors that the
+ * aggregation-preconditioned CG leaves after a few iterations of a SimPL
+ * solve), the share of their A-energy outside span(z):
+ *   L = mean_t (1 - (z^T A e_t)^2 / ((z^T A z)(e_t^T A e_t))).
+ * ktg_learned_coarse_loss_grad: loss and parameter gradient on axis `axis`
+ * of ctx's current systems; e holds num_vec (1..4) host vectors of n
+ * doubles. ktg_learned_coarse_train_step: the same, then one clipped Adam
+ * step. ktg_learned_prepare_coarse: computes z for both axes of ctx's
+ * current systems on ctx's stream (the embedding is recomputed only when
+ * the netlist or the parameters changed) for the next mixed solve with
+ * "coarse" = 3; a new build invalidates it. */
+int ktg_learned_coarse_loss_grad(ktg_learned *h, ktg_ctx *ctx, int axis, const double *e,
+                                 int32_t num_vec, double *loss, float *grad);
+int ktg_learned_coarse_train_step(ktg_learned *h, ktg_ctx *ctx, int axis, const double *e,
+                                  int32_t num_vec, double *loss);
+int ktg_learned_prepare_coarse(ktg_learned *h, ktg_ctx *ctx);
+
 /* ---- aggregation preconditioner (no reference counterpart) ---------------
  * With ktg_set_option(ctx, "precond", 2), ktg_solve_mixed preconditions its
  * FP32 inner PCG with the exact inverses of A's diagonal blocks over

@@ -148,6 +148,11 @@ SIGNATURES = [
                                               ctypes.POINTER(ctypes.c_double)]),
     ("ktg_learned_prepare", ctypes.c_int, [_vp, _vp]),
     ("ktg_learned_launch_count", ctypes.c_int64, [_vp]),
+    ("ktg_learned_coarse_loss_grad", ctypes.c_int,
+     [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_double), _vp]),
+    ("ktg_learned_coarse_train_step", ctypes.c_int,
+     [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
+    ("ktg_learned_prepare_coarse", ctypes.c_int, [_vp, _vp]),
     ("ktg_hpwl_noalloc", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                         ctypes.c_int64, _vp, _vp]),
 ]

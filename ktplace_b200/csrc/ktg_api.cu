@@ -169,6 +169,7 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
         c->val32_valid = false;
         c->precond_ready = false;
         c->agg_ready = false;
+        c->coarse_z_ready = false;
         c->sys_cap_nnz = nnz;
     }
     return KTG_OK;
@@ -241,6 +242,7 @@ void ktg_destroy(ktg_ctx *c) {
     free_systems(c);
     ktg::free_agg(c);
     ktg::free_lal(c);
+    dev_free(c->coarse_z_buf);
     dev_free(c->exact_prod);
     dev_free(c->exact_cpart);
     dev_free(c->partials);
@@ -475,6 +477,7 @@ int ktg_upload_netlist(ktg_ctx *c, const ktg_netlist_view *nl) {
     if ((rc = upload(c, c->area, area.data(), n))) return rc;
     if ((rc = sync(c))) return rc;
     c->have_netlist = true;
+    ++c->netlist_gen;
     c->have_system = false;
     c->sys_n = n;
     return KTG_OK;
@@ -509,6 +512,7 @@ int ktg_build_b2b(ktg_ctx *c, const double *x, const double *y, double alpha, co
     c->val32_valid = false;
     c->precond_ready = false;
     c->agg_ready = false;
+    c->coarse_z_ready = false;
     if (c->ptr_mode == KTG_PTR_HOST) {
         const int st = device_status(c);
         if (st < 0) return st;
@@ -539,6 +543,7 @@ int ktg_build_b2b_kraftwerk2(ktg_ctx *c, const double *x, const double *y, int w
     c->val32_valid = false;
     c->precond_ready = false;
     c->agg_ready = false;
+    c->coarse_z_ready = false;
     if (c->ptr_mode == KTG_PTR_HOST) {
         const int st = device_status(c);
         if (st < 0) return st;
@@ -570,6 +575,7 @@ int ktg_kraftwerk2_adjust(ktg_ctx *c, const double *move_weight, const double *t
     c->val32_valid = false;
     c->precond_ready = false;
     c->agg_ready = false;
+    c->coarse_z_ready = false;
     if (c->ptr_mode == KTG_PTR_HOST) return sync(c);
     return KTG_OK;
 }
@@ -587,6 +593,7 @@ int ktg_build_star(ktg_ctx *c, int64_t *size) {
     c->val32_valid = false;
     c->precond_ready = false;
     c->agg_ready = false;
+    c->coarse_z_ready = false;
     *size = rows;
     return KTG_OK;
 }
@@ -684,6 +691,7 @@ int ktg_upload_system(ktg_ctx *c, int axis, int64_t n, const int64_t *row_ptr, c
     c->val32_valid = false;
     c->precond_ready = false;
     c->agg_ready = false;
+    c->coarse_z_ready = false;
     c->sys_n = n;
     c->have_system = c->axis_valid[0] && c->axis_valid[1];
     return KTG_OK;

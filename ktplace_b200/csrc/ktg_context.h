@@ -103,6 +103,9 @@ struct ktg_ctx {
                                    // 1 constant, 2 coupling share, 3 learned
     const float *coarse_z = nullptr;  // learned coarse vector [2n] (combined natural order)
     bool coarse_z_ready = false;      // coarse_z belongs to the current systems
+    float *coarse_z_buf = nullptr;    // storage of the learned coarse vector
+    int64_t coarse_z_cap = 0;
+    int64_t netlist_gen = 0;          // bumped by every ktg_upload_netlist
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
     int64_t sys_cap_nnz = 0;  // allocated entries for col/val

@@ -41,10 +41,18 @@ constexpr int HID = 64;
 constexpr int PROJ = 16;
 constexpr int NFEAT = 8;
 constexpr int LAYERS = 3;
+// coarse-vector head: input = p (PROJ), coupling share, log diag
+constexpr int HEAD_IN = PROJ + 2;
+constexpr int HEAD_H = 16;
+constexpr int kMaxVec = 4;  // test vectors per coarse loss
+// softplus^-1(1): the head's output bias at initialisation, so that the
+// untrained head gives the constant coarse vector
+constexpr double kSoftplusInvOne = 0.5413248546129181;
 
 // Parameter layout (FP32 master, same order as oracle/learned_ref.py).
 struct Layout {
-    int64_t W_in, b_in, Wa[LAYERS], ba[LAYERS], Wb[LAYERS], Wc[LAYERS], bb[LAYERS], P, total;
+    int64_t W_in, b_in, Wa[LAYERS], ba[LAYERS], Wb[LAYERS], Wc[LAYERS], bb[LAYERS], P;
+    int64_t Wh, bh, wz, bz, total;
 };
 
 inline Layout layout() {
@@ -60,6 +68,10 @@ inline Layout layout() {
         L.bb[l] = o; o += HID;
     }
     L.P = o; o += HID * PROJ;
+    L.Wh = o; o += HEAD_IN * HEAD_H;
+    L.bh = o; o += HEAD_H;
+    L.wz = o; o += HEAD_H;
+    L.bz = o; o += 1;
     L.total = o;
     return L;
 }
@@ -391,6 +403,212 @@ __global__ void k_reduce_partials(const float *partials, int blocks, int nout, f
 }
 
 // ---------------------------------------------------------------------------
+// learned coarse vector: topology features, head, projection loss
+// ---------------------------------------------------------------------------
+// Per-cell features of the netlist alone (no positions), the trunk's input
+// when it predicts the coarse vector; computed once per netlist:
+//   1, pins/8, mean over the cell's nets of (movable pins - 1)/8, of fixed
+//   pins/4, share of its nets with a fixed pin, mean 1/(degree - 1),
+//   log(area)/8, log1p(pins)/2.
+__global__ void k_topo_features(const int32_t *pin_start, const int2 *pin_ref,
+                                const int32_t *net_start, const int32_t *net_mov,
+                                const double *area, int32_t n, float *x) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t e0 = pin_start[i], e1 = pin_start[i + 1];
+    double smov = 0.0, sfix = 0.0, anyfix = 0.0, sinv = 0.0;
+    for (int32_t q = e0; q < e1; ++q) {
+        const int32_t k = pin_ref[q].x;
+        const int32_t deg = net_start[k + 1] - net_start[k];
+        const int32_t mov = net_mov[k];
+        smov += mov - 1;
+        sfix += deg - mov;
+        anyfix += deg > mov ? 1.0 : 0.0;
+        sinv += deg >= 2 ? 1.0 / (deg - 1) : 0.0;
+    }
+    const double k = static_cast<double>(e1 - e0);
+    const double inv = k > 0.0 ? 1.0 / k : 0.0;
+    const double a = area[i];
+    float *xi = x + static_cast<int64_t>(i) * NFEAT;
+    xi[0] = 1.0f;
+    xi[1] = static_cast<float>(k / 8.0);
+    xi[2] = static_cast<float>(smov * inv / 8.0);
+    xi[3] = static_cast<float>(sfix * inv / 4.0);
+    xi[4] = static_cast<float>(anyfix * inv);
+    xi[5] = static_cast<float>(sinv * inv);
+    xi[6] = static_cast<float>(a > 0.0 ? log(a) / 8.0 : 0.0);
+    xi[7] = static_cast<float>(log1p(k) / 2.0);
+}
+
+struct HeadArgs {
+    const int32_t *rp;
+    const double *val;
+    const double *diag;
+    int32_t n;
+    const double *logd_mean;
+    const float *p;   // [n x PROJ] trunk embedding
+    const float *w;   // parameters (FP32 master)
+    int64_t Wh, bh, wz, bz;
+    float *u;         // [n x HEAD_IN] head inputs (training) or null
+    float *hh;        // [n x HEAD_H] hidden activations (training) or null
+    float *o;         // [n] pre-softplus output (training) or null
+    double *zd;       // [n] z in FP64 (training) or null
+    float *zf;        // [n] z in FP32 (inference) or null
+};
+
+// z_i = softplus(relu(u_i Wh + bh) . wz + bz), u_i = (p_i, c_i, l_i) with the
+// coupling share c_i = sum_j |a_ij| / a_ii and l_i = log a_ii - mean log a.
+__global__ void __launch_bounds__(256) k_coarse_head(HeadArgs A) {
+    __shared__ float ws[HEAD_IN * HEAD_H + 2 * HEAD_H + 1];
+    for (int t = threadIdx.x; t < HEAD_IN * HEAD_H; t += blockDim.x) ws[t] = A.w[A.Wh + t];
+    for (int t = threadIdx.x; t < HEAD_H; t += blockDim.x) {
+        ws[HEAD_IN * HEAD_H + t] = A.w[A.bh + t];
+        ws[HEAD_IN * HEAD_H + HEAD_H + t] = A.w[A.wz + t];
+    }
+    if (threadIdx.x == 0) ws[HEAD_IN * HEAD_H + 2 * HEAD_H] = A.w[A.bz];
+    __syncthreads();
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    double rowabs = 0.0;
+    for (int32_t e = A.rp[i]; e < A.rp[i + 1]; ++e) rowabs += fabs(A.val[e]);
+    const double d = A.diag[i];
+    float u[HEAD_IN];
+#pragma unroll
+    for (int k = 0; k < PROJ; ++k) u[k] = A.p[static_cast<int64_t>(i) * PROJ + k];
+    u[PROJ] = static_cast<float>(rowabs / d);
+    u[PROJ + 1] = static_cast<float>(log(d) - *A.logd_mean);
+    float o = ws[HEAD_IN * HEAD_H + 2 * HEAD_H];
+#pragma unroll
+    for (int j = 0; j < HEAD_H; ++j) {
+        float t = ws[HEAD_IN * HEAD_H + j];
+#pragma unroll
+        for (int k = 0; k < HEAD_IN; ++k) t += u[k] * ws[k * HEAD_H + j];
+        t = t > 0.0f ? t : 0.0f;
+        if (A.hh) A.hh[static_cast<int64_t>(i) * HEAD_H + j] = t;
+        o += t * ws[HEAD_IN * HEAD_H + HEAD_H + j];
+    }
+    const float z = o > 20.0f ? o : log1pf(expf(o));
+    if (A.u)
+#pragma unroll
+        for (int k = 0; k < HEAD_IN; ++k) A.u[static_cast<int64_t>(i) * HEAD_IN + k] = u[k];
+    if (A.o) A.o[i] = o;
+    if (A.zd) A.zd[i] = z;
+    if (A.zf) A.zf[i] = z;
+}
+
+// out = A in (FP64, one thread per row; training only).
+__global__ void k_spmv_rows(const int32_t *rp, const int32_t *col, const double *val,
+                            const double *diag, int32_t n, const double *in, double *out) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = diag[i] * in[i];
+    for (int32_t e = rp[i]; e < rp[i + 1]; ++e) s += val[e] * in[col[e]];
+    out[i] = s;
+}
+
+// Projection loss of the test vectors e_t on z in the A-inner product,
+//   L = (1/T) sum_t (1 - (z^T A e_t)^2 / ((z^T A z)(e_t^T A e_t))),
+// from az = A z and a_t = A e_t: block partials of q = z.az, p_t = z.a_t,
+// S_t = e_t.a_t, summed in block order by the last block, which writes
+// out = {L, beta, alpha_0..alpha_{T-1}, q, p_0.., S_0..} with
+// dL/dz = beta az + sum_t alpha_t a_t.
+__global__ void __launch_bounds__(256) k_coarse_dots(int32_t n, int T, const double *z,
+                                                     const double *az, const double *a,
+                                                     const double *e, double *partials,
+                                                     unsigned *ticket, double *out) {
+    __shared__ double red[33 * (1 + 2 * kMaxVec)];
+    constexpr int K = 1 + 2 * kMaxVec;
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = 0.0;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double zi = z[i];
+        v[0] += zi * az[i];
+#pragma unroll
+        for (int t = 0; t < kMaxVec; ++t) {
+            if (t >= T) break;
+            const double at = a[static_cast<int64_t>(t) * n + i];
+            v[1 + t] += zi * at;
+            v[1 + kMaxVec + t] += e[static_cast<int64_t>(t) * n + i] * at;
+        }
+    }
+    block_sum_k<K>(v, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < K; ++k) __stcg(partials + static_cast<int64_t>(blockIdx.x) * K + k, v[k]);
+    if (last_block_done(ticket)) {
+        double t[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) t[k] = 0.0;
+        for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x)
+#pragma unroll
+            for (int k = 0; k < K; ++k) t[k] += __ldcg(partials + static_cast<int64_t>(b) * K + k);
+        block_sum_k<K>(t, red);
+        if (threadIdx.x == 0) {
+            const double q = t[0];
+            double L = 0.0, beta = 0.0;
+            int used = 0;
+            for (int j = 0; j < T; ++j)
+                if (t[1 + kMaxVec + j] > 0.0) ++used;
+            for (int j = 0; j < T; ++j) {
+                const double pj = t[1 + j], Sj = t[1 + kMaxVec + j];
+                double al = 0.0;
+                if (q > 0.0 && Sj > 0.0) {
+                    L += (1.0 - pj * pj / (q * Sj)) / used;
+                    al = -2.0 * pj / (used * q * Sj);
+                    beta += 2.0 * pj * pj / (used * q * q * Sj);
+                }
+                out[2 + j] = al;
+                out[2 + kMaxVec + 1 + j] = pj;
+                out[2 + 2 * kMaxVec + 1 + j] = Sj;
+            }
+            out[0] = L;
+            out[1] = beta;
+            out[2 + kMaxVec] = q;
+        }
+    }
+}
+
+__global__ void k_coarse_dz(int32_t n, int T, const double *az, const double *a,
+                            const double *coef, float *dz) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double g = coef[1] * az[i];
+    for (int t = 0; t < T; ++t) g += coef[2 + t] * a[static_cast<int64_t>(t) * n + i];
+    dz[i] = static_cast<float>(g);
+}
+
+// Head backward per row: d o = dz sigmoid(o); dh = d o wz (h > 0);
+// du = dh Wh^T, whose first PROJ entries are dL/dp.
+__global__ void __launch_bounds__(256) k_coarse_head_bwd(int32_t n, const float *w, int64_t Wh,
+                                                         int64_t wz, const float *hh,
+                                                         const float *o, const float *dz,
+                                                         float *dhh, float *dout, float *dp) {
+    __shared__ float ws[HEAD_IN * HEAD_H + HEAD_H];
+    for (int t = threadIdx.x; t < HEAD_IN * HEAD_H; t += blockDim.x) ws[t] = w[Wh + t];
+    for (int t = threadIdx.x; t < HEAD_H; t += blockDim.x) ws[HEAD_IN * HEAD_H + t] = w[wz + t];
+    __syncthreads();
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float oi = o[i];
+    const float dod = dz[i] * (oi > 20.0f ? 1.0f : 1.0f / (1.0f + expf(-oi)));
+    dout[i] = dod;
+    float dh[HEAD_H];
+#pragma unroll
+    for (int j = 0; j < HEAD_H; ++j) {
+        const float hv = hh[static_cast<int64_t>(i) * HEAD_H + j];
+        dh[j] = hv > 0.0f ? dod * ws[HEAD_IN * HEAD_H + j] : 0.0f;
+        dhh[static_cast<int64_t>(i) * HEAD_H + j] = dh[j];
+    }
+#pragma unroll
+    for (int k = 0; k < PROJ; ++k) {
+        float s = 0.0f;
+#pragma unroll
+        for (int j = 0; j < HEAD_H; ++j) s += dh[j] * ws[k * HEAD_H + j];
+        dp[static_cast<int64_t>(i) * PROJ + k] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // entry head, probe loss and their gradients
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int32_t row_of_entry(const int32_t *rp, int32_t n, int32_t e) {
@@ -608,6 +826,20 @@ struct ktg_learned {
     double *h_scal = nullptr;
     cudaStream_t stream = nullptr;
     int64_t launches = 0;
+    int64_t version = 0;  // bumped whenever the parameters change
+    // coarse-vector network: work buffers (grown on demand)
+    int64_t cap_coarse = 0;
+    int cap_vec = 0;
+    float *cu = nullptr, *chh = nullptr, *co = nullptr, *cdz = nullptr, *cdhh = nullptr,
+          *cdo = nullptr;                                // [n x 18], [n x 16], [n] ...
+    double *czd = nullptr, *caz = nullptr;               // [n]
+    double *ce = nullptr, *ca = nullptr;                 // [T x n] test vectors, A e
+    double *cscal = nullptr;                             // [2 + 3 * kMaxVec + 1]
+    // trunk embedding of the last prepared netlist (reused across systems)
+    float *pc = nullptr;
+    int64_t cap_pc = 0;
+    const ktg_ctx *pc_ctx = nullptr;
+    int64_t pc_gen = -1, pc_version = -1;
 };
 
 namespace {
@@ -732,17 +964,11 @@ int wgrad(ktg_learned *h, const float *x, int k, const float *dy, const float *y
     return KTG_OK;
 }
 
-// Forward pass to p and the entry values (t, s) of one axis system.
-int forward(ktg_learned *h, ktg_ctx *c, const SysView &S, float *s_out, bool keep_t) {
+// The trunk (message passing over the cell-net graph) from the features in
+// h->x to the embedding p = h3 P in h->p.
+int trunk_forward(ktg_learned *h, ktg_ctx *c, int64_t n) {
     int rc;
-    const int64_t n = S.n, N = c->N;
-    if ((rc = reserve_work(h, n, N, S.m))) return rc;
-    const int tb = 256;
-    ktg::learned::k_logd_sum<<<std::min<int>(1024, (S.n + tb - 1) / tb + 1), tb, 0, h->stream>>>(
-        S.diag, S.n, h->dpart, h->ticket, h->scal + 0);
-    ktg::learned::k_features<<<(S.n + tb - 1) / tb, tb, 0, h->stream>>>(
-        S.rp, S.col, S.val, S.diag, c->pin_start, S.n, h->scal + 0, h->x);
-    h->launches += 2;
+    const int64_t N = c->N;
     const Layout &L = h->L;
     if ((rc = dense(h, h->x, NFEAT, nullptr, L.W_in, 0, L.b_in, cell_act(h, 0), n, HID, true,
                     false, false, nullptr)))
@@ -765,6 +991,23 @@ int forward(ktg_learned *h, ktg_ctx *c, const SysView &S, float *s_out, bool kee
     if ((rc = dense(h, cell_act(h, LAYERS), HID, nullptr, L.P, 0, -1, h->p, n, PROJ, false, false,
                     false, nullptr)))
         return rc;
+    KTG_LCUDA(h, cudaGetLastError());
+    return KTG_OK;
+}
+
+// Forward pass to p and the entry values (t, s) of one axis system (the
+// learned sparse approximate inverse, system features as the trunk's input).
+int forward(ktg_learned *h, ktg_ctx *c, const SysView &S, float *s_out, bool keep_t) {
+    int rc;
+    const int64_t n = S.n, N = c->N;
+    if ((rc = reserve_work(h, n, N, S.m))) return rc;
+    const int tb = 256;
+    ktg::learned::k_logd_sum<<<std::min<int>(1024, (S.n + tb - 1) / tb + 1), tb, 0, h->stream>>>(
+        S.diag, S.n, h->dpart, h->ticket, h->scal + 0);
+    ktg::learned::k_features<<<(S.n + tb - 1) / tb, tb, 0, h->stream>>>(
+        S.rp, S.col, S.val, S.diag, c->pin_start, S.n, h->scal + 0, h->x);
+    h->launches += 2;
+    if ((rc = trunk_forward(h, c, n))) return rc;
     if (S.m > 0) {
         ktg::learned::k_head<<<(S.m + tb - 1) / tb, tb, 0, h->stream>>>(
             S.rp, S.col, S.val, S.diag, S.n, S.m, h->p, keep_t ? h->t : nullptr, s_out);
@@ -773,6 +1016,8 @@ int forward(ktg_learned *h, ktg_ctx *c, const SysView &S, float *s_out, bool kee
     KTG_LCUDA(h, cudaGetLastError());
     return KTG_OK;
 }
+
+int trunk_backward(ktg_learned *h, ktg_ctx *c, int64_t n);
 
 // Loss and gradients (accumulated into h->g, which the caller zeroes).
 int loss_grad(ktg_learned *h, ktg_ctx *c, int axis, uint64_t seed, double *loss) {
@@ -804,8 +1049,21 @@ int loss_grad(ktg_learned *h, ktg_ctx *c, int axis, uint64_t seed, double *loss)
     }
     ktg::learned::k_dp<<<nblk, tb, 0, h->stream>>>(S.rp, S.col, h->tr, S.n, h->dphi, h->p, h->dp);
     ++h->launches;
+    if ((rc = trunk_backward(h, c, S.n))) return rc;
+    double l = 0.0;
+    KTG_LCUDA(h, cudaMemcpyAsync(h->h_scal, h->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
+    l = h->h_scal[0];
+    if (loss) *loss = l;
+    return KTG_OK;
+}
+
+// Gradients of the trunk's parameters from dL/dp in h->dp (accumulated into
+// h->g), through the activations the last trunk_forward kept.
+int trunk_backward(ktg_learned *h, ktg_ctx *c, int64_t n) {
+    int rc;
     const Layout &L = h->L;
-    const int64_t n = S.n, N = c->N;
+    const int64_t N = c->N;
     // p = h3 P: dP = h3^T dp, dh = dp P^T
     if ((rc = wgrad(h, cell_act(h, LAYERS), HID, h->dp, nullptr, PROJ, n, L.P, -1))) return rc;
     if ((rc = dense(h, h->dp, PROJ, nullptr, L.P, 0, -1, h->dh, n, HID, false, true, false, nullptr)))
@@ -841,11 +1099,6 @@ int loss_grad(ktg_learned *h, ktg_ctx *c, int axis, uint64_t seed, double *loss)
     }
     // h0 = relu(x W_in + b_in)
     if ((rc = wgrad(h, h->x, NFEAT, h->dh, cell_act(h, 0), HID, n, L.W_in, L.b_in))) return rc;
-    double l = 0.0;
-    KTG_LCUDA(h, cudaMemcpyAsync(h->h_scal, h->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
-    l = h->h_scal[0];
-    if (loss) *loss = l;
     return KTG_OK;
 }
 
@@ -853,7 +1106,132 @@ int refresh_bf16(ktg_learned *h) {
     ktg::learned::k_to_bf16<<<static_cast<int>((h->L.total + 255) / 256), 256, 0, h->stream>>>(
         h->w, h->wh, h->L.total);
     ++h->launches;
+    ++h->version;
     KTG_LCUDA(h, cudaGetLastError());
+    return KTG_OK;
+}
+
+// ---- learned coarse vector ----------------------------------------------------
+
+int reserve_coarse(ktg_learned *h, int64_t n, int T) {
+    int rc;
+    if (n > h->cap_coarse) {
+        const int64_t c = std::max(n, h->cap_coarse * 3 / 2);
+        if ((rc = lalloc(h, &h->cu, c * HEAD_IN)) || (rc = lalloc(h, &h->chh, c * HEAD_H)) ||
+            (rc = lalloc(h, &h->co, c)) || (rc = lalloc(h, &h->cdz, c)) ||
+            (rc = lalloc(h, &h->cdhh, c * HEAD_H)) || (rc = lalloc(h, &h->cdo, c)) ||
+            (rc = lalloc(h, &h->czd, c)) || (rc = lalloc(h, &h->caz, c)))
+            return rc;
+        h->cap_coarse = c;
+        h->cap_vec = 0;
+    }
+    if (T > h->cap_vec) {
+        if ((rc = lalloc(h, &h->ce, h->cap_coarse * kMaxVec)) ||
+            (rc = lalloc(h, &h->ca, h->cap_coarse * kMaxVec)))
+            return rc;
+        h->cap_vec = kMaxVec;
+    }
+    if (!h->cscal && (rc = lalloc(h, &h->cscal, 4 + 3 * kMaxVec))) return rc;
+    return KTG_OK;
+}
+
+// The trunk on the netlist's topology features: h->p = embedding per cell.
+int topo_trunk(ktg_learned *h, ktg_ctx *c) {
+    const int64_t n = c->n;
+    int rc;
+    if ((rc = reserve_work(h, n, c->N, 0))) return rc;
+    if (n > 0) {
+        ktg::learned::k_topo_features<<<static_cast<int>((n + 255) / 256), 256, 0, h->stream>>>(
+            c->pin_start, c->pin_ref, c->net_start, c->net_mov, c->area,
+            static_cast<int32_t>(n), h->x);
+        ++h->launches;
+    }
+    return trunk_forward(h, c, n);
+}
+
+HeadArgs head_args(ktg_learned *h, const SysView &S, const float *p) {
+    HeadArgs A{};
+    A.rp = S.rp;
+    A.val = S.val;
+    A.diag = S.diag;
+    A.n = S.n;
+    A.logd_mean = h->scal + 0;
+    A.p = p;
+    A.w = h->w;
+    A.Wh = h->L.Wh;
+    A.bh = h->L.bh;
+    A.wz = h->L.wz;
+    A.bz = h->L.bz;
+    return A;
+}
+
+int logd_mean(ktg_learned *h, const SysView &S) {
+    const int tb = 256;
+    ktg::learned::k_logd_sum<<<std::min<int>(1024, (S.n + tb - 1) / tb + 1), tb, 0, h->stream>>>(
+        S.diag, S.n, h->dpart, h->ticket, h->scal + 0);
+    ++h->launches;
+    KTG_LCUDA(h, cudaGetLastError());
+    return KTG_OK;
+}
+
+// Projection loss of the host test vectors e [T x n] on the predicted z of
+// one axis and its gradient (accumulated into h->g).
+int coarse_loss_grad(ktg_learned *h, ktg_ctx *c, int axis, const double *e, int T,
+                     double *loss) {
+    SysView S;
+    int rc = sys_view(h, c, axis, &S);
+    if (rc) return rc;
+    const int64_t n = S.n;
+    if ((rc = reserve_coarse(h, n, T))) return rc;
+    if ((rc = topo_trunk(h, c))) return rc;
+    if ((rc = logd_mean(h, S))) return rc;
+    const int tb = 256, nb = static_cast<int>((n + tb - 1) / tb);
+    HeadArgs A = head_args(h, S, h->p);
+    A.u = h->cu;
+    A.hh = h->chh;
+    A.o = h->co;
+    A.zd = h->czd;
+    ktg::learned::k_coarse_head<<<nb, tb, 0, h->stream>>>(A);
+    KTG_LCUDA(h, cudaMemcpyAsync(h->ce, e, sizeof(double) * n * T, cudaMemcpyHostToDevice,
+                                 h->stream));
+    for (int t = 0; t < T; ++t)
+        ktg::learned::k_spmv_rows<<<nb, tb, 0, h->stream>>>(S.rp, S.col, S.val, S.diag, S.n,
+                                                            h->ce + t * n, h->ca + t * n);
+    ktg::learned::k_spmv_rows<<<nb, tb, 0, h->stream>>>(S.rp, S.col, S.val, S.diag, S.n, h->czd,
+                                                        h->caz);
+    ktg::learned::k_coarse_dots<<<std::min(nb, 512), tb, 0, h->stream>>>(
+        S.n, T, h->czd, h->caz, h->ca, h->ce, h->dpart, h->ticket, h->cscal);
+    ktg::learned::k_coarse_dz<<<nb, tb, 0, h->stream>>>(S.n, T, h->caz, h->ca, h->cscal, h->cdz);
+    ktg::learned::k_coarse_head_bwd<<<nb, tb, 0, h->stream>>>(
+        S.n, h->w, h->L.Wh, h->L.wz, h->chh, h->co, h->cdz, h->cdhh, h->cdo, h->dp);
+    h->launches += 5 + T;
+    const Layout &L = h->L;
+    if ((rc = wgrad(h, h->cu, HEAD_IN, h->cdhh, nullptr, HEAD_H, n, L.Wh, L.bh))) return rc;
+    if ((rc = wgrad(h, h->chh, HEAD_H, h->cdo, nullptr, 1, n, L.wz, L.bz))) return rc;
+    if ((rc = trunk_backward(h, c, n))) return rc;
+    KTG_LCUDA(h, cudaMemcpyAsync(h->h_scal, h->cscal, sizeof(double), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
+    if (loss) *loss = h->h_scal[0];
+    return KTG_OK;
+}
+
+int adam_step(ktg_learned *h) {
+    ktg::learned::k_sumsq<<<64, 256, 0, h->stream>>>(h->g, h->L.total, h->dpart, h->ticket, h->scal + 2);
+    KTG_LCUDA(h, cudaMemcpyAsync(h->h_scal + 2, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
+    const double gn = std::sqrt(h->h_scal[2]);
+    const float scale = gn > h->clip ? static_cast<float>(h->clip / gn) : 1.0f;
+    ++h->step;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, static_cast<float>(h->step));
+    const float c2 = 1.0f - std::pow(b2, static_cast<float>(h->step));
+    ktg::learned::k_adam<<<static_cast<int>((h->L.total + 255) / 256), 256, 0, h->stream>>>(
+        h->w, h->g, h->m1, h->m2, h->L.total, h->lr, b1, b2, 1e-8f, c1, c2, scale);
+    h->launches += 2;
+    int rc = refresh_bf16(h);
+    if (rc) return rc;
+    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
     return KTG_OK;
 }
 
@@ -905,6 +1283,9 @@ int ktg_learned_create(int device, uint64_t seed, ktg_learned **out) {
         fill(L.Wc[l], HID, HID, 1.0);
     }
     fill(L.P, HID, PROJ, 0.05);
+    fill(L.Wh, HEAD_IN, HEAD_H, 1.0);
+    fill(L.wz, HEAD_H, 1, 0.1);
+    w[L.bz] = static_cast<float>(kSoftplusInvOne);  // untrained head: z = 1 (constant)
     if (cudaMemcpy(h->w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(h->m1, 0, sizeof(float) * P) != cudaSuccess ||
         cudaMemset(h->m2, 0, sizeof(float) * P) != cudaSuccess ||
@@ -923,7 +1304,8 @@ void ktg_learned_destroy(ktg_learned *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->w, h->g, h->m1, h->m2, h->wh, h->x, h->act_c, h->act_n, h->p, h->dp,
                     h->dh, h->dh2, h->dg, h->dm, h->de, h->t, h->ds, h->dphi, h->tr, h->u,
-                    h->gq, h->wpart, h->dpart, h->ticket, h->scal};
+                    h->gq, h->wpart, h->dpart, h->ticket, h->scal, h->cu, h->chh, h->co,
+                    h->cdz, h->cdhh, h->cdo, h->czd, h->caz, h->ce, h->ca, h->cscal, h->pc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -977,23 +1359,83 @@ int ktg_learned_train_step(ktg_learned *h, ktg_ctx *c, int axis, uint64_t seed, 
     double l = 0.0;
     int rc = ktg_learned_loss_grad(h, c, axis, seed, &l, nullptr);
     if (rc) return rc;
-    // global-norm clipping
-    ktg::learned::k_sumsq<<<64, 256, 0, h->stream>>>(h->g, h->L.total, h->dpart, h->ticket, h->scal + 2);
-    KTG_LCUDA(h, cudaMemcpyAsync(h->h_scal + 2, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
-    const double gn = std::sqrt(h->h_scal[2]);
-    const float scale = gn > h->clip ? static_cast<float>(h->clip / gn) : 1.0f;
-    ++h->step;
-    const float b1 = 0.9f, b2 = 0.999f;
-    const float c1 = 1.0f - std::pow(b1, static_cast<float>(h->step));
-    const float c2 = 1.0f - std::pow(b2, static_cast<float>(h->step));
-    ktg::learned::k_adam<<<static_cast<int>((h->L.total + 255) / 256), 256, 0, h->stream>>>(
-        h->w, h->g, h->m1, h->m2, h->L.total, h->lr, b1, b2, 1e-8f, c1, c2, scale);
-    h->launches += 2;
-    rc = refresh_bf16(h);
-    if (rc) return rc;
-    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
+    if ((rc = adam_step(h))) return rc;  // global-norm clipped Adam
     if (loss) *loss = l;
+    return KTG_OK;
+}
+
+int ktg_learned_coarse_loss_grad(ktg_learned *h, ktg_ctx *c, int axis, const double *e,
+                                 int32_t num_vec, double *loss, float *grad) {
+    if (!h || !c || (axis != 0 && axis != 1) || !e || num_vec < 1 || num_vec > kMaxVec)
+        return KTG_ERR_ARG;
+    KTG_LCUDA(h, cudaSetDevice(h->device));
+    KTG_LCUDA(h, cudaStreamSynchronize(c->stream));
+    KTG_LCUDA(h, cudaMemsetAsync(h->g, 0, sizeof(float) * h->L.total, h->stream));
+    int rc = coarse_loss_grad(h, c, axis, e, num_vec, loss);
+    if (rc) return rc;
+    if (grad) KTG_LCUDA(h, cudaMemcpy(grad, h->g, sizeof(float) * h->L.total, cudaMemcpyDeviceToHost));
+    return KTG_OK;
+}
+
+int ktg_learned_coarse_train_step(ktg_learned *h, ktg_ctx *c, int axis, const double *e,
+                                  int32_t num_vec, double *loss) {
+    double l = 0.0;
+    int rc = ktg_learned_coarse_loss_grad(h, c, axis, e, num_vec, &l, nullptr);
+    if (rc) return rc;
+    if ((rc = adam_step(h))) return rc;
+    if (loss) *loss = l;
+    return KTG_OK;
+}
+
+int ktg_learned_prepare_coarse(ktg_learned *h, ktg_ctx *c) {
+    if (!h || !c) return KTG_ERR_ARG;
+    if (!c->have_system || !c->axis_valid[0] || !c->axis_valid[1] || c->sys_n != c->n)
+        return lerr(h, KTG_ERR_STATE, "context needs the B2B systems of its netlist");
+    KTG_LCUDA(h, cudaSetDevice(h->device));
+    const int64_t n = c->n;
+    if (c->coarse_z_cap < 2 * n) {  // grows once per netlist size (synchronising)
+        if (c->coarse_z_buf) cudaFree(c->coarse_z_buf);
+        c->coarse_z_buf = nullptr;
+        KTG_LCUDA(h, cudaMalloc(&c->coarse_z_buf, sizeof(float) * std::max<int64_t>(2 * n, 1)));
+        c->coarse_z_cap = 2 * n;
+    }
+    if (h->cap_pc < n) {
+        int rc = lalloc(h, &h->pc, std::max<int64_t>(n, 1) * PROJ);
+        if (rc) return rc;
+        h->cap_pc = n;
+        h->pc_ctx = nullptr;
+    }
+    // Everything below is enqueued on the context's stream.
+    cudaStream_t own = h->stream;
+    h->stream = c->stream;
+    int rc = KTG_OK;
+    if (h->pc_ctx != c || h->pc_gen != c->netlist_gen || h->pc_version != h->version) {
+        rc = topo_trunk(h, c);  // once per netlist and parameter set
+        if (!rc && n > 0 && cudaMemcpyAsync(h->pc, h->p, sizeof(float) * n * PROJ,
+                                            cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
+            rc = lerr(h, KTG_ERR_CUDA, "embedding copy failed");
+        if (!rc) {
+            h->pc_ctx = c;
+            h->pc_gen = c->netlist_gen;
+            h->pc_version = h->version;
+        }
+    }
+    for (int axis = 0; axis < 2 && !rc; ++axis) {
+        SysView S{c->sys[axis].row_ptr, c->sys[axis].col, c->sys[axis].val, c->sys[axis].diag,
+                  static_cast<int32_t>(n), 0};
+        if ((rc = logd_mean(h, S))) break;
+        HeadArgs A = head_args(h, S, h->pc);
+        A.zf = c->coarse_z_buf + axis * n;
+        if (n > 0) {
+            ktg::learned::k_coarse_head<<<static_cast<int>((n + 255) / 256), 256, 0, h->stream>>>(A);
+            ++h->launches;
+        }
+    }
+    h->stream = own;
+    if (rc) return rc;
+    KTG_LCUDA(h, cudaGetLastError());
+    c->coarse_z = c->coarse_z_buf;
+    c->coarse_z_ready = true;
     return KTG_OK;
 }
 

@@ -116,11 +116,44 @@ class Learned:
     def prepare(self, ctx: Context):
         self._check(self.lib.ktg_learned_prepare(self.h, ctx.h))
 
+    # -- learned coarse vector ---------------------------------------------------
+    def coarse_loss_grad(self, ctx: Context, axis: int, vectors):
+        """Projection loss of the test vectors ([T, n], T <= 4) on the
+        predicted coarse vector of one axis, and the parameter gradient."""
+        e = np.ascontiguousarray(np.atleast_2d(vectors), dtype=np.float64)
+        loss = ctypes.c_double()
+        g = np.zeros(self.num_params, np.float32)
+        self._check(self.lib.ktg_learned_coarse_loss_grad(
+            self.h, ctx.h, axis, ctypes.c_void_p(e.ctypes.data), e.shape[0], ctypes.byref(loss),
+            ctypes.c_void_p(g.ctypes.data)))
+        return float(loss.value), g
+
+    def coarse_train_step(self, ctx: Context, axis: int, vectors) -> float:
+        e = np.ascontiguousarray(np.atleast_2d(vectors), dtype=np.float64)
+        loss = ctypes.c_double()
+        self._check(self.lib.ktg_learned_coarse_train_step(
+            self.h, ctx.h, axis, ctypes.c_void_p(e.ctypes.data), e.shape[0], ctypes.byref(loss)))
+        return float(loss.value)
+
+    def prepare_coarse(self, ctx: Context):
+        """Coarse vectors of ctx's current systems for "coarse" = 3 (enqueued
+        on ctx's stream)."""
+        self._check(self.lib.ktg_learned_prepare_coarse(self.h, ctx.h))
+
+    prepare_coarse_dev = prepare_coarse
+
     def save(self, path: str):
         np.save(path, self.get_params())
 
     def load(self, path: str):
-        self.set_params(np.load(path))
+        w = np.load(path).astype(np.float32)
+        if w.shape[0] < self.num_params:
+            # weights saved before the coarse-vector head existed: keep the
+            # freshly initialised head (the constant coarse vector)
+            cur = self.get_params()
+            cur[:w.shape[0]] = w
+            w = cur
+        self.set_params(w)
 
 
 def train(learned: Learned, designs: Iterable, iters: int = 8, epochs: int = 2,
