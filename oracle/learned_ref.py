@@ -21,6 +21,13 @@ Network over the cell-net bipartite graph (mean aggregation), hidden 64:
         h   = relu(h Wb_l + g Wc_l + bb_l)
     p = h P                                                      P: 64 x 16
 Loss over K Rademacher probes v:  L = mean_k ||M A v_k - v_k||^2 / n.
+
+Learned coarse vector (the two-level aggregation preconditioner's z): the
+same trunk on features of the netlist alone (topo_features), then per system
+    u_i = (p_i, c_i, l_i),  c_i = sum_j |a_ij| / a_ii,  l_i = log a_ii - mean log a
+    z_i = softplus(relu(u_i Wh + bh) . wz + bz)
+and the projection loss of test vectors e_t on z in the A-inner product
+    L = mean_t (1 - (z^T A e_t)^2 / ((z^T A z)(e_t^T A e_t))).
 """
 from __future__ import annotations
 
@@ -36,6 +43,9 @@ for _l in range(LAYERS):
     PARAM_SHAPES += [(f"Wa{_l}", (HID, HID)), (f"ba{_l}", (HID,)), (f"Wb{_l}", (HID, HID)),
                      (f"Wc{_l}", (HID, HID)), (f"bb{_l}", (HID,))]
 PARAM_SHAPES += [("P", (HID, PROJ))]
+HEAD_IN = PROJ + 2
+HEAD_H = 16
+PARAM_SHAPES += [("Wh", (HEAD_IN, HEAD_H)), ("bh", (HEAD_H,)), ("wz", (HEAD_H,)), ("bz", (1,))]
 
 
 def num_params() -> int:
@@ -215,6 +225,13 @@ def loss_and_grad(params, s, nl, k: int = 4, seed: int = 0, graph: Graph | None 
     np.add.at(dp, rows, dphi[:, None] * p[cols] / 4.0)
     np.add.at(dp, cols, dphi[:, None] * p[rows] / 4.0)
     grads = {name: np.zeros(shape) for name, shape in PARAM_SHAPES}
+    trunk_backward(params, cache, graph, dp, grads)
+    return L, grads, sv
+
+
+def trunk_backward(params, cache, graph, dp, grads):
+    """Accumulates the trunk's parameter gradients from dL/dp."""
+    x = cache["x"]
     h = cache[f"h{LAYERS}"]
     grads["P"] = h.T @ dp
     dh = dp @ params["P"].T
@@ -235,17 +252,100 @@ def loss_and_grad(params, s, nl, k: int = 4, seed: int = 0, graph: Graph | None 
     dzin = dh * (cache["z_in"] > 0)
     grads["W_in"] = x.T @ dzin
     grads["b_in"] = dzin.sum(0)
-    return L, grads, sv
+
+
+def topo_features(nl) -> np.ndarray:
+    """Per-cell features of the netlist alone (no positions): 1, pins/8,
+    mean over the cell's nets of (movable pins - 1)/8, of fixed pins/4, share
+    of its nets with a fixed pin, mean 1/(degree - 1), log(area)/8,
+    log1p(pins)/2."""
+    n = nl.num_movable
+    N = nl.num_nets
+    deg = np.diff(nl.net_start).astype(np.float64)
+    pv = nl.var_of_vertex[nl.pin_cell]
+    net_of_pin = np.repeat(np.arange(N), np.diff(nl.net_start))
+    mov = np.bincount(net_of_pin[pv >= 0], minlength=N).astype(np.float64)
+    cell = np.repeat(np.arange(n), np.diff(nl.pin_start))
+    k = np.diff(nl.pin_start).astype(np.float64)
+    nets = nl.pin_net.astype(np.int64)
+    inv = np.where(k > 0, 1.0 / np.maximum(k, 1.0), 0.0)
+    smov = np.bincount(cell, weights=mov[nets] - 1.0, minlength=n)
+    sfix = np.bincount(cell, weights=deg[nets] - mov[nets], minlength=n)
+    anyfix = np.bincount(cell, weights=(deg[nets] > mov[nets]).astype(np.float64), minlength=n)
+    sinv = np.bincount(cell, weights=np.where(deg[nets] >= 2, 1.0 / np.maximum(deg[nets] - 1, 1),
+                                              0.0), minlength=n)
+    area = nl.width * nl.height
+    x = np.zeros((n, NFEAT))
+    x[:, 0] = 1.0
+    x[:, 1] = k / 8.0
+    x[:, 2] = smov * inv / 8.0
+    x[:, 3] = sfix * inv / 4.0
+    x[:, 4] = anyfix * inv
+    x[:, 5] = sinv * inv
+    x[:, 6] = np.where(area > 0, np.log(np.maximum(area, 1e-300)) / 8.0, 0.0)
+    x[:, 7] = np.log1p(k) / 2.0
+    return x
+
+
+def softplus(o):
+    return np.where(o > 20.0, o, np.log1p(np.exp(np.minimum(o, 20.0))))
+
+
+def coarse_head(params, p, s):
+    """z and the head's intermediates for one axis system."""
+    rows = rows_of(s)
+    n = s["diag"].shape[0]
+    d = s["diag"]
+    c = np.bincount(rows, weights=np.abs(s["val"]), minlength=n) / d
+    logd = np.log(d)
+    u = np.concatenate([p, c[:, None], (logd - logd.mean())[:, None]], axis=1)
+    zh = u @ params["Wh"] + params["bh"]
+    hh = relu(zh)
+    o = hh @ params["wz"] + params["bz"][0]
+    return softplus(o), dict(u=u, zh=zh, hh=hh, o=o)
+
+
+def coarse_loss_and_grad(params, s, nl, E, graph: Graph | None = None):
+    """Projection loss of the test vectors E [T, n] on the predicted coarse
+    vector of system s, and its analytic parameter gradients."""
+    graph = graph or Graph(nl)
+    x = topo_features(nl)
+    p, cache = forward(params, x, graph)
+    z, hc = coarse_head(params, p, s)
+    E = np.atleast_2d(E)
+    T = E.shape[0]
+    az = spmv(s, z)
+    q = float(z @ az)
+    A_e = np.stack([spmv(s, e) for e in E])
+    pt = A_e @ z
+    St = np.einsum("ij,ij->i", E, A_e)
+    L = float(np.mean(1.0 - pt * pt / (q * St)))
+    dz = np.zeros_like(z)
+    for t in range(T):
+        dz += -2.0 * pt[t] * A_e[t] / (T * q * St[t]) + 2.0 * pt[t] ** 2 * az / (T * q * q * St[t])
+    sig = np.where(hc["o"] > 20.0, 1.0, 1.0 / (1.0 + np.exp(-np.minimum(hc["o"], 20.0))))
+    do = dz * sig
+    grads = {name: np.zeros(shape) for name, shape in PARAM_SHAPES}
+    grads["wz"] = hc["hh"].T @ do
+    grads["bz"] = np.array([do.sum()])
+    dzh = np.outer(do, params["wz"]) * (hc["zh"] > 0)
+    grads["Wh"] = hc["u"].T @ dzh
+    grads["bh"] = dzh.sum(0)
+    dp = (dzh @ params["Wh"].T)[:, :PROJ]
+    trunk_backward(params, cache, graph, dp, grads)
+    return L, grads, z
 
 
 def init_params(seed: int = 0) -> dict:
     rng = np.random.default_rng(seed)
     out = {}
     for name, shape in PARAM_SHAPES:
-        if name.startswith("b"):
+        if name.startswith("b") or len(shape) == 1:
             out[name] = np.zeros(shape)
         else:
             fan = shape[0] + shape[1]
             scale = np.sqrt(2.0 / fan) * (0.05 if name == "P" else 1.0)
             out[name] = rng.standard_normal(shape) * scale
+    out["wz"] = rng.standard_normal(HEAD_H) * np.sqrt(2.0 / (HEAD_H + 1)) * 0.1
+    out["bz"] = np.array([0.5413248546129181])
     return out

@@ -111,3 +111,78 @@ def test_training_reduces_iterations(gpu_ctx):
         assert max(r["learned"]["resid"]) <= TOL * 1.0001
     assert lrn < jac, (lrn, jac)
     learned.close()
+
+
+def test_coarse_gradients_match_cpu_oracle(tiny, gpu_ctx):
+    """Learned coarse vector: the GPU's projection loss and parameter
+    gradient (trunk on topology features, head, loss, all hand-written
+    kernels, FP32 CUDA-core path) against the float64 oracle."""
+    from ktplace_b200.learned import Learned
+    raw, nl, x, y, ax, ay, alpha = tiny
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, alpha, ax, ay, fx, fy)
+    params = lr.init_params(5)
+    params["P"] *= 20.0
+    params["wz"] *= 10.0
+    flat = lr.flatten(params).astype(np.float32)
+    learned = Learned(0, seed=1)
+    learned.set_params(flat)
+    learned.set_option("tensor_cores", 0)
+    E = np.random.default_rng(3).standard_normal((2, nl.num_movable))
+    p32 = lr.unflatten(flat.astype(np.float64))
+    for axis in (0, 1):
+        s = gpu_ctx.system(axis)
+        L_ref, g_ref, _ = lr.coarse_loss_and_grad(p32, s, nl, E)
+        L_gpu, g_gpu = learned.coarse_loss_grad(gpu_ctx, axis, E)
+        assert abs(L_gpu - L_ref) <= 1e-4 * abs(L_ref), (L_gpu, L_ref)
+        gr = lr.flatten(g_ref)
+        assert rel(g_gpu.astype(np.float64), gr) <= 2e-3
+        for name, shape in lr.PARAM_SHAPES:
+            a = lr.unflatten(g_gpu.astype(np.float64))[name]
+            b = g_ref[name]
+            if np.linalg.norm(b) > 1e-4 * np.linalg.norm(gr):
+                assert rel(a, b) <= 1e-2, (axis, name, rel(a, b))
+    learned.close()
+
+
+def test_prepared_coarse_vector_matches_oracle(tiny, gpu_ctx):
+    """ktg_learned_prepare_coarse's z for both axes (permuted into the
+    aggregation order) against the oracle's head on the same parameters."""
+    from ktplace_b200.learned import Learned
+    raw, nl, x, y, ax, ay, alpha = tiny
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, alpha, ax, ay, fx, fy)
+    params = lr.init_params(6)
+    params["P"] *= 20.0
+    params["wz"] *= 10.0
+    flat = lr.flatten(params).astype(np.float32)
+    learned = Learned(0, seed=1)
+    learned.set_params(flat)
+    learned.set_option("tensor_cores", 0)
+    p32 = lr.unflatten(flat.astype(np.float64))
+    p, _ = lr.forward(p32, lr.topo_features(nl), lr.Graph(nl))
+    want = np.concatenate([lr.coarse_head(p32, p, gpu_ctx.system(a))[0] for a in (0, 1)])
+    gpu_ctx.set_option("precond", 2)
+    try:
+        learned.prepare_coarse(gpu_ctx)
+        gpu_ctx.set_option("coarse", 3)
+        got = gpu_ctx.coarse()
+        order = gpu_ctx.aggregates()["order"]
+        assert rel(got["z"].astype(np.float64), want[order]) <= 1e-4
+        r = gpu_ctx.solve_mixed(x, y, TOL)
+        sx = gpu_ctx.system(0)
+        assert true_resid_of(sx, r["x"]) <= TOL * 1.0001
+    finally:
+        gpu_ctx.set_option("coarse", 0)
+        gpu_ctx.set_option("precond", 0)
+        learned.close()
+
+
+def true_resid_of(s, v):
+    n = s["diag"].shape[0]
+    rows = np.repeat(np.arange(n), np.diff(s["row_ptr"]))
+    av = s["diag"] * v
+    np.add.at(av, rows, s["val"] * v[s["col"]])
+    return np.linalg.norm(s["rhs"] - av) / np.linalg.norm(s["rhs"])
