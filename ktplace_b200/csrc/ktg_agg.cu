@@ -30,6 +30,7 @@
 #include "ktg_agg.h"
 #include "ktg_common.cuh"
 #include "ktg_context.h"
+#include "ktg_spmv.cuh"
 
 #include <algorithm>
 
@@ -709,7 +710,7 @@ __global__ void k_plen(LevelView L, int32_t rows, const int32_t *order, int32_t 
 __global__ void k_pfill(LevelView L, int32_t rows, const int32_t *order, const int32_t *newpos,
                         const int32_t *prp, const double *rhs0, const double *rhs1,
                         int32_t *pcol, double *pval, float *pval32, double *pdiag,
-                        double *prhs) {
+                        double *prhs, int coarse_mode, const float *zin, double *zd) {
     const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= rows) return;
     const int32_t c = order[k];
@@ -721,6 +722,7 @@ __global__ void k_pfill(LevelView L, int32_t rows, const int32_t *order, const i
     double *dv = pval + prp[k] - r.e0;
     float *dv32 = pval32 + prp[k] - r.e0;
     int32_t e = r.e0;
+    double sabs = 0.0;  // sum of |a_ij| for the coupling-share coarse vector
     for (; e + 4 <= r.e1; e += 4) {
         int32_t col[4];
         double v[4];
@@ -732,6 +734,8 @@ __global__ void k_pfill(LevelView L, int32_t rows, const int32_t *order, const i
 #pragma unroll
         for (int q = 0; q < 4; ++q) col[q] = newpos[col[q] + off] - off;
 #pragma unroll
+        for (int q = 0; q < 4; ++q) sabs += fabs(v[q]);
+#pragma unroll
         for (int q = 0; q < 4; ++q) {
             dc[e + q] = col[q];
             dv[e + q] = v[q];
@@ -740,12 +744,18 @@ __global__ void k_pfill(LevelView L, int32_t rows, const int32_t *order, const i
     }
     for (; e < r.e1; ++e) {
         const double v = __ldg(r.val + e);
+        sabs += fabs(v);
         dc[e] = newpos[__ldg(r.col + e) + off] - off;
         dv[e] = v;
         dv32[e] = static_cast<float>(v);
     }
-    pdiag[k] = __ldg((y ? L.diag1 : L.diag0) + i);
+    const double d = __ldg((y ? L.diag1 : L.diag0) + i);
+    pdiag[k] = d;
     prhs[k] = __ldg((y ? rhs1 : rhs0) + i);
+    if (coarse_mode > 0)  // the coarse vector, rounded to FP32 as the solve uses it
+        zd[k] = coarse_mode == 1   ? 1.0
+                : coarse_mode == 2 ? static_cast<double>(static_cast<float>(sabs / d))
+                                   : static_cast<double>(__ldg(zin + c));
 }
 
 // Eight lanes per aggregate, lane m owning row m of the block: the block
@@ -929,7 +939,7 @@ __global__ void k_perm_out(int32_t rows, int32_t n, const int32_t *order, const 
 //           learned coarse vector).
 __global__ void k_coarse_z(int mode, int32_t rows, const int32_t *prp, const double *pval,
                            const double *pdiag, const int32_t *order, const float *zin,
-                           float2 *zaz) {
+                           double *zd) {
     const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= rows) return;
     float z = 1.0f;
@@ -940,29 +950,46 @@ __global__ void k_coarse_z(int mode, int32_t rows, const int32_t *prp, const dou
     } else if (mode == 3) {
         z = __ldg(zin + __ldg(order + k));
     }
-    zaz[k] = make_float2(z, 0.0f);
+    zd[k] = z;
 }
 
 // (A z)_k in FP64 (row sums of a Laplacian-like system cancel: the FP32
-// result keeps its relative precision only if it is formed in FP64), stored
-// beside z; block partials of z^T A z per axis, summed in block order by the
-// last block, which writes 1 / (z^T A z) (0 when not positive).
-__global__ void __launch_bounds__(256) k_coarse_az(int32_t rows, int32_t n, const int32_t *prp,
-                                                   const int32_t *pcol, const double *pval,
-                                                   const double *pdiag, float2 *zaz,
-                                                   double *part, unsigned *ticket, double *einv) {
+// result keeps its relative precision only if it is formed in FP64) as warp
+// tiles over the permuted system, stored with z as (z, A z) in FP32; block
+// partials of z^T A z per axis, summed in block order by the last block,
+// which writes 1 / (z^T A z) (0 when not positive).
+constexpr int kAzThreads = 256;
+__global__ void __launch_bounds__(kAzThreads)
+    k_coarse_az(const int32_t *__restrict__ prp, const int32_t *__restrict__ pcol,
+                const double *__restrict__ pval, const double *__restrict__ pdiag,
+                const double *__restrict__ zd, int32_t n, int32_t rows_total,
+                int32_t rows_per_block, float2 *__restrict__ zaz, double *part, unsigned *ticket,
+                double *einv) {
+    __shared__ __align__(16) double tilebuf[(kAzThreads / 32) * kTileChunk];
+    __shared__ int32_t wb[kAzThreads / 32 + 1];
     __shared__ double red[33 * 2];
-    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t r0 = static_cast<int32_t>(blockIdx.x) * rows_per_block;
+    const int32_t R = min(rows_per_block, rows_total - r0);
+    const int32_t base = __ldg(prp + r0);
+    warp_row_bounds(R, wb, [&](int32_t l) {
+        return int64_t(__ldg(prp + r0 + l)) - base + int64_t(kRowCost) * l;
+    });
     double e[2] = {0.0, 0.0};
-    if (k < rows) {
-        const int32_t off = k >= n ? n : 0;
-        const double zk = zaz[k].x;
-        double az = __ldg(pdiag + k) * zk;
-        for (int32_t q = __ldg(prp + k); q < __ldg(prp + k + 1); ++q)
-            az += __ldg(pval + q) * static_cast<double>(zaz[__ldg(pcol + q) + off].x);
-        zaz[k].y = static_cast<float>(az);
-        e[off ? 1 : 0] = zk * az;
-    }
+    warp_tile_spmv<double>(
+        r0, n, R, nullptr, wb, tilebuf,
+        [&](int pass, const int32_t *&trp, const int32_t *&tcol, const double *&tval,
+            const double *&tin) {
+            trp = prp + (pass ? n : 0);
+            tcol = pcol;
+            tval = pval;
+            tin = zd + (pass ? n : 0);
+        },
+        [&](int32_t l, int, int32_t) { return __ldg(pdiag + r0 + l) * __ldg(zd + r0 + l); },
+        [&](int32_t l, int axis, int32_t, double az) {
+            const double z = __ldg(zd + r0 + l);
+            zaz[r0 + l] = make_float2(static_cast<float>(z), static_cast<float>(az));
+            e[axis] += z * az;
+        });
     block_sum_k<2>(e, red);
     if (threadIdx.x == 0) {
         __stcg(part + 2 * blockIdx.x, e[0]);
@@ -1006,6 +1033,7 @@ int reserve(ktg_ctx *c, AggState *s, int64_t rows, int64_t nnz) {
             if ((rc = grow(c, p, rows))) return rc;
         if ((rc = grow(c, &s->minv, rows * kAggMax))) return rc;
         if ((rc = grow(c, &s->zaz, rows))) return rc;
+        if ((rc = grow(c, &s->zd, rows))) return rc;
         if ((rc = grow(c, &s->coarse_part, 2 * ((rows + kT - 1) / kT)))) return rc;
         s->tiles_cap = (std::max(rows, nnz) + kScanTile - 1) / kScanTile + 1;
         if ((rc = grow(c, &s->tile_sum, s->tiles_cap))) return rc;
@@ -1059,7 +1087,7 @@ void free_agg(ktg_ctx *c) {
                     (void *)s->pcol, (void *)s->pval, (void *)s->pval32, (void *)s->pdiag,
                     (void *)s->prhs, (void *)s->px, (void *)s->minv, (void *)s->meta,
                     (void *)s->blk_start, (void *)s->gslice, (void *)s->ea, (void *)s->eb,
-                    (void *)s->la, (void *)s->zaz, (void *)s->coarse_einv,
+                    (void *)s->la, (void *)s->zaz, (void *)s->zd, (void *)s->coarse_einv,
                     (void *)s->coarse_part, (void *)s->ticket})
         if (p) cudaFree(p);
     delete s;
@@ -1167,9 +1195,12 @@ int build_agg(ktg_ctx *c) {
     c->launches += 2;
     // prp: exclusive scan of the permuted row lengths (cnt[6] = R), total at prp[R]
     scan(c, s, s->prp, s->prp, cnt + 6, rows, s->prp + R);
+    // the coarse vector of the current mode comes with the permuted system
+    // (the learned one only when it is ready)
+    const int zmode = (c->coarse == 3 && !c->coarse_z_ready) ? 0 : c->coarse;
     k_pfill<<<gR, kT, 0, c->stream>>>(L0, R, s->order, s->newpos, s->prp, c->sys[0].rhs,
                                       c->sys[1].rhs, s->pcol, s->pval, s->pval32, s->pdiag,
-                                      s->prhs);
+                                      s->prhs, zmode, c->coarse_z, s->zd);
     k_blockinv<<<blocks_for(rows * kAggMax, 256), 256, 0, c->stream>>>(
         nagg, s->agg_start, size_old, static_cast<int32_t>(n), s->prp, s->pcol, s->pval, s->pdiag,
         s->minv, s->meta);
@@ -1177,6 +1208,8 @@ int build_agg(ktg_ctx *c) {
     KTG_CUDA(c, cudaGetLastError());
     s->blk_grid = 0;  // row ranges follow the new aggregates
     s->coarse_mode = 0;
+    s->z_mode = zmode;  // z of this mode is in s->zd; A z not formed yet
+    s->z_gen = c->coarse_z_gen;
     c->agg_ready = true;
     return KTG_OK;
 }
@@ -1188,19 +1221,30 @@ int agg_coarse_setup(ktg_ctx *c, int mode, const float *zin) {
     const int64_t rows = 2 * c->sys_n;
     if (!s || !c->agg_ready) return set_error(c, KTG_ERR_STATE, "no aggregates to correct");
     if (mode == 3 && !zin) return set_error(c, KTG_ERR_STATE, "no learned coarse vector");
-    if (s->coarse_mode == mode && mode != 3) return KTG_OK;
+    if (s->coarse_mode == mode && (mode != 3 || s->z_gen == c->coarse_z_gen)) return KTG_OK;
     if (rows == 0) {
         KTG_CUDA(c, cudaMemsetAsync(s->coarse_einv, 0, 2 * sizeof(double), c->stream));
         s->coarse_mode = mode;
         return KTG_OK;
     }
     const int32_t R = static_cast<int32_t>(rows), n = static_cast<int32_t>(c->sys_n);
-    const int g = blocks_for(rows, kT);
-    k_coarse_z<<<g, kT, 0, c->stream>>>(mode, R, s->prp, s->pval, s->pdiag, s->order, zin,
-                                        s->zaz);
-    k_coarse_az<<<g, kT, 0, c->stream>>>(R, n, s->prp, s->pcol, s->pval, s->pdiag, s->zaz,
-                                         s->coarse_part, s->ticket, s->coarse_einv);
-    c->launches += 2;
+    if (s->z_mode != mode || (mode == 3 && s->z_gen != c->coarse_z_gen)) {  // z is stale
+        k_coarse_z<<<blocks_for(rows, kT), kT, 0, c->stream>>>(mode, R, s->prp, s->pval, s->pdiag,
+                                                              s->order, zin, s->zd);
+        ++c->launches;
+        s->z_mode = mode;
+        s->z_gen = c->coarse_z_gen;
+    }
+    // one even wave of 256-thread blocks (6 per SM), at least 256 rows each
+    const int64_t slots = 6ll * c->num_sms;
+    const int32_t per = static_cast<int32_t>(std::max<int64_t>(256, (rows + slots - 1) / slots));
+    const int blocks = static_cast<int>((rows + per - 1) / per);
+    if (2 * blocks > 2 * ((rows + kT - 1) / kT))
+        return set_error(c, KTG_ERR_STATE, "coarse partials buffer too small");
+    k_coarse_az<<<blocks, kAzThreads, 0, c->stream>>>(s->prp, s->pcol, s->pval, s->pdiag, s->zd, n,
+                                                      R, per, s->zaz, s->coarse_part, s->ticket,
+                                                      s->coarse_einv);
+    ++c->launches;
     KTG_CUDA(c, cudaGetLastError());
     s->coarse_mode = mode;
     return KTG_OK;

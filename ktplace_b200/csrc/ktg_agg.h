@@ -41,6 +41,9 @@ struct AggState {
     // coarse correction (the mixed solve's u = B^-1 r + z c): per permuted row
     // (z, (A z)) in FP32, per axis 1 / (z^T A z) (0: no correction)
     float2 *zaz = nullptr;         // [2n]
+    double *zd = nullptr;          // [2n] z in FP64 (the SpMV's input)
+    int z_mode = 0;                // mode whose z is in zd (0: none)
+    int64_t z_gen = -1;            // learned coarse vector generation in zd (mode 3)
     double *coarse_einv = nullptr; // [2]
     double *coarse_part = nullptr; // [2 * blocks] per-block z^T A z
     unsigned *ticket = nullptr;    // last-block ticket of the coarse set-up

@@ -769,9 +769,12 @@ int ktg_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inner_t
         if ((rc = ktg::launch_solve_mixed(c, x, y, tol, inner_tol, max_inner, max_outer, mi,
                                           hist_x, hist_y, hist_cap)))
             return rc;
-        // FP64 pass: finishes a stalled axis, returns at once otherwise.
-        if ((rc = ktg::launch_solve(c, x, y, tol, max_inner, c->info_dev, nullptr, nullptr, 0)))
-            return rc;
+        // FP64 pass: finishes a stalled or unfinished axis; every block returns
+        // at once (before any work) when the mixed result says both converged.
+        c->pcg_gate = mi;
+        rc = ktg::launch_solve(c, x, y, tol, max_inner, c->info_dev, nullptr, nullptr, 0);
+        c->pcg_gate = nullptr;
+        if (rc) return rc;
         k_copy_fp64_iters<<<1, 1, 0, c->stream>>>(c->info_dev, mi);
         ++c->launches;
         KTG_CUDA(c, cudaGetLastError());

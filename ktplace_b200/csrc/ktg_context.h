@@ -103,9 +103,11 @@ struct ktg_ctx {
                                    // 1 constant, 2 coupling share, 3 learned
     const float *coarse_z = nullptr;  // learned coarse vector [2n] (combined natural order)
     bool coarse_z_ready = false;      // coarse_z belongs to the current systems
+    int64_t coarse_z_gen = 0;         // bumped whenever coarse_z is rewritten
     float *coarse_z_buf = nullptr;    // storage of the learned coarse vector
     int64_t coarse_z_cap = 0;
     int64_t netlist_gen = 0;          // bumped by every ktg_upload_netlist
+    const ktg_mixed_info *pcg_gate = nullptr;  // see PcgArgs::gate (ktg_pcg.cu)
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
     int64_t sys_cap_nnz = 0;  // allocated entries for col/val

@@ -1436,6 +1436,7 @@ int ktg_learned_prepare_coarse(ktg_learned *h, ktg_ctx *c) {
     KTG_LCUDA(h, cudaGetLastError());
     c->coarse_z = c->coarse_z_buf;
     c->coarse_z_ready = true;
+    ++c->coarse_z_gen;
     return KTG_OK;
 }
 

@@ -86,7 +86,31 @@ struct PcgArgs {
     double *prod;     // [3][total_rows], row index axis * n + i
     double *cpart;    // [6][nchunk]
     int32_t nchunk;   // ceil(n / kGrain)
+    // FP64 pass after a device-mode mixed solve: when this mixed result shows
+    // both axes converged and none stalled, the kernel returns at once
+    const ktg_mixed_info *gate;
 };
+
+// True (in every thread) when the gate says there is nothing left to solve;
+// block 0 then reports zero iterations with the mixed solve's residuals.
+__device__ __forceinline__ bool gated_off(const PcgArgs &A) {
+    if (!A.gate) return false;
+    const ktg_mixed_info g = *A.gate;
+    if (!(g.status == 0 && g.stalled == 0 && g.resid_x <= A.tol && g.resid_y <= A.tol))
+        return false;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ktg_solve_info inf;
+        inf.resid_x = g.resid_x;
+        inf.resid_y = g.resid_y;
+        inf.iters = 0;
+        inf.iters_x = 0;
+        inf.iters_y = 0;
+        inf.status = 0;
+        inf.live = 0;
+        *A.info = inf;
+    }
+    return true;
+}
 
 enum Slot { kBB = 0, kRZ0 = 1, kRR0 = 2, kPAP = 3, kRR = 4, kRZ = 5 };
 
@@ -252,6 +276,7 @@ constexpr int kTileWarps = kPcgThreads / 32;
 // the direct product; iterates agree to rounding.
 template <bool Smem, int Lanes, bool Exact = false, bool Rec = false>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
+    if (gated_off(A)) return;
     extern __shared__ __align__(16) double dyn[];
     __shared__ double scratch[33 * 4];
     __shared__ double exstage[Exact ? kStageSum : 1];  // reference-order sums
@@ -644,6 +669,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
 // match; p and x round exactly as in the reference, r through s.
 template <bool Smem, int Lanes>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
+    if (gated_off(A)) return;
     extern __shared__ __align__(16) double dyn[];
     __shared__ double scratch[33 * 4];
     __shared__ PcgAxis sax[2];
@@ -1053,6 +1079,7 @@ int launch_solve(ktg_ctx *c, double *x, double *y, double tol, int64_t max_iter,
     A.bar_gen = c->counters + 3;
     A.status = c->status;
     A.info = info_dev;
+    A.gate = c->pcg_gate;
     A.hist_x = hist_x;
     A.hist_y = hist_y;
     A.hist_cap = hist_cap;

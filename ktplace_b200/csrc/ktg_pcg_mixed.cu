@@ -23,6 +23,9 @@ namespace ktg {
 namespace {
 
 constexpr int kMixThreads = 1024;
+// An inner solve also stops once its residual is below kFinish * tol * ||b||:
+// the round then ends within the tolerance instead of over-solving.
+constexpr double kFinish = 0.5;
 constexpr int kMixSmemBytes = 216 * 1024;
 
 struct MixAxis {
@@ -243,7 +246,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed(MixArgs A) {
             for (int a = 0; a < 2; ++a) {
                 rho[a] = s[a * 2 + 0];
                 in_resid[a] = sqrt(s[a * 2 + 1]);
-                target[a] = A.inner_tol * r_norm[a];
+                target[a] = fmax(A.inner_tol * r_norm[a], kFinish * A.tol * b_norm[a]);
                 in_live[a] = live[a] && rho[a] > 0.0;
             }
         }
@@ -633,7 +636,10 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         // ---- inner FP32 PCG (Chronopoulos-Gear) -------------------------------
         bool in_live[2] = {live[0], live[1]}, first[2] = {true, true};
         double gamma_prev[2] = {0.0, 0.0}, alpha_prev[2] = {0.0, 0.0};
-        const double target[2] = {A.inner_tol * r_norm[0], A.inner_tol * r_norm[1]};
+        // inner stop: the round's reduction inner_tol, or as soon as the
+        // correction is good enough to finish (half the tolerance left over)
+        const double target[2] = {fmax(A.inner_tol * r_norm[0], kFinish * A.tol * b_norm[0]),
+                                  fmax(A.inner_tol * r_norm[1], kFinish * A.tol * b_norm[1])};
         for (;;) {
             // gamma, delta, rr, z.w per axis
             double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};

@@ -1,15 +1,18 @@
-"""Learned preconditioner: training data, training loop and evaluation.
+"""Learned networks of the mixed-precision solve: training data, training
+loops, the training-set file and evaluation.
 
-The network, its training and its use all run in the CUDA library
+The networks, their training and their use all run in the CUDA library
 (csrc/ktg_learned.cu, include/ktplace_b200.h); this module orchestrates them.
 
-Training systems come from a SimPL-style loop run on the GPU path itself:
-each iteration builds the B2B systems at the current lower-bound positions
-with anchors at a spread (upper-bound) placement and an anchor weight that
-grows linearly from 0.01 to 1.0 over 30 iterations, then solves them warm
-started. The spread placement is a 1-D area-proportional redistribution per
-axis (cells keep their order, their centres move to equal-area slots of the
-die), a stand-in for look-ahead legalization, which is not part of this path.
+Two uses of the same message-passing network over the cell-net graph:
+  * the learned coarse vector of the two-level aggregation preconditioner
+    ("coarse" = 3): trained on systems of the GPU SimPL loop
+    (simpl.GlobalLoop: B2B initial rounds, then global iterations anchored
+    at the look-ahead-legalized positions, ktg_lal), with test vectors taken
+    from the solves themselves (train_coarse, CoarseDataset);
+  * the learned sparse approximate inverse on A's pattern (precond 1), kept
+    for comparison; its training systems come from simpl_like_systems, whose
+    anchors are a 1-D area-proportional spread.
 """
 from __future__ import annotations
 
@@ -196,6 +199,171 @@ def compare_solvers(learned: Learned, ctx: Context, nl, x0, y0, iters: int, tol:
             if pre:
                 learned.prepare(ctx)
             row[name] = ctx.solve_mixed(x, y, tol, inner_tol)
+        ctx.set_option("precond", 0)
+        out.append(row)
+    return out
+
+
+# ---- learned coarse vector ----------------------------------------------------
+
+DATASET_MAGIC = b"KTGCOARS"
+DATASET_VERSION = 1
+_REC = np.dtype([("design", "<i4"), ("seed", "<i8"), ("cells", "<i8"), ("nets", "<i8"),
+                 ("iteration", "<i4"), ("alpha", "<f8"), ("n", "<i8"), ("nnz_x", "<i8"),
+                 ("nnz_y", "<i8"), ("fp64_iters_x", "<i4"), ("fp64_iters_y", "<i4"),
+                 ("agg_iters_x", "<i4"), ("agg_iters_y", "<i4"), ("loss_x", "<f8"),
+                 ("loss_y", "<f8"), ("system_sha", "S32"), ("solution_sha", "S32")])
+
+
+class CoarseDataset:
+    """The training set of the learned coarse vector as a versioned binary
+    file: the 8-byte magic KTGCOARS, a little-endian u32 version and u32
+    record count, then one fixed-size record per (A, b, x*) system. A record
+    names the system by how it is produced (training design index and
+    generator seed, SimPL global iteration, anchor weight: the GPU SimPL loop
+    is deterministic, so these regenerate the system exactly) and pins it by
+    SHA-256 digests of A, b (CSR, diag, rhs of both axes) and of the FP64
+    solution x*, beside its sizes, the FP64 and aggregation iteration counts
+    and the training loss of each axis. The arrays themselves are not stored
+    (a 2,000-system set of 5k-500k-cell netlists would take tens of GB)."""
+
+    def __init__(self):
+        self.records = []
+
+    def add(self, **fields):
+        self.records.append(fields)
+
+    def save(self, path: str):
+        arr = np.zeros(len(self.records), dtype=_REC)
+        for i, r in enumerate(self.records):
+            for k in _REC.names:
+                arr[i][k] = r[k]
+        with open(path, "wb") as f:
+            f.write(DATASET_MAGIC)
+            f.write(np.array([DATASET_VERSION, len(arr)], dtype="<u4").tobytes())
+            f.write(arr.tobytes())
+
+    @staticmethod
+    def load(path: str) -> np.ndarray:
+        with open(path, "rb") as f:
+            if f.read(8) != DATASET_MAGIC:
+                raise ValueError(f"{path}: not a coarse-vector training set")
+            version, count = np.frombuffer(f.read(8), dtype="<u4")
+            if version != DATASET_VERSION:
+                raise ValueError(f"{path}: version {version}, expected {DATASET_VERSION}")
+            return np.frombuffer(f.read(), dtype=_REC, count=int(count))
+
+
+def _sha(*arrays) -> bytes:
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.digest()
+
+
+def coarse_test_vectors(ctx: Context, x, y, xs, ys, ks=(4, 8), tol: float = 1e-6):
+    """Errors the aggregation-preconditioned FP32 PCG leaves after k inner
+    iterations from the warm start (x, y), against the FP64 solution (xs, ys):
+    the slow error components a coarse vector has to capture. Returns
+    ([T, n] for x, [T, n] for y) and the inner iterations of a full solve."""
+    ctx.set_option("precond", 2)
+    ctx.set_option("coarse", 0)
+    ex, ey = [], []
+    for k in ks:
+        r = ctx.solve_mixed(x, y, tol, 1e-3, max_inner=k)
+        ex.append(r["x"] - xs)
+        ey.append(r["y"] - ys)
+    full = ctx.solve_mixed(x, y, tol, 1e-3)
+    ctx.set_option("precond", 0)
+    return np.stack(ex), np.stack(ey), full["inner"]
+
+
+def coarse_training_systems(ctx: Context, nl, x0, y0, iters: int, init_rounds: int = 3,
+                            tol: float = 1e-6):
+    """Runs the GPU SimPL loop (simpl.GlobalLoop) on netlist nl and, after
+    every global iteration's build, yields (state, FP64 result, test vectors
+    per axis, aggregation inner iterations) while ctx holds that system."""
+    from . import grid as kgrid
+    from . import simpl
+    g = kgrid.build_grid(nl, kgrid.default_bins_per_axis(nl.num_movable), 1.0)
+    loop = simpl.GlobalLoop(ctx, nl, g, kgrid.build_free_space(nl), tol=tol)
+    x, y = loop.initial_rounds(x0, y0, init_rounds)
+    last = {}
+
+    def solve(px, py):
+        return last["x"], last["y"]
+
+    for st in loop.iterations(x, y, iters, solve=solve):
+        f = ctx.solve(st.x, st.y, tol, 100000)
+        last["x"], last["y"] = f["x"], f["y"]
+        ex, ey, agg_inner = coarse_test_vectors(ctx, st.x, st.y, f["x"], f["y"], tol=tol)
+        yield st, f, (ex, ey), agg_inner
+
+
+def train_coarse(learned: Learned, designs: Iterable, iters: int = 30, epochs: int = 1,
+                 ctx: Optional[Context] = None, dataset: Optional[CoarseDataset] = None,
+                 log=None) -> list:
+    """Trains the coarse-vector head and trunk: one Adam step per axis system
+    of every global iteration of the GPU SimPL loop on every design
+    ((netlist, x0, y0, seed) tuples). Returns the per-step losses; records
+    every system in `dataset` (first epoch) when given."""
+    own = ctx is None
+    ctx = ctx or Context(0)
+    if epochs > 1:
+        designs = list(designs)  # replayed; one epoch streams them
+    losses = []
+    for ep in range(epochs):
+        for d, (nl, x0, y0, seed) in enumerate(designs):
+            ctx.upload_netlist(nl)
+            for st, f, (ex, ey), agg_inner in coarse_training_systems(ctx, nl, x0, y0, iters):
+                lx = learned.coarse_train_step(ctx, 0, ex)
+                ly = learned.coarse_train_step(ctx, 1, ey)
+                losses += [lx, ly]
+                if dataset is not None and ep == 0:
+                    sx, sy = ctx.system(0), ctx.system(1)
+                    dataset.add(design=d, seed=seed, cells=nl.num_movable, nets=nl.num_nets,
+                                iteration=st.it, alpha=st.alpha, n=nl.num_movable,
+                                nnz_x=len(sx["val"]), nnz_y=len(sy["val"]),
+                                fp64_iters_x=f["iters_x"], fp64_iters_y=f["iters_y"],
+                                agg_iters_x=agg_inner[0], agg_iters_y=agg_inner[1],
+                                loss_x=lx, loss_y=ly,
+                                system_sha=_sha(*[sx[k] for k in ("row_ptr", "col", "val",
+                                                                  "diag", "rhs")],
+                                                *[sy[k] for k in ("row_ptr", "col", "val",
+                                                                  "diag", "rhs")]),
+                                solution_sha=_sha(f["x"], f["y"]))
+            if log:
+                log(f"epoch {ep} design {d} ({nl.num_movable} cells): "
+                    f"loss {np.mean(losses[-2 * iters:]):.4e}")
+    if own:
+        ctx.close()
+    return losses
+
+
+def compare_coarse(learned: Optional[Learned], ctx: Context, nl, x0, y0, iters: int,
+                   tol: float = 1e-6, init_rounds: int = 3) -> list:
+    """For each global iteration of the GPU SimPL loop, the aggregation mixed
+    solve of that iteration's systems with no coarse vector, the constant one
+    (the network switched off), the coupling share and the learned one, from
+    the same warm start: inner iterations, rounds and the true residuals."""
+    from . import grid as kgrid
+    from . import simpl
+    g = kgrid.build_grid(nl, kgrid.default_bins_per_axis(nl.num_movable), 1.0)
+    loop = simpl.GlobalLoop(ctx, nl, g, kgrid.build_free_space(nl), tol=tol)
+    x, y = loop.initial_rounds(x0, y0, init_rounds)
+    out = []
+    for st in loop.iterations(x, y, iters):
+        row = {"iteration": st.it}
+        ctx.set_option("precond", 2)
+        for name, mode in (("none", 0), ("constant", 1), ("coupling", 2), ("learned", 3)):
+            if mode == 3:
+                if learned is None:
+                    continue
+                learned.prepare_coarse(ctx)
+            ctx.set_option("coarse", mode)
+            row[name] = ctx.solve_mixed(st.x, st.y, tol, 1e-3)
+        ctx.set_option("coarse", 0)
         ctx.set_option("precond", 0)
         out.append(row)
     return out

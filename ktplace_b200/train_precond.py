@@ -1,7 +1,21 @@
-"""Trains the learned preconditioner and writes its weights.
+"""Trains the learned networks of the mixed solve and writes their weights.
+
+    python -m ktplace_b200.train_precond --coarse [--designs 64] [--iters 30]
+        [--min-cells 5000] [--max-cells 500000]
+        [--out ktplace_b200/weights/learned_coarse.npy]
+        [--dataset ktplace_b200/weights/coarse_dataset.bin]
+
+trains the learned coarse vector of the two-level aggregation preconditioner
+on the systems of the GPU SimPL loop (B2B initial rounds, then global
+iterations anchored at the look-ahead-legalized positions, anchor weight
+0.01 -> 1.0) of seeded synthetic netlists with log-uniform cell counts,
+designs x iters x 2 systems (3,840 with the defaults), and writes the
+training set's record file (learned.CoarseDataset) beside the weights.
 
     python -m ktplace_b200.train_precond [--designs 40] [--iters 25] [--epochs 3]
                                           [--out ktplace_b200/weights/learned_precond.npy]
+
+trains the learned sparse approximate inverse (precond 1):
 
 Training systems: the B2B x and y systems of every iteration of a SimPL-style
 run (ktplace_b200.learned.simpl_like_systems) on seeded synthetic netlists in
@@ -21,6 +35,31 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "weights", "learned_precond.npy")
+COARSE_OUT = os.path.join(HERE, "weights", "learned_coarse.npy")
+COARSE_DATASET = os.path.join(HERE, "weights", "coarse_dataset.bin")
+
+
+def coarse_designs(count: int, seed: int = 9000, min_cells: int = 5_000,
+                   max_cells: int = 500_000):
+    """Seeded synthetic netlists in the shape of the single-netlist and batch
+    configurations, cell counts log-uniform in [min_cells, max_cells];
+    yields (netlist, x0, y0, seed)."""
+    from . import synth, netlist
+    rng = np.random.default_rng(seed)
+    for k in range(count):
+        cells = int(round(math.exp(rng.uniform(math.log(min_cells), math.log(max_cells)))))
+        s = seed + k
+        spec = synth.SynthSpec(num_movable=cells, num_nets=int(cells * 1.05),
+                               num_pads=max(50, int(200 * math.sqrt(cells / 12_000))),
+                               num_rows=max(20, int(120 * math.sqrt(cells / 12_000))),
+                               utilization=0.6 if k % 2 else 0.7,
+                               num_macros=int(cells / 400) if k % 3 == 0 else 0,
+                               degree_exponent=synth.exponent_for_mean(3.5) if k % 2 else 2.5,
+                               seed=s, name=f"coarse{k}")
+        raw = synth.generate(spec)
+        nl = netlist.flatten(raw)
+        x0, y0 = synth.seed_positions(raw, nl.num_movable, s + 500)
+        yield nl, x0, y0, s
 
 
 def training_designs(count: int, seed: int = 7000, max_cells: int = 100_000):
@@ -52,8 +91,16 @@ def main(argv=None) -> int:
     ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--coarse", action="store_true",
+                    help="train the learned coarse vector instead of the approximate inverse")
+    ap.add_argument("--min-cells", type=int, default=5_000)
+    ap.add_argument("--max-cells", type=int, default=500_000)
+    ap.add_argument("--dataset", default=COARSE_DATASET)
     args = ap.parse_args(argv)
+    if args.coarse:
+        return main_coarse(args)
+    args.out = args.out or DEFAULT_OUT
     from .gpu import Context
     from .learned import Learned, train
     t0 = time.time()
@@ -72,6 +119,30 @@ def main(argv=None) -> int:
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     learned.save(args.out)
     print("wrote", args.out)
+    ctx.close()
+    learned.close()
+    return 0
+
+
+def main_coarse(args) -> int:
+    from .gpu import Context
+    from .learned import Learned, CoarseDataset, train_coarse
+    out = args.out or COARSE_OUT
+    learned = Learned(0, seed=args.seed)
+    learned.set_option("lr", args.lr)
+    ctx = Context(0)
+    ds = CoarseDataset()
+    t0 = time.time()
+    designs = coarse_designs(args.designs, min_cells=args.min_cells, max_cells=args.max_cells)
+    losses = train_coarse(learned, designs, iters=args.iters, epochs=1, ctx=ctx, dataset=ds,
+                          log=lambda m: print(m, f"({time.time() - t0:.0f}s)", flush=True))
+    k = max(1, len(losses) // 10)
+    print(f"{len(losses)} steps in {time.time() - t0:.1f}s; mean loss first tenth "
+          f"{np.mean(losses[:k]):.4e}, last tenth {np.mean(losses[-k:]):.4e}", flush=True)
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    learned.save(out)
+    ds.save(args.dataset)
+    print("wrote", out, "and", args.dataset, f"({len(ds.records)} systems)")
     ctx.close()
     learned.close()
     return 0
