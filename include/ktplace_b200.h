@@ -439,6 +439,16 @@ int ktg_download_aggregates(ktg_ctx *ctx, int32_t *order, int32_t *meta, float *
  * 0 when not positive). Any pointer may be NULL. Host memory. */
 int ktg_download_coarse(ktg_ctx *ctx, float *z, float *az, double *einv);
 
+/* Phase timestamps of the last mixed solve (no reference counterpart), for
+ * profiling: with ktg_set_option(ctx, "mixed_trace", cap) for cap > 0 block
+ * 0 of the Chronopoulos-Gear mixed kernel records up to cap words
+ * tag << 56 | %globaltimer ns at its phase boundaries (0 entry, 1 prologue
+ * done, 2 refinement round start, 3 round residual reduced, 4 inner SpMV and
+ * partials done, 5 scalars reduced, 6 inner iteration done, 7 exit); 0 turns
+ * it off. ktg_download_mixed_trace copies min(cap, capacity) words to host
+ * memory (unused words are 0). */
+int ktg_download_mixed_trace(ktg_ctx *ctx, uint64_t *out, int64_t cap);
+
 /* ---- Bookshelf reader ----------------------------------------------------
  * Reads a Bookshelf design directory <dir>/<name>.{nodes,wts,nets,pl,scl}
  * (name = the directory's own name, ".gz" variants read through zlib) with

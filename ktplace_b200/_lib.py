@@ -104,6 +104,7 @@ SIGNATURES = [
     ("ktg_set_option", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64]),
     ("ktg_download_aggregates", ctypes.c_int, [_vp, _i32p, _i32p, _f32p]),
     ("ktg_download_coarse", ctypes.c_int, [_vp, _f32p, _f32p, _f64p]),
+    ("ktg_download_mixed_trace", ctypes.c_int, [_vp, _vp, ctypes.c_int64]),
     ("ktg_bookshelf_read", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ktg_bookshelf_free", None, [_vp]),
     ("ktg_bookshelf_last_error", ctypes.c_char_p, []),

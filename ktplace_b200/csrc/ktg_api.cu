@@ -243,6 +243,7 @@ void ktg_destroy(ktg_ctx *c) {
     ktg::free_agg(c);
     ktg::free_lal(c);
     dev_free(c->coarse_z_buf);
+    dev_free(c->mixed_trace);
     dev_free(c->exact_prod);
     dev_free(c->exact_cpart);
     dev_free(c->partials);
@@ -304,6 +305,18 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
     if (k == "coarse") {
         if (value < 0 || value > 3) return set_error(c, KTG_ERR_ARG, "coarse must be 0, 1, 2 or 3");
         c->coarse = static_cast<int>(value);
+        return KTG_OK;
+    }
+    if (k == "mixed_trace") {  // capacity of the mixed solve's phase stamps (0: off)
+        if (value < 0 || value > (1 << 20)) return set_error(c, KTG_ERR_ARG, "mixed_trace range");
+        dev_free(c->mixed_trace);
+        c->mixed_trace_cap = 0;
+        if (value > 0) {
+            int rc = dev_alloc(c, &c->mixed_trace, value);
+            if (rc) return rc;
+            KTG_CUDA(c, cudaMemset(c->mixed_trace, 0, sizeof(unsigned long long) * value));
+            c->mixed_trace_cap = static_cast<int32_t>(value);
+        }
         return KTG_OK;
     }
     if (k == "pcg_form") {
@@ -843,6 +856,17 @@ int ktg_download_aggregates(ktg_ctx *c, int32_t *order, int32_t *meta, float *mi
             KTG_CUDA(c, cudaMemcpyAsync(minv, g->minv, sizeof(float) * 8 * rows,
                                         cudaMemcpyDeviceToHost, c->stream));
     }
+    return sync(c);
+}
+
+int ktg_download_mixed_trace(ktg_ctx *c, uint64_t *out, int64_t cap) {
+    if (!c || !out || cap < 0) return KTG_ERR_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int64_t k = std::min<int64_t>(cap, c->mixed_trace_cap);
+    if (k > 0)
+        KTG_CUDA(c, cudaMemcpyAsync(out, c->mixed_trace, sizeof(uint64_t) * k,
+                                    cudaMemcpyDeviceToHost, c->stream));
     return sync(c);
 }
 

@@ -108,6 +108,8 @@ struct ktg_ctx {
     int64_t coarse_z_cap = 0;
     int64_t netlist_gen = 0;          // bumped by every ktg_upload_netlist
     const ktg_mixed_info *pcg_gate = nullptr;  // see PcgArgs::gate (ktg_pcg.cu)
+    unsigned long long *mixed_trace = nullptr;  // phase stamps of the mixed solve (null: off)
+    int32_t mixed_trace_cap = 0;
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs
     int64_t sys_cap_nnz = 0;  // allocated entries for col/val

@@ -73,6 +73,9 @@ struct MixArgs {
     // and per axis 1 / (z^T A z) (0 turns the axis's correction off)
     const float2 *zaz;
     const double *coarse_einv;
+    // optional phase timestamps of block 0 (null: none): tag << 56 | %globaltimer
+    unsigned long long *trace;
+    int32_t trace_cap;
 };
 
 enum MixSlot { kTRR = 0, kTBB = 1, kIRZ0 = 2, kIPAP = 3, kIRR = 4, kIRZ = 5, kIZW = 6, kTZR = 7 };
@@ -456,6 +459,15 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     float *su = sr + cap, *sw = su + cap, *sp = sw + cap, *ss = sp + cap, *sdd = ss + cap;
     float2 *szaz = reinterpret_cast<float2 *>(sdd + cap);  // (z, A z) per row (coarse only)
     const int32_t n0 = sax[0].n;
+    // phase stamps (tags: 0 entry, 1 prologue done, 2 round start, 3 round's
+    // residual reduced, 4 SpMV + partials done, 5 scalars reduced, 6
+    // iteration done, 7 exit)
+    int32_t ntrace = 0;
+    auto stamp = [&](unsigned long long tag) {
+        if (A.trace && blockIdx.x == 0 && threadIdx.x == 0 && ntrace < A.trace_cap)
+            A.trace[ntrace++] = (tag << 56) | (global_timer_ns() & ((1ull << 56) - 1));
+    };
+    stamp(0);
     auto locate = [&](int32_t l, int &axis, int32_t &i) {
         const int32_t c = r0 + l;
         axis = c >= n0 ? 1 : 0;
@@ -546,7 +558,9 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     int32_t outer[2] = {0, 0};
     int64_t inner[2] = {0, 0};
 
+    stamp(1);
     for (int round = 0;; ++round) {
+        stamp(2);
         // ---- FP64 residual r = b - A x; r32, and u (Jacobi) or D^-1/2 r -----
         {
             // rr x, bb x, rr y, bb y, z.r x, z.r y
@@ -640,6 +654,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         // correction is good enough to finish (half the tolerance left over)
         const double target[2] = {fmax(A.inner_tol * r_norm[0], kFinish * A.tol * b_norm[0]),
                                   fmax(A.inner_tol * r_norm[1], kFinish * A.tol * b_norm[1])};
+        stamp(3);
         for (;;) {
             // gamma, delta, rr, z.w per axis
             double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -679,6 +694,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 const int ax[6] = {0, 0, 0, 1, 1, 1};
                 mstore<6>(A, a6, sl, ax, scratch);
             }
+            stamp(4);
             if (!sync()) return;
             float alpha[2] = {0.0f, 0.0f}, beta[2] = {0.0f, 0.0f};
             float cu_next[2] = {cu[0], cu[1]};
@@ -729,6 +745,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     }
                 }
             }
+            stamp(5);
             if (!(ok[0] || ok[1])) break;
             for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
                 int axis;
@@ -762,6 +779,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 cu[a] = cu_next[a];
             }
             if (!sync()) return;
+            stamp(6);
             if (pre) {
                 apply_m(ok);
                 if (!sync()) return;
@@ -781,6 +799,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
             if (live[a]) ++outer[a];
         if (!sync()) return;
     }
+    stamp(7);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ktg_mixed_info inf;
         inf.resid_x = true_resid[0];
@@ -841,6 +860,8 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     A.gslice = nullptr;
     A.zaz = nullptr;
     A.coarse_einv = nullptr;
+    A.trace = c->mixed_trace;
+    A.trace_cap = c->mixed_trace_cap;
     AggState *g = nullptr;
     if (agg) {
         if ((rc = agg_prepare_solve(c, grid, x, y, &A.rows_per_block))) return rc;

@@ -189,6 +189,14 @@ class Context:
                                                  einv.ctypes.data_as(P(ctypes.c_double))))
         return dict(z=z[:2 * n], az=az[:2 * n], einv=einv)
 
+    def mixed_trace(self, cap: int) -> np.ndarray:
+        """Phase stamps of the last mixed solve (option "mixed_trace"): rows
+        of (tag, ns)."""
+        w = np.zeros(cap, np.uint64)
+        self._check(self.lib.ktg_download_mixed_trace(self.h, ctypes.c_void_p(w.ctypes.data), cap))
+        w = w[w != 0]
+        return np.stack([w >> np.uint64(56), w & np.uint64((1 << 56) - 1)], 1).astype(np.int64)
+
     def system(self, axis: int) -> dict:
         n, m = self.system_info(axis)
         s = dict(row_ptr=np.zeros(n + 1, np.int64), col=np.zeros(max(m, 1), np.int32),
