@@ -42,6 +42,18 @@ GRID = 512
 MIXED_INNER_TOL = 1e-3
 WORKLOAD = ("simpl-global-iteration on synth211k (adaptec1-shaped): B2B build x+y (alpha 0.2), "
             "FP64 Jacobi-PCG x+y warm-start to rtol 1e-6, HPWL, 512x512 density+overflow")
+# The reference's own results for this workload (its CPU code, the --impl
+# reference arm: HPWL and scaled overflow of the step's solution); the GPU
+# arm's step is checked against them: HPWL within 1e-6 relative (the solve's
+# summation order differs, solutions agree to about 1e-9), overflow within
+# 1e-4 (a cell centre may land in a neighbouring bin).
+REFERENCE_RESULT = {"hpwl": 322413208.70273274, "overflow": 0.46628111185456594}
+
+
+def config_of(nl) -> dict:
+    """The workload's config, printed identically by both arms."""
+    return {"workload": WORKLOAD, "cells": nl.num_movable, "nets": nl.num_nets,
+            "pins": nl.num_pins, "grid": GRID}
 
 
 def parse():
@@ -151,8 +163,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, adaptec1 shape)",
-        "config": {"workload": WORKLOAD, "cells": nl.num_movable, "nets": nl.num_nets,
-                   "pins": nl.num_pins, "grid": GRID, "cg_iters": res["iters"]},
+        "config": config_of(nl),
+        "workload_detail": {"cg_iters": res["iters"]},
         "cpu_baseline": {"value": ms, "unit": UNIT, "cores": used, "kind": "reference",
                          "sample": f"{args.steps} full steps on {cpu_model()}"},
         "e2e": {"value": ms, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -329,6 +341,12 @@ def run_ours(args):
     solve_ms = [s_starts[k].elapsed_time(s_ends[k]) for k in range(args.steps)]
     total_ms = float(sum(step_ms))
     inf = SolveInfo.from_buffer_copy(bytes(info.cpu().numpy()))
+    result = {"hpwl": float(scal[0].item()), "overflow": float(scal[1].item())}
+    hrel = (result["hpwl"] - REFERENCE_RESULT["hpwl"]) / REFERENCE_RESULT["hpwl"]
+    oabs = result["overflow"] - REFERENCE_RESULT["overflow"]
+    result_check = {"hpwl_rel": hrel, "overflow_abs": oabs,
+                    "ok": bool(abs(hrel) <= 1e-6 and abs(oabs) <= 1e-4) if rank == 0 and
+                    nl.num_movable == 211000 else None}
     sx_n, sx_m = ctx.system_info(0)
     _, sy_m = ctx.system_info(1)
 
@@ -407,15 +425,21 @@ def run_ours(args):
                        "sample": f"{args.cpu_sample_steps} full steps of the same workload "
                                  f"(oracle/_ref, OpenMP on {cpu_model()})",
                        "cg_iters": res["iters"]}
+                t1, _, used1 = reference_steps(nl, x, y, ax, ay, 1, 1)
+                cpu["single_thread"] = {"value": 1000.0 * t1[0], "unit": UNIT, "cores": used1,
+                                        "sample": "1 full step of the same workload, 1 thread"}
+                oracle.set_ref_threads(threads)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": value * world,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, adaptec1 shape; 256 MiB L2 flush between steps)",
-            "config": {"workload": WORKLOAD, "cells": n, "nets": nl.num_nets,
-                       "pins": nl.num_pins, "nnz_x": sx_m, "nnz_y": sy_m, "grid": GRID,
-                       "cg_iters": int(inf.iters), "l2": "flushed between steps",
-                       "parallelism": f"replicas x{world} (independent netlists)"},
+            "config": config_of(nl),
+            "workload_detail": {"nnz_x": sx_m, "nnz_y": sy_m, "cg_iters": int(inf.iters),
+                                "l2": "flushed between steps",
+                                "parallelism": f"replicas x{world} (independent netlists)"},
+            "result": result,
+            "result_vs_reference": result_check,
             "breakdown": {"solve_ms": solve_med, "solve_ms_per_cg_iter": solve_med / inf.iters,
                           "other_ms": statistics.median(step_ms) - solve_med},
             "solve_variants": variants,

@@ -73,3 +73,38 @@ def test_exact_pcg_matches_live_reference_211k(max_iter, exact_form):
     k = r["iters"]
     assert np.array_equal(r["hist_x"][:k], rr["hist_x"][:k])
     assert np.array_equal(r["hist_y"][:k], rr["hist_y"][:k])
+
+
+def test_default_form_matches_live_reference_211k(gpu_ctx):
+    """The library's default solve (pcg_form 3, the fastest) on the 211k-cell
+    bench workload, run to full convergence (rtol 1e-6, no iteration cap),
+    against the reference's solveBothAxes run live on the same system: same
+    iteration count within one, solutions within 1e-9 relative, final
+    residuals within the tolerance; the step's HPWL and overflow match the
+    reference's."""
+    if not oracle.ref_available():
+        pytest.skip("reference library not built")
+    from ktplace_b200 import grid as kgrid
+    raw = synth.generate(synth.spec_adaptec1_like(1))
+    nl = netlist.flatten(raw)
+    x, y = synth.seed_positions(raw, nl.num_movable, 101)
+    ax, ay = synth.seed_positions(raw, nl.num_movable, 201)
+    ref = oracle.RefDesign.from_netlist(nl)
+    ref.build_b2b(x, y, 0.2, ax, ay)
+    rr = ref.solve(x, y, 1e-6, 100000)
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, 0.2, ax, ay, fx, fy)
+    r = gpu_ctx.solve(x, y, 1e-6, 100000)
+    assert abs(r["iters"] - rr["iters"]) <= 1, (r["iters"], rr["iters"])
+    for k in ("x", "y"):
+        err = np.linalg.norm(r[k] - rr[k]) / np.linalg.norm(rr[k])
+        assert err <= 1e-9, (k, err)
+    assert max(r["resid"]) <= 1e-6
+    h_ref = ref.hpwl(rr["x"], rr["y"])
+    assert abs(gpu_ctx.hpwl(r["x"], r["y"]) - h_ref) <= 1e-6 * h_ref
+    ref.grid(512, 1.0)
+    _, ov_ref = ref.occupancy_map(rr["x"], rr["y"], 512 * 512)
+    gpu_ctx.set_grid(kgrid.build_grid(nl, 512, 1.0))
+    _, ov = gpu_ctx.occupancy(r["x"], r["y"], want_map=False)
+    assert abs(ov - ov_ref) <= 1e-4
