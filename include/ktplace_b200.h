@@ -498,6 +498,11 @@ int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacl
  *                sums in order): solutions, iteration counts and residual
  *                histories are bit-identical to solveBothAxes (about 3x the
  *                time of form 3)
+ *   "hpwl_order" ktg_hpwl's sum of the (exact) per-net terms: 0 (default)
+ *                a block tree; 2 the reference's getDeterministicSum order
+ *                (simpl_parallel.h:35-51: chunks of 4,096 nets summed left to
+ *                right, then the chunk sums in order), bit-identical to
+ *                simplPlacer::Impl::getHpwl
  *   "precond"    0: Jacobi, 1: learned M (after ktg_learned_prepare),
  *                2: aggregation block-Jacobi, in ktg_solve_mixed
  *   "mixed_form" 1 (default): Chronopoulos-Gear mixed solve with per-block

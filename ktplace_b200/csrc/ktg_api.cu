@@ -244,6 +244,7 @@ void ktg_destroy(ktg_ctx *c) {
     ktg::free_lal(c);
     dev_free(c->coarse_z_buf);
     dev_free(c->mixed_trace);
+    dev_free(c->hpwl_terms);
     dev_free(c->exact_prod);
     dev_free(c->exact_cpart);
     dev_free(c->partials);
@@ -305,6 +306,11 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
     if (k == "coarse") {
         if (value < 0 || value > 3) return set_error(c, KTG_ERR_ARG, "coarse must be 0, 1, 2 or 3");
         c->coarse = static_cast<int>(value);
+        return KTG_OK;
+    }
+    if (k == "hpwl_order") {
+        if (value != 0 && value != 2) return set_error(c, KTG_ERR_ARG, "hpwl_order must be 0 or 2");
+        c->hpwl_order = static_cast<int>(value);
         return KTG_OK;
     }
     if (k == "mixed_trace") {  // capacity of the mixed solve's phase stamps (0: off)

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kBuildThreads)
                  uint32_t *__restrict__ lo_x, uint32_t *__restrict__ hi_x,
                  uint32_t *__restrict__ lo_y, uint32_t *__restrict__ hi_y,
                  double *__restrict__ partials, unsigned *__restrict__ ticket,
-                 double *__restrict__ hpwl_out) {
+                 double *__restrict__ hpwl_out, double *__restrict__ terms = nullptr) {
     __shared__ double scratch[40];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     double term = 0.0;
@@ -123,13 +123,41 @@ __global__ void __launch_bounds__(kBuildThreads)
         }
         // getHalfPerimeter: 0 for an empty box; nets with < 2 pins add 0.
         if (deg >= 2 && !(bx0 > bx1 || by0 > by1)) term = (bx1 - bx0) + (by1 - by0);
+        if (terms) terms[k] = term;
     }
+    if (terms) return;  // summed in the reference's order by k_hpwl_ref_order
     const double bs = block_sum(term, scratch);
     if (threadIdx.x == 0) __stcg(partials + blockIdx.x, bs);
     if (last_block_done(ticket)) {
         const double total = sum_partials(partials, gridDim.x, scratch);
         if (threadIdx.x == 0) *hpwl_out = total;
     }
+}
+
+// HPWL in the reference's summation order (getDeterministicSum,
+// simpl_parallel.h:35-51): the per-net terms in chunks of kGrain nets, each
+// chunk summed left to right by one thread, then the chunk sums in order.
+constexpr int64_t kGrain = 4096;
+__global__ void __launch_bounds__(1024)
+    k_hpwl_ref_order(const double *__restrict__ terms, int64_t N, double *__restrict__ out) {
+    __shared__ double chunk[1024];
+    const int64_t chunks = (N + kGrain - 1) / kGrain;
+    double total = 0.0;
+    for (int64_t c0 = 0; c0 < chunks; c0 += blockDim.x) {
+        const int64_t c = c0 + threadIdx.x;
+        double s = 0.0;
+        if (c < chunks) {
+            const int64_t e = min(N, (c + 1) * kGrain);
+            for (int64_t i = c * kGrain; i < e; ++i) s += terms[i];
+        }
+        chunk[threadIdx.x] = s;
+        __syncthreads();
+        const int64_t here = chunks - c0 < blockDim.x ? chunks - c0 : blockDim.x;
+        if (threadIdx.x == 0)
+            for (int64_t k = 0; k < here; ++k) total += chunk[k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = total;
 }
 
 // Edges of movable cell i's row on one axis, in the reference's order.
@@ -588,6 +616,21 @@ int launch_hpwl(ktg_ctx *c, const double *x, const double *y, double *out_dev) {
     }
     const NetlistDev nl = view_of(c);
     const int net_blocks = static_cast<int>((c->N + kBuildThreads - 1) / kBuildThreads);
+    if (c->hpwl_order == 2) {
+        if (c->hpwl_terms_cap < c->N) {
+            if (c->hpwl_terms) cudaFree(c->hpwl_terms);
+            c->hpwl_terms = nullptr;
+            KTG_CUDA(c, cudaMalloc(&c->hpwl_terms, sizeof(double) * c->N));
+            c->hpwl_terms_cap = c->N;
+        }
+        k_bound_pins<false><<<net_blocks, kBuildThreads, 0, c->stream>>>(
+            nl, x, y, nullptr, nullptr, nullptr, nullptr, c->partials, c->counters + 0, out_dev,
+            c->hpwl_terms);
+        k_hpwl_ref_order<<<1, 1024, 0, c->stream>>>(c->hpwl_terms, c->N, out_dev);
+        c->launches += 2;
+        KTG_CUDA(c, cudaGetLastError());
+        return KTG_OK;
+    }
     k_bound_pins<false><<<net_blocks, kBuildThreads, 0, c->stream>>>(
         nl, x, y, nullptr, nullptr, nullptr, nullptr, c->partials, c->counters + 0, out_dev);
     ++c->launches;

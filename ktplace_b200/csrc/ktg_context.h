@@ -109,6 +109,9 @@ struct ktg_ctx {
     int64_t netlist_gen = 0;          // bumped by every ktg_upload_netlist
     const ktg_mixed_info *pcg_gate = nullptr;  // see PcgArgs::gate (ktg_pcg.cu)
     unsigned long long *mixed_trace = nullptr;  // phase stamps of the mixed solve (null: off)
+    int hpwl_order = 0;               // 0 block tree, 2 the reference's chunked order
+    double *hpwl_terms = nullptr;     // per-net terms for hpwl_order 2
+    int64_t hpwl_terms_cap = 0;
     int32_t mixed_trace_cap = 0;
     int64_t sys_n = 0;        // rows of the current systems (n, or more after upload)
     int64_t sys_cap_n = 0;    // allocated rows for r/z/p/ap/diag/rhs

@@ -28,6 +28,7 @@
 #include "util/kt_log.h"
 
 #include "ktplace_b200.h"
+#include "simpl_hooks_b200.h"
 
 #include <algorithm>
 #include <cstdint>
@@ -50,6 +51,11 @@ struct GpuState {
     std::size_t devRows = 0;
     bool hostCsr = true;
     std::vector<double> histX, histY;
+    bool sizes = false;  // the uploaded netlist carries the cells' real sizes
+    // the bin grid installed for ktg_occupancy
+    std::size_t gridNx = 0, gridNy = 0;
+    double gridOx = 0.0, gridOy = 0.0, gridDx = 0.0, gridDy = 0.0, gridTotal = -1.0;
+    double gridLimit = -1.0;
 };
 
 GpuState &state() {
@@ -75,15 +81,20 @@ ktg_ctx *context() {
         s.hostCsr = !(csr != nullptr && std::string(csr) == "0");
         check("ktg_create", ktg_create(dev ? std::atoi(dev) : 0, &s.ctx));
         check("ktg_set_option", ktg_set_option(s.ctx, "pcg_form", form ? std::atoi(form) : 2));
+        const char *ho = std::getenv("KTPLACE_B200_HPWL_ORDER");
+        check("ktg_set_option", ktg_set_option(s.ctx, "hpwl_order", ho ? std::atoi(ho) : 2));
     }
     return s.ctx;
 }
 
-// SimPL's Netlist as the C ABI's structure of arrays (one-time per design).
-void ensureNetlist(const Netlist &nl) {
+// SimPL's Netlist as the C ABI's structure of arrays (one-time per design;
+// again once when the density hook first brings the cells' sizes).
+void ensureNetlist(const Netlist &nl, const std::vector<double> *width = nullptr,
+                   const std::vector<double> *height = nullptr) {
     GpuState &s = state();
     ktg_ctx *c = context();
-    if (s.netlist == &nl && s.netlistMovable == nl.numMovable && s.netlistNets == nl.nets.size())
+    if (s.netlist == &nl && s.netlistMovable == nl.numMovable && s.netlistNets == nl.nets.size() &&
+        (width == nullptr || s.sizes))
         return;
     const std::size_t V = nl.varOfVertex.size();
     const std::size_t n = nl.numMovable;
@@ -111,16 +122,20 @@ void ensureNetlist(const Netlist &nl) {
         pinNet[e] = static_cast<int32_t>(nl.pinsOfCell[e].net);
         pinQ[e] = static_cast<int32_t>(nl.pinsOfCell[e].pin);
     }
-    // Cell sizes are not part of Netlist; the density entry points take them
-    // from the placer's Design (simpl_dm.h), not from here. Unit sizes keep the
-    // upload valid for the assembly and solve.
+    // Cell sizes are not part of Netlist: the density hook hands over the
+    // placer's (Design::width/height); until then unit sizes keep the upload
+    // valid for the assembly and solve.
     std::vector<double> ones(std::max<std::size_t>(n, 1), 1.0);
+    const double *w = width ? width->data() : ones.data();
+    const double *h = height ? height->data() : ones.data();
     ktg_netlist_view view{static_cast<int64_t>(V), static_cast<int64_t>(n),
                           static_cast<int64_t>(nl.nets.size()), movVertex.data(), varOf.data(),
                           nl.fixedX.data(), nl.fixedY.data(), netStart.data(), pinCell.data(),
                           offX.data(), offY.data(), weight.data(), pinStart.data(), pinNet.data(),
-                          pinQ.data(), ones.data(), ones.data()};
+                          pinQ.data(), w, h};
     check("ktg_upload_netlist", ktg_upload_netlist(c, &view));
+    s.sizes = width != nullptr;
+    s.gridNx = s.gridNy = 0;  // the grid goes with the old upload
     s.netlist = &nl;
     s.netlistMovable = n;
     s.netlistNets = nl.nets.size();
@@ -226,5 +241,48 @@ Residuals solveBothAxes(const SparseSystem &sysX, std::vector<double> &x, const 
     }
     return Residuals(info.resid_x, info.resid_y);
 }
+
+namespace b200 {
+
+double hpwl(const Netlist &netlist, const std::vector<double> &x, const std::vector<double> &y) {
+    ensureNetlist(netlist);
+    ktg_ctx *c = state().ctx;
+    check("ktg_set_pointer_mode", ktg_set_pointer_mode(c, KTG_PTR_HOST));
+    double h = 0.0;
+    check("ktg_hpwl", ktg_hpwl(c, x.data(), y.data(), &h));
+    return h;
+}
+
+std::vector<double> occupancy(const Netlist &netlist, const std::vector<double> &width,
+                              const std::vector<double> &height, const BinGrid &grid,
+                              double densityLimit, const std::vector<double> &x,
+                              const std::vector<double> &y) {
+    GpuState &s = state();
+    ensureNetlist(netlist, &width, &height);
+    ktg_ctx *c = s.ctx;
+    if (s.gridNx != grid.nx || s.gridNy != grid.ny || s.gridOx != grid.origin.x ||
+        s.gridOy != grid.origin.y || s.gridDx != grid.dx || s.gridDy != grid.dy ||
+        s.gridTotal != grid.totalAvail || s.gridLimit != densityLimit) {
+        const ktg_grid_view g{grid.origin.x, grid.origin.y, grid.dx, grid.dy,
+                              static_cast<int64_t>(grid.nx), static_cast<int64_t>(grid.ny),
+                              grid.avail.data(), grid.totalAvail, densityLimit};
+        check("ktg_set_grid", ktg_set_grid(c, &g));
+        s.gridNx = grid.nx;
+        s.gridNy = grid.ny;
+        s.gridOx = grid.origin.x;
+        s.gridOy = grid.origin.y;
+        s.gridDx = grid.dx;
+        s.gridDy = grid.dy;
+        s.gridTotal = grid.totalAvail;
+        s.gridLimit = densityLimit;
+    }
+    check("ktg_set_pointer_mode", ktg_set_pointer_mode(c, KTG_PTR_HOST));
+    std::vector<double> occ(grid.size(), 0.0);
+    double overflow = 0.0;
+    check("ktg_occupancy", ktg_occupancy(c, x.data(), y.data(), occ.data(), &overflow));
+    return occ;
+}
+
+}  // namespace b200
 
 }  // namespace ktplace::simpl

@@ -152,3 +152,29 @@ def test_full_simpl_run_211k_identical():
     cx, cy = oracle.RefDesign.from_netlist(nl, "cpu").run_simpl()
     gx, gy = oracle.RefDesign.from_netlist(nl, "gpu").run_simpl()
     assert np.array_equal(cx, gx) and np.array_equal(cy, gy)
+
+
+@pytest.mark.parametrize("name", ["tiny_macros", "small12k"])
+def test_dropin_hooks_hpwl_occupancy_bit_exact(name):
+    """The reference's simplPlacer::Impl::getHpwl and getOccupancy
+    (simpl_placer.cc:256-289) with their bodies routed to the GPU hooks
+    (simpl_hooks_b200.h; the drop-in library's simpl_placer.cc is the
+    reference's with those two bodies replaced by oracle/hooks/
+    apply_hooks.py): the same HPWL, summed in the reference's order, and the
+    same occupancy map and overflow, bit for bit, on grids of 16 to 512 bins
+    per axis."""
+    raw, nl, x, y, ax, ay, alpha, bins = build_case(name)
+    cpu = oracle.RefDesign.from_netlist(nl, "cpu")
+    gpu = oracle.RefDesign.from_netlist(nl, "gpu")
+    rng = np.random.default_rng(11)
+    lx, ly, ux, uy = nl.die
+    for k in range(2):
+        px = x if k == 0 else lx + rng.random(nl.num_movable) * (ux - lx - nl.width)
+        py = y if k == 0 else ly + rng.random(nl.num_movable) * (uy - ly - nl.height)
+        assert gpu.hpwl(px, py) == cpu.hpwl(px, py)
+        for per_axis in (16, 512):
+            cpu.grid(per_axis, 1.0)
+            gpu.grid(per_axis, 1.0)
+            oc, vc = cpu.occupancy_map(px, py, per_axis * per_axis)
+            og, vg = gpu.occupancy_map(px, py, per_axis * per_axis)
+            assert np.array_equal(oc, og) and vc == vg, (name, k, per_axis)
