@@ -551,9 +551,14 @@ def solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, in
     return out
 
 
-SIMPL_VARIANTS = (("fp64_jacobi", None, 0), ("fp32_jacobi", 0, 0), ("fp32_aggregation", 2, 0),
-                  ("fp32_aggregation_coarse_const", 2, 1),
-                  ("fp32_aggregation_coarse_coupling", 2, 2))
+# (name, precond, coarse vector, agg_reuse): agg_reuse > 0 keeps an
+# aggregate structure across the run's builds, so that variant solves on a
+# context of its own whose aggregation history is only its own
+SIMPL_VARIANTS = (("fp64_jacobi", None, 0, 0), ("fp32_jacobi", 0, 0, 0),
+                  ("fp32_aggregation", 2, 0, 0), ("fp32_aggregation_coarse_const", 2, 1, 0),
+                  ("fp32_aggregation_coarse_coupling", 2, 2, 0),
+                  ("fp32_aggregation_coarse_coupling_reuse", 2, 2, 4),
+                  ("fp32_learned", 2, 3, 0), ("fp32_learned_reuse", 2, 3, 4))
 
 
 def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: int = 5,
@@ -578,6 +583,9 @@ def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: i
     ctx = Context(dev.index or 0)
     ctx.set_stream(stream.cuda_stream)
     ctx.upload_netlist(nl)
+    rctx = Context(dev.index or 0)  # the agg_reuse variants' own context
+    rctx.set_stream(stream.cuda_stream)
+    rctx.upload_netlist(nl)
     g = kgrid.build_grid(nl, kgrid.default_bins_per_axis(nl.num_movable), 1.0)
     loop = simpl.GlobalLoop(ctx, nl, g, kgrid.build_free_space(nl), tol=TOL, max_iter=MAX_ITER)
     with torch.cuda.stream(stream):
@@ -592,35 +600,47 @@ def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: i
     x, y = loop.initial_rounds(x0, y0, init_rounds)
     rows = []
     fx, fy = loop.fx, loop.fy
+    for vctx in (ctx, rctx):  # untimed: every solver's buffers allocated once
+        vctx.build_b2b(x, y, 0.0, None, None, fx, fy)
+        for pre, coarse in ((0, 0), (2, 2)):
+            vctx.set_option("precond", pre)
+            vctx.set_option("coarse", coarse)
+            vctx.solve_mixed(x, y, TOL, MIXED_INNER_TOL)
+        vctx.set_option("precond", 0)
+        vctx.set_option("coarse", 0)
+        vctx.solve(x, y, TOL, MAX_ITER)
     for st in loop.iterations(x, y, iters):
         row = {"it": st.it, "alpha": st.alpha}
         ref = None
-        for name, pre, coarse in variants:
+        for name, pre, coarse, reuse in variants:
             if coarse == 3 and learned is None:
                 continue
-            ctx.build_b2b(st.x, st.y, st.alpha, st.ux, st.uy, fx, fy)  # fresh systems
+            vctx = rctx if reuse else ctx
+            vctx.build_b2b(st.x, st.y, st.alpha, st.ux, st.uy, fx, fy)  # fresh systems
             with torch.cuda.stream(stream):
                 dx.copy_(torch.from_numpy(st.x))
                 dy.copy_(torch.from_numpy(st.y))
                 flush.zero_()
             torch.cuda.synchronize(dev)
             if pre is not None:
-                ctx.set_option("precond", pre)
-                ctx.set_option("coarse", coarse)
+                vctx.set_option("precond", pre)
+                vctx.set_option("coarse", coarse)
+                # the run's first global iteration builds its aggregates fresh
+                vctx.set_option("agg_reuse", reuse if st.it > 0 else 0)
             with torch.cuda.stream(stream):
                 e0.record(stream)
                 if coarse == 3:
-                    learned.prepare_coarse_dev(ctx)
+                    learned.prepare_coarse_dev(vctx)
                 if pre is None:
-                    ctx.solve_dev(dx, dy, TOL, MAX_ITER, info)
+                    vctx.solve_dev(dx, dy, TOL, MAX_ITER, info)
                 else:
-                    ctx.solve_mixed_dev(dx, dy, TOL, MIXED_INNER_TOL, MAX_ITER, 50, minfo)
+                    vctx.solve_mixed_dev(dx, dy, TOL, MIXED_INNER_TOL, MAX_ITER, 50, minfo)
                 e1.record(stream)
-                ctx.hpwl_dev(dx, dy, hp)
+                vctx.hpwl_dev(dx, dy, hp)
             e1.synchronize()
             ms = e0.elapsed_time(e1)
-            ctx.set_option("precond", 0)
-            ctx.set_option("coarse", 0)
+            vctx.set_option("precond", 0)
+            vctx.set_option("coarse", 0)
             sol = np.concatenate([dx.cpu().numpy(), dy.cpu().numpy()])
             h = float(hp.item())
             if pre is None:
@@ -639,6 +659,7 @@ def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: i
                              "hpwl_rel_vs_fp64": (h - ref[1]) / ref[1]}
         rows.append(row)
     ctx.close()
+    rctx.close()
     names = [v[0] for v in variants if v[0] in rows[0]]
     summary = {}
     base = sum(r["fp64_jacobi"]["ms"] for r in rows)

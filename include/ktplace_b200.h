@@ -498,6 +498,14 @@ int ktg_bookshelf_geometry(const ktg_bookshelf *b, double *die4, double *obstacl
  *                sums in order): solutions, iteration counts and residual
  *                histories are bit-identical to solveBothAxes (about 3x the
  *                time of form 3)
+ *   "agg_reuse"  K >= 0 (default 0): with the aggregation preconditioner, up
+ *                to K builds in a row of the same netlist keep the last full
+ *                build's aggregates and row order and only take the new
+ *                values (permuted system, block inverses, coarse vector),
+ *                skipping the matching and coarsening; the next build after
+ *                K such builds, or after a new netlist, rebuilds everything.
+ *                For SimPL's sequence of systems (one build per global
+ *                iteration), whose couplings change little between builds.
  *   "hpwl_order" ktg_hpwl's sum of the (exact) per-net terms: 0 (default)
  *                a block tree; 2 the reference's getDeterministicSum order
  *                (simpl_parallel.h:35-51: chunks of 4,096 nets summed left to

@@ -1191,8 +1191,44 @@ int build_agg(ktg_ctx *c) {
     const int32_t *nagg = cnt + kLevels;
     scan(c, s, size_old, s->agg_start, nagg, rows, cnt + 5);
     k_newpos<<<gR, kT, 0, c->stream>>>(R, s->cur, s->pos, s->agg_start, s->newpos, s->order);
+    ++c->launches;
+    KTG_CUDA(c, cudaGetLastError());
+    s->final_size = size_old;
+    s->struct_rows = rows;
+    s->struct_gen = c->netlist_gen;
+    s->blk_grid = 0;  // row ranges follow the new aggregates
+    s->builds_on_struct = 0;
+    return build_agg_values(c);
+}
+
+// The numeric part for the current systems on the aggregates in place
+// (the row order, the aggregates' sizes and starts): the permuted system and
+// its FP32 copy, the block inverses and the coarse vector's z.
+int build_agg_values(ktg_ctx *c) {
+    AggState *s = c->agg;
+    const int64_t n = c->sys_n;
+    const int64_t rows = 2 * n;
+    const int32_t R = static_cast<int32_t>(rows);
+    if (rows == 0) {
+        c->agg_ready = true;
+        return KTG_OK;
+    }
+    const int gR = blocks_for(rows, kT);
+    LevelView L0{};
+    L0.fine = true;
+    L0.n = static_cast<int32_t>(n);
+    L0.rp0 = c->sys[0].row_ptr;
+    L0.rp1 = c->sys[1].row_ptr;
+    L0.col0 = c->sys[0].col;
+    L0.col1 = c->sys[1].col;
+    L0.val0 = c->sys[0].val;
+    L0.val1 = c->sys[1].val;
+    L0.diag0 = c->sys[0].diag;
+    L0.diag1 = c->sys[1].diag;
+    int32_t *cnt = s->counts;
+    const int32_t *nagg = cnt + kLevels;
     k_plen<<<gR, kT, 0, c->stream>>>(L0, R, s->order, s->prp);
-    c->launches += 2;
+    ++c->launches;
     // prp: exclusive scan of the permuted row lengths (cnt[6] = R), total at prp[R]
     scan(c, s, s->prp, s->prp, cnt + 6, rows, s->prp + R);
     // the coarse vector of the current mode comes with the permuted system
@@ -1202,16 +1238,30 @@ int build_agg(ktg_ctx *c) {
                                       c->sys[1].rhs, s->pcol, s->pval, s->pval32, s->pdiag,
                                       s->prhs, zmode, c->coarse_z, s->zd);
     k_blockinv<<<blocks_for(rows * kAggMax, 256), 256, 0, c->stream>>>(
-        nagg, s->agg_start, size_old, static_cast<int32_t>(n), s->prp, s->pcol, s->pval, s->pdiag,
-        s->minv, s->meta);
+        nagg, s->agg_start, s->final_size, static_cast<int32_t>(n), s->prp, s->pcol, s->pval,
+        s->pdiag, s->minv, s->meta);
     c->launches += 2;
     KTG_CUDA(c, cudaGetLastError());
-    s->blk_grid = 0;  // row ranges follow the new aggregates
     s->coarse_mode = 0;
     s->z_mode = zmode;  // z of this mode is in s->zd; A z not formed yet
     s->z_gen = c->coarse_z_gen;
     c->agg_ready = true;
     return KTG_OK;
+}
+
+// The aggregation preconditioner for the current systems: the whole build,
+// or, with the "agg_reuse" option K > 0, the numeric part alone on the
+// aggregates of an earlier build of the same netlist for up to K builds in a
+// row (SimPL's systems change little from one global iteration to the next;
+// the cell grouping stays good while the values are taken afresh).
+int prepare_agg(ktg_ctx *c) {
+    AggState *s = c->agg;
+    const bool reuse = c->agg_reuse > 0 && s && s->struct_rows == 2 * c->sys_n &&
+                       s->struct_gen == c->netlist_gen && s->builds_on_struct < c->agg_reuse &&
+                       s->cap_nnz >= 2 * c->sys_cap_nnz;
+    if (!reuse) return build_agg(c);
+    ++s->builds_on_struct;
+    return build_agg_values(c);
 }
 
 // The coarse vector of `mode` (1, 2, or 3 with zin) for the current

@@ -43,6 +43,12 @@ struct AggState {
     float2 *zaz = nullptr;         // [2n]
     double *zd = nullptr;          // [2n] z in FP64 (the SpMV's input)
     int z_mode = 0;                // mode whose z is in zd (0: none)
+    // aggregate structure of the last full build: sizes buffer, rows and
+    // netlist it belongs to, later builds that reused it
+    const int32_t *final_size = nullptr;
+    int64_t struct_rows = -1;
+    int64_t struct_gen = -1;
+    int builds_on_struct = 0;
     int64_t z_gen = -1;            // learned coarse vector generation in zd (mode 3)
     double *coarse_einv = nullptr; // [2]
     double *coarse_part = nullptr; // [2 * blocks] per-block z^T A z

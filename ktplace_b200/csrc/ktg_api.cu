@@ -308,6 +308,11 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         c->coarse = static_cast<int>(value);
         return KTG_OK;
     }
+    if (k == "agg_reuse") {
+        if (value < 0 || value > 1000000) return set_error(c, KTG_ERR_ARG, "agg_reuse range");
+        c->agg_reuse = static_cast<int>(value);
+        return KTG_OK;
+    }
     if (k == "hpwl_order") {
         if (value != 0 && value != 2) return set_error(c, KTG_ERR_ARG, "hpwl_order must be 0 or 2");
         c->hpwl_order = static_cast<int>(value);

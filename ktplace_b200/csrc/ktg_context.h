@@ -99,6 +99,7 @@ struct ktg_ctx {
     int precond = 0;             // 0 Jacobi, 1 learned, 2 aggregation (ktg_set_option "precond")
     ktg::AggState *agg = nullptr;  // aggregation preconditioner of the current systems
     bool agg_ready = false;        // agg holds aggregates of the current systems
+    int agg_reuse = 0;             // aggregation: builds that may reuse the last structure
     int coarse = 0;                // coarse vector of the aggregation solve: 0 none,
                                    // 1 constant, 2 coupling share, 3 learned
     const float *coarse_z = nullptr;  // learned coarse vector [2n] (combined natural order)
@@ -183,6 +184,8 @@ int build_star(ktg_ctx *ctx, int64_t *size_out, int (*reserve)(ktg_ctx *, int64_
 // Aggregation preconditioner (ktg_agg.cu): build for the current systems,
 // per-solve set-up (block row ranges, permuted positions) and write-back.
 int build_agg(ktg_ctx *ctx);
+int build_agg_values(ktg_ctx *ctx);
+int prepare_agg(ktg_ctx *ctx);
 int agg_prepare_solve(ktg_ctx *ctx, int grid, const double *x, const double *y, int32_t *rows_cap);
 int agg_finish_solve(ktg_ctx *ctx, double *x, double *y);
 double *agg_global_slices(ktg_ctx *ctx, int64_t doubles);

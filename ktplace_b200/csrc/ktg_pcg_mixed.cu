@@ -835,7 +835,7 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
     const bool agg = c->precond == 2;
     const bool learned = c->precond == 1 && c->precond_ready;
     int rc = KTG_OK;
-    if (agg && !c->agg_ready && (rc = build_agg(c))) return rc;
+    if (agg && !c->agg_ready && (rc = prepare_agg(c))) return rc;
     if (!agg && !c->val32_valid) {
         for (int a = 0; a < 2; ++a) {
             int32_t m = 0;

@@ -136,3 +136,37 @@ def test_coarse_on_simpl_systems(coarse_ctx):
         assert inner[1] < inner[0], inner
         saved += inner[0] - inner[1]
     assert saved > 0
+
+
+def test_agg_reuse_on_simpl_systems(gpu_ctx):
+    """agg_reuse: along a SimPL run the aggregates of a full build serve the
+    next builds (only the values are taken afresh). Every solve still meets
+    the FP64 tolerance on the true residual and agrees with the FP64 solve,
+    and the inner iterations stay within a third of the fresh builds'."""
+    from ktplace_b200.gpu import Context
+    fresh, reused = 0, 0
+    with Context(0) as other:
+        other.set_option("precond", 2)
+        other.set_option("coarse", 2)
+        other.set_option("agg_reuse", 3)
+        gpu_ctx.set_option("precond", 2)
+        gpu_ctx.set_option("coarse", 2)
+        try:
+            for nl, st in simpl_systems(gpu_ctx, 8):
+                if other.nl is not nl:
+                    other.upload_netlist(nl)
+                fx, fy = nl.floors()
+                other.build_b2b(st.x, st.y, st.alpha, st.ux, st.uy, fx, fy)
+                sx, sy = other.system(0), other.system(1)
+                r = other.solve_mixed(st.x, st.y, TOL)
+                f = gpu_ctx.solve_mixed(st.x, st.y, TOL)
+                assert true_resid(sx, r["x"]) <= TOL * 1.0001
+                assert true_resid(sy, r["y"]) <= TOL * 1.0001
+                for k in ("x", "y"):
+                    assert np.linalg.norm(r[k] - f[k]) / np.linalg.norm(f[k]) <= SOL_RTOL
+                fresh += sum(f["inner"])
+                reused += sum(r["inner"])
+        finally:
+            gpu_ctx.set_option("coarse", 0)
+            gpu_ctx.set_option("precond", 0)
+    assert reused <= 1.34 * fresh, (reused, fresh)
