@@ -704,191 +704,176 @@ __global__ void k_plen(LevelView L, int32_t rows, const int32_t *order, int32_t 
     plen[k] = r.e1 - r.e0;
 }
 
-// One thread per permuted row (several rows' gathers in flight per warp):
-// columns renumbered (per-axis local), values in FP64 and FP32, diag and rhs
-// moved.
-__global__ void k_pfill(LevelView L, int32_t rows, const int32_t *order, const int32_t *newpos,
-                        const int32_t *prp, const double *rhs0, const double *rhs1,
-                        int32_t *pcol, double *pval, float *pval32, double *pdiag,
-                        double *prhs, int coarse_mode, const float *zin, double *zd) {
-    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+// The permuted system as warp tiles: a warp takes 32 consecutive permuted
+// rows, whose entries are consecutive in the output; the lanes walk those
+// entries 32 at a time (each lane finding its row by a search over the
+// warp's exclusive row offsets), so the writes are coalesced and the reads
+// stream each source row. Columns renumbered (per-axis local), values in FP64
+// and FP32; diag, rhs and the coarse vector's z by the row's own lane (z of
+// mode 2 sums the row's |a_ij| in storage order).
+constexpr int kPfWarps = 8;
+__global__ void __launch_bounds__(32 * kPfWarps)
+    k_pfill_tiles(LevelView L, int32_t rows, const int32_t *__restrict__ order,
+                  const int32_t *__restrict__ newpos, const int32_t *__restrict__ prp,
+                  const double *__restrict__ rhs0, const double *__restrict__ rhs1,
+                  int32_t *__restrict__ pcol, double *__restrict__ pval,
+                  float *__restrict__ pval32, double *__restrict__ pdiag,
+                  double *__restrict__ prhs, int coarse_mode, const float *__restrict__ zin,
+                  double *__restrict__ zd) {
+    const int lane = threadIdx.x & 31;
+    const int32_t k0 = (static_cast<int32_t>(blockIdx.x) * kPfWarps + (threadIdx.x >> 5)) * 32;
+    if (k0 >= rows) return;  // whole warp
+    const int32_t k = k0 + lane;
+    int32_t c = 0, e0 = 0, len = 0;
+    bool yax = false;
+    if (k < rows) {
+        c = __ldg(order + k);
+        const RowRef r = row_of(L, c);
+        e0 = r.e0;
+        len = r.e1 - r.e0;
+        yax = r.off != 0;
+    }
+    int32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int32_t excl = incl - len;
+    const int32_t T = __shfl_sync(0xffffffffu, incl, 31);
+    const int32_t dst0 = __shfl_sync(0xffffffffu, k < rows ? __ldg(prp + k) : 0, 0);
+    for (int32_t t0 = 0; t0 < T; t0 += 32) {
+        const int32_t t = t0 + lane;
+        int row = 0;  // the last lane whose exclusive offset is <= t
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cand = row + step;
+            const int32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+            if (cand < 32 && ex <= t) row = cand;
+        }
+        const int32_t re0 = __shfl_sync(0xffffffffu, e0, row);
+        const int32_t rex = __shfl_sync(0xffffffffu, excl, row);
+        const bool ry = __shfl_sync(0xffffffffu, yax, row);
+        if (t < T) {
+            const int32_t e = re0 + (t - rex);
+            const int32_t off = ry ? L.n : 0;
+            const int32_t *col = ry ? L.col1 : L.col0;
+            const double *val = ry ? L.val1 : L.val0;
+            const double v = __ldg(val + e);
+            pcol[dst0 + t] = newpos[__ldg(col + e) + off] - off;
+            pval[dst0 + t] = v;
+            pval32[dst0 + t] = static_cast<float>(v);
+        }
+    }
     if (k >= rows) return;
-    const int32_t c = order[k];
-    const bool y = c >= L.n;
+    const bool y = yax;
     const int32_t i = y ? c - L.n : c;
-    const RowRef r = row_of(L, c);
-    const int32_t off = y ? L.n : 0;
-    int32_t *dc = pcol + prp[k] - r.e0;
-    double *dv = pval + prp[k] - r.e0;
-    float *dv32 = pval32 + prp[k] - r.e0;
-    int32_t e = r.e0;
-    double sabs = 0.0;  // sum of |a_ij| for the coupling-share coarse vector
-    for (; e + 4 <= r.e1; e += 4) {
-        int32_t col[4];
-        double v[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            col[q] = __ldg(r.col + e + q);
-            v[q] = __ldg(r.val + e + q);
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) col[q] = newpos[col[q] + off] - off;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) sabs += fabs(v[q]);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            dc[e + q] = col[q];
-            dv[e + q] = v[q];
-            dv32[e + q] = static_cast<float>(v[q]);
-        }
-    }
-    for (; e < r.e1; ++e) {
-        const double v = __ldg(r.val + e);
-        sabs += fabs(v);
-        dc[e] = newpos[__ldg(r.col + e) + off] - off;
-        dv[e] = v;
-        dv32[e] = static_cast<float>(v);
-    }
     const double d = __ldg((y ? L.diag1 : L.diag0) + i);
     pdiag[k] = d;
     prhs[k] = __ldg((y ? rhs1 : rhs0) + i);
-    if (coarse_mode > 0)  // the coarse vector, rounded to FP32 as the solve uses it
-        zd[k] = coarse_mode == 1   ? 1.0
-                : coarse_mode == 2 ? static_cast<double>(static_cast<float>(sabs / d))
-                                   : static_cast<double>(__ldg(zin + c));
+    if (coarse_mode > 0) {  // the coarse vector, rounded to FP32 as the solve uses it
+        double z = 1.0;
+        if (coarse_mode == 2) {
+            const double *val = y ? L.val1 : L.val0;
+            double sabs = 0.0;
+            for (int32_t e = e0; e < e0 + len; ++e) sabs += fabs(__ldg(val + e));
+            z = static_cast<double>(static_cast<float>(sabs / d));
+        } else if (coarse_mode == 3) {
+            z = static_cast<double>(__ldg(zin + c));
+        }
+        zd[k] = z;
+    }
 }
 
-// Eight lanes per aggregate, lane m owning row m of the block: the block
-// row from the permuted CSR, a row-oriented Cholesky B = L L^T in FP64 with
-// the finished rows broadcast by shuffles (one division per pivot), L^-1 by
-// forward substitution and inv = L^-T L^-1, written as 8 floats per row. All arrays are indexed by
-// compile-time constants, so they stay in registers.
-__global__ void __launch_bounds__(256) k_blockinv(const int32_t *count, const int32_t *agg_start,
-                                                  const int32_t *size, int32_t n,
-                                                  const int32_t *prp, const int32_t *pcol,
-                                                  const double *pval, const double *pdiag,
-                                                  float *minv, int32_t *meta) {
-    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int32_t J = static_cast<int32_t>(t / kAggMax);
-    const int m = threadIdx.x & (kAggMax - 1);
-    const bool validJ = J < *count;
-    int32_t first = 0;
-    int k = 1;
-    if (validJ) {
-        first = agg_start[J];
-        k = size[J];
-    }
-    const bool act = validJ && m < k;
+// One thread per aggregate: its block of A (the aggregate's rows and
+// columns, duplicates summed in storage order after the diagonal) in the
+// thread's shared-memory slot, an FP64 Cholesky B = L L^T (row by row, one
+// reciprocal per pivot), L^-1 by forward substitution and B^-1 = L^-T L^-1,
+// written as 8 FP32 per row (zero past the aggregate's size). A non-positive
+// pivot gives the aggregate the inverse of its diagonal instead. The slot
+// stride of 65 doubles keeps a half-warp's 64-bit accesses on distinct banks.
+constexpr int kInvThreads = 64;
+constexpr int kSlot = kAggMax * kAggMax + 1;
+__global__ void __launch_bounds__(kInvThreads)
+    k_blockinv_slots(const int32_t *count, const int32_t *__restrict__ agg_start,
+                     const int32_t *__restrict__ size, int32_t n, const int32_t *__restrict__ prp,
+                     const int32_t *__restrict__ pcol, const double *__restrict__ pval,
+                     const double *__restrict__ pdiag, float *__restrict__ minv,
+                     int32_t *__restrict__ meta) {
+    __shared__ double slots[kInvThreads * kSlot];
+    const int32_t J = static_cast<int32_t>(blockIdx.x) * kInvThreads + threadIdx.x;
+    if (J >= *count) return;
+    double *B = slots + threadIdx.x * kSlot;  // B[r * 8 + c]
+    const int32_t first = __ldg(agg_start + J);
+    const int k = __ldg(size + J);
     const int32_t first_l = first >= n ? first - n : first;
-    double l[kAggMax];
-#pragma unroll
-    for (int q = 0; q < kAggMax; ++q) l[q] = 0.0;
-    if (act) {
+    for (int q = 0; q < kAggMax * kAggMax; ++q) B[q] = 0.0;
+    for (int m = 0; m < k; ++m) {
         const int32_t row = first + m;
-        const double d = pdiag[row];
-#pragma unroll
-        for (int q = 0; q < kAggMax; ++q)
-            if (q == m) l[q] += d;
-        const int32_t e0 = prp[row], e1 = prp[row + 1];
-        int32_t e = e0;
-        for (; e + 4 <= e1; e += 4) {
-            int32_t qe[4];
-            double v[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                qe[u] = pcol[e + u] - first_l;
-                v[u] = pval[e + u];
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int32_t qq = qe[u] < k ? qe[u] : -1;
-#pragma unroll
-                for (int q = 0; q < kAggMax; ++q) l[q] += q == qq ? v[u] : 0.0;
-            }
-        }
-        for (; e < e1; ++e) {
-            const int32_t qe = pcol[e] - first_l;
-            const int32_t qq = qe < k ? qe : -1;
-            const double v = pval[e];
-#pragma unroll
-            for (int q = 0; q < kAggMax; ++q) l[q] += q == qq ? v : 0.0;
+        double *Bm = B + m * kAggMax;
+        Bm[m] += __ldg(pdiag + row);
+        const int32_t e1 = __ldg(prp + row + 1);
+        for (int32_t e = __ldg(prp + row); e < e1; ++e) {
+            const int32_t qe = __ldg(pcol + e) - first_l;
+            if (qe >= 0 && qe < k) Bm[qe] += __ldg(pval + e);
         }
     }
-    // Cholesky: after step j, lane j holds L[j][0..j] and lanes i > j hold L[i][j];
-    // one reciprocal per pivot (rinv = 1 / L[m][m] kept by lane m).
+    // Cholesky in place: L[r][c] for c <= r overwrites B[r][c]
     bool ok = true;
-    double rinv = 1.0;
-#pragma unroll
-    for (int j = 0; j < kAggMax; ++j) {
-        if (m == j && act) {
-            double s = l[j];
-#pragma unroll
-            for (int q = 0; q < j; ++q) s -= l[q] * l[q];
-            ok = s > 0.0;
-            l[j] = ok ? sqrt(s) : 1.0;
-            rinv = 1.0 / l[j];
-        }
-        double rj[kAggMax];
-#pragma unroll
-        for (int q = 0; q < j; ++q) rj[q] = __shfl_sync(0xffffffffu, l[q], j, kAggMax);
-        const double rjinv = __shfl_sync(0xffffffffu, rinv, j, kAggMax);
-        if (act && m > j && j < k) {
-            double u = l[j];
-#pragma unroll
-            for (int q = 0; q < j; ++q) u -= l[q] * rj[q];
-            l[j] = u * rjinv;
+    double rinv[kAggMax];
+    for (int j = 0; j < k && ok; ++j) {
+        double *Bj = B + j * kAggMax;
+        double sj = Bj[j];
+        for (int q = 0; q < j; ++q) sj -= Bj[q] * Bj[q];
+        ok = sj > 0.0;
+        if (!ok) break;
+        Bj[j] = sqrt(sj);
+        rinv[j] = 1.0 / Bj[j];
+        for (int i = j + 1; i < k; ++i) {
+            double *Bi = B + i * kAggMax;
+            double u = Bi[j];
+            for (int q = 0; q < j; ++q) u -= Bi[q] * Bj[q];
+            Bi[j] = u * rinv[j];
         }
     }
-    const unsigned bad = __ballot_sync(0xffffffffu, !ok);
-    const bool group_ok = ((bad >> (threadIdx.x & 31 & ~(kAggMax - 1))) & 0xffu) == 0u;
-    // L^-1, row m in li; acc[c] = sum over finished rows t < m of L[m][t] Li[t][c]
-    double li[kAggMax], acc[kAggMax];
-#pragma unroll
-    for (int q = 0; q < kAggMax; ++q) {
-        li[q] = 0.0;
-        acc[q] = 0.0;
-    }
-#pragma unroll
-    for (int r = 0; r < kAggMax; ++r) {
-        if (m == r && act) {
-#pragma unroll
-            for (int c = 0; c <= r; ++c) li[c] = ((c == r ? 1.0 : 0.0) - acc[c]) * rinv;
+    float *dst = minv + static_cast<size_t>(first) * kAggMax;
+    if (!ok) {
+        for (int m = 0; m < k; ++m) {
+            for (int q = 0; q < kAggMax; ++q)
+                dst[m * kAggMax + q] = q == m ? static_cast<float>(1.0 / __ldg(pdiag + first + m))
+                                              : 0.0f;
+            meta[first + m] = first_l * kAggMax + (k - 1);
         }
-        double rt[kAggMax];
-#pragma unroll
-        for (int c = 0; c <= r; ++c) rt[c] = __shfl_sync(0xffffffffu, li[c], r, kAggMax);
-        if (act && m > r && r < k) {
-#pragma unroll
-            for (int c = 0; c <= r; ++c) acc[c] += l[r] * rt[c];
+        return;
+    }
+    // L^-1 (lower) into the upper triangle's mirror: Li[r][c] kept at B[c][r]
+    // for c < r (the strict upper part, free after the factorisation) and the
+    // diagonal rinv
+    for (int r = 0; r < k; ++r) {
+        for (int c2 = 0; c2 < r; ++c2) {
+            double acc = 0.0;  // sum_{t = c2}^{r-1} L[r][t] Li[t][c2]
+            for (int t = c2; t < r; ++t)
+                acc += B[r * kAggMax + t] * (t == c2 ? rinv[c2] : B[c2 * kAggMax + t]);
+            B[c2 * kAggMax + r] = -acc * rinv[r];
         }
     }
-    // inv row m = sum over t of Li[t][m] * Li[t][.]
-    double inv[kAggMax];
-#pragma unroll
-    for (int q = 0; q < kAggMax; ++q) inv[q] = 0.0;
-#pragma unroll
-    for (int r = 0; r < kAggMax; ++r) {
-        double rt[kAggMax];
-#pragma unroll
-        for (int c = 0; c <= r; ++c) rt[c] = __shfl_sync(0xffffffffu, li[c], r, kAggMax);
-        if (act && r < k) {
-            double tm = 0.0;
-#pragma unroll
-            for (int c = 0; c <= r; ++c)
-                if (c == m) tm = rt[c];
-#pragma unroll
-            for (int c = 0; c <= r; ++c) inv[c] += tm * rt[c];
+    // B^-1[i][c] = sum_{t >= max(i, c)} Li[t][i] Li[t][c]
+    for (int m = 0; m < k; ++m) {
+        for (int q = 0; q < kAggMax; ++q) {
+            float v = 0.0f;
+            if (q < k) {
+                double acc = 0.0;
+                for (int t = m > q ? m : q; t < k; ++t) {
+                    const double a = t == m ? rinv[m] : B[m * kAggMax + t];
+                    const double b = t == q ? rinv[q] : B[q * kAggMax + t];
+                    acc += a * b;
+                }
+                v = static_cast<float>(acc);
+            }
+            dst[m * kAggMax + q] = v;
         }
+        meta[first + m] = first_l * kAggMax + (k - 1);
     }
-    if (!act) return;
-    float *dst = minv + static_cast<size_t>(first + m) * kAggMax;
-    const double dm = group_ok ? 0.0 : 1.0 / pdiag[first + m];
-#pragma unroll
-    for (int q = 0; q < kAggMax; ++q) {
-        const double v = group_ok ? inv[q] : (q == m ? dm : 0.0);
-        dst[q] = q < k ? static_cast<float>(v) : 0.0f;
-    }
-    meta[first + m] = first_l * kAggMax + (k - 1);
 }
 
 // blk_start[b] = first aggregate start >= b * ceil(rows / grid).
@@ -1234,10 +1219,10 @@ int build_agg_values(ktg_ctx *c) {
     // the coarse vector of the current mode comes with the permuted system
     // (the learned one only when it is ready)
     const int zmode = (c->coarse == 3 && !c->coarse_z_ready) ? 0 : c->coarse;
-    k_pfill<<<gR, kT, 0, c->stream>>>(L0, R, s->order, s->newpos, s->prp, c->sys[0].rhs,
-                                      c->sys[1].rhs, s->pcol, s->pval, s->pval32, s->pdiag,
-                                      s->prhs, zmode, c->coarse_z, s->zd);
-    k_blockinv<<<blocks_for(rows * kAggMax, 256), 256, 0, c->stream>>>(
+    k_pfill_tiles<<<blocks_for(rows, 32 * kPfWarps), 32 * kPfWarps, 0, c->stream>>>(
+        L0, R, s->order, s->newpos, s->prp, c->sys[0].rhs, c->sys[1].rhs, s->pcol, s->pval,
+        s->pval32, s->pdiag, s->prhs, zmode, c->coarse_z, s->zd);
+    k_blockinv_slots<<<blocks_for(rows, kInvThreads), kInvThreads, 0, c->stream>>>(
         nagg, s->agg_start, s->final_size, static_cast<int32_t>(n), s->prp, s->pcol, s->pval,
         s->pdiag, s->minv, s->meta);
     c->launches += 2;
