@@ -399,8 +399,9 @@ def run_ours(args):
             coarse_net.close()
 
     batch_line = None
-    if world == 1 and not args.no_batch:
-        batch_line = run_batch_leg(torch, dev, stream, max(3, args.steps // 10))
+    if not args.no_batch:  # every rank takes the same steps (barriers, the max reduction)
+        batch_line = run_batch_leg(torch, dev, stream, max(3, args.steps // 10), rank, world,
+                                   dist)
 
     # ---- max over ranks --------------------------------------------------------
     vals = torch.tensor([total_ms, float(np.mean(e2e_ms)) * args.steps], dtype=torch.float64,
@@ -873,66 +874,101 @@ def bookshelf_leg(raw, cpu: bool) -> dict:
     return out
 
 
-def batch_workload(count: int = 64):
-    """The batched-solve workload: `count` netlists of the batch generator
-    (log-uniform 5k-200k cells, mean degree 3.5, 65% density), each with its
-    own seeded positions and anchors; returns their B2B systems loaded into a
-    Batch (x and y of every netlist), plus the number of rows per system."""
+def batch_unit(k: int):
+    """Netlist k of the batched-solve workload (log-uniform 5k-200k cells,
+    mean degree 3.5, 65% density) with its own seeded positions and anchors:
+    (netlist, x, y, anchor_x, anchor_y, alpha)."""
     from ktplace_b200 import synth, netlist
+    raw = synth.generate(synth.spec_batch_member(k))
+    nl = netlist.flatten(raw)
+    x, y = synth.seed_positions(raw, nl.num_movable, 300 + k)
+    ax, ay = synth.seed_positions(raw, nl.num_movable, 400 + k)
+    return nl, x, y, ax, ay, ALPHA
+
+
+def batch_workload(count: int = 64):
+    """The batched-solve workload loaded into one Batch (x and y of every
+    netlist); returns it with the number of rows per system."""
     from ktplace_b200.gpu import Context, Batch
     ctx = Context(0)
     batch = Batch(0)
     rows = []
     for k in range(count):
-        raw = synth.generate(synth.spec_batch_member(k))
-        nl = netlist.flatten(raw)
-        x, y = synth.seed_positions(raw, nl.num_movable, 300 + k)
-        ax, ay = synth.seed_positions(raw, nl.num_movable, 400 + k)
+        nl, x, y, ax, ay, alpha = batch_unit(k)
         fx, fy = nl.floors()
         ctx.upload_netlist(nl)
-        ctx.build_b2b(x, y, ALPHA, ax, ay, fx, fy)
+        ctx.build_b2b(x, y, alpha, ax, ay, fx, fy)
         batch.add_from_context(ctx, x, y)
         rows += [nl.num_movable, nl.num_movable]
     ctx.close()
     return batch, rows
 
 
-def run_batch_leg(torch, dev, stream, steps: int):
-    batch, rows = batch_workload()
-    batch.set_stream(stream.cuda_stream)
-    cluster, threads, _ = batch.autotune(TOL, precision=1, inner_tol=MIXED_INNER_TOL,
-                                         probe_iter=40)
+def run_batch_leg(torch, dev, stream, steps: int, rank: int = 0, world: int = 1, dist=None,
+                  count: int = 64):
+    """The batched solve of `count` netlists (2 systems each). Every rank
+    builds and solves its LPT share (shard.ShardPlan over the netlists' row
+    counts) as one autotuned Batch on its GPU; the step time is the max over
+    ranks, and the host slices of the solutions are written by
+    shard.run_share after the timed steps."""
+    from ktplace_b200 import shard, synth
+    cells = [synth.spec_batch_member(k).num_movable for k in range(count)]
+    plan = shard.ShardPlan([2 * c for c in cells], [2 * c for c in cells], world)
+    mine = plan.share(rank)
+    solver = shard.BatchShardSolver(batch_unit, device=dev.index or 0, tol=TOL, max_iter=MAX_ITER,
+                                    precision=1, inner_tol=MIXED_INNER_TOL,
+                                    stream=stream.cuda_stream)
+    if mine:
+        solver.load(mine)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     times, lat, iters = [], [], []
     for k in range(steps + 3):
-        batch.reset_x()
+        if mine:
+            solver.batch.reset_x()
         with torch.cuda.stream(stream):
             flush.zero_()
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
         e0.record(stream)
-        batch.solve(TOL, MAX_ITER, precision=1, inner_tol=MIXED_INNER_TOL)
+        if mine:
+            solver.solve(reset=False)
         e1.record(stream)
         e1.synchronize()
         if k >= 3:
             times.append(e0.elapsed_time(e1))
-            res = batch.results()
-            lat += [r["latency_ns"] / 1e6 for r in res]
-            iters += [r["iters"] for r in res]
-            bad = [r for r in res if r["status"] != 0 or r["resid"] > TOL]
-            if bad:
-                raise RuntimeError(f"batched solve left {len(bad)} systems unconverged")
+            if mine:
+                res = solver.batch.results()
+                lat += [r["latency_ns"] / 1e6 for r in res]
+                iters += [r["iters"] for r in res]
+                bad = [r for r in res if r["status"] != 0 or r["resid"] > TOL]
+                if bad:
+                    raise RuntimeError(f"batched solve left {len(bad)} systems unconverged")
     ms = statistics.median(times)
-    batch.close()
-    return {"workload": "64 synthetic netlists (log-uniform 5k-200k cells), x+y = 128 systems, "
-                        "FP32 PCG in FP64 refinement to true rtol 1e-6, one graph-replayed "
-                        "persistent cluster launch",
-            "systems": len(rows), "rows_total": int(sum(rows)), "ms_per_batch": ms,
-            "systems_per_s": len(rows) / (ms * 1e-3),
-            "latency_ms_p50": float(np.percentile(lat, 50)),
-            "latency_ms_p99": float(np.percentile(lat, 99)),
-            "inner_iters_p50": float(np.percentile(iters, 50)),
-            "autotuned_shape": {"cluster": cluster, "threads": threads}}
+    out = np.zeros(plan.total)
+    shard.run_share(plan, rank, solver, out)  # host slices (untimed)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    shape, split = solver.shape, solver.split
+    solver.close()
+    systems = 2 * count
+    return {"workload": f"{count} synthetic netlists (log-uniform 5k-200k cells), x+y = "
+                        f"{systems} systems, FP32 PCG in FP64 refinement to true rtol 1e-6, "
+                        "persistent cluster launches (size classes) replayed as one graph",
+            "systems": systems, "rows_total": int(plan.total), "ms_per_batch": ms_max,
+            "systems_per_s": systems / (ms_max * 1e-3),
+            "sharding": {"ranks": world, "units_per_rank": len(mine),
+                         "rows_this_rank": int(sum(plan.sizes[u] for u in mine)),
+                         "lpt_makespan_rows": plan.makespan(), "scaling": "strong"},
+            "latency_ms_p50": float(np.percentile(lat, 50)) if lat else None,
+            "latency_ms_p99": float(np.percentile(lat, 99)) if lat else None,
+            "inner_iters_p50": float(np.percentile(iters, 50)) if iters else None,
+            "autotuned_shape": {"cluster": shape[0], "threads": shape[1]} if shape else None,
+            "size_split": split}
 
 
 def profile_once():

@@ -332,6 +332,21 @@ int ktg_batch_get_shape(const ktg_batch *b, int *cluster, int *threads);
  * probe_iter and keeps the fastest (the project autotuner). Resets x. */
 int ktg_batch_autotune(ktg_batch *b, double tol, int precision, double inner_tol,
                        int64_t probe_iter, int *cluster, int *threads, float *best_ms);
+/* Size classes: systems of at least `rows` rows (0 turns the split off) are
+ * solved by a second persistent launch of `clusters` clusters of `cluster`
+ * CTAs (1-16; 16 is a non-portable size) of `threads` threads, concurrent
+ * with the launch of the batch shape over the rest, whose grid is cut to the
+ * SMs left free. Each class drains its own work queue largest first. */
+int ktg_batch_set_split(ktg_batch *b, int64_t rows, int cluster, int threads, int clusters);
+/* The split in force and how many systems it puts in the large class. */
+int ktg_batch_get_split(const ktg_batch *b, int64_t *rows, int *cluster, int *threads,
+                        int *clusters, int *num_large);
+/* Times full solves (iteration cap max_iter) with no split and with splits
+ * that move the 1-16 largest systems to 16x1024, 8x1024 or 16x512 clusters
+ * (1-8 of them), and keeps the fastest; run it after ktg_batch_autotune.
+ * *base_ms: the unsplit time, *best_ms: the kept one. Resets x. */
+int ktg_batch_autotune_split(ktg_batch *b, double tol, int precision, double inner_tol,
+                             int64_t max_iter, float *base_ms, float *best_ms);
 /* Restores every system's start vector. */
 int ktg_batch_reset_x(ktg_batch *b);
 /* Enqueues the solve of every system on the batch's stream (graph replay). */

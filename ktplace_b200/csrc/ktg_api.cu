@@ -224,8 +224,12 @@ int ktg_create(int device, ktg_ctx **out) {
     if (cudaMallocHost(&c->h_minfo, sizeof(ktg_mixed_info)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
     if ((rc = dev_alloc(c, &c->nnz_dev, 2))) return fail(rc);
     if ((rc = reserve_partials(c, 16384))) return fail(rc);
-    if (cudaMemset(c->counters, 0, 8 * sizeof(unsigned)) != cudaSuccess) return fail(KTG_ERR_CUDA);
-    if (cudaMemset(c->status, 0, sizeof(int)) != cudaSuccess) return fail(KTG_ERR_CUDA);
+    // stream-ordered (and finished before the handle is returned): the
+    // context's stream is non-blocking, so it would not wait for a plain memset
+    if (cudaMemsetAsync(c->counters, 0, 8 * sizeof(unsigned), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->status, 0, sizeof(int), c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return fail(KTG_ERR_CUDA);
     if (cudaMallocHost(&c->h_scalars, 8 * sizeof(double)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
     if (cudaMallocHost(&c->h_info, sizeof(ktg_solve_info)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
     if (cudaMallocHost(&c->h_nnz, 2 * sizeof(int64_t)) != cudaSuccess) return fail(KTG_ERR_NOMEM);
@@ -243,6 +247,7 @@ void ktg_destroy(ktg_ctx *c) {
     ktg::free_agg(c);
     ktg::free_lal(c);
     dev_free(c->coarse_z_buf);
+    dev_free(c->coarse_emb);
     dev_free(c->mixed_trace);
     dev_free(c->hpwl_terms);
     dev_free(c->exact_prod);
@@ -325,7 +330,8 @@ int ktg_set_option(ktg_ctx *c, const char *key, int64_t value) {
         if (value > 0) {
             int rc = dev_alloc(c, &c->mixed_trace, value);
             if (rc) return rc;
-            KTG_CUDA(c, cudaMemset(c->mixed_trace, 0, sizeof(unsigned long long) * value));
+            KTG_CUDA(c, cudaMemsetAsync(c->mixed_trace, 0, sizeof(unsigned long long) * value,
+                                        c->stream));
             c->mixed_trace_cap = static_cast<int32_t>(value);
         }
         return KTG_OK;

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <functional>
 #include <new>
 #include <numeric>
 #include <string>
@@ -359,7 +360,8 @@ struct ktg_batch {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     std::string err;
-    int64_t launches = 0;
+    int64_t launches = 0;       // kernels launched by solves (graph replays included)
+    int graph_kernels = 0;      // kernels in the captured graph
     // host mirror of the descriptors
     std::vector<ktg::SysDesc> sys;
     std::vector<int64_t> cost;
@@ -381,11 +383,21 @@ struct ktg_batch {
     // launch shape
     int cluster = 8;
     int threads = 512;
+    // size classes: systems of at least split_rows rows (0: none) are solved
+    // by a second, concurrent launch of split_clusters clusters of
+    // split_cluster CTAs of split_threads threads, with their own queue
+    int64_t split_rows = 0;
+    int split_cluster = 16, split_threads = 1024, split_clusters = 1;
+    int num_large = 0;           // systems in the large class (first in d_order)
+    unsigned *queue2 = nullptr;  // the large class's work queue
+    int64_t order_split_rows = -1;  // split the uploaded order was built for
     // graph cache
     cudaGraphExec_t graph = nullptr;
     double g_tol = -1, g_inner = -1;
     int64_t g_max_iter = -1;
     int g_mixed = -1, g_cluster = -1, g_threads = -1;
+    int64_t g_split_rows = -1;
+    int g_split_cluster = -1, g_split_threads = -1, g_split_clusters = -1;
 };
 
 namespace {
@@ -471,7 +483,8 @@ int ktg_batch_create(int device, ktg_batch **out) {
     if (cudaSetDevice(device) != cudaSuccess ||
         cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&b->queue, sizeof(unsigned)) != cudaSuccess) {
+        cudaMalloc(&b->queue, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&b->queue2, sizeof(unsigned)) != cudaSuccess) {
         ktg_batch_destroy(b);
         return KTG_ERR_CUDA;
     }
@@ -487,7 +500,7 @@ void ktg_batch_destroy(ktg_batch *b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     void *ptrs[] = {b->d_sys, b->d_order, b->rp, b->col, b->val, b->val32, b->diag, b->rhs,
                     b->x, b->x0, b->r, b->z, b->p, b->ap, b->d32, b->ri32, b->z32, b->p32,
-                    b->ap32, b->queue, b->results};
+                    b->ap32, b->queue, b->queue2, b->results};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->own_stream) cudaStreamDestroy(b->own_stream);
@@ -595,6 +608,39 @@ int ktg_batch_get_shape(const ktg_batch *b, int *cluster, int *threads) {
     return KTG_OK;
 }
 
+int ktg_batch_set_split(ktg_batch *b, int64_t rows, int cluster, int threads, int clusters) {
+    if (!b) return KTG_ERR_ARG;
+    if (rows < 0) return berr(b, KTG_ERR_ARG, "negative split rows");
+    if (rows > 0) {
+        if (!(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8 || cluster == 16))
+            return berr(b, KTG_ERR_ARG, "cluster must be 1, 2, 4, 8 or 16");
+        if (!(threads == 128 || threads == 256 || threads == 512 || threads == 1024))
+            return berr(b, KTG_ERR_ARG, "threads must be 128, 256, 512 or 1024");
+        if (clusters < 1) return berr(b, KTG_ERR_ARG, "clusters must be >= 1");
+        b->split_cluster = cluster;
+        b->split_threads = threads;
+        b->split_clusters = clusters;
+    }
+    b->split_rows = rows;
+    return KTG_OK;
+}
+
+int ktg_batch_get_split(const ktg_batch *b, int64_t *rows, int *cluster, int *threads,
+                        int *clusters, int *num_large) {
+    if (!b) return KTG_ERR_ARG;
+    if (rows) *rows = b->split_rows;
+    if (cluster) *cluster = b->split_cluster;
+    if (threads) *threads = b->split_threads;
+    if (clusters) *clusters = b->split_clusters;
+    if (num_large) {
+        int64_t k = 0;
+        if (b->split_rows > 0)
+            for (const ktg::SysDesc &d : b->sys) k += d.n >= b->split_rows;
+        *num_large = static_cast<int>(k);
+    }
+    return KTG_OK;
+}
+
 int ktg_batch_reset_x(ktg_batch *b) {
     if (!b) return KTG_ERR_ARG;
     if (b->rows)
@@ -603,19 +649,20 @@ int ktg_batch_reset_x(ktg_batch *b) {
     return KTG_OK;
 }
 
-// How many clusters of the current shape can be resident at once.
-static int resident_clusters(ktg_batch *b, int *out) {
+// How many clusters of `cluster` CTAs of `threads` threads can be resident
+// at once on the whole device.
+static int resident_clusters(ktg_batch *b, int cluster, int threads, int *out) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = b->cluster;
+    attr[0].val.clusterDim.x = cluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(b->threads);
-    cfg.gridDim = dim3(b->cluster);
+    cfg.blockDim = dim3(threads);
+    cfg.gridDim = dim3(cluster);
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (b->cluster > 8)
+    if (cluster > 8)
         KTG_BCUDA(b, cudaFuncSetAttribute(ktg::k_batch_pcg,
                                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     KTG_BCUDA(b, cudaOccupancyMaxActiveClusters(out, ktg::k_batch_pcg, &cfg));
@@ -623,30 +670,92 @@ static int resident_clusters(ktg_batch *b, int *out) {
     return KTG_OK;
 }
 
-static int batch_enqueue(ktg_batch *b, double tol, int64_t max_iter, int mixed, double inner_tol,
-                         int max_clusters, cudaStream_t st) {
-    const int ns = static_cast<int>(b->sys.size());
+// One persistent launch over the systems order[first, first + count): `clusters`
+// clusters of `cluster` CTAs of `threads` threads draining `queue`.
+static int enqueue_class(ktg_batch *b, int first, int count, unsigned *queue, int cluster,
+                         int threads, int clusters, double tol, int64_t max_iter, int mixed,
+                         double inner_tol, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = b->cluster;
+    attr[0].val.clusterDim.x = cluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(b->threads);
+    cfg.blockDim = dim3(threads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const int clusters = std::min(max_clusters, std::max(ns, 1));
-    cfg.gridDim = dim3(clusters * b->cluster);
-    ktg::BatchArgs A{b->d_sys, b->d_order, ns, b->rp, b->col, b->val, b->val32, b->diag,
-                     b->rhs, b->x, b->r, b->z, b->p, b->ap, b->d32, b->ri32, b->z32, b->p32,
-                     b->ap32, b->queue, b->results, tol, inner_tol, max_iter, 50, mixed,
+    cfg.gridDim = dim3(std::max(1, std::min(clusters, count)) * cluster);
+    ktg::BatchArgs A{b->d_sys, b->d_order + first, count, b->rp, b->col, b->val, b->val32,
+                     b->diag, b->rhs, b->x, b->r, b->z, b->p, b->ap, b->d32, b->ri32, b->z32,
+                     b->p32, b->ap32, queue, b->results, tol, inner_tol, max_iter, 50, mixed,
                      120000000000ull};
-    KTG_BCUDA(b, cudaMemsetAsync(b->queue, 0, sizeof(unsigned), st));
+    KTG_BCUDA(b, cudaMemsetAsync(queue, 0, sizeof(unsigned), st));
     KTG_BCUDA(b, cudaLaunchKernelEx(&cfg, ktg::k_batch_pcg, A));
-    ++b->launches;
     return KTG_OK;
+}
+
+// Enqueues the whole batch solve on `st`. Without a size split it is one
+// launch of the batch shape sized to the device. With one, the large class
+// runs on a forked stream as its own launch while the small class's grid is
+// cut to the SMs the large clusters leave free; the two launches share no
+// state besides the solution arrays of disjoint systems, so neither waits on
+// the other and the fork is joined back into `st` at the end.
+static int batch_enqueue(ktg_batch *b, double tol, int64_t max_iter, int mixed, double inner_tol,
+                         cudaStream_t st) {
+    const int ns = static_cast<int>(b->sys.size());
+    const int nl = b->num_large;
+    int res_small = 0;
+    int rc = resident_clusters(b, b->cluster, b->threads, &res_small);
+    if (rc) return rc;
+    if (nl == 0) {
+        rc = enqueue_class(b, 0, ns, b->queue, b->cluster, b->threads, res_small, tol, max_iter,
+                           mixed, inner_tol, st);
+        b->graph_kernels = 1;
+        return rc;
+    }
+    int res_large = 0;
+    if ((rc = resident_clusters(b, b->split_cluster, b->split_threads, &res_large))) return rc;
+    const int large_clusters = std::min({b->split_clusters, res_large, nl});
+    if (nl == ns) {
+        rc = enqueue_class(b, 0, ns, b->queue2, b->split_cluster, b->split_threads, large_clusters,
+                           tol, max_iter, mixed, inner_tol, st);
+        b->graph_kernels = 1;
+        return rc;
+    }
+    // SMs held by the large class, from its CTAs per SM when the device is full.
+    const int sms = std::max(1, b->num_sms);
+    const int large_per_sm = std::max(1, res_large * b->split_cluster / sms);
+    const int large_sms = (large_clusters * b->split_cluster + large_per_sm - 1) / large_per_sm;
+    const int small_per_sm = std::max(1, res_small * b->cluster / sms);
+    const int free_sms = std::max(b->cluster, sms - large_sms);
+    const int small_clusters = std::max(1, std::min(res_small, free_sms * small_per_sm / b->cluster));
+    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side = nullptr;
+    KTG_BCUDA(b, cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    if (cudaEventCreateWithFlags(&join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        return berr(b, KTG_ERR_CUDA, "fork stream creation failed");
+    }
+    if (cudaEventRecord(fork, st) != cudaSuccess || cudaStreamWaitEvent(side, fork, 0) != cudaSuccess)
+        rc = berr(b, KTG_ERR_CUDA, "stream fork failed");
+    if (!rc)
+        rc = enqueue_class(b, 0, nl, b->queue2, b->split_cluster, b->split_threads, large_clusters,
+                           tol, max_iter, mixed, inner_tol, side);
+    if (!rc)
+        rc = enqueue_class(b, nl, ns - nl, b->queue, b->cluster, b->threads, small_clusters, tol,
+                           max_iter, mixed, inner_tol, st);
+    if (!rc && (cudaEventRecord(join, side) != cudaSuccess ||
+                cudaStreamWaitEvent(st, join, 0) != cudaSuccess))
+        rc = berr(b, KTG_ERR_CUDA, "stream join failed");
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
+    cudaStreamDestroy(side);
+    b->graph_kernels = 2;
+    return rc;
 }
 
 int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, double inner_tol) {
@@ -657,17 +766,24 @@ int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, d
     if (max_iter < 0) return berr(b, KTG_ERR_ARG, "negative max_iter");
     if (b->sys.empty()) return KTG_OK;
     if (cudaSetDevice(b->device) != cudaSuccess) return KTG_ERR_CUDA;
-    if (b->dirty) {
+    if (b->dirty || b->order_split_rows != b->split_rows) {
+        // Largest first within each class; the large class (rows >= split_rows)
+        // occupies the front of the order.
         std::vector<int32_t> order(b->sys.size());
         std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(),
-                         [&](int32_t p, int32_t q) { return b->cost[p] > b->cost[q]; });
+        auto large = [&](int32_t p) { return b->split_rows > 0 && b->sys[p].n >= b->split_rows; };
+        std::stable_sort(order.begin(), order.end(), [&](int32_t p, int32_t q) {
+            if (large(p) != large(q)) return large(p);
+            return b->cost[p] > b->cost[q];
+        });
+        b->num_large = static_cast<int>(std::count_if(order.begin(), order.end(), large));
         KTG_BCUDA(b, cudaMemcpyAsync(b->d_sys, b->sys.data(), sizeof(ktg::SysDesc) * b->sys.size(),
                                      cudaMemcpyHostToDevice, b->stream));
         KTG_BCUDA(b, cudaMemcpyAsync(b->d_order, order.data(), sizeof(int32_t) * order.size(),
                                      cudaMemcpyHostToDevice, b->stream));
         KTG_BCUDA(b, cudaStreamSynchronize(b->stream));
         b->dirty = false;
+        b->order_split_rows = b->split_rows;
         if (b->graph) {
             cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
@@ -675,15 +791,15 @@ int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, d
     }
     const bool same = b->graph && b->g_tol == tol && b->g_max_iter == max_iter &&
                       b->g_mixed == precision && b->g_inner == inner_tol &&
-                      b->g_cluster == b->cluster && b->g_threads == b->threads;
+                      b->g_cluster == b->cluster && b->g_threads == b->threads &&
+                      b->g_split_rows == b->split_rows && b->g_split_cluster == b->split_cluster &&
+                      b->g_split_threads == b->split_threads &&
+                      b->g_split_clusters == b->split_clusters;
     if (!same) {
         if (b->graph) {
             cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
         }
-        int max_clusters = 0;
-        int rc0 = resident_clusters(b, &max_clusters);
-        if (rc0) return rc0;
         // Capture the whole batch solve once on a private stream.
         cudaStream_t cap;
         KTG_BCUDA(b, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
@@ -693,7 +809,7 @@ int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, d
             cudaStreamDestroy(cap);
             return berr(b, KTG_ERR_CUDA, "stream capture failed to start");
         }
-        rc = batch_enqueue(b, tol, max_iter, precision, inner_tol, max_clusters, cap);
+        rc = batch_enqueue(b, tol, max_iter, precision, inner_tol, cap);
         const cudaError_t ec = cudaStreamEndCapture(cap, &g);
         cudaStreamDestroy(cap);
         if (rc) {
@@ -710,9 +826,13 @@ int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, d
         b->g_inner = inner_tol;
         b->g_cluster = b->cluster;
         b->g_threads = b->threads;
+        b->g_split_rows = b->split_rows;
+        b->g_split_cluster = b->split_cluster;
+        b->g_split_threads = b->split_threads;
+        b->g_split_clusters = b->split_clusters;
     }
     KTG_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
-    ++b->launches;
+    b->launches += b->graph_kernels;
     return KTG_OK;
 }
 
@@ -752,7 +872,7 @@ int ktg_batch_autotune(ktg_batch *b, double tol, int precision, double inner_tol
         for (int t : kThreads) {
             if ((rc = ktg_batch_set_shape(b, c, t))) break;
             int resident = 0;
-            if (resident_clusters(b, &resident) != KTG_OK) {
+            if (resident_clusters(b, c, t, &resident) != KTG_OK) {
                 b->err.clear();
                 continue;  // shape not launchable on this device
             }
@@ -781,6 +901,88 @@ int ktg_batch_autotune(ktg_batch *b, double tol, int precision, double inner_tol
     if ((rc = ktg_batch_reset_x(b))) return rc;
     if (cluster) *cluster = bc;
     if (threads) *threads = bt;
+    if (best_ms) *best_ms = best;
+    return KTG_OK;
+}
+
+// Times one full solve (from reset x) of the current configuration.
+static int time_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, double inner_tol,
+                      cudaEvent_t e0, cudaEvent_t e1, float *ms) {
+    int rc;
+    if ((rc = ktg_batch_reset_x(b))) return rc;
+    KTG_BCUDA(b, cudaEventRecord(e0, b->stream));
+    if ((rc = ktg_batch_solve(b, tol, max_iter, precision, inner_tol))) return rc;
+    KTG_BCUDA(b, cudaEventRecord(e1, b->stream));
+    KTG_BCUDA(b, cudaEventSynchronize(e1));
+    KTG_BCUDA(b, cudaEventElapsedTime(ms, e0, e1));
+    return KTG_OK;
+}
+
+int ktg_batch_autotune_split(ktg_batch *b, double tol, int precision, double inner_tol,
+                             int64_t max_iter, float *base_ms, float *best_ms) {
+    if (!b || max_iter <= 0) return KTG_ERR_ARG;
+    if (b->sys.empty()) return berr(b, KTG_ERR_STATE, "empty batch");
+    // Thresholds that put the 1, 2, 4, 8 or 16 largest systems (ties
+    // included) in the large class.
+    std::vector<int64_t> sizes;
+    for (const ktg::SysDesc &d : b->sys) sizes.push_back(d.n);
+    std::sort(sizes.begin(), sizes.end(), std::greater<int64_t>());
+    std::vector<int64_t> cuts;
+    for (size_t k : {1, 2, 4, 8, 16}) {
+        if (k >= sizes.size()) break;
+        const int64_t t = sizes[k - 1];
+        if (t > sizes.back() && (cuts.empty() || cuts.back() != t)) cuts.push_back(t);
+    }
+    static const int kShapes[][2] = {{16, 1024}, {8, 1024}, {16, 512}};
+    static const int kCount[] = {1, 2, 4, 8};
+    cudaEvent_t e0, e1;
+    KTG_BCUDA(b, cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return berr(b, KTG_ERR_CUDA, "event creation failed");
+    }
+    int rc = ktg_batch_set_split(b, 0, 0, 0, 0);
+    float none = 0.0f, ms = 0.0f;
+    for (int rep = 0; rep < 2 && !rc; ++rep) rc = time_solve(b, tol, max_iter, precision, inner_tol, e0, e1, &none);
+    float best = none;
+    int64_t br = 0;
+    int bc = b->split_cluster, bt = b->split_threads, bn = b->split_clusters;
+    for (int64_t cut : cuts) {
+        if (rc) break;
+        for (const auto &sh : kShapes) {
+            if (rc) break;
+            int resident = 0;
+            if (resident_clusters(b, sh[0], sh[1], &resident) != KTG_OK) {
+                b->err.clear();
+                continue;  // shape not launchable on this device
+            }
+            for (int n : kCount) {
+                if (n > resident) break;
+                if ((rc = ktg_batch_set_split(b, cut, sh[0], sh[1], n))) break;
+                int nl = 0;
+                ktg_batch_get_split(b, nullptr, nullptr, nullptr, nullptr, &nl);
+                if (n > nl) break;
+                float t = 1e30f;
+                for (int rep = 0; rep < 2 && !rc; ++rep) {
+                    rc = time_solve(b, tol, max_iter, precision, inner_tol, e0, e1, &ms);
+                    t = std::min(t, ms);
+                }
+                if (!rc && t < best) {
+                    best = t;
+                    br = cut;
+                    bc = sh[0];
+                    bt = sh[1];
+                    bn = n;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if ((rc = ktg_batch_set_split(b, br, bc, bt, bn))) return rc;
+    if ((rc = ktg_batch_reset_x(b))) return rc;
+    if (base_ms) *base_ms = none;
     if (best_ms) *best_ms = best;
     return KTG_OK;
 }

@@ -107,6 +107,12 @@ struct ktg_ctx {
     int64_t coarse_z_gen = 0;         // bumped whenever coarse_z is rewritten
     float *coarse_z_buf = nullptr;    // storage of the learned coarse vector
     int64_t coarse_z_cap = 0;
+    // trunk embedding of this context's netlist under one learned parameter
+    // set (computed once per netlist, reused by every build's head pass)
+    float *coarse_emb = nullptr;      // [n x 16]
+    int64_t coarse_emb_cap = 0;
+    uint64_t coarse_emb_owner = 0;    // id of the learned handle that wrote it
+    int64_t coarse_emb_version = -1, coarse_emb_gen = -1;
     int64_t netlist_gen = 0;          // bumped by every ktg_upload_netlist
     const ktg_mixed_info *pcg_gate = nullptr;  // see PcgArgs::gate (ktg_pcg.cu)
     unsigned long long *mixed_trace = nullptr;  // phase stamps of the mixed solve (null: off)

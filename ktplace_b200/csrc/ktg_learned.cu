@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <new>
@@ -835,11 +836,7 @@ struct ktg_learned {
     double *czd = nullptr, *caz = nullptr;               // [n]
     double *ce = nullptr, *ca = nullptr;                 // [T x n] test vectors, A e
     double *cscal = nullptr;                             // [2 + 3 * kMaxVec + 1]
-    // trunk embedding of the last prepared netlist (reused across systems)
-    float *pc = nullptr;
-    int64_t cap_pc = 0;
-    const ktg_ctx *pc_ctx = nullptr;
-    int64_t pc_gen = -1, pc_version = -1;
+    uint64_t uid = 0;  // process-unique id (tags the embeddings it leaves in contexts)
 };
 
 namespace {
@@ -1252,6 +1249,8 @@ int ktg_learned_create(int device, uint64_t seed, ktg_learned **out) {
         delete h;
         return KTG_ERR_CUDA;
     }
+    static std::atomic<uint64_t> next_uid{1};
+    h->uid = next_uid.fetch_add(1);
     const int64_t P = h->L.total;
     if (lalloc(h, &h->w, P) || lalloc(h, &h->g, P) || lalloc(h, &h->m1, P) ||
         lalloc(h, &h->m2, P) || lalloc(h, &h->wh, P) ||
@@ -1286,10 +1285,14 @@ int ktg_learned_create(int device, uint64_t seed, ktg_learned **out) {
     fill(L.Wh, HEAD_IN, HEAD_H, 1.0);
     fill(L.wz, HEAD_H, 1, 0.1);
     w[L.bz] = static_cast<float>(kSoftplusInvOne);  // untrained head: z = 1 (constant)
-    if (cudaMemcpy(h->w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(h->m1, 0, sizeof(float) * P) != cudaSuccess ||
-        cudaMemset(h->m2, 0, sizeof(float) * P) != cudaSuccess ||
-        cudaMemset(h->ticket, 0, sizeof(unsigned)) != cudaSuccess || refresh_bf16(h) != KTG_OK ||
+    // Every upload is ordered on the handle's stream ahead of the BF16 copy: a
+    // plain cudaMemcpy from pageable memory may return before its DMA lands,
+    // and the non-blocking stream would not wait for it.
+    if (cudaMemcpyAsync(h->w, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->m1, 0, sizeof(float) * P, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->m2, 0, sizeof(float) * P, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->ticket, 0, sizeof(unsigned), h->stream) != cudaSuccess ||
+        refresh_bf16(h) != KTG_OK ||
         cudaStreamSynchronize(h->stream) != cudaSuccess) {
         ktg_learned_destroy(h);
         return KTG_ERR_CUDA;
@@ -1305,7 +1308,7 @@ void ktg_learned_destroy(ktg_learned *h) {
     void *ptrs[] = {h->w, h->g, h->m1, h->m2, h->wh, h->x, h->act_c, h->act_n, h->p, h->dp,
                     h->dh, h->dh2, h->dg, h->dm, h->de, h->t, h->ds, h->dphi, h->tr, h->u,
                     h->gq, h->wpart, h->dpart, h->ticket, h->scal, h->cu, h->chh, h->co,
-                    h->cdz, h->cdhh, h->cdo, h->czd, h->caz, h->ce, h->ca, h->cscal, h->pc};
+                    h->cdz, h->cdhh, h->cdo, h->czd, h->caz, h->ce, h->ca, h->cscal};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -1336,7 +1339,8 @@ int ktg_learned_get_params(ktg_learned *h, float *out) {
 int ktg_learned_set_params(ktg_learned *h, const float *in) {
     if (!h || !in) return KTG_ERR_ARG;
     KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
-    KTG_LCUDA(h, cudaMemcpy(h->w, in, sizeof(float) * h->L.total, cudaMemcpyHostToDevice));
+    KTG_LCUDA(h, cudaMemcpyAsync(h->w, in, sizeof(float) * h->L.total, cudaMemcpyHostToDevice,
+                                 h->stream));  // stream-ordered ahead of the BF16 copy
     int rc = refresh_bf16(h);
     if (rc) return rc;
     KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
@@ -1399,32 +1403,35 @@ int ktg_learned_prepare_coarse(ktg_learned *h, ktg_ctx *c) {
         KTG_LCUDA(h, cudaMalloc(&c->coarse_z_buf, sizeof(float) * std::max<int64_t>(2 * n, 1)));
         c->coarse_z_cap = 2 * n;
     }
-    if (h->cap_pc < n) {
-        int rc = lalloc(h, &h->pc, std::max<int64_t>(n, 1) * PROJ);
-        if (rc) return rc;
-        h->cap_pc = n;
-        h->pc_ctx = nullptr;
+    if (c->coarse_emb_cap < n) {  // the context keeps its netlist's embedding
+        if (c->coarse_emb) cudaFree(c->coarse_emb);
+        c->coarse_emb = nullptr;
+        c->coarse_emb_cap = 0;
+        c->coarse_emb_owner = 0;
+        KTG_LCUDA(h, cudaMalloc(&c->coarse_emb, sizeof(float) * std::max<int64_t>(n, 1) * PROJ));
+        c->coarse_emb_cap = n;
     }
     // Everything below is enqueued on the context's stream.
     cudaStream_t own = h->stream;
     h->stream = c->stream;
     int rc = KTG_OK;
-    if (h->pc_ctx != c || h->pc_gen != c->netlist_gen || h->pc_version != h->version) {
+    if (c->coarse_emb_owner != h->uid || c->coarse_emb_gen != c->netlist_gen ||
+        c->coarse_emb_version != h->version) {
         rc = topo_trunk(h, c);  // once per netlist and parameter set
-        if (!rc && n > 0 && cudaMemcpyAsync(h->pc, h->p, sizeof(float) * n * PROJ,
+        if (!rc && n > 0 && cudaMemcpyAsync(c->coarse_emb, h->p, sizeof(float) * n * PROJ,
                                             cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
             rc = lerr(h, KTG_ERR_CUDA, "embedding copy failed");
         if (!rc) {
-            h->pc_ctx = c;
-            h->pc_gen = c->netlist_gen;
-            h->pc_version = h->version;
+            c->coarse_emb_owner = h->uid;
+            c->coarse_emb_gen = c->netlist_gen;
+            c->coarse_emb_version = h->version;
         }
     }
     for (int axis = 0; axis < 2 && !rc; ++axis) {
         SysView S{c->sys[axis].row_ptr, c->sys[axis].col, c->sys[axis].val, c->sys[axis].diag,
                   static_cast<int32_t>(n), 0};
         if ((rc = logd_mean(h, S))) break;
-        HeadArgs A = head_args(h, S, h->pc);
+        HeadArgs A = head_args(h, S, c->coarse_emb);
         A.zf = c->coarse_z_buf + axis * n;
         if (n > 0) {
             ktg::learned::k_coarse_head<<<static_cast<int>((n + 255) / 256), 256, 0, h->stream>>>(A);

@@ -447,6 +447,29 @@ class Batch:
                                                 ctypes.byref(ms)))
         return int(c.value), int(t.value), float(ms.value)
 
+    def set_split(self, rows: int, cluster: int = 16, threads: int = 1024, clusters: int = 1):
+        """Systems of >= rows rows go to a concurrent launch of `clusters`
+        clusters of cluster x threads (rows 0: no split)."""
+        self._check(self.lib.ktg_batch_set_split(self.h, rows, cluster, threads, clusters))
+
+    def split(self) -> dict:
+        r, c, t, n, nl = (ctypes.c_int64(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(),
+                          ctypes.c_int())
+        self._check(self.lib.ktg_batch_get_split(self.h, ctypes.byref(r), ctypes.byref(c),
+                                                 ctypes.byref(t), ctypes.byref(n),
+                                                 ctypes.byref(nl)))
+        return dict(rows=int(r.value), cluster=int(c.value), threads=int(t.value),
+                    clusters=int(n.value), num_large=int(nl.value))
+
+    def autotune_split(self, tol: float, precision: int = 1, inner_tol: float = 1e-3,
+                       max_iter: int = 100000):
+        """Picks the size split by timing full solves; returns
+        (split dict, unsplit ms, kept ms)."""
+        base, best = ctypes.c_float(), ctypes.c_float()
+        self._check(self.lib.ktg_batch_autotune_split(self.h, tol, precision, inner_tol, max_iter,
+                                                      ctypes.byref(base), ctypes.byref(best)))
+        return self.split(), float(base.value), float(best.value)
+
     def reset_x(self):
         self._check(self.lib.ktg_batch_reset_x(self.h))
 

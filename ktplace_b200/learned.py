@@ -86,6 +86,11 @@ class Learned:
         except Exception:
             pass
 
+    @property
+    def launches(self) -> int:
+        """Kernels this handle has launched."""
+        return int(self.lib.ktg_learned_launch_count(self.h))
+
     def _check(self, rc: int):
         if rc != 0:
             raise KtgError(rc, self.lib.ktg_learned_last_error(self.h).decode())

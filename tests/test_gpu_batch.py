@@ -89,3 +89,91 @@ def test_batch_autotune_and_replay(systems):
     for (s, _), i, a in zip(systems, ids, first):
         assert np.array_equal(b.get_x(i, s["diag"].shape[0]), a)
     b.close()
+
+
+@pytest.mark.parametrize("cluster,threads,clusters", [(16, 1024, 1), (8, 1024, 2), (16, 512, 2)])
+def test_batch_size_split_matches_oracle(systems, cluster, threads, clusters):
+    """The 12k-cell design's two systems go to the large class; every system
+    still matches the oracle's PCG exactly as without the split."""
+    b, ids = make_batch(systems)
+    b.set_shape(4, 256)
+    rows = sorted((s["diag"].shape[0] for s, _ in systems), reverse=True)
+    b.set_split(rows[1], cluster, threads, clusters)
+    sp = b.split()
+    assert sp["num_large"] == sum(r >= rows[1] for r in rows) and sp["cluster"] == cluster
+    launches = b.launches
+    b.solve(TOL, MAX_ITER, precision=0)
+    assert b.launches - launches == 2
+    res = b.results()
+    for (s, x0), sid in zip(systems, ids):
+        ref = oracle.port_pcg_axis(s, x0, TOL, MAX_ITER)
+        got = b.get_x(sid, s["diag"].shape[0])
+        assert res[sid]["status"] == 0
+        assert res[sid]["iters"] == ref["iters"], (sid, res[sid], ref["iters"])
+        assert np.linalg.norm(got - ref["x"]) <= 1e-9 * np.linalg.norm(ref["x"])
+    # mixed precision through the split, then switching the split off again
+    b.reset_x()
+    b.solve(TOL, MAX_ITER, precision=1, inner_tol=1e-3)
+    res = b.results()
+    for (s, _), sid in zip(systems, ids):
+        assert res[sid]["status"] == 0 and true_resid(s, b.get_x(sid, s["diag"].shape[0])) <= TOL * 1.0001
+    b.set_split(0)
+    assert b.split()["num_large"] == 0
+    b.reset_x()
+    b.solve(TOL, MAX_ITER, precision=0)
+    assert all(r["status"] == 0 for r in b.results())
+    b.close()
+
+
+def test_batch_all_large_and_autotune_split(systems):
+    b, ids = make_batch(systems)
+    b.set_split(1, 8, 512, 4)  # every system in the large class: one launch
+    launches = b.launches
+    b.solve(TOL, MAX_ITER, precision=0)
+    assert b.launches - launches == 1
+    assert all(r["status"] == 0 for r in b.results())
+    b.set_split(0)
+    sp, base, best = b.autotune_split(TOL, precision=0, max_iter=MAX_ITER)
+    assert base > 0 and 0 < best <= base
+    assert sp["rows"] == 0 or sp["num_large"] >= 1
+    b.solve(TOL, MAX_ITER, precision=0)
+    for (s, x0), sid in zip(systems, ids):
+        ref = oracle.port_pcg_axis(s, x0, TOL, MAX_ITER)
+        assert np.linalg.norm(b.get_x(sid, s["diag"].shape[0]) - ref["x"]) <= 1e-9 * np.linalg.norm(ref["x"])
+    b.close()
+
+
+def test_sharded_batch_product_path(port_built):
+    """shard.ShardPlan + shard.run_share with the GPU share solver: the two
+    shares of a world-2 plan solved one after the other on this GPU (they
+    never wait on each other), assembled and checked against the oracle."""
+    from ktplace_b200 import shard
+    names = ("small12k", "tiny_macros", "edge_alpha", "edge_alpha0")
+    cases = {}
+
+    def make_unit(u):
+        if u not in cases:
+            raw, nl, x, y, ax, ay, alpha, _ = build_case(names[u])
+            cases[u] = (nl, x, y, ax, ay, alpha)
+        return cases[u]
+
+    sizes = [2 * make_unit(u)[0].num_movable for u in range(len(names))]
+    plan = shard.ShardPlan(sizes, sizes, world=2)
+    out = np.full(plan.total, np.nan)
+    for rank in range(2):
+        solver = shard.BatchShardSolver(make_unit, device=0, tol=TOL, max_iter=MAX_ITER,
+                                        precision=0, autotune=rank == 0)
+        assert sorted(shard.run_share(plan, rank, solver, out)) == sorted(plan.share(rank))
+        solver.close()
+    assert not np.isnan(out).any()
+    for u in range(len(names)):
+        nl, x, y, ax, ay, alpha = make_unit(u)
+        port = oracle.PortNetlist(nl)
+        fx, fy = nl.floors()
+        n = nl.num_movable
+        got = out[plan.slice(u)]
+        for axis, (pos, fl, anc) in enumerate(((x, fx, ax), (y, fy, ay))):
+            s = port.b2b_axis(axis == 0, pos, fl, alpha, anc if alpha > 0 else None)
+            ref = oracle.port_pcg_axis(s, pos, TOL, MAX_ITER)["x"]
+            mine = got[axis * n:(axis + 1) * n]
+            assert np.linalg.norm(mine - ref) <= 1e-9 * np.linalg.norm(ref), (names[u], axis)

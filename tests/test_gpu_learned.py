@@ -174,6 +174,21 @@ def test_prepared_coarse_vector_matches_oracle(tiny, gpu_ctx):
         r = gpu_ctx.solve_mixed(x, y, TOL)
         sx = gpu_ctx.system(0)
         assert true_resid_of(sx, r["x"]) <= TOL * 1.0001
+        # the trunk embedding stays with each context: alternating two
+        # contexts of the same netlist reruns only the per-system head
+        from ktplace_b200.gpu import Context
+        with Context(0) as other:
+            other.upload_netlist(nl)
+            other.build_b2b(x, y, alpha, ax, ay, fx, fy)
+            other.set_option("precond", 2)
+            learned.prepare_coarse(other)  # trunk for the second context
+            k0 = learned.launches
+            learned.prepare_coarse(gpu_ctx)
+            learned.prepare_coarse(other)
+            assert learned.launches - k0 <= 2 * 4, learned.launches - k0
+            other.set_option("coarse", 3)
+            assert rel(other.coarse()["z"].astype(np.float64), want[order]) <= 1e-4
+        assert rel(gpu_ctx.coarse()["z"].astype(np.float64), want[order]) <= 1e-4
     finally:
         gpu_ctx.set_option("coarse", 0)
         gpu_ctx.set_option("precond", 0)
