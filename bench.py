@@ -88,6 +88,9 @@ def parse():
     ap.add_argument("--simpl-report", type=int, default=0, metavar="ITERS",
                     help="only the mixed-precision study on the systems of ITERS SimPL global "
                          "iterations of the 211k design (prints one JSON line)")
+    ap.add_argument("--coarse-weights", default=None, metavar="NPY",
+                    help="weights of the learned coarse vector for the SimPL study (default: "
+                         "the committed ktplace_b200/weights/learned_coarse.npy)")
     ap.add_argument("--no-simpl-report", action="store_true",
                     help="skip the 30-iteration SimPL study in the default run")
     ap.add_argument("--profile-once", action="store_true",
@@ -572,8 +575,11 @@ def solve_variants(torch, dev, stream, ctx, dx, dy, dax, day, fx, fy, wx, wy, in
 SIMPL_VARIANTS = (("fp64_jacobi", None, 0, 0), ("fp32_jacobi", 0, 0, 0),
                   ("fp32_aggregation", 2, 0, 0), ("fp32_aggregation_coarse_const", 2, 1, 0),
                   ("fp32_aggregation_coarse_coupling", 2, 2, 0),
+                  ("fp32_learned", 2, 3, 0),
+                  ("fp32_aggregation_reuse", 2, 0, 4),
+                  ("fp32_aggregation_coarse_const_reuse", 2, 1, 4),
                   ("fp32_aggregation_coarse_coupling_reuse", 2, 2, 4),
-                  ("fp32_learned", 2, 3, 0), ("fp32_learned_reuse", 2, 3, 4))
+                  ("fp32_learned_reuse", 2, 3, 4))
 
 
 def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: int = 5,
@@ -595,12 +601,16 @@ def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: i
     from ktplace_b200 import simpl
     from ktplace_b200._lib import MixedInfo, SolveInfo
     from ktplace_b200.gpu import Context
-    ctx = Context(dev.index or 0)
-    ctx.set_stream(stream.cuda_stream)
-    ctx.upload_netlist(nl)
-    rctx = Context(dev.index or 0)  # the agg_reuse variants' own context
-    rctx.set_stream(stream.cuda_stream)
-    rctx.upload_netlist(nl)
+    def new_ctx():
+        c = Context(dev.index or 0)
+        c.set_stream(stream.cuda_stream)
+        c.upload_netlist(nl)
+        return c
+
+    ctx = new_ctx()
+    # every agg_reuse variant keeps its own context: the reused structure is
+    # the one its own previous builds left
+    vctxs = {name: (new_ctx() if reuse else ctx) for name, _, _, reuse in variants}
     g = kgrid.build_grid(nl, kgrid.default_bins_per_axis(nl.num_movable), 1.0)
     loop = simpl.GlobalLoop(ctx, nl, g, kgrid.build_free_space(nl), tol=TOL, max_iter=MAX_ITER)
     with torch.cuda.stream(stream):
@@ -615,7 +625,7 @@ def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: i
     x, y = loop.initial_rounds(x0, y0, init_rounds)
     rows = []
     fx, fy = loop.fx, loop.fy
-    for vctx in (ctx, rctx):  # untimed: every solver's buffers allocated once
+    for vctx in {id(c): c for c in vctxs.values()}.values():  # untimed: buffers allocated once
         vctx.build_b2b(x, y, 0.0, None, None, fx, fy)
         for pre, coarse in ((0, 0), (2, 2)):
             vctx.set_option("precond", pre)
@@ -630,7 +640,7 @@ def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: i
         for name, pre, coarse, reuse in variants:
             if coarse == 3 and learned is None:
                 continue
-            vctx = rctx if reuse else ctx
+            vctx = vctxs[name]
             vctx.build_b2b(st.x, st.y, st.alpha, st.ux, st.uy, fx, fy)  # fresh systems
             with torch.cuda.stream(stream):
                 dx.copy_(torch.from_numpy(st.x))
@@ -673,8 +683,8 @@ def simpl_report(torch, dev, stream, nl, x0, y0, iters: int = 30, init_rounds: i
                                                       np.linalg.norm(ref[0])),
                              "hpwl_rel_vs_fp64": (h - ref[1]) / ref[1]}
         rows.append(row)
-    ctx.close()
-    rctx.close()
+    for c in {id(c): c for c in vctxs.values()}.values():
+        c.close()
     names = [v[0] for v in variants if v[0] in rows[0]]
     summary = {}
     base = sum(r["fp64_jacobi"]["ms"] for r in rows)
@@ -1188,13 +1198,13 @@ def run_config4(args) -> int:
     return 0
 
 
-def run_simpl_report(iters: int) -> int:
+def run_simpl_report(iters: int, weights: str = None) -> int:
     import torch
     dev = torch.device("cuda:0")
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
     raw, nl, x, y, ax, ay = make_workload(1)
-    learned = load_coarse_network(dev)
+    learned = load_coarse_network(dev, weights)
     rep = simpl_report(torch, dev, stream, nl, x, y, iters, learned=learned)
     if learned is not None:
         learned.close()
@@ -1205,13 +1215,14 @@ def run_simpl_report(iters: int) -> int:
 COARSE_WEIGHTS = os.path.join(ROOT, "ktplace_b200", "weights", "learned_coarse.npy")
 
 
-def load_coarse_network(dev):
+def load_coarse_network(dev, path: str = None):
     """The trained coarse-vector network, or None when no weights exist."""
-    if not os.path.exists(COARSE_WEIGHTS):
+    path = path or COARSE_WEIGHTS
+    if not os.path.exists(path):
         return None
     from ktplace_b200.learned import Learned
     learned = Learned(dev.index or 0)
-    learned.load(COARSE_WEIGHTS)
+    learned.load(path)
     return learned
 
 
@@ -1224,7 +1235,7 @@ def main():
     if args.config4:
         return run_config4(args)
     if args.simpl_report:
-        return run_simpl_report(args.simpl_report)
+        return run_simpl_report(args.simpl_report, args.coarse_weights)
     if args.profile_once:
         return profile_once()
     if args.profile_lal:

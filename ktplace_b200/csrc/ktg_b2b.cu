@@ -4,9 +4,10 @@
 // simpl_lss.cc:11-114) and simplPlacer::Impl::getHpwl (simpl_placer.cc:
 // 256-275). Five launches build both axes at once:
 //
-//   k_bound_pins  one thread per net: first-index argmin/argmax of the pin
-//                 coordinate for x and y (simpl_lss.cc:32-45) and, from the
-//                 same pass, the net's half perimeter (HPWL of the inputs).
+//   k_bound_pins  one lane per net, pins staged by the warp: first-index
+//                 argmin/argmax of the pin coordinate for x and y
+//                 (simpl_lss.cc:32-45) and, from the same pass, the net's
+//                 half perimeter (HPWL of the inputs).
 //   k_row_count   one thread per (axis, movable cell): number of movable
 //                 other ends of its B2B edges (simpl_lss.cc:75-83), plus a
 //                 per-block total.
@@ -70,7 +71,19 @@ __device__ __forceinline__ double cell_pos(const double *pos, const double *fixe
     return var >= 0 ? pos[var] : fixed[cell];
 }
 
-// One thread per net. WithBounds: also choose the bound pins of both axes.
+// Pins staged per warp and round by k_bound_pins (two per lane).
+constexpr int kPinChunk = 64;
+
+// One lane per net, the pins staged by the warp. Each warp owns 32
+// consecutive nets, whose pins are contiguous; the warp walks that pin range
+// in chunks of kPinChunk, every lane loading and positioning pins of the
+// chunk (coalesced pin reads, independent position gathers), and then each
+// lane scans the part of its own net that falls in the chunk from shared
+// memory, in pin order, carrying its running bounds across chunks. The scan
+// order and the comparisons are the reference's, so the bound pins (first
+// index wins on ties) and the half perimeters are the sequential ones; a
+// net's term lands in the same thread as with one thread per net, so the
+// block sums are too. WithBounds: also choose the bound pins of both axes.
 template <bool WithBounds, int R = kSimpl>
 __global__ void __launch_bounds__(kBuildThreads)
     k_bound_pins(NetlistDev nl, const double *__restrict__ x, const double *__restrict__ y,
@@ -79,24 +92,43 @@ __global__ void __launch_bounds__(kBuildThreads)
                  double *__restrict__ partials, unsigned *__restrict__ ticket,
                  double *__restrict__ hpwl_out, double *__restrict__ terms = nullptr) {
     __shared__ double scratch[40];
+    __shared__ double spx[kBuildThreads / 32][kPinChunk];
+    __shared__ double spy[kBuildThreads / 32][kPinChunk];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    double term = 0.0;
+    const int kw0 = blockIdx.x * blockDim.x + (wid << 5);  // the warp's first net
+    int32_t s = 0, e = 0, p0 = 0, p1 = 0;
     if (k < nl.N) {
-        const int32_t s = nl.net_start[k];
-        const int32_t deg = nl.net_start[k + 1] - s;
-        uint32_t lx = 0, hx = 0, ly = 0, hy = 0;
-        double vlx = 0.0, vhx = 0.0, vly = 0.0, vhy = 0.0;
-        // BBox::getEmpty then BBox::extend (geometry/kt_geometry.cc:70-75)
-        double bx0 = __longlong_as_double(0x7ff0000000000000ll);   // +inf
-        double by0 = bx0;
-        double bx1 = -bx0;
-        double by1 = -bx0;
-        for (int32_t q = 0; q < deg; ++q) {
-            const int32_t p = s + q;
-            const int32_t cell = nl.pin_cell[p];
-            const int32_t var = nl.pin_var[p];
-            const double px = cell_pos(x, nl.fixed_x, var, cell) + nl.off_x[p];
-            const double py = cell_pos(y, nl.fixed_y, var, cell) + nl.off_y[p];
+        s = nl.net_start[k];
+        e = nl.net_start[k + 1];
+    }
+    if (kw0 < nl.N) {  // warp-uniform pin range of nets [kw0, kw0 + 32)
+        p0 = nl.net_start[kw0];
+        p1 = nl.net_start[min(kw0 + 32, nl.N)];
+    }
+    uint32_t lx = 0, hx = 0, ly = 0, hy = 0;
+    double vlx = 0.0, vhx = 0.0, vly = 0.0, vhy = 0.0;
+    // BBox::getEmpty then BBox::extend (geometry/kt_geometry.cc:70-75)
+    double bx0 = __longlong_as_double(0x7ff0000000000000ll);  // +inf
+    double by0 = bx0;
+    double bx1 = -bx0;
+    double by1 = -bx0;
+    for (int32_t cb = p0; cb < p1; cb += kPinChunk) {
+        for (int j = lane; j < kPinChunk; j += 32) {
+            const int32_t p = cb + j;
+            if (p < p1) {
+                const int32_t cell = nl.pin_cell[p];
+                const int32_t var = nl.pin_var[p];
+                spx[wid][j] = cell_pos(x, nl.fixed_x, var, cell) + nl.off_x[p];
+                spy[wid][j] = cell_pos(y, nl.fixed_y, var, cell) + nl.off_y[p];
+            }
+        }
+        __syncwarp();
+        const int32_t qa = max(s, cb), qb = min(e, cb + kPinChunk);
+        for (int32_t p = qa; p < qb; ++p) {
+            const int32_t q = p - s;
+            const double px = spx[wid][p - cb];
+            const double py = spy[wid][p - cb];
             if (WithBounds) {
                 if (q == 0) {
                     vlx = vhx = px;
@@ -115,6 +147,10 @@ __global__ void __launch_bounds__(kBuildThreads)
             bx1 = ref_max(bx1, px);
             by1 = ref_max(by1, py);
         }
+        __syncwarp();
+    }
+    double term = 0.0;
+    if (k < nl.N) {
         if (WithBounds) {
             lo_x[k] = lx;
             hi_x[k] = hx;
@@ -122,7 +158,7 @@ __global__ void __launch_bounds__(kBuildThreads)
             hi_y[k] = hy;
         }
         // getHalfPerimeter: 0 for an empty box; nets with < 2 pins add 0.
-        if (deg >= 2 && !(bx0 > bx1 || by0 > by1)) term = (bx1 - bx0) + (by1 - by0);
+        if (e - s >= 2 && !(bx0 > bx1 || by0 > by1)) term = (bx1 - bx0) + (by1 - by0);
         if (terms) terms[k] = term;
     }
     if (terms) return;  // summed in the reference's order by k_hpwl_ref_order

@@ -212,12 +212,13 @@ def compare_solvers(learned: Learned, ctx: Context, nl, x0, y0, iters: int, tol:
 # ---- learned coarse vector ----------------------------------------------------
 
 DATASET_MAGIC = b"KTGCOARS"
-DATASET_VERSION = 1
+DATASET_VERSION = 2
 _REC = np.dtype([("design", "<i4"), ("seed", "<i8"), ("cells", "<i8"), ("nets", "<i8"),
                  ("iteration", "<i4"), ("alpha", "<f8"), ("n", "<i8"), ("nnz_x", "<i8"),
                  ("nnz_y", "<i8"), ("fp64_iters_x", "<i4"), ("fp64_iters_y", "<i4"),
                  ("agg_iters_x", "<i4"), ("agg_iters_y", "<i4"), ("loss_x", "<f8"),
-                 ("loss_y", "<f8"), ("system_sha", "S32"), ("solution_sha", "S32")])
+                 ("loss_y", "<f8"), ("system_sha", "u1", (32,)),
+                 ("solution_sha", "u1", (32,))])
 
 
 class CoarseDataset:
@@ -242,7 +243,8 @@ class CoarseDataset:
         arr = np.zeros(len(self.records), dtype=_REC)
         for i, r in enumerate(self.records):
             for k in _REC.names:
-                arr[i][k] = r[k]
+                v = r[k]
+                arr[i][k] = np.frombuffer(v, dtype=np.uint8) if isinstance(v, bytes) else v
         with open(path, "wb") as f:
             f.write(DATASET_MAGIC)
             f.write(np.array([DATASET_VERSION, len(arr)], dtype="<u4").tobytes())
@@ -343,6 +345,42 @@ def train_coarse(learned: Learned, designs: Iterable, iters: int = 30, epochs: i
                     f"loss {np.mean(losses[-2 * iters:]):.4e}")
     if own:
         ctx.close()
+    return losses
+
+
+def train_coarse_recorded(learned: Learned, records, ctx: Optional[Context] = None, log=None,
+                          epoch: int = 0) -> list:
+    """One epoch over a recorded training set (CoarseDataset.load): every
+    design is regenerated from its record, its GPU SimPL loop rerun, and each
+    recorded system checked against its digests (A, b and the FP64 solution
+    x*) before its Adam steps. Returns the per-step losses."""
+    from .train_precond import dataset_designs
+    own = ctx is None
+    ctx = ctx or Context(0)
+    want = {(int(r["design"]), int(r["iteration"])): r for r in records}
+    losses = []
+    try:
+        for k, (nl, x0, y0, _), its in dataset_designs(records):
+            ctx.upload_netlist(nl)
+            for st, f, (ex, ey), _ in coarse_training_systems(ctx, nl, x0, y0, its[-1] + 1):
+                rec = want.get((k, st.it))
+                if rec is None:
+                    continue
+                sx, sy = ctx.system(0), ctx.system(1)
+                sha = _sha(*[sx[q] for q in ("row_ptr", "col", "val", "diag", "rhs")],
+                           *[sy[q] for q in ("row_ptr", "col", "val", "diag", "rhs")])
+                if (sha != rec["system_sha"].tobytes() or
+                        _sha(f["x"], f["y"]) != rec["solution_sha"].tobytes()):
+                    raise RuntimeError(f"design {k} iteration {st.it}: regenerated system "
+                                       "differs from the recorded one")
+                losses += [learned.coarse_train_step(ctx, 0, ex),
+                           learned.coarse_train_step(ctx, 1, ey)]
+            if log:
+                log(f"epoch {epoch} (recorded) design {k} ({nl.num_movable} cells): "
+                    f"loss {np.mean(losses[-2 * len(its):]):.4e}")
+    finally:
+        if own:
+            ctx.close()
     return losses
 
 

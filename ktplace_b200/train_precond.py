@@ -1,16 +1,22 @@
 """Trains the learned networks of the mixed solve and writes their weights.
 
     python -m ktplace_b200.train_precond --coarse [--designs 64] [--iters 30]
-        [--min-cells 5000] [--max-cells 500000]
+        [--min-cells 5000] [--max-cells 500000] [--epochs-from-dataset E]
         [--out ktplace_b200/weights/learned_coarse.npy]
         [--dataset ktplace_b200/weights/coarse_dataset.bin]
+    python -m ktplace_b200.train_precond --coarse --from-dataset FILE
+        [--epochs-from-dataset E]
 
 trains the learned coarse vector of the two-level aggregation preconditioner
 on the systems of the GPU SimPL loop (B2B initial rounds, then global
 iterations anchored at the look-ahead-legalized positions, anchor weight
 0.01 -> 1.0) of seeded synthetic netlists with log-uniform cell counts,
-designs x iters x 2 systems (3,840 with the defaults), and writes the
-training set's record file (learned.CoarseDataset) beside the weights.
+designs x iters x 2 systems (3,840 with the defaults). The first epoch
+streams the systems as the loop produces them and writes the training set's
+record file (learned.CoarseDataset); further epochs, or a run from an
+existing file, consume that file: each recorded system is regenerated from
+its design and iteration and checked against its recorded digests before it
+is used.
 
     python -m ktplace_b200.train_precond [--designs 40] [--iters 25] [--epochs 3]
                                           [--out ktplace_b200/weights/learned_precond.npy]
@@ -39,27 +45,47 @@ COARSE_OUT = os.path.join(HERE, "weights", "learned_coarse.npy")
 COARSE_DATASET = os.path.join(HERE, "weights", "coarse_dataset.bin")
 
 
+def coarse_design(k: int, cells: int, s: int):
+    """Training design k: `cells` movable cells, generator seed s; returns
+    (netlist, x0, y0, s). Odd designs have mean degree 3.5 and 60% density,
+    even ones a heavier-tailed degree law and 70%; every third carries
+    macros."""
+    from . import synth, netlist
+    spec = synth.SynthSpec(num_movable=cells, num_nets=int(cells * 1.05),
+                           num_pads=max(50, int(200 * math.sqrt(cells / 12_000))),
+                           num_rows=max(20, int(120 * math.sqrt(cells / 12_000))),
+                           utilization=0.6 if k % 2 else 0.7,
+                           num_macros=int(cells / 400) if k % 3 == 0 else 0,
+                           degree_exponent=synth.exponent_for_mean(3.5) if k % 2 else 2.5,
+                           seed=s, name=f"coarse{k}")
+    raw = synth.generate(spec)
+    nl = netlist.flatten(raw)
+    x0, y0 = synth.seed_positions(raw, nl.num_movable, s + 500)
+    return nl, x0, y0, s
+
+
 def coarse_designs(count: int, seed: int = 9000, min_cells: int = 5_000,
                    max_cells: int = 500_000):
     """Seeded synthetic netlists in the shape of the single-netlist and batch
     configurations, cell counts log-uniform in [min_cells, max_cells];
     yields (netlist, x0, y0, seed)."""
-    from . import synth, netlist
     rng = np.random.default_rng(seed)
     for k in range(count):
         cells = int(round(math.exp(rng.uniform(math.log(min_cells), math.log(max_cells)))))
-        s = seed + k
-        spec = synth.SynthSpec(num_movable=cells, num_nets=int(cells * 1.05),
-                               num_pads=max(50, int(200 * math.sqrt(cells / 12_000))),
-                               num_rows=max(20, int(120 * math.sqrt(cells / 12_000))),
-                               utilization=0.6 if k % 2 else 0.7,
-                               num_macros=int(cells / 400) if k % 3 == 0 else 0,
-                               degree_exponent=synth.exponent_for_mean(3.5) if k % 2 else 2.5,
-                               seed=s, name=f"coarse{k}")
-        raw = synth.generate(spec)
-        nl = netlist.flatten(raw)
-        x0, y0 = synth.seed_positions(raw, nl.num_movable, s + 500)
-        yield nl, x0, y0, s
+        yield coarse_design(k, cells, seed + k)
+
+
+def dataset_designs(records):
+    """The designs a recorded training set was drawn from, regenerated from
+    the records (design index, cells, seed), with the global iterations
+    recorded for each: yields (design index, (netlist, x0, y0, seed),
+    iterations)."""
+    seen = {}
+    for r in records:
+        key = (int(r["design"]), int(r["cells"]), int(r["seed"]))
+        seen.setdefault(key, set()).add(int(r["iteration"]))
+    for (k, cells, s), its in seen.items():
+        yield k, coarse_design(k, cells, s), sorted(its)
 
 
 def training_designs(count: int, seed: int = 7000, max_cells: int = 100_000):
@@ -97,6 +123,11 @@ def main(argv=None) -> int:
     ap.add_argument("--min-cells", type=int, default=5_000)
     ap.add_argument("--max-cells", type=int, default=500_000)
     ap.add_argument("--dataset", default=COARSE_DATASET)
+    ap.add_argument("--epochs-from-dataset", type=int, default=0,
+                    help="further epochs over the recorded training set (regenerated and "
+                         "checked against its digests)")
+    ap.add_argument("--from-dataset", default=None,
+                    help="train only from this recorded training set")
     args = ap.parse_args(argv)
     if args.coarse:
         return main_coarse(args)
@@ -126,23 +157,34 @@ def main(argv=None) -> int:
 
 def main_coarse(args) -> int:
     from .gpu import Context
-    from .learned import Learned, CoarseDataset, train_coarse
+    from .learned import Learned, CoarseDataset, train_coarse, train_coarse_recorded
     out = args.out or COARSE_OUT
     learned = Learned(0, seed=args.seed)
     learned.set_option("lr", args.lr)
     ctx = Context(0)
-    ds = CoarseDataset()
     t0 = time.time()
-    designs = coarse_designs(args.designs, min_cells=args.min_cells, max_cells=args.max_cells)
-    losses = train_coarse(learned, designs, iters=args.iters, epochs=1, ctx=ctx, dataset=ds,
-                          log=lambda m: print(m, f"({time.time() - t0:.0f}s)", flush=True))
+    log = lambda m: print(m, f"({time.time() - t0:.0f}s)", flush=True)  # noqa: E731
+    losses = []
+    if args.from_dataset:
+        records = CoarseDataset.load(args.from_dataset)
+        epochs = max(1, args.epochs_from_dataset)
+    else:
+        ds = CoarseDataset()
+        designs = coarse_designs(args.designs, min_cells=args.min_cells, max_cells=args.max_cells)
+        losses = train_coarse(learned, designs, iters=args.iters, epochs=1, ctx=ctx, dataset=ds,
+                              log=log)
+        ds.save(args.dataset)
+        print("wrote", args.dataset, f"({len(ds.records)} systems)", flush=True)
+        records = CoarseDataset.load(args.dataset)
+        epochs = args.epochs_from_dataset
+    for ep in range(epochs):
+        losses += train_coarse_recorded(learned, records, ctx=ctx, log=log, epoch=ep)
     k = max(1, len(losses) // 10)
     print(f"{len(losses)} steps in {time.time() - t0:.1f}s; mean loss first tenth "
           f"{np.mean(losses[:k]):.4e}, last tenth {np.mean(losses[-k:]):.4e}", flush=True)
     os.makedirs(os.path.dirname(out), exist_ok=True)
     learned.save(out)
-    ds.save(args.dataset)
-    print("wrote", out, "and", args.dataset, f"({len(ds.records)} systems)")
+    print("wrote", out)
     ctx.close()
     learned.close()
     return 0
