@@ -1,7 +1,8 @@
 // GPU bodies for two private members of KTPlace's simplPlacer::Impl
-// (globalPlacer/simpl/simpl_placer.cc:256-289), for a simpl_placer.cc
-// patched to call them (oracle/hooks/simpl_placer_b200.patch shows the
-// patch): getHpwl -> ktg_hpwl, getOccupancy -> ktg_occupancy. They run on the
+// (globalPlacer/simpl/simpl_placer.cc:256-289), for a simpl_placer.cc whose
+// two member bodies are replaced by calls to them (oracle/hooks/
+// apply_hooks.py writes such a copy): getHpwl -> ktg_hpwl, getOccupancy ->
+// ktg_occupancy; getOverflow keeps its host loop over the returned map. They run on the
 // same GPU context as the drop-in's buildB2B / solveBothAxes
 // (simpl_lss_b200.cc), which then holds the cells' real sizes.
 #pragma once

@@ -170,3 +170,82 @@ def test_agg_reuse_on_simpl_systems(gpu_ctx):
             gpu_ctx.set_option("coarse", 0)
             gpu_ctx.set_option("precond", 0)
     assert reused <= 1.34 * fresh, (reused, fresh)
+
+
+def test_trained_coarse_vector_beats_network_off():
+    """The committed trained coarse-vector network against the same solver
+    with the network switched off (the aggregation preconditioner with no
+    coarse vector), along a SimPL run of a held-out 60k-cell design: the
+    learned vector (prepared per build) needs fewer inner iterations and
+    less device time (CUDA events, per-netlist set-up untimed), and every
+    solve meets the FP64 tolerance on the true residual."""
+    import torch
+    from ktplace_b200 import grid as kgrid
+    from ktplace_b200 import simpl
+    from ktplace_b200.gpu import Context
+    from ktplace_b200.learned import Learned
+    from ktplace_b200.train_precond import coarse_design, COARSE_OUT
+    from ktplace_b200._lib import MixedInfo
+    import ctypes
+    nl, x0, y0, _ = coarse_design(1, 60_000, 4242)  # seed outside the training set
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.Stream(device=dev)
+    learned = Learned(0)
+    learned.load(COARSE_OUT)
+    ctxs = {}
+    for name, coarse in (("off", 0), ("learned", 3)):
+        c = Context(0)
+        c.set_stream(stream.cuda_stream)
+        c.upload_netlist(nl)
+        c.set_option("precond", 2)
+        c.set_option("coarse", coarse)
+        c.set_option("agg_reuse", 4)
+        ctxs[name] = c
+    loop_ctx = Context(0)
+    try:
+        loop_ctx.upload_netlist(nl)
+        g = kgrid.build_grid(nl, kgrid.default_bins_per_axis(nl.num_movable), 1.0)
+        loop = simpl.GlobalLoop(loop_ctx, nl, g, kgrid.build_free_space(nl), tol=TOL,
+                                max_iter=MAX_ITER)
+        x, y = loop.initial_rounds(x0, y0, 3)
+        fx, fy = nl.floors()
+        for c in ctxs.values():  # untimed: buffers, and the per-netlist trunk
+            c.build_b2b(x, y, 0.0, None, None, fx, fy)
+            learned.prepare_coarse(c)
+            c.solve_mixed(x, y, TOL)
+        ms = {k: 0.0 for k in ctxs}
+        inner = {k: 0 for k in ctxs}
+        with torch.cuda.stream(stream):
+            dx = torch.zeros(nl.num_movable, dtype=torch.float64, device=dev)
+            dy = torch.zeros_like(dx)
+            minfo = torch.zeros(ctypes.sizeof(MixedInfo), dtype=torch.uint8, device=dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for st in loop.iterations(x, y, 10):
+            for name, c in ctxs.items():
+                c.build_b2b(st.x, st.y, st.alpha, st.ux, st.uy, fx, fy)
+                with torch.cuda.stream(stream):
+                    dx.copy_(torch.from_numpy(st.x))
+                    dy.copy_(torch.from_numpy(st.y))
+                torch.cuda.synchronize(dev)
+                with torch.cuda.stream(stream):
+                    e0.record(stream)
+                    if name == "learned":
+                        learned.prepare_coarse(c)
+                    c.solve_mixed_dev(dx, dy, TOL, 1e-3, MAX_ITER, 50, minfo)
+                    e1.record(stream)
+                e1.synchronize()
+                if st.it > 0:  # the run's first build makes the aggregates afresh in both
+                    ms[name] += e0.elapsed_time(e1)
+                mi = MixedInfo.from_buffer_copy(bytes(minfo.cpu().numpy()))
+                inner[name] += int(mi.inner_x) + int(mi.inner_y)
+                sx, sy = c.system(0), c.system(1)
+                assert true_resid(sx, dx.cpu().numpy()) <= TOL * 1.0001
+                assert true_resid(sy, dy.cpu().numpy()) <= TOL * 1.0001
+        assert inner["learned"] < inner["off"], inner
+        assert ms["learned"] < ms["off"], (ms, inner)
+    finally:
+        for c in ctxs.values():
+            c.close()
+        loop_ctx.close()
+        learned.close()
