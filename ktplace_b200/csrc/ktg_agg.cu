@@ -785,95 +785,128 @@ __global__ void __launch_bounds__(32 * kPfWarps)
     }
 }
 
-// One thread per aggregate: its block of A (the aggregate's rows and
-// columns, duplicates summed in storage order after the diagonal) in the
-// thread's shared-memory slot, an FP64 Cholesky B = L L^T (row by row, one
-// reciprocal per pivot), L^-1 by forward substitution and B^-1 = L^-T L^-1,
-// written as 8 FP32 per row (zero past the aggregate's size). A non-positive
-// pivot gives the aggregate the inverse of its diagonal instead. The slot
-// stride of 65 doubles keeps a half-warp's 64-bit accesses on distinct banks.
-constexpr int kInvThreads = 64;
-constexpr int kSlot = kAggMax * kAggMax + 1;
-__global__ void __launch_bounds__(kInvThreads)
-    k_blockinv_slots(const int32_t *count, const int32_t *__restrict__ agg_start,
+// Eight lanes per aggregate (lane m holds row m of its block), four
+// aggregates per warp, everything in registers. Each lane forms its row of
+// the block of A (the diagonal, then the row's entries inside the aggregate
+// in storage order, duplicates summed), the group factors B = L L^T in FP64
+// row by row (the pivot lane takes sqrt and one reciprocal, its row reaches
+// the others by shuffles), and lane m then solves L L^T x = e_m by forward
+// and back substitution, fetching the rows of L it needs by shuffles: x is
+// column m of B^-1, that is row m, written as 8 FP32 (zero past the
+// aggregate's size; two 16-byte stores, consecutive lanes on consecutive
+// rows). A non-positive pivot gives the aggregate the inverse of its
+// diagonal instead. Every loop runs over the full eight rows with the
+// aggregate's size as a predicate, so the shuffles see all lanes.
+constexpr int kInvWarps = 8;
+constexpr int kInvPerBlock = kInvWarps * 4;  // aggregates per block
+__global__ void __launch_bounds__(32 * kInvWarps)
+    k_blockinv_lanes(const int32_t *count, const int32_t *__restrict__ agg_start,
                      const int32_t *__restrict__ size, int32_t n, const int32_t *__restrict__ prp,
                      const int32_t *__restrict__ pcol, const double *__restrict__ pval,
                      const double *__restrict__ pdiag, float *__restrict__ minv,
                      int32_t *__restrict__ meta) {
-    __shared__ double slots[kInvThreads * kSlot];
-    const int32_t J = static_cast<int32_t>(blockIdx.x) * kInvThreads + threadIdx.x;
-    if (J >= *count) return;
-    double *B = slots + threadIdx.x * kSlot;  // B[r * 8 + c]
-    const int32_t first = __ldg(agg_start + J);
-    const int k = __ldg(size + J);
-    const int32_t first_l = first >= n ? first - n : first;
-    for (int q = 0; q < kAggMax * kAggMax; ++q) B[q] = 0.0;
-    for (int m = 0; m < k; ++m) {
+    const int lane = threadIdx.x & 31;
+    const int g0 = lane & ~7;  // first lane of this aggregate's group
+    const int m = lane & 7;
+    const int32_t J = (static_cast<int32_t>(blockIdx.x) * kInvWarps + (threadIdx.x >> 5)) * 4 + (lane >> 3);
+    const int32_t cnt = *count;
+    if ((static_cast<int32_t>(blockIdx.x) * kInvWarps + (threadIdx.x >> 5)) * 4 >= cnt) return;  // whole warp
+    int k = 0;
+    int32_t first = 0, first_l = 0;
+    if (J < cnt) {
+        first = __ldg(agg_start + J);
+        k = __ldg(size + J);
+        first_l = first >= n ? first - n : first;
+    }
+    const bool mine = m < k;
+    double b[kAggMax];
+#pragma unroll
+    for (int t = 0; t < kAggMax; ++t) b[t] = 0.0;
+    double d = 1.0;
+    if (mine) {
         const int32_t row = first + m;
-        double *Bm = B + m * kAggMax;
-        Bm[m] += __ldg(pdiag + row);
+        d = __ldg(pdiag + row);
+#pragma unroll
+        for (int t = 0; t < kAggMax; ++t)
+            if (t == m) b[t] += d;
+        // four entries per round with independent loads (the value loads do
+        // not wait for the column test), added in storage order
         const int32_t e1 = __ldg(prp + row + 1);
-        for (int32_t e = __ldg(prp + row); e < e1; ++e) {
-            const int32_t qe = __ldg(pcol + e) - first_l;
-            if (qe >= 0 && qe < k) Bm[qe] += __ldg(pval + e);
-        }
-    }
-    // Cholesky in place: L[r][c] for c <= r overwrites B[r][c]
-    bool ok = true;
-    double rinv[kAggMax];
-    for (int j = 0; j < k && ok; ++j) {
-        double *Bj = B + j * kAggMax;
-        double sj = Bj[j];
-        for (int q = 0; q < j; ++q) sj -= Bj[q] * Bj[q];
-        ok = sj > 0.0;
-        if (!ok) break;
-        Bj[j] = sqrt(sj);
-        rinv[j] = 1.0 / Bj[j];
-        for (int i = j + 1; i < k; ++i) {
-            double *Bi = B + i * kAggMax;
-            double u = Bi[j];
-            for (int q = 0; q < j; ++q) u -= Bi[q] * Bj[q];
-            Bi[j] = u * rinv[j];
-        }
-    }
-    float *dst = minv + static_cast<size_t>(first) * kAggMax;
-    if (!ok) {
-        for (int m = 0; m < k; ++m) {
-            for (int q = 0; q < kAggMax; ++q)
-                dst[m * kAggMax + q] = q == m ? static_cast<float>(1.0 / __ldg(pdiag + first + m))
-                                              : 0.0f;
-            meta[first + m] = first_l * kAggMax + (k - 1);
-        }
-        return;
-    }
-    // L^-1 (lower) into the upper triangle's mirror: Li[r][c] kept at B[c][r]
-    // for c < r (the strict upper part, free after the factorisation) and the
-    // diagonal rinv
-    for (int r = 0; r < k; ++r) {
-        for (int c2 = 0; c2 < r; ++c2) {
-            double acc = 0.0;  // sum_{t = c2}^{r-1} L[r][t] Li[t][c2]
-            for (int t = c2; t < r; ++t)
-                acc += B[r * kAggMax + t] * (t == c2 ? rinv[c2] : B[c2 * kAggMax + t]);
-            B[c2 * kAggMax + r] = -acc * rinv[r];
-        }
-    }
-    // B^-1[i][c] = sum_{t >= max(i, c)} Li[t][i] Li[t][c]
-    for (int m = 0; m < k; ++m) {
-        for (int q = 0; q < kAggMax; ++q) {
-            float v = 0.0f;
-            if (q < k) {
-                double acc = 0.0;
-                for (int t = m > q ? m : q; t < k; ++t) {
-                    const double a = t == m ? rinv[m] : B[m * kAggMax + t];
-                    const double b = t == q ? rinv[q] : B[q * kAggMax + t];
-                    acc += a * b;
-                }
-                v = static_cast<float>(acc);
+        for (int32_t e = __ldg(prp + row); e < e1; e += 4) {
+            int32_t cq[4];
+            double cv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                cq[u] = e + u < e1 ? __ldg(pcol + e + u) - first_l : -1;
+                cv[u] = e + u < e1 ? __ldg(pval + e + u) : 0.0;
             }
-            dst[m * kAggMax + q] = v;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int32_t q = cq[u];
+#pragma unroll
+                for (int t = 0; t < kAggMax; ++t)
+                    if (t == q && q < k) b[t] += cv[u];
+            }
         }
-        meta[first + m] = first_l * kAggMax + (k - 1);
     }
+    // Cholesky: b becomes row m of L (entries past m unused)
+    bool ok = true;
+    double rinv = 0.0;  // 1 / L[m][m]
+#pragma unroll
+    for (int j = 0; j < kAggMax; ++j) {
+        double s = b[j];
+#pragma unroll
+        for (int q = 0; q < j; ++q) s -= b[q] * b[q];
+        const bool piv = m == j && mine;
+        const int good = (piv && !(s > 0.0)) ? 0 : 1;
+        const bool gok = __shfl_sync(0xffffffffu, good, g0 + j) != 0;  // the group's pivot
+        if (piv && s > 0.0) {
+            b[j] = sqrt(s);
+            rinv = 1.0 / b[j];
+        }
+        const double rj = __shfl_sync(0xffffffffu, rinv, g0 + j);
+        double u = b[j];
+#pragma unroll
+        for (int q = 0; q < j; ++q) u -= b[q] * __shfl_sync(0xffffffffu, b[q], g0 + j);
+        if (j < k) ok = ok && gok;
+        if (mine && m > j && j < k) b[j] = u * rj;
+    }
+    // (the substitutions run on every lane, so the shuffles stay uniform;
+    // a failed group's result is discarded below)
+    float out[kAggMax];
+    {
+        // forward: y = L^-1 e_m (y[i] = 0 for i < m)
+        double y[kAggMax];
+#pragma unroll
+        for (int i = 0; i < kAggMax; ++i) {
+            const double ri = __shfl_sync(0xffffffffu, rinv, g0 + i);
+            double acc = 0.0;
+#pragma unroll
+            for (int q = 0; q < i; ++q) acc += __shfl_sync(0xffffffffu, b[q], g0 + i) * y[q];
+            y[i] = i < m ? 0.0 : (i == m ? ri : -acc * ri);
+        }
+        // back: x = L^-T y, in place (y[i] is read before x[i] replaces it)
+#pragma unroll
+        for (int i = kAggMax - 1; i >= 0; --i) {
+            const double ri = __shfl_sync(0xffffffffu, rinv, g0 + i);
+            double acc = y[i];
+#pragma unroll
+            for (int q = i + 1; q < kAggMax; ++q) {
+                const double lqi = __shfl_sync(0xffffffffu, b[i], g0 + q);  // L[q][i]
+                if (q < k) acc -= lqi * y[q];
+            }
+            y[i] = acc * ri;
+        }
+#pragma unroll
+        for (int t = 0; t < kAggMax; ++t)
+            out[t] = ok ? (t < k ? static_cast<float>(y[t]) : 0.0f)
+                        : (t == m ? static_cast<float>(1.0 / d) : 0.0f);
+    }
+    if (!mine) return;
+    float4 *dst = reinterpret_cast<float4 *>(minv + static_cast<size_t>(first + m) * kAggMax);
+    dst[0] = make_float4(out[0], out[1], out[2], out[3]);
+    dst[1] = make_float4(out[4], out[5], out[6], out[7]);
+    meta[first + m] = first_l * kAggMax + (k - 1);
 }
 
 // blk_start[b] = first aggregate start >= b * ceil(rows / grid).
@@ -1222,7 +1255,7 @@ int build_agg_values(ktg_ctx *c) {
     k_pfill_tiles<<<blocks_for(rows, 32 * kPfWarps), 32 * kPfWarps, 0, c->stream>>>(
         L0, R, s->order, s->newpos, s->prp, c->sys[0].rhs, c->sys[1].rhs, s->pcol, s->pval,
         s->pval32, s->pdiag, s->prhs, zmode, c->coarse_z, s->zd);
-    k_blockinv_slots<<<blocks_for(rows, kInvThreads), kInvThreads, 0, c->stream>>>(
+    k_blockinv_lanes<<<blocks_for(rows, kInvPerBlock), 32 * kInvWarps, 0, c->stream>>>(
         nagg, s->agg_start, s->final_size, static_cast<int32_t>(n), s->prp, s->pcol, s->pval,
         s->pdiag, s->minv, s->meta);
     c->launches += 2;

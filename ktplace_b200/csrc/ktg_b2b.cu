@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(1024)
 constexpr int32_t kHeavyRow = 32;
 
 template <int R = kSimpl>
-__global__ void __launch_bounds__(kBuildThreads)
+__global__ void __launch_bounds__(kBuildThreads, 4)
     k_fill(NetlistDev nl, AxisArgs ax, AxisArgs ay, int32_t blocks_per_axis, double alpha,
            const int32_t *__restrict__ row_cnt, const int64_t *__restrict__ block_first,
            int64_t cap, const int *__restrict__ status, int32_t *__restrict__ heavy) {
