@@ -968,12 +968,14 @@ def run_batch_leg(torch, dev, stream, steps: int, rank: int = 0, world: int = 1,
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    shape, split = solver.shape, solver.split
+    shape, split, offload = solver.shape, solver.split, solver.offload
     solver.close()
     systems = 2 * count
     return {"workload": f"{count} synthetic netlists (log-uniform 5k-200k cells), x+y = "
-                        f"{systems} systems, FP32 PCG in FP64 refinement to true rtol 1e-6, "
-                        "persistent cluster launches (size classes) replayed as one graph",
+                        f"{systems} systems, FP32 PCG in FP64 refinement to true rtol 1e-6; "
+                        "the largest x/y pairs on the whole GPU (aggregation-preconditioned), "
+                        "the rest in persistent cluster launches (size classes) replayed as "
+                        "one graph",
             "systems": systems, "rows_total": int(plan.total), "ms_per_batch": ms_max,
             "systems_per_s": systems / (ms_max * 1e-3),
             "sharding": {"ranks": world, "units_per_rank": len(mine),
@@ -983,7 +985,8 @@ def run_batch_leg(torch, dev, stream, steps: int, rank: int = 0, world: int = 1,
             "latency_ms_p99": float(np.percentile(lat, 99)) if lat else None,
             "inner_iters_p50": float(np.percentile(iters, 50)) if iters else None,
             "autotuned_shape": {"cluster": shape[0], "threads": shape[1]} if shape else None,
-            "size_split": split}
+            "size_split": split,
+            "whole_gpu_pairs": offload}
 
 
 def profile_once():

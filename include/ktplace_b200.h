@@ -183,7 +183,9 @@ int ktg_download_system(ktg_ctx *ctx, int axis, int64_t *row_ptr, int32_t *col, 
 int ktg_download_bound_pins(ktg_ctx *ctx, int axis, uint32_t *lo, uint32_t *hi);
 
 /* Installs a caller-built system for one axis (host memory), for solving
- * systems assembled elsewhere (e.g. buildStar, simpl_lss.cc:116-201). */
+ * systems assembled elsewhere (e.g. buildStar, simpl_lss.cc:116-201). The
+ * other axis's system is kept when this one needs more room; a system of
+ * another size than the other axis's invalidates that axis. */
 int ktg_upload_system(ktg_ctx *ctx, int axis, int64_t n, const int64_t *row_ptr,
                       const int32_t *col, const double *val, const double *diag,
                       const double *rhs);
@@ -347,6 +349,24 @@ int ktg_batch_get_split(const ktg_batch *b, int64_t *rows, int *cluster, int *th
  * *base_ms: the unsplit time, *best_ms: the kept one. Resets x. */
 int ktg_batch_autotune_split(ktg_batch *b, double tol, int precision, double inner_tol,
                              int64_t max_iter, float *base_ms, float *best_ms);
+/* Whole-GPU path for the largest systems: pairs of consecutive systems of
+ * equal size >= `rows` (the x and y systems of one netlist, as
+ * ktg_batch_add_from_context adds them; 0 turns it off) are solved one pair
+ * after another by an internal context on the whole GPU, before the cluster
+ * launches take the rest: with precision 1 the mixed solve with
+ * preconditioner `precond` (0 Jacobi, 2 aggregation) and coarse vector
+ * `coarse` (0 none, 1 constant, 2 coupling share), with precision 0 the FP64
+ * solve. Their results carry the mixed inner iterations and rounds (or the
+ * FP64 iterations), the final true residual, status 1 when it misses tol,
+ * and the latency from the pair's start. */
+int ktg_batch_set_offload(ktg_batch *b, int64_t rows, int precond, int coarse);
+/* The threshold in force and how many pairs it sends to the whole GPU. */
+int ktg_batch_get_offload(const ktg_batch *b, int64_t *rows, int *pairs);
+/* Times full solves with no offload and with the 2-64 largest systems
+ * offloaded (split off during the trials, restored after) and keeps the
+ * fastest; run it before ktg_batch_autotune_split. Resets x. */
+int ktg_batch_autotune_offload(ktg_batch *b, double tol, int precision, double inner_tol,
+                               int64_t max_iter, float *base_ms, float *best_ms);
 /* Restores every system's start vector. */
 int ktg_batch_reset_x(ktg_batch *b);
 /* Enqueues the solve of every system on the batch's stream (graph replay). */

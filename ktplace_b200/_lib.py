@@ -141,6 +141,13 @@ SIGNATURES = [
                                                 ctypes.c_double, ctypes.c_int64,
                                                 ctypes.POINTER(ctypes.c_float),
                                                 ctypes.POINTER(ctypes.c_float)]),
+    ("ktg_batch_set_offload", ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
+    ("ktg_batch_get_offload", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64),
+                                             ctypes.POINTER(ctypes.c_int)]),
+    ("ktg_batch_autotune_offload", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int,
+                                                  ctypes.c_double, ctypes.c_int64,
+                                                  ctypes.POINTER(ctypes.c_float),
+                                                  ctypes.POINTER(ctypes.c_float)]),
     ("ktg_batch_reset_x", ctypes.c_int, [_vp]),
     ("ktg_batch_solve", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int64, ctypes.c_int,
                                        ctypes.c_double]),

@@ -133,13 +133,38 @@ void free_systems(ktg_ctx *c) {
 
 // Makes room for systems of `rows` rows and `nnz` entries per axis and for
 // per-net bound pins of the current netlist.
+// A larger array that keeps the first `keep` elements of the old one (the
+// copy is stream-ordered; cudaFree waits for it).
+template <typename T>
+int dev_grow_keep(ktg_ctx *c, T **p, int64_t keep, int64_t count) {
+    T *np = nullptr;
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&np), sizeof(T) * std::max<int64_t>(count, 1));
+    if (e != cudaSuccess) return ktg::cuda_check(c, e, "cudaMalloc");
+    if (*p && keep > 0) {
+        const cudaError_t ec = cudaMemcpyAsync(np, *p, sizeof(T) * keep, cudaMemcpyDeviceToDevice,
+                                               c->stream);
+        if (ec != cudaSuccess) {
+            cudaFree(np);
+            return ktg::cuda_check(c, ec, "cudaMemcpyAsync");
+        }
+    }
+    if (*p) cudaFree(*p);
+    *p = np;
+    return KTG_OK;
+}
+
+// Room for systems of `rows` rows and `nnz` entries per axis. The arrays
+// that hold a system (row pointers, columns, values, diagonal, right-hand
+// side) keep their contents when they grow, so an axis installed earlier
+// stays valid; the solver scratch is just reallocated.
 int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
     int rc;
     if (rows > c->sys_cap_n) {
+        const int64_t old = c->sys_cap_n;
         for (auto &s : c->sys) {
-            if ((rc = dev_alloc(c, &s.row_ptr, rows + 1))) return rc;
-            if ((rc = dev_alloc(c, &s.diag, rows))) return rc;
-            if ((rc = dev_alloc(c, &s.rhs, rows))) return rc;
+            if ((rc = dev_grow_keep(c, &s.row_ptr, old > 0 ? old + 1 : 0, rows + 1))) return rc;
+            if ((rc = dev_grow_keep(c, &s.diag, old, rows))) return rc;
+            if ((rc = dev_grow_keep(c, &s.rhs, old, rows))) return rc;
             if ((rc = dev_alloc(c, &s.r, rows))) return rc;
             if ((rc = dev_alloc(c, &s.z, rows))) return rc;
             if ((rc = dev_alloc(c, &s.p, rows))) return rc;
@@ -160,9 +185,10 @@ int reserve_systems(ktg_ctx *c, int64_t rows, int64_t nnz) {
         c->stage_cap = rows;
     }
     if (nnz > c->sys_cap_nnz) {
+        const int64_t old = c->sys_cap_nnz;
         for (auto &s : c->sys) {
-            if ((rc = dev_alloc(c, &s.col, nnz))) return rc;
-            if ((rc = dev_alloc(c, &s.val, nnz))) return rc;
+            if ((rc = dev_grow_keep(c, &s.col, old, nnz))) return rc;
+            if ((rc = dev_grow_keep(c, &s.val, old, nnz))) return rc;
             if ((rc = dev_alloc(c, &s.val32, nnz))) return rc;
             if ((rc = dev_alloc(c, &s.s32, nnz))) return rc;
         }
@@ -185,6 +211,55 @@ int reserve_partials(ktg_ctx *c, int64_t count) {
 }
 
 }  // namespace
+
+namespace ktg {
+
+int reserve_system_arrays(ktg_ctx *c, int64_t rows, int64_t nnz) {  // contents kept
+    int rc = set_device(c);
+    if (rc) return rc;
+    return reserve_systems(c, rows, nnz);
+}
+
+// The system of one axis from device arrays (row pointers with offsets from
+// the row's system start, m entries), copied on the context's stream: what
+// ktg_upload_system does for host arrays, for callers that already hold the
+// system on this device (the batch's whole-GPU path).
+int load_system_device(ktg_ctx *c, int axis, int64_t n, int64_t m, const int32_t *rp,
+                       const int32_t *col, const double *val, const double *diag,
+                       const double *rhs) {
+    if (!c || (axis != 0 && axis != 1) || n < 0 || m < 0 || !rp) return KTG_ERR_ARG;
+    if (n > 0x3fffffffll || m > 0x7fffffffll)
+        return set_error(c, KTG_ERR_RANGE, "system exceeds 32-bit indices");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = reserve_systems(c, n, std::max<int64_t>(m, c->sys_cap_nnz)))) return rc;
+    AxisSystem &s = c->sys[axis];
+    KTG_CUDA(c, cudaMemcpyAsync(s.row_ptr, rp, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToDevice,
+                                c->stream));
+    if (m) {
+        KTG_CUDA(c, cudaMemcpyAsync(s.col, col, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice,
+                                    c->stream));
+        KTG_CUDA(c, cudaMemcpyAsync(s.val, val, sizeof(double) * m, cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    }
+    if (n) {
+        KTG_CUDA(c, cudaMemcpyAsync(s.diag, diag, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                    c->stream));
+        KTG_CUDA(c, cudaMemcpyAsync(s.rhs, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    }
+    if (n != c->sys_n) c->axis_valid[1 - axis] = false;
+    c->axis_valid[axis] = true;
+    c->val32_valid = false;
+    c->precond_ready = false;
+    c->agg_ready = false;
+    c->coarse_z_ready = false;
+    c->sys_n = n;
+    c->have_system = c->axis_valid[0] && c->axis_valid[1];
+    return KTG_OK;
+}
+
+}  // namespace ktg
 
 extern "C" {
 

@@ -391,6 +391,20 @@ struct ktg_batch {
     int num_large = 0;           // systems in the large class (first in d_order)
     unsigned *queue2 = nullptr;  // the large class's work queue
     int64_t order_split_rows = -1;  // split the uploaded order was built for
+    int num_queued = 0;             // systems the cluster launches take (in d_order)
+    // whole-GPU path: pairs of consecutive systems of equal size >=
+    // offload_rows (the x and y systems of one netlist) are solved one pair
+    // after another by an internal context (aggregation-preconditioned mixed
+    // solve, or the FP64 solve), before the cluster launches take the rest
+    int64_t offload_rows = 0;
+    int offload_precond = 2, offload_coarse = 0;
+    int64_t order_offload_rows = -1;
+    std::vector<int32_t> off_first;  // first system of each offloaded pair
+    ktg_ctx *octx = nullptr;
+    int64_t octx_launches = 0;
+    ktg_mixed_info *d_minfo = nullptr;
+    ktg_solve_info *d_sinfo = nullptr;
+    unsigned long long *d_stamp = nullptr;
     // graph cache
     cudaGraphExec_t graph = nullptr;
     double g_tol = -1, g_inner = -1;
@@ -470,6 +484,34 @@ __global__ void k_batch_f32(const double *a, float *b, int64_t n) {
         b[i] = static_cast<float>(a[i]);
 }
 
+__global__ void k_stamp(unsigned long long *t) { *t = ktg::global_timer_ns(); }
+
+// Results of an offloaded pair (systems sx, sy) from its solve's info: the
+// mixed solve's inner iterations, rounds and final true residuals (the FP64
+// pass's when it ran), or the FP64 solve's iterations and residuals; status
+// the solve's error, else 0 when the residual meets tol and 1 when not.
+__global__ void k_offload_results(const ktg_mixed_info *mi, const ktg_solve_info *si, int mixed,
+                                  double tol, int32_t sx, int32_t sy,
+                                  const unsigned long long *t0, ktg_batch_result *res) {
+    const int64_t lat = static_cast<int64_t>(ktg::global_timer_ns() - *t0);
+    for (int a = 0; a < 2; ++a) {
+        ktg_batch_result r;
+        if (mixed) {
+            r.iters = a ? mi->inner_y : mi->inner_x;
+            r.outer = a ? mi->outer_y : mi->outer_x;
+            r.resid = a ? mi->resid_y : mi->resid_x;
+            r.status = mi->status != 0 ? mi->status : (r.resid <= tol ? 0 : 1);
+        } else {
+            r.iters = a ? si->iters_y : si->iters_x;
+            r.outer = 0;
+            r.resid = a ? si->resid_y : si->resid_x;
+            r.status = si->status != 0 ? si->status : (r.resid <= tol ? 0 : 1);
+        }
+        r.latency_ns = lat;
+        res[a ? sy : sx] = r;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -500,9 +542,11 @@ void ktg_batch_destroy(ktg_batch *b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     void *ptrs[] = {b->d_sys, b->d_order, b->rp, b->col, b->val, b->val32, b->diag, b->rhs,
                     b->x, b->x0, b->r, b->z, b->p, b->ap, b->d32, b->ri32, b->z32, b->p32,
-                    b->ap32, b->queue, b->queue2, b->results};
+                    b->ap32, b->queue, b->queue2, b->results, b->d_minfo, b->d_sinfo,
+                    b->d_stamp};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (b->octx) ktg_destroy(b->octx);
     if (b->own_stream) cudaStreamDestroy(b->own_stream);
     delete b;
 }
@@ -625,6 +669,38 @@ int ktg_batch_set_split(ktg_batch *b, int64_t rows, int cluster, int threads, in
     return KTG_OK;
 }
 
+int ktg_batch_set_offload(ktg_batch *b, int64_t rows, int precond, int coarse) {
+    if (!b) return KTG_ERR_ARG;
+    if (rows < 0) return berr(b, KTG_ERR_ARG, "negative offload rows");
+    if (precond < 0 || precond > 2) return berr(b, KTG_ERR_ARG, "precond must be 0, 1 or 2");
+    if (coarse < 0 || coarse > 2) return berr(b, KTG_ERR_ARG, "coarse must be 0, 1 or 2");
+    if (precond == 1) return berr(b, KTG_ERR_ARG, "the learned inverse needs a prepared network");
+    b->offload_rows = rows;
+    b->offload_precond = precond;
+    b->offload_coarse = coarse;
+    return KTG_OK;
+}
+
+int ktg_batch_get_offload(const ktg_batch *b, int64_t *rows, int *pairs) {
+    if (!b) return KTG_ERR_ARG;
+    if (rows) *rows = b->offload_rows;
+    if (pairs) {
+        int k = 0;
+        const int32_t ns = static_cast<int32_t>(b->sys.size());
+        if (b->offload_rows > 0)
+            for (int32_t i = 0; i + 1 < ns;) {
+                if (b->sys[i].n >= b->offload_rows && b->sys[i + 1].n == b->sys[i].n) {
+                    ++k;
+                    i += 2;
+                } else {
+                    ++i;
+                }
+            }
+        *pairs = k;
+    }
+    return KTG_OK;
+}
+
 int ktg_batch_get_split(const ktg_batch *b, int64_t *rows, int *cluster, int *threads,
                         int *clusters, int *num_large) {
     if (!b) return KTG_ERR_ARG;
@@ -704,7 +780,7 @@ static int enqueue_class(ktg_batch *b, int first, int count, unsigned *queue, in
 // the other and the fork is joined back into `st` at the end.
 static int batch_enqueue(ktg_batch *b, double tol, int64_t max_iter, int mixed, double inner_tol,
                          cudaStream_t st) {
-    const int ns = static_cast<int>(b->sys.size());
+    const int ns = b->num_queued;
     const int nl = b->num_large;
     int res_small = 0;
     int rc = resident_clusters(b, b->cluster, b->threads, &res_small);
@@ -758,6 +834,55 @@ static int batch_enqueue(ktg_batch *b, double tol, int64_t max_iter, int mixed, 
     return rc;
 }
 
+// The offloaded pairs, one after another on the batch's stream, each through
+// the internal context: its x and y systems copied in (device to device),
+// then the whole-GPU solve on the batch's own solution slices, then the
+// pair's results.
+static int solve_offloaded(ktg_batch *b, double tol, int64_t max_iter, int precision,
+                           double inner_tol) {
+    int rc;
+    if (!b->octx) {
+        if ((rc = ktg_create(b->device, &b->octx))) return berr(b, rc, "internal context");
+        if (cudaMalloc(&b->d_minfo, sizeof(ktg_mixed_info)) != cudaSuccess ||
+            cudaMalloc(&b->d_sinfo, sizeof(ktg_solve_info)) != cudaSuccess ||
+            cudaMalloc(&b->d_stamp, sizeof(unsigned long long)) != cudaSuccess)
+            return berr(b, KTG_ERR_NOMEM, "offload buffers");
+    }
+    ktg_ctx *c = b->octx;
+    const int64_t launches0 = c->launches;
+    if ((rc = ktg_set_stream(c, b->stream)) || (rc = ktg_set_pointer_mode(c, KTG_PTR_DEVICE)) ||
+        (rc = ktg_set_option(c, "precond", b->offload_precond)) ||
+        (rc = ktg_set_option(c, "coarse", b->offload_coarse)))
+        return berr(b, rc, std::string("internal context: ") + c->err);
+    for (int32_t f : b->off_first) {
+        const ktg::SysDesc &X = b->sys[f], &Y = b->sys[f + 1];
+        k_stamp<<<1, 1, 0, b->stream>>>(b->d_stamp);
+        ++b->launches;
+        const int64_t mx = b->cost[f] - X.n, my = b->cost[f + 1] - Y.n;
+        // room for both axes at once (one growth at most)
+        if ((rc = ktg::reserve_system_arrays(c, X.n, std::max(mx, my))) ||
+            (rc = ktg::load_system_device(c, 0, X.n, mx, b->rp + X.row_base + f,
+                                          b->col + X.nnz_base, b->val + X.nnz_base,
+                                          b->diag + X.row_base, b->rhs + X.row_base)) ||
+            (rc = ktg::load_system_device(c, 1, Y.n, my, b->rp + Y.row_base + f + 1,
+                                          b->col + Y.nnz_base, b->val + Y.nnz_base,
+                                          b->diag + Y.row_base, b->rhs + Y.row_base)))
+            return berr(b, rc, std::string("offload load: ") + c->err);
+        if (!c->have_system) return berr(b, KTG_ERR_STATE, "offload load: pair not complete");
+        double *x = b->x + X.row_base, *y = b->x + Y.row_base;
+        rc = precision == 1 ? ktg_solve_mixed(c, x, y, tol, inner_tol, max_iter, 50, b->d_minfo,
+                                              nullptr, nullptr, 0)
+                            : ktg_solve(c, x, y, tol, max_iter, b->d_sinfo, nullptr, nullptr, 0);
+        if (rc) return berr(b, rc, std::string("offload solve: ") + c->err);
+        k_offload_results<<<1, 1, 0, b->stream>>>(b->d_minfo, b->d_sinfo, precision, tol, f,
+                                                        f + 1, b->d_stamp, b->results);
+        ++b->launches;
+        KTG_BCUDA(b, cudaGetLastError());
+    }
+    b->launches += c->launches - launches0;
+    return KTG_OK;
+}
+
 int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, double inner_tol) {
     if (!b) return KTG_ERR_ARG;
     if (precision != 0 && precision != 1) return berr(b, KTG_ERR_ARG, "precision must be 0 or 1");
@@ -766,11 +891,28 @@ int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, d
     if (max_iter < 0) return berr(b, KTG_ERR_ARG, "negative max_iter");
     if (b->sys.empty()) return KTG_OK;
     if (cudaSetDevice(b->device) != cudaSuccess) return KTG_ERR_CUDA;
-    if (b->dirty || b->order_split_rows != b->split_rows) {
-        // Largest first within each class; the large class (rows >= split_rows)
-        // occupies the front of the order.
-        std::vector<int32_t> order(b->sys.size());
-        std::iota(order.begin(), order.end(), 0);
+    if (b->dirty || b->order_split_rows != b->split_rows ||
+        b->order_offload_rows != b->offload_rows) {
+        // Offloaded pairs first leave the queues; then largest first within
+        // each class, the large class (rows >= split_rows) at the front.
+        const int32_t ns = static_cast<int32_t>(b->sys.size());
+        std::vector<char> off(ns, 0);
+        b->off_first.clear();
+        if (b->offload_rows > 0) {
+            for (int32_t k = 0; k + 1 < ns;) {
+                if (b->sys[k].n >= b->offload_rows && b->sys[k + 1].n == b->sys[k].n) {
+                    b->off_first.push_back(k);
+                    off[k] = off[k + 1] = 1;
+                    k += 2;
+                } else {
+                    ++k;
+                }
+            }
+        }
+        std::vector<int32_t> order;
+        for (int32_t k = 0; k < ns; ++k)
+            if (!off[k]) order.push_back(k);
+        b->num_queued = static_cast<int>(order.size());
         auto large = [&](int32_t p) { return b->split_rows > 0 && b->sys[p].n >= b->split_rows; };
         std::stable_sort(order.begin(), order.end(), [&](int32_t p, int32_t q) {
             if (large(p) != large(q)) return large(p);
@@ -779,16 +921,23 @@ int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, d
         b->num_large = static_cast<int>(std::count_if(order.begin(), order.end(), large));
         KTG_BCUDA(b, cudaMemcpyAsync(b->d_sys, b->sys.data(), sizeof(ktg::SysDesc) * b->sys.size(),
                                      cudaMemcpyHostToDevice, b->stream));
-        KTG_BCUDA(b, cudaMemcpyAsync(b->d_order, order.data(), sizeof(int32_t) * order.size(),
-                                     cudaMemcpyHostToDevice, b->stream));
+        if (!order.empty())
+            KTG_BCUDA(b, cudaMemcpyAsync(b->d_order, order.data(), sizeof(int32_t) * order.size(),
+                                         cudaMemcpyHostToDevice, b->stream));
         KTG_BCUDA(b, cudaStreamSynchronize(b->stream));
         b->dirty = false;
         b->order_split_rows = b->split_rows;
+        b->order_offload_rows = b->offload_rows;
         if (b->graph) {
             cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
         }
     }
+    if (!b->off_first.empty()) {
+        int rc = solve_offloaded(b, tol, max_iter, precision, inner_tol);
+        if (rc) return rc;
+    }
+    if (b->num_queued == 0) return KTG_OK;
     const bool same = b->graph && b->g_tol == tol && b->g_max_iter == max_iter &&
                       b->g_mixed == precision && b->g_inner == inner_tol &&
                       b->g_cluster == b->cluster && b->g_threads == b->threads &&
@@ -981,6 +1130,63 @@ int ktg_batch_autotune_split(ktg_batch *b, double tol, int precision, double inn
     cudaEventDestroy(e1);
     if (rc) return rc;
     if ((rc = ktg_batch_set_split(b, br, bc, bt, bn))) return rc;
+    if ((rc = ktg_batch_reset_x(b))) return rc;
+    if (base_ms) *base_ms = none;
+    if (best_ms) *best_ms = best;
+    return KTG_OK;
+}
+
+int ktg_batch_autotune_offload(ktg_batch *b, double tol, int precision, double inner_tol,
+                               int64_t max_iter, float *base_ms, float *best_ms) {
+    if (!b || max_iter <= 0) return KTG_ERR_ARG;
+    if (b->sys.empty()) return berr(b, KTG_ERR_STATE, "empty batch");
+    std::vector<int64_t> sizes;
+    for (const ktg::SysDesc &d : b->sys) sizes.push_back(d.n);
+    std::sort(sizes.begin(), sizes.end(), std::greater<int64_t>());
+    std::vector<int64_t> cuts;  // the 2, 4, ... 64 largest systems (pairs of them)
+    for (size_t k : {2, 4, 8, 16, 24, 32, 48, 64}) {
+        if (k > sizes.size()) break;
+        const int64_t t = sizes[k - 1];
+        if (t > 0 && (cuts.empty() || cuts.back() != t)) cuts.push_back(t);
+    }
+    cudaEvent_t e0, e1;
+    KTG_BCUDA(b, cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return berr(b, KTG_ERR_CUDA, "event creation failed");
+    }
+    const int64_t split0 = b->split_rows;
+    int rc = ktg_batch_set_split(b, 0, 0, 0, 0);
+    const int pre = b->offload_precond, co = b->offload_coarse;
+    if (!rc) rc = ktg_batch_set_offload(b, 0, pre, co);
+    float none = 1e30f, ms = 0.0f;
+    for (int rep = 0; rep < 2 && !rc; ++rep) {
+        rc = time_solve(b, tol, max_iter, precision, inner_tol, e0, e1, &ms);
+        none = std::min(none, ms);
+    }
+    float best = none;
+    int64_t br = 0;
+    for (int64_t cut : cuts) {
+        if (rc) break;
+        if ((rc = ktg_batch_set_offload(b, cut, pre, co))) break;
+        int pairs = 0;
+        ktg_batch_get_offload(b, nullptr, &pairs);
+        if (pairs == 0) continue;
+        float t = 1e30f;
+        for (int rep = 0; rep < 2 && !rc; ++rep) {
+            rc = time_solve(b, tol, max_iter, precision, inner_tol, e0, e1, &ms);
+            t = std::min(t, ms);
+        }
+        if (!rc && t < best) {
+            best = t;
+            br = cut;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if ((rc = ktg_batch_set_offload(b, br, pre, co))) return rc;
+    b->split_rows = split0;
     if ((rc = ktg_batch_reset_x(b))) return rc;
     if (base_ms) *base_ms = none;
     if (best_ms) *best_ms = best;

@@ -186,6 +186,12 @@ int launch_solve_mixed(ktg_ctx *ctx, double *x, double *y, double tol, double in
                        double *hist_x, double *hist_y, int64_t hist_cap);
 
 int build_star(ktg_ctx *ctx, int64_t *size_out, int (*reserve)(ktg_ctx *, int64_t, int64_t));
+// Capacity for systems of `rows` rows and `nnz` entries per axis (growing
+// keeps the installed systems).
+int reserve_system_arrays(ktg_ctx *ctx, int64_t rows, int64_t nnz);
+int load_system_device(ktg_ctx *ctx, int axis, int64_t n, int64_t m, const int32_t *rp,
+                       const int32_t *col, const double *val, const double *diag,
+                       const double *rhs);
 
 // Aggregation preconditioner (ktg_agg.cu): build for the current systems,
 // per-solve set-up (block row ranges, permuted positions) and write-back.

@@ -470,6 +470,26 @@ class Batch:
                                                       ctypes.byref(base), ctypes.byref(best)))
         return self.split(), float(base.value), float(best.value)
 
+    def set_offload(self, rows: int, precond: int = 2, coarse: int = 0):
+        """Pairs of consecutive equal-size systems of >= rows rows are solved
+        on the whole GPU before the cluster launches (rows 0: off)."""
+        self._check(self.lib.ktg_batch_set_offload(self.h, rows, precond, coarse))
+
+    def offload(self) -> dict:
+        r, k = ctypes.c_int64(), ctypes.c_int()
+        self._check(self.lib.ktg_batch_get_offload(self.h, ctypes.byref(r), ctypes.byref(k)))
+        return dict(rows=int(r.value), pairs=int(k.value))
+
+    def autotune_offload(self, tol: float, precision: int = 1, inner_tol: float = 1e-3,
+                         max_iter: int = 100000):
+        """Picks the whole-GPU threshold by timing full solves; returns
+        (offload dict, ms without, kept ms)."""
+        base, best = ctypes.c_float(), ctypes.c_float()
+        self._check(self.lib.ktg_batch_autotune_offload(self.h, tol, precision, inner_tol,
+                                                        max_iter, ctypes.byref(base),
+                                                        ctypes.byref(best)))
+        return self.offload(), float(base.value), float(best.value)
+
     def reset_x(self):
         self._check(self.lib.ktg_batch_reset_x(self.h))
 

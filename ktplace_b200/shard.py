@@ -119,8 +119,8 @@ def gather_to_root(plan: ShardPlan, rank: int, out, group=None):
 class BatchShardSolver:
     """The GPU solver of one rank's share of a batch of netlists: each owned
     netlist's x and y B2B systems are built on this rank's GPU and loaded into
-    one persistent-cluster Batch, which is autotuned once (shape, then size
-    split) and solved by graph replay. `make_unit(u)` returns
+    one Batch, which is autotuned once (cluster shape, then the pairs sent
+    to the whole GPU, then the size split) and solved by graph replay. `make_unit(u)` returns
     (netlist, x, y, anchor_x, anchor_y, alpha) for netlist u; a unit's host
     result is its x solution followed by its y solution.
     """
@@ -139,6 +139,7 @@ class BatchShardSolver:
         self.rows = []
         self.shape = None
         self.split = None
+        self.offload = None
 
     def load(self, units) -> None:
         """Builds and loads the systems of `units` (once)."""
@@ -160,6 +161,9 @@ class BatchShardSolver:
             c, t, _ = self.batch.autotune(self.tol, precision=self.precision,
                                           inner_tol=self.inner_tol, probe_iter=40)
             self.shape = (c, t)
+            self.offload, _, _ = self.batch.autotune_offload(
+                self.tol, precision=self.precision, inner_tol=self.inner_tol,
+                max_iter=self.max_iter)
             self.split, _, _ = self.batch.autotune_split(self.tol, precision=self.precision,
                                                          inner_tol=self.inner_tol,
                                                          max_iter=self.max_iter)

@@ -177,3 +177,67 @@ def test_sharded_batch_product_path(port_built):
             ref = oracle.port_pcg_axis(s, pos, TOL, MAX_ITER)["x"]
             mine = got[axis * n:(axis + 1) * n]
             assert np.linalg.norm(mine - ref) <= 1e-9 * np.linalg.norm(ref), (names[u], axis)
+
+
+@pytest.mark.parametrize("rows", [1, "big"])
+def test_batch_offload_matches_oracle(systems, rows):
+    """Pairs of consecutive equal-size systems at or above the threshold go to
+    the whole-GPU path (an internal context), the rest to the cluster
+    launches; FP64: every system matches the oracle's PCG (iterations and
+    solution), mixed (aggregation, coarse vector): every system meets the
+    tolerance on its true residual."""
+    b, ids = make_batch(systems)
+    sizes = [s["diag"].shape[0] for s, _ in systems]
+    thr = 1 if rows == 1 else max(sizes)
+    b.set_offload(thr, precond=2, coarse=2)
+    off = b.offload()
+    want_pairs = sum(1 for k in range(0, len(sizes) - 1, 2)
+                     if sizes[k] >= thr and sizes[k + 1] == sizes[k])
+    assert off["pairs"] == want_pairs >= 1
+    b.solve(TOL, MAX_ITER, precision=0)
+    res = b.results()
+    for (s, x0), sid in zip(systems, ids):
+        ref = oracle.port_pcg_axis(s, x0, TOL, MAX_ITER)
+        got = b.get_x(sid, s["diag"].shape[0])
+        assert res[sid]["status"] == 0, (sid, res[sid])
+        assert res[sid]["iters"] == ref["iters"], (sid, res[sid], ref["iters"])
+        assert np.linalg.norm(got - ref["x"]) <= 1e-9 * np.linalg.norm(ref["x"])
+    for rep in range(2):  # the second solve reloads the pairs' systems afresh
+        b.reset_x()
+        b.solve(TOL, MAX_ITER, precision=1, inner_tol=1e-3)
+        res = b.results()
+        for (s, _), sid in zip(systems, ids):
+            got = b.get_x(sid, s["diag"].shape[0])
+            assert res[sid]["status"] == 0, (sid, res[sid])
+            assert true_resid(s, got) <= TOL * 1.0001
+            assert res[sid]["latency_ns"] > 0
+    b.close()
+
+
+def test_batch_autotune_offload(systems):
+    b, ids = make_batch(systems)
+    off, base, best = b.autotune_offload(TOL, precision=1, inner_tol=1e-3, max_iter=MAX_ITER)
+    assert base > 0 and 0 < best <= base
+    assert off["rows"] == 0 or off["pairs"] >= 1
+    b.solve(TOL, MAX_ITER, precision=1, inner_tol=1e-3)
+    for (s, _), r, sid in zip(systems, b.results(), ids):
+        assert r["status"] == 0 and true_resid(s, b.get_x(sid, s["diag"].shape[0])) <= TOL * 1.0001
+    b.close()
+
+
+def test_upload_second_axis_larger_keeps_first(systems):
+    """Installing the y system when it needs more entries than the context
+    holds keeps the x system installed just before (the arrays grow with
+    their contents), so the solve matches the oracle on both axes."""
+    from ktplace_b200.gpu import Context
+    (sx, x0), (sy, y0) = systems[0], systems[1]
+    small, large = (sx, sy) if len(sx["val"]) <= len(sy["val"]) else (sy, sx)
+    s0, s1 = (small, large)
+    v0, v1 = (x0, y0) if s0 is sx else (y0, x0)
+    with Context(0) as c:
+        c.upload_system(0, s0)
+        c.upload_system(1, s1)
+        r = c.solve(v0, v1, TOL, MAX_ITER)
+    for s, v, got in ((s0, v0, r["x"]), (s1, v1, r["y"])):
+        ref = oracle.port_pcg_axis(s, v, TOL, MAX_ITER)
+        assert np.linalg.norm(got - ref["x"]) <= 1e-9 * np.linalg.norm(ref["x"])
