@@ -786,31 +786,39 @@ __global__ void __launch_bounds__(32 * kPfWarps)
 }
 
 // Eight lanes per aggregate (lane m holds row m of its block), four
-// aggregates per warp, everything in registers. Each lane forms its row of
-// the block of A (the diagonal, then the row's entries inside the aggregate
-// in storage order, duplicates summed), the group factors B = L L^T in FP64
-// row by row (the pivot lane takes sqrt and one reciprocal, its row reaches
-// the others by shuffles), and lane m then solves L L^T x = e_m by forward
-// and back substitution, fetching the rows of L it needs by shuffles: x is
-// column m of B^-1, that is row m, written as 8 FP32 (zero past the
-// aggregate's size; two 16-byte stores, consecutive lanes on consecutive
-// rows). A non-positive pivot gives the aggregate the inverse of its
-// diagonal instead. Every loop runs over the full eight rows with the
-// aggregate's size as a predicate, so the shuffles see all lanes.
+// aggregates per warp, the rows in shared memory (a padded row per lane):
+// each lane forms its row of the block of A (the diagonal, then the row's
+// entries inside the aggregate in storage order, duplicates summed), the
+// group factors B = L L^T in FP64 row by row (the pivot lane takes sqrt and
+// one reciprocal; the other lanes read the pivot row from shared memory),
+// and lane m then solves L L^T x = e_m by forward and back substitution,
+// reading the rows of L it needs: x is column m of B^-1, that is row m,
+// written as 8 FP32 (zero past the aggregate's size; two 16-byte stores,
+// consecutive lanes on consecutive rows). A non-positive pivot gives the
+// aggregate the inverse of its diagonal instead. Rows indexed in shared
+// memory rather than as register arrays keep the assembly free of
+// compare-and-select chains and the registers low enough for more warps.
 constexpr int kInvWarps = 8;
 constexpr int kInvPerBlock = kInvWarps * 4;  // aggregates per block
+constexpr int kInvStride = kAggMax + 1;      // doubles per row slot (bank spread)
 __global__ void __launch_bounds__(32 * kInvWarps)
     k_blockinv_lanes(const int32_t *count, const int32_t *__restrict__ agg_start,
                      const int32_t *__restrict__ size, int32_t n, const int32_t *__restrict__ prp,
                      const int32_t *__restrict__ pcol, const double *__restrict__ pval,
                      const double *__restrict__ pdiag, float *__restrict__ minv,
                      int32_t *__restrict__ meta) {
-    const int lane = threadIdx.x & 31;
+    __shared__ double rows_s[kInvWarps][32][kInvStride];
+    __shared__ double rinv_s[kInvWarps][32];
+    __shared__ int ok_s[kInvWarps][4];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g0 = lane & ~7;  // first lane of this aggregate's group
     const int m = lane & 7;
-    const int32_t J = (static_cast<int32_t>(blockIdx.x) * kInvWarps + (threadIdx.x >> 5)) * 4 + (lane >> 3);
+    const int32_t J = (static_cast<int32_t>(blockIdx.x) * kInvWarps + w) * 4 + (lane >> 3);
     const int32_t cnt = *count;
-    if ((static_cast<int32_t>(blockIdx.x) * kInvWarps + (threadIdx.x >> 5)) * 4 >= cnt) return;  // whole warp
+    if ((static_cast<int32_t>(blockIdx.x) * kInvWarps + w) * 4 >= cnt) return;  // whole warp
+    double (*R)[kInvStride] = rows_s[w] + g0;  // the group's rows
+    double *me = rows_s[w][lane];
+    double *rv = rinv_s[w] + g0;
     int k = 0;
     int32_t first = 0, first_l = 0;
     if (J < cnt) {
@@ -819,18 +827,16 @@ __global__ void __launch_bounds__(32 * kInvWarps)
         first_l = first >= n ? first - n : first;
     }
     const bool mine = m < k;
-    double b[kAggMax];
 #pragma unroll
-    for (int t = 0; t < kAggMax; ++t) b[t] = 0.0;
+    for (int t = 0; t < kAggMax; ++t) me[t] = 0.0;
+    rv[m] = 0.0;
+    if (m == 0) ok_s[w][lane >> 3] = 1;
     double d = 1.0;
     if (mine) {
         const int32_t row = first + m;
         d = __ldg(pdiag + row);
-#pragma unroll
-        for (int t = 0; t < kAggMax; ++t)
-            if (t == m) b[t] += d;
-        // four entries per round with independent loads (the value loads do
-        // not wait for the column test), added in storage order
+        me[m] += d;
+        // four entries per round with independent loads, added in storage order
         const int32_t e1 = __ldg(prp + row + 1);
         for (int32_t e = __ldg(prp + row); e < e1; e += 4) {
             int32_t cq[4];
@@ -841,66 +847,60 @@ __global__ void __launch_bounds__(32 * kInvWarps)
                 cv[u] = e + u < e1 ? __ldg(pval + e + u) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int32_t q = cq[u];
-#pragma unroll
-                for (int t = 0; t < kAggMax; ++t)
-                    if (t == q && q < k) b[t] += cv[u];
+            for (int u = 0; u < 4; ++u)
+                if (cq[u] >= 0 && cq[u] < k) me[cq[u]] += cv[u];
+        }
+    }
+    __syncwarp();
+    // Cholesky: row m becomes row m of L (entries past m unused)
+    for (int j = 0; j < kAggMax; ++j) {
+        if (mine && m == j) {
+            double sj = me[j];
+            for (int q = 0; q < j; ++q) sj -= me[q] * me[q];
+            if (sj > 0.0) {
+                me[j] = sqrt(sj);
+                rv[j] = 1.0 / me[j];
+            } else {
+                ok_s[w][lane >> 3] = 0;
             }
         }
-    }
-    // Cholesky: b becomes row m of L (entries past m unused)
-    bool ok = true;
-    double rinv = 0.0;  // 1 / L[m][m]
-#pragma unroll
-    for (int j = 0; j < kAggMax; ++j) {
-        double s = b[j];
-#pragma unroll
-        for (int q = 0; q < j; ++q) s -= b[q] * b[q];
-        const bool piv = m == j && mine;
-        const int good = (piv && !(s > 0.0)) ? 0 : 1;
-        const bool gok = __shfl_sync(0xffffffffu, good, g0 + j) != 0;  // the group's pivot
-        if (piv && s > 0.0) {
-            b[j] = sqrt(s);
-            rinv = 1.0 / b[j];
+        __syncwarp();
+        if (mine && m > j) {
+            const double *Lj = R[j];
+            double u = me[j];
+            for (int q = 0; q < j; ++q) u -= me[q] * Lj[q];
+            me[j] = u * rv[j];
         }
-        const double rj = __shfl_sync(0xffffffffu, rinv, g0 + j);
-        double u = b[j];
-#pragma unroll
-        for (int q = 0; q < j; ++q) u -= b[q] * __shfl_sync(0xffffffffu, b[q], g0 + j);
-        if (j < k) ok = ok && gok;
-        if (mine && m > j && j < k) b[j] = u * rj;
+        __syncwarp();
     }
-    // (the substitutions run on every lane, so the shuffles stay uniform;
-    // a failed group's result is discarded below)
+    const bool ok = ok_s[w][lane >> 3] != 0;
     float out[kAggMax];
-    {
+    if (ok && mine) {
         // forward: y = L^-1 e_m (y[i] = 0 for i < m)
         double y[kAggMax];
 #pragma unroll
         for (int i = 0; i < kAggMax; ++i) {
-            const double ri = __shfl_sync(0xffffffffu, rinv, g0 + i);
+            const double ri = i < k ? rv[i] : 0.0;
             double acc = 0.0;
 #pragma unroll
-            for (int q = 0; q < i; ++q) acc += __shfl_sync(0xffffffffu, b[q], g0 + i) * y[q];
+            for (int q = 0; q < i; ++q) acc += (i < k ? R[i][q] : 0.0) * y[q];
             y[i] = i < m ? 0.0 : (i == m ? ri : -acc * ri);
         }
         // back: x = L^-T y, in place (y[i] is read before x[i] replaces it)
 #pragma unroll
         for (int i = kAggMax - 1; i >= 0; --i) {
-            const double ri = __shfl_sync(0xffffffffu, rinv, g0 + i);
+            const double ri = i < k ? rv[i] : 0.0;
             double acc = y[i];
 #pragma unroll
-            for (int q = i + 1; q < kAggMax; ++q) {
-                const double lqi = __shfl_sync(0xffffffffu, b[i], g0 + q);  // L[q][i]
-                if (q < k) acc -= lqi * y[q];
-            }
+            for (int q = i + 1; q < kAggMax; ++q)
+                if (q < k) acc -= R[q][i] * y[q];  // L[q][i]
             y[i] = acc * ri;
         }
 #pragma unroll
-        for (int t = 0; t < kAggMax; ++t)
-            out[t] = ok ? (t < k ? static_cast<float>(y[t]) : 0.0f)
-                        : (t == m ? static_cast<float>(1.0 / d) : 0.0f);
+        for (int t = 0; t < kAggMax; ++t) out[t] = t < k ? static_cast<float>(y[t]) : 0.0f;
+    } else {
+#pragma unroll
+        for (int t = 0; t < kAggMax; ++t) out[t] = t == m ? static_cast<float>(1.0 / d) : 0.0f;
     }
     if (!mine) return;
     float4 *dst = reinterpret_cast<float4 *>(minv + static_cast<size_t>(first + m) * kAggMax);
