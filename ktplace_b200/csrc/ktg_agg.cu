@@ -28,6 +28,7 @@
 // of nnz(x) + nnz(y) entries, and the permuted system (row_ptr, col, FP64 and
 // FP32 values, diag, rhs, x) plus the block inverses (8 floats per row).
 #include "ktg_agg.h"
+#include "ktg_coarse_head.cuh"
 #include "ktg_common.cuh"
 #include "ktg_context.h"
 #include "ktg_spmv.cuh"
@@ -718,7 +719,8 @@ __global__ void __launch_bounds__(32 * kPfWarps)
                   const double *__restrict__ rhs0, const double *__restrict__ rhs1,
                   int32_t *__restrict__ pcol, double *__restrict__ pval,
                   float *__restrict__ pval32, double *__restrict__ pdiag,
-                  double *__restrict__ prhs, int coarse_mode, const float *__restrict__ zin,
+                  double *__restrict__ prhs, int coarse_mode, const float *__restrict__ hw,
+                  const float *__restrict__ emb, const double *__restrict__ logd,
                   double *__restrict__ zd) {
     const int lane = threadIdx.x & 31;
     const int32_t k0 = (static_cast<int32_t>(blockIdx.x) * kPfWarps + (threadIdx.x >> 5)) * 32;
@@ -773,13 +775,16 @@ __global__ void __launch_bounds__(32 * kPfWarps)
     prhs[k] = __ldg((y ? rhs1 : rhs0) + i);
     if (coarse_mode > 0) {  // the coarse vector, rounded to FP32 as the solve uses it
         double z = 1.0;
-        if (coarse_mode == 2) {
+        if (coarse_mode >= 2) {
             const double *val = y ? L.val1 : L.val0;
             double sabs = 0.0;
             for (int32_t e = e0; e < e0 + len; ++e) sabs += fabs(__ldg(val + e));
-            z = static_cast<double>(static_cast<float>(sabs / d));
-        } else if (coarse_mode == 3) {
-            z = static_cast<double>(__ldg(zin + c));
+            if (coarse_mode == 2)
+                z = static_cast<double>(static_cast<float>(sabs / d));
+            else  // the learned head on the cell's embedding
+                z = static_cast<double>(coarse_head_z(emb + static_cast<int64_t>(i) * kCoarseProj,
+                                                      sabs, d, __ldg(logd + (y ? 1 : 0)),
+                                                      [&](int t) { return __ldg(hw + t); }));
         }
         zd[k] = z;
     }
@@ -953,20 +958,26 @@ __global__ void k_perm_out(int32_t rows, int32_t n, const int32_t *order, const 
 //   mode 2  the share of the row's weight that couples to other movable
 //           cells, sum_j |a_ij| / a_ii (cells held only by fixed pins and
 //           anchors do not take part in the rigid motion);
-//   mode 3  a caller-provided vector in the combined natural order (the
-//           learned coarse vector).
-__global__ void k_coarse_z(int mode, int32_t rows, const int32_t *prp, const double *pval,
-                           const double *pdiag, const int32_t *order, const float *zin,
-                           double *zd) {
+//   mode 3  the learned head on the row's cell embedding, its coupling share
+//           and its log diagonal (ktg_coarse_head.cuh).
+__global__ void k_coarse_z(int mode, int32_t rows, int32_t n, const int32_t *prp,
+                           const double *pval, const double *pdiag, const int32_t *order,
+                           const float *hw, const float *emb, const double *logd, double *zd) {
     const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= rows) return;
     float z = 1.0f;
-    if (mode == 2) {
+    if (mode >= 2) {
         double sabs = 0.0;
         for (int32_t e = __ldg(prp + k); e < __ldg(prp + k + 1); ++e) sabs += fabs(__ldg(pval + e));
-        z = static_cast<float>(sabs / __ldg(pdiag + k));
-    } else if (mode == 3) {
-        z = __ldg(zin + __ldg(order + k));
+        const double d = __ldg(pdiag + k);
+        if (mode == 2) {
+            z = static_cast<float>(sabs / d);
+        } else {
+            const int32_t c = __ldg(order + k);
+            const bool y = c >= n;
+            z = coarse_head_z(emb + static_cast<int64_t>(y ? c - n : c) * kCoarseProj, sabs, d,
+                              __ldg(logd + (y ? 1 : 0)), [&](int t) { return __ldg(hw + t); });
+        }
     }
     zd[k] = z;
 }
@@ -1254,7 +1265,8 @@ int build_agg_values(ktg_ctx *c) {
     const int zmode = (c->coarse == 3 && !c->coarse_z_ready) ? 0 : c->coarse;
     k_pfill_tiles<<<blocks_for(rows, 32 * kPfWarps), 32 * kPfWarps, 0, c->stream>>>(
         L0, R, s->order, s->newpos, s->prp, c->sys[0].rhs, c->sys[1].rhs, s->pcol, s->pval,
-        s->pval32, s->pdiag, s->prhs, zmode, c->coarse_z, s->zd);
+        s->pval32, s->pdiag, s->prhs, zmode, c->coarse_head_w, c->coarse_emb, c->coarse_logd,
+        s->zd);
     k_blockinv_lanes<<<blocks_for(rows, kInvPerBlock), 32 * kInvWarps, 0, c->stream>>>(
         nagg, s->agg_start, s->final_size, static_cast<int32_t>(n), s->prp, s->pcol, s->pval,
         s->pdiag, s->minv, s->meta);
@@ -1284,11 +1296,12 @@ int prepare_agg(ktg_ctx *c) {
 
 // The coarse vector of `mode` (1, 2, or 3 with zin) for the current
 // aggregates and its A z and 1 / (z^T A z); kept until the next build.
-int agg_coarse_setup(ktg_ctx *c, int mode, const float *zin) {
+int agg_coarse_setup(ktg_ctx *c, int mode) {
     AggState *s = c->agg;
     const int64_t rows = 2 * c->sys_n;
     if (!s || !c->agg_ready) return set_error(c, KTG_ERR_STATE, "no aggregates to correct");
-    if (mode == 3 && !zin) return set_error(c, KTG_ERR_STATE, "no learned coarse vector");
+    if (mode == 3 && (!c->coarse_z_ready || !c->coarse_head_w))
+        return set_error(c, KTG_ERR_STATE, "no learned coarse vector");
     if (s->coarse_mode == mode && (mode != 3 || s->z_gen == c->coarse_z_gen)) return KTG_OK;
     if (rows == 0) {
         KTG_CUDA(c, cudaMemsetAsync(s->coarse_einv, 0, 2 * sizeof(double), c->stream));
@@ -1297,8 +1310,9 @@ int agg_coarse_setup(ktg_ctx *c, int mode, const float *zin) {
     }
     const int32_t R = static_cast<int32_t>(rows), n = static_cast<int32_t>(c->sys_n);
     if (s->z_mode != mode || (mode == 3 && s->z_gen != c->coarse_z_gen)) {  // z is stale
-        k_coarse_z<<<blocks_for(rows, kT), kT, 0, c->stream>>>(mode, R, s->prp, s->pval, s->pdiag,
-                                                              s->order, zin, s->zd);
+        k_coarse_z<<<blocks_for(rows, kT), kT, 0, c->stream>>>(
+            mode, R, n, s->prp, s->pval, s->pdiag, s->order, c->coarse_head_w, c->coarse_emb,
+            c->coarse_logd, s->zd);
         ++c->launches;
         s->z_mode = mode;
         s->z_gen = c->coarse_z_gen;

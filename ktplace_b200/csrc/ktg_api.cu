@@ -321,7 +321,8 @@ void ktg_destroy(ktg_ctx *c) {
     free_systems(c);
     ktg::free_agg(c);
     ktg::free_lal(c);
-    dev_free(c->coarse_z_buf);
+    dev_free(c->coarse_head_w);
+    dev_free(c->coarse_logd);
     dev_free(c->coarse_emb);
     dev_free(c->mixed_trace);
     dev_free(c->hpwl_terms);
@@ -971,7 +972,7 @@ int ktg_download_coarse(ktg_ctx *c, float *z, float *az, double *einv) {
     int rc = set_device(c);
     if (rc) return rc;
     if (!c->agg_ready && (rc = ktg::build_agg(c))) return rc;
-    if ((rc = ktg::agg_coarse_setup(c, c->coarse, c->coarse_z))) return rc;
+    if ((rc = ktg::agg_coarse_setup(c, c->coarse))) return rc;
     const int64_t rows = 2 * c->sys_n;
     const ktg::AggState *g = c->agg;
     if (rows > 0 && (z || az)) {

@@ -102,11 +102,13 @@ struct ktg_ctx {
     int agg_reuse = 0;             // aggregation: builds that may reuse the last structure
     int coarse = 0;                // coarse vector of the aggregation solve: 0 none,
                                    // 1 constant, 2 coupling share, 3 learned
-    const float *coarse_z = nullptr;  // learned coarse vector [2n] (combined natural order)
-    bool coarse_z_ready = false;      // coarse_z belongs to the current systems
-    int64_t coarse_z_gen = 0;         // bumped whenever coarse_z is rewritten
-    float *coarse_z_buf = nullptr;    // storage of the learned coarse vector
-    int64_t coarse_z_cap = 0;
+    // inputs of the learned coarse vector (coarse 3), evaluated per row by the
+    // aggregation build: the head's parameters (a copy, ktg_coarse_head.cuh),
+    // the trunk embedding below and each axis's mean log diagonal
+    float *coarse_head_w = nullptr;   // [kCoarseHeadParams]
+    double *coarse_logd = nullptr;    // [2]
+    bool coarse_z_ready = false;      // those inputs belong to the current systems
+    int64_t coarse_z_gen = 0;         // bumped whenever they are rewritten
     // trunk embedding of this context's netlist under one learned parameter
     // set (computed once per netlist, reused by every build's head pass)
     float *coarse_emb = nullptr;      // [n x 16]
@@ -201,7 +203,7 @@ int prepare_agg(ktg_ctx *ctx);
 int agg_prepare_solve(ktg_ctx *ctx, int grid, const double *x, const double *y, int32_t *rows_cap);
 int agg_finish_solve(ktg_ctx *ctx, double *x, double *y);
 double *agg_global_slices(ktg_ctx *ctx, int64_t doubles);
-int agg_coarse_setup(ktg_ctx *ctx, int mode, const float *zin);
+int agg_coarse_setup(ktg_ctx *ctx, int mode);
 void free_agg(ktg_ctx *ctx);
 
 // Look-ahead legalization (ktg_lal.cu): free space (host arrays) and the

@@ -31,6 +31,7 @@
 #include <string>
 #include <vector>
 
+#include "ktg_coarse_head.cuh"
 #include "ktg_common.cuh"
 #include "ktg_context.h"
 #include "ktplace_b200.h"
@@ -45,6 +46,8 @@ constexpr int LAYERS = 3;
 // coarse-vector head: input = p (PROJ), coupling share, log diag
 constexpr int HEAD_IN = PROJ + 2;
 constexpr int HEAD_H = 16;
+static_assert(PROJ == ktg::kCoarseProj && HEAD_IN == ktg::kCoarseIn && HEAD_H == ktg::kCoarseHid,
+              "the coarse head's shape is shared with the aggregation build");
 constexpr int kMaxVec = 4;  // test vectors per coarse loss
 // softplus^-1(1): the head's output bias at initialisation, so that the
 // untrained head gives the constant coarse vector
@@ -1397,11 +1400,9 @@ int ktg_learned_prepare_coarse(ktg_learned *h, ktg_ctx *c) {
         return lerr(h, KTG_ERR_STATE, "context needs the B2B systems of its netlist");
     KTG_LCUDA(h, cudaSetDevice(h->device));
     const int64_t n = c->n;
-    if (c->coarse_z_cap < 2 * n) {  // grows once per netlist size (synchronising)
-        if (c->coarse_z_buf) cudaFree(c->coarse_z_buf);
-        c->coarse_z_buf = nullptr;
-        KTG_LCUDA(h, cudaMalloc(&c->coarse_z_buf, sizeof(float) * std::max<int64_t>(2 * n, 1)));
-        c->coarse_z_cap = 2 * n;
+    if (!c->coarse_head_w) {  // once per context
+        KTG_LCUDA(h, cudaMalloc(&c->coarse_head_w, sizeof(float) * ktg::kCoarseHeadParams));
+        KTG_LCUDA(h, cudaMalloc(&c->coarse_logd, 2 * sizeof(double)));
     }
     if (c->coarse_emb_cap < n) {  // the context keeps its netlist's embedding
         if (c->coarse_emb) cudaFree(c->coarse_emb);
@@ -1427,21 +1428,22 @@ int ktg_learned_prepare_coarse(ktg_learned *h, ktg_ctx *c) {
             c->coarse_emb_version = h->version;
         }
     }
+    // the per-axis mean log diagonal and a copy of the head's parameters; the
+    // head itself is evaluated per row by the aggregation build
     for (int axis = 0; axis < 2 && !rc; ++axis) {
-        SysView S{c->sys[axis].row_ptr, c->sys[axis].col, c->sys[axis].val, c->sys[axis].diag,
-                  static_cast<int32_t>(n), 0};
-        if ((rc = logd_mean(h, S))) break;
-        HeadArgs A = head_args(h, S, c->coarse_emb);
-        A.zf = c->coarse_z_buf + axis * n;
-        if (n > 0) {
-            ktg::learned::k_coarse_head<<<static_cast<int>((n + 255) / 256), 256, 0, h->stream>>>(A);
-            ++h->launches;
-        }
+        const int tb = 256;
+        ktg::learned::k_logd_sum<<<std::min<int>(1024, (static_cast<int>(n) + tb - 1) / tb + 1), tb,
+                                   0, h->stream>>>(c->sys[axis].diag, static_cast<int32_t>(n),
+                                                   h->dpart, h->ticket, c->coarse_logd + axis);
+        ++h->launches;
     }
+    if (!rc && cudaMemcpyAsync(c->coarse_head_w, h->w + h->L.Wh,
+                               sizeof(float) * ktg::kCoarseHeadParams, cudaMemcpyDeviceToDevice,
+                               h->stream) != cudaSuccess)
+        rc = lerr(h, KTG_ERR_CUDA, "head parameter copy failed");
     h->stream = own;
     if (rc) return rc;
     KTG_LCUDA(h, cudaGetLastError());
-    c->coarse_z = c->coarse_z_buf;
     c->coarse_z_ready = true;
     ++c->coarse_z_gen;
     return KTG_OK;

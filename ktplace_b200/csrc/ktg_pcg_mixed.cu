@@ -870,7 +870,7 @@ int launch_solve_mixed(ktg_ctx *c, double *x, double *y, double tol, double inne
         if (c->coarse > 0) {
             if (c->coarse == 3 && !c->coarse_z_ready)
                 return set_error(c, KTG_ERR_STATE, "learned coarse vector not prepared");
-            if ((rc = agg_coarse_setup(c, c->coarse, c->coarse_z))) return rc;
+            if ((rc = agg_coarse_setup(c, c->coarse))) return rc;
             A.zaz = g->zaz;
             A.coarse_einv = g->coarse_einv;
         }
