@@ -68,6 +68,10 @@ def parse():
                     help="skip the batched-solve leg (64 netlists, 128 systems)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="run the batched-solve workload once for an ncu capture")
+    ap.add_argument("--profile-batch-full", action="store_true",
+                    help="the 64-netlist batched solve once, with the whole-GPU threshold and "
+                         "shape the autotuners pick on B200 (44,725 rows; 4 x 1024 clusters), "
+                         "for an ncu launch list")
     ap.add_argument("--profile-pcg", type=int, default=0, metavar="CELLS",
                     help="only one B2B build and FP64 solve of a synthetic design with CELLS "
                          "movable cells (scaled from the 211k design), timed, with its "
@@ -1255,6 +1259,16 @@ def main():
         return profile_lal()
     if args.profile_agg:
         return profile_agg()
+    if args.profile_batch_full:
+        batch, rows = batch_workload(64)
+        batch.set_shape(4, 1024)
+        batch.set_offload(44725, precond=2, coarse=0)
+        batch.solve(TOL, MAX_ITER, precision=1, inner_tol=MIXED_INNER_TOL)
+        res = batch.results()
+        bad = [r for r in res if r["status"] != 0 or r["resid"] > TOL]
+        print(f"profile-batch-full: {len(rows)} systems, {batch.offload()['pairs']} pairs on the "
+              f"whole GPU, {len(bad)} unconverged")
+        return 1 if bad else 0
     if args.profile_batch:
         batch, rows = batch_workload(16)
         batch.solve(TOL, MAX_ITER, precision=1, inner_tol=MIXED_INNER_TOL)
