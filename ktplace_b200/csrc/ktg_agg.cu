@@ -12,21 +12,30 @@
 // The x and y systems are handled as one block-diagonal system of 2n rows
 // (row c < n is x row c, c >= n is y row c - n). Everything is
 // deterministic: matching by handshake on strengths with index tie-breaks,
-// Galerkin sums in raw storage order, numbering by prefix sums.
+// sums in fixed orders, numbering by prefix sums.
 //
-// Level rules (one level = matching + coarsening):
-//   strength of a stored entry (I, J, v): s = -v / sqrt(d_I d_J)
-//   kRounds handshake rounds: each unmatched I picks the unmatched J != I of
-//     largest s > 0 (ties: smaller J); mutual picks are matched;
-//   leaders (unmatched, or the smaller of a pair) are numbered in order;
-//   coarse row of J = (a, b): entries of row a then row b mapped to coarse
-//     ids, those landing on J summed into the coarse diagonal, the others
-//     summed per id in that raw order and stored with the ids ascending.
+// Level rules (one level = matching of the level's nodes; the nodes of level
+// 0 are the rows, a node of level l + 1 is a matched pair or a single node of
+// level l, so it holds at most 2^(l+1) rows):
+//   dc(N): the node's Galerkin diagonal, the sum over its member rows m in
+//     position order of t_m = d_m + (m's entries whose column lies in N, in
+//     storage order); dc = d at level 0;
+//   strength of a stored entry (i, j, v) between nodes A (of i) != B (of j):
+//     s = -v / sqrt(dc(A) dc(B));
+//   kRounds handshake rounds: each unmatched A picks the unmatched B of
+//     largest s > 0 over all its member rows' entries (ties: smaller B);
+//     mutual picks are matched;
+//   leaders (unmatched, or the smaller of a pair) are numbered in order; a
+//     row of the second node of a pair moves behind the first's rows.
+// The nodes' couplings are the strongest single entries between them, so no
+// coarse matrix is formed: a level reads the fine entries with the node of
+// each column.
 //
-// Device memory (per context, grown with the systems): level arrays over 2n
-// nodes (mate, pick, flags, ids, children, sizes), two compact coarse CSRs
-// of nnz(x) + nnz(y) entries, and the permuted system (row_ptr, col, FP64 and
-// FP32 values, diag, rhs, x) plus the block inverses (8 floats per row).
+// Device memory (per context, grown with the systems): per-node and per-row
+// level arrays over 2n, the strength and neighbour node of every fine entry,
+// and the permuted system (row_ptr, col, FP64 and FP32 values, diag, rhs, x)
+// plus the block inverses (8 floats per row).
+
 #include "ktg_agg.h"
 #include "ktg_coarse_head.cuh"
 #include "ktg_common.cuh"
@@ -45,21 +54,15 @@ constexpr int kAggMax = 8;
 constexpr int kT = 256;
 constexpr int kScanTile = 2048;  // 1024 threads x 2
 
-// Rows of one level: the two axis CSRs (level 0) or a compact coarse CSR.
-// Axis arrays are separate fields chosen with a conditional, so that no
-// thread copies the parameter block to local memory.
+// The two axis CSRs of the combined row space. Axis arrays are separate
+// fields chosen with a conditional, so that no thread copies the parameter
+// block to local memory.
 struct LevelView {
-    bool fine;
-    int32_t n;  // rows per axis (level 0)
+    int32_t n;  // rows per axis
     const int32_t *rp0, *rp1;
     const int32_t *col0, *col1;
     const double *val0, *val1;
     const double *diag0, *diag1;
-    const int32_t *start;
-    const int32_t *len;
-    const int32_t *ccol;
-    const double *cval;
-    const double *cdiag;
 };
 
 struct RowRef {
@@ -70,35 +73,25 @@ struct RowRef {
 
 __device__ __forceinline__ RowRef row_of(const LevelView &L, int32_t I) {
     RowRef r;
-    if (L.fine) {
-        const bool y = I >= L.n;
-        const int32_t i = y ? I - L.n : I;
-        const int32_t *rp = y ? L.rp1 : L.rp0;
-        r.e0 = __ldg(rp + i);
-        r.e1 = __ldg(rp + i + 1);
-        r.off = y ? L.n : 0;
-        r.col = y ? L.col1 : L.col0;
-        r.val = y ? L.val1 : L.val0;
-    } else {
-        r.e0 = __ldg(L.start + I);
-        r.e1 = r.e0 + __ldg(L.len + I);
-        r.off = 0;
-        r.col = L.ccol;
-        r.val = L.cval;
-    }
+    const bool y = I >= L.n;
+    const int32_t i = y ? I - L.n : I;
+    const int32_t *rp = y ? L.rp1 : L.rp0;
+    r.e0 = __ldg(rp + i);
+    r.e1 = __ldg(rp + i + 1);
+    r.off = y ? L.n : 0;
+    r.col = y ? L.col1 : L.col0;
+    r.val = y ? L.val1 : L.val0;
     return r;
 }
 
 __device__ __forceinline__ double diag_of(const LevelView &L, int32_t I) {
-    if (L.fine) {
-        const bool y = I >= L.n;
-        return __ldg((y ? L.diag1 : L.diag0) + (y ? I - L.n : I));
-    }
-    return __ldg(L.cdiag + I);
+    const bool y = I >= L.n;
+    return __ldg((y ? L.diag1 : L.diag0) + (y ? I - L.n : I));
 }
 
 __global__ void k_init(int32_t rows, int32_t *cur, int32_t *pos, int32_t *size, int32_t *mate,
                        int32_t *counts) {
+    pdl_enter();
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c == 0) {
         for (int k = 0; k < 8; ++k) counts[k] = 0;
@@ -127,13 +120,15 @@ __device__ __forceinline__ void pick_merge(double ob, int32_t oj, double &best, 
     }
 }
 
-// kFirst (first round of a level: nothing is matched yet): computes every
-// entry's strength and stores it in sbuf (y rows of level 0 at offset yoff);
-// later rounds read it back and gather only the neighbour's mate.
+// Level 0, where the nodes are the rows. kFirst (first round of a level:
+// nothing is matched yet): computes every entry's strength and stores it in
+// sbuf (y rows at offset yoff); later rounds read it back and gather only the
+// neighbour's mate.
 template <bool kFirst>
 __global__ void __launch_bounds__(32 * kPickWarps) k_pick(LevelView L, const int32_t *count,
                                                           const int32_t *mate, int32_t *pick,
                                                           double *sbuf, int64_t yoff) {
+    pdl_enter();
     __shared__ double best_s[kPickWarps][32];
     __shared__ int32_t best_j[kPickWarps][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -181,12 +176,12 @@ __global__ void __launch_bounds__(32 * kPickWarps) k_pick(LevelView L, const int
         int32_t sj = -1;
         if (t < T) {
             const int32_t e = re0 + (t - rex);
-            const int32_t *col = L.fine ? (ry ? L.col1 : L.col0) : L.ccol;
+            const int32_t *col = ry ? L.col1 : L.col0;
             const int32_t J = __ldg(col + e) + (ry ? L.n : 0);
             double *sp = sbuf + (ry ? yoff : 0) + e;
             double st;
             if (kFirst) {
-                const double *val = L.fine ? (ry ? L.val1 : L.val0) : L.cval;
+                const double *val = ry ? L.val1 : L.val0;
                 st = -__ldg(val + e) / sqrt(rd * diag_of(L, J));
                 *sp = st;
             } else {
@@ -219,7 +214,132 @@ __global__ void __launch_bounds__(32 * kPickWarps) k_pick(LevelView L, const int
     if (I < cnt) pick[I] = act ? best_j[w][lane] : -1;
 }
 
+// Levels 1 and up: the same walk over the fine rows whose node is
+// unmatched, each entry's column mapped to its node B (cur) and B's diagonal
+// (dcr, the diagonal of each row's node: two independent gathers); every
+// row's best entry to another unmatched node goes to (cand_s, cand_b), and
+// k_nodepick takes the best over a node's member rows. kFirst stores each
+// entry's strength and B (sbuf, bbuf) for the level's later rounds.
+template <bool kFirst>
+__global__ void __launch_bounds__(32 * kPickWarps) k_rowpick(LevelView L, int32_t rows,
+                                                             const int32_t *cur,
+                                                             const int32_t *mate, const double *dcr,
+                                                             double *sbuf, int32_t *bbuf,
+                                                             int64_t yoff, double *cand_s,
+                                                             int32_t *cand_b) {
+    pdl_enter();
+    __shared__ double best_s[kPickWarps][32];
+    __shared__ int32_t best_j[kPickWarps][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int32_t base = (blockIdx.x * kPickWarps + w) * 32;
+    if (base >= rows) return;  // whole warp
+    const int32_t I = base + lane;
+    bool act = false, yax = false;
+    int32_t e0 = 0, len = 0, A = -1;
+    double dA = 1.0;
+    if (I < rows) {
+        A = cur[I];
+        if (kFirst || mate[A] < 0) {
+            act = true;
+            const RowRef r = row_of(L, I);
+            e0 = r.e0;
+            len = r.e1 - r.e0;
+            yax = r.off != 0;
+            if (kFirst) dA = dcr[I];
+        }
+    }
+    int32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int32_t excl = incl - len;
+    const int32_t T = __shfl_sync(0xffffffffu, incl, 31);
+    best_s[w][lane] = 0.0;
+    best_j[w][lane] = -1;
+    __syncwarp();
+    for (int32_t t0 = 0; t0 < T; t0 += 32) {
+        const int32_t t = t0 + lane;
+        int row = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cand = row + step;
+            const int32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+            if (cand < 32 && ex <= t) row = cand;
+        }
+        const int32_t re0 = __shfl_sync(0xffffffffu, e0, row);
+        const int32_t rex = __shfl_sync(0xffffffffu, excl, row);
+        const bool ry = __shfl_sync(0xffffffffu, yax, row);
+        const double rd = __shfl_sync(0xffffffffu, dA, row);
+        const int32_t rA = __shfl_sync(0xffffffffu, A, row);
+        double sv = 0.0;
+        int32_t sj = -1;
+        if (t < T) {
+            const int32_t e = re0 + (t - rex);
+            const int64_t ei = (ry ? yoff : 0) + e;
+            int32_t B;
+            double st;
+            if (kFirst) {
+                const int32_t J = __ldg((ry ? L.col1 : L.col0) + e) + (ry ? L.n : 0);
+                B = cur[J];
+                st = -__ldg((ry ? L.val1 : L.val0) + e) / sqrt(rd * dcr[J]);
+                sbuf[ei] = st;
+                bbuf[ei] = B;
+            } else {
+                B = bbuf[ei];
+                st = sbuf[ei];
+            }
+            if (B != rA && st > 0.0 && (kFirst || mate[B] < 0)) {
+                sv = st;
+                sj = B;
+            }
+        }
+        const int rowv = t < T ? row : -1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double os = __shfl_down_sync(0xffffffffu, sv, o);
+            const int32_t oj = __shfl_down_sync(0xffffffffu, sj, o);
+            const int orow = __shfl_down_sync(0xffffffffu, rowv, o);
+            if (lane + o < 32 && orow == rowv) pick_merge(os, oj, sv, sj);
+        }
+        const int prow = __shfl_up_sync(0xffffffffu, rowv, 1);
+        if (rowv >= 0 && (lane == 0 || prow != rowv)) {
+            double b = best_s[w][rowv];
+            int32_t bj = best_j[w][rowv];
+            pick_merge(sv, sj, b, bj);
+            best_s[w][rowv] = b;
+            best_j[w][rowv] = bj;
+        }
+        __syncwarp();
+    }
+    if (I < rows) {
+        cand_s[I] = best_s[w][lane];
+        cand_b[I] = act ? best_j[w][lane] : -1;
+    }
+}
+
+// A node's pick: the best candidate of its member rows (mem, by position).
+__global__ void k_nodepick(const int32_t *count, const int32_t *size, const int32_t *mem,
+                           const double *cand_s, const int32_t *cand_b, const int32_t *mate,
+                           int32_t *pick) {
+    pdl_enter();
+    const int32_t A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= *count) return;
+    double best = 0.0;
+    int32_t bj = -1;
+    if (mate[A] < 0) {
+        const int k = size[A];
+        for (int p = 0; p < k; ++p) {
+            const int32_t m = mem[4 * A + p];
+            pick_merge(cand_s[m], cand_b[m], best, bj);
+        }
+    }
+    pick[A] = bj;
+}
+
 __global__ void k_handshake(const int32_t *count, const int32_t *pick, int32_t *mate) {
+    pdl_enter();
     const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= *count) return;
     const int32_t J = pick[I];
@@ -227,6 +347,7 @@ __global__ void k_handshake(const int32_t *count, const int32_t *pick, int32_t *
 }
 
 __global__ void k_leader_flag(const int32_t *count, const int32_t *mate, int32_t *flag) {
+    pdl_enter();
     const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= *count) return;
     const int32_t m = mate[I];
@@ -266,6 +387,7 @@ __device__ __forceinline__ int32_t block_excl_scan(int32_t v, int32_t *warp_tot,
 
 __global__ void __launch_bounds__(1024) k_scan_tiles(const int32_t *in, int32_t *out,
                                                      const int32_t *count, int32_t *tile_sum) {
+    pdl_enter();
     __shared__ int32_t warp_tot[33];
     const int32_t n = *count;
     const int64_t base = static_cast<int64_t>(blockIdx.x) * kScanTile;
@@ -282,6 +404,7 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(const int32_t *in, int32_t 
 
 __global__ void __launch_bounds__(1024) k_scan_sums(int32_t *tile_sum, const int32_t *count,
                                                     int32_t *total_out) {
+    pdl_enter();
     __shared__ int32_t warp_tot[33];
     __shared__ int32_t carry;
     const int32_t n = *count;
@@ -302,6 +425,7 @@ __global__ void __launch_bounds__(1024) k_scan_sums(int32_t *tile_sum, const int
 }
 
 __global__ void k_scan_add(int32_t *out, const int32_t *count, const int32_t *tile_sum) {
+    pdl_enter();
     const int32_t n = *count;
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -311,24 +435,24 @@ __global__ void k_scan_add(int32_t *out, const int32_t *count, const int32_t *ti
 // ---- level bookkeeping --------------------------------------------------------
 
 __global__ void k_number(const int32_t *count, const int32_t *mate, const int32_t *scan,
-                         int32_t *cid, int32_t *child0, int32_t *child1,
-                         const int32_t *size_old, int32_t *size_new) {
+                         int32_t *cid, const int32_t *size_old, int32_t *size_new) {
+    pdl_enter();
     const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= *count) return;
     const int32_t m = mate[I];
     if (m < 0 || I < m) {
         const int32_t J = scan[I];
         cid[I] = J;
-        child0[J] = I;
-        child1[J] = m;
         size_new[J] = size_old[I] + (m >= 0 ? size_old[m] : 0);
     } else {
         cid[I] = scan[m];
     }
 }
 
+// The last level: every row to its aggregate and position (in place).
 __global__ void k_follow(int32_t rows, int32_t *cur, int32_t *pos, const int32_t *mate,
                          const int32_t *cid, const int32_t *size_old) {
+    pdl_enter();
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= rows) return;
     const int32_t a = cur[c];
@@ -337,360 +461,123 @@ __global__ void k_follow(int32_t rows, int32_t *cur, int32_t *pos, const int32_t
     cur[c] = cid[a];
 }
 
-__global__ void k_reset_mate(const int32_t *count, int32_t *mate) {
-    const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
-    if (I < *count) mate[I] = -1;
+// Levels with a next level: row c moves to its new node J (cur_out) and
+// position, is listed as J's member at that position (mem, at most 4 per node
+// at the levels that read it), and forms t_c = d_c + (its entries whose
+// column lies in J, in storage order) for J's diagonal. J is the row's node a
+// and its mate b, so an entry is inside J when its column's node (the column
+// itself at level 0, kIdentity) is a or b. One warp per 32 rows walks their
+// entries 32 at a time as k_pick does; the matching values are staged in
+// shared memory with a ballot mask and each lane adds its own row's in
+// storage order.
+template <bool kIdentity>
+__global__ void __launch_bounds__(32 * kPickWarps) k_follow_t(LevelView L, int32_t rows,
+                                                              const int32_t *cur_in,
+                                                              int32_t *cur_out, int32_t *pos,
+                                                              const int32_t *mate,
+                                                              const int32_t *cid,
+                                                              const int32_t *size_old,
+                                                              int32_t *mem, double *tbuf) {
+    pdl_enter();
+    __shared__ double sv_s[kPickWarps][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int32_t base = (blockIdx.x * kPickWarps + w) * 32;
+    if (base >= rows) return;  // whole warp
+    const int32_t c = base + lane;
+    int32_t a = -1, b = -1, e0 = 0, len = 0;
+    bool yax = false;
+    double t = 0.0;
+    if (c < rows) {
+        a = kIdentity ? c : cur_in[c];
+        b = mate[a];
+        int32_t p = pos[c];
+        if (b >= 0 && b < a) p += size_old[b];
+        const int32_t J = cid[a];
+        cur_out[c] = J;
+        pos[c] = p;
+        mem[4 * J + p] = c;
+        const RowRef r = row_of(L, c);
+        e0 = r.e0;
+        len = r.e1 - r.e0;
+        yax = r.off != 0;
+        t = diag_of(L, c);
+    }
+    int32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    const int32_t excl = incl - len;
+    const int32_t T = __shfl_sync(0xffffffffu, incl, 31);
+    for (int32_t t0 = 0; t0 < T; t0 += 32) {
+        const int32_t q = t0 + lane;
+        int row = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int cand = row + step;
+            const int32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+            if (cand < 32 && ex <= q) row = cand;
+        }
+        const int32_t re0 = __shfl_sync(0xffffffffu, e0, row);
+        const int32_t rex = __shfl_sync(0xffffffffu, excl, row);
+        const bool ry = __shfl_sync(0xffffffffu, yax, row);
+        const int32_t ra = __shfl_sync(0xffffffffu, a, row);
+        const int32_t rb = __shfl_sync(0xffffffffu, b, row);
+        double v = 0.0;
+        bool hit = false;
+        if (q < T) {
+            const int32_t e = re0 + (q - rex);
+            const int32_t col = __ldg((ry ? L.col1 : L.col0) + e) + (ry ? L.n : 0);
+            const int32_t node = kIdentity ? col : cur_in[col];
+            hit = node == ra || node == rb;
+            if (hit) v = __ldg((ry ? L.val1 : L.val0) + e);
+        }
+        const unsigned hm = __ballot_sync(0xffffffffu, hit);
+        sv_s[w][lane] = v;
+        __syncwarp();
+        if (hm != 0u && len > 0) {
+            const int32_t lo = excl > t0 ? excl : t0;
+            const int32_t hi = excl + len < t0 + 32 ? excl + len : t0 + 32;
+            for (int32_t k = lo; k < hi; ++k)
+                if ((hm >> (k - t0)) & 1u) t += sv_s[w][k - t0];
+        }
+        __syncwarp();
+    }
+    if (c < rows) tbuf[c] = t;
 }
 
-// Raw length of every coarse row, and where its children's rows start
-// (row a at ea[J] with la[J] entries, row b at eb[J]), so that the coarse
-// kernels fetch all of a row's metadata in one round of independent loads.
-__global__ void k_rawlen(LevelView L, const int32_t *count, const int32_t *child0,
-                         const int32_t *child1, int32_t *rawlen, int32_t *ea, int32_t *eb,
-                         int32_t *la_out) {
+// Node J of the next level: its diagonal, the members' t in position order,
+// given to each member row (dcr), and its mate cleared for the next level's
+// matching.
+__global__ void k_dc(const int32_t *count, const int32_t *size, const int32_t *mem,
+                     const double *tbuf, double *dcr, int32_t *mate) {
+    pdl_enter();
     const int32_t J = blockIdx.x * blockDim.x + threadIdx.x;
     if (J >= *count) return;
-    const RowRef ra = row_of(L, child0[J]);
-    const int32_t la = ra.e1 - ra.e0;
-    int32_t len = la, e0b = ra.e0;
-    const int32_t b = child1[J];
-    if (b >= 0) {
-        const RowRef rb = row_of(L, b);
-        len += rb.e1 - rb.e0;
-        e0b = rb.e0;
-    }
-    rawlen[J] = len;
-    ea[J] = ra.e0;
-    eb[J] = e0b;
-    la_out[J] = la;
-}
-
-// Coarse row J = (a, b): the raw entries (row a's, then row b's) mapped to
-// coarse ids; ids equal to J fold into the diagonal in raw order
-// (d_a, a's entries, d_b, b's entries); the others are summed per id in raw
-// order and stored with the ids ascending. Two persistent grid-stride kernels:
-//   k_coarse_warp: one warp per row of raw length R <= kWarpRaw, two raw
-//     entries per lane in registers; for every entry the warp walks all R
-//     entries by shuffles to find whether it is the first of its id, its
-//     rank among the distinct ids and its raw-order sum; longer rows are
-//     appended to a list (order free: each row is processed on its own);
-//   k_coarse_heavy: one block per listed row: bitonic sort of (id, raw
-//     index) in shared memory for R <= kHeavyMax, output ranks by a block
-//     scan; longer rows by sorted insertion in one thread directly in the
-//     output row (rare: rows that long need nets of hundreds of pins).
-constexpr int kWarpRaw = 64;
-constexpr int kWarpWarps = 8;
-constexpr int kHeavyMax = 2048;
-constexpr int kHeavyThreads = 256;
-
-struct CoarseArgs {
-    LevelView L;
-    const int32_t *count;
-    const int32_t *child0, *child1, *cid, *start, *rawlen;
-    const int32_t *ea, *eb, *la;  // children's row starts and row a's length
-    int32_t *out_len, *out_col;
-    double *out_val, *out_diag;
-    int32_t *heavy;        // rows with R > kWarpRaw
-    int32_t *heavy_count;  // zero before k_coarse_warp
-};
-
-// Sorted insertion of (K, v) into keys/sums[0..k) (stride apart).
-template <typename KeyPtr, typename SumPtr>
-__device__ __forceinline__ void sorted_add(KeyPtr keys, SumPtr sums, int stride, int &k,
-                                           int32_t K, double v) {
-    int p = 0;
-    while (p < k && keys[p * stride] < K) ++p;
-    if (p < k && keys[p * stride] == K) {
-        sums[p * stride] += v;
-        return;
-    }
-    for (int q = k; q > p; --q) {
-        keys[q * stride] = keys[(q - 1) * stride];
-        sums[q * stride] = sums[(q - 1) * stride];
-    }
-    keys[p * stride] = K;
-    sums[p * stride] = v;
-    ++k;
-}
-
-// Row references of coarse row J's children from the precomputed starts
-// (both children are rows of the same axis at level 0).
-__device__ __forceinline__ void child_rows(const CoarseArgs &A, int32_t J, int32_t a, RowRef &ra,
-                                           RowRef &rb, int &la) {
-    const LevelView &L = A.L;
-    la = A.la[J];
-    const bool y = L.fine && a >= L.n;
-    ra.e0 = A.ea[J];
-    ra.e1 = ra.e0 + la;
-    ra.off = y ? L.n : 0;
-    ra.col = L.fine ? (y ? L.col1 : L.col0) : L.ccol;
-    ra.val = L.fine ? (y ? L.val1 : L.val0) : L.cval;
-    rb = ra;
-    rb.e0 = A.eb[J];
-    rb.e1 = rb.e0;  // unused: raw index e >= la selects row b
-}
-
-// Raw entry e of coarse row (a, b): its coarse id and value.
-__device__ __forceinline__ void raw_entry(const CoarseArgs &A, const RowRef &ra, const RowRef &rb,
-                                          int la, int e, int32_t &K, double &v) {
-    const bool in_a = e < la;
-    const int32_t idx = in_a ? ra.e0 + e : rb.e0 + (e - la);
-    K = A.cid[__ldg((in_a ? ra.col : rb.col) + idx) + (in_a ? ra.off : rb.off)];
-    v = __ldg((in_a ? ra.val : rb.val) + idx);
-}
-
-// Compare-exchange of a bitonic network: keep the smaller key when this
-// position should hold the smaller one.
-template <typename KeyT>
-__device__ __forceinline__ KeyT bitonic_keep(KeyT mine, KeyT other, bool keep_small) {
-    const bool less = mine < other;
-    return (less == keep_small) ? mine : other;
-}
-
-// Bitonic sort of P keys held two per lane (positions 2 * lane and
-// 2 * lane + 1), ascending; fully unrolled so every direction mask is a
-// constant. Positions at or beyond P (lanes >= P / 2) are left alone.
-template <int P, typename KeyT>
-__device__ __forceinline__ void bitonic_pairs(KeyT &k0, KeyT &k1, int lane) {
+    const int k = size[J];
+    int32_t m[4];
+    m[0] = mem[4 * J];
+    double d = tbuf[m[0]];
 #pragma unroll
-    for (int kk = 2; kk <= P; kk <<= 1) {
+    for (int p = 1; p < 4; ++p) {
+        if (p < k) {
+            m[p] = mem[4 * J + p];
+            d += tbuf[m[p]];
+        }
+    }
+    dcr[m[0]] = d;
 #pragma unroll
-        for (int j = kk >> 1; j > 0; j >>= 1) {
-            const int p0 = 2 * lane;
-            const bool asc = (p0 & kk) == 0;  // the same for p0 and p0 + 1
-            if (j == 1) {
-                const KeyT lo = k0 < k1 ? k0 : k1, hi = k0 < k1 ? k1 : k0;
-                k0 = asc ? lo : hi;
-                k1 = asc ? hi : lo;
-            } else {
-                const KeyT o0 = __shfl_xor_sync(0xffffffffu, k0, j >> 1);
-                const KeyT o1 = __shfl_xor_sync(0xffffffffu, k1, j >> 1);
-                const bool keep_small = ((p0 & j) == 0) == asc;  // p0 + 1 has the same bit j
-                k0 = bitonic_keep(k0, o0, keep_small);
-                k1 = bitonic_keep(k1, o1, keep_small);
-            }
-        }
-    }
-}
-
-// Keys are (coarse id << kShift) | raw index: 32-bit when the ids fit in
-// 26 bits, else 64-bit.
-template <typename KeyT>
-__global__ void __launch_bounds__(32 * kWarpWarps) k_coarse_warp(CoarseArgs A) {
-    constexpr int kShift = sizeof(KeyT) == 8 ? 32 : 6;
-    constexpr KeyT kPad = ~KeyT(0);
-    // per warp: the sorted (key, value) sequence, for the segment folds
-    __shared__ KeyT skey_s[kWarpWarps][kWarpRaw];
-    __shared__ double sval_s[kWarpWarps][kWarpRaw];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    KeyT *skey = skey_s[w];
-    double *sval = sval_s[w];
-    const LevelView &L = A.L;
-    const int32_t cnt = *A.count;
-    const int32_t warps = gridDim.x * kWarpWarps;
-    for (int32_t J = blockIdx.x * kWarpWarps + w; J < cnt; J += warps) {
-        const int32_t R = A.rawlen[J];
-        if (R > kWarpRaw) {
-            if (lane == 0) A.heavy[atomicAdd(A.heavy_count, 1)] = J;
-            continue;
-        }
-        const int32_t a = A.child0[J], b = A.child1[J];
-        RowRef ra, rb;
-        int la;
-        child_rows(A, J, a, ra, rb, la);
-        // positions p = 2 * lane + r hold raw entries e = p (r = 0, 1)
-        KeyT k0 = kPad, k1 = kPad;
-        double v0 = 0.0, v1 = 0.0;
-        {
-            const int e0 = 2 * lane, e1 = 2 * lane + 1;
-            int32_t K;
-            if (e0 < R) {
-                raw_entry(A, ra, rb, la, e0, K, v0);
-                k0 = (static_cast<KeyT>(static_cast<uint32_t>(K)) << kShift) | KeyT(e0);
-            }
-            if (e1 < R) {
-                raw_entry(A, ra, rb, la, e1, K, v1);
-                k1 = (static_cast<KeyT>(static_cast<uint32_t>(K)) << kShift) | KeyT(e1);
-            }
-        }
-        // raw values by raw index, for the folds after the sort
-        sval[2 * lane] = v0;
-        sval[2 * lane + 1] = v1;
-        // bitonic sort of the keys over P = 32 or 64 positions
-        if (R <= 32) bitonic_pairs<32>(k0, k1, lane);
-        else bitonic_pairs<64>(k0, k1, lane);
-        skey[2 * lane] = k0;
-        skey[2 * lane + 1] = k1;
-        __syncwarp();
-        // segment heads: first position of each id; ids != J are output rows
-        const uint32_t uJ = static_cast<uint32_t>(J);
-        const uint32_t K0 = static_cast<uint32_t>(k0 >> kShift), K1 = static_cast<uint32_t>(k1 >> kShift);
-        const uint32_t Kprev = lane == 0 ? 0xffffffffu
-                                         : static_cast<uint32_t>(skey[2 * lane - 1] >> kShift);
-        const bool in0 = 2 * lane < R, in1 = 2 * lane + 1 < R;
-        const bool first0 = in0 && (lane == 0 || Kprev != K0);
-        const bool first1 = in1 && K1 != K0;
-        const bool h0 = first0 && K0 != uJ, h1 = first1 && K1 != uJ;
-        const unsigned b0 = __ballot_sync(0xffffffffu, h0), b1 = __ballot_sync(0xffffffffu, h1);
-        const unsigned below = (1u << lane) - 1u;
-        const int rank0 = __popc(b0 & below) + __popc(b1 & below);
-        const int rank1 = rank0 + (h0 ? 1 : 0);
-        const int32_t st = A.start[J];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const bool h = r == 0 ? h0 : h1;
-            const bool dh = (r == 0 ? first0 : first1) && (r == 0 ? K0 : K1) == uJ;
-            const int p = 2 * lane + r;
-            const uint32_t K = r == 0 ? K0 : K1;
-            if (h) {
-                double sum = sval[static_cast<uint32_t>(skey[p] & ((KeyT(1) << kShift) - 1))];
-                for (int q = p + 1; q < R && static_cast<uint32_t>(skey[q] >> kShift) == K; ++q)
-                    sum += sval[static_cast<uint32_t>(skey[q] & ((KeyT(1) << kShift) - 1))];
-                const int rank = r == 0 ? rank0 : rank1;
-                A.out_col[st + rank] = static_cast<int32_t>(K);
-                A.out_val[st + rank] = sum;
-            }
-            if (dh) {
-                double dacc = diag_of(L, a);
-                bool added_b = false;
-                for (int q = p; q < R && static_cast<uint32_t>(skey[q] >> kShift) == K; ++q) {
-                    const uint32_t idx = static_cast<uint32_t>(skey[q] & ((KeyT(1) << kShift) - 1));
-                    if (!added_b && static_cast<int>(idx) >= la) {
-                        dacc += diag_of(L, b);
-                        added_b = true;
-                    }
-                    dacc += sval[idx];
-                }
-                if (!added_b && b >= 0) dacc += diag_of(L, b);
-                A.out_diag[J] = dacc;
-            }
-        }
-        const bool any_diag = __any_sync(0xffffffffu, (first0 && K0 == uJ) || (first1 && K1 == uJ));
-        if (lane == 0) {
-            A.out_len[J] = __popc(b0) + __popc(b1);
-            if (!any_diag) A.out_diag[J] = b >= 0 ? diag_of(L, a) + diag_of(L, b) : diag_of(L, a);
-        }
-        __syncwarp();
-    }
-}
-
-__global__ void __launch_bounds__(kHeavyThreads) k_coarse_heavy(CoarseArgs A) {
-    __shared__ unsigned long long key[kHeavyMax];
-    __shared__ double vr[kHeavyMax];
-    __shared__ int32_t warp_tot[33];
-    const LevelView &L = A.L;
-    const int tid = threadIdx.x;
-    const int32_t nh = *A.heavy_count;
-    for (int32_t h = blockIdx.x; h < nh; h += gridDim.x) {
-        const int32_t J = A.heavy[h];
-        const int32_t R = A.rawlen[J];
-        const int32_t a = A.child0[J], b = A.child1[J];
-        RowRef ra, rb;
-        int la;
-        child_rows(A, J, a, ra, rb, la);
-        if (R > kHeavyMax) {
-            if (tid == 0) {
-                int32_t *keys = A.out_col + A.start[J];
-                double *sums = A.out_val + A.start[J];
-                int k = 0;
-                double dacc = diag_of(L, a);
-                for (int e = 0; e < R; ++e) {
-                    if (e == la) dacc += diag_of(L, b);
-                    int32_t K;
-                    double v;
-                    raw_entry(A, ra, rb, la, e, K, v);
-                    if (K == J) dacc += v;
-                    else sorted_add(keys, sums, 1, k, K, v);
-                }
-                if (la == R && b >= 0) dacc += diag_of(L, b);
-                A.out_len[J] = k;
-                A.out_diag[J] = dacc;
-            }
-            __syncthreads();
-            continue;
-        }
-        int P = 1;
-        while (P < R) P <<= 1;
-        for (int e = tid; e < P; e += kHeavyThreads) {
-            if (e < R) {
-                int32_t K;
-                double v;
-                raw_entry(A, ra, rb, la, e, K, v);
-                key[e] = (static_cast<unsigned long long>(static_cast<uint32_t>(K)) << 32) |
-                         static_cast<uint32_t>(e);
-                vr[e] = v;
-            } else {
-                key[e] = ~0ull;
-            }
-        }
-        __syncthreads();
-        for (int kk = 2; kk <= P; kk <<= 1) {
-            for (int j = kk >> 1; j > 0; j >>= 1) {
-                for (int i = tid; i < P; i += kHeavyThreads) {
-                    const int ixj = i ^ j;
-                    if (ixj > i) {
-                        const unsigned long long x = key[i], y = key[ixj];
-                        if ((x > y) == ((i & kk) == 0)) {
-                            key[i] = y;
-                            key[ixj] = x;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
-        }
-        // segment heads (ids != J) in ascending order, ranked by a block scan
-        const uint32_t uJ = static_cast<uint32_t>(J);
-        int32_t running = 0;
-        int any_diag = 0;
-        for (int i0 = 0; i0 < R; i0 += kHeavyThreads) {
-            const int i = i0 + tid;
-            bool head = false, dhead = false;
-            uint32_t K = 0;
-            if (i < R) {
-                K = static_cast<uint32_t>(key[i] >> 32);
-                const bool first = i == 0 || static_cast<uint32_t>(key[i - 1] >> 32) != K;
-                head = first && K != uJ;
-                dhead = first && K == uJ;
-            }
-            int32_t tot;
-            const int32_t ex = block_excl_scan(head ? 1 : 0, warp_tot, tot);
-            if (head) {
-                double sum = vr[static_cast<uint32_t>(key[i])];
-                for (int q = i + 1; q < R && static_cast<uint32_t>(key[q] >> 32) == K; ++q)
-                    sum += vr[static_cast<uint32_t>(key[q])];
-                A.out_col[A.start[J] + running + ex] = static_cast<int32_t>(K);
-                A.out_val[A.start[J] + running + ex] = sum;
-            }
-            if (dhead) {
-                double dacc = diag_of(L, a);
-                bool added_b = false;
-                for (int q = i; q < R && static_cast<uint32_t>(key[q] >> 32) == K; ++q) {
-                    const uint32_t idx = static_cast<uint32_t>(key[q]);
-                    if (!added_b && static_cast<int>(idx) >= la) {
-                        dacc += diag_of(L, b);
-                        added_b = true;
-                    }
-                    dacc += vr[idx];
-                }
-                if (!added_b && b >= 0) dacc += diag_of(L, b);
-                A.out_diag[J] = dacc;
-            }
-            any_diag |= __syncthreads_or(dhead ? 1 : 0);
-            running += tot;
-        }
-        if (tid == 0) {
-            A.out_len[J] = running;
-            if (!any_diag) A.out_diag[J] = b >= 0 ? diag_of(L, a) + diag_of(L, b) : diag_of(L, a);
-        }
-        __syncthreads();
-    }
+    for (int p = 1; p < 4; ++p)
+        if (p < k) dcr[m[p]] = d;
+    mate[J] = -1;
 }
 
 // ---- final layout, permuted system, block inverses -------------------------
 
 __global__ void k_newpos(int32_t rows, const int32_t *cur, const int32_t *pos,
                          const int32_t *agg_start, int32_t *newpos, int32_t *order) {
+    pdl_enter();
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= rows) return;
     const int32_t p = agg_start[cur[c]] + pos[c];
@@ -699,6 +586,7 @@ __global__ void k_newpos(int32_t rows, const int32_t *cur, const int32_t *pos,
 }
 
 __global__ void k_plen(LevelView L, int32_t rows, const int32_t *order, int32_t *plen) {
+    pdl_enter();
     const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= rows) return;
     const RowRef r = row_of(L, order[k]);
@@ -722,6 +610,7 @@ __global__ void __launch_bounds__(32 * kPfWarps)
                   double *__restrict__ prhs, int coarse_mode, const float *__restrict__ hw,
                   const float *__restrict__ emb, const double *__restrict__ logd,
                   double *__restrict__ zd) {
+    pdl_enter();
     const int lane = threadIdx.x & 31;
     const int32_t k0 = (static_cast<int32_t>(blockIdx.x) * kPfWarps + (threadIdx.x >> 5)) * 32;
     if (k0 >= rows) return;  // whole warp
@@ -812,6 +701,7 @@ __global__ void __launch_bounds__(32 * kInvWarps)
                      const int32_t *__restrict__ pcol, const double *__restrict__ pval,
                      const double *__restrict__ pdiag, float *__restrict__ minv,
                      int32_t *__restrict__ meta) {
+    pdl_enter();
     __shared__ double rows_s[kInvWarps][32][kInvStride];
     __shared__ double rinv_s[kInvWarps][32];
     __shared__ int ok_s[kInvWarps][4];
@@ -917,6 +807,7 @@ __global__ void __launch_bounds__(32 * kInvWarps)
 // blk_start[b] = first aggregate start >= b * ceil(rows / grid).
 __global__ void k_blkstart(int grid, int32_t rows, const int32_t *count, const int32_t *agg_start,
                            int32_t *blk_start) {
+    pdl_enter();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b > grid) return;
     const int32_t per = (rows + grid - 1) / grid;
@@ -933,6 +824,7 @@ __global__ void k_blkstart(int grid, int32_t rows, const int32_t *count, const i
 
 __global__ void k_perm_in(int32_t rows, int32_t n, const int32_t *order, const double *x,
                           const double *y, double *px) {
+    pdl_enter();
     const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= rows) return;
     const int32_t c = order[k];
@@ -963,6 +855,7 @@ __global__ void k_perm_out(int32_t rows, int32_t n, const int32_t *order, const 
 __global__ void k_coarse_z(int mode, int32_t rows, int32_t n, const int32_t *prp,
                            const double *pval, const double *pdiag, const int32_t *order,
                            const float *hw, const float *emb, const double *logd, double *zd) {
+    pdl_enter();
     const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= rows) return;
     float z = 1.0f;
@@ -994,6 +887,7 @@ __global__ void __launch_bounds__(kAzThreads)
                 const double *__restrict__ zd, int32_t n, int32_t rows_total,
                 int32_t rows_per_block, float2 *__restrict__ zaz, double *part, unsigned *ticket,
                 double *einv) {
+    pdl_enter();
     __shared__ __align__(16) double tilebuf[(kAzThreads / 32) * kTileChunk];
     __shared__ int32_t wb[kAzThreads / 32 + 1];
     __shared__ double red[33 * 2];
@@ -1051,14 +945,14 @@ int grow(ktg_ctx *c, T **p, int64_t count) {
 int reserve(ktg_ctx *c, AggState *s, int64_t rows, int64_t nnz) {
     int rc = KTG_OK;
     if (rows > s->cap_rows) {
-        for (int32_t **p : {&s->mate, &s->pick, &s->flag, &s->cid, &s->child0, &s->child1,
-                            &s->size_a, &s->size_b, &s->cur, &s->pos, &s->cstart[0], &s->cstart[1],
-                            &s->clen[0], &s->clen[1], &s->order, &s->newpos, &s->meta, &s->ea,
-                            &s->eb, &s->la})
+        for (int32_t **p : {&s->mate, &s->pick, &s->flag, &s->cid, &s->size_a, &s->size_b,
+                            &s->cur, &s->cur2, &s->pos, &s->cand_b, &s->order, &s->newpos,
+                            &s->meta})
             if ((rc = grow(c, p, rows))) return rc;
+        if ((rc = grow(c, &s->mem, 4 * rows))) return rc;
         if ((rc = grow(c, &s->agg_start, rows + 1))) return rc;
         if ((rc = grow(c, &s->prp, rows + 1))) return rc;
-        for (double **p : {&s->cdiag[0], &s->cdiag[1], &s->pdiag, &s->prhs, &s->px})
+        for (double **p : {&s->cand_s, &s->tbuf, &s->dc, &s->pdiag, &s->prhs, &s->px})
             if ((rc = grow(c, p, rows))) return rc;
         if ((rc = grow(c, &s->minv, rows * kAggMax))) return rc;
         if ((rc = grow(c, &s->zaz, rows))) return rc;
@@ -1069,10 +963,8 @@ int reserve(ktg_ctx *c, AggState *s, int64_t rows, int64_t nnz) {
         s->cap_rows = rows;
     }
     if (nnz > s->cap_nnz) {
-        for (int t = 0; t < 2; ++t) {
-            if ((rc = grow(c, &s->ccol[t], nnz))) return rc;
-            if ((rc = grow(c, &s->cval[t], nnz))) return rc;
-        }
+        if ((rc = grow(c, &s->sbuf, nnz))) return rc;
+        if ((rc = grow(c, &s->bbuf, nnz))) return rc;
         if ((rc = grow(c, &s->pcol, nnz))) return rc;
         if ((rc = grow(c, &s->pval, nnz))) return rc;
         if ((rc = grow(c, &s->pval32, nnz))) return rc;
@@ -1091,14 +983,33 @@ int blocks_for(int64_t items, int threads) {
     return static_cast<int>(std::max<int64_t>(1, (items + threads - 1) / threads));
 }
 
+// Launches a set-up kernel on the context's stream as a programmatic
+// dependent launch (the kernel starts with pdl_enter), so that its blocks are
+// scheduled while the kernel before it drains; failures surface through
+// cudaGetLastError at the end of each set-up step.
+template <typename... P, typename... A>
+void launch(ktg_ctx *c, void (*kernel)(P...), int grid, int block, A &&...args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+    ++c->launches;
+}
+
 // Exclusive scan of in[0 .. *count) into out, total into *total.
 void scan(ktg_ctx *c, AggState *s, const int32_t *in, int32_t *out, const int32_t *count,
           int64_t upper, int32_t *total) {
     const int tiles = blocks_for(upper, kScanTile);
-    k_scan_tiles<<<tiles, 1024, 0, c->stream>>>(in, out, count, s->tile_sum);
-    k_scan_sums<<<1, 1024, 0, c->stream>>>(s->tile_sum, count, total);
-    k_scan_add<<<blocks_for(upper, kT), kT, 0, c->stream>>>(out, count, s->tile_sum);
-    c->launches += 3;
+    launch(c, k_scan_tiles, tiles, 1024, in, out, count, s->tile_sum);
+    launch(c, k_scan_sums, 1, 1024, s->tile_sum, count, total);
+    launch(c, k_scan_add, blocks_for(upper, kT), kT, out, count, s->tile_sum);
 }
 
 }  // namespace
@@ -1107,16 +1018,14 @@ void free_agg(ktg_ctx *c) {
     AggState *s = c->agg;
     if (!s) return;
     for (void *p : {(void *)s->mate, (void *)s->pick, (void *)s->flag, (void *)s->cid,
-                    (void *)s->child0, (void *)s->child1, (void *)s->size_a, (void *)s->size_b,
-                    (void *)s->cur, (void *)s->pos, (void *)s->cstart[0], (void *)s->cstart[1],
-                    (void *)s->clen[0], (void *)s->clen[1], (void *)s->ccol[0], (void *)s->ccol[1],
-                    (void *)s->cval[0], (void *)s->cval[1], (void *)s->cdiag[0],
-                    (void *)s->cdiag[1], (void *)s->counts, (void *)s->tile_sum,
-                    (void *)s->agg_start, (void *)s->order, (void *)s->newpos, (void *)s->prp,
-                    (void *)s->pcol, (void *)s->pval, (void *)s->pval32, (void *)s->pdiag,
-                    (void *)s->prhs, (void *)s->px, (void *)s->minv, (void *)s->meta,
-                    (void *)s->blk_start, (void *)s->gslice, (void *)s->ea, (void *)s->eb,
-                    (void *)s->la, (void *)s->zaz, (void *)s->zd, (void *)s->coarse_einv,
+                    (void *)s->size_a, (void *)s->size_b, (void *)s->cur, (void *)s->cur2,
+                    (void *)s->pos, (void *)s->mem, (void *)s->cand_b, (void *)s->cand_s,
+                    (void *)s->tbuf, (void *)s->dc, (void *)s->sbuf, (void *)s->bbuf,
+                    (void *)s->counts, (void *)s->tile_sum, (void *)s->agg_start,
+                    (void *)s->order, (void *)s->newpos, (void *)s->prp, (void *)s->pcol,
+                    (void *)s->pval, (void *)s->pval32, (void *)s->pdiag, (void *)s->prhs,
+                    (void *)s->px, (void *)s->minv, (void *)s->meta, (void *)s->blk_start,
+                    (void *)s->gslice, (void *)s->zaz, (void *)s->zd, (void *)s->coarse_einv,
                     (void *)s->coarse_part, (void *)s->ticket})
         if (p) cudaFree(p);
     delete s;
@@ -1138,15 +1047,13 @@ int build_agg(ktg_ctx *c) {
     if (rc) return rc;
     const int32_t R = static_cast<int32_t>(rows);
     if (rows == 0) {  // counts all zero: empty row ranges for the solve
-        k_init<<<1, kT, 0, c->stream>>>(0, s->cur, s->pos, s->size_a, s->mate, s->counts);
-        ++c->launches;
+        launch(c, k_init, 1, kT, 0, s->cur, s->pos, s->size_a, s->mate, s->counts);
         s->blk_grid = 0;
         c->agg_ready = true;
         KTG_CUDA(c, cudaGetLastError());
         return KTG_OK;
     }
     LevelView L0{};
-    L0.fine = true;
     L0.n = static_cast<int32_t>(n);
     L0.rp0 = c->sys[0].row_ptr;
     L0.rp1 = c->sys[1].row_ptr;
@@ -1158,69 +1065,57 @@ int build_agg(ktg_ctx *c) {
     L0.diag1 = c->sys[1].diag;
     int32_t *cnt = s->counts;  // cnt[l] = nodes at level l; 4, 6, 7 scratch counts
     const int gR = blocks_for(rows, kT);
-    k_init<<<gR, kT, 0, c->stream>>>(R, s->cur, s->pos, s->size_a, s->mate, cnt);
-    ++c->launches;
+    const int gP = blocks_for(rows, 32 * kPickWarps);
+    launch(c, k_init, gR, kT, R, s->cur, s->pos, s->size_a, s->mate, cnt);
     int32_t *size_old = s->size_a, *size_new = s->size_b;
-    LevelView L = L0;
+    int32_t *cur = s->cur, *cur_next = s->cur2;
+    // per-entry strengths (and, above level 0, neighbour nodes): y rows at yoff
+    const int64_t yoff = c->sys_cap_nnz;
     for (int level = 0; level < kLevels; ++level) {
         const int32_t *count = cnt + level;
-        // strengths of this level's entries live in cval[level & 1] until this
-        // level's coarsening overwrites that buffer (level 0 reads the axis
-        // CSRs, level l > 0 reads cval[(l - 1) & 1])
-        double *sbuf = s->cval[level & 1];
-        const int64_t yoff = c->sys_cap_nnz;
-        const int gP = blocks_for(rows, 32 * kPickWarps);
         for (int round = 0; round < kRounds; ++round) {
-            if (round == 0)
-                k_pick<true><<<gP, 32 * kPickWarps, 0, c->stream>>>(L, count, s->mate, s->pick, sbuf, yoff);
-            else
-                k_pick<false><<<gP, 32 * kPickWarps, 0, c->stream>>>(L, count, s->mate, s->pick, sbuf, yoff);
-            k_handshake<<<gR, kT, 0, c->stream>>>(count, s->pick, s->mate);
-            c->launches += 2;
+            if (level == 0) {
+                if (round == 0)
+                    launch(c, k_pick<true>, gP, 32 * kPickWarps, L0, count, s->mate, s->pick,
+                           s->sbuf, yoff);
+                else
+                    launch(c, k_pick<false>, gP, 32 * kPickWarps, L0, count, s->mate, s->pick,
+                           s->sbuf, yoff);
+            } else {
+                if (round == 0)
+                    launch(c, k_rowpick<true>, gP, 32 * kPickWarps, L0, R, cur, s->mate, s->dc,
+                           s->sbuf, s->bbuf, yoff, s->cand_s, s->cand_b);
+                else
+                    launch(c, k_rowpick<false>, gP, 32 * kPickWarps, L0, R, cur, s->mate, s->dc,
+                           s->sbuf, s->bbuf, yoff, s->cand_s, s->cand_b);
+                launch(c, k_nodepick, gR, kT, count, size_old, s->mem, s->cand_s, s->cand_b,
+                       s->mate, s->pick);
+            }
+            launch(c, k_handshake, gR, kT, count, s->pick, s->mate);
         }
-        k_leader_flag<<<gR, kT, 0, c->stream>>>(count, s->mate, s->flag);
-        ++c->launches;
+        launch(c, k_leader_flag, gR, kT, count, s->mate, s->flag);
         scan(c, s, s->flag, s->flag, count, rows, cnt + level + 1);
-        k_number<<<gR, kT, 0, c->stream>>>(count, s->mate, s->flag, s->cid, s->child0, s->child1,
-                                           size_old, size_new);
-        k_follow<<<gR, kT, 0, c->stream>>>(R, s->cur, s->pos, s->mate, s->cid, size_old);
-        c->launches += 2;
+        launch(c, k_number, gR, kT, count, s->mate, s->flag, s->cid, size_old, size_new);
         if (level + 1 < kLevels) {
-            const int t = level & 1;
-            const int32_t *next = cnt + level + 1;
-            // raw lengths in s->pick (free until the next level's matching);
-            // the heavy-row list in s->flag (its scan was used by k_number)
-            k_rawlen<<<gR, kT, 0, c->stream>>>(L, next, s->child0, s->child1, s->pick, s->ea,
-                                               s->eb, s->la);
-            scan(c, s, s->pick, s->cstart[t], next, rows, cnt + 4);
-            KTG_CUDA(c, cudaMemsetAsync(cnt + 7, 0, sizeof(int32_t), c->stream));
-            const CoarseArgs CA{L,          next,         s->child0, s->child1,  s->cid,
-                                s->cstart[t], s->pick,    s->ea,     s->eb,      s->la,
-                                s->clen[t], s->ccol[t],   s->cval[t], s->cdiag[t], s->flag,
-                                cnt + 7};
-            if (rows < (1ll << 26))
-                k_coarse_warp<uint32_t><<<8 * c->num_sms, 32 * kWarpWarps, 0, c->stream>>>(CA);
+            // rows to the next level's nodes, members and diagonals
+            if (level == 0)
+                launch(c, k_follow_t<true>, gP, 32 * kPickWarps, L0, R, cur, cur_next, s->pos,
+                       s->mate, s->cid, size_old, s->mem, s->tbuf);
             else
-                k_coarse_warp<unsigned long long><<<8 * c->num_sms, 32 * kWarpWarps, 0, c->stream>>>(CA);
-            k_coarse_heavy<<<4 * c->num_sms, kHeavyThreads, 0, c->stream>>>(CA);
-            k_reset_mate<<<gR, kT, 0, c->stream>>>(next, s->mate);
-            c->launches += 4;
-            LevelView C{};
-            C.fine = false;
-            C.start = s->cstart[t];
-            C.len = s->clen[t];
-            C.ccol = s->ccol[t];
-            C.cval = s->cval[t];
-            C.cdiag = s->cdiag[t];
-            L = C;
+                launch(c, k_follow_t<false>, gP, 32 * kPickWarps, L0, R, cur, cur_next, s->pos,
+                       s->mate, s->cid, size_old, s->mem, s->tbuf);
+            launch(c, k_dc, gR, kT, cnt + level + 1, size_new, s->mem, s->tbuf, s->dc,
+                   s->mate);
+            std::swap(cur, cur_next);
+        } else {
+            launch(c, k_follow, gR, kT, R, cur, s->pos, s->mate, s->cid, size_old);
         }
         std::swap(size_old, size_new);
     }
     // size_old now holds the aggregate sizes; cnt[kLevels] the aggregate count
     const int32_t *nagg = cnt + kLevels;
     scan(c, s, size_old, s->agg_start, nagg, rows, cnt + 5);
-    k_newpos<<<gR, kT, 0, c->stream>>>(R, s->cur, s->pos, s->agg_start, s->newpos, s->order);
-    ++c->launches;
+    launch(c, k_newpos, gR, kT, R, cur, s->pos, s->agg_start, s->newpos, s->order);
     KTG_CUDA(c, cudaGetLastError());
     s->final_size = size_old;
     s->struct_rows = rows;
@@ -1244,7 +1139,6 @@ int build_agg_values(ktg_ctx *c) {
     }
     const int gR = blocks_for(rows, kT);
     LevelView L0{};
-    L0.fine = true;
     L0.n = static_cast<int32_t>(n);
     L0.rp0 = c->sys[0].row_ptr;
     L0.rp1 = c->sys[1].row_ptr;
@@ -1256,21 +1150,18 @@ int build_agg_values(ktg_ctx *c) {
     L0.diag1 = c->sys[1].diag;
     int32_t *cnt = s->counts;
     const int32_t *nagg = cnt + kLevels;
-    k_plen<<<gR, kT, 0, c->stream>>>(L0, R, s->order, s->prp);
-    ++c->launches;
+    launch(c, k_plen, gR, kT, L0, R, s->order, s->prp);
     // prp: exclusive scan of the permuted row lengths (cnt[6] = R), total at prp[R]
     scan(c, s, s->prp, s->prp, cnt + 6, rows, s->prp + R);
     // the coarse vector of the current mode comes with the permuted system
     // (the learned one only when it is ready)
     const int zmode = (c->coarse == 3 && !c->coarse_z_ready) ? 0 : c->coarse;
-    k_pfill_tiles<<<blocks_for(rows, 32 * kPfWarps), 32 * kPfWarps, 0, c->stream>>>(
-        L0, R, s->order, s->newpos, s->prp, c->sys[0].rhs, c->sys[1].rhs, s->pcol, s->pval,
-        s->pval32, s->pdiag, s->prhs, zmode, c->coarse_head_w, c->coarse_emb, c->coarse_logd,
-        s->zd);
-    k_blockinv_lanes<<<blocks_for(rows, kInvPerBlock), 32 * kInvWarps, 0, c->stream>>>(
-        nagg, s->agg_start, s->final_size, static_cast<int32_t>(n), s->prp, s->pcol, s->pval,
-        s->pdiag, s->minv, s->meta);
-    c->launches += 2;
+    launch(c, k_pfill_tiles, blocks_for(rows, 32 * kPfWarps), 32 * kPfWarps, L0, R, s->order,
+           s->newpos, s->prp, c->sys[0].rhs, c->sys[1].rhs, s->pcol, s->pval, s->pval32, s->pdiag,
+           s->prhs, zmode, c->coarse_head_w, c->coarse_emb, c->coarse_logd, s->zd);
+    launch(c, k_blockinv_lanes, blocks_for(rows, kInvPerBlock), 32 * kInvWarps, nagg,
+           s->agg_start, s->final_size, static_cast<int32_t>(n), s->prp, s->pcol, s->pval,
+           s->pdiag, s->minv, s->meta);
     KTG_CUDA(c, cudaGetLastError());
     s->coarse_mode = 0;
     s->z_mode = zmode;  // z of this mode is in s->zd; A z not formed yet
@@ -1310,10 +1201,8 @@ int agg_coarse_setup(ktg_ctx *c, int mode) {
     }
     const int32_t R = static_cast<int32_t>(rows), n = static_cast<int32_t>(c->sys_n);
     if (s->z_mode != mode || (mode == 3 && s->z_gen != c->coarse_z_gen)) {  // z is stale
-        k_coarse_z<<<blocks_for(rows, kT), kT, 0, c->stream>>>(
-            mode, R, n, s->prp, s->pval, s->pdiag, s->order, c->coarse_head_w, c->coarse_emb,
-            c->coarse_logd, s->zd);
-        ++c->launches;
+        launch(c, k_coarse_z, blocks_for(rows, kT), kT, mode, R, n, s->prp, s->pval, s->pdiag,
+               s->order, c->coarse_head_w, c->coarse_emb, c->coarse_logd, s->zd);
         s->z_mode = mode;
         s->z_gen = c->coarse_z_gen;
     }
@@ -1323,10 +1212,9 @@ int agg_coarse_setup(ktg_ctx *c, int mode) {
     const int blocks = static_cast<int>((rows + per - 1) / per);
     if (2 * blocks > 2 * ((rows + kT - 1) / kT))
         return set_error(c, KTG_ERR_STATE, "coarse partials buffer too small");
-    k_coarse_az<<<blocks, kAzThreads, 0, c->stream>>>(s->prp, s->pcol, s->pval, s->pdiag, s->zd, n,
-                                                      R, per, s->zaz, s->coarse_part, s->ticket,
-                                                      s->coarse_einv);
-    ++c->launches;
+    launch(c, k_coarse_az, blocks, kAzThreads, s->prp, s->pcol, s->pval, s->pdiag, s->zd, n,
+           R, per, s->zaz, s->coarse_part, s->ticket,
+           s->coarse_einv);
     KTG_CUDA(c, cudaGetLastError());
     s->coarse_mode = mode;
     return KTG_OK;
@@ -1343,16 +1231,14 @@ int agg_prepare_solve(ktg_ctx *c, int grid, const double *x, const double *y, in
             if (rc) return rc;
             s->grid_cap = grid + 1;
         }
-        k_blkstart<<<blocks_for(grid + 1, kT), kT, 0, c->stream>>>(
-            grid, static_cast<int32_t>(rows), s->counts + kLevels, s->agg_start, s->blk_start);
-        ++c->launches;
+        launch(c, k_blkstart, blocks_for(grid + 1, kT), kT, grid, static_cast<int32_t>(rows),
+               s->counts + kLevels, s->agg_start, s->blk_start);
         s->blk_grid = grid;
     }
     *rows_cap = static_cast<int32_t>((rows + grid - 1) / grid + kAggMax);
     if (rows > 0) {
-        k_perm_in<<<blocks_for(rows, kT), kT, 0, c->stream>>>(
-            static_cast<int32_t>(rows), static_cast<int32_t>(c->sys_n), s->order, x, y, s->px);
-        ++c->launches;
+        launch(c, k_perm_in, blocks_for(rows, kT), kT, static_cast<int32_t>(rows),
+               static_cast<int32_t>(c->sys_n), s->order, x, y, s->px);
     }
     KTG_CUDA(c, cudaGetLastError());
     return KTG_OK;

@@ -11,16 +11,20 @@ struct AggState {
     int64_t cap_rows = 0;  // 2n capacity
     int64_t cap_nnz = 0;   // nnz(x) + nnz(y) capacity
     int grid_cap = 0;
-    // level work
+    // level work: per node of the current level (mate, pick, flag, cid,
+    // sizes, members by position), per fine row (its node in cur / cur2,
+    // position, best candidate, internal sum, its node's diagonal dc), per
+    // fine entry (strength sbuf and neighbour node bbuf of the level)
     int32_t *mate = nullptr, *pick = nullptr, *flag = nullptr, *cid = nullptr;
-    int32_t *child0 = nullptr, *child1 = nullptr, *size_a = nullptr, *size_b = nullptr;
-    int32_t *cur = nullptr, *pos = nullptr;
-    int32_t *ea = nullptr, *eb = nullptr, *la = nullptr;  // coarse rows' children row starts
-    int32_t *cstart[2] = {nullptr, nullptr};
-    int32_t *clen[2] = {nullptr, nullptr};
-    int32_t *ccol[2] = {nullptr, nullptr};
-    double *cval[2] = {nullptr, nullptr};
-    double *cdiag[2] = {nullptr, nullptr};
+    int32_t *size_a = nullptr, *size_b = nullptr;
+    int32_t *cur = nullptr, *cur2 = nullptr, *pos = nullptr;
+    int32_t *mem = nullptr;        // [4 * 2n] members of a node by position
+    int32_t *cand_b = nullptr;     // [2n]
+    double *cand_s = nullptr;      // [2n]
+    double *tbuf = nullptr;        // [2n]
+    double *dc = nullptr;          // [2n]
+    double *sbuf = nullptr;        // [nnz]
+    int32_t *bbuf = nullptr;       // [nnz]
     int32_t *counts = nullptr;     // [8] node counts per level, totals
     int32_t *tile_sum = nullptr;   // scan tiles
     int64_t tiles_cap = 0;

@@ -47,6 +47,19 @@ __device__ __forceinline__ void red_add_release_gpu(unsigned *p, unsigned v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
+// Programmatic dependent launch. A kernel launched with the programmatic
+// stream serialization attribute may be scheduled while the kernel before it
+// in the stream is still draining. It calls pdl_enter() before touching
+// memory: griddepcontrol.wait returns once the previous kernel has completed
+// and its writes are visible (so every kernel of such a chain orders after all
+// earlier ones), and launch_dependents lets the next kernel's blocks be
+// scheduled in turn. In a kernel launched without the attribute both are
+// no-ops.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Sum over a warp in a fixed butterfly order; every lane gets the total.
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

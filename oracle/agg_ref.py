@@ -6,21 +6,24 @@ permutation and block inverses can be compared exactly on small systems.
 
 The x and y systems are treated as one block-diagonal system of 2n rows
 (row c < n is x row c, row c >= n is y row c - n); no entry couples the axes,
-so no aggregate mixes them. Three levels of pairwise aggregation:
+so no aggregate mixes them. Three levels of pairwise aggregation; the nodes
+of level 0 are the rows of A (off-diagonal CSR, duplicates unmerged), a node
+of level l + 1 is a matched pair or a single node of level l:
 
-  level 0 nodes are the rows of A (off-diagonal CSR, duplicates unmerged);
-  strength of a stored entry (I, J, v):  s = -v / sqrt(d_I * d_J)
-  ROUNDS handshake rounds: every unmatched node I picks the unmatched J != I
-     with the largest s > 0 over its stored entries (ties: smaller J);
-     I and J are matched when they picked each other;
-  leaders: unmatched nodes and the smaller node of each pair; coarse ids
-     number the leaders in order;
-  coarse row of J = (a, b) (b = -1 if a is alone): the entries of row a, then
-     of row b, mapped to coarse ids; entries mapping to J add to the coarse
-     diagonal (d_a + entries(a -> J) + d_b + entries(b -> J), in that order),
-     the others are summed per coarse id in that same (raw) order and stored
-     with the ids ascending;
+  dc(N): the node's Galerkin diagonal, the sum over its member rows m in
+     position order of t_m = d_m + (m's entries whose column's node is N, in
+     storage order); dc = d at level 0;
+  strength of a stored entry (i, j, v) between the nodes A of i and B != A
+     of j:  s = -v / sqrt(dc(A) * dc(B));
+  ROUNDS handshake rounds: every unmatched node A picks the unmatched B
+     with the largest s > 0 over all its member rows' entries (ties: smaller
+     B); A and B are matched when they picked each other;
+  leaders: unmatched nodes and the smaller node of each pair; the next
+     level's ids number the leaders in order;
   fine row c follows its node: pos_c += size(a) when its node is b.
+
+A node's coupling to another is its strongest single entry to it, so no
+coarse matrix is formed.
 
 Aggregates (at most 8 rows) are laid out contiguously in coarse-id order
 (newpos = start of its aggregate + pos), which puts every x row before every
@@ -39,7 +42,7 @@ AGG_MAX = 1 << LEVELS
 
 
 class _Level:
-    """Rows of one level: lists of (col, val) in storage order, and diag."""
+    """The fine rows: lists of (col, val) in storage order, and diag."""
 
     def __init__(self, cols, vals, diag):
         self.cols = cols
@@ -59,54 +62,52 @@ def _fine_level(sx: dict, sy: dict) -> _Level:
     return _Level(cols, vals, np.concatenate([sx["diag"], sy["diag"]]).astype(np.float64))
 
 
-def _match(lv: _Level) -> np.ndarray:
-    N = lv.diag.shape[0]
-    d = lv.diag
+def _match(lv: _Level, cur: np.ndarray, dc: np.ndarray, N: int) -> np.ndarray:
+    members = [[] for _ in range(N)]
+    for c in range(cur.shape[0]):
+        members[int(cur[c])].append(c)
     mate = np.full(N, -1, np.int64)
     for _ in range(ROUNDS):
         pick = np.full(N, -1, np.int64)
-        for I in range(N):
-            if mate[I] >= 0:
+        for A in range(N):
+            if mate[A] >= 0:
                 continue
             best, bj = 0.0, -1
-            for J, v in zip(lv.cols[I], lv.vals[I]):
-                J = int(J)
-                if J == I or mate[J] >= 0:
-                    continue
-                s = -v / np.sqrt(d[I] * d[J])
-                if s > 0.0 and (s > best or (s == best and J < bj)):
-                    best, bj = s, J
-            pick[I] = bj
-        for I in range(N):
-            J = pick[I]
-            if mate[I] < 0 and J >= 0 and pick[J] == I:
-                mate[I] = J
+            for m in members[A]:
+                for J, v in zip(lv.cols[m], lv.vals[m]):
+                    B = int(cur[int(J)])
+                    if B == A or mate[B] >= 0:
+                        continue
+                    s = -v / np.sqrt(dc[A] * dc[B])
+                    if s > 0.0 and (s > best or (s == best and B < bj)):
+                        best, bj = s, B
+            pick[A] = bj
+        for A in range(N):
+            B = pick[A]
+            if mate[A] < 0 and B >= 0 and pick[B] == A:
+                mate[A] = B
     return mate
 
 
-def _coarsen(lv: _Level, mate: np.ndarray, cid: np.ndarray, leaders: np.ndarray) -> _Level:
-    cols, vals = [], []
-    diag = np.zeros(leaders.shape[0])
-    for J, a in enumerate(leaders):
-        b = int(mate[a])
-        sums: dict = {}
-        dacc = lv.diag[a]
-        for node in ((a, b) if b >= 0 else (a,)):
-            if node == b:
-                dacc = dacc + lv.diag[b]
-            for col, v in zip(lv.cols[node], lv.vals[node]):
-                K = int(cid[int(col)])
-                if K == J:
-                    dacc = dacc + v
-                elif K in sums:
-                    sums[K] = sums[K] + v
-                else:
-                    sums[K] = v
-        diag[J] = dacc
-        keys = sorted(sums)
-        cols.append(np.array(keys, np.int64))
-        vals.append(np.array([sums[k] for k in keys], np.float64))
-    return _Level(cols, vals, diag)
+def _diagonals(lv: _Level, cur: np.ndarray, pos: np.ndarray, size: np.ndarray) -> np.ndarray:
+    """dc of the nodes `cur` maps the rows to (positions pos, sizes size)."""
+    R = cur.shape[0]
+    t = np.empty(R)
+    for c in range(R):
+        acc = lv.diag[c]
+        for J, v in zip(lv.cols[c], lv.vals[c]):
+            if cur[int(J)] == cur[c]:
+                acc = acc + v
+        t[c] = acc
+    mem = np.full((size.shape[0], AGG_MAX), -1, np.int64)
+    mem[cur, pos] = np.arange(R)
+    dc = np.empty(size.shape[0])
+    for J in range(size.shape[0]):
+        d = t[mem[J, 0]]
+        for p in range(1, int(size[J])):
+            d = d + t[mem[J, p]]
+        dc[J] = d
+    return dc
 
 
 def aggregate(sx: dict, sy: dict) -> dict:
@@ -116,9 +117,10 @@ def aggregate(sx: dict, sy: dict) -> dict:
     cur = np.arange(R, dtype=np.int64)
     pos = np.zeros(R, np.int64)
     size = np.ones(R, np.int64)
+    dc = lv.diag.copy()
+    N = R
     for level in range(LEVELS):
-        mate = _match(lv)
-        N = lv.diag.shape[0]
+        mate = _match(lv, cur, dc, N)
         idx = np.arange(N)
         leader = (mate < 0) | (idx < mate)
         leaders = idx[leader]
@@ -128,10 +130,11 @@ def aggregate(sx: dict, sy: dict) -> dict:
         second = ~leader
         pos += np.where(second[cur], size[np.maximum(mate[cur], 0)], 0)
         new_size = size[leaders] + np.where(mate[leaders] >= 0, size[np.maximum(mate[leaders], 0)], 0)
-        if level + 1 < LEVELS:
-            lv = _coarsen(lv, mate, cid, leaders)
         cur = cid[cur]
         size = new_size
+        N = leaders.shape[0]
+        if level + 1 < LEVELS:
+            dc = _diagonals(lv, cur, pos, size)
     start = np.concatenate([[0], np.cumsum(size)])
     newpos = start[cur] + pos
     order = np.empty(R, np.int64)
