@@ -536,11 +536,16 @@ __global__ void __launch_bounds__(32 * kPickWarps) k_follow_t(LevelView L, int32
         const unsigned hm = __ballot_sync(0xffffffffu, hit);
         sv_s[w][lane] = v;
         __syncwarp();
-        if (hm != 0u && len > 0) {
-            const int32_t lo = excl > t0 ? excl : t0;
-            const int32_t hi = excl + len < t0 + 32 ? excl + len : t0 + 32;
-            for (int32_t k = lo; k < hi; ++k)
-                if ((hm >> (k - t0)) & 1u) t += sv_s[w][k - t0];
+        // this lane's row occupies chunk positions [lo, hi): its hits, lowest
+        // (earliest stored) first
+        const int32_t lo = excl > t0 ? excl - t0 : 0;
+        const int32_t hi = excl + len < t0 + 32 ? excl + len - t0 : 32;
+        unsigned mine = 0u;
+        if (hi > lo) mine = hm & ((hi - lo == 32 ? 0xffffffffu : ((1u << (hi - lo)) - 1u)) << lo);
+        while (mine) {
+            const int k = __ffs(mine) - 1;
+            t += sv_s[w][k];
+            mine &= mine - 1u;
         }
         __syncwarp();
     }
