@@ -340,13 +340,16 @@ int ktg_batch_autotune(ktg_batch *b, double tol, int precision, double inner_tol
  * with the launch of the batch shape over the rest, whose grid is cut to the
  * SMs left free. Each class drains its own work queue largest first. */
 int ktg_batch_set_split(ktg_batch *b, int64_t rows, int cluster, int threads, int clusters);
-/* The split in force and how many systems it puts in the large class. */
+/* The split in force and how many systems it puts in the large class (of the
+ * systems left in the queues: offloaded pairs are in neither class). */
 int ktg_batch_get_split(const ktg_batch *b, int64_t *rows, int *cluster, int *threads,
                         int *clusters, int *num_large);
 /* Times full solves (iteration cap max_iter) with no split and with splits
- * that move the 1-16 largest systems to 16x1024, 8x1024 or 16x512 clusters
- * (1-8 of them), and keeps the fastest; run it after ktg_batch_autotune.
- * *base_ms: the unsplit time, *best_ms: the kept one. Resets x. */
+ * that move the 1-16 largest queued systems to 16x1024, 8x1024 or 16x512
+ * clusters (1-8 of them), and keeps the fastest; run it after
+ * ktg_batch_autotune and ktg_batch_autotune_offload. *base_ms: the unsplit
+ * time, *best_ms: the kept one (both 0 when every system is offloaded).
+ * Resets x. */
 int ktg_batch_autotune_split(ktg_batch *b, double tol, int precision, double inner_tol,
                              int64_t max_iter, float *base_ms, float *best_ms);
 /* Whole-GPU path for the largest systems: pairs of consecutive systems of

@@ -514,6 +514,27 @@ __global__ void k_offload_results(const ktg_mixed_info *mi, const ktg_solve_info
 
 }  // namespace
 
+// Systems that leave the queues for the whole GPU at the current offload
+// threshold: consecutive systems of equal size (an x/y pair) of at least
+// offload_rows rows, paired from the front.
+static std::vector<char> offloaded(const ktg_batch *b, std::vector<int32_t> *first = nullptr) {
+    const int32_t ns = static_cast<int32_t>(b->sys.size());
+    std::vector<char> off(ns, 0);
+    if (first) first->clear();
+    if (b->offload_rows > 0) {
+        for (int32_t k = 0; k + 1 < ns;) {
+            if (b->sys[k].n >= b->offload_rows && b->sys[k + 1].n == b->sys[k].n) {
+                if (first) first->push_back(k);
+                off[k] = off[k + 1] = 1;
+                k += 2;
+            } else {
+                ++k;
+            }
+        }
+    }
+    return off;
+}
+
 extern "C" {
 
 int ktg_batch_create(int device, ktg_batch **out) {
@@ -709,9 +730,11 @@ int ktg_batch_get_split(const ktg_batch *b, int64_t *rows, int *cluster, int *th
     if (threads) *threads = b->split_threads;
     if (clusters) *clusters = b->split_clusters;
     if (num_large) {
+        // systems of the queues only: offloaded pairs are in no class
+        const std::vector<char> off = offloaded(b);
         int64_t k = 0;
         if (b->split_rows > 0)
-            for (const ktg::SysDesc &d : b->sys) k += d.n >= b->split_rows;
+            for (size_t i = 0; i < b->sys.size(); ++i) k += !off[i] && b->sys[i].n >= b->split_rows;
         *num_large = static_cast<int>(k);
     }
     return KTG_OK;
@@ -896,19 +919,7 @@ int ktg_batch_solve(ktg_batch *b, double tol, int64_t max_iter, int precision, d
         // Offloaded pairs first leave the queues; then largest first within
         // each class, the large class (rows >= split_rows) at the front.
         const int32_t ns = static_cast<int32_t>(b->sys.size());
-        std::vector<char> off(ns, 0);
-        b->off_first.clear();
-        if (b->offload_rows > 0) {
-            for (int32_t k = 0; k + 1 < ns;) {
-                if (b->sys[k].n >= b->offload_rows && b->sys[k + 1].n == b->sys[k].n) {
-                    b->off_first.push_back(k);
-                    off[k] = off[k + 1] = 1;
-                    k += 2;
-                } else {
-                    ++k;
-                }
-            }
-        }
+        const std::vector<char> off = offloaded(b, &b->off_first);
         std::vector<int32_t> order;
         for (int32_t k = 0; k < ns; ++k)
             if (!off[k]) order.push_back(k);
@@ -1071,10 +1082,17 @@ int ktg_batch_autotune_split(ktg_batch *b, double tol, int precision, double inn
                              int64_t max_iter, float *base_ms, float *best_ms) {
     if (!b || max_iter <= 0) return KTG_ERR_ARG;
     if (b->sys.empty()) return berr(b, KTG_ERR_STATE, "empty batch");
-    // Thresholds that put the 1, 2, 4, 8 or 16 largest systems (ties
-    // included) in the large class.
+    // Thresholds that put the 1, 2, 4, 8 or 16 largest queued systems (ties
+    // included) in the large class; offloaded pairs are in no class.
     std::vector<int64_t> sizes;
-    for (const ktg::SysDesc &d : b->sys) sizes.push_back(d.n);
+    const std::vector<char> off = offloaded(b);
+    for (size_t i = 0; i < b->sys.size(); ++i)
+        if (!off[i]) sizes.push_back(b->sys[i].n);
+    if (sizes.empty()) {  // every system is offloaded: nothing to split
+        if (base_ms) *base_ms = 0.0f;
+        if (best_ms) *best_ms = 0.0f;
+        return ktg_batch_set_split(b, 0, 0, 0, 0);
+    }
     std::sort(sizes.begin(), sizes.end(), std::greater<int64_t>());
     std::vector<int64_t> cuts;
     for (size_t k : {1, 2, 4, 8, 16}) {

@@ -214,6 +214,50 @@ def test_batch_offload_matches_oracle(systems, rows):
     b.close()
 
 
+def offloaded_ids(sizes, thr):
+    """Systems the whole-GPU path takes at threshold thr: equal-size
+    consecutive pairs of >= thr rows, paired from the front."""
+    out, k = set(), 0
+    while k + 1 < len(sizes):
+        if sizes[k] >= thr and sizes[k + 1] == sizes[k]:
+            out |= {k, k + 1}
+            k += 2
+        else:
+            k += 1
+    return out
+
+
+def test_batch_split_counts_queued_systems(systems):
+    """With pairs on the whole GPU the size split covers only the systems left
+    in the queues (its count and the autotuner's thresholds); with every
+    system offloaded the autotuner keeps no split. Every system still meets
+    the tolerance on its true residual."""
+    b, ids = make_batch(systems)
+    sizes = [s["diag"].shape[0] for s, _ in systems]
+    thr = max(sizes)
+    b.set_offload(thr, precond=2, coarse=0)
+    off = offloaded_ids(sizes, thr)
+    assert b.offload()["pairs"] == len(off) // 2 >= 1
+    b.set_split(1, 8, 512, 1)
+    assert b.split()["num_large"] == len(sizes) - len(off)
+    b.set_split(0)
+    sp, base, best = b.autotune_split(TOL, precision=1, inner_tol=1e-3, max_iter=MAX_ITER)
+    assert 0 < best <= base
+    queued = [n for k, n in enumerate(sizes) if k not in off]
+    assert sp["rows"] == 0 or (sp["rows"] in queued and sp["num_large"] >= 1)
+    b.solve(TOL, MAX_ITER, precision=1, inner_tol=1e-3)
+    for (s, _), r, sid in zip(systems, b.results(), ids):
+        assert r["status"] == 0 and true_resid(s, b.get_x(sid, s["diag"].shape[0])) <= TOL * 1.0001
+    if len(offloaded_ids(sizes, 1)) == len(sizes):
+        b.set_offload(1, precond=2, coarse=0)
+        sp, base, best = b.autotune_split(TOL, precision=1, inner_tol=1e-3, max_iter=MAX_ITER)
+        assert sp["rows"] == 0 and base == 0.0 and best == 0.0
+        b.solve(TOL, MAX_ITER, precision=1, inner_tol=1e-3)
+        for (s, _), r, sid in zip(systems, b.results(), ids):
+            assert r["status"] == 0
+    b.close()
+
+
 def test_batch_autotune_offload(systems):
     b, ids = make_batch(systems)
     off, base, best = b.autotune_offload(TOL, precision=1, inner_tol=1e-3, max_iter=MAX_ITER)
