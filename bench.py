@@ -97,6 +97,11 @@ def parse():
                          "the committed ktplace_b200/weights/learned_coarse.npy)")
     ap.add_argument("--no-simpl-report", action="store_true",
                     help="skip the 30-iteration SimPL study in the default run")
+    ap.add_argument("--profile-dense", action="store_true",
+                    help="only the learned network's forward pass (ktg_learned_prepare: "
+                         "features, the 3-layer message-passing trunk, the head) on the 211k "
+                         "design with each dense-layer engine (tcgen05, mma.sync, FP32 cores); "
+                         "prints one JSON line")
     ap.add_argument("--profile-once", action="store_true",
                     help="run the workload once (build, FP64 and mixed solves, HPWL, "
                          "density) for an ncu capture; prints no bench line")
@@ -1037,6 +1042,44 @@ def profile_agg():
     return 0
 
 
+def profile_dense(reps: int = 5) -> int:
+    """The learned network's forward pass on the 211k-cell workload's x and
+    y systems with each dense-layer engine: tensor_cores 2 (tcgen05.mma, FP32
+    accumulator in tensor memory), 1 (mma.sync) and 0 (FP32 CUDA cores).
+    Times are host wall clock around ktg_learned_prepare (features, trunk and
+    head for both axes; it synchronises its streams before returning), median
+    of `reps` after one warm-up; the dense layers' FLOPs are 2 x rows x K x
+    OUT summed over the trunk's layers and both axes."""
+    import torch
+    from ktplace_b200.gpu import Context
+    from ktplace_b200.learned import Learned
+    raw, nl, x, y, ax, ay = make_workload(1)
+    fx, fy = nl.floors()
+    ctx = Context(0)
+    ctx.upload_netlist(nl)
+    ctx.build_b2b(x, y, ALPHA, ax, ay, fx, fy)
+    n, N = nl.num_movable, len(nl.net_start) - 1
+    hid, proj = 64, 16
+    flops = 2 * 2.0 * (n * 16 * hid + 3 * (N * hid * hid + n * 2 * hid * hid) + n * hid * proj)
+    learned = Learned(0, seed=1)
+    out = {"workload": "learned network forward (features, 3-layer trunk, head) on synth211k",
+           "cells": n, "nets": N, "dense_gflop": flops / 1e9}
+    for mode, name in ((2, "tcgen05"), (1, "mma_sync"), (0, "fp32_cores")):
+        learned.set_option("tensor_cores", mode)
+        learned.prepare(ctx)
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            learned.prepare(ctx)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        out[name + "_ms"] = float(np.median(ts))
+    learned.close()
+    ctx.close()
+    print(json.dumps(out))
+    return 0
+
+
 def profile_lal():
     """The capture workload of the legalizer profiles: one B2B build and
     FP64 PCG solve of the 211k-cell workload from its seed positions, then
@@ -1255,6 +1298,8 @@ def main():
         return run_simpl_report(args.simpl_report, args.coarse_weights)
     if args.profile_once:
         return profile_once()
+    if args.profile_dense:
+        return profile_dense()
     if args.profile_lal:
         return profile_lal()
     if args.profile_agg:

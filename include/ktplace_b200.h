@@ -396,7 +396,10 @@ int64_t ktg_learned_num_params(void);
 int ktg_learned_create(int device, uint64_t seed, ktg_learned **out);
 void ktg_learned_destroy(ktg_learned *h);
 const char *ktg_learned_last_error(const ktg_learned *h);
-/* "tensor_cores" (1: BF16 mma, 0: FP32 CUDA cores), "lr", "probes", "clip". */
+/* "tensor_cores" (2: BF16 tcgen05.mma with the accumulator in tensor memory,
+ * the default; 1: BF16 mma.sync; 0: FP32 CUDA cores), "tc_ctas" (cap on the
+ * tcgen05 layers' persistent CTAs, each walking 128-row tiles; 0 = four per
+ * SM), "lr", "probes", "clip". */
 int ktg_learned_set_option(ktg_learned *h, const char *key, double value);
 /* FP32 parameters in the layout of oracle/learned_ref.py (host memory). */
 int ktg_learned_get_params(ktg_learned *h, float *out);

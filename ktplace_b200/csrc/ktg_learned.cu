@@ -15,8 +15,9 @@
 //              g = mean_nets->cell(e), h = relu(h Wb + g Wc + bb)
 //   p = h P
 // Dense layers keep FP32 master weights and use BF16 copies on the tensor
-// cores (mma.sync m16n8k16, FP32 accumulation); an FP32 CUDA-core path of
-// the same kernels exists for gradient checks. Training minimises
+// cores: tcgen05.mma with the FP32 accumulator in tensor memory (default),
+// or the older warp-level mma.sync m16n8k16; an FP32 CUDA-core path of the
+// same layers exists for gradient checks. Training minimises
 //   L = mean over K Rademacher probes v of ||M A v - v||^2 / n
 // on systems the GPU SimPL loop produces. Every reduction (weight gradients,
 // loss) runs in a fixed order, so training is reproducible run to run.
@@ -317,6 +318,240 @@ __global__ void __launch_bounds__(128) k_dense_tc(DenseArgs A) {
             o[1] = v[3];
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// The same layer on the 5th-generation tensor cores (tcgen05.mma, sm_100a).
+//
+// A persistent CTA of four warps stages the weights once as the MMA's B
+// operand (OUT x K, K-major, BF16) and then walks 128-row tiles: the threads
+// convert the tile's rows of X1 (masked) and X2 to BF16 in shared memory (A
+// operand, 128 x K, K-major), one thread issues K/16 tcgen05.mma (kind::f16,
+// M = 128, N = OUT, FP32 accumulator in tensor memory) and commits them to an
+// mbarrier, and each warp reads its 32 accumulator lanes (= rows) back with
+// tcgen05.ld for the bias / ReLU / accumulate epilogue. K = kpad(K1) + 64 when
+// X2 is present (at most 128), so one tile is at most eight MMAs.
+// Operand layout (no swizzle, K-major): 8 x 8 core matrices of 16-byte rows;
+// element (r, k) sits at (r / 8) * SBO + (k / 8) * 128 + (r % 8) * 16 +
+// (k % 8) * 2 bytes, SBO = (K / 8) * 128 (the descriptor's leading offset is
+// the 128-byte step to the next 8 k, its stride offset SBO the step to the
+// next 8 rows).
+// ---------------------------------------------------------------------------
+constexpr int kUmmaM = 128;
+constexpr int kUmmaKMax = 128;
+constexpr int kUmmaNMax = 64;
+constexpr uint32_t kUmmaTmemCols = 64;  // power of two >= 32, >= OUT
+constexpr int kUmmaSmemA = kUmmaM * kUmmaKMax * 2;     // 32 KiB
+constexpr int kUmmaSmemB = kUmmaNMax * kUmmaKMax * 2;  // 16 KiB
+// 49 KiB of dynamic shared memory per CTA: at most four CTAs fit on an SM
+// (228 KiB), so at most 4 x 64 of its 512 tensor-memory columns are held at
+// once and tcgen05.alloc never waits on another CTA.
+constexpr int kUmmaSmem = kUmmaSmemA + kUmmaSmemB + 1024;
+constexpr int kUmmaCtasPerSm = 4;
+constexpr uint64_t kUmmaWaitNs = 200ull * 1000 * 1000;  // bound on one tile's MMA wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: start, leading and stride byte offsets
+// (each >> 4), descriptor version 1 (sm_100), no swizzle, base offset 0.
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) |
+           (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16
+// A and B (bits 7-9 and 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at
+// bit 24.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+           (static_cast<uint32_t>(kUmmaM >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t core_offset(int r, int k, int sbo) {
+    return static_cast<uint32_t>((r >> 3) * sbo + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Bounded wait for an mbarrier phase; false when the bound ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t t0 = ktg::global_timer_ns();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+        if (ktg::global_timer_ns() - t0 > limit_ns) return false;
+    }
+}
+
+struct UmmaArgs {
+    DenseArgs d;
+    int *status;  // set to 1 when a tile's MMA wait ran out (the layer's output is then invalid)
+};
+
+__global__ void __launch_bounds__(128) k_dense_umma(UmmaArgs U) {
+    const DenseArgs &A = U.d;
+    extern __shared__ __align__(1024) uint8_t umma_smem[];
+    uint8_t *sa = umma_smem;
+    uint8_t *sb = umma_smem + kUmmaSmemA;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ float bias_s[kUmmaNMax];
+    __shared__ int abort_s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kp1 = (A.k + 15) & ~15;
+    const int kt = kp1 + (A.x2 ? 64 : 0);
+    const int sbo = (kt / 8) * 128;
+    const int out = A.out;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_base_s)), "r"(kUmmaTmemCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        abort_s = 0;
+    }
+    // B operand: B[n][k] = W1[k][n] for k < kp1 (zero past K1), W2[k - kp1][n] after
+    for (int idx = threadIdx.x; idx < out * kt; idx += blockDim.x) {
+        const int nn = idx / kt, kk = idx - nn * kt;
+        __nv_bfloat16 v = __float2bfloat16(0.0f);
+        if (kk < kp1) {
+            if (kk < A.k) v = A.transpose ? A.w1h[nn * A.k + kk] : A.w1h[kk * out + nn];
+        } else {
+            const int k2 = kk - kp1;
+            v = A.transpose ? A.w2h[nn * 64 + k2] : A.w2h[k2 * out + nn];
+        }
+        *reinterpret_cast<__nv_bfloat16 *>(sb + core_offset(nn, kk, sbo)) = v;
+    }
+    for (int c = threadIdx.x; c < out; c += blockDim.x) bias_s[c] = A.bias ? A.bias[c] : 0.0f;
+
+    const int64_t tiles = (static_cast<int64_t>(A.rows) + kUmmaM - 1) / kUmmaM;
+    const int chunks = kt / 8;  // 16-byte rows of 8 k per operand row
+    const uint32_t idesc = umma_idesc_bf16(out);
+    uint32_t phase = 0;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t row0 = tile * kUmmaM;
+        // A operand: rows of X1 (masked, zero past K1) then X2, as BF16
+        for (int idx = threadIdx.x; idx < kUmmaM * chunks; idx += blockDim.x) {
+            const int r = idx / chunks, kc = idx - r * chunks;
+            const int64_t row = row0 + r;
+            float v[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+            if (row < A.rows) {
+                const int k0 = kc * 8;
+                if (k0 < kp1) {
+                    if (k0 < A.k) {  // K1 is a multiple of 8: the chunk lies inside X1
+                        const float4 *src = reinterpret_cast<const float4 *>(A.x1 + row * A.k + k0);
+                        const float4 a = __ldg(src), b = __ldg(src + 1);
+                        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+                        v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+                        if (A.mask) {
+                            const float4 *ms = reinterpret_cast<const float4 *>(A.mask + row * A.k + k0);
+                            const float4 ma = __ldg(ms), mb = __ldg(ms + 1);
+                            const float mv[8] = {ma.x, ma.y, ma.z, ma.w, mb.x, mb.y, mb.z, mb.w};
+#pragma unroll
+                            for (int q = 0; q < 8; ++q)
+                                if (!(mv[q] > 0.0f)) v[q] = 0.0f;
+                        }
+                    }
+                } else {
+                    const float4 *src =
+                        reinterpret_cast<const float4 *>(A.x2 + row * 64 + (k0 - kp1));
+                    const float4 a = __ldg(src), b = __ldg(src + 1);
+                    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+                    v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+                }
+            }
+            uint4 pk;
+            pk.x = pack_bf16(v[0], v[1]);
+            pk.y = pack_bf16(v[2], v[3]);
+            pk.z = pack_bf16(v[4], v[5]);
+            pk.w = pack_bf16(v[6], v[7]);
+            *reinterpret_cast<uint4 *>(sa + core_offset(r, kc * 8, sbo)) = pk;
+        }
+        // shared-memory writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        const uint32_t tmem = tmem_base_s;
+        if (threadIdx.x == 0) {
+            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+            for (int ks = 0; ks < kt / 16; ++ks) {
+                const uint64_t ad = umma_smem_desc(a0 + ks * 256, 128, sbo);
+                const uint64_t bd = umma_smem_desc(b0 + ks * 256, 128, sbo);
+                const uint32_t acc = ks > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                :: "r"(smem_u32(&mbar)) : "memory");
+        }
+        if (!mbar_wait_bounded(smem_u32(&mbar), phase, kUmmaWaitNs)) abort_s = 1;
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();
+        if (abort_s) break;
+        // epilogue: warp w reads accumulator lanes 32 w .. 32 w + 31 (its rows)
+        const int64_t row = row0 + warp * 32 + lane;
+        for (int c0 = 0; c0 < out; c0 += 16) {
+            uint32_t rg[16];
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(rg[0]), "=r"(rg[1]), "=r"(rg[2]), "=r"(rg[3]), "=r"(rg[4]), "=r"(rg[5]),
+                  "=r"(rg[6]), "=r"(rg[7]), "=r"(rg[8]), "=r"(rg[9]), "=r"(rg[10]), "=r"(rg[11]),
+                  "=r"(rg[12]), "=r"(rg[13]), "=r"(rg[14]), "=r"(rg[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < A.rows) {
+                float v[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    v[q] = __uint_as_float(rg[q]) + bias_s[c0 + q];
+                    if (A.relu) v[q] = v[q] > 0.0f ? v[q] : 0.0f;
+                }
+                float4 *dst = reinterpret_cast<float4 *>(A.y + row * out + c0);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    float4 o = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    if (A.accumulate) {
+                        const float4 p = dst[q];
+                        o.x += p.x, o.y += p.y, o.z += p.z, o.w += p.w;
+                    }
+                    dst[q] = o;
+                }
+            }
+        }
+        // every warp's reads of the accumulator end before the next tile's MMA
+        tc_fence_before();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (abort_s && threadIdx.x == 0) atomicExch(U.status, 1);
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem_base_s), "r"(kUmmaTmemCols) : "memory");
 }
 
 // FP32 CUDA-core path of the same operation (one thread per output element).
@@ -808,7 +1043,13 @@ struct ktg_learned {
     float *w = nullptr, *g = nullptr, *m1 = nullptr, *m2 = nullptr;
     __nv_bfloat16 *wh = nullptr;
     int64_t step = 0;
-    bool tensor_cores = true;
+    // dense layers: 2 tcgen05 (BF16 operands in shared memory, FP32
+    // accumulator in tensor memory), 1 BF16 mma.sync, 0 FP32 CUDA cores
+    int tensor_cores = 2;
+    int num_sms = 148;
+    int tc_ctas = 0;           // cap on the tcgen05 layers' persistent CTAs (0: 4 per SM)
+    int *tc_status = nullptr;  // set by a tcgen05 layer whose MMA wait ran out
+    bool umma_used = false;
     float lr = 1e-3f;
     int probes = 4;
     float clip = 1.0f;
@@ -938,7 +1179,19 @@ int dense(ktg_learned *h, const float *x1, int k, const float *x2, int64_t w1, i
     A.relu = relu;
     A.transpose = transpose;
     A.accumulate = accumulate;
-    if (h->tensor_cores) {
+    auto aligned16 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    const bool umma_ok = h->tensor_cores == 2 && k % 8 == 0 && k <= 64 && out % 16 == 0 &&
+                         out <= ktg::learned::kUmmaNMax && aligned16(x1) && aligned16(y) &&
+                         (!x2 || aligned16(x2)) && (!mask || aligned16(mask));
+    if (umma_ok) {
+        const int64_t tiles = (rows + ktg::learned::kUmmaM - 1) / ktg::learned::kUmmaM;
+        int64_t cap = static_cast<int64_t>(h->num_sms) * ktg::learned::kUmmaCtasPerSm;
+        if (h->tc_ctas > 0) cap = std::min<int64_t>(cap, h->tc_ctas);
+        const int blocks = static_cast<int>(std::min<int64_t>(tiles, cap));
+        ktg::learned::UmmaArgs U{A, h->tc_status};
+        ktg::learned::k_dense_umma<<<blocks, 128, ktg::learned::kUmmaSmem, h->stream>>>(U);
+        h->umma_used = true;
+    } else if (h->tensor_cores) {
         const int blocks = static_cast<int>((rows + 63) / 64);
         ktg::learned::k_dense_tc<64, 64><<<blocks, 128, 0, h->stream>>>(A);
     } else {
@@ -966,6 +1219,21 @@ int wgrad(ktg_learned *h, const float *x, int k, const float *dy, const float *y
 
 // The trunk (message passing over the cell-net graph) from the features in
 // h->x to the embedding p = h3 P in h->p.
+// Reads the status word of the tcgen05 layers launched since the last check
+// (one stream synchronisation; nothing when none ran).
+int tc_check(ktg_learned *h) {
+    if (!h->umma_used) return KTG_OK;
+    h->umma_used = false;
+    int st = 0;
+    KTG_LCUDA(h, cudaMemcpyAsync(&st, h->tc_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
+    if (st != 0) {
+        cudaMemsetAsync(h->tc_status, 0, sizeof(int), h->stream);
+        return lerr(h, KTG_ERR_TIMEOUT, "tensor-core dense layer: MMA completion wait ran out");
+    }
+    return KTG_OK;
+}
+
 int trunk_forward(ktg_learned *h, ktg_ctx *c, int64_t n) {
     int rc;
     const int64_t N = c->N;
@@ -992,7 +1260,7 @@ int trunk_forward(ktg_learned *h, ktg_ctx *c, int64_t n) {
                     false, nullptr)))
         return rc;
     KTG_LCUDA(h, cudaGetLastError());
-    return KTG_OK;
+    return tc_check(h);
 }
 
 // Forward pass to p and the entry values (t, s) of one axis system (the
@@ -1055,7 +1323,7 @@ int loss_grad(ktg_learned *h, ktg_ctx *c, int axis, uint64_t seed, double *loss)
     KTG_LCUDA(h, cudaStreamSynchronize(h->stream));
     l = h->h_scal[0];
     if (loss) *loss = l;
-    return KTG_OK;
+    return tc_check(h);
 }
 
 // Gradients of the trunk's parameters from dL/dp in h->dp (accumulated into
@@ -1259,6 +1527,7 @@ int ktg_learned_create(int device, uint64_t seed, ktg_learned **out) {
         lalloc(h, &h->m2, P) || lalloc(h, &h->wh, P) ||
         lalloc(h, &h->wpart, static_cast<int64_t>(kWgradBlocks) * (HID * HID + HID)) ||
         lalloc(h, &h->dpart, 8192) || lalloc(h, &h->ticket, 1) || lalloc(h, &h->scal, 4) ||
+        lalloc(h, &h->tc_status, 1) ||
         cudaMallocHost(&h->h_scal, 4 * sizeof(double)) != cudaSuccess) {
         ktg_learned_destroy(h);
         return KTG_ERR_NOMEM;
@@ -1295,6 +1564,10 @@ int ktg_learned_create(int device, uint64_t seed, ktg_learned **out) {
         cudaMemsetAsync(h->m1, 0, sizeof(float) * P, h->stream) != cudaSuccess ||
         cudaMemsetAsync(h->m2, 0, sizeof(float) * P, h->stream) != cudaSuccess ||
         cudaMemsetAsync(h->ticket, 0, sizeof(unsigned), h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->tc_status, 0, sizeof(int), h->stream) != cudaSuccess ||
+        cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaFuncSetAttribute(ktg::learned::k_dense_umma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             ktg::learned::kUmmaSmem) != cudaSuccess ||
         refresh_bf16(h) != KTG_OK ||
         cudaStreamSynchronize(h->stream) != cudaSuccess) {
         ktg_learned_destroy(h);
@@ -1310,7 +1583,7 @@ void ktg_learned_destroy(ktg_learned *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->w, h->g, h->m1, h->m2, h->wh, h->x, h->act_c, h->act_n, h->p, h->dp,
                     h->dh, h->dh2, h->dg, h->dm, h->de, h->t, h->ds, h->dphi, h->tr, h->u,
-                    h->gq, h->wpart, h->dpart, h->ticket, h->scal, h->cu, h->chh, h->co,
+                    h->gq, h->wpart, h->dpart, h->ticket, h->scal, h->tc_status, h->cu, h->chh, h->co,
                     h->cdz, h->cdhh, h->cdo, h->czd, h->caz, h->ce, h->ca, h->cscal};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -1324,7 +1597,9 @@ const char *ktg_learned_last_error(const ktg_learned *h) { return h ? h->err.c_s
 int ktg_learned_set_option(ktg_learned *h, const char *key, double value) {
     if (!h || !key) return KTG_ERR_ARG;
     const std::string k(key);
-    if (k == "tensor_cores") h->tensor_cores = value != 0.0;
+    if (k == "tensor_cores" && (value == 0 || value == 1 || value == 2))
+        h->tensor_cores = static_cast<int>(value);
+    else if (k == "tc_ctas" && value >= 0 && value <= 1 << 20) h->tc_ctas = static_cast<int>(value);
     else if (k == "lr") h->lr = static_cast<float>(value);
     else if (k == "probes" && value >= 1 && value <= 64) h->probes = static_cast<int>(value);
     else if (k == "clip" && value > 0) h->clip = static_cast<float>(value);

@@ -3,7 +3,8 @@
 // Each warp takes 32 consecutive rows of its block and streams their
 // (contiguous) nonzeros in chunks of kTileChunk, every lane loading
 // consecutive entries: coalesced column and value loads and kTileQ
-// independent gathers in flight per lane. The products go to the warp's
+// independent gathers in flight per lane (FP32 tiles issue the next chunk's
+// column loads behind them). The products go to the warp's
 // slice of shared memory and each lane adds its own row's products in
 // storage order onto the row's first term, carrying the running sum across
 // chunks, so every row sum is the same sequence of roundings as a
@@ -113,20 +114,31 @@ __device__ __forceinline__ void warp_tile_spmv(int32_t r0, int32_t n0, int32_t R
             // [rs of the first, re of the last)
             const int32_t k_begin = __shfl_sync(0xffffffffu, rs, __ffs(m) - 1);
             const int32_t k_end = __shfl_sync(0xffffffffu, re, 31 - __clz(m));
-#pragma unroll 1
-            for (int32_t k0 = k_begin; k0 < k_end; k0 += kTileChunk) {
-                int32_t cl[kTileQ];
+            int32_t cl[kTileQ];
+            auto load_cols = [&](int32_t kb) {
 #pragma unroll
                 for (int q = 0; q < kTileQ; ++q) {
-                    const int32_t k = k0 + lane + 32 * q;
+                    const int32_t k = kb + lane + 32 * q;
                     cl[q] = k < k_end ? __ldg(col + k) : -1;
                 }
+            };
+            // FP32 tiles load the next chunk's columns while the chunk's own
+            // gathers are in flight (one memory round trip per chunk instead
+            // of two; 3% off the FP32 solves at 211k cells). The FP64 tiles
+            // keep the plain order: with their 8-byte products the extra
+            // registers cost the register-capped FP64 solve about as much.
+            constexpr bool kAhead = sizeof(T) == 4;
+            if (kAhead) load_cols(k_begin);
+#pragma unroll 1
+            for (int32_t k0 = k_begin; k0 < k_end; k0 += kTileChunk) {
+                if (!kAhead) load_cols(k0);
                 T pr[kTileQ];
 #pragma unroll
                 for (int q = 0; q < kTileQ; ++q) {
                     const int32_t k = k0 + lane + 32 * q;
                     pr[q] = cl[q] >= 0 ? __ldg(val + k) * __ldcg(in + cl[q]) : T(0);
                 }
+                if (kAhead) load_cols(k0 + kTileChunk);
 #pragma unroll
                 for (int q = 0; q < kTileQ; ++q) buf[lane + 32 * q] = pr[q];
                 __syncwarp();

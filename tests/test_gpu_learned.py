@@ -66,6 +66,42 @@ def test_gradients_match_cpu_oracle(tiny, gpu_ctx):
     learned.close()
 
 
+def test_tcgen05_dense_layers_match_mma_sync(tiny, gpu_ctx):
+    """The tcgen05 dense layers (BF16 operands, FP32 accumulator in tensor
+    memory) against the warp-level mma.sync layers on the same BF16 weights:
+    forward, transposed and masked backward layers through the loss and its
+    gradient. One CTA walking all 128-row tiles (mbarrier phases alternating,
+    accumulator reused) gives the same bits as one CTA per tile."""
+    from ktplace_b200.learned import Learned
+    raw, nl, x, y, ax, ay, alpha = tiny
+    gpu_ctx.upload_netlist(nl)
+    fx, fy = nl.floors()
+    gpu_ctx.build_b2b(x, y, alpha, ax, ay, fx, fy)
+    params = lr.init_params(5)
+    params["P"] *= 20.0
+    learned = Learned(0, seed=2)
+    learned.set_params(lr.flatten(params).astype(np.float32))
+    learned.set_option("probes", 2)
+    out = {}
+    for mode, ctas in ((1, 0), (2, 0), (2, 1), (0, 0)):
+        learned.set_option("tensor_cores", mode)
+        learned.set_option("tc_ctas", ctas)
+        out[(mode, ctas)] = learned.loss_grad(gpu_ctx, 0, seed=5)
+    L2, g2 = out[(2, 0)]
+    L2b, g2b = out[(2, 1)]
+    L1, g1 = out[(1, 0)]
+    L0, g0 = out[(0, 0)]
+    assert nl.num_movable > 128 and nl.num_movable % 128  # several tiles, the last partial
+    assert L2b == L2 and np.array_equal(g2b, g2)
+    assert np.isfinite(L2) and np.all(np.isfinite(g2))
+    # same BF16 products, FP32 sums in another order
+    assert abs(L2 - L1) <= 1e-4 * abs(L1)
+    assert rel(g2, g1) <= 1e-3
+    assert abs(L2 - L0) <= 3e-2 * abs(L0)
+    assert rel(g2, g0) <= 3e-2
+    learned.close()
+
+
 def test_learned_preconditioner_solves_exactly(tiny, gpu_ctx):
     from ktplace_b200.learned import Learned
     raw, nl, x, y, ax, ay, alpha = tiny
