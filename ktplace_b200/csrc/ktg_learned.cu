@@ -323,13 +323,14 @@ __global__ void __launch_bounds__(128) k_dense_tc(DenseArgs A) {
 // ---------------------------------------------------------------------------
 // The same layer on the 5th-generation tensor cores (tcgen05.mma, sm_100a).
 //
-// A persistent CTA of four warps stages the weights once as the MMA's B
+// A persistent CTA of eight warps stages the weights once as the MMA's B
 // operand (OUT x K, K-major, BF16) and then walks 128-row tiles: the threads
 // convert the tile's rows of X1 (masked) and X2 to BF16 in shared memory (A
 // operand, 128 x K, K-major), one thread issues K/16 tcgen05.mma (kind::f16,
 // M = 128, N = OUT, FP32 accumulator in tensor memory) and commits them to an
-// mbarrier, and each warp reads its 32 accumulator lanes (= rows) back with
-// tcgen05.ld for the bias / ReLU / accumulate epilogue. K = kpad(K1) + 64 when
+// mbarrier, and warps w and w + 4 read accumulator lanes 32 w .. 32 w + 31
+// (= rows), alternate 16-column chunks each, back with tcgen05.ld for the
+// bias / ReLU / accumulate epilogue. K = kpad(K1) + 64 when
 // X2 is present (at most 128), so one tile is at most eight MMAs.
 // Operand layout (no swizzle, K-major): 8 x 8 core matrices of 16-byte rows;
 // element (r, k) sits at (r / 8) * SBO + (k / 8) * 128 + (r % 8) * 16 +
@@ -343,10 +344,15 @@ constexpr int kUmmaNMax = 64;
 constexpr uint32_t kUmmaTmemCols = 64;  // power of two >= 32, >= OUT
 constexpr int kUmmaSmemA = kUmmaM * kUmmaKMax * 2;     // 32 KiB
 constexpr int kUmmaSmemB = kUmmaNMax * kUmmaKMax * 2;  // 16 KiB
-// 49 KiB of dynamic shared memory per CTA: at most four CTAs fit on an SM
-// (228 KiB), so at most 4 x 64 of its 512 tensor-memory columns are held at
-// once and tcgen05.alloc never waits on another CTA.
+// Eight warps per CTA and a grid of four CTAs per SM. Dynamic shared memory
+// per CTA bounds how many CTAs can share an SM (228 KiB), and with it the
+// tensor memory they hold (64 of the SM's 512 columns each), so that
+// tcgen05.alloc never waits on another CTA: layers with K <= 64 take 26 KiB
+// (at most eight CTAs, 8 x 64 columns), layers with K = 128 49 KiB (at most
+// four).
+constexpr int kUmmaThreads = 256;
 constexpr int kUmmaSmem = kUmmaSmemA + kUmmaSmemB + 1024;
+constexpr int kUmmaSmemSmall = 26 * 1024;
 constexpr int kUmmaCtasPerSm = 4;
 constexpr uint64_t kUmmaWaitNs = 200ull * 1000 * 1000;  // bound on one tile's MMA wait
 
@@ -401,11 +407,11 @@ struct UmmaArgs {
     int *status;  // set to 1 when a tile's MMA wait ran out (the layer's output is then invalid)
 };
 
-__global__ void __launch_bounds__(128) k_dense_umma(UmmaArgs U) {
+__global__ void __launch_bounds__(kUmmaThreads, kUmmaCtasPerSm) k_dense_umma(UmmaArgs U) {
     const DenseArgs &A = U.d;
     extern __shared__ __align__(1024) uint8_t umma_smem[];
     uint8_t *sa = umma_smem;
-    uint8_t *sb = umma_smem + kUmmaSmemA;
+    uint8_t *sb;
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base_s;
     __shared__ float bias_s[kUmmaNMax];
@@ -415,6 +421,7 @@ __global__ void __launch_bounds__(128) k_dense_umma(UmmaArgs U) {
     const int kt = kp1 + (A.x2 ? 64 : 0);
     const int sbo = (kt / 8) * 128;
     const int out = A.out;
+    sb = sa + kUmmaM * kt * 2;  // B follows the 128 x K A tile
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -428,7 +435,15 @@ __global__ void __launch_bounds__(128) k_dense_umma(UmmaArgs U) {
     }
     // B operand: B[n][k] = W1[k][n] for k < kp1 (zero past K1), W2[k - kp1][n] after
     for (int idx = threadIdx.x; idx < out * kt; idx += blockDim.x) {
-        const int nn = idx / kt, kk = idx - nn * kt;
+        // consecutive threads read consecutive weights ([OUT x K] or [K x OUT])
+        int nn, kk;
+        if (A.transpose) {
+            nn = idx / kt;
+            kk = idx - nn * kt;
+        } else {
+            kk = idx / out;
+            nn = idx - kk * out;
+        }
         __nv_bfloat16 v = __float2bfloat16(0.0f);
         if (kk < kp1) {
             if (kk < A.k) v = A.transpose ? A.w1h[nn * A.k + kk] : A.w1h[kk * out + nn];
@@ -510,11 +525,14 @@ __global__ void __launch_bounds__(128) k_dense_umma(UmmaArgs U) {
         tc_fence_after();
         __syncthreads();
         if (abort_s) break;
-        // epilogue: warp w reads accumulator lanes 32 w .. 32 w + 31 (its rows)
-        const int64_t row = row0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < out; c0 += 16) {
+        // epilogue: warp w reads accumulator lanes 32 (w % 4) .. + 31 (its
+        // rows); with eight warps, warps 4-7 take every other 16 columns
+        const int quad = warp & 3;
+        const int64_t row = row0 + quad * 32 + lane;
+        const int cstep = 16 * static_cast<int>(blockDim.x >> 7);
+        for (int c0 = 16 * (warp >> 2); c0 < out; c0 += cstep) {
             uint32_t rg[16];
-            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0;
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + c0;
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
@@ -1185,11 +1203,14 @@ int dense(ktg_learned *h, const float *x1, int k, const float *x2, int64_t w1, i
                          (!x2 || aligned16(x2)) && (!mask || aligned16(mask));
     if (umma_ok) {
         const int64_t tiles = (rows + ktg::learned::kUmmaM - 1) / ktg::learned::kUmmaM;
+        const int kt = ((k + 15) & ~15) + (x2 ? 64 : 0);
+        const bool small = ktg::learned::kUmmaM * kt * 2 + out * kt * 2 <= ktg::learned::kUmmaSmemSmall;
+        const int smem = small ? ktg::learned::kUmmaSmemSmall : ktg::learned::kUmmaSmem;
         int64_t cap = static_cast<int64_t>(h->num_sms) * ktg::learned::kUmmaCtasPerSm;
         if (h->tc_ctas > 0) cap = std::min<int64_t>(cap, h->tc_ctas);
         const int blocks = static_cast<int>(std::min<int64_t>(tiles, cap));
         ktg::learned::UmmaArgs U{A, h->tc_status};
-        ktg::learned::k_dense_umma<<<blocks, 128, ktg::learned::kUmmaSmem, h->stream>>>(U);
+        ktg::learned::k_dense_umma<<<blocks, ktg::learned::kUmmaThreads, smem, h->stream>>>(U);
         h->umma_used = true;
     } else if (h->tensor_cores) {
         const int blocks = static_cast<int>((rows + 63) / 64);
