@@ -904,7 +904,7 @@ __global__ void __launch_bounds__(kAzThreads)
     });
     double e[2] = {0.0, 0.0};
     warp_tile_spmv<double>(
-        r0, n, R, nullptr, wb, tilebuf,
+        r0, n, R, kAllAxes, wb, tilebuf,
         [&](int pass, const int32_t *&trp, const int32_t *&tcol, const double *&tval,
             const double *&tin) {
             trp = prp + (pass ? n : 0);

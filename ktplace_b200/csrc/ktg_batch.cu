@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
                 double w[1] = {0.0};
                 double pcur = 0.0;
                 warp_tile_spmv<double>(
-                    a, INT32_MAX, b - a, nullptr, wb, tilebuf,
+                    a, INT32_MAX, b - a, kAllAxes, wb, tilebuf,
                     [&](int, const int32_t *&trp, const int32_t *&tcol, const double *&tval,
                         const double *&tin) {
                         trp = rp;
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(1024) k_batch_pcg(BatchArgs A) {
                     double w[1] = {0.0};
                     float pcur = 0.0f;
                     warp_tile_spmv<float>(
-                        a, INT32_MAX, b - a, nullptr, wb, reinterpret_cast<float *>(tilebuf),
+                        a, INT32_MAX, b - a, kAllAxes, wb, reinterpret_cast<float *>(tilebuf),
                         [&](int, const int32_t *&trp, const int32_t *&tcol, const float *&tval,
                             const float *&tin) {
                             trp = rp;

@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
     // SpMV over this block's rows: out[l] = diag * in_own + A_off in_global.
     // `own` reads the row's own input element, `in` selects the gathered
     // vector per axis.
-    auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
+    auto spmv = [&](auto own, auto in_of, auto emit, unsigned live) {
         if (Lanes == 32) {
             double vcur = 0.0;
             warp_tile_spmv<double>(
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                 int axis;
                 int32_t i;
                 locate(l, axis, i);
-                if (live && !live[axis]) continue;
+                if (!((live >> axis) & 1u)) continue;
                 const PcgAxis &S = sax[axis];
                 const double d = __ldg(S.diag + i);
                 const double v = own(l, axis, i);
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                 int32_t i = 0;
                 bool valid = l < R;
                 if (valid) locate(l, axis, i);
-                if (valid && live && !live[axis]) valid = false;
+                if (valid && !((live >> axis) & 1u)) valid = false;
                 const PcgAxis &S = sax[axis];
                 const double s = row_offdiag_vec4(S, i, valid, in_of(axis));
                 if (valid && (threadIdx.x & 3) == 0) {
@@ -410,13 +410,17 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                      __stcg(prod_ptr(A, 0) + ci, b * b);
                      __stcg(prod_ptr(A, 1) + ci, r * z);
                      __stcg(prod_ptr(A, 2) + ci, r * r);
+                 } else if (axis) {
+                     acc[3] += b * b;
+                     acc[4] += r * z;
+                     acc[5] += r * r;
                  } else {
-                     acc[axis * 3 + 0] += b * b;
-                     acc[axis * 3 + 1] += r * z;
-                     acc[axis * 3 + 2] += r * r;
+                     acc[0] += b * b;
+                     acc[1] += r * z;
+                     acc[2] += r * r;
                  }
              },
-             nullptr);
+             kAllAxes);
         if constexpr (!Exact) {
             double v0[3] = {acc[0], acc[1], acc[2]};
             double v1[3] = {acc[3], acc[4], acc[5]};
@@ -484,16 +488,22 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                  },
                  [&](int axis) -> const double * { return sax[axis].z; },
                  [&](int32_t l, int axis, int32_t i, double zi, double w) {
+                     // per-axis values by select: no runtime array index, so
+                     // they stay in registers
                      double pn = zi, apn = w;
-                     if (!first_rec[axis]) {
-                         pn = zi + beta_rec[axis] * KTG_V(sp, p);
-                         apn = w + beta_rec[axis] * KTG_V(sap, ap);
+                     if (!(axis ? first_rec[1] : first_rec[0])) {
+                         const double be = axis ? beta_rec[1] : beta_rec[0];
+                         pn = zi + be * KTG_V(sp, p);
+                         apn = w + be * KTG_V(sap, ap);
                      }
                      KTG_V(sp, p) = pn;
                      KTG_V(sap, ap) = apn;
-                     pap_acc[axis] += pn * apn;
+                     if (axis)
+                         pap_acc[1] += pn * apn;
+                     else
+                         pap_acc[0] += pn * apn;
                  },
-                 live);
+                 axis_mask(live[0], live[1]));
         } else {
             spmv([&](int32_t l, int axis, int32_t i) {
                      return Smem ? sp[l] : __ldcg(sax[axis].p + i);
@@ -506,10 +516,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                          sax[axis].ap[i] = ap;
                      if constexpr (Exact)
                          __stcg(prod_ptr(A, 0) + (axis ? n0 + i : i), pi * ap);
+                     else if (axis)
+                         pap_acc[1] += pi * ap;
                      else
-                         pap_acc[axis] += pi * ap;
+                         pap_acc[0] += pi * ap;
                  },
-                 live);
+                 axis_mask(live[0], live[1]));
         }
         if constexpr (!Exact) {
             const int sl[2] = {kPAP, kPAP};
@@ -545,9 +557,9 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
             int axis;
             int32_t i;
             locate(l, axis, i);
-            if (!ok[axis]) continue;
+            if (!(axis ? ok[1] : ok[0])) continue;
             const PcgAxis &S = sax[axis];
-            const double a = alpha[axis];
+            const double a = axis ? alpha[1] : alpha[0];
             const double pi = KTG_V(sp, p);
             const double apv = KTG_V(sap, ap);
             const double d = __ldg(S.diag + i);
@@ -561,9 +573,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                 const int32_t ci = axis ? n0 + i : i;
                 __stcg(prod_ptr(A, 1) + ci, r * r);
                 __stcg(prod_ptr(A, 2) + ci, r * z);
+            } else if (axis) {
+                acc[2] += r * r;
+                acc[3] += r * z;
             } else {
-                acc[axis * 2 + 0] += r * r;
-                acc[axis * 2 + 1] += r * z;
+                acc[0] += r * r;
+                acc[1] += r * z;
             }
         }
         if constexpr (!Exact) {
@@ -604,8 +619,8 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg(PcgArgs A) {
                 int axis;
                 int32_t i;
                 locate(l, axis, i);
-                if (!ok2[axis]) continue;
-                const double pn = KTG_V(sz, z) + beta[axis] * KTG_V(sp, p);
+                if (!(axis ? ok2[1] : ok2[0])) continue;
+                const double pn = KTG_V(sz, z) + (axis ? beta[1] : beta[0]) * KTG_V(sp, p);
                 if (Smem) sp[l] = pn;
                 __stcg(sax[axis].p + i, pn);
             }
@@ -723,7 +738,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
         __syncthreads();
     }
 
-    auto spmv = [&](auto own, auto in_of, auto emit, const bool *live) {
+    auto spmv = [&](auto own, auto in_of, auto emit, unsigned live) {
         if (Lanes == 32) {
             double vcur = 0.0;
             warp_tile_spmv<double>(
@@ -746,7 +761,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
                 int axis;
                 int32_t i;
                 locate(l, axis, i);
-                if (live && !live[axis]) continue;
+                if (!((live >> axis) & 1u)) continue;
                 const PcgAxis &S = sax[axis];
                 const double d = Smem ? sd[l] : __ldg(S.diag + i);
                 const double v = own(l, axis, i);
@@ -762,7 +777,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
                 int32_t i = 0;
                 bool valid = l < R;
                 if (valid) locate(l, axis, i);
-                if (valid && live && !live[axis]) valid = false;
+                if (valid && !((live >> axis) & 1u)) valid = false;
                 const PcgAxis &S = sax[axis];
                 const double s = row_offdiag_vec4(S, i, valid, in_of(axis));
                 if (valid && (threadIdx.x & 3) == 0) {
@@ -792,11 +807,17 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
                      S.r[i] = r;
                  }
                  __stcg(S.z + i, z);
-                 acc[axis * 3 + 0] += b * b;
-                 acc[axis * 3 + 1] += r * z;
-                 acc[axis * 3 + 2] += r * r;
+                 if (axis) {
+                     acc[3] += b * b;
+                     acc[4] += r * z;
+                     acc[5] += r * r;
+                 } else {
+                     acc[0] += b * b;
+                     acc[1] += r * z;
+                     acc[2] += r * r;
+                 }
              },
-             nullptr);
+             kAllAxes);
         double v0[3] = {acc[0], acc[1], acc[2]};
         double v1[3] = {acc[3], acc[4], acc[5]};
         const int sl[3] = {kBB, kRZ0, kRR0};
@@ -872,9 +893,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
                      sw[l] = w;
                  else
                      sax[axis].ap[i] = w;
-                 wz[axis] += w * zi;
+                 if (axis)
+                     wz[1] += w * zi;
+                 else
+                     wz[0] += w * zi;
              },
-             live);
+             axis_mask(live[0], live[1]));
         {
             const int sl[2] = {kPAP, kPAP};
             const int ax[2] = {0, 1};
@@ -909,16 +933,17 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
             int axis;
             int32_t i;
             locate(l, axis, i);
-            if (!ok[axis]) continue;
+            if (!(axis ? ok[1] : ok[0])) continue;
             const PcgAxis &S = sax[axis];
             const double zi = KTG_V(sz, z);
             const double wi = Smem ? sw[l] : S.ap[i];
-            const bool f = first[axis];
-            const double pn = f ? zi : zi + beta[axis] * KTG_V(sp, p);
-            const double sn = f ? wi : wi + beta[axis] * KTG_V(ss, s);
+            const bool f = axis ? first[1] : first[0];
+            const double be = axis ? beta[1] : beta[0];
+            const double pn = f ? zi : zi + be * KTG_V(sp, p);
+            const double sn = f ? wi : wi + be * KTG_V(ss, s);
             KTG_V(sp, p) = pn;
             KTG_V(ss, s) = sn;
-            const double a = alpha[axis];
+            const double a = axis ? alpha[1] : alpha[0];
             KTG_V(sx, x) += a * pn;
             const double r = KTG_V(sr, r) - a * sn;
             const double d = Smem ? sd[l] : __ldg(S.diag + i);
@@ -926,8 +951,13 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cg(PcgArgs A) {
             KTG_V(sr, r) = r;
             if (Smem) sz[l] = z;
             __stcg(S.z + i, z);
-            acc[axis * 2 + 0] += r * r;
-            acc[axis * 2 + 1] += r * z;
+            if (axis) {
+                acc[2] += r * r;
+                acc[3] += r * z;
+            } else {
+                acc[0] += r * r;
+                acc[1] += r * z;
+            }
         }
         {
             const int sl[4] = {kRR, kRZ, kRR, kRZ};

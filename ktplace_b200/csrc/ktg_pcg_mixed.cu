@@ -507,13 +507,13 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
 
     // u = M r for own rows with the aggregation preconditioner: the block
     // inverse row of each row times r over its aggregate (own slice).
-    auto apply_blocks = [&](const bool *live) {
+    auto apply_blocks = [&](unsigned live) {
         __syncthreads();
         for (int32_t l = threadIdx.x; l < R; l += blockDim.x) {
             int axis;
             int32_t i;
             locate(l, axis, i);
-            if (!live[axis]) continue;
+            if (!((live >> axis) & 1u)) continue;
             const MixAxis &S = sax[axis];
             const int32_t meta = __ldg(S.meta + i);
             const int k = (meta & 7) + 1;
@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
     // u = M r for own rows (learned M), reading the published D^-1/2 r: the
     // sum over A's pattern runs as warp tiles, adding in the order and with
     // the roundings of apply_m_row.
-    auto apply_m = [&](const bool *live) {
+    auto apply_m = [&](unsigned live) {
         warp_tile_spmv<float>(
             r0, n0, R, live, wb, tile32,
             [&](int pass, const int32_t *&rp, const int32_t *&col, const float *&val,
@@ -566,7 +566,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
             // rr x, bb x, rr y, bb y, z.r x, z.r y
             double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             warp_tile_spmv<double>(
-                r0, n0, R, nullptr, wb, tile64,
+                r0, n0, R, kAllAxes, wb, tile64,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const double *&val,
                     const double *&in) {
                     rp = sax[pass].rp;
@@ -589,14 +589,18 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                         su[l] = u;
                         __stcg(S.z + i, u);
                     }
-                    acc[axis * 2 + 0] += r * r;
-                    acc[axis * 2 + 1] += b * b;
-                    if (coarse) acc[4 + axis] += static_cast<double>(szaz[l].x) * r;
+                    const double zr = coarse ? static_cast<double>(szaz[l].x) * r : 0.0;
+                    if (axis) {  // per-axis sums in registers (no runtime array index)
+                        acc[2] += r * r;
+                        acc[3] += b * b;
+                        acc[5] += zr;
+                    } else {
+                        acc[0] += r * r;
+                        acc[1] += b * b;
+                        acc[4] += zr;
+                    }
                 });
-            if (PRE == kPreAgg) {
-                const bool all[2] = {true, true};
-                apply_blocks(all);
-            }
+            if (PRE == kPreAgg) apply_blocks(kAllAxes);
             const int sl[6] = {kTRR, kTBB, kTRR, kTBB, kTZR, kTZR};
             const int ax[6] = {0, 0, 1, 1, 0, 1};
             mstore<6>(A, acc, sl, ax, scratch);
@@ -644,7 +648,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
         }
         if (!(live[0] || live[1])) break;
         if (pre) {
-            apply_m(live);
+            apply_m(axis_mask(live[0], live[1]));
             if (!sync()) return;
         }
         // ---- inner FP32 PCG (Chronopoulos-Gear) -------------------------------
@@ -659,7 +663,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
             // gamma, delta, rr, z.w per axis
             double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             warp_tile_spmv<float>(
-                r0, n0, R, in_live, wb, tile32,
+                r0, n0, R, axis_mask(in_live[0], in_live[1]), wb, tile32,
                 [&](int pass, const int32_t *&rp, const int32_t *&col, const float *&val,
                     const float *&in) {
                     rp = sax[pass].rp;
@@ -672,17 +676,30 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 },
                 [&](int32_t l, int axis, int32_t, float w) {
                     float ui = su[l];
+                    double zw = 0.0;
                     if (coarse) {  // A (u_b + z c) = A u_b + (A z) c
                         const float2 za = szaz[l];
-                        ui += za.x * cu[axis];
-                        w += za.y * cu[axis];
-                        acc[axis * 4 + 3] += static_cast<double>(za.x) * w;
+                        const float c = axis ? cu[1] : cu[0];
+                        ui += za.x * c;
+                        w += za.y * c;
+                        zw = static_cast<double>(za.x) * w;
                     }
                     sw[l] = w;
                     const float r = sr[l];
-                    acc[axis * 4 + 0] += static_cast<double>(r) * ui;
-                    acc[axis * 4 + 1] += static_cast<double>(w) * ui;
-                    acc[axis * 4 + 2] += static_cast<double>(r) * r;
+                    const double g = static_cast<double>(r) * ui;
+                    const double d = static_cast<double>(w) * ui;
+                    const double rr = static_cast<double>(r) * r;
+                    if (axis) {  // per-axis sums in registers (no runtime array index)
+                        acc[4] += g;
+                        acc[5] += d;
+                        acc[6] += rr;
+                        acc[7] += zw;
+                    } else {
+                        acc[0] += g;
+                        acc[1] += d;
+                        acc[2] += rr;
+                        acc[3] += zw;
+                    }
                 });
             if (coarse) {  // one block sum for both axes (each value summed as alone)
                 const int sl[8] = {kIRZ, kIPAP, kIRR, kIZW, kIRZ, kIPAP, kIRR, kIZW};
@@ -751,16 +768,18 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                 int axis;
                 int32_t i;
                 locate(l, axis, i);
-                if (!ok[axis]) continue;
+                if (!(axis ? ok[1] : ok[0])) continue;
                 const MixAxis &S = sax[axis];
-                const bool f = first[axis];
-                const float ui = coarse ? su[l] + szaz[l].x * cu[axis] : su[l];
-                const float pn = f ? ui : ui + beta[axis] * sp[l];
-                const float sn = f ? sw[l] : sw[l] + beta[axis] * ss[l];
+                const bool f = axis ? first[1] : first[0];
+                const float al = axis ? alpha[1] : alpha[0];
+                const float be = axis ? beta[1] : beta[0];
+                const float ui = coarse ? su[l] + szaz[l].x * (axis ? cu[1] : cu[0]) : su[l];
+                const float pn = f ? ui : ui + be * sp[l];
+                const float sn = f ? sw[l] : sw[l] + be * ss[l];
                 sp[l] = pn;
                 ss[l] = sn;
-                sdd[l] += alpha[axis] * pn;
-                const float r = sr[l] - alpha[axis] * sn;
+                sdd[l] += al * pn;
+                const float r = sr[l] - al * sn;
                 sr[l] = r;
                 if (pre) {
                     __stcg(S.rs + i, r * rsqrtf(static_cast<float>(__ldg(S.diag + i))));
@@ -770,7 +789,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
                     __stcg(S.z + i, u);
                 }
             }
-            if (PRE == kPreAgg) apply_blocks(ok);
+            if (PRE == kPreAgg) apply_blocks(axis_mask(ok[0], ok[1]));
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
                 if (!ok[a]) continue;
@@ -781,7 +800,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
             if (!sync()) return;
             stamp(6);
             if (pre) {
-                apply_m(ok);
+                apply_m(axis_mask(ok[0], ok[1]));
                 if (!sync()) return;
             }
         }
@@ -790,7 +809,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_pcg_mixed_cg(MixArgs A) {
             int axis;
             int32_t i;
             locate(l, axis, i);
-            if (!live[axis]) continue;
+            if (!(axis ? live[1] : live[0])) continue;
             sx[l] += static_cast<double>(sdd[l]);
             sax[axis].x[i] = sx[l];
         }

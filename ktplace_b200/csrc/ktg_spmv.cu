@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(kSpmvThreads)
         return int64_t(__ldg(rp + r0 + l)) - base + int64_t(kRowCost) * l;
     });
     warp_tile_spmv<double>(
-        r0, INT32_MAX, R, nullptr, wb, tilebuf,
+        r0, INT32_MAX, R, kAllAxes, wb, tilebuf,
         [&](int, const int32_t *&trp, const int32_t *&tcol, const double *&tval,
             const double *&tin) {
             trp = rp;

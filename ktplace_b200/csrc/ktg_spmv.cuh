@@ -66,10 +66,18 @@ __device__ __forceinline__ void warp_row_bounds(int32_t R, int32_t *wb, Cost cos
     __syncthreads();
 }
 
+// Per-axis flags as a bit mask (bit a: axis a), passed by value so that a
+// kernel's flags stay in registers (a bool array indexed by a runtime axis
+// would live in local memory).
+constexpr unsigned kAllAxes = 3u;
+__device__ __forceinline__ unsigned axis_mask(bool a0, bool a1) {
+    return (a0 ? 1u : 0u) | (a1 ? 2u : 0u);
+}
+
 // Rows [r0, r0 + R) of a block's slice of the combined row space
 // [axis 0 rows | axis 1 rows] (axis 1 starts at row n0); rows of an axis
-// with live[axis] false are skipped (live may be null). All threads of the
-// block call it.
+// whose bit in `live` is clear are skipped. All threads of the block call
+// it.
 //   wb: per-warp row ranges from warp_row_bounds, or null for tiles dealt
 //       to the warps in turn (warp w takes tiles w, w + nw, ...);
 //   csr(pass, rp, col, val, in): the axis's CSR arrays and gathered vector;
@@ -77,7 +85,7 @@ __device__ __forceinline__ void warp_row_bounds(int32_t R, int32_t *wb, Cost cos
 //   emit(l, pass, i, sum): the finished row sum.
 // tilebuf holds kTileChunk elements per warp, 16-byte aligned.
 template <typename T, class Csr, class Start, class Emit>
-__device__ __forceinline__ void warp_tile_spmv(int32_t r0, int32_t n0, int32_t R, const bool *live,
+__device__ __forceinline__ void warp_tile_spmv(int32_t r0, int32_t n0, int32_t R, unsigned live,
                                                const int32_t *wb, T *tilebuf, Csr csr, Start start,
                                                Emit emit) {
     using P2 = typename TilePair<T>::type;
@@ -93,7 +101,7 @@ __device__ __forceinline__ void warp_tile_spmv(int32_t r0, int32_t n0, int32_t R
         const int32_t c = r0 + l;
         const int axis = c >= n0 ? 1 : 0;
         const int32_t i = c - (axis ? n0 : 0);
-        const bool mine = l < end && (!live || live[axis]);
+        const bool mine = l < end && ((live >> axis) & 1u);
         // a tile that straddles the axis boundary takes one pass per axis
 #pragma unroll 1
         for (int pass = 0; pass < 2; ++pass) {
