@@ -260,7 +260,7 @@ def spmv_bytes(n: int, m: int) -> float:
 # DRAM bytes (read + write) per launch of the dominant kernel on this
 # workload, from an ncu capture of bench.py --profile-once (dram__bytes_read.sum +
 # dram__bytes_write.sum of the k_pcg launch).
-NCU_TRAFFIC_BYTES = {"k_pcg": 111.045376e6 + 41.966848e6}
+NCU_TRAFFIC_BYTES = {"k_pcg": 100.221184e6 + 14.856192e6}
 
 
 def measured_peak():
@@ -469,7 +469,7 @@ def run_ours(args):
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": NCU_TRAFFIC_BYTES["k_pcg"], "algorithmic_bytes": byts,
                          "note": "working set is L2-resident: traffic << algorithmic bytes",
-                         "limiter": "L1TEX data pipe: 56% of peak over the whole solve in the ncu "
+                         "limiter": "L1TEX data pipe: 57% of peak over the whole solve in the ncu "
                                     "capture (random 8-byte gathers, one LSU wavefront each); "
                                     "L2 39%, DRAM 0.2% (ncu of bench.py --profile-once)"},
             "cpu_baseline": cpu,
